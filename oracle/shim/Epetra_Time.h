@@ -1,0 +1,2 @@
+/* Oracle shim: forwards to the single-rank stand-ins. */
+#include "shim_trilinos.h"
