@@ -1,0 +1,699 @@
+// engine.cu -- context, device-table upload and the C ABI of include/mcb200.h.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "engine_kernels.h"
+#include "flight_physics.cuh"
+#include "fullband_tables.h"
+#include "mcb200.h"
+
+using namespace mcb200;
+
+namespace {
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+void ck(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+T *dalloc(size_t n, std::vector<void *> &owned) {
+  void *p = nullptr;
+  ck(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)), "cudaMalloc");
+  owned.push_back(p);
+  return static_cast<T *>(p);
+}
+
+template <typename T>
+T *dupload(const std::vector<T> &v, std::vector<void *> &owned) {
+  T *p = dalloc<T>(v.size(), owned);
+  if (!v.empty()) ck(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload table");
+  return p;
+}
+
+struct ParticleBuffers {
+  DevParticles d{};
+  void alloc(size_t cap, std::vector<void *> &owned) {
+    d.x = dalloc<double>(cap, owned); d.y = dalloc<double>(cap, owned); d.z = dalloc<double>(cap, owned);
+    d.kx = dalloc<double>(cap, owned); d.ky = dalloc<double>(cap, owned); d.kz = dalloc<double>(cap, owned);
+    d.energy = dalloc<double>(cap, owned); d.charge = dalloc<double>(cap, owned);
+    d.cell = dalloc<uint32_t>(cap, owned); d.itet = dalloc<int32_t>(cap, owned);
+    d.meta = dalloc<uint32_t>(cap, owned); d.uid = dalloc<uint32_t>(cap, owned);
+  }
+};
+
+struct ChildBuffers {
+  DevChildren d{};
+  void alloc(int cap, std::vector<void *> &owned) {
+    d.x = dalloc<double>(cap, owned); d.y = dalloc<double>(cap, owned); d.z = dalloc<double>(cap, owned);
+    d.kx = dalloc<double>(cap, owned); d.ky = dalloc<double>(cap, owned); d.kz = dalloc<double>(cap, owned);
+    d.energy = dalloc<double>(cap, owned); d.charge = dalloc<double>(cap, owned);
+    d.left_time = dalloc<double>(cap, owned);
+    d.cell = dalloc<uint32_t>(cap, owned); d.itet = dalloc<int32_t>(cap, owned);
+    d.meta = dalloc<uint32_t>(cap, owned);
+    d.parent_uid = dalloc<uint32_t>(cap, owned); d.sub = dalloc<uint32_t>(cap, owned);
+    d.count = dalloc<unsigned int>(1, owned);
+    d.capacity = cap;
+  }
+};
+
+}  // namespace
+
+struct mcb200_ctx {
+  std::string error;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<void *> owned;   // every cudaMalloc of the context
+  std::vector<void *> mesh_owned;
+  FullBandTables tab;
+  DevTables dt{};
+  DevMesh mesh{};
+  bool mesh_set = false, cells_set = false, fields_set = false;
+  std::vector<double> hlx, hly, hlz;
+  // particles: two buffers, the store ping-pongs through the cell sort
+  size_t capacity = 0;
+  ParticleBuffers pb[2];
+  int cur = 0;
+  size_t n = 0;
+  uint32_t next_uid = 0;
+  // mid-step copies: one buffer per generation
+  static constexpr int kGenerations = 4;
+  ChildBuffers cb[kGenerations];
+  int child_cap = 0;
+  uint64_t *child_keys = nullptr;
+  uint8_t *child_alive = nullptr;
+  uint32_t *child_uids = nullptr;
+  unsigned int *append_count = nullptr;
+  // tallies
+  DevTallies y{};
+  // sort scratch
+  unsigned int *hist = nullptr, *offsets = nullptr, *tile_sums = nullptr, *total = nullptr;
+  int ncells = 0;
+  unsigned int *h_pinned = nullptr;  // small pinned readback area
+  int sm_count = 148;
+
+  ~mcb200_ctx() {
+    if (device < 0) return;
+    cudaSetDevice(device);
+    for (void *p : mesh_owned) cudaFree(p);
+    for (void *p : owned) cudaFree(p);
+    if (h_pinned) cudaFreeHost(h_pinned);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+int fail(mcb200_ctx *c, int code, const std::string &msg) {
+  if (c) c->error = msg;
+  return code;
+}
+
+// Uniform k-space locator for the tetrahedron search (see flight_physics.cuh).
+void build_kgrid(mcb200_ctx *c, int g) {
+  const FullBandTables &t = c->tab;
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int i = 0; i < t.nk; ++i) {
+    const double v[3] = {t.xkk[i], t.ykk[i], t.zkk[i]};
+    for (int a = 0; a < 3; ++a) { lo[a] = std::min(lo[a], v[a]); hi[a] = std::max(hi[a], v[a]); }
+  }
+  const double pad = 1e-9 * t.u.a0pi;
+  for (int a = 0; a < 3; ++a) { lo[a] -= pad; hi[a] += pad; }
+  double inv[3];
+  for (int a = 0; a < 3; ++a) inv[a] = g / (hi[a] - lo[a]);
+  const int cells = g * g * g;
+  std::vector<std::vector<int>> lists((size_t)kMNB * cells);
+  for (int it = t.nt - 1; it >= 0; --it) {  // descending tet order inside each cell
+    double blo[3] = {1e300, 1e300, 1e300}, bhi[3] = {-1e300, -1e300, -1e300};
+    for (int v = 0; v < 4; ++v) {
+      const int nd = t.T(v, it);
+      const double p[3] = {t.xkk[nd], t.ykk[nd], t.zkk[nd]};
+      for (int a = 0; a < 3; ++a) { blo[a] = std::min(blo[a], p[a]); bhi[a] = std::max(bhi[a], p[a]); }
+    }
+    int c0[3], c1[3];
+    for (int a = 0; a < 3; ++a) {
+      c0[a] = std::max(0, std::min(g - 1, (int)std::floor((blo[a] - pad - lo[a]) * inv[a])));
+      c1[a] = std::max(0, std::min(g - 1, (int)std::floor((bhi[a] + pad - lo[a]) * inv[a])));
+    }
+    for (int i = c0[0]; i <= c1[0]; ++i)
+      for (int j = c0[1]; j <= c1[1]; ++j)
+        for (int k = c0[2]; k <= c1[2]; ++k) lists[(size_t)t.ibt[it] * cells + (i * g + j) * g + k].push_back(it);
+  }
+  std::vector<int> start((size_t)kMNB * (cells + 1)), tets;
+  for (int b = 0; b < kMNB; ++b) {
+    int *st = &start[(size_t)b * (cells + 1)];
+    for (int q = 0; q < cells; ++q) {
+      st[q] = (int)tets.size();
+      const auto &l = lists[(size_t)b * cells + q];
+      tets.insert(tets.end(), l.begin(), l.end());
+    }
+    st[cells] = (int)tets.size();
+  }
+  c->dt.grid_n = g;
+  for (int a = 0; a < 3; ++a) { c->dt.grid_lo[a] = lo[a]; c->dt.grid_inv[a] = inv[a]; }
+  c->dt.grid_start = dupload(start, c->owned);
+  c->dt.grid_tets = dupload(tets, c->owned);
+}
+
+void upload_tables(mcb200_ctx *c) {
+  const FullBandTables &t = c->tab;
+  DevTables &d = c->dt;
+  d.nt = t.nt; d.nk = t.nk; d.nbt = t.nbt;
+  for (int i = 0; i < 3; ++i) { d.nband[i] = t.nband[i]; d.bandof[i] = t.bandof[i]; d.difpr[i] = t.difpr[i]; }
+  d.scpre = t.scpre; d.scprh = t.scprh;
+  d.dtable = t.dtable; d.emax = t.emax; d.dlist = t.dlist; d.dlists = t.dlists;
+  d.temptag = t.temptag; d.templag = t.templag; d.templog = t.templog;
+  d.temptaf = t.temptaf; d.templaf = t.templaf; d.temptof = t.temptof; d.temphop = t.temphop;
+  d.mell = t.mell; d.melt = t.melt; d.meld = t.meld;
+  d.a0pi = t.u.a0pi; d.sieg = t.u.sieg; d.eV0 = t.u.eV0; d.conc0 = t.u.conc0; d.scrt0 = t.u.scrt0;
+  d.eps_si = t.u.eps_silicon; d.frickel = t.u.frickel;
+  std::vector<TetFlight> tf(t.nt);
+  std::vector<TetShape> ts(t.nt);
+  std::vector<int4> tn(t.nt), tb(t.nt);
+  for (int it = 0; it < t.nt; ++it) {
+    for (int f = 0; f < 4; ++f)
+      for (int cc = 0; cc < 4; ++cc) tf[it].n[f][cc] = t.D(cc, f, it);
+    for (int cc = 0; cc < 4; ++cc) tf[it].v[cc] = t.vt[(size_t)4 * it + cc];
+    for (int v = 0; v < 4; ++v) ts[it].e[v] = t.eek[t.T(v, it)];
+    ts[it].fac[0] = t.faclow[it]; ts[it].fac[1] = t.facmedium[it]; ts[it].fac[2] = t.fachigh[it];
+    ts[it].vgt = t.vgt[it];
+    tn[it] = make_int4(t.T(0, it), t.T(1, it), t.T(2, it), t.T(3, it));
+    tb[it] = make_int4(t.N(0, it), t.N(1, it), t.N(2, it), t.N(3, it));
+  }
+  d.tf = dupload(tf, c->owned);
+  d.ts = dupload(ts, c->owned);
+  d.tnode = dupload(tn, c->owned);
+  d.tneib = dupload(tb, c->owned);
+  d.ibt = dupload(t.ibt, c->owned);
+  d.gamtet = dupload(t.gamtet, c->owned);
+  std::vector<double4> kn(t.nk);
+  for (int i = 0; i < t.nk; ++i) kn[i] = make_double4(t.xkk[i], t.ykk[i], t.zkk[i], t.eek[i]);
+  d.knode = dupload(kn, c->owned);
+  d.energy = dupload(t.energy, c->owned);
+  d.sumscatt = dupload(t.sumscatt, c->owned);
+  d.scatte = dupload(t.scatte, c->owned);
+  d.dose = dupload(t.dose, c->owned);
+  d.scattiie = dupload(t.scattiie, c->owned);
+  d.scatth = dupload(t.scatth, c->owned);
+  d.dosh = dupload(t.dosh, c->owned);
+  d.scattiih = dupload(t.scattiih, c->owned);
+  d.dostetmax = dupload(t.dostetmax, c->owned);
+  d.ntlist = dupload(t.ntlist, c->owned); d.ptlist = dupload(t.ptlist, c->owned); d.tlist = dupload(t.tlist, c->owned);
+  d.nslist = dupload(t.nslist, c->owned); d.pslist = dupload(t.pslist, c->owned); d.slist = dupload(t.slist, c->owned);
+  d.ntlists = dupload(t.ntlists, c->owned); d.ptlists = dupload(t.ptlists, c->owned); d.tlists = dupload(t.tlists, c->owned);
+  std::vector<int> symi(48 * 6), newisym(5 * 48), indmat(t.indmat, t.indmat + 729), refl(3 * 48);
+  std::vector<double> bz(3 * 5 * 48);
+  for (int s = 0; s < 48; ++s)
+    for (int cc = 0; cc < 6; ++cc) symi[s * 6 + cc] = t.matsym[cc][s];
+  for (int iv = 0; iv < 5; ++iv)
+    for (int s = 0; s < 48; ++s) {
+      newisym[iv * 48 + s] = t.newisym[iv][s];
+      bz[(0 * 5 + iv) * 48 + s] = t.xbz[iv][s];
+      bz[(1 * 5 + iv) * 48 + s] = t.ybz[iv][s];
+      bz[(2 * 5 + iv) * 48 + s] = t.zbz[iv][s];
+    }
+  // Reflect / Diffuse mirror tables: isym after negating k_x, k_y or k_z
+  // (src/CellHit.cpp:217-238, the indmat lookups with one sign flipped).
+  for (int axis = 0; axis < 3; ++axis)
+    for (int s = 0; s < 48; ++s) {
+      int sg[3] = {t.matsym[3][s], t.matsym[4][s], t.matsym[5][s]};
+      sg[axis] = -sg[axis];
+      const int idx = (((((sg[0] + 1) * 3 + (sg[1] + 1)) * 3 + (sg[2] + 1)) * 3 + (t.matsym[0][s] - 1)) * 3 +
+                       (t.matsym[1][s] - 1)) * 3 + (t.matsym[2][s] - 1);
+      refl[axis * 48 + s] = t.indmat[idx];
+    }
+  d.symi = dupload(symi, c->owned);
+  d.newisym = dupload(newisym, c->owned);
+  d.bz = dupload(bz, c->owned);
+  d.indmat = dupload(indmat, c->owned);
+  d.reflect_isym = dupload(refl, c->owned);
+  build_kgrid(c, 40);
+}
+
+template <typename T>
+void copy_vec(const std::vector<T> &v, void *out, size_t bytes, size_t *needed) {
+  *needed = v.size() * sizeof(T);
+  if (out && bytes >= *needed) std::memcpy(out, v.data(), *needed);
+}
+
+int grid_for(const mcb200_ctx *c, size_t n, int block) {
+  const size_t want = (n + block - 1) / block;
+  const size_t cap = (size_t)c->sm_count * 8;
+  return (int)std::max<size_t>(1, std::min(want, cap));
+}
+
+void free_mesh(mcb200_ctx *c) {
+  for (void *p : c->mesh_owned) cudaFree(p);
+  c->mesh_owned.clear();
+}
+
+}  // namespace
+
+extern "C" {
+
+int mcb200_create(const char *table_dir, double kelvin, int device, size_t max_particles, mcb200_ctx **out) {
+  if (!out || !table_dir || max_particles == 0) return MCB200_ERR_ARG;
+  *out = nullptr;
+  mcb200_ctx *c = new mcb200_ctx;
+  c->device = device;
+  try {
+    c->tab = FullBandTables::build(table_dir, kelvin);
+  } catch (const std::exception &e) {
+    c->device = -1;
+    int code = fail(c, MCB200_ERR_IO, e.what());
+    *out = c;
+    return code;
+  }
+  if (device < 0) {  // host-only context: tables are built, nothing is uploaded
+    *out = c;
+    return MCB200_OK;
+  }
+  try {
+    ck(cudaSetDevice(device), "cudaSetDevice");
+    ck(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    ck(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device), "device attribute");
+    upload_tables(c);
+    c->capacity = max_particles;
+    c->pb[0].alloc(max_particles, c->owned);
+    c->pb[1].alloc(max_particles, c->owned);
+    c->child_cap = (int)std::min<size_t>(std::max<size_t>(max_particles / 8, 4096), 1u << 22);
+    for (int g = 0; g < mcb200_ctx::kGenerations; ++g) c->cb[g].alloc(c->child_cap, c->owned);
+    const size_t all_children = (size_t)c->child_cap * mcb200_ctx::kGenerations;
+    c->child_keys = dalloc<uint64_t>(all_children, c->owned);
+    c->child_alive = dalloc<uint8_t>(all_children, c->owned);
+    c->child_uids = dalloc<uint32_t>(all_children, c->owned);
+    c->append_count = dalloc<unsigned int>(1, c->owned);
+    c->y.counters = dalloc<unsigned long long>(kCntNumCounters, c->owned);
+    c->y.contact = dalloc<long long>(kMaxContacts * 6, c->owned);
+    c->total = dalloc<unsigned int>(1, c->owned);
+    ck(cudaMallocHost(&c->h_pinned, 64 * sizeof(unsigned int)), "cudaMallocHost");
+    ck(cudaMemsetAsync(c->y.counters, 0, sizeof(unsigned long long) * kCntNumCounters, c->stream), "memset");
+    ck(cudaMemsetAsync(c->y.contact, 0, sizeof(long long) * kMaxContacts * 6, c->stream), "memset");
+    ck(cudaStreamSynchronize(c->stream), "sync");
+  } catch (const std::exception &e) {
+    int code = fail(c, MCB200_ERR_CUDA, e.what());
+    *out = c;
+    return code;
+  }
+  *out = c;
+  return MCB200_OK;
+}
+
+void mcb200_destroy(mcb200_ctx *ctx) { delete ctx; }
+
+const char *mcb200_last_error(const mcb200_ctx *ctx) { return ctx ? ctx->error.c_str() : "null context"; }
+
+int mcb200_units(const mcb200_ctx *c, double *out, int n) {
+  if (!c || !out) return MCB200_ERR_ARG;
+  const Units &u = c->tab.u;
+  const double v[14] = {u.T0, u.eV0, u.spr0, u.time0, u.conc0, u.field0, u.scrt0,
+                        u.pot0, u.a0pi, u.sieg, u.eps_silicon, u.eps_oxide, u.curr0, u.dens0};
+  for (int i = 0; i < n && i < 14; ++i) out[i] = v[i];
+  return MCB200_OK;
+}
+
+int mcb200_copy_table(const mcb200_ctx *c, const char *name, void *out, size_t bytes, size_t *needed) {
+  if (!c || !name || !needed) return MCB200_ERR_ARG;
+  const FullBandTables &t = c->tab;
+  const std::string n(name);
+  std::vector<int> iv;
+  std::vector<double> dv;
+  if (n == "gamtet") { copy_vec(t.gamtet, out, bytes, needed); return 0; }
+  if (n == "vt") { copy_vec(t.vt, out, bytes, needed); return 0; }
+  if (n == "vgt") { copy_vec(t.vgt, out, bytes, needed); return 0; }
+  if (n == "datantlin") { copy_vec(t.datantlin, out, bytes, needed); return 0; }
+  if (n == "faclow") { copy_vec(t.faclow, out, bytes, needed); return 0; }
+  if (n == "facmedium") { copy_vec(t.facmedium, out, bytes, needed); return 0; }
+  if (n == "fachigh") { copy_vec(t.fachigh, out, bytes, needed); return 0; }
+  if (n == "tet") { copy_vec(t.tet, out, bytes, needed); return 0; }
+  if (n == "NeibrTet") { copy_vec(t.neib, out, bytes, needed); return 0; }
+  if (n == "ibt") { copy_vec(t.ibt, out, bytes, needed); return 0; }
+  if (n == "xkk") { copy_vec(t.xkk, out, bytes, needed); return 0; }
+  if (n == "ykk") { copy_vec(t.ykk, out, bytes, needed); return 0; }
+  if (n == "zkk") { copy_vec(t.zkk, out, bytes, needed); return 0; }
+  if (n == "eek") { copy_vec(t.eek, out, bytes, needed); return 0; }
+  if (n == "ntlist") { copy_vec(t.ntlist, out, bytes, needed); return 0; }
+  if (n == "ptlist") { copy_vec(t.ptlist, out, bytes, needed); return 0; }
+  if (n == "tlist") { copy_vec(t.tlist, out, bytes, needed); return 0; }
+  if (n == "nslist") { copy_vec(t.nslist, out, bytes, needed); return 0; }
+  if (n == "pslist") { copy_vec(t.pslist, out, bytes, needed); return 0; }
+  if (n == "slist") { copy_vec(t.slist, out, bytes, needed); return 0; }
+  if (n == "ntlists") { copy_vec(t.ntlists, out, bytes, needed); return 0; }
+  if (n == "ptlists") { copy_vec(t.ptlists, out, bytes, needed); return 0; }
+  if (n == "tlists") { copy_vec(t.tlists, out, bytes, needed); return 0; }
+  if (n == "dos") { copy_vec(t.dos, out, bytes, needed); return 0; }
+  if (n == "sumdos") { copy_vec(t.sumdos, out, bytes, needed); return 0; }
+  if (n == "dostetmax") { copy_vec(t.dostetmax, out, bytes, needed); return 0; }
+  if (n == "sumscatt") { copy_vec(t.sumscatt, out, bytes, needed); return 0; }
+  if (n == "scatte") { copy_vec(t.scatte, out, bytes, needed); return 0; }
+  if (n == "dose") { copy_vec(t.dose, out, bytes, needed); return 0; }
+  if (n == "scattiie") { copy_vec(t.scattiie, out, bytes, needed); return 0; }
+  if (n == "scatth") { copy_vec(t.scatth, out, bytes, needed); return 0; }
+  if (n == "dosh") { copy_vec(t.dosh, out, bytes, needed); return 0; }
+  if (n == "scattiih") { copy_vec(t.scattiih, out, bytes, needed); return 0; }
+  if (n == "energy") { copy_vec(t.energy, out, bytes, needed); return 0; }
+  if (n == "matsym") { iv.assign(&t.matsym[0][0], &t.matsym[0][0] + 6 * 48); copy_vec(iv, out, bytes, needed); return 0; }
+  if (n == "indmat") { iv.assign(t.indmat, t.indmat + 729); copy_vec(iv, out, bytes, needed); return 0; }
+  if (n == "newisym") { iv.assign(&t.newisym[0][0], &t.newisym[0][0] + 5 * 48); copy_vec(iv, out, bytes, needed); return 0; }
+  if (n == "xbz") { dv.assign(&t.xbz[0][0], &t.xbz[0][0] + 5 * 48); copy_vec(dv, out, bytes, needed); return 0; }
+  if (n == "ybz") { dv.assign(&t.ybz[0][0], &t.ybz[0][0] + 5 * 48); copy_vec(dv, out, bytes, needed); return 0; }
+  if (n == "zbz") { dv.assign(&t.zbz[0][0], &t.zbz[0][0] + 5 * 48); copy_vec(dv, out, bytes, needed); return 0; }
+  return fail(const_cast<mcb200_ctx *>(c), MCB200_ERR_ARG, "unknown table " + n);
+}
+
+int mcb200_set_mesh(mcb200_ctx *c, int nx, int ny, int nz, const double *lx, const double *ly, const double *lz) {
+  if (c && c->device < 0) return fail(c, MCB200_ERR_STATE, "host-only context");
+  if (!c || nx <= 0 || ny <= 0 || nz <= 0 || nx > 1023 || ny > 1023 || nz > 1023 || !lx || !ly || !lz)
+    return c ? fail(c, MCB200_ERR_ARG, "bad mesh") : MCB200_ERR_ARG;
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    ck(cudaStreamSynchronize(c->stream), "sync");
+    free_mesh(c);
+    c->hlx.assign(lx, lx + nx + 1);
+    c->hly.assign(ly, ly + ny + 1);
+    c->hlz.assign(lz, lz + nz + 1);
+    std::vector<double> dx(nx), dy(ny), dz(nz);
+    for (int i = 0; i < nx; ++i) dx[i] = c->hlx[i + 1] - c->hlx[i];
+    for (int i = 0; i < ny; ++i) dy[i] = c->hly[i + 1] - c->hly[i];
+    for (int i = 0; i < nz; ++i) dz[i] = c->hlz[i + 1] - c->hlz[i];
+    DevMesh &m = c->mesh;
+    m = DevMesh{};
+    m.nx = nx; m.ny = ny; m.nz = nz;
+    m.lx = dupload(c->hlx, c->mesh_owned); m.ly = dupload(c->hly, c->mesh_owned); m.lz = dupload(c->hlz, c->mesh_owned);
+    m.dx = dupload(dx, c->mesh_owned); m.dy = dupload(dy, c->mesh_owned); m.dz = dupload(dz, c->mesh_owned);
+    const size_t cells = (size_t)nx * ny * nz, nodes = (size_t)(nx + 1) * (ny + 1) * (nz + 1);
+    c->ncells = (int)cells;
+    m.motion = dalloc<int>(cells * 6, c->mesh_owned);
+    m.contact = dalloc<int>(cells, c->mesh_owned);
+    m.in_surf = dalloc<int>(cells, c->mesh_owned);
+    m.nearest_surf = dalloc<int>(cells, c->mesh_owned);
+    m.efield = dalloc<double>(cells * 3, c->mesh_owned);
+    m.hfield = dalloc<double>(cells * 3, c->mesh_owned);
+    m.rho = dalloc<double>(cells, c->mesh_owned);
+    m.da = dalloc<double>(cells, c->mesh_owned);
+    m.e_rough = dalloc<double>(cells, c->mesh_owned);
+    m.e_sphon = dalloc<double>(cells, c->mesh_owned);
+    m.h_rough = dalloc<double>(cells, c->mesh_owned);
+    m.h_sphon = dalloc<double>(cells, c->mesh_owned);
+    for (const void *p : {(const void *)m.e_rough, (const void *)m.e_sphon, (const void *)m.h_rough, (const void *)m.h_sphon})
+      ck(cudaMemsetAsync(const_cast<void *>(p), 0, cells * sizeof(double), c->stream), "memset");
+    c->y.lcurrent = dalloc<long long>(ny + 1, c->mesh_owned);
+    c->y.rcurrent = dalloc<long long>(ny + 1, c->mesh_owned);
+    c->y.heat_e = dalloc<long long>(nodes, c->mesh_owned);
+    c->y.heat_h = dalloc<long long>(nodes, c->mesh_owned);
+    c->hist = dalloc<unsigned int>(cells, c->mesh_owned);
+    c->offsets = dalloc<unsigned int>(cells, c->mesh_owned);
+    c->tile_sums = dalloc<unsigned int>((cells + 1023) / 1024 + 1, c->mesh_owned);
+    ck(cudaStreamSynchronize(c->stream), "sync");
+    c->mesh_set = true;
+    c->cells_set = c->fields_set = false;
+    return mcb200_reset_tallies(c);
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_set_cells(mcb200_ctx *c, const int32_t *motion_rule, const int32_t *attached_contact,
+                     const int32_t *in_surf_region, const int32_t *nearest_surf, const int32_t *surface_dir,
+                     int n_surface_dir, const double *da, int flags) {
+  if (!c) return MCB200_ERR_ARG;
+  if (!c->mesh_set) return fail(c, MCB200_ERR_STATE, "mcb200_set_cells before mcb200_set_mesh");
+  if (!motion_rule || !da || n_surface_dir < 0 || n_surface_dir > kMaxSurfaces)
+    return fail(c, MCB200_ERR_ARG, "mcb200_set_cells: motion_rule and da are required");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    const size_t cells = (size_t)c->ncells;
+    DevMesh &m = c->mesh;
+    ck(cudaMemcpy(const_cast<int *>(m.motion), motion_rule, cells * 6 * sizeof(int), cudaMemcpyHostToDevice), "copy");
+    auto put_i = [&](const int *dst, const int32_t *src) {
+      if (src) ck(cudaMemcpy(const_cast<int *>(dst), src, cells * sizeof(int), cudaMemcpyHostToDevice), "copy");
+      else ck(cudaMemset(const_cast<int *>(dst), 0, cells * sizeof(int)), "memset");
+    };
+    put_i(m.contact, attached_contact);
+    put_i(m.in_surf, in_surf_region);
+    put_i(m.nearest_surf, nearest_surf);
+    ck(cudaMemcpy(const_cast<double *>(m.da), da, cells * sizeof(double), cudaMemcpyHostToDevice), "copy");
+    for (int s = 0; s < kMaxSurfaces; ++s) m.surface_dir[s] = (surface_dir && s < n_surface_dir) ? surface_dir[s] : 0;
+    m.surface_scatter = (flags & MCB200_FLAG_SURFACE_SCATTER) ? 1 : 0;
+    m.surface_impurity = (flags & MCB200_FLAG_SURFACE_IMPURITY) ? 1 : 0;
+    m.heat = (flags & MCB200_FLAG_HEAT) ? 1 : 0;
+    c->cells_set = true;
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_set_fields(mcb200_ctx *c, const double *efield_xyz, const double *hfield_xyz, const double *rho) {
+  if (!c || !efield_xyz || !hfield_xyz || !rho) return MCB200_ERR_ARG;
+  if (!c->mesh_set) return fail(c, MCB200_ERR_STATE, "mcb200_set_fields before mcb200_set_mesh");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    const size_t cells = (size_t)c->ncells;
+    ck(cudaMemcpyAsync(const_cast<double *>(c->mesh.efield), efield_xyz, cells * 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream), "copy");
+    ck(cudaMemcpyAsync(const_cast<double *>(c->mesh.hfield), hfield_xyz, cells * 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream), "copy");
+    ck(cudaMemcpyAsync(const_cast<double *>(c->mesh.rho), rho, cells * sizeof(double), cudaMemcpyHostToDevice, c->stream), "copy");
+    ck(cudaStreamSynchronize(c->stream), "sync");
+    c->fields_set = true;
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_set_surface_rates(mcb200_ctx *c, const double *e_rough, const double *e_phonon, const double *h_rough,
+                             const double *h_phonon) {
+  if (!c || !e_rough || !e_phonon || !h_rough || !h_phonon) return MCB200_ERR_ARG;
+  if (!c->mesh_set) return fail(c, MCB200_ERR_STATE, "mcb200_set_surface_rates before mcb200_set_mesh");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    const size_t b = (size_t)c->ncells * sizeof(double);
+    ck(cudaMemcpy(const_cast<double *>(c->mesh.e_rough), e_rough, b, cudaMemcpyHostToDevice), "copy");
+    ck(cudaMemcpy(const_cast<double *>(c->mesh.e_sphon), e_phonon, b, cudaMemcpyHostToDevice), "copy");
+    ck(cudaMemcpy(const_cast<double *>(c->mesh.h_rough), h_rough, b, cudaMemcpyHostToDevice), "copy");
+    ck(cudaMemcpy(const_cast<double *>(c->mesh.h_sphon), h_phonon, b, cudaMemcpyHostToDevice), "copy");
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_upload_particles(mcb200_ctx *c, size_t n, const mcb200_particles *p) {
+  if (!c || !p) return MCB200_ERR_ARG;
+  if (n > c->capacity) return fail(c, MCB200_ERR_CAPACITY, "more particles than the context capacity");
+  if (!c->mesh_set) return fail(c, MCB200_ERR_STATE, "mcb200_upload_particles before mcb200_set_mesh");
+  if (c->device < 0) return fail(c, MCB200_ERR_STATE, "host-only context");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    std::vector<uint32_t> cell(n), meta(n);
+    uint32_t maxuid = 0;
+    for (size_t q = 0; q < n; ++q) {
+      const int i = p->i[q], j = p->j[q], k = p->k[q];
+      if (i < 0 || j < 0 || k < 0 || i >= c->mesh.nx || j >= c->mesh.ny || k >= c->mesh.nz)
+        return fail(c, MCB200_ERR_ARG, "particle outside the mesh");
+      if (p->isym[q] < 0 || p->isym[q] > 47 || p->itet[q] < 0 || p->itet[q] >= c->tab.nt || p->type[q] < 0 ||
+          p->type[q] > 1)
+        return fail(c, MCB200_ERR_ARG, "particle state out of range");
+      cell[q] = pack_cell(i, j, k);
+      meta[q] = (uint32_t)p->isym[q] | ((uint32_t)p->type[q] << 8);
+      maxuid = std::max(maxuid, p->uid[q] + 1);
+    }
+    const DevParticles &d = c->pb[0].d;
+    c->cur = 0;
+    auto put = [&](void *dst, const void *src, size_t sz) {
+      ck(cudaMemcpyAsync(dst, src, n * sz, cudaMemcpyHostToDevice, c->stream), "upload particles");
+    };
+    put(d.x, p->x, 8); put(d.y, p->y, 8); put(d.z, p->z, 8);
+    put(d.kx, p->kx, 8); put(d.ky, p->ky, 8); put(d.kz, p->kz, 8);
+    put(d.energy, p->energy, 8); put(d.charge, p->charge, 8);
+    put(d.cell, cell.data(), 4); put(d.itet, p->itet, 4); put(d.meta, meta.data(), 4); put(d.uid, p->uid, 4);
+    ck(cudaStreamSynchronize(c->stream), "sync");
+    c->n = n;
+    c->next_uid = maxuid;
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_download_particles(mcb200_ctx *c, mcb200_particles *p, size_t capacity, size_t *n_out) {
+  if (!c || !p) return MCB200_ERR_ARG;
+  if (n_out) *n_out = c->n;
+  if (capacity < c->n) return fail(c, MCB200_ERR_CAPACITY, "host buffers smaller than the particle count");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    const size_t n = c->n;
+    std::vector<uint32_t> cell(n), meta(n);
+    const DevParticles &d = c->pb[c->cur].d;
+    auto get = [&](void *dst, const void *src, size_t sz) {
+      ck(cudaMemcpyAsync(dst, src, n * sz, cudaMemcpyDeviceToHost, c->stream), "download particles");
+    };
+    get(p->x, d.x, 8); get(p->y, d.y, 8); get(p->z, d.z, 8);
+    get(p->kx, d.kx, 8); get(p->ky, d.ky, 8); get(p->kz, d.kz, 8);
+    get(p->energy, d.energy, 8); get(p->charge, d.charge, 8);
+    get(cell.data(), d.cell, 4); get(p->itet, d.itet, 4); get(meta.data(), d.meta, 4); get(p->uid, d.uid, 4);
+    ck(cudaStreamSynchronize(c->stream), "sync");
+    for (size_t q = 0; q < n; ++q) {
+      p->i[q] = cell[q] & 1023;
+      p->j[q] = (cell[q] >> 10) & 1023;
+      p->k[q] = (cell[q] >> 20) & 1023;
+      p->isym[q] = meta[q] & 255;
+      p->type[q] = (meta[q] >> 8) & 255;
+    }
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+size_t mcb200_num_particles(const mcb200_ctx *c) { return c ? c->n : 0; }
+
+int mcb200_step(mcb200_ctx *c, uint32_t step, uint64_t seed, double dt) {
+  if (!c) return MCB200_ERR_ARG;
+  if (!c->mesh_set || !c->cells_set || !c->fields_set)
+    return fail(c, MCB200_ERR_STATE, "mcb200_step needs mesh, cells and fields");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    cudaStream_t s = c->stream;
+    FlightCtx F;
+    F.T = c->dt;
+    F.M = c->mesh;
+    F.Y = c->y;
+    F.dt = dt;
+    F.seed = seed;
+    F.step = step;
+    const int block = 256;
+    // 1. main flight; copies go to generation 0
+    ck(cudaMemsetAsync(c->cb[0].d.count, 0, sizeof(unsigned int), s), "memset");
+    F.C = c->cb[0].d;
+    launch_flight(F, c->pb[c->cur].d, (int)c->n, grid_for(c, c->n, block), block, s);
+    ck(cudaGetLastError(), "flight kernel");
+    // 2. copies fly the rest of the step, generation by generation
+    unsigned int counts[mcb200_ctx::kGenerations] = {0, 0, 0, 0};
+    int gens = 0;
+    for (int g = 0; g < mcb200_ctx::kGenerations; ++g) {
+      ck(cudaMemcpyAsync(c->h_pinned, c->cb[g].d.count, sizeof(unsigned int), cudaMemcpyDeviceToHost, s), "count");
+      ck(cudaStreamSynchronize(s), "sync");
+      counts[g] = std::min<unsigned int>(c->h_pinned[0], (unsigned int)c->child_cap);
+      if (counts[g] == 0) break;
+      gens = g + 1;
+      if (g + 1 < mcb200_ctx::kGenerations) {
+        ck(cudaMemsetAsync(c->cb[g + 1].d.count, 0, sizeof(unsigned int), s), "memset");
+        F.C = c->cb[g + 1].d;
+      } else {
+        F.C = c->cb[g].d;  // a fifth generation would overflow: counted, not flown
+        F.C.capacity = 0;
+      }
+      launch_child_flight(F, c->cb[g].d, grid_for(c, counts[g], block), block, s);
+      ck(cudaGetLastError(), "child flight kernel");
+    }
+    // 3. uids for surviving copies, then append them to the store
+    size_t total_children = 0;
+    for (int g = 0; g < gens; ++g) {
+      launch_child_keys(c->cb[g].d, counts[g], c->child_keys + total_children, c->child_alive + total_children, s);
+      total_children += counts[g];
+    }
+    size_t n_all = c->n;
+    if (total_children > 0) {
+      if (c->n + total_children > c->capacity) return fail(c, MCB200_ERR_CAPACITY, "particle store full after GENERATE");
+      launch_child_rank(c->child_keys, c->child_alive, (int)total_children, c->next_uid, c->child_uids, s);
+      ck(cudaMemsetAsync(c->append_count, 0, sizeof(unsigned int), s), "memset");
+      size_t off = 0;
+      for (int g = 0; g < gens; ++g) {
+        launch_children_to_particles(c->cb[g].d, counts[g], c->child_uids + off, c->child_alive + off,
+                                     c->pb[c->cur].d, (int)c->n, c->append_count, s);
+        off += counts[g];
+      }
+      ck(cudaMemcpyAsync(c->h_pinned, c->append_count, sizeof(unsigned int), cudaMemcpyDeviceToHost, s), "count");
+      ck(cudaStreamSynchronize(s), "sync");
+      const unsigned int appended = c->h_pinned[0];
+      n_all = c->n + appended;
+      c->next_uid += appended;
+    }
+    // 4. drop caught particles and counting-sort the store by cell
+    const int other = 1 - c->cur;
+    launch_cell_sort(c->pb[c->cur].d, (int)n_all, c->pb[other].d, c->ncells, c->mesh.nx, c->mesh.nz, c->hist,
+                     c->offsets, c->tile_sums, c->total, grid_for(c, n_all, 256), s);
+    ck(cudaGetLastError(), "cell sort");
+    ck(cudaMemcpyAsync(c->h_pinned, c->total, sizeof(unsigned int), cudaMemcpyDeviceToHost, s), "count");
+    ck(cudaStreamSynchronize(s), "sync");
+    c->n = c->h_pinned[0];
+    c->cur = other;
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_sync(mcb200_ctx *c) {
+  if (!c) return MCB200_ERR_ARG;
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  return e == cudaSuccess ? MCB200_OK : fail(c, MCB200_ERR_CUDA, cudaGetErrorString(e));
+}
+
+int mcb200_get_tallies(mcb200_ctx *c, uint64_t *counters, double *contact, double *lcurrent, double *rcurrent,
+                       double *heat_e, double *heat_h) {
+  if (!c) return MCB200_ERR_ARG;
+  if (!c->mesh_set) return fail(c, MCB200_ERR_STATE, "mcb200_get_tallies before mcb200_set_mesh");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    ck(cudaStreamSynchronize(c->stream), "sync");
+    if (counters) ck(cudaMemcpy(counters, c->y.counters, sizeof(uint64_t) * kCntNumCounters, cudaMemcpyDeviceToHost), "copy");
+    if (contact) {
+      std::vector<long long> v(kMaxContacts * 6);
+      ck(cudaMemcpy(v.data(), c->y.contact, sizeof(long long) * v.size(), cudaMemcpyDeviceToHost), "copy");
+      for (int i = 0; i < kMaxContacts; ++i) {
+        contact[i * 6 + 0] = (double)v[i * 6 + 0];
+        contact[i * 6 + 1] = (double)v[i * 6 + 1] / kChargeScale;
+        contact[i * 6 + 2] = (double)v[i * 6 + 2] / kEnergyScale;
+        contact[i * 6 + 3] = (double)v[i * 6 + 3];
+        contact[i * 6 + 4] = (double)v[i * 6 + 4] / kChargeScale;
+        contact[i * 6 + 5] = (double)v[i * 6 + 5] / kEnergyScale;
+      }
+    }
+    auto get = [&](double *dst, const long long *src, size_t n, double scale) {
+      if (!dst) return;
+      std::vector<long long> v(n);
+      ck(cudaMemcpy(v.data(), src, sizeof(long long) * n, cudaMemcpyDeviceToHost), "copy");
+      for (size_t i = 0; i < n; ++i) dst[i] = (double)v[i] / scale;
+    };
+    const size_t nodes = (size_t)(c->mesh.nx + 1) * (c->mesh.ny + 1) * (c->mesh.nz + 1);
+    get(lcurrent, c->y.lcurrent, c->mesh.ny + 1, kChargeScale);
+    get(rcurrent, c->y.rcurrent, c->mesh.ny + 1, kChargeScale);
+    get(heat_e, c->y.heat_e, nodes, kEnergyScale);
+    get(heat_h, c->y.heat_h, nodes, kEnergyScale);
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_reset_tallies(mcb200_ctx *c) {
+  if (!c) return MCB200_ERR_ARG;
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    cudaStream_t s = c->stream;
+    ck(cudaMemsetAsync(c->y.counters, 0, sizeof(unsigned long long) * kCntNumCounters, s), "memset");
+    ck(cudaMemsetAsync(c->y.contact, 0, sizeof(long long) * kMaxContacts * 6, s), "memset");
+    if (c->mesh_set) {
+      const size_t nodes = (size_t)(c->mesh.nx + 1) * (c->mesh.ny + 1) * (c->mesh.nz + 1);
+      ck(cudaMemsetAsync(c->y.lcurrent, 0, sizeof(long long) * (c->mesh.ny + 1), s), "memset");
+      ck(cudaMemsetAsync(c->y.rcurrent, 0, sizeof(long long) * (c->mesh.ny + 1), s), "memset");
+      ck(cudaMemsetAsync(c->y.heat_e, 0, sizeof(long long) * nodes, s), "memset");
+      ck(cudaMemsetAsync(c->y.heat_h, 0, sizeof(long long) * nodes, s), "memset");
+    }
+    ck(cudaStreamSynchronize(s), "sync");
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,233 @@
+// flight_kernels.cu -- free-flight kernels and the per-step particle
+// bookkeeping (mid-step copies, removal of caught particles, counting sort
+// by mesh cell).
+//
+// Step structure (replaces MeshQuantities::update_particle +
+// local_migrate, src/mcmodel.cpp:1460-1505 and :1615-1638):
+//   1. flight_kernel: every particle flies dt on its own random stream;
+//      caught particles are marked dead in their meta word.
+//   2. child_flight_kernel, repeated: copies made by GENERATE / GENREF fly
+//      the rest of the step (they may make copies of their own).
+//   3. child_rank_kernel: copies get uids next_uid + rank of (parent, sub).
+//   4. cell_histogram / cell_scan / cell_scatter: survivors and copies are
+//      counting-sorted by cell into the second particle buffer.
+#include "engine_kernels.h"
+#include "flight_physics.cuh"
+#include "flight_physics_impl.cuh"
+
+namespace mcb200 {
+
+constexpr uint32_t kMetaDead = 1u << 16;
+constexpr uint32_t kMetaUnfinished = 1u << 17;
+
+__device__ void load_sym(SymSmem &S, const DevTables &T) {
+  for (int i = threadIdx.x; i < 48 * 6; i += blockDim.x) S.symi[i] = T.symi[i];
+  for (int i = threadIdx.x; i < 5 * 48; i += blockDim.x) S.newisym[i] = T.newisym[i];
+  for (int i = threadIdx.x; i < 3 * 5 * 48; i += blockDim.x) S.bz[i] = T.bz[i];
+  for (int i = threadIdx.x; i < 3 * 48; i += blockDim.x) S.refl[i] = T.reflect_isym[i];
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) flight_kernel(FlightCtx F, DevParticles P, int n) {
+  __shared__ SymSmem S;
+  load_sym(S, F.T);
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const uint32_t meta = P.meta[p];
+    if (meta & kMetaDead) continue;
+    Flyer f(F, S);
+    f.x = P.x[p]; f.y = P.y[p]; f.z = P.z[p];
+    f.kx = P.kx[p]; f.ky = P.ky[p]; f.kz = P.kz[p];
+    f.energy = P.energy[p];
+    f.charge = P.charge[p];
+    const uint32_t c = P.cell[p];
+    f.ic = c & 1023; f.jc = (c >> 10) & 1023; f.kc = (c >> 20) & 1023;
+    f.itet = P.itet[p];
+    f.isym = meta & 255;
+    f.type = (meta >> 8) & 255;
+    f.uid = P.uid[p];
+    f.sub = 0;
+    f.n = 0;
+    f.nchild = 0;
+    f.left_time = F.dt;
+    const int r = f.fly();
+    P.x[p] = f.x; P.y[p] = f.y; P.z[p] = f.z;
+    P.kx[p] = f.kx; P.ky[p] = f.ky; P.kz[p] = f.kz;
+    P.energy[p] = f.energy;
+    P.cell[p] = pack_cell(f.ic, f.jc, f.kc);
+    P.itet[p] = f.itet;
+    uint32_t m = (uint32_t)f.isym | ((uint32_t)f.type << 8);
+    if (r == 1) m |= kMetaDead;
+    if (r == 2) m |= kMetaUnfinished;
+    P.meta[p] = m;
+  }
+}
+
+// Copies made during the previous pass (buffer `in`) fly the rest of their
+// step; copies they make go to `F.C`.
+__global__ void __launch_bounds__(256) child_flight_kernel(FlightCtx F, DevChildren in) {
+  __shared__ SymSmem S;
+  load_sym(S, F.T);
+  const int n = min((int)*in.count, in.capacity);
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    Flyer f(F, S);
+    f.x = in.x[p]; f.y = in.y[p]; f.z = in.z[p];
+    f.kx = in.kx[p]; f.ky = in.ky[p]; f.kz = in.kz[p];
+    f.energy = in.energy[p];
+    f.charge = in.charge[p];
+    const uint32_t c = in.cell[p];
+    f.ic = c & 1023; f.jc = (c >> 10) & 1023; f.kc = (c >> 20) & 1023;
+    f.itet = in.itet[p];
+    f.isym = in.meta[p] & 255;
+    f.type = (in.meta[p] >> 8) & 255;
+    f.uid = in.parent_uid[p];
+    f.sub = in.sub[p];
+    f.n = 0;
+    f.nchild = 0;
+    f.left_time = in.left_time[p];
+    const int r = f.fly();
+    in.x[p] = f.x; in.y[p] = f.y; in.z[p] = f.z;
+    in.kx[p] = f.kx; in.ky[p] = f.ky; in.kz[p] = f.kz;
+    in.energy[p] = f.energy;
+    in.cell[p] = pack_cell(f.ic, f.jc, f.kc);
+    in.itet[p] = f.itet;
+    uint32_t m = (uint32_t)f.isym | ((uint32_t)f.type << 8);
+    if (r == 1) m |= kMetaDead;
+    if (r == 2) m |= kMetaUnfinished;
+    in.meta[p] = m;
+  }
+}
+
+// uid of each surviving copy: next_uid + number of surviving copies with a
+// smaller (parent uid, sub) key, over all copies of this step.  The key set
+// is the concatenation of the child generations (one buffer per generation).
+__global__ void child_rank_kernel(const uint64_t *keys, const uint8_t *alive, int n, uint32_t next_uid,
+                                  uint32_t *uid_out) {
+  __shared__ uint64_t tile[256];
+  __shared__ uint8_t tile_alive[256];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t my = i < n ? keys[i] : 0;
+  uint32_t rank = 0;
+  for (int base = 0; base < n; base += 256) {
+    const int j = base + threadIdx.x;
+    tile[threadIdx.x] = j < n ? keys[j] : ~0ull;
+    tile_alive[threadIdx.x] = j < n ? alive[j] : 0;
+    __syncthreads();
+    const int m = min(256, n - base);
+    for (int q = 0; q < m; ++q) rank += (tile_alive[q] && tile[q] < my) ? 1u : 0u;
+    __syncthreads();
+  }
+  if (i < n) uid_out[i] = next_uid + rank;
+}
+
+// ---- counting sort by cell ------------------------------------------------
+__device__ __forceinline__ int cell_linear(uint32_t c, int nx, int nz) {
+  return (int)((((c >> 10) & 1023) * nx + (c & 1023)) * nz + ((c >> 20) & 1023));
+}
+
+__global__ void cell_histogram(const uint32_t *cell, const uint32_t *meta, int n, int nx, int nz,
+                               unsigned int *hist) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
+    if (!(meta[p] & kMetaDead)) atomicAdd(&hist[cell_linear(cell[p], nx, nz)], 1u);
+}
+
+// Exclusive scan of `count` values, single pass per 1024-wide tile plus a
+// tile-sum pass (cells are at most ~10^6, so three small launches suffice).
+__global__ void scan_tiles(const unsigned int *in, unsigned int *out, unsigned int *tile_sums, int n) {
+  __shared__ unsigned int s[1024];
+  const int i = blockIdx.x * 1024 + threadIdx.x;
+  const unsigned int v = i < n ? in[i] : 0u;
+  s[threadIdx.x] = v;
+  __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {
+    unsigned int t = threadIdx.x >= (unsigned)off ? s[threadIdx.x - off] : 0u;
+    __syncthreads();
+    s[threadIdx.x] += t;
+    __syncthreads();
+  }
+  if (i < n) out[i] = s[threadIdx.x] - v;
+  if (threadIdx.x == 1023) tile_sums[blockIdx.x] = s[1023];
+}
+__global__ void scan_tile_sums(unsigned int *tile_sums, int ntiles, unsigned int *total) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    unsigned int run = 0;
+    for (int t = 0; t < ntiles; ++t) {
+      const unsigned int v = tile_sums[t];
+      tile_sums[t] = run;
+      run += v;
+    }
+    *total = run;
+  }
+}
+__global__ void scan_add(unsigned int *out, const unsigned int *tile_sums, int n) {
+  const int i = blockIdx.x * 1024 + threadIdx.x;
+  if (i < n) out[i] += tile_sums[blockIdx.x];
+}
+
+__global__ void cell_scatter(DevParticles src, int n, DevParticles dst, unsigned int *cursor, int nx, int nz) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const uint32_t m = src.meta[p];
+    if (m & kMetaDead) continue;
+    const unsigned int q = atomicAdd(&cursor[cell_linear(src.cell[p], nx, nz)], 1u);
+    dst.x[q] = src.x[p]; dst.y[q] = src.y[p]; dst.z[q] = src.z[p];
+    dst.kx[q] = src.kx[p]; dst.ky[q] = src.ky[p]; dst.kz[q] = src.kz[p];
+    dst.energy[q] = src.energy[p]; dst.charge[q] = src.charge[p];
+    dst.cell[q] = src.cell[p];
+    dst.itet[q] = src.itet[p];
+    dst.meta[q] = m & 0xffffu;
+    dst.uid[q] = src.uid[p];
+  }
+}
+
+// Append surviving copies (already flown) to the particle store, with uids.
+__global__ void children_to_particles(DevChildren c, int n, const uint32_t *uids, const uint8_t *alive,
+                                      DevParticles dst, int dst_offset, unsigned int *dst_count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !alive[i]) return;
+  const unsigned int q = dst_offset + atomicAdd(dst_count, 1u);
+  dst.x[q] = c.x[i]; dst.y[q] = c.y[i]; dst.z[q] = c.z[i];
+  dst.kx[q] = c.kx[i]; dst.ky[q] = c.ky[i]; dst.kz[q] = c.kz[i];
+  dst.energy[q] = c.energy[i]; dst.charge[q] = c.charge[i];
+  dst.cell[q] = c.cell[i];
+  dst.itet[q] = c.itet[i];
+  dst.meta[q] = c.meta[i] & 0xffffu;
+  dst.uid[q] = uids[i];
+}
+
+__global__ void child_keys(DevChildren c, int n, uint64_t *keys, uint8_t *alive) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  keys[i] = ((uint64_t)c.parent_uid[i] << 32) | c.sub[i];
+  alive[i] = (c.meta[i] & kMetaDead) ? 0 : 1;
+}
+
+// ---- host-side launchers ----------------------------------------------------
+void launch_flight(const FlightCtx &F, const DevParticles &P, int n, int grid, int block, cudaStream_t s) {
+  if (n > 0) flight_kernel<<<grid, block, 0, s>>>(F, P, n);
+}
+void launch_child_flight(const FlightCtx &F, const DevChildren &in, int grid, int block, cudaStream_t s) {
+  child_flight_kernel<<<grid, block, 0, s>>>(F, in);
+}
+void launch_child_keys(const DevChildren &c, int n, uint64_t *keys, uint8_t *alive, cudaStream_t s) {
+  if (n > 0) child_keys<<<(n + 255) / 256, 256, 0, s>>>(c, n, keys, alive);
+}
+void launch_child_rank(const uint64_t *keys, const uint8_t *alive, int n, uint32_t next_uid, uint32_t *uid_out,
+                       cudaStream_t s) {
+  if (n > 0) child_rank_kernel<<<(n + 255) / 256, 256, 0, s>>>(keys, alive, n, next_uid, uid_out);
+}
+void launch_children_to_particles(const DevChildren &c, int n, const uint32_t *uids, const uint8_t *alive,
+                                  const DevParticles &dst, int dst_offset, unsigned int *dst_count, cudaStream_t s) {
+  if (n > 0) children_to_particles<<<(n + 255) / 256, 256, 0, s>>>(c, n, uids, alive, dst, dst_offset, dst_count);
+}
+void launch_cell_sort(const DevParticles &src, int n, const DevParticles &dst, int ncells, int nx, int nz,
+                      unsigned int *hist, unsigned int *offsets, unsigned int *tile_sums, unsigned int *total,
+                      int grid, cudaStream_t s) {
+  cudaMemsetAsync(hist, 0, sizeof(unsigned int) * ncells, s);
+  if (n > 0) cell_histogram<<<grid, 256, 0, s>>>(src.cell, src.meta, n, nx, nz, hist);
+  const int tiles = (ncells + 1023) / 1024;
+  scan_tiles<<<tiles, 1024, 0, s>>>(hist, offsets, tile_sums, ncells);
+  scan_tile_sums<<<1, 32, 0, s>>>(tile_sums, tiles, total);
+  scan_add<<<tiles, 1024, 0, s>>>(offsets, tile_sums, ncells);
+  if (n > 0) cell_scatter<<<grid, 256, 0, s>>>(src, n, dst, offsets, nx, nz);
+}
+
+}  // namespace mcb200

@@ -1,0 +1,231 @@
+"""ctypes binding of the B200 carrier engine's C ABI (include/mcb200.h).
+
+This module is a thin host-side mirror for Python callers (the test suite,
+bench.py).  All computation happens in libmcb200.so on the GPU; importing
+this module fails loudly if the library has not been built, and every call
+raises EngineError when the library reports an error.  There is no CPU
+fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "libmcb200.so")
+DEFAULT_TABLE_DIR = os.path.join(PKG_DIR, "tables")
+
+OK = 0
+COUNTER_NAMES = [
+    "phonon", "impurity", "caught", "generated", "events", "unfinished", "too_many_events",
+    "child_overflow", "no_tet",
+]
+NUM_COUNTERS = 16
+FLAG_SURFACE_SCATTER = 1
+FLAG_SURFACE_IMPURITY = 2
+FLAG_HEAT = 4
+UNIT_NAMES = ["T0", "eV0", "spr0", "time0", "conc0", "field0", "scrt0", "pot0", "a0pi", "sieg",
+              "eps_silicon", "eps_oxide", "curr0", "dens0"]
+
+
+class EngineError(RuntimeError):
+    pass
+
+
+class _Particles(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in
+                ("x", "y", "z", "kx", "ky", "kz", "charge", "energy", "i", "j", "k", "itet", "isym", "type", "uid")]
+
+
+PARTICLE_FIELDS = {
+    "x": np.float64, "y": np.float64, "z": np.float64, "kx": np.float64, "ky": np.float64, "kz": np.float64,
+    "charge": np.float64, "energy": np.float64, "i": np.int32, "j": np.int32, "k": np.int32,
+    "itet": np.int32, "isym": np.int32, "type": np.int32, "uid": np.uint32,
+}
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    if not os.path.exists(path):
+        raise EngineError(f"{path} is missing: build it with `make -C c-mc_electron_b200` "
+                          "(or __graft_entry__.build())")
+    lib = ctypes.CDLL(path)
+    c = ctypes
+    vp, i32p, dp = c.c_void_p, c.POINTER(c.c_int32), c.POINTER(c.c_double)
+    lib.mcb200_create.argtypes = [c.c_char_p, c.c_double, c.c_int, c.c_size_t, c.POINTER(vp)]
+    lib.mcb200_destroy.argtypes = [vp]
+    lib.mcb200_destroy.restype = None
+    lib.mcb200_last_error.argtypes = [vp]
+    lib.mcb200_last_error.restype = c.c_char_p
+    lib.mcb200_units.argtypes = [vp, dp, c.c_int]
+    lib.mcb200_copy_table.argtypes = [vp, c.c_char_p, vp, c.c_size_t, c.POINTER(c.c_size_t)]
+    lib.mcb200_set_mesh.argtypes = [vp, c.c_int, c.c_int, c.c_int, dp, dp, dp]
+    lib.mcb200_set_cells.argtypes = [vp, i32p, i32p, i32p, i32p, i32p, c.c_int, dp, c.c_int]
+    lib.mcb200_set_fields.argtypes = [vp, dp, dp, dp]
+    lib.mcb200_set_surface_rates.argtypes = [vp, dp, dp, dp, dp]
+    lib.mcb200_upload_particles.argtypes = [vp, c.c_size_t, c.POINTER(_Particles)]
+    lib.mcb200_download_particles.argtypes = [vp, c.POINTER(_Particles), c.c_size_t, c.POINTER(c.c_size_t)]
+    lib.mcb200_num_particles.argtypes = [vp]
+    lib.mcb200_num_particles.restype = c.c_size_t
+    lib.mcb200_step.argtypes = [vp, c.c_uint32, c.c_uint64, c.c_double]
+    lib.mcb200_sync.argtypes = [vp]
+    lib.mcb200_get_tallies.argtypes = [vp, c.POINTER(c.c_uint64), dp, dp, dp, dp, dp]
+    lib.mcb200_reset_tallies.argtypes = [vp]
+    return lib
+
+
+_LIB = None
+
+
+def lib() -> ctypes.CDLL:
+    global _LIB
+    if _LIB is None:
+        _LIB = load_library()
+    return _LIB
+
+
+def _ptr(a: np.ndarray | None, ctype):
+    if a is None:
+        return None
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+@dataclass
+class Mesh:
+    nx: int
+    ny: int
+    nz: int
+    lx: np.ndarray
+    ly: np.ndarray
+    lz: np.ndarray
+
+    @property
+    def ncells(self) -> int:
+        return self.nx * self.ny * self.nz
+
+    @property
+    def nnodes(self) -> int:
+        return (self.nx + 1) * (self.ny + 1) * (self.nz + 1)
+
+
+class Engine:
+    """One engine context: full-band tables, mesh, particles, tallies on one GPU."""
+
+    def __init__(self, table_dir: str = DEFAULT_TABLE_DIR, kelvin: float = 300.0, device: int = 0,
+                 max_particles: int = 1 << 20):
+        self._lib = lib()
+        self._ctx = ctypes.c_void_p()
+        rc = self._lib.mcb200_create(table_dir.encode(), kelvin, device, max_particles, ctypes.byref(self._ctx))
+        if rc != OK:
+            msg = self._lib.mcb200_last_error(self._ctx).decode() if self._ctx else "no context"
+            if self._ctx:
+                self._lib.mcb200_destroy(self._ctx)
+                self._ctx = ctypes.c_void_p()
+            raise EngineError(f"mcb200_create failed ({rc}): {msg}")
+        self.mesh: Mesh | None = None
+
+    def close(self):
+        if self._ctx:
+            self._lib.mcb200_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, what: str):
+        if rc != OK:
+            raise EngineError(f"{what} failed ({rc}): {self._lib.mcb200_last_error(self._ctx).decode()}")
+
+    def units(self) -> dict:
+        out = np.zeros(len(UNIT_NAMES))
+        self._check(self._lib.mcb200_units(self._ctx, _ptr(out, ctypes.c_double), len(out)), "units")
+        return dict(zip(UNIT_NAMES, out.tolist()))
+
+    def table(self, name: str, dtype) -> np.ndarray:
+        need = ctypes.c_size_t()
+        self._check(self._lib.mcb200_copy_table(self._ctx, name.encode(), None, 0, ctypes.byref(need)), name)
+        out = np.empty(need.value // np.dtype(dtype).itemsize, dtype=dtype)
+        self._check(self._lib.mcb200_copy_table(self._ctx, name.encode(), out.ctypes.data_as(ctypes.c_void_p),
+                                                out.nbytes, ctypes.byref(need)), name)
+        return out
+
+    def set_mesh(self, lx, ly, lz):
+        lx, ly, lz = (np.ascontiguousarray(a, dtype=np.float64) for a in (lx, ly, lz))
+        m = Mesh(len(lx) - 1, len(ly) - 1, len(lz) - 1, lx, ly, lz)
+        self._check(self._lib.mcb200_set_mesh(self._ctx, m.nx, m.ny, m.nz, _ptr(lx, ctypes.c_double),
+                                              _ptr(ly, ctypes.c_double), _ptr(lz, ctypes.c_double)), "set_mesh")
+        self.mesh = m
+
+    def set_cells(self, motion_rule, da, attached_contact=None, in_surf_region=None, nearest_surf=None,
+                  surface_dir=None, flags: int = 0):
+        i32 = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.int32)
+        mr, ac, isr, ns, sd = (i32(a) for a in (motion_rule, attached_contact, in_surf_region, nearest_surf,
+                                                  surface_dir))
+        da = np.ascontiguousarray(da, dtype=np.float64)
+        assert mr.size == 6 * self.mesh.ncells and da.size == self.mesh.ncells
+        nsd = 0 if sd is None else int(sd.size)
+        self._check(self._lib.mcb200_set_cells(self._ctx, _ptr(mr, ctypes.c_int32), _ptr(ac, ctypes.c_int32),
+                                               _ptr(isr, ctypes.c_int32), _ptr(ns, ctypes.c_int32),
+                                               _ptr(sd, ctypes.c_int32), nsd, _ptr(da, ctypes.c_double), flags),
+                    "set_cells")
+
+    def set_fields(self, efield_xyz, hfield_xyz, rho):
+        e, h, r = (np.ascontiguousarray(a, dtype=np.float64) for a in (efield_xyz, hfield_xyz, rho))
+        assert e.size == 3 * self.mesh.ncells and h.size == 3 * self.mesh.ncells and r.size == self.mesh.ncells
+        self._check(self._lib.mcb200_set_fields(self._ctx, _ptr(e, ctypes.c_double), _ptr(h, ctypes.c_double),
+                                                _ptr(r, ctypes.c_double)), "set_fields")
+
+    def set_surface_rates(self, e_rough, e_phonon, h_rough, h_phonon):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (e_rough, e_phonon, h_rough, h_phonon)]
+        self._check(self._lib.mcb200_set_surface_rates(self._ctx, *[_ptr(a, ctypes.c_double) for a in arrs]),
+                    "set_surface_rates")
+
+    @staticmethod
+    def _soa(arrays: dict) -> _Particles:
+        p = _Particles()
+        for name in PARTICLE_FIELDS:
+            setattr(p, name, arrays[name].ctypes.data)
+        return p
+
+    def upload(self, particles: dict):
+        arrs = {k: np.ascontiguousarray(particles[k], dtype=t) for k, t in PARTICLE_FIELDS.items()}
+        n = len(arrs["x"])
+        self._check(self._lib.mcb200_upload_particles(self._ctx, n, ctypes.byref(self._soa(arrs))), "upload")
+
+    def num_particles(self) -> int:
+        return int(self._lib.mcb200_num_particles(self._ctx))
+
+    def download(self) -> dict:
+        n = self.num_particles()
+        arrs = {k: np.empty(n, dtype=t) for k, t in PARTICLE_FIELDS.items()}
+        got = ctypes.c_size_t()
+        self._check(self._lib.mcb200_download_particles(self._ctx, ctypes.byref(self._soa(arrs)), n,
+                                                        ctypes.byref(got)), "download")
+        return arrs
+
+    def step(self, step: int, seed: int, dt: float):
+        self._check(self._lib.mcb200_step(self._ctx, step, seed, dt), "step")
+
+    def sync(self):
+        self._check(self._lib.mcb200_sync(self._ctx), "sync")
+
+    def tallies(self) -> dict:
+        m = self.mesh
+        counters = np.zeros(NUM_COUNTERS, dtype=np.uint64)
+        contact = np.zeros(16 * 6)
+        lcur, rcur = np.zeros(m.ny + 1), np.zeros(m.ny + 1)
+        he, hh = np.zeros(m.nnodes), np.zeros(m.nnodes)
+        self._check(self._lib.mcb200_get_tallies(
+            self._ctx, _ptr(counters, ctypes.c_uint64), _ptr(contact, ctypes.c_double), _ptr(lcur, ctypes.c_double),
+            _ptr(rcur, ctypes.c_double), _ptr(he, ctypes.c_double), _ptr(hh, ctypes.c_double)), "tallies")
+        out = {name: int(counters[i]) for i, name in enumerate(COUNTER_NAMES)}
+        out.update(contact=contact.reshape(16, 6), lcurrent=lcur, rcurrent=rcur, heat_e=he, heat_h=hh)
+        return out
+
+    def reset_tallies(self):
+        self._check(self._lib.mcb200_reset_tallies(self._ctx), "reset_tallies")

@@ -1,0 +1,151 @@
+/*
+ * mcb200.h -- C ABI of the B200 ensemble Monte Carlo carrier engine.
+ *
+ * The engine replaces the per-step carrier update of the reference
+ * simulator (chenglinye18-crypto/C-MC_electron), whose seam is the member
+ * MeshQuantities::update_particle() (src/mcmodel.cpp:1460) and the routines
+ * it reaches: particle_fly (src/mcmodel.cpp:1874-2161), TetHit / CellHit
+ * (src/TetHit.cpp, src/CellHit.cpp), the phonon / impurity / surface
+ * scattering files, and the bookkeeping local_migrate (:1615-1638).  The
+ * reference has no plugin or FFI layer of its own; these entry points are
+ * what its host code (or any C / C++ / ctypes caller) binds instead.
+ *
+ * Conventions.
+ *  - Plain pointers and sizes; every host buffer is owned by the caller,
+ *    every device buffer by the context.  Nothing here retains a caller
+ *    pointer after the call returns.
+ *  - Units are the reference's normalised ones (energy kB*T, length spr0,
+ *    time hbar/(kB*T)); mcb200_units() returns the scales.
+ *  - Mesh cell (i, j, k) has linear index (j * nx + i) * nz + k, the
+ *    reference's single-rank layout (C_LINDEX_GHOST_ONE, include/defs.h);
+ *    mesh node (i, j, k) has index (j * (nx+1) + i) * (nz+1) + k.
+ *  - Every call returns MCB200_OK (0) or an error code; the reference's
+ *    exit() paths become error codes or counters, never a process exit.
+ *    mcb200_last_error() describes the last failure of a context.
+ *  - One context per host thread; each context runs on its own CUDA stream.
+ */
+#ifndef MCB200_H
+#define MCB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MCB200_OK 0
+#define MCB200_ERR_ARG 1       /* a bad argument or size */
+#define MCB200_ERR_CUDA 2      /* a CUDA call failed (no GPU, out of memory, ...) */
+#define MCB200_ERR_IO 3        /* a table or deck file could not be read */
+#define MCB200_ERR_CAPACITY 4  /* more particles than the context was sized for */
+#define MCB200_ERR_STATE 5     /* call made before the data it needs was set */
+
+typedef struct mcb200_ctx mcb200_ctx;
+
+/* Particles as structure-of-arrays host buffers (the reference's Particle,
+ * include/utils.h:130-141, minus the per-step bookkeeping fields).
+ * i, j, k: cell; itet: tetrahedron; isym: BZ wedge (0..47); type: 0 electron,
+ * 1 hole; uid: unique id, the key of the particle's random stream. */
+typedef struct {
+  double *x, *y, *z;
+  double *kx, *ky, *kz;
+  double *charge, *energy;
+  int32_t *i, *j, *k;
+  int32_t *itet, *isym, *type;
+  uint32_t *uid;
+} mcb200_particles;
+
+/* Counters returned by mcb200_get_tallies (index into counters[]). */
+#define MCB200_CNT_PHONON 0        /* real phonon events  (sttt.phononScatter) */
+#define MCB200_CNT_IMPURITY 1      /* real impurity events (sttt.impurityScatter) */
+#define MCB200_CNT_CAUGHT 2        /* particles removed    (catch_par_num) */
+#define MCB200_CNT_GENERATED 3     /* GENERATE copies      (gen_par) */
+#define MCB200_CNT_EVENTS 4        /* free-flight loop iterations */
+#define MCB200_CNT_UNFINISHED 5    /* PASS across the outer y boundary */
+#define MCB200_CNT_TOO_MANY 6      /* particles over the per-step event cap */
+#define MCB200_CNT_CHILD_OVERFLOW 7
+#define MCB200_CNT_NO_TET 8        /* tetrahedron search failed (particle caught) */
+#define MCB200_NUM_COUNTERS 16
+
+/* Build the full-band tables from `table_dir` (the reference's input/
+ * directory: bs.si.asc, zd.si.asc; Band::IELEC, src/Band.cpp:4271-4476) at
+ * lattice temperature `kelvin`, and upload them to CUDA device `device`.
+ * `max_particles` sizes the particle store.  device = -1 builds the tables
+ * on the host only (for inspection with mcb200_copy_table; every device
+ * call then returns MCB200_ERR_STATE).  On failure *out may still hold a
+ * context whose mcb200_last_error() says why; destroy it either way. */
+int mcb200_create(const char *table_dir, double kelvin, int device, size_t max_particles, mcb200_ctx **out);
+void mcb200_destroy(mcb200_ctx *ctx);
+const char *mcb200_last_error(const mcb200_ctx *ctx);
+
+/* Normalisation scales (MeshQuantities::init_phpysical_parameter,
+ * src/mcmodel.cpp:4007-4122): out[0..n) = T0, eV0, spr0, time0, conc0,
+ * field0, scrt0, pot0, a0pi, sieg, eps_silicon, eps_oxide, curr0, dens0. */
+int mcb200_units(const mcb200_ctx *ctx, double *out, int n);
+
+/* Copy a host-built table (for inspection and parity checks) into `out`
+ * (capacity `bytes`); `*needed` receives its size in bytes.  Names follow
+ * the reference's Band members: "gamtet", "vt", "vgt", "datantlin",
+ * "faclow", "facmedium", "fachigh", "tet", "NeibrTet", "ibt", "xkk", "ykk",
+ * "zkk", "eek", "matsym", "indmat", "newisym", "xbz", "ybz", "zbz",
+ * "ntlist", "ptlist", "tlist", "nslist", "pslist", "slist", "ntlists",
+ * "ptlists", "tlists", "dos", "sumdos", "dostetmax", "sumscatt", "scatte",
+ * "dose", "scattiie", "scatth", "dosh", "scattiih", "energy". */
+int mcb200_copy_table(const mcb200_ctx *ctx, const char *name, void *out, size_t bytes, size_t *needed);
+
+/* Mesh node coordinates in normalised length (lx: nx+1 values, ...);
+ * replaces the lx/ly/lz/dx/dy/dz globals (include/utils.h:81-83). */
+int mcb200_set_mesh(mcb200_ctx *ctx, int nx, int ny, int nz, const double *lx, const double *ly,
+                    const double *lz);
+
+#define MCB200_FLAG_SURFACE_SCATTER 1   /* Flag_SurfaceScatter */
+#define MCB200_FLAG_SURFACE_IMPURITY 2  /* Flag_SurfaceImpurityScatter */
+#define MCB200_FLAG_HEAT 4              /* flag_heat: phonon events tally heat */
+
+/* Per-cell data of the device (c_motion_rule: 6 ints per cell in face
+ * order UP, DOWN, LEFT, RIGHT, FRONT, BACK; c_attached_contact (1-based);
+ * c_InSurfRegion; c_nearestSurf; c_da) and the surface directions
+ * (SurfaceDir, up to 30).  NULL optional arrays mean zero. */
+int mcb200_set_cells(mcb200_ctx *ctx, const int32_t *motion_rule, const int32_t *attached_contact,
+                     const int32_t *in_surf_region, const int32_t *nearest_surf, const int32_t *surface_dir,
+                     int n_surface_dir, const double *da, int flags);
+
+/* Cell fields as felt by each carrier type (3 values per cell, the
+ * reference's c_field_* / c_h_field_* times ChargeSign), and the screening
+ * density Rho (c_par_charge after compute_cell_charge). */
+int mcb200_set_fields(mcb200_ctx *ctx, const double *efield_xyz, const double *hfield_xyz, const double *rho);
+
+/* Per-cell surface scattering rates (c_e_roughnessRate, c_e_surfPhononRate,
+ * c_h_roughnessRate, c_h_surfPhononRate). */
+int mcb200_set_surface_rates(mcb200_ctx *ctx, const double *e_rough, const double *e_phonon,
+                             const double *h_rough, const double *h_phonon);
+
+/* Particle store. */
+int mcb200_upload_particles(mcb200_ctx *ctx, size_t n, const mcb200_particles *p);
+int mcb200_download_particles(mcb200_ctx *ctx, mcb200_particles *p, size_t capacity, size_t *n_out);
+size_t mcb200_num_particles(const mcb200_ctx *ctx);
+
+/* One transport step: every particle flies `dt` with the reference's event
+ * loop on its own random stream (seed, uid, step), copies made by
+ * GENERATE / GENREF finish the step, caught particles are removed, copies
+ * join with fresh uids, and the store is counting-sorted by cell.
+ * Asynchronous on the context's stream; tallies accumulate. */
+int mcb200_step(mcb200_ctx *ctx, uint32_t step, uint64_t seed, double dt);
+
+/* Wait for the context's stream. */
+int mcb200_sync(mcb200_ctx *ctx);
+
+/* Tallies since the last reset.  Any output may be NULL.
+ * counters[MCB200_NUM_COUNTERS]; contact[16*6] per contact {NumParGen,
+ * CharGen, EnergyGen, NumParCatch, CharCatch, EnergyCatch};
+ * lcurrent / rcurrent[ny+1]; heat_e / heat_h per mesh node. */
+int mcb200_get_tallies(mcb200_ctx *ctx, uint64_t *counters, double *contact, double *lcurrent, double *rcurrent,
+                       double *heat_e, double *heat_h);
+int mcb200_reset_tallies(mcb200_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MCB200_H */

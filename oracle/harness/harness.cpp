@@ -93,12 +93,14 @@ extern "C" {
  * band tables read from `table_dir` instead of <exe>/../input.  Particle
  * initialisation draws from the sequential stream (seed, 0xffffffff,
  * 0xfffffffe, 0).  Every particle gets a uid (stored in par_id) in list
- * order.  The deck's own directory becomes the working directory, as the
- * reference expects.  Returns 0 on success. */
+ * order.  The deck is read from its own directory, as the reference
+ * expects; the caller's working directory is restored.  Returns 0 on success. */
 int orc_init(const char *input_file, const char *table_dir, uint64_t seed, int make_particles) {
   g_seed = seed;
   set_stream(0xffffffffu, 0xfffffffeu, 0);
   std::string path(input_file);
+  char saved_cwd[4096];
+  if (!getcwd(saved_cwd, sizeof(saved_cwd))) return 1;
   size_t slash = path.rfind('/');
   if (slash != std::string::npos) {
     if (chdir(path.substr(0, slash).c_str()) != 0) return 1;
@@ -137,7 +139,7 @@ int orc_init(const char *input_file, const char *table_dir, uint64_t seed, int m
   g_next_uid = 0;
   for (auto &l : mq->par_list)
     for (auto &p : l) p.par_id = (int)g_next_uid++;
-  return 0;
+  return chdir(saved_cwd) == 0 ? 0 : 1;
 }
 
 /* ---- scalar / array accessors --------------------------------------- */

@@ -1,0 +1,122 @@
+"""Shared parity scenarios: the same device state and the same Philox draws
+are given to the CPU oracle (the reference's particle_fly) and to the B200
+engine, and the results are compared particle by particle.
+
+TEST INFRASTRUCTURE (used by tests/ and by __graft_entry__.smoke()).
+"""
+from __future__ import annotations
+
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, os.path.join(ROOT, "c-mc_electron_b200"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+import mcb200  # noqa: E402
+from mcb200 import decks  # noqa: E402
+from oracle_bridge import ORACLE_TABLES, Oracle  # noqa: E402
+
+CONT_FIELDS = ["x", "y", "z", "kx", "ky", "kz", "energy", "charge"]
+DISC_FIELDS = ["i", "j", "k", "itet", "isym", "type"]
+# Kinematics tolerance: the only differences allowed come from libm
+# transcendentals (log / sin / cos / pow with a negative exponent), which
+# CUDA and glibc may round 1 ulp apart; a few flight segments later that is
+# still a relative 1e-9 at most.
+REL_TOL = 1e-9
+ABS_TOL = 1e-12
+
+
+def engine_from_oracle(orc: Oracle, max_particles: int, flags: int = 0) -> mcb200.Engine:
+    """Engine context carrying the oracle's mesh, cell data and fields."""
+    eng = mcb200.Engine(table_dir=ORACLE_TABLES, kelvin=orc.scalar("T0"), device=0, max_particles=max_particles)
+    eng.set_mesh(orc.array("lx"), orc.array("ly"), orc.array("lz"))
+    surf_dir = orc.array("SurfaceDir").astype(np.int32)
+    eng.set_cells(orc.array("c_motion_rule").astype(np.int32), orc.array("c_da"),
+                  attached_contact=orc.array("c_attached_contact").astype(np.int32),
+                  in_surf_region=orc.array("c_InSurfRegion").astype(np.int32),
+                  nearest_surf=orc.array("c_nearestSurf").astype(np.int32), surface_dir=surf_dir, flags=flags)
+    push_fields(orc, eng)
+    return eng
+
+
+def push_fields(orc: Oracle, eng: mcb200.Engine):
+    """Fields as felt by each carrier (ChargeSign = {-1, +1},
+    src/Constant_GlobalVariable_MathFunction.cpp:18) and the screening density."""
+    e = -np.stack([orc.array("c_field_x"), orc.array("c_field_y"), orc.array("c_field_z")], axis=1)
+    h = np.stack([orc.array("c_h_field_x"), orc.array("c_h_field_y"), orc.array("c_h_field_z")], axis=1)
+    eng.set_fields(e.ravel(), h.ravel(), orc.array("c_par_charge"))
+
+
+def set_uniform_field(orc: Oracle, ex_v_per_m: float, ey=0.0, ez=0.0):
+    f0 = orc.scalar("field0")
+    n = len(orc.array("c_field_x"))
+    for name, v in (("x", ex_v_per_m), ("y", ey), ("z", ez)):
+        orc.set_array(f"c_field_{name}", np.full(n, v / f0))
+        orc.set_array(f"c_h_field_{name}", np.full(n, v / f0))
+
+
+def compare(a: dict, b: dict) -> dict:
+    """Particle-by-particle comparison keyed by uid."""
+    ia, ib = np.argsort(a["uid"]), np.argsort(b["uid"])
+    ua, ub = a["uid"][ia], b["uid"][ib]
+    out = {"n_oracle": len(ua), "n_engine": len(ub)}
+    if len(ua) != len(ub) or not np.array_equal(ua, ub):
+        out.update(mismatch=-1, uid_mismatch=True)
+        return out
+    bad = np.zeros(len(ua), dtype=bool)
+    worst = 0.0
+    for f in DISC_FIELDS:
+        bad |= a[f][ia] != b[f][ib]
+    for f in CONT_FIELDS:
+        x, y = a[f][ia], b[f][ib]
+        err = np.abs(x - y)
+        lim = ABS_TOL + REL_TOL * np.maximum(np.abs(x), np.abs(y))
+        bad |= err > lim
+        rel = err / np.maximum(np.maximum(np.abs(x), np.abs(y)), 1e-300)
+        worst = max(worst, float(np.max(rel[err > 0], initial=0.0)))
+    out.update(mismatch=int(bad.sum()), worst_rel=worst)
+    return out
+
+
+def run_bulk_parity(n_particles: int = 2000, steps: int = 3, seed: int = 11, field_v_per_m: float = 1e6,
+                    cells=(8, 6, 6), heat: bool = False) -> dict:
+    """Bulk n-Si box, frozen uniform field: `steps` transport steps through
+    both implementations from the oracle's own initial ensemble."""
+    nx, ny, nz = cells
+    with tempfile.TemporaryDirectory() as tmp:
+        deck = decks.bulk_box(tmp, nx=nx, ny=ny, nz=nz, electrons=n_particles, holes=n_particles // 4)
+        orc = Oracle()
+        orc.init(deck["input"], seed=seed, make_particles=True)
+    set_uniform_field(orc, field_v_per_m)
+    orc.compute_cell_charge()
+    if heat:
+        orc.set_scalar("flag_heat", 1)
+    dt = orc.scalar("dt")
+    p0 = orc.particles()
+    n0 = len(p0["x"])
+    eng = engine_from_oracle(orc, max_particles=max(4 * n0, 4096), flags=mcb200.FLAG_HEAT if heat else 0)
+    eng.upload(p0)
+    orc.reset_tallies()
+    worst = {"mismatch": 0}
+    for s in range(steps):
+        orc.flight_step(s)
+        eng.step(s, seed, dt)
+        res = compare(orc.particles(), eng.download())
+        if res["mismatch"] != 0:
+            res["step"] = s
+            worst = res
+            break
+        worst = res
+    t = eng.tallies()
+    worst.update(n_start=n0, phonon_engine=t["phonon"], phonon_oracle=int(orc.scalar("phonon_scatter")),
+                 impurity_engine=t["impurity"], impurity_oracle=int(orc.scalar("impurity_scatter")),
+                 events=t["events"], caught_engine=t["caught"], caught_oracle=int(orc.scalar("catch_par_num")))
+    if heat:
+        worst["heat_engine"] = t["heat_e"]
+        worst["heat_oracle"] = orc.array("p_electron_heat")
+    eng.close()
+    return worst
