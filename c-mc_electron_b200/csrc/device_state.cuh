@@ -15,6 +15,8 @@ constexpr int kMWLE = 325;      // coarse tetrahedron-list bins (40 meV)
 constexpr int kMWLES = 60;      // fine tetrahedron-list bins (2 meV)
 constexpr int kMaxContacts = 16;
 constexpr int kMaxSurfaces = 30;
+// `step` word of the random stream used for initial-ensemble sampling.
+constexpr uint32_t kSeedStreamStep = 0xfffffffdu;
 
 // Motion rules (ldg actions), include/Constant_GlobalVariable_MathFunction.h:229-243.
 enum MotionRule : int { kPass = 1, kReflect = 2, kScattOx = 3, kPeriod = 4, kGenerate = 5, kCatch = 6, kCatchGate = 7, kGenRef = 8 };
@@ -60,6 +62,9 @@ struct DevTables {
   const double *dosh;        // [4][3][kNT]
   const double *scattiih;    // [3][3][kNT]
   const double *dostetmax;   // [kMNB][kNT]
+  const double *dos;         // [kMNB][kNT]  (initial-state sampling)
+  const double *sumdos;      // [kNT][3]
+  double dosmax[3];
   const int *ntlist, *ptlist, *tlist;     // [kMWLE][kMNB], list
   const int *nslist, *pslist, *slist;
   const int *ntlists, *ptlists, *tlists;  // [kMWLES][kMNB], list

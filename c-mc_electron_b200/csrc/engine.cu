@@ -98,10 +98,17 @@ struct mcb200_ctx {
   int ncells = 0;
   unsigned int *h_pinned = nullptr;  // small pinned readback area
   int sm_count = 148;
+  // CUDA-event timing on the context's stream (mcb200_timing)
+  bool timing = false;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  double flight_ms = 0, step_ms = 0;
+  uint64_t flight_launches = 0, steps = 0, particles_flown = 0, launches = 0;
 
   ~mcb200_ctx() {
     if (device < 0) return;
     cudaSetDevice(device);
+    for (cudaEvent_t e : ev)
+      if (e) cudaEventDestroy(e);
     for (void *p : mesh_owned) cudaFree(p);
     for (void *p : owned) cudaFree(p);
     if (h_pinned) cudaFreeHost(h_pinned);
@@ -205,6 +212,9 @@ void upload_tables(mcb200_ctx *c) {
   d.dosh = dupload(t.dosh, c->owned);
   d.scattiih = dupload(t.scattiih, c->owned);
   d.dostetmax = dupload(t.dostetmax, c->owned);
+  d.dos = dupload(t.dos, c->owned);
+  d.sumdos = dupload(t.sumdos, c->owned);
+  for (int i = 0; i < 3; ++i) d.dosmax[i] = t.dosmax[i];
   d.ntlist = dupload(t.ntlist, c->owned); d.ptlist = dupload(t.ptlist, c->owned); d.tlist = dupload(t.tlist, c->owned);
   d.nslist = dupload(t.nslist, c->owned); d.pslist = dupload(t.pslist, c->owned); d.slist = dupload(t.slist, c->owned);
   d.ntlists = dupload(t.ntlists, c->owned); d.ptlists = dupload(t.ptlists, c->owned); d.tlists = dupload(t.tlists, c->owned);
@@ -555,6 +565,42 @@ int mcb200_download_particles(mcb200_ctx *c, mcb200_particles *p, size_t capacit
 
 size_t mcb200_num_particles(const mcb200_ctx *c) { return c ? c->n : 0; }
 
+int mcb200_seed_particles(mcb200_ctx *c, size_t n, const int32_t *cell_of, const double *charge, int type,
+                          uint64_t seed) {
+  if (!c || (n > 0 && (!cell_of || !charge)) || type < 0 || type > 1) return MCB200_ERR_ARG;
+  if (!c->mesh_set || !c->cells_set) return fail(c, MCB200_ERR_STATE, "mcb200_seed_particles needs mesh and cells");
+  if (c->n + n > c->capacity) return fail(c, MCB200_ERR_CAPACITY, "more particles than the context capacity");
+  for (size_t q = 0; q < n; ++q)
+    if (cell_of[q] < 0 || cell_of[q] >= c->ncells) return fail(c, MCB200_ERR_ARG, "cell index outside the mesh");
+  if (n == 0) return MCB200_OK;
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    std::vector<void *> tmp;
+    int *dcell = dalloc<int>(n, tmp);
+    double *dq = dalloc<double>(n, tmp);
+    ck(cudaMemcpyAsync(dcell, cell_of, n * sizeof(int), cudaMemcpyHostToDevice, c->stream), "copy");
+    ck(cudaMemcpyAsync(dq, charge, n * sizeof(double), cudaMemcpyHostToDevice, c->stream), "copy");
+    FlightCtx F;
+    F.T = c->dt;
+    F.M = c->mesh;
+    F.Y = c->y;
+    F.C = c->cb[0].d;
+    F.C.capacity = 0;
+    F.dt = 0;
+    F.seed = seed;
+    F.step = kSeedStreamStep;
+    launch_seed(F, c->pb[c->cur].d, (int)c->n, (int)n, dcell, dq, type, c->next_uid, grid_for(c, n, 256), c->stream);
+    ck(cudaGetLastError(), "seed kernel");
+    ck(cudaStreamSynchronize(c->stream), "sync");
+    for (void *p : tmp) cudaFree(p);
+    c->n += n;
+    c->next_uid += (uint32_t)n;
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
 int mcb200_step(mcb200_ctx *c, uint32_t step, uint64_t seed, double dt) {
   if (!c) return MCB200_ERR_ARG;
   if (!c->mesh_set || !c->cells_set || !c->fields_set)
@@ -570,11 +616,16 @@ int mcb200_step(mcb200_ctx *c, uint32_t step, uint64_t seed, double dt) {
     F.seed = seed;
     F.step = step;
     const int block = 256;
+    if (c->timing) ck(cudaEventRecord(c->ev[0], s), "event");
     // 1. main flight; copies go to generation 0
     ck(cudaMemsetAsync(c->cb[0].d.count, 0, sizeof(unsigned int), s), "memset");
     F.C = c->cb[0].d;
+    if (c->timing) ck(cudaEventRecord(c->ev[1], s), "event");
     launch_flight(F, c->pb[c->cur].d, (int)c->n, grid_for(c, c->n, block), block, s);
     ck(cudaGetLastError(), "flight kernel");
+    if (c->timing) ck(cudaEventRecord(c->ev[2], s), "event");
+    const size_t flown = c->n;
+    c->launches += c->n > 0 ? 1 : 0;
     // 2. copies fly the rest of the step, generation by generation
     unsigned int counts[mcb200_ctx::kGenerations] = {0, 0, 0, 0};
     int gens = 0;
@@ -593,6 +644,7 @@ int mcb200_step(mcb200_ctx *c, uint32_t step, uint64_t seed, double dt) {
       }
       launch_child_flight(F, c->cb[g].d, grid_for(c, counts[g], block), block, s);
       ck(cudaGetLastError(), "child flight kernel");
+      c->launches += 1;
     }
     // 3. uids for surviving copies, then append them to the store
     size_t total_children = 0;
@@ -616,20 +668,57 @@ int mcb200_step(mcb200_ctx *c, uint32_t step, uint64_t seed, double dt) {
       const unsigned int appended = c->h_pinned[0];
       n_all = c->n + appended;
       c->next_uid += appended;
+      c->launches += 2 * gens + 1;
     }
     // 4. drop caught particles and counting-sort the store by cell
     const int other = 1 - c->cur;
     launch_cell_sort(c->pb[c->cur].d, (int)n_all, c->pb[other].d, c->ncells, c->mesh.nx, c->mesh.nz, c->hist,
                      c->offsets, c->tile_sums, c->total, grid_for(c, n_all, 256), s);
     ck(cudaGetLastError(), "cell sort");
+    c->launches += n_all > 0 ? 5 : 3;
     ck(cudaMemcpyAsync(c->h_pinned, c->total, sizeof(unsigned int), cudaMemcpyDeviceToHost, s), "count");
+    if (c->timing) ck(cudaEventRecord(c->ev[3], s), "event");
     ck(cudaStreamSynchronize(s), "sync");
     c->n = c->h_pinned[0];
     c->cur = other;
+    if (c->timing) {
+      float ms_flight = 0, ms_step = 0;
+      ck(cudaEventElapsedTime(&ms_flight, c->ev[1], c->ev[2]), "elapsed");
+      ck(cudaEventElapsedTime(&ms_step, c->ev[0], c->ev[3]), "elapsed");
+      c->flight_ms += ms_flight;
+      c->step_ms += ms_step;
+      c->flight_launches += flown > 0 ? 1 : 0;
+      c->particles_flown += flown;
+      c->steps += 1;
+    }
     return MCB200_OK;
   } catch (const std::exception &e) {
     return fail(c, MCB200_ERR_CUDA, e.what());
   }
+}
+
+int mcb200_set_timing(mcb200_ctx *c, int enable) {
+  if (!c) return MCB200_ERR_ARG;
+  if (c->device < 0) return fail(c, MCB200_ERR_STATE, "host-only context");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    for (cudaEvent_t &e : c->ev)
+      if (!e) ck(cudaEventCreate(&e), "cudaEventCreate");
+    c->timing = enable != 0;
+    c->flight_ms = c->step_ms = 0;
+    c->flight_launches = c->steps = c->particles_flown = c->launches = 0;
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_get_timing(const mcb200_ctx *c, double *out, int n) {
+  if (!c || !out) return MCB200_ERR_ARG;
+  const double v[6] = {c->flight_ms, (double)c->flight_launches, c->step_ms, (double)c->steps,
+                       (double)c->particles_flown, (double)c->launches};
+  for (int i = 0; i < n && i < 6; ++i) out[i] = v[i];
+  return MCB200_OK;
 }
 
 int mcb200_sync(mcb200_ctx *c) {

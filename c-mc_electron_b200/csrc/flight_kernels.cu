@@ -200,7 +200,74 @@ __global__ void child_keys(DevChildren c, int n, uint64_t *keys, uint8_t *alive)
   alive[i] = (c.meta[i] & kMetaDead) ? 0 : 1;
 }
 
+// ---- initial ensemble ---------------------------------------------------------
+// New particle q (uid = uid0 + q) of carrier `type` in cell cell_of[q]:
+// position uniform in the cell (init_particle_data,
+// src/particle_init.cpp:185-207) and k-state from select_kstate
+// (src/mcmodel.cpp:3006-3057): energy from the Boltzmann distribution,
+// accepted against the DOS, band by the DOS share, k uniform on the
+// iso-energy surface.  Draws: stream (seed, uid, kSeedStreamStep, 0).
+
+__global__ void __launch_bounds__(256) seed_kernel(FlightCtx F, DevParticles P, int offset, int n,
+                                                   const int *cell_of, const double *charge, int type,
+                                                   uint32_t uid0) {
+  __shared__ SymSmem S;
+  load_sym(S, F.T);
+  const DevTables &T = F.T;
+  const double tmp_const = 1 - exp(-T.emax);
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    Flyer f(F, S);
+    const int c = cell_of[q];
+    const int kc = c % F.M.nz, ic = (c / F.M.nz) % F.M.nx, jc = c / (F.M.nz * F.M.nx);
+    f.ic = ic; f.jc = jc; f.kc = kc;
+    f.type = type;
+    f.uid = uid0 + q;
+    f.sub = 0;
+    f.n = 0;
+    double lamda = f.Random();
+    f.x = lamda * F.M.lx[ic] + (1 - lamda) * F.M.lx[ic + 1];
+    lamda = f.Random();
+    f.y = lamda * F.M.ly[jc] + (1 - lamda) * F.M.ly[jc + 1];
+    lamda = f.Random();
+    f.z = lamda * F.M.lz[kc] + (1 - lamda) * F.M.lz[kc + 1];
+    f.itet = 0;
+    f.kx = f.ky = f.kz = 0;
+    bool ok = false;
+    for (int attempt = 0; attempt < 100000 && !ok; ++attempt) {
+      f.energy = -log(1 - f.Random() * tmp_const);
+      // CALDOSSUM (src/Band.cpp:2267-2295) and CALDOS (:2234-2264)
+      const TabPos p = tab_pos(T, f.energy);
+      const double ddos = tab_at_strided(T.sumdos + type, 3, p);
+      double rdos = f.Random() * T.dosmax[type];
+      if (rdos > ddos) continue;
+      for (f.iband = T.bandof[type]; f.iband < T.bandof[type] + T.nband[type]; f.iband++) {
+        rdos -= tab_at(T.dos + (size_t)f.iband * kNT, p);
+        if (rdos < 0) break;
+      }
+      f.isym = ((int)(f.Random() * 48)) % 48;
+      if (f.iband >= T.bandof[type] + T.nband[type]) continue;  // rounding left no band: draw again
+      f.get_state();
+      if (f.self) continue;
+      ok = true;
+    }
+    if (!ok) count(F.Y, kCntNoTet);
+    const int o = offset + q;
+    P.x[o] = f.x; P.y[o] = f.y; P.z[o] = f.z;
+    P.kx[o] = f.kx; P.ky[o] = f.ky; P.kz[o] = f.kz;
+    P.energy[o] = f.energy;
+    P.charge[o] = charge[q];
+    P.cell[o] = pack_cell(ic, jc, kc);
+    P.itet[o] = f.itet;
+    P.meta[o] = (uint32_t)f.isym | ((uint32_t)type << 8) | (ok ? 0u : kMetaDead);
+    P.uid[o] = f.uid;
+  }
+}
+
 // ---- host-side launchers ----------------------------------------------------
+void launch_seed(const FlightCtx &F, const DevParticles &P, int offset, int n, const int *cell_of,
+                 const double *charge, int type, uint32_t uid0, int grid, cudaStream_t s) {
+  if (n > 0) seed_kernel<<<grid, 256, 0, s>>>(F, P, offset, n, cell_of, charge, type, uid0);
+}
 void launch_flight(const FlightCtx &F, const DevParticles &P, int n, int grid, int block, cudaStream_t s) {
   if (n > 0) flight_kernel<<<grid, block, 0, s>>>(F, P, n);
 }

@@ -308,7 +308,7 @@ struct Flyer {
     const double *d = F.T.dostetmax + (size_t)ib * kNT;
     if (eed <= 0.0) return d[0];
     if (eed >= F.T.emax) return d[kNT - 1];
-    const int itab = (int)(eed / F.T.dtable);
+    const int itab = min((int)(eed / F.T.dtable), kNT - 2);  // eed just below emax may round to the last point
     return d[itab] > d[itab + 1] ? d[itab] : d[itab + 1];
   }
 
@@ -378,7 +378,7 @@ struct Flyer {
     const double *s = F.T.sumscatt;
     if (eed <= 0.0) return s[ib];
     if (eed >= F.T.emax) return s[(size_t)(kNT - 1) * kMNB + ib];
-    const int itab = (int)(eed / F.T.dtable);
+    const int itab = min((int)(eed / F.T.dtable), kNT - 2);
     const double intp = (eed - F.T.energy[itab]) / (F.T.energy[itab + 1] - F.T.energy[itab]);
     return s[(size_t)itab * kMNB + ib] + intp * (s[(size_t)(itab + 1) * kMNB + ib] - s[(size_t)itab * kMNB + ib]);
   }
@@ -590,8 +590,20 @@ struct Flyer {
   }
   // Diffuse, src/CellHit.cpp:243-386.
   __device__ void Diffuse();
-  // Pass, src/CellHit.cpp:389-413.
+  __device__ bool inside_mesh(int i, int j, int k) const {
+    return i >= 0 && j >= 0 && k >= 0 && i < F.M.nx && j < F.M.ny && k < F.M.nz;
+  }
+  // Pass, src/CellHit.cpp:389-413.  A PASS rule on the outer x / z boundary
+  // would move the particle off the mesh (the reference indexes out of its
+  // arrays there); the engine removes such a particle and counts it.
   __device__ void Pass() {
+    int ni, nj, nk;
+    neighbour(ni, nj, nk);
+    if (!inside_mesh(ni, nj, nk)) {
+      count(F.Y, kCntUnfinished);
+      catch_ = true;
+      return;
+    }
     const DevMesh &M = F.M;
     switch (idir) {
       case kUp: x = M.lx[ic]; ic--; break;
@@ -649,6 +661,10 @@ struct Flyer {
     if (idir == kLeft) tally_add_i64(F.Y.lcurrent + jc, charge, kChargeScale);
     int i, j, k;
     neighbour(i, j, k);
+    if (!inside_mesh(i, j, k)) {
+      count(F.Y, kCntUnfinished);
+      return;
+    }
     const DevChildren &C = F.C;
     const unsigned slot = atomicAdd(C.count, 1u);
     const uint32_t csub = sub * 16u + 1u + (uint32_t)nchild++;
@@ -669,7 +685,7 @@ struct Flyer {
   __device__ void Catch(bool with_current) {
     int i, j, k;
     neighbour(i, j, k);
-    const int icont = F.M.contact[cell_index(i, j, k)] - 1;
+    const int icont = inside_mesh(i, j, k) ? F.M.contact[cell_index(i, j, k)] - 1 : -1;
     if (with_current) {
       if (idir == kRight) tally_add_i64(F.Y.rcurrent + jc + 1, charge, kChargeScale);
       if (idir == kLeft) tally_add_i64(F.Y.lcurrent + jc, charge, kChargeScale);
@@ -725,7 +741,7 @@ struct Flyer {
   // surface-phonon branches' drand defined (see file note).
   __device__ void ParticleSurfaceScatter() {
     if (Random() * surf_gamma < rough_rate) {
-      idir = F.M.surface_dir[F.M.nearest_surf[cell_index()]];
+      idir = F.M.surface_dir[min(max(F.M.nearest_surf[cell_index()], 0), kMaxSurfaces - 1)];
       Diffuse();
       return;
     }

@@ -134,7 +134,7 @@ __device__ __forceinline__ TabPos tab_pos(const DevTables &T, double eed) {
   else if (eed >= T.emax) { p.mode = 1; p.itab = kNT - 1; p.intp = 0; }
   else {
     p.mode = 2;
-    p.itab = (int)(eed / T.dtable);
+    p.itab = min((int)(eed / T.dtable), kNT - 2);
     p.intp = (eed - T.energy[p.itab]) / (T.energy[p.itab + 1] - T.energy[p.itab]);
   }
   return p;
@@ -142,6 +142,11 @@ __device__ __forceinline__ TabPos tab_pos(const DevTables &T, double eed) {
 __device__ __forceinline__ double tab_at(const double *tab, const TabPos &p) {
   if (p.mode != 2) return tab[p.itab];
   return tab[p.itab] + p.intp * (tab[p.itab + 1] - tab[p.itab]);
+}
+__device__ __forceinline__ double tab_at_strided(const double *tab, int stride, const TabPos &p) {
+  if (p.mode != 2) return tab[(size_t)p.itab * stride];
+  const double a = tab[(size_t)p.itab * stride], b = tab[(size_t)(p.itab + 1) * stride];
+  return a + p.intp * (b - a);
 }
 
 // Entry idx of Band::CALSCATTE (src/Band.cpp:2165-2231) for initial band ib.

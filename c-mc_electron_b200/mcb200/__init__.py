@@ -73,6 +73,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mcb200_sync.argtypes = [vp]
     lib.mcb200_get_tallies.argtypes = [vp, c.POINTER(c.c_uint64), dp, dp, dp, dp, dp]
     lib.mcb200_reset_tallies.argtypes = [vp]
+    lib.mcb200_seed_particles.argtypes = [vp, c.c_size_t, i32p, dp, c.c_int, c.c_uint64]
+    lib.mcb200_set_timing.argtypes = [vp, c.c_int]
+    lib.mcb200_get_timing.argtypes = [vp, dp, c.c_int]
     return lib
 
 
@@ -196,6 +199,22 @@ class Engine:
         arrs = {k: np.ascontiguousarray(particles[k], dtype=t) for k, t in PARTICLE_FIELDS.items()}
         n = len(arrs["x"])
         self._check(self._lib.mcb200_upload_particles(self._ctx, n, ctypes.byref(self._soa(arrs))), "upload")
+
+    def seed(self, cell_of, charge, carrier_type: int, seed: int):
+        """Append particles sampled on the GPU (mcb200_seed_particles)."""
+        cell_of = np.ascontiguousarray(cell_of, dtype=np.int32)
+        charge = np.ascontiguousarray(charge, dtype=np.float64)
+        self._check(self._lib.mcb200_seed_particles(self._ctx, cell_of.size, _ptr(cell_of, ctypes.c_int32),
+                                                    _ptr(charge, ctypes.c_double), carrier_type, seed), "seed")
+
+    def set_timing(self, enable: bool = True):
+        self._check(self._lib.mcb200_set_timing(self._ctx, int(enable)), "set_timing")
+
+    def timing(self) -> dict:
+        out = np.zeros(6)
+        self._check(self._lib.mcb200_get_timing(self._ctx, _ptr(out, ctypes.c_double), 6), "timing")
+        keys = ["flight_ms", "flight_launches", "step_ms", "steps", "particles_flown", "launches"]
+        return dict(zip(keys, out.tolist()))
 
     def num_particles(self) -> int:
         return int(self._lib.mcb200_num_particles(self._ctx))

@@ -126,6 +126,17 @@ int mcb200_upload_particles(mcb200_ctx *ctx, size_t n, const mcb200_particles *p
 int mcb200_download_particles(mcb200_ctx *ctx, mcb200_particles *p, size_t capacity, size_t *n_out);
 size_t mcb200_num_particles(const mcb200_ctx *ctx);
 
+/* Append n particles of carrier `type` (0 electron, 1 hole) sampled on the
+ * GPU the way the reference initialises them: cell_of[q] is the cell of new
+ * particle q and charge[q] its charge; the position is uniform in the cell
+ * (init_particle_data, src/particle_init.cpp:112-219) and the k-state follows
+ * select_kstate (src/mcmodel.cpp:3006-3057): Boltzmann energy accepted
+ * against the DOS, band by DOS share, k uniform on the iso-energy surface.
+ * New uids continue after the largest uid in the store; each particle draws
+ * from its own stream (seed, uid, 0xfffffffd, 0). */
+int mcb200_seed_particles(mcb200_ctx *ctx, size_t n, const int32_t *cell_of, const double *charge, int type,
+                          uint64_t seed);
+
 /* One transport step: every particle flies `dt` with the reference's event
  * loop on its own random stream (seed, uid, step), copies made by
  * GENERATE / GENREF finish the step, caught particles are removed, copies
@@ -135,6 +146,13 @@ int mcb200_step(mcb200_ctx *ctx, uint32_t step, uint64_t seed, double dt);
 
 /* Wait for the context's stream. */
 int mcb200_sync(mcb200_ctx *ctx);
+
+/* Device timing of mcb200_step with CUDA events on the context's own stream
+ * (enable != 0 resets the accumulators and turns timing on).
+ * mcb200_get_timing: out[0..n) = flight-kernel ms, flight-kernel launches,
+ * whole-step ms, steps, particles flown, engine kernel launches. */
+int mcb200_set_timing(mcb200_ctx *ctx, int enable);
+int mcb200_get_timing(const mcb200_ctx *ctx, double *out, int n);
 
 /* Tallies since the last reset.  Any output may be NULL.
  * counters[MCB200_NUM_COUNTERS]; contact[16*6] per contact {NumParGen,

@@ -108,6 +108,11 @@ int orc_init(const char *input_file, const char *table_dir, uint64_t seed, int m
   }
   std::vector<char> fname(path.begin(), path.end());
   fname.push_back('\0');
+  /* The mesh lives in globals that read_grid_file appends to
+   * (src/utils.cpp:16-18, src/mcmodel.cpp:4651-4672): start them empty so a
+   * second initialisation in the same process sees only its own deck. */
+  lx.clear(); ly.clear(); lz.clear();
+  dx.clear(); dy.clear(); dz.clear();
   MeshQuantities *mq = new MeshQuantities;
   g_mq = mq;
   mq->init_phpysical_parameter(fname.data());
