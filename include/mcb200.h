@@ -162,6 +162,39 @@ int mcb200_get_tallies(mcb200_ctx *ctx, uint64_t *counters, double *contact, dou
                        double *heat_e, double *heat_h);
 int mcb200_reset_tallies(mcb200_ctx *ctx);
 
+/* Particle store in device memory, in the engine's own layout (what
+ * mcb200_step keeps per particle): cell packs i | j << 10 | k << 20; meta
+ * packs isym | type << 8, and bit 16 set marks a particle to be dropped. */
+typedef struct {
+  double *x, *y, *z;
+  double *kx, *ky, *kz;
+  double *energy, *charge;
+  uint32_t *cell;
+  int32_t *itet;
+  uint32_t *meta;
+  uint32_t *uid;
+} mcb200_device_particles;
+
+#define MCB200_STATIC_SORT_MAX_CELLS 262144
+
+/* No counterpart in the reference.  Counting sort of a caller-owned device
+ * particle store by mesh cell (the sort mcb200_step runs after each flight)
+ * that allocates no device memory: for callers that cannot call cudaMalloc,
+ * such as a host framework that owns every device buffer and lends out
+ * slices of its own pool, or code that must not allocate while other work
+ * holds the device.  The caller passes the input and the output arrays
+ * (n entries each; particles with meta bit 16 are dropped, *n_out receives
+ * how many remain); the scratch is one static device array of
+ * MCB200_STATIC_SORT_MAX_CELLS cells (2 MiB, held by every GPU that loads
+ * the library until the process exits), and larger meshes return
+ * MCB200_ERR_CAPACITY.  The first call on a device looks the array's device
+ * address up and caches it; make that first call before any stream capture.
+ * Every call shares the array, so calls that overlap on the GPU (two
+ * streams, two threads) race: serialise them.  Order within a cell is not
+ * specified.  `stream` is a cudaStream_t (NULL: the legacy default stream). */
+int mcb200_sort_particles_static(const mcb200_device_particles *in, size_t n, int nx, int ny, int nz,
+                                 const mcb200_device_particles *out, size_t *n_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
