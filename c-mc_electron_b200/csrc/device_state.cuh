@@ -15,6 +15,7 @@ constexpr int kMWLE = 325;      // coarse tetrahedron-list bins (40 meV)
 constexpr int kMWLES = 60;      // fine tetrahedron-list bins (2 meV)
 constexpr int kMaxContacts = 16;
 constexpr int kMaxSurfaces = 30;
+constexpr int kSeedGridN = 96;  // cells per axis of the lowest-band walk-seed grid
 // `step` word of the random stream used for initial-ensemble sampling.
 constexpr uint32_t kSeedStreamStep = 0xfffffffdu;
 
@@ -75,6 +76,10 @@ struct DevTables {
   double grid_lo[3], grid_inv[3];
   const int *grid_start;      // [kMNB][grid_n^3 + 1]
   const int *grid_tets;
+  // seed grid of the lowest conduction band: kSeedGridN^3 cells over the
+  // same box, each holding a starting tetrahedron for the mesh walk (-1: none)
+  double seed_inv[3];
+  const int *seed_grid;
   // symmetry (copied to shared memory by each block)
   const int *symi;            // [48*6] matsym[c][s] stored as s*6+c
   const int *newisym;         // [5][48]

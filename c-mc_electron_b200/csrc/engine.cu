@@ -7,9 +7,11 @@
 #include <vector>
 
 #include "engine_kernels.h"
+#include "field_kernels.h"
 #include "flight_physics.cuh"
 #include "fullband_tables.h"
 #include "mcb200.h"
+#include "poisson_setup.h"
 
 using namespace mcb200;
 
@@ -98,6 +100,10 @@ struct mcb200_ctx {
   int ncells = 0;
   unsigned int *h_pinned = nullptr;  // small pinned readback area
   int sm_count = 148;
+  // deposition / Poisson (mcb200_set_device)
+  FieldBuffers fb{};
+  bool device_set = false;
+  double *h_scratch = nullptr;  // pinned, 8 doubles
   // CUDA-event timing on the context's stream (mcb200_timing)
   bool timing = false;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -112,6 +118,7 @@ struct mcb200_ctx {
     for (void *p : mesh_owned) cudaFree(p);
     for (void *p : owned) cudaFree(p);
     if (h_pinned) cudaFreeHost(h_pinned);
+    if (h_scratch) cudaFreeHost(h_scratch);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -167,6 +174,41 @@ void build_kgrid(mcb200_ctx *c, int g) {
   for (int a = 0; a < 3; ++a) { c->dt.grid_lo[a] = lo[a]; c->dt.grid_inv[a] = inv[a]; }
   c->dt.grid_start = dupload(start, c->owned);
   c->dt.grid_tets = dupload(tets, c->owned);
+
+  // Seed grid for the lowest conduction band (the band impurity scattering
+  // lands in): per fine cell, a tetrahedron that contains the cell centre,
+  // else the first tetrahedron overlapping it, else -1.  A mesh walk from
+  // the seed reaches the target point in a step or two.
+  const int sg = kSeedGridN;
+  std::vector<int> seed((size_t)sg * sg * sg, -1);
+  const int band = t.bandof[0];
+  const int *bst = &start[(size_t)band * (cells + 1)];
+  auto contains = [&](int it, double a, double b, double cc) {
+    for (int f = 0; f < 4; ++f)
+      if (t.D(0, f, it) * a + t.D(1, f, it) * b + t.D(2, f, it) * cc - t.D(3, f, it) < -1e-13) return false;
+    return true;
+  };
+  for (int i = 0; i < sg; ++i)
+    for (int j = 0; j < sg; ++j)
+      for (int k = 0; k < sg; ++k) {
+        const double p[3] = {lo[0] + (i + 0.5) * (hi[0] - lo[0]) / sg, lo[1] + (j + 0.5) * (hi[1] - lo[1]) / sg,
+                             lo[2] + (k + 0.5) * (hi[2] - lo[2]) / sg};
+        int q[3];
+        for (int a = 0; a < 3; ++a) q[a] = std::max(0, std::min(g - 1, (int)std::floor((p[a] - lo[a]) * inv[a])));
+        const int coarse = (q[0] * g + q[1]) * g + q[2];
+        int pick = -1;
+        for (int e = bst[coarse]; e < bst[coarse + 1]; ++e) {
+          const int it = tets[e];
+          if (pick < 0) pick = it;
+          if (contains(it, p[0], p[1], p[2])) {
+            pick = it;
+            break;
+          }
+        }
+        seed[((size_t)i * sg + j) * sg + k] = pick;
+      }
+  for (int a = 0; a < 3; ++a) c->dt.seed_inv[a] = sg / (hi[a] - lo[a]);
+  c->dt.seed_grid = dupload(seed, c->owned);
 }
 
 void upload_tables(mcb200_ctx *c) {
@@ -378,7 +420,8 @@ int mcb200_copy_table(const mcb200_ctx *c, const char *name, void *out, size_t b
   return fail(const_cast<mcb200_ctx *>(c), MCB200_ERR_ARG, "unknown table " + n);
 }
 
-int mcb200_set_mesh(mcb200_ctx *c, int nx, int ny, int nz, const double *lx, const double *ly, const double *lz) {
+int mcb200_set_mesh(mcb200_ctx *c, int nx, int ny, int nz, const double *lx, const double *ly, const double *lz,
+                    const double *wx, const double *wy, const double *wz) {
   if (c && c->device < 0) return fail(c, MCB200_ERR_STATE, "host-only context");
   if (!c || nx <= 0 || ny <= 0 || nz <= 0 || nx > 1023 || ny > 1023 || nz > 1023 || !lx || !ly || !lz)
     return c ? fail(c, MCB200_ERR_ARG, "bad mesh") : MCB200_ERR_ARG;
@@ -390,9 +433,9 @@ int mcb200_set_mesh(mcb200_ctx *c, int nx, int ny, int nz, const double *lx, con
     c->hly.assign(ly, ly + ny + 1);
     c->hlz.assign(lz, lz + nz + 1);
     std::vector<double> dx(nx), dy(ny), dz(nz);
-    for (int i = 0; i < nx; ++i) dx[i] = c->hlx[i + 1] - c->hlx[i];
-    for (int i = 0; i < ny; ++i) dy[i] = c->hly[i + 1] - c->hly[i];
-    for (int i = 0; i < nz; ++i) dz[i] = c->hlz[i + 1] - c->hlz[i];
+    for (int i = 0; i < nx; ++i) dx[i] = wx ? wx[i] : c->hlx[i + 1] - c->hlx[i];
+    for (int i = 0; i < ny; ++i) dy[i] = wy ? wy[i] : c->hly[i + 1] - c->hly[i];
+    for (int i = 0; i < nz; ++i) dz[i] = wz ? wz[i] : c->hlz[i + 1] - c->hlz[i];
     DevMesh &m = c->mesh;
     m = DevMesh{};
     m.nx = nx; m.ny = ny; m.nz = nz;
@@ -423,7 +466,8 @@ int mcb200_set_mesh(mcb200_ctx *c, int nx, int ny, int nz, const double *lx, con
     c->tile_sums = dalloc<unsigned int>((cells + 1023) / 1024 + 1, c->mesh_owned);
     ck(cudaStreamSynchronize(c->stream), "sync");
     c->mesh_set = true;
-    c->cells_set = c->fields_set = false;
+    c->cells_set = c->fields_set = c->device_set = false;
+    c->fb = FieldBuffers{};
     return mcb200_reset_tallies(c);
   } catch (const std::exception &e) {
     return fail(c, MCB200_ERR_CUDA, e.what());
@@ -779,6 +823,152 @@ int mcb200_reset_tallies(mcb200_ctx *c) {
       ck(cudaMemsetAsync(c->y.heat_h, 0, sizeof(long long) * nodes, s), "memset");
     }
     ck(cudaStreamSynchronize(s), "sync");
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_set_device(mcb200_ctx *c, const int32_t *material, const double *donor, const double *acceptor,
+                      int n_contacts, const double *vapp, const double *phims, int n_planes, const int32_t *planes) {
+  if (!c || !material || !donor || !acceptor || n_contacts < 0 || n_contacts > kMaxContacts || n_planes < 0 ||
+      (n_planes > 0 && !planes) || (n_contacts > 0 && (!vapp || !phims)))
+    return c ? fail(c, MCB200_ERR_ARG, "mcb200_set_device: bad arguments") : MCB200_ERR_ARG;
+  if (!c->mesh_set) return fail(c, MCB200_ERR_STATE, "mcb200_set_device before mcb200_set_mesh");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    const DevMesh &m = c->mesh;
+    std::vector<double> dx(m.nx), dy(m.ny), dz(m.nz);
+    ck(cudaMemcpy(dx.data(), m.dx, dx.size() * 8, cudaMemcpyDeviceToHost), "copy");
+    ck(cudaMemcpy(dy.data(), m.dy, dy.size() * 8, cudaMemcpyDeviceToHost), "copy");
+    ck(cudaMemcpy(dz.data(), m.dz, dz.size() * 8, cudaMemcpyDeviceToHost), "copy");
+    std::vector<ContactPlane> pl(n_planes);
+    for (int q = 0; q < n_planes; ++q) {
+      const int32_t *r = planes + 7 * q;
+      pl[q] = ContactPlane{r[0], r[1], r[2], r[3], r[4], r[5], r[6]};
+    }
+    const Units &u = c->tab.u;
+    const double eps[6] = {0.0, u.eps_vacuum, u.eps_oxide, u.eps_silicon, 0.0, 0.0};
+    const PoissonSetup s = PoissonSetup::build(m.nx, m.ny, m.nz, dx.data(), dy.data(), dz.data(), material, donor,
+                                               acceptor, c->tab.ni, eps, pl,
+                                               std::vector<double>(vapp, vapp + n_contacts),
+                                               std::vector<double>(phims, phims + n_contacts));
+    const size_t cells = (size_t)c->ncells, nodes = (size_t)s.nodes();
+    std::vector<double> dinv(nodes);
+    for (size_t p = 0; p < nodes; ++p) dinv[p] = 1.0 / s.stencil[p * 7 + 6];
+    FieldBuffers &f = c->fb;
+    f.cvol = dupload(s.cvol, c->mesh_owned);
+    f.pvol = dupload(s.pvol, c->mesh_owned);
+    f.pdop = dupload(s.pdop, c->mesh_owned);
+    f.vadd = dupload(s.vadd, c->mesh_owned);
+    f.stencil = dupload(s.stencil, c->mesh_owned);
+    f.diag_inv = dupload(dinv, c->mesh_owned);
+    f.dirichlet = dupload(s.dirichlet, c->mesh_owned);
+    f.bc_vapp = dupload(s.bc_vapp, c->mesh_owned);
+    f.bc_phims = dupload(s.bc_phims, c->mesh_owned);
+    f.acc_cell = dalloc<long long>(3 * cells, c->mesh_owned);
+    f.acc_node = dalloc<long long>(nodes, c->mesh_owned);
+    f.cell_e = dalloc<double>(cells, c->mesh_owned);
+    f.cell_h = dalloc<double>(cells, c->mesh_owned);
+    f.density = dalloc<double>(nodes, c->mesh_owned);
+    f.rhs = dalloc<double>(nodes, c->mesh_owned);
+    f.potential = dalloc<double>(nodes, c->mesh_owned);
+    f.cg_r = dalloc<double>(nodes, c->mesh_owned);
+    f.cg_z = dalloc<double>(nodes, c->mesh_owned);
+    f.cg_p = dalloc<double>(nodes, c->mesh_owned);
+    f.cg_q = dalloc<double>(nodes, c->mesh_owned);
+    f.cg_part = dalloc<double>(512, c->mesh_owned);
+    f.cg_scalars = dalloc<double>(8, c->mesh_owned);
+    f.abs_sum = dalloc<unsigned long long>(4, c->mesh_owned);
+    ck(cudaMemset(f.potential, 0, nodes * sizeof(double)), "memset");
+    ck(cudaMemset(f.density, 0, nodes * sizeof(double)), "memset");
+    if (!c->h_scratch) ck(cudaMallocHost(&c->h_scratch, 8 * sizeof(double)), "cudaMallocHost");
+    c->device_set = true;
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_ARG, e.what());
+  }
+}
+
+int mcb200_deposit(mcb200_ctx *c) {
+  if (!c) return MCB200_ERR_ARG;
+  if (!c->device_set || !c->cells_set) return fail(c, MCB200_ERR_STATE, "mcb200_deposit needs set_device and set_cells");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    cudaStream_t s = c->stream;
+    const DevParticles &P = c->pb[c->cur].d;
+    const int grid = grid_for(c, c->n, 256);
+    launch_charge_bounds(P, (int)c->n, c->fb.abs_sum, grid, s);
+    ck(cudaMemcpyAsync(c->h_scratch, c->fb.abs_sum, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
+       "copy");
+    ck(cudaStreamSynchronize(s), "sync");
+    unsigned long long b[4];
+    std::memcpy(b, c->h_scratch, sizeof(b));
+    double qmax[2];
+    std::memcpy(&qmax[0], &b[0], 8);
+    std::memcpy(&qmax[1], &b[1], 8);
+    // count x max|q| bounds every sum of a type; each sum gets 61 bits of range
+    auto unit = [](double bound) {
+      return std::ldexp(1.0, 61 - (int)std::ceil(std::log2(std::max(bound, 1e-300))));
+    };
+    const double be = (double)b[2] * qmax[0], bh = (double)b[3] * qmax[1];
+    const DepositScales S{{unit(be), unit(bh), unit(be + bh)}};
+    launch_deposit(P, (int)c->n, c->mesh, c->fb, S, grid, s);
+    ck(cudaGetLastError(), "deposit");
+    ck(cudaStreamSynchronize(s), "sync");
+    c->fields_set = true;
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_solve_poisson(mcb200_ctx *c, double rel_tol, int max_iter, int *iterations, double *rel_residual) {
+  if (!c || rel_tol <= 0 || max_iter < 0) return MCB200_ERR_ARG;
+  if (!c->device_set) return fail(c, MCB200_ERR_STATE, "mcb200_solve_poisson needs mcb200_set_device");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    cudaStream_t s = c->stream;
+    const int nodes = (c->mesh.nx + 1) * (c->mesh.ny + 1) * (c->mesh.nz + 1);
+    launch_rhs(nodes, c->fb, s);
+    if (cg_solve(c->mesh, c->fb, rel_tol, max_iter, s, c->h_scratch, iterations, rel_residual))
+      return fail(c, MCB200_ERR_CUDA, "Poisson solve failed");
+    launch_pot2field(c->mesh, c->fb.potential, s);
+    ck(cudaGetLastError(), "pot2field");
+    ck(cudaStreamSynchronize(s), "sync");
+    c->fields_set = true;
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_get_array(mcb200_ctx *c, const char *name, double *out, size_t n) {
+  if (!c || !name || !out) return MCB200_ERR_ARG;
+  if (!c->mesh_set) return fail(c, MCB200_ERR_STATE, "mcb200_get_array before mcb200_set_mesh");
+  const std::string nm(name);
+  const size_t cells = (size_t)c->ncells, nodes = (size_t)(c->mesh.nx + 1) * (c->mesh.ny + 1) * (c->mesh.nz + 1);
+  const double *src = nullptr;
+  size_t len = 0;
+  if (nm == "rho") { src = c->mesh.rho; len = cells; }
+  else if (nm == "efield") { src = c->mesh.efield; len = 3 * cells; }
+  else if (nm == "hfield") { src = c->mesh.hfield; len = 3 * cells; }
+  else if (c->device_set && nm == "cell_charge_e") { src = c->fb.cell_e; len = cells; }
+  else if (c->device_set && nm == "cell_charge_h") { src = c->fb.cell_h; len = cells; }
+  else if (c->device_set && nm == "cell_volume") { src = c->fb.cvol; len = cells; }
+  else if (c->device_set && nm == "node_density") { src = c->fb.density; len = nodes; }
+  else if (c->device_set && nm == "node_volume") { src = c->fb.pvol; len = nodes; }
+  else if (c->device_set && nm == "node_doping") { src = c->fb.pdop; len = nodes; }
+  else if (c->device_set && nm == "vadd") { src = c->fb.vadd; len = nodes; }
+  else if (c->device_set && nm == "rhs") { src = c->fb.rhs; len = nodes; }
+  else if (c->device_set && nm == "potential") { src = c->fb.potential; len = nodes; }
+  else if (c->device_set && nm == "stencil") { src = c->fb.stencil; len = 7 * nodes; }
+  else return fail(c, MCB200_ERR_ARG, "unknown array " + nm);
+  if (n < len) return fail(c, MCB200_ERR_CAPACITY, "output smaller than array " + nm);
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    ck(cudaStreamSynchronize(c->stream), "sync");
+    ck(cudaMemcpy(out, src, len * sizeof(double), cudaMemcpyDeviceToHost), "copy");
     return MCB200_OK;
   } catch (const std::exception &e) {
     return fail(c, MCB200_ERR_CUDA, e.what());

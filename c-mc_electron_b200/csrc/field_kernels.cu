@@ -1,0 +1,350 @@
+// field_kernels.cu -- deposition, Poisson solve and field update on the GPU.
+//
+//  * deposit: MeshQuantities::compute_cell_charge (src/mcmodel.cpp:2664-2712)
+//    and particle_to_density (:348-417) in one pass over the particle store,
+//    summed in int64 fixed point so the result does not depend on thread
+//    order.  The fixed-point unit is chosen per call from the store's total
+//    |charge| (every cell or node sum is bounded by it), 2^61 / sum.
+//  * Poisson: the reference factorises its FV matrix with KLU and solves it
+//    every step (linear_poisson_solver, :2714-2730).  Here the Dirichlet
+//    contact rows are eliminated, which leaves a symmetric positive-definite
+//    system, and Jacobi-preconditioned CG iterates it in FP64 to the
+//    requested relative residual.  Dot products use fixed-order two-stage
+//    reductions, so a solve is bit-reproducible.
+//  * pot2field (:2776-2855): cell field from the 8 corner potentials,
+//    stored as felt by each carrier (ChargeSign applied).
+#include "device_state.cuh"
+#include "field_kernels.h"
+
+namespace mcb200 {
+
+constexpr uint32_t kDeadBit = 1u << 16;
+
+// Per carrier type: the largest |q| (as its IEEE bit pattern, which orders
+// like the value for non-negative doubles) and the particle count.  count x
+// max |q| bounds every cell or node sum of that type, exactly and
+// independently of thread order.  out = {max_e bits, max_h bits, n_e, n_h}.
+__global__ void charge_bounds_kernel(const double *charge, const uint32_t *meta, int n, unsigned long long *out) {
+  unsigned long long mx[2] = {0, 0}, cnt[2] = {0, 0};
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const uint32_t m = meta[p];
+    if (m & kDeadBit) continue;
+    const int t = ((m >> 8) & 255) == 0 ? 0 : 1;
+    const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(charge[p]));
+    mx[t] = b > mx[t] ? b : mx[t];
+    cnt[t] += 1;
+  }
+  for (int t = 0; t < 2; ++t) {
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long om = __shfl_down_sync(0xffffffffu, mx[t], o);
+      mx[t] = om > mx[t] ? om : mx[t];
+      cnt[t] += __shfl_down_sync(0xffffffffu, cnt[t], o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicMax(out + t, mx[t]);
+      atomicAdd(out + 2 + t, cnt[t]);
+    }
+  }
+}
+
+__device__ __forceinline__ void fx_add(long long *p, double v, double scale) {
+  atomicAdd(reinterpret_cast<unsigned long long *>(p), (unsigned long long)__double2ll_rn(v * scale));
+}
+
+// scale[0]: electron cell sums, [1]: hole cell sums, [2]: |q| and node sums.
+__global__ void deposit_kernel(DevParticles P, int n, DevMesh M, DepositScales S, long long *cell_e,
+                               long long *cell_h, long long *cell_abs, long long *node_q) {
+  const int px = M.nx + 1, pz = M.nz + 1;
+  const double scale = S.s[2];
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const uint32_t meta = P.meta[p];
+    if (meta & kDeadBit) continue;
+    const uint32_t c = P.cell[p];
+    const int i = c & 1023, j = (c >> 10) & 1023, k = (c >> 20) & 1023;
+    const int cell = (j * M.nx + i) * M.nz + k;
+    const double cc = P.charge[p];
+    if (((meta >> 8) & 255) == 0) fx_add(cell_e + cell, cc, S.s[0]);
+    else fx_add(cell_h + cell, cc, S.s[1]);
+    fx_add(cell_abs + cell, fabs(cc), scale);
+    const double rx = (P.x[p] - M.lx[i]) / M.dx[i];
+    const double ry = (P.y[p] - M.ly[j]) / M.dy[j];
+    const double rz = (P.z[p] - M.lz[k]) / M.dz[k];
+    auto node = [&](int a, int b, int d) { return node_q + ((size_t)b * px + a) * pz + d; };
+    fx_add(node(i, j, k), cc * (1 - ry) * (1 - rx) * (1 - rz), scale);
+    fx_add(node(i + 1, j, k), cc * (1 - ry) * rx * (1 - rz), scale);
+    fx_add(node(i, j, k + 1), cc * (1 - ry) * (1 - rx) * rz, scale);
+    fx_add(node(i + 1, j, k + 1), cc * (1 - ry) * rx * rz, scale);
+    fx_add(node(i, j + 1, k), cc * ry * (1 - rx) * (1 - rz), scale);
+    fx_add(node(i + 1, j + 1, k), cc * ry * rx * (1 - rz), scale);
+    fx_add(node(i, j + 1, k + 1), cc * ry * (1 - rx) * rz, scale);
+    fx_add(node(i + 1, j + 1, k + 1), cc * ry * rx * rz, scale);
+  }
+}
+
+// compute_cell_charge's final loop (:2705-2710) and the per-cell sums.
+__global__ void deposit_cells_kernel(int cells, DepositScales S, const long long *cell_e, const long long *cell_h,
+                                     const long long *cell_abs, const double *cvol, const double *da, double *e_out,
+                                     double *h_out, double *rho_out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cells) return;
+  e_out[c] = (double)cell_e[c] / S.s[0];
+  h_out[c] = (double)cell_h[c] / S.s[1];
+  const double r = (double)cell_abs[c] / S.s[2] / cvol[c];
+  const double half = 0.5 * da[c];
+  rho_out[c] = r > half ? r : half;
+}
+
+// particle_to_density's volume division (:408-416).
+__global__ void deposit_nodes_kernel(int nodes, double scale, const long long *node_q, const double *pvol,
+                                     double *density) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nodes) return;
+  const double q = (double)node_q[p] / scale;
+  density[p] = fabs(pvol[p]) > 0 ? q / pvol[p] : q;
+}
+
+// compute_rhs, src/mcmodel.cpp:2858-2893.
+__global__ void rhs_kernel(int nodes, const double *density, const double *pvol, const double *pdop,
+                           const uint8_t *dirichlet, const double *vapp, const double *vadd, const double *phims,
+                           double *rhs) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nodes) return;
+  if (dirichlet[p]) rhs[p] = vapp[p] + vadd[p] + phims[p];
+  else rhs[p] = fabs(density[p]) > 0 ? density[p] * pvol[p] + pdop[p] : 0.0;
+}
+
+struct Grid3 {
+  int px, py, pz;
+};
+__device__ __forceinline__ void node_ijk(int p, const Grid3 &g, int &i, int &j, int &k) {
+  k = p % g.pz;
+  const int t = p / g.pz;
+  i = t % g.px;
+  j = t / g.px;
+}
+
+// y = A_ff x on free nodes (Dirichlet neighbours excluded); Dirichlet rows: y = 0.
+// With `rhs`, writes b_ff - A x instead, where b_ff folds the Dirichlet values
+// into the free rows (elimination of the contact rows).
+__global__ void stencil_apply(int nodes, Grid3 g, const double *st, const uint8_t *dir, const double *x,
+                              const double *rhs, double *y) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nodes) return;
+  if (dir[p]) {
+    y[p] = 0.0;
+    return;
+  }
+  int i, j, k;
+  node_ijk(p, g, i, j, k);
+  const double *a = st + (size_t)p * 7;
+  double acc = a[6] * x[p];
+  double fold = 0.0;  // contributions of Dirichlet neighbours (known values)
+  const int nb[6] = {i > 0 ? p - g.pz : -1, i + 1 < g.px ? p + g.pz : -1, j > 0 ? p - g.px * g.pz : -1,
+                     j + 1 < g.py ? p + g.px * g.pz : -1, k > 0 ? p - 1 : -1, k + 1 < g.pz ? p + 1 : -1};
+#pragma unroll
+  for (int s = 0; s < 6; ++s) {
+    const int q = nb[s];
+    if (q < 0 || a[s] == 0.0) continue;
+    if (dir[q]) fold += a[s] * x[q];
+    else acc += a[s] * x[q];
+  }
+  y[p] = rhs ? (rhs[p] - fold) - acc : acc;
+}
+
+// Fixed-order block partial sums of a[i]*b[i] (first stage of a dot product).
+template <int B>
+__device__ double block_sum(double v) {
+  __shared__ double s[B];
+  s[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = B / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) s[threadIdx.x] += s[threadIdx.x + o];
+    __syncthreads();
+  }
+  const double r = s[0];
+  __syncthreads();
+  return r;
+}
+
+constexpr int kRedBlock = 256;
+constexpr int kRedGrid = 296;  // 2 x 148 SMs; fixed so the reduction order is fixed
+
+__global__ void __launch_bounds__(kRedBlock) dot_partial(int n, const double *a, const double *b, double *part) {
+  double v = 0.0;
+  for (int i = blockIdx.x * kRedBlock + threadIdx.x; i < n; i += kRedGrid * kRedBlock) v += a[i] * b[i];
+  const double s = block_sum<kRedBlock>(v);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+__global__ void __launch_bounds__(kRedBlock) dot_final(const double *part, double *out) {
+  double v = 0.0;
+  for (int i = threadIdx.x; i < kRedGrid; i += kRedBlock) v += part[i];
+  const double s = block_sum<kRedBlock>(v);
+  if (threadIdx.x == 0) *out = s;
+}
+
+// CG scalars live in device memory: [0] rz, [1] pq, [2] rz_new, [3] rr, [4] alpha, [5] beta
+__global__ void cg_alpha(double *sc) { sc[4] = sc[0] / sc[1]; }
+__global__ void cg_beta(double *sc) {
+  sc[5] = sc[2] / sc[0];
+  sc[0] = sc[2];
+}
+__global__ void cg_update_xr(int n, const double *sc, const double *p, const double *q, double *x, double *r,
+                             const double *diag_inv, double *z, const uint8_t *dir) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || dir[i]) return;
+  const double alpha = sc[4];
+  x[i] += alpha * p[i];
+  r[i] -= alpha * q[i];
+  z[i] = r[i] * diag_inv[i];
+}
+__global__ void cg_update_p(int n, const double *sc, const double *z, double *p, const uint8_t *dir) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || dir[i]) return;
+  p[i] = z[i] + sc[5] * p[i];
+}
+__global__ void cg_init(int n, const double *r, const double *diag_inv, double *z, double *p, const uint8_t *dir,
+                        const double *rhs, double *x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (dir[i]) {
+    x[i] = rhs[i];
+    z[i] = 0.0;
+    p[i] = 0.0;
+    return;
+  }
+  z[i] = r[i] * diag_inv[i];
+  p[i] = z[i];
+}
+// Free-row right-hand side with the Dirichlet values folded in (for ||b||).
+__global__ void folded_rhs(int nodes, Grid3 g, const double *st, const uint8_t *dir, const double *rhs, double *b) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nodes) return;
+  if (dir[p]) {
+    b[p] = 0.0;
+    return;
+  }
+  int i, j, k;
+  node_ijk(p, g, i, j, k);
+  const double *a = st + (size_t)p * 7;
+  double fold = 0.0;
+  const int nb[6] = {i > 0 ? p - g.pz : -1, i + 1 < g.px ? p + g.pz : -1, j > 0 ? p - g.px * g.pz : -1,
+                     j + 1 < g.py ? p + g.px * g.pz : -1, k > 0 ? p - 1 : -1, k + 1 < g.pz ? p + 1 : -1};
+  for (int s = 0; s < 6; ++s)
+    if (nb[s] >= 0 && a[s] != 0.0 && dir[nb[s]]) fold += a[s] * rhs[nb[s]];
+  b[p] = rhs[p] - fold;
+}
+__global__ void set_dirichlet(int nodes, const uint8_t *dir, const double *rhs, double *x) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < nodes && dir[p]) x[p] = rhs[p];
+}
+
+// pot2field / pot2field_for_hole, src/mcmodel.cpp:2732-2855 (no quantum
+// correction): the same field for both carriers, stored as felt.
+__global__ void pot2field_kernel(DevMesh M, const double *pot, double *efield, double *hfield) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int cells = M.nx * M.ny * M.nz;
+  if (c >= cells) return;
+  const int k = c % M.nz, t = c / M.nz, i = t % M.nx, j = t / M.nx;
+  const int px = M.nx + 1, pz = M.nz + 1;
+  auto P = [&](int a, int b, int d) { return pot[((size_t)b * px + a) * pz + d]; };
+  const double fx = -(P(i + 1, j, k) - P(i, j, k) + P(i + 1, j + 1, k) - P(i, j + 1, k) + P(i + 1, j, k + 1) -
+                      P(i, j, k + 1) + P(i + 1, j + 1, k + 1) - P(i, j + 1, k + 1)) / (4.0 * M.dx[i]);
+  const double fy = -(P(i, j + 1, k) + P(i + 1, j + 1, k) + P(i, j + 1, k + 1) + P(i + 1, j + 1, k + 1) -
+                      P(i, j, k) - P(i + 1, j, k) - P(i, j, k + 1) - P(i + 1, j, k + 1)) / (4.0 * M.dy[j]);
+  const double fz = -(P(i, j, k + 1) + P(i + 1, j, k + 1) + P(i, j + 1, k + 1) + P(i + 1, j + 1, k + 1) -
+                      P(i, j, k) - P(i + 1, j, k) - P(i, j + 1, k) - P(i + 1, j + 1, k)) / (4.0 * M.dz[k]);
+  // ChargeSign = {-1, +1} (src/Constant_GlobalVariable_MathFunction.cpp:18)
+  efield[3 * (size_t)c + 0] = -1.0 * fx;
+  efield[3 * (size_t)c + 1] = -1.0 * fy;
+  efield[3 * (size_t)c + 2] = -1.0 * fz;
+  hfield[3 * (size_t)c + 0] = fx;
+  hfield[3 * (size_t)c + 1] = fy;
+  hfield[3 * (size_t)c + 2] = fz;
+}
+
+// ---------------------------------------------------------------------------
+static inline int blocks(long long n, int b) { return (int)((n + b - 1) / b); }
+
+void launch_charge_bounds(const DevParticles &P, int n, unsigned long long *out, int grid, cudaStream_t s) {
+  cudaMemsetAsync(out, 0, 4 * sizeof(unsigned long long), s);
+  if (n > 0) charge_bounds_kernel<<<grid, 256, 0, s>>>(P.charge, P.meta, n, out);
+}
+
+void launch_deposit(const DevParticles &P, int n, const DevMesh &M, const FieldBuffers &f, const DepositScales &S,
+                    int grid, cudaStream_t s) {
+  const int cells = M.nx * M.ny * M.nz, nodes = (M.nx + 1) * (M.ny + 1) * (M.nz + 1);
+  cudaMemsetAsync(f.acc_cell, 0, sizeof(long long) * 3 * (size_t)cells, s);
+  cudaMemsetAsync(f.acc_node, 0, sizeof(long long) * (size_t)nodes, s);
+  if (n > 0)
+    deposit_kernel<<<grid, 256, 0, s>>>(P, n, M, S, f.acc_cell, f.acc_cell + cells, f.acc_cell + 2 * (size_t)cells,
+                                         f.acc_node);
+  deposit_cells_kernel<<<blocks(cells, 256), 256, 0, s>>>(cells, S, f.acc_cell, f.acc_cell + cells,
+                                                           f.acc_cell + 2 * (size_t)cells, f.cvol, M.da, f.cell_e,
+                                                           f.cell_h, const_cast<double *>(M.rho));
+  deposit_nodes_kernel<<<blocks(nodes, 256), 256, 0, s>>>(nodes, S.s[2], f.acc_node, f.pvol, f.density);
+}
+
+void launch_rhs(int nodes, const FieldBuffers &f, cudaStream_t s) {
+  rhs_kernel<<<blocks(nodes, 256), 256, 0, s>>>(nodes, f.density, f.pvol, f.pdop, f.dirichlet, f.bc_vapp, f.vadd,
+                                                 f.bc_phims, f.rhs);
+}
+
+static void dot(int n, const double *a, const double *b, double *part, double *out, cudaStream_t s) {
+  dot_partial<<<kRedGrid, kRedBlock, 0, s>>>(n, a, b, part);
+  dot_final<<<1, kRedBlock, 0, s>>>(part, out);
+}
+
+int cg_solve(const DevMesh &M, const FieldBuffers &f, double rel_tol, int max_iter, cudaStream_t s,
+             double *host_scratch, int *iterations, double *rel_residual) {
+  const int nodes = (M.nx + 1) * (M.ny + 1) * (M.nz + 1);
+  const Grid3 g{M.nx + 1, M.ny + 1, M.nz + 1};
+  const int nb = blocks(nodes, 256);
+  double *sc = f.cg_scalars;
+  // ||b_free|| with the Dirichlet values folded in
+  set_dirichlet<<<nb, 256, 0, s>>>(nodes, f.dirichlet, f.rhs, f.potential);
+  folded_rhs<<<nb, 256, 0, s>>>(nodes, g, f.stencil, f.dirichlet, f.rhs, f.cg_q);
+  dot(nodes, f.cg_q, f.cg_q, f.cg_part, sc + 6, s);
+  // r = b - A x (x: the previous potential, a warm start)
+  stencil_apply<<<nb, 256, 0, s>>>(nodes, g, f.stencil, f.dirichlet, f.potential, f.rhs, f.cg_r);
+  cg_init<<<nb, 256, 0, s>>>(nodes, f.cg_r, f.diag_inv, f.cg_z, f.cg_p, f.dirichlet, f.rhs, f.potential);
+  dot(nodes, f.cg_r, f.cg_z, f.cg_part, sc + 0, s);
+  dot(nodes, f.cg_r, f.cg_r, f.cg_part, sc + 3, s);
+  cudaMemcpyAsync(host_scratch, sc, 8 * sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return 1;
+  const double bnorm = sqrt(host_scratch[6]) > 0 ? sqrt(host_scratch[6]) : 1.0;
+  double res = sqrt(host_scratch[3]) / bnorm;
+  int it = 0;
+  const int check = 8;
+  while (res > rel_tol && it < max_iter) {
+    for (int q = 0; q < check && it < max_iter; ++q, ++it) {
+      stencil_apply<<<nb, 256, 0, s>>>(nodes, g, f.stencil, f.dirichlet, f.cg_p, nullptr, f.cg_q);
+      dot(nodes, f.cg_p, f.cg_q, f.cg_part, sc + 1, s);
+      cg_alpha<<<1, 1, 0, s>>>(sc);
+      cg_update_xr<<<nb, 256, 0, s>>>(nodes, sc, f.cg_p, f.cg_q, f.potential, f.cg_r, f.diag_inv, f.cg_z,
+                                      f.dirichlet);
+      dot(nodes, f.cg_r, f.cg_z, f.cg_part, sc + 2, s);
+      cg_beta<<<1, 1, 0, s>>>(sc);
+      cg_update_p<<<nb, 256, 0, s>>>(nodes, sc, f.cg_z, f.cg_p, f.dirichlet);
+    }
+    dot(nodes, f.cg_r, f.cg_r, f.cg_part, sc + 3, s);
+    cudaMemcpyAsync(host_scratch, sc, 8 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return 1;
+    res = sqrt(host_scratch[3]) / bnorm;
+  }
+  // true residual of the final iterate
+  stencil_apply<<<nb, 256, 0, s>>>(nodes, g, f.stencil, f.dirichlet, f.potential, f.rhs, f.cg_r);
+  dot(nodes, f.cg_r, f.cg_r, f.cg_part, sc + 3, s);
+  cudaMemcpyAsync(host_scratch, sc, 8 * sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return 1;
+  if (iterations) *iterations = it;
+  if (rel_residual) *rel_residual = sqrt(host_scratch[3]) / bnorm;
+  return 0;
+}
+
+void launch_pot2field(const DevMesh &M, const double *pot, cudaStream_t s) {
+  const int cells = M.nx * M.ny * M.nz;
+  pot2field_kernel<<<blocks(cells, 256), 256, 0, s>>>(M, pot, const_cast<double *>(M.efield),
+                                                        const_cast<double *>(M.hfield));
+}
+
+}  // namespace mcb200

@@ -1,0 +1,45 @@
+// field_kernels.h -- device buffers and launchers of deposition, the Poisson
+// solve and the field update (field_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "device_state.cuh"
+
+namespace mcb200 {
+
+struct FieldBuffers {
+  // device description (poisson_setup.h), uploaded once
+  double *cvol = nullptr, *pvol = nullptr, *pdop = nullptr, *vadd = nullptr;
+  double *stencil = nullptr, *diag_inv = nullptr;
+  uint8_t *dirichlet = nullptr;
+  double *bc_vapp = nullptr, *bc_phims = nullptr;
+  // deposition results
+  long long *acc_cell = nullptr;  // [3][cells] fixed-point sums: electron q, hole q, |q|
+  long long *acc_node = nullptr;  // [nodes]
+  double *cell_e = nullptr, *cell_h = nullptr;  // c_electron_charge, c_hole_charge
+  double *density = nullptr;                    // p_par_charge (charge / node volume)
+  // Poisson
+  double *rhs = nullptr, *potential = nullptr;
+  double *cg_r = nullptr, *cg_z = nullptr, *cg_p = nullptr, *cg_q = nullptr, *cg_part = nullptr,
+         *cg_scalars = nullptr;
+  unsigned long long *abs_sum = nullptr;
+};
+
+// Fixed-point units (powers of two) of the deposition sums: electron cell
+// charge, hole cell charge, |charge| and node charge.
+struct DepositScales {
+  double s[3];
+};
+
+// out[4] = {max |q| bits of electrons, of holes, electron count, hole count}
+void launch_charge_bounds(const DevParticles &P, int n, unsigned long long *out, int grid, cudaStream_t s);
+void launch_deposit(const DevParticles &P, int n, const DevMesh &M, const FieldBuffers &f, const DepositScales &S,
+                    int grid, cudaStream_t s);
+void launch_rhs(int nodes, const FieldBuffers &f, cudaStream_t s);
+// Returns 0 on success; host_scratch must hold 8 doubles (pinned).
+int cg_solve(const DevMesh &M, const FieldBuffers &f, double rel_tol, int max_iter, cudaStream_t s,
+             double *host_scratch, int *iterations, double *rel_residual);
+void launch_pot2field(const DevMesh &M, const double *pot, cudaStream_t s);
+
+}  // namespace mcb200

@@ -28,7 +28,7 @@ __device__ void load_sym(SymSmem &S, const DevTables &T) {
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(256) flight_kernel(FlightCtx F, DevParticles P, int n) {
+__global__ void __launch_bounds__(256, 2) flight_kernel(FlightCtx F, DevParticles P, int n) {
   __shared__ SymSmem S;
   load_sym(S, F.T);
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(256) flight_kernel(FlightCtx F, DevParticles P
 
 // Copies made during the previous pass (buffer `in`) fly the rest of their
 // step; copies they make go to `F.C`.
-__global__ void __launch_bounds__(256) child_flight_kernel(FlightCtx F, DevChildren in) {
+__global__ void __launch_bounds__(256, 2) child_flight_kernel(FlightCtx F, DevChildren in) {
   __shared__ SymSmem S;
   load_sym(S, F.T);
   const int n = min((int)*in.count, in.capacity);

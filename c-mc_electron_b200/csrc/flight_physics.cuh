@@ -17,11 +17,12 @@
 //    TOO_MANY_LOOPS (src/mcmodel.cpp:2156);
 //  * surface-phonon mechanism choice uses drand = Random() * sum(rates): the
 //    reference reads an uninitialised local there (src/ParSurfaceScatter.cpp:94,149);
-//  * the wedge / tetrahedron search after an impurity event (Getisym,
-//    src/ParticleUtils.cpp:395-625) looks the point up in a uniform k-grid
-//    instead of the reference's lists; both return the tetrahedron of the
-//    band that contains k (they could differ only for a k within 1e-13 of a
-//    face shared by two tetrahedra).
+//  * the tetrahedron search after an impurity event (Getisym,
+//    src/ParticleUtils.cpp:395-625) walks the mesh from the current
+//    tetrahedron through face neighbours, falling back to a uniform k-grid
+//    lookup, instead of scanning the reference's lists; both return the
+//    tetrahedron of the band that contains k (they could differ only for a
+//    k within 1e-13 of a face shared by two tetrahedra).
 #pragma once
 
 #include "device_state.cuh"
@@ -179,17 +180,45 @@ struct Flyer {
     }
   }
 
+  // Point location by walking the tetrahedral mesh: from `start`, repeatedly
+  // step through the face whose plane the point lies furthest outside of,
+  // until every face test passes (the reference's containment test,
+  // d >= -MY_ZERO).  Returns -1 when the walk reaches a wedge boundary or
+  // does not settle within the step cap; the caller then uses the k-grid.
+  __device__ int walk_to(int start, double a, double b, double c) const {
+    int it = start;
+    for (int s = 0; s < 64; ++s) {
+      int fmin = -1;
+      double dmin = -kMyZero;
+#pragma unroll
+      for (int f = 0; f < 4; ++f) {
+        const double d = face_dist(it, f, a, b, c);
+        if (d < dmin) {
+          dmin = d;
+          fmin = f;
+        }
+      }
+      if (fmin < 0) return it;
+      const int nb = (&F.T.tneib[it].x)[fmin];
+      if (nb < 0) return -1;
+      it = nb;
+    }
+    return -1;
+  }
+
   // Getisym, src/ParticleUtils.cpp:395-625: wedge from k, then the tet of
   // band iband that contains the wedge vector (k-grid lookup, see file note).
   __device__ void Getisym() {
-    int pos[3] = {1, 1, 1}, mink, maxk;
+    int mink, maxk;
     double tmin, tmax;
     if (fabs(kx) > fabs(ky)) { tmin = fabs(ky); tmax = fabs(kx); mink = 1; maxk = 0; }
     else { tmin = fabs(kx); tmax = fabs(ky); mink = 0; maxk = 1; }
     if (fabs(kz) < tmin) mink = 2;
     else if (fabs(kz) > tmax) maxk = 2;
-    pos[mink] = 2;
-    pos[maxk] = 0;
+    // pos[mink] = 2, pos[maxk] = 0, else 1 (mink != maxk always)
+    const int p0 = maxk == 0 ? 0 : (mink == 0 ? 2 : 1);
+    const int p1 = maxk == 1 ? 0 : (mink == 1 ? 2 : 1);
+    const int p2 = maxk == 2 ? 0 : (mink == 2 ? 2 : 1);
     auto sgn = [](double v) { return (int)(fabs(v) / v); };  // utils.cpp sign()
     const int sx = sgn(kx) + 1, sy = sgn(ky) + 1, sz = sgn(kz) + 1;
     if (sx < 0 || sx > 2 || sy < 0 || sy > 2 || sz < 0 || sz > 2) {  // a zero component: sign() is NaN in the reference
@@ -197,10 +226,26 @@ struct Flyer {
       catch_ = true;
       return;
     }
-    isym = F.T.indmat[((((sx * 3 + sy) * 3 + sz) * 3 + pos[0]) * 3 + pos[1]) * 3 + pos[2]];
+    isym = F.T.indmat[((((sx * 3 + sy) * 3 + sz) * 3 + p0) * 3 + p1) * 3 + p2];
     double a, b, c;
     in_wedge(a, b, c, kx, ky, kz);
     if (iband == F.T.ibt[itet] && tet_contains(itet, a, b, c)) return;
+    int start = iband == F.T.ibt[itet] ? itet : -1;
+    if (iband == F.T.bandof[0]) {  // lowest conduction band: start next to the point
+      const int sg = kSeedGridN;
+      const int si = min(max((int)floor((a - F.T.grid_lo[0]) * F.T.seed_inv[0]), 0), sg - 1);
+      const int sj = min(max((int)floor((b - F.T.grid_lo[1]) * F.T.seed_inv[1]), 0), sg - 1);
+      const int sk = min(max((int)floor((c - F.T.grid_lo[2]) * F.T.seed_inv[2]), 0), sg - 1);
+      const int s0 = F.T.seed_grid[((size_t)si * sg + sj) * sg + sk];
+      if (s0 >= 0) start = s0;
+    }
+    if (start >= 0) {
+      const int w = walk_to(start, a, b, c);
+      if (w >= 0) {
+        itet = w;
+        return;
+      }
+    }
     const int g = F.T.grid_n;
     int gi = (int)floor((a - F.T.grid_lo[0]) * F.T.grid_inv[0]);
     int gj = (int)floor((b - F.T.grid_lo[1]) * F.T.grid_inv[1]);
@@ -260,7 +305,12 @@ struct Flyer {
     }
   }
 
-  // TALIND, src/ParticleUtils.cpp:626-748: final valley (and a random wedge in it).
+  // TALIND, src/ParticleUtils.cpp:626-748: final valley (and a random wedge
+  // in it).  The reference's talend[] lookups are written as arithmetic on
+  // the drawn index (1..4); an index of 5 (u*4+1 rounding up to 5, possible
+  // only for u within 2^-51 of 1) reads past the reference's table and is
+  // clamped to 4 here.
+  __device__ __forceinline__ int talend_index() { return min((int)(Random() * 4.0 + 1.0), 4); }
   __device__ void TALIND(int ityp) {
     int ital = 1;
     const double ax = fabs(kx), ay = fabs(ky), az = fabs(kz);
@@ -268,36 +318,36 @@ struct Flyer {
       if (kx >= 0.0) {
         if (ityp == 1) ital = 1;
         if (ityp == 2) ital = 2;
-        if (ityp == 3) { const int tb[5] = {0, 3, 4, 5, 6}; ital = tb[(int)(Random() * 4.0 + 1.0)]; }
+        if (ityp == 3) ital = talend_index() + 2;  // {3,4,5,6}
       }
       if (kx < 0.0) {
         if (ityp == 1) ital = 2;
         if (ityp == 2) ital = 1;
-        if (ityp == 3) { const int tb[5] = {0, 3, 4, 5, 6}; ital = tb[(int)(Random() * 4.0 + 1.0)]; }
+        if (ityp == 3) ital = talend_index() + 2;
       }
     }
     if (ay >= az && ay >= ax) {
       if (ky >= 0.0) {
         if (ityp == 1) ital = 3;
         if (ityp == 2) ital = 4;
-        if (ityp == 3) { const int tb[5] = {0, 1, 2, 5, 6}; ital = tb[(int)(Random() * 4.0 + 1.0)]; }
+        if (ityp == 3) { const int i = talend_index(); ital = i <= 2 ? i : i + 2; }  // {1,2,5,6}
       }
       if (ky < 0.0) {
         if (ityp == 1) ital = 4;
         if (ityp == 2) ital = 3;
-        if (ityp == 3) { const int tb[5] = {0, 1, 2, 5, 6}; ital = tb[(int)(Random() * 4.0 + 1.0)]; }
+        if (ityp == 3) { const int i = talend_index(); ital = i <= 2 ? i : i + 2; }
       }
     }
     if (az > ay && az > ax) {
       if (kz >= 0.0) {
         if (ityp == 1) ital = 5;
         if (ityp == 2) ital = 6;
-        if (ityp == 3) { const int tb[5] = {0, 1, 2, 3, 4}; ital = tb[(int)(Random() * 4.0 + 1.0)]; }
+        if (ityp == 3) ital = talend_index();  // {1,2,3,4}
       }
       if (kz < 0.0) {
         if (ityp == 1) ital = 6;
         if (ityp == 2) ital = 5;
-        if (ityp == 3) { const int tb[5] = {0, 1, 2, 3, 4}; ital = tb[(int)(Random() * 4.0 + 1.0)]; }
+        if (ityp == 3) ital = talend_index();
       }
     }
     isym = (int)(Random() * 8.0) + 8 * (ital - 1);

@@ -693,6 +693,26 @@ FullBandTables FullBandTables::build(const std::string &dir, double kelvin) {
         }
     }
   }
+  // GETINDENS, src/Band.cpp:3609-3656: intrinsic density from the DOS tables.
+  {
+    double en0 = 0.0, ep0 = 0.0, eelmo = t.energy[0];
+    for (int i = 1; i <= kMaxTab; ++i) {
+      const double eel = t.energy[i];
+      double dosl = t.caldossum(eel, 0), doslmo = t.caldossum(eelmo, 0);
+      en0 = en0 + ((doslmo * eel - dosl * eelmo) * (std::exp(-eelmo) - std::exp(-eel)) +
+                   (dosl - doslmo) * ((eelmo + 1e0) * std::exp(-eelmo) - (eel + 1e0) * std::exp(-eel))) /
+                      (eel - eelmo);
+      dosl = t.caldossum(eel, 1);
+      doslmo = t.caldossum(eelmo, 1);
+      ep0 = ep0 + ((doslmo * eel - dosl * eelmo) * (std::exp(-eelmo) - std::exp(-eel)) +
+                   (dosl - doslmo) * ((eelmo + 1e0) * std::exp(-eelmo) - (eel + 1e0) * std::exp(-eel))) /
+                      (eel - eelmo);
+      eelmo = eel;
+    }
+    en0 = 2e0 * en0;
+    ep0 = 2e0 * ep0;
+    t.ni = std::sqrt(en0 * ep0 * std::exp(-u.sieg));
+  }
   // gamtet: majorant of the total rate over the tet's energy span, :1890-1906
   t.gamtet.assign(nt, 0.0);
   for (int it = 0; it < nt; ++it) {

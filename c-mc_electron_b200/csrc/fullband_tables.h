@@ -91,6 +91,7 @@ struct FullBandTables {
   double temptag, templag, templog, temptaf, templaf, temptof, temphop;
   double difpr[3];
   double mell, melt, meld;
+  double ni = 0;         // intrinsic carrier density (GETINDENS), normalised
   bool seciifl = false;  // secondary particles from impact ionisation (off in the reference)
 
   // Build everything from a directory holding bs.si.asc and zd.si.asc.

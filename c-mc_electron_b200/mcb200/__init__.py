@@ -61,7 +61,11 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mcb200_last_error.restype = c.c_char_p
     lib.mcb200_units.argtypes = [vp, dp, c.c_int]
     lib.mcb200_copy_table.argtypes = [vp, c.c_char_p, vp, c.c_size_t, c.POINTER(c.c_size_t)]
-    lib.mcb200_set_mesh.argtypes = [vp, c.c_int, c.c_int, c.c_int, dp, dp, dp]
+    lib.mcb200_set_mesh.argtypes = [vp, c.c_int, c.c_int, c.c_int, dp, dp, dp, dp, dp, dp]
+    lib.mcb200_set_device.argtypes = [vp, i32p, dp, dp, c.c_int, dp, dp, c.c_int, i32p]
+    lib.mcb200_deposit.argtypes = [vp]
+    lib.mcb200_solve_poisson.argtypes = [vp, c.c_double, c.c_int, c.POINTER(c.c_int), dp]
+    lib.mcb200_get_array.argtypes = [vp, c.c_char_p, dp, c.c_size_t]
     lib.mcb200_set_cells.argtypes = [vp, i32p, i32p, i32p, i32p, i32p, c.c_int, dp, c.c_int]
     lib.mcb200_set_fields.argtypes = [vp, dp, dp, dp]
     lib.mcb200_set_surface_rates.argtypes = [vp, dp, dp, dp, dp]
@@ -157,12 +161,44 @@ class Engine:
                                                 out.nbytes, ctypes.byref(need)), name)
         return out
 
-    def set_mesh(self, lx, ly, lz):
+    def set_mesh(self, lx, ly, lz, dx=None, dy=None, dz=None):
         lx, ly, lz = (np.ascontiguousarray(a, dtype=np.float64) for a in (lx, ly, lz))
+        w = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (dx, dy, dz)]
         m = Mesh(len(lx) - 1, len(ly) - 1, len(lz) - 1, lx, ly, lz)
         self._check(self._lib.mcb200_set_mesh(self._ctx, m.nx, m.ny, m.nz, _ptr(lx, ctypes.c_double),
-                                              _ptr(ly, ctypes.c_double), _ptr(lz, ctypes.c_double)), "set_mesh")
+                                              _ptr(ly, ctypes.c_double), _ptr(lz, ctypes.c_double),
+                                              *[_ptr(a, ctypes.c_double) for a in w]), "set_mesh")
         self.mesh = m
+
+    def set_device(self, material, donor, acceptor, vapp=(), phims=(), planes=()):
+        """Deposition / Poisson description (mcb200_set_device); planes: rows of
+        (contact, i0, i1, j0, j1, k0, k1) node ranges."""
+        mat = np.ascontiguousarray(material, dtype=np.int32)
+        don, acc = (np.ascontiguousarray(a, dtype=np.float64) for a in (donor, acceptor))
+        va, ph = (np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in (vapp, phims))
+        pl = np.ascontiguousarray(planes, dtype=np.int32).reshape(-1)
+        self._check(self._lib.mcb200_set_device(self._ctx, _ptr(mat, ctypes.c_int32), _ptr(don, ctypes.c_double),
+                                                _ptr(acc, ctypes.c_double), len(va), _ptr(va, ctypes.c_double),
+                                                _ptr(ph, ctypes.c_double), len(pl) // 7, _ptr(pl, ctypes.c_int32)),
+                    "set_device")
+
+    def deposit(self):
+        self._check(self._lib.mcb200_deposit(self._ctx), "deposit")
+
+    def solve_poisson(self, rel_tol=1e-10, max_iter=20000):
+        it, res = ctypes.c_int(), ctypes.c_double()
+        self._check(self._lib.mcb200_solve_poisson(self._ctx, rel_tol, max_iter, ctypes.byref(it),
+                                                   ctypes.byref(res)), "solve_poisson")
+        return it.value, res.value
+
+    def array(self, name: str) -> np.ndarray:
+        m = self.mesh
+        per = {"rho": m.ncells, "efield": 3 * m.ncells, "hfield": 3 * m.ncells, "cell_charge_e": m.ncells,
+               "cell_charge_h": m.ncells, "cell_volume": m.ncells, "stencil": 7 * m.nnodes}
+        out = np.zeros(per.get(name, m.nnodes))
+        self._check(self._lib.mcb200_get_array(self._ctx, name.encode(), _ptr(out, ctypes.c_double), out.size),
+                    name)
+        return out
 
     def set_cells(self, motion_rule, da, attached_contact=None, in_surf_region=None, nearest_surf=None,
                   surface_dir=None, flags: int = 0):

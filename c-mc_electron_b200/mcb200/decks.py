@@ -34,6 +34,41 @@ def write_input(path: str, **kv):
             f.write(f"{k}={v}\n")
 
 
+def contact_bar(dirpath: str, nx=8, ny=10, nz=6, cell_nm=5.0, donor_m3=1e24, vd=0.3, electrons=4000, holes=0,
+                dt=1e-15, kelvin=300.0) -> dict:
+    """n-Si bar with a grounded contact on the y = 0 node plane and a contact
+    at `vd` volts on the far y plane (REFLECT on every face): the smallest
+    device with Dirichlet rows in its Poisson problem."""
+    os.makedirs(dirpath, exist_ok=True)
+    X, Y, Z = nx * cell_nm, ny * cell_nm, nz * cell_nm
+    write_grid(os.path.join(dirpath, "lgrid.txt"), np.arange(nx + 1) * cell_nm, np.arange(ny + 1) * cell_nm,
+               np.arange(nz + 1) * cell_nm)
+    g = lambda v: f"{v:g}"
+    box = f"0 {g(X)} 0 {g(Y)} 0 {g(Z)}"
+    lines = [
+        "default_par_number 1 0",
+        f"region {box} SILICON",
+        f"donor {box} {donor_m3:g}",
+        f"acceptor {box} 0",
+        f"motioncube {box} PASS PASS PASS PASS PASS PASS",
+        f"motionplane 0 0 0 {g(Y)} 0 {g(Z)} UP REFLECT",
+        f"motionplane {g(X)} {g(X)} 0 {g(Y)} 0 {g(Z)} DOWN REFLECT",
+        f"motionplane 0 {g(X)} 0 0 0 {g(Z)} LEFT REFLECT",
+        f"motionplane 0 {g(X)} {g(Y)} {g(Y)} 0 {g(Z)} RIGHT REFLECT",
+        f"motionplane 0 {g(X)} 0 {g(Y)} 0 0 FRONT REFLECT",
+        f"motionplane 0 {g(X)} 0 {g(Y)} {g(Z)} {g(Z)} BACK REFLECT",
+        "contact", "1 0", f"0 {g(X)} 0 0 0 {g(Z)}", "0",
+        "contact", "1 0", f"0 {g(X)} {g(Y)} {g(Y)} 0 {g(Z)}", f"{vd:g}",
+        "end",
+    ]
+    with open(os.path.join(dirpath, "ldg.txt"), "w") as f:
+        f.write("\n".join(lines) + "\n")
+    write_input(os.path.join(dirpath, "input.txt"), dt=dt, Temperature=kelvin, Flag_SurfaceScatter=0,
+                ElectronNumber=electrons, HoleNumber=holes)
+    return dict(input=os.path.join(dirpath, "input.txt"), grid=os.path.join(dirpath, "lgrid.txt"),
+                device=os.path.join(dirpath, "ldg.txt"))
+
+
 def bulk_box(dirpath: str, nx=40, ny=20, nz=20, cell_nm=5.0, donor_m3=1e23, electrons=20000, holes=0,
              min_electrons=1, min_holes=0, dt=1e-15, kelvin=300.0) -> dict:
     """n-Si box of nx*ny*nz cubic cells, uniform donors, REFLECT on all six faces

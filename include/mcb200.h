@@ -94,10 +94,44 @@ int mcb200_units(const mcb200_ctx *ctx, double *out, int n);
  * "dose", "scattiie", "scatth", "dosh", "scattiih", "energy". */
 int mcb200_copy_table(const mcb200_ctx *ctx, const char *name, void *out, size_t bytes, size_t *needed);
 
-/* Mesh node coordinates in normalised length (lx: nx+1 values, ...);
- * replaces the lx/ly/lz/dx/dy/dz globals (include/utils.h:81-83). */
+/* Mesh node coordinates in normalised length (lx: nx+1 values, ...) and,
+ * optionally, the cell widths dx/dy/dz (nx, ny, nz values; NULL: taken as
+ * node differences).  The reference scales its widths separately from its
+ * node coordinates, so passing its own dx/dy/dz keeps the deposition and
+ * Poisson weights bit-identical.  Replaces the lx/ly/lz/dx/dy/dz globals
+ * (include/utils.h:81-83).  Resets cells, fields and the device description. */
 int mcb200_set_mesh(mcb200_ctx *ctx, int nx, int ny, int nz, const double *lx, const double *ly,
-                    const double *lz);
+                    const double *lz, const double *dx, const double *dy, const double *dz);
+
+/* Device description for deposition and the Poisson solve: per cell the
+ * material (0 void, 1 vacuum, 2 oxide, 3 silicon) and donor / acceptor
+ * concentrations (normalised by conc0); contacts: per contact the applied
+ * potential Vapp and the work-function difference PhiMS (normalised by
+ * pot0), and n_planes planes of 7 ints {contact (0-based), i0, i1, j0, j1,
+ * k0, k1} (inclusive node ranges) whose nodes are Dirichlet rows.  Builds
+ * node volumes, doping and built-in potential (init_cell_data /
+ * init_point_data, src/mcmodel.cpp:3187-3390) and the FV stencil
+ * (init_matrix, :4695-4869). */
+int mcb200_set_device(mcb200_ctx *ctx, const int32_t *material, const double *donor, const double *acceptor,
+                      int n_contacts, const double *vapp, const double *phims, int n_planes, const int32_t *planes);
+
+/* Charge deposition from the particle store: per-cell carrier charge and
+ * the screening density Rho the flight uses (compute_cell_charge,
+ * src/mcmodel.cpp:2664-2712) and the node charge density of the Poisson
+ * right-hand side (particle_to_density, :348-417); int64 fixed point. */
+int mcb200_deposit(mcb200_ctx *ctx);
+
+/* Poisson solve from the last deposit (compute_rhs + linear_poisson_solver,
+ * src/mcmodel.cpp:2714-2893): Jacobi-preconditioned CG in FP64, warm-started
+ * from the previous potential, to ||b - Ax|| / ||b|| <= rel_tol; then the
+ * cell fields of both carriers (pot2field, :2732-2855). */
+int mcb200_solve_poisson(mcb200_ctx *ctx, double rel_tol, int max_iter, int *iterations, double *rel_residual);
+
+/* Copy a device array to the host: "rho", "efield", "hfield" (3 per cell),
+ * "cell_charge_e", "cell_charge_h", "cell_volume" (per cell);
+ * "node_density", "node_volume", "node_doping", "vadd", "rhs", "potential"
+ * (per node); "stencil" (7 per node). */
+int mcb200_get_array(mcb200_ctx *ctx, const char *name, double *out, size_t n);
 
 #define MCB200_FLAG_SURFACE_SCATTER 1   /* Flag_SurfaceScatter */
 #define MCB200_FLAG_SURFACE_IMPURITY 2  /* Flag_SurfaceImpurityScatter */

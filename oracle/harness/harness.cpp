@@ -39,6 +39,7 @@
 #include <iomanip>
 #include <iostream>
 #include <list>
+#include <memory>
 #include <set>
 #include <sstream>
 #include <string>
@@ -49,6 +50,7 @@
 #include "mcb200_rng.h"
 #define class struct
 #include "mcmodel.h"
+#include "PoissonSolver.h"
 #undef class
 
 /* ------------------------------------------------------- random hook -- */
@@ -347,6 +349,68 @@ int orc_set_particles(int n, const double *d, const int *iv) {
   }
   g_next_uid = maxuid;
   return 0;
+}
+
+/* The field half of density() (src/mcmodel.cpp:424-471): node charge
+ * density from the particles (particle_to_density), the Poisson solve and
+ * both carriers' fields (compute_field), then the cell charge
+ * (compute_cell_charge). */
+int orc_density_and_field() {
+  MeshQuantities *mq = g_mq;
+  mq->p_par_charge->PutScalar(0);
+  mq->particle_to_density(mq->p_par_charge, 2);
+  mq->compute_field();
+  mq->compute_cell_charge();
+  return 0;
+}
+
+/* Contacts as parsed from the deck (after scaling): per contact
+ * {nplanes, Vapp, PhiMS}, planes as {contact, i0, i1, j0, j1, k0, k1}. */
+int orc_contact_info(double *per_contact, int *planes, int max_planes) {
+  int np = 0;
+  for (size_t c = 0; c < g_mq->contact.size(); ++c) {
+    const Contact &ct = g_mq->contact[c];
+    per_contact[3 * c + 0] = ct.NumContactPlane;
+    per_contact[3 * c + 1] = ct.CurrentVapp;
+    per_contact[3 * c + 2] = ct.PhiMS;
+    for (int p = 0; p < ct.NumContactPlane && np < max_planes; ++p, ++np) {
+      int *r = planes + 7 * np;
+      r[0] = (int)c;
+      r[1] = ct.BeginI[p]; r[2] = ct.EndI[p];
+      r[3] = ct.BeginJ[p]; r[4] = ct.EndJ[p];
+      r[5] = ct.BeginK[p]; r[6] = ct.EndK[p];
+    }
+  }
+  return np;
+}
+
+/* The reference's Poisson matrix (init_matrix, src/mcmodel.cpp:4695-4869) as
+ * dense 7-slot rows in the engine's stencil order (-x, +x, -y, +y, -z, +z,
+ * diagonal), node index (j*(nx+1)+i)*(nz+1)+k. */
+int orc_poisson_stencil(double *out) {
+  /* the solver keeps its copy protected; init_matrix builds the same one again */
+  std::unique_ptr<Epetra_CrsMatrix> own(g_mq->init_matrix());
+  const Epetra_CrsMatrix *A = own.get();
+  const Epetra_Map &m = A->RowMap();
+  for (int r = 0; r < A->NumMyRows(); ++r) {
+    const int g = m.GID(r);
+    const int j = g / p_numxz, rem = g % p_numxz, i = rem / p_numz, k = rem % p_numz;
+    double *row = out + 7 * (size_t)g;
+    for (int s = 0; s < 7; ++s) row[s] = 0;
+    for (const auto &e : A->Row(r)) {
+      const int q = e.first;
+      const int qj = q / p_numxz, qrem = q % p_numxz, qi = qrem / p_numz, qk = qrem % p_numz;
+      int slot = 6;
+      if (qi == i - 1) slot = 0;
+      else if (qi == i + 1) slot = 1;
+      else if (qj == j - 1) slot = 2;
+      else if (qj == j + 1) slot = 3;
+      else if (qk == k - 1) slot = 4;
+      else if (qk == k + 1) slot = 5;
+      row[slot] = e.second;
+    }
+  }
+  return A->NumMyRows();
 }
 
 /* Reference charge bookkeeping used by the flight (Rho = screening density):

@@ -151,6 +151,24 @@ class Oracle:
     def reset_tallies(self):
         self.lib.orc_reset_tallies()
 
+    def density_and_field(self):
+        """particle_to_density -> compute_field (Poisson + pot2field) -> compute_cell_charge."""
+        self.lib.orc_density_and_field()
+
+    def contact_info(self):
+        per = np.zeros(16 * 3)
+        planes = np.zeros(64 * 7, dtype=np.int32)
+        n = self.lib.orc_contact_info(per.ctypes.data, planes.ctypes.data, 64)
+        nc = int(self.scalar("num_contact"))
+        per = per[:3 * nc].reshape(nc, 3)
+        return per[:, 1].copy(), per[:, 2].copy(), planes[:7 * n].reshape(n, 7).copy()
+
+    def poisson_stencil(self) -> np.ndarray:
+        nx, ny, nz, px, py, pz = self.dims()
+        out = np.zeros(px * py * pz * 7)
+        self.lib.orc_poisson_stencil(out.ctypes.data)
+        return out
+
     def contacts(self) -> np.ndarray:
         out = np.zeros((16, 6))
         n = self.lib.orc_contacts(out.ctypes.data)

@@ -33,7 +33,8 @@ ABS_TOL = 1e-12
 def engine_from_oracle(orc: Oracle, max_particles: int, flags: int = 0) -> mcb200.Engine:
     """Engine context carrying the oracle's mesh, cell data and fields."""
     eng = mcb200.Engine(table_dir=ORACLE_TABLES, kelvin=orc.scalar("T0"), device=0, max_particles=max_particles)
-    eng.set_mesh(orc.array("lx"), orc.array("ly"), orc.array("lz"))
+    eng.set_mesh(orc.array("lx"), orc.array("ly"), orc.array("lz"), orc.array("dx"), orc.array("dy"),
+                 orc.array("dz"))
     surf_dir = orc.array("SurfaceDir").astype(np.int32)
     eng.set_cells(orc.array("c_motion_rule").astype(np.int32), orc.array("c_da"),
                   attached_contact=orc.array("c_attached_contact").astype(np.int32),
