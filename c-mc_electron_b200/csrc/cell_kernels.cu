@@ -1,0 +1,195 @@
+// cell_kernels.cu -- per-cell kernels: surface scattering rates and
+// MultipleRefresh.
+//
+//  * surface_rates: MeshQuantities::GetSurfRoughnessPhononScRate
+//    (src/GetSurfRoughnessPhononScRate.cpp:4-70), one thread per cell, for
+//    electrons and holes.  Inputs are the cell field (both carriers feel the
+//    same field here), the screening density and the direction of the
+//    nearest Si/SiO2 surface.
+//  * multiple refresh: MeshQuantities::MultipleRefresh / gen_new_par_mr
+//    (src/MultipleRefresh.cpp:9-143), one thread per cell.  The store is
+//    sorted by cell; inside a cell the particles are taken in uid order
+//    (the reference takes its list order).  Each (cell, carrier) draws from
+//    its own stream (seed, cell, step, kRefreshSub + type).  Resampled
+//    particles get fresh uids in (cell, type, draw) order.
+#include "cell_kernels.h"
+
+namespace mcb200 {
+
+constexpr double kPiC = 3.141592653589793238462643e0;
+
+__global__ void surface_rates_kernel(int cells, SurfaceRateParams q, const double *field, const double *rho,
+                                     const int *eeff_dir, double *e_rough, double *e_phon, double *h_rough,
+                                     double *h_phon) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cells) return;
+  const double Rho = rho[c];
+  double Eeff = fabs(field[3 * (size_t)c + min(max(eeff_dir[c], 0), 2)]);
+  if (Eeff < 1e-20) Eeff = 1e-20;
+  for (int t = 0; t < 2; ++t) {
+    const double effmass = t == 0 ? 0.286 : 0.8;  // MASSeff, src/Constant_GlobalVariable_MathFunction.cpp:28
+    double rough = 0, phon = 0;
+    if (q.roughness) {
+      const double a = q.delta * q.ail * Eeff * q.eps_si / (q.eps_si + q.eps_ox);
+      rough = 2 * kPiC * effmass * (a * a);
+    }
+    if (q.phonon) {
+      const double Wcl = pow(q.Tn, q.nbmod) * q.boltz * q.T0 / (Eeff * q.field0);
+      const double Wq = pow(12.0 * effmass * q.em0 * (Eeff * q.field0) / q.ec0 / q.hq0 / q.hq0, -1.0 / 3.0);
+      const double Pf = q.pft * q.Tn + q.pfn * pow(Rho * q.conc0 / (1e17 * 1e6), q.npf) / q.Tn;
+      const double Wclq = (q.gama * Wcl + q.theta * Wq) / Pf;
+      phon = effmass * q.em0 * q.boltz * q.T0 * q.xiph * q.xiph /
+                 (q.hq0 * q.hq0 * q.hq0 * q.sirho * (9050.02 * 9050.02) * Wclq) / q.scrt0 +
+             q.ec0 / (effmass * q.em0 * q.kpha * pow(q.Tn, 2.24)) / q.scrt0;
+    }
+    if (t == 0) { e_rough[c] = rough; e_phon[c] = phon; }
+    else { h_rough[c] = rough; h_phon[c] = phon; }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// MultipleRefresh.  Pass 1 (count): order each cell's particles by uid (in
+// place, the cell is contiguous), decide per carrier whether to resample and
+// how many particles the cell will hold.  Pass 2 (emit): write the cell's
+// new population at its scanned offset.
+struct Decision {
+  int keep;      // 1: keep the old population of this type
+  int old_num;   // particles with |q| >= pckill
+  double tot;    // their total charge
+};
+
+__device__ void order_cell_by_uid(DevParticles P, int b, int e) {
+  for (int i = b + 1; i < e; ++i) {  // insertion sort on uid, moving whole particles
+    const uint32_t u = P.uid[i];
+    const double x = P.x[i], y = P.y[i], z = P.z[i], kx = P.kx[i], ky = P.ky[i], kz = P.kz[i];
+    const double en = P.energy[i], ch = P.charge[i];
+    const uint32_t cl = P.cell[i], me = P.meta[i];
+    const int32_t it = P.itet[i];
+    int j = i - 1;
+    while (j >= b && P.uid[j] > u) {
+      P.uid[j + 1] = P.uid[j]; P.x[j + 1] = P.x[j]; P.y[j + 1] = P.y[j]; P.z[j + 1] = P.z[j];
+      P.kx[j + 1] = P.kx[j]; P.ky[j + 1] = P.ky[j]; P.kz[j + 1] = P.kz[j];
+      P.energy[j + 1] = P.energy[j]; P.charge[j + 1] = P.charge[j];
+      P.cell[j + 1] = P.cell[j]; P.meta[j + 1] = P.meta[j]; P.itet[j + 1] = P.itet[j];
+      --j;
+    }
+    P.uid[j + 1] = u; P.x[j + 1] = x; P.y[j + 1] = y; P.z[j + 1] = z;
+    P.kx[j + 1] = kx; P.ky[j + 1] = ky; P.kz[j + 1] = kz;
+    P.energy[j + 1] = en; P.charge[j + 1] = ch;
+    P.cell[j + 1] = cl; P.meta[j + 1] = me; P.itet[j + 1] = it;
+  }
+}
+
+// gen_new_par_mr's test (src/MultipleRefresh.cpp:18-33) for one carrier type.
+__device__ Decision decide(const DevParticles &P, int b, int e, int type, int new_num, const RefreshParams &r) {
+  Decision d{1, 0, 0.0};
+  double tmp = 0;
+  for (int i = b; i < e; ++i) {
+    if (((P.meta[i] >> 8) & 255) != (uint32_t)type || fabs(P.charge[i]) < r.pckill) continue;
+    d.old_num++;
+    d.tot += P.charge[i];
+    tmp += P.charge[i] * P.charge[i];
+  }
+  if (d.old_num == 0) return d;
+  if (((d.old_num > new_num / r.rpar) && (d.old_num < new_num * r.rpar)) &&
+      (tmp < (d.tot * d.tot * r.rsqr / d.old_num)))
+    return d;
+  d.keep = 0;
+  return d;
+}
+
+__global__ void refresh_count_kernel(DevParticles P, const unsigned int *cell_end, const unsigned int *cell_count,
+                                     int cells, const int *desired_e, const int *desired_h, RefreshParams r,
+                                     unsigned int *out_count, unsigned int *new_count) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cells) return;
+  const int e = (int)cell_end[c], b = e - (int)cell_count[c];
+  order_cell_by_uid(P, b, e);
+  unsigned int total = 0, fresh = 0;
+  for (int t = 0; t < 2; ++t) {
+    const int want = t == 0 ? desired_e[c] : desired_h[c];
+    const Decision d = decide(P, b, e, t, want, r);
+    if (d.keep) total += d.old_num;
+    else {
+      total += want;
+      fresh += want;
+    }
+  }
+  out_count[c] = total;
+  new_count[c] = fresh;
+}
+
+__global__ void refresh_emit_kernel(DevParticles P, const unsigned int *cell_end, const unsigned int *cell_count,
+                                    int cells, const int *desired_e, const int *desired_h, RefreshParams r,
+                                    const unsigned int *out_offset, const unsigned int *uid_offset, uint32_t uid0,
+                                    DevParticles dst, unsigned long long *mr_gen) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cells) return;
+  const int e = (int)cell_end[c], b = e - (int)cell_count[c];
+  unsigned int o = out_offset[c];
+  uint32_t uid = uid0 + uid_offset[c];
+  auto copy = [&](int from, unsigned int to) {
+    dst.x[to] = P.x[from]; dst.y[to] = P.y[from]; dst.z[to] = P.z[from];
+    dst.kx[to] = P.kx[from]; dst.ky[to] = P.ky[from]; dst.kz[to] = P.kz[from];
+    dst.energy[to] = P.energy[from]; dst.charge[to] = P.charge[from];
+    dst.cell[to] = P.cell[from]; dst.itet[to] = P.itet[from]; dst.meta[to] = P.meta[from] & 0xffffu;
+    dst.uid[to] = P.uid[from];
+  };
+  int produced = 0;
+  for (int t = 0; t < 2; ++t) {
+    const int want = t == 0 ? desired_e[c] : desired_h[c];
+    const Decision d = decide(P, b, e, t, want, r);
+    if (d.keep) {
+      for (int i = b; i < e; ++i)
+        if (((P.meta[i] >> 8) & 255) == (uint32_t)t && fabs(P.charge[i]) >= r.pckill) copy(i, o++);
+      produced += d.old_num;
+      continue;
+    }
+    // draw `want` particles with probability |q| / sum|q| (lower_bound on the
+    // running sum, src/MultipleRefresh.cpp:35-44); the new charge is tot/want
+    const double aver = d.tot / want;
+    for (int q = 0; q < want; ++q) {
+      const double s = mcb200_uniform(r.seed, (uint32_t)c, r.step, kRefreshSub + t, (uint32_t)q) * fabs(d.tot);
+      double w = 0;
+      int pick = -1, last = -1;
+      for (int i = b; i < e; ++i) {
+        if (((P.meta[i] >> 8) & 255) != (uint32_t)t || fabs(P.charge[i]) < r.pckill) continue;
+        last = i;
+        w += fabs(P.charge[i]);
+        if (w >= s) {  // first running sum not below s
+          pick = i;
+          break;
+        }
+      }
+      if (pick < 0) pick = last;  // s above the last sum (rounding): the reference prints and skips; keep the count
+      copy(pick, o);
+      dst.charge[o] = aver;
+      dst.uid[o] = uid++;
+      ++o;
+    }
+    produced += want;
+  }
+  atomicAdd(mr_gen, (unsigned long long)(long long)(produced - (e - b)));
+}
+
+void launch_surface_rates(int cells, const SurfaceRateParams &q, const double *field, const double *rho,
+                          const int *eeff_dir, double *e_rough, double *e_phon, double *h_rough, double *h_phon,
+                          cudaStream_t s) {
+  surface_rates_kernel<<<(cells + 255) / 256, 256, 0, s>>>(cells, q, field, rho, eeff_dir, e_rough, e_phon, h_rough,
+                                                           h_phon);
+}
+void launch_refresh_count(const DevParticles &P, const unsigned int *cell_end, const unsigned int *cell_count,
+                          int cells, const int *desired_e, const int *desired_h, const RefreshParams &r,
+                          unsigned int *out_count, unsigned int *new_count, cudaStream_t s) {
+  refresh_count_kernel<<<(cells + 127) / 128, 128, 0, s>>>(P, cell_end, cell_count, cells, desired_e, desired_h, r,
+                                                           out_count, new_count);
+}
+void launch_refresh_emit(const DevParticles &P, const unsigned int *cell_end, const unsigned int *cell_count,
+                         int cells, const int *desired_e, const int *desired_h, const RefreshParams &r,
+                         const unsigned int *out_offset, const unsigned int *uid_offset, uint32_t uid0,
+                         const DevParticles &dst, unsigned long long *mr_gen, cudaStream_t s) {
+  refresh_emit_kernel<<<(cells + 127) / 128, 128, 0, s>>>(P, cell_end, cell_count, cells, desired_e, desired_h, r,
+                                                          out_offset, uid_offset, uid0, dst, mr_gen);
+}
+
+}  // namespace mcb200

@@ -1,0 +1,40 @@
+// cell_kernels.h -- per-cell kernels (cell_kernels.cu): surface scattering
+// rates and MultipleRefresh.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "device_state.cuh"
+#include "mcb200_rng.h"
+
+namespace mcb200 {
+
+// `sub` word of the refresh streams: kRefreshSub + carrier type.
+constexpr uint32_t kRefreshSub = 0x4d520000u;
+
+// GetSurfRoughnessPhononScRate inputs: the SurfSc_* parameters
+// (src/mcmodel.cpp:4107-4121) and the unit constants they are combined with.
+struct SurfaceRateParams {
+  double delta, ail, xiph, theta, gama, nbmod, npf, pft, pfn, kpha;
+  int roughness, phonon;
+  double eps_si, eps_ox, Tn, T0, boltz, field0, em0, ec0, hq0, conc0, sirho, scrt0;
+};
+
+struct RefreshParams {
+  uint64_t seed;
+  uint32_t step;
+  double rpar, rsqr, pckill;
+};
+
+void launch_surface_rates(int cells, const SurfaceRateParams &q, const double *field, const double *rho,
+                          const int *eeff_dir, double *e_rough, double *e_phon, double *h_rough, double *h_phon,
+                          cudaStream_t s);
+void launch_refresh_count(const DevParticles &P, const unsigned int *cell_end, const unsigned int *cell_count,
+                          int cells, const int *desired_e, const int *desired_h, const RefreshParams &r,
+                          unsigned int *out_count, unsigned int *new_count, cudaStream_t s);
+void launch_refresh_emit(const DevParticles &P, const unsigned int *cell_end, const unsigned int *cell_count,
+                         int cells, const int *desired_e, const int *desired_h, const RefreshParams &r,
+                         const unsigned int *out_offset, const unsigned int *uid_offset, uint32_t uid0,
+                         const DevParticles &dst, unsigned long long *mr_gen, cudaStream_t s);
+
+}  // namespace mcb200

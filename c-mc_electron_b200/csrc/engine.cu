@@ -6,6 +6,7 @@
 #include <string>
 #include <vector>
 
+#include "cell_kernels.h"
 #include "engine_kernels.h"
 #include "field_kernels.h"
 #include "flight_physics.cuh"
@@ -943,6 +944,84 @@ int mcb200_solve_poisson(mcb200_ctx *c, double rel_tol, int max_iter, int *itera
   }
 }
 
+int mcb200_surface_rates(mcb200_ctx *c, const mcb200_surface_params *p, const int32_t *eeff_direction) {
+  if (!c || !p || !eeff_direction) return MCB200_ERR_ARG;
+  if (!c->mesh_set) return fail(c, MCB200_ERR_STATE, "mcb200_surface_rates before mcb200_set_mesh");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    const Units &u = c->tab.u;
+    SurfaceRateParams q{};
+    q.delta = p->delta; q.ail = p->ail; q.xiph = p->xiph; q.theta = p->theta; q.gama = p->gama;
+    q.nbmod = p->nbmod; q.npf = p->npf; q.pft = p->pft; q.pfn = p->pfn; q.kpha = p->kpha;
+    q.roughness = p->roughness; q.phonon = p->phonon;
+    q.eps_si = u.eps_silicon; q.eps_ox = u.eps_oxide; q.Tn = u.Tn; q.T0 = u.T0; q.boltz = 8.617343e-5;
+    q.field0 = u.field0; q.em0 = u.em0; q.ec0 = u.ec0; q.hq0 = u.hq0; q.conc0 = u.conc0; q.sirho = u.sirho;
+    q.scrt0 = u.scrt0;
+    std::vector<void *> tmp;
+    int *dir = dalloc<int>(c->ncells, tmp);
+    ck(cudaMemcpyAsync(dir, eeff_direction, sizeof(int) * c->ncells, cudaMemcpyHostToDevice, c->stream), "copy");
+    const DevMesh &m = c->mesh;
+    launch_surface_rates(c->ncells, q, m.hfield, m.rho, dir, const_cast<double *>(m.e_rough),
+                         const_cast<double *>(m.e_sphon), const_cast<double *>(m.h_rough),
+                         const_cast<double *>(m.h_sphon), c->stream);
+    ck(cudaGetLastError(), "surface rates");
+    ck(cudaStreamSynchronize(c->stream), "sync");
+    for (void *q2 : tmp) cudaFree(q2);
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_multiple_refresh(mcb200_ctx *c, const int32_t *desired_e, const int32_t *desired_h, uint32_t step,
+                            uint64_t seed, int64_t *generated) {
+  if (!c || !desired_e || !desired_h) return MCB200_ERR_ARG;
+  if (!c->mesh_set) return fail(c, MCB200_ERR_STATE, "mcb200_multiple_refresh before mcb200_set_mesh");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    cudaStream_t s = c->stream;
+    const int cells = c->ncells;
+    size_t want = 0;
+    for (int q = 0; q < cells; ++q) want += (size_t)std::max(desired_e[q], 0) + (size_t)std::max(desired_h[q], 0);
+    if (want > c->capacity) return fail(c, MCB200_ERR_CAPACITY, "refresh targets exceed the particle capacity");
+    std::vector<void *> tmp;
+    int *de = dalloc<int>(cells, tmp), *dh = dalloc<int>(cells, tmp);
+    unsigned int *out_count = dalloc<unsigned int>(cells, tmp), *new_count = dalloc<unsigned int>(cells, tmp);
+    unsigned int *out_off = dalloc<unsigned int>(cells, tmp), *uid_off = dalloc<unsigned int>(cells, tmp);
+    unsigned int *tiles = dalloc<unsigned int>((cells + 1023) / 1024 + 1, tmp), *tot = dalloc<unsigned int>(2, tmp);
+    unsigned long long *gen = dalloc<unsigned long long>(1, tmp);
+    ck(cudaMemcpyAsync(de, desired_e, sizeof(int) * cells, cudaMemcpyHostToDevice, s), "copy");
+    ck(cudaMemcpyAsync(dh, desired_h, sizeof(int) * cells, cudaMemcpyHostToDevice, s), "copy");
+    ck(cudaMemsetAsync(gen, 0, sizeof(unsigned long long), s), "memset");
+    // group the store by cell into the other buffer (hist = counts, offsets =
+    // cell ends); the refreshed population then goes back to this buffer
+    const int sorted = 1 - c->cur, other = c->cur;
+    launch_cell_sort(c->pb[c->cur].d, (int)c->n, c->pb[sorted].d, cells, c->mesh.nx, c->mesh.nz, c->hist,
+                     c->offsets, c->tile_sums, c->total, grid_for(c, c->n, 256), s);
+    const RefreshParams r{seed, step, 2.0, 2.0, 1.0e-30};  // Rpar, Rsqr, pckill: src/mcmodel.cpp:3878-3880
+    const DevParticles &P = c->pb[sorted].d;
+    launch_refresh_count(P, c->offsets, c->hist, cells, de, dh, r, out_count, new_count, s);
+    launch_exclusive_scan(out_count, out_off, tiles, tot, cells, s);
+    launch_exclusive_scan(new_count, uid_off, tiles, tot + 1, cells, s);
+    launch_refresh_emit(P, c->offsets, c->hist, cells, de, dh, r, out_off, uid_off, c->next_uid, c->pb[other].d, gen,
+                        s);
+    ck(cudaGetLastError(), "refresh");
+    unsigned int totals[2];
+    long long g = 0;
+    ck(cudaMemcpyAsync(totals, tot, sizeof(totals), cudaMemcpyDeviceToHost, s), "copy");
+    ck(cudaMemcpyAsync(&g, gen, sizeof(g), cudaMemcpyDeviceToHost, s), "copy");
+    ck(cudaStreamSynchronize(s), "sync");
+    for (void *q : tmp) cudaFree(q);
+    c->cur = other;
+    c->n = totals[0];
+    c->next_uid += totals[1];
+    if (generated) *generated = g;
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
 int mcb200_get_array(mcb200_ctx *c, const char *name, double *out, size_t n) {
   if (!c || !name || !out) return MCB200_ERR_ARG;
   if (!c->mesh_set) return fail(c, MCB200_ERR_STATE, "mcb200_get_array before mcb200_set_mesh");
@@ -951,6 +1030,10 @@ int mcb200_get_array(mcb200_ctx *c, const char *name, double *out, size_t n) {
   const double *src = nullptr;
   size_t len = 0;
   if (nm == "rho") { src = c->mesh.rho; len = cells; }
+  else if (nm == "e_rough") { src = c->mesh.e_rough; len = cells; }
+  else if (nm == "e_phonon") { src = c->mesh.e_sphon; len = cells; }
+  else if (nm == "h_rough") { src = c->mesh.h_rough; len = cells; }
+  else if (nm == "h_phonon") { src = c->mesh.h_sphon; len = cells; }
   else if (nm == "efield") { src = c->mesh.efield; len = 3 * cells; }
   else if (nm == "hfield") { src = c->mesh.hfield; len = 3 * cells; }
   else if (c->device_set && nm == "cell_charge_e") { src = c->fb.cell_e; len = cells; }

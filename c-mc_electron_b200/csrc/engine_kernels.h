@@ -18,6 +18,8 @@ void launch_children_to_particles(const DevChildren &c, int n, const uint32_t *u
                                   const DevParticles &dst, int dst_offset, unsigned int *dst_count, cudaStream_t s);
 void launch_seed(const FlightCtx &F, const DevParticles &P, int offset, int n, const int *cell_of,
                  const double *charge, int type, uint32_t uid0, int grid, cudaStream_t s);
+void launch_exclusive_scan(const unsigned int *in, unsigned int *out, unsigned int *tile_sums, unsigned int *total,
+                           int n, cudaStream_t s);
 void launch_cell_sort(const DevParticles &src, int n, const DevParticles &dst, int ncells, int nx, int nz,
                       unsigned int *hist, unsigned int *offsets, unsigned int *tile_sums, unsigned int *total,
                       int grid, cudaStream_t s);

@@ -285,6 +285,13 @@ void launch_children_to_particles(const DevChildren &c, int n, const uint32_t *u
                                   const DevParticles &dst, int dst_offset, unsigned int *dst_count, cudaStream_t s) {
   if (n > 0) children_to_particles<<<(n + 255) / 256, 256, 0, s>>>(c, n, uids, alive, dst, dst_offset, dst_count);
 }
+void launch_exclusive_scan(const unsigned int *in, unsigned int *out, unsigned int *tile_sums, unsigned int *total,
+                           int n, cudaStream_t s) {
+  const int tiles = (n + 1023) / 1024;
+  scan_tiles<<<tiles, 1024, 0, s>>>(in, out, tile_sums, n);
+  scan_tile_sums<<<1, 32, 0, s>>>(tile_sums, tiles, total);
+  scan_add<<<tiles, 1024, 0, s>>>(out, tile_sums, n);
+}
 void launch_cell_sort(const DevParticles &src, int n, const DevParticles &dst, int ncells, int nx, int nz,
                       unsigned int *hist, unsigned int *offsets, unsigned int *tile_sums, unsigned int *total,
                       int grid, cudaStream_t s) {

@@ -40,6 +40,18 @@ class _Particles(ctypes.Structure):
                 ("x", "y", "z", "kx", "ky", "kz", "charge", "energy", "i", "j", "k", "itet", "isym", "type", "uid")]
 
 
+class SurfaceParams(ctypes.Structure):
+    """mcb200_surface_params; defaults are the reference's SurfSc_* values
+    (src/mcmodel.cpp:4107-4121) with lengths in metres (converted by
+    Engine.surface_rates)."""
+    _fields_ = [(n, ctypes.c_double) for n in ("delta", "ail", "xiph", "theta", "gama", "nbmod", "npf", "pft",
+                                               "pfn", "kpha")] + [("roughness", ctypes.c_int),
+                                                                  ("phonon", ctypes.c_int)]
+
+
+SURFACE_DEFAULTS = dict(delta_m=0.1126755e-9, ail_m=2.0e-9, xiph=12.0, theta=2.857703, gama=1.5, nbmod=2.0,
+                        npf=-0.6, pft=0.7, pfn=0.3, kpha=3600e-4, roughness=1, phonon=1)
+
 PARTICLE_FIELDS = {
     "x": np.float64, "y": np.float64, "z": np.float64, "kx": np.float64, "ky": np.float64, "kz": np.float64,
     "charge": np.float64, "energy": np.float64, "i": np.int32, "j": np.int32, "k": np.int32,
@@ -66,6 +78,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mcb200_deposit.argtypes = [vp]
     lib.mcb200_solve_poisson.argtypes = [vp, c.c_double, c.c_int, c.POINTER(c.c_int), dp]
     lib.mcb200_get_array.argtypes = [vp, c.c_char_p, dp, c.c_size_t]
+    lib.mcb200_surface_rates.argtypes = [vp, c.POINTER(SurfaceParams), i32p]
+    lib.mcb200_multiple_refresh.argtypes = [vp, i32p, i32p, c.c_uint32, c.c_uint64, c.POINTER(c.c_int64)]
     lib.mcb200_set_cells.argtypes = [vp, i32p, i32p, i32p, i32p, i32p, c.c_int, dp, c.c_int]
     lib.mcb200_set_fields.argtypes = [vp, dp, dp, dp]
     lib.mcb200_set_surface_rates.argtypes = [vp, dp, dp, dp, dp]
@@ -182,6 +196,23 @@ class Engine:
                                                 _ptr(ph, ctypes.c_double), len(pl) // 7, _ptr(pl, ctypes.c_int32)),
                     "set_device")
 
+    def surface_rates(self, eeff_direction, **overrides):
+        """Per-cell surface rates from the current fields (mcb200_surface_rates)."""
+        p = dict(SURFACE_DEFAULTS, **overrides)
+        spr0 = self.units()["spr0"]
+        sp = SurfaceParams(p["delta_m"] / spr0, p["ail_m"] / spr0, p["xiph"], p["theta"], p["gama"], p["nbmod"],
+                           p["npf"], p["pft"], p["pfn"], p["kpha"], int(p["roughness"]), int(p["phonon"]))
+        d = np.ascontiguousarray(eeff_direction, dtype=np.int32)
+        self._check(self._lib.mcb200_surface_rates(self._ctx, ctypes.byref(sp), _ptr(d, ctypes.c_int32)),
+                    "surface_rates")
+
+    def multiple_refresh(self, desired_e, desired_h, step: int, seed: int) -> int:
+        de, dh = (np.ascontiguousarray(a, dtype=np.int32) for a in (desired_e, desired_h))
+        gen = ctypes.c_int64()
+        self._check(self._lib.mcb200_multiple_refresh(self._ctx, _ptr(de, ctypes.c_int32), _ptr(dh, ctypes.c_int32),
+                                                      step, seed, ctypes.byref(gen)), "multiple_refresh")
+        return gen.value
+
     def deposit(self):
         self._check(self._lib.mcb200_deposit(self._ctx), "deposit")
 
@@ -194,7 +225,8 @@ class Engine:
     def array(self, name: str) -> np.ndarray:
         m = self.mesh
         per = {"rho": m.ncells, "efield": 3 * m.ncells, "hfield": 3 * m.ncells, "cell_charge_e": m.ncells,
-               "cell_charge_h": m.ncells, "cell_volume": m.ncells, "stencil": 7 * m.nnodes}
+               "cell_charge_h": m.ncells, "cell_volume": m.ncells, "stencil": 7 * m.nnodes,
+               "e_rough": m.ncells, "e_phonon": m.ncells, "h_rough": m.ncells, "h_phonon": m.ncells}
         out = np.zeros(per.get(name, m.nnodes))
         self._check(self._lib.mcb200_get_array(self._ctx, name.encode(), _ptr(out, ctypes.c_double), out.size),
                     name)

@@ -35,10 +35,12 @@ def write_input(path: str, **kv):
 
 
 def contact_bar(dirpath: str, nx=8, ny=10, nz=6, cell_nm=5.0, donor_m3=1e24, vd=0.3, electrons=4000, holes=0,
-                dt=1e-15, kelvin=300.0) -> dict:
+                dt=1e-15, kelvin=300.0, surfaces=False) -> dict:
     """n-Si bar with a grounded contact on the y = 0 node plane and a contact
     at `vd` volts on the far y plane (REFLECT on every face): the smallest
-    device with Dirichlet rows in its Poisson problem."""
+    device with Dirichlet rows in its Poisson problem.  surfaces=True adds
+    Si/SiO2 surfaces at x = 0 and z = 0 with surface scattering in the whole
+    bar (the `surfaces` and `surface_scatter_range` keywords)."""
     os.makedirs(dirpath, exist_ok=True)
     X, Y, Z = nx * cell_nm, ny * cell_nm, nz * cell_nm
     write_grid(os.path.join(dirpath, "lgrid.txt"), np.arange(nx + 1) * cell_nm, np.arange(ny + 1) * cell_nm,
@@ -59,11 +61,13 @@ def contact_bar(dirpath: str, nx=8, ny=10, nz=6, cell_nm=5.0, donor_m3=1e24, vd=
         f"motionplane 0 {g(X)} 0 {g(Y)} {g(Z)} {g(Z)} BACK REFLECT",
         "contact", "1 0", f"0 {g(X)} 0 0 0 {g(Z)}", "0",
         "contact", "1 0", f"0 {g(X)} {g(Y)} {g(Y)} 0 {g(Z)}", f"{vd:g}",
-        "end",
     ]
+    if surfaces:
+        lines += ["surfaces 2", "0 0 0", "2 0 4", f"surface_scatter_range {box}"]
+    lines.append("end")
     with open(os.path.join(dirpath, "ldg.txt"), "w") as f:
         f.write("\n".join(lines) + "\n")
-    write_input(os.path.join(dirpath, "input.txt"), dt=dt, Temperature=kelvin, Flag_SurfaceScatter=0,
+    write_input(os.path.join(dirpath, "input.txt"), dt=dt, Temperature=kelvin, Flag_SurfaceScatter=int(surfaces),
                 ElectronNumber=electrons, HoleNumber=holes)
     return dict(input=os.path.join(dirpath, "input.txt"), grid=os.path.join(dirpath, "lgrid.txt"),
                 device=os.path.join(dirpath, "ldg.txt"))

@@ -127,7 +127,36 @@ int mcb200_deposit(mcb200_ctx *ctx);
  * cell fields of both carriers (pot2field, :2732-2855). */
 int mcb200_solve_poisson(mcb200_ctx *ctx, double rel_tol, int max_iter, int *iterations, double *rel_residual);
 
-/* Copy a device array to the host: "rho", "efield", "hfield" (3 per cell),
+/* Surface scattering parameters (the SurfSc_* members set in
+ * init_phpysical_parameter, src/mcmodel.cpp:4107-4121): delta and ail are the
+ * roughness rms height and correlation length in normalised length; the
+ * reference hard-codes 0.1126755 nm and 2 nm. */
+typedef struct {
+  double delta, ail, xiph, theta, gama, nbmod, npf, pft, pfn, kpha;
+  int roughness; /* Flag_SurfaceRoughnessScatter */
+  int phonon;    /* Flag_SurfacePhononScatter */
+} mcb200_surface_params;
+
+/* Per-cell surface roughness and surface phonon rates of both carriers from
+ * the current fields and screening density (GetSurfRoughnessPhononScRate,
+ * src/GetSurfRoughnessPhononScRate.cpp:4-70); eeff_direction per cell is the
+ * axis (0 x, 1 y, 2 z) of the nearest Si/SiO2 surface (c_EeffDirection,
+ * init_surface_roughness, src/mcmodel.cpp:3155-3185). */
+int mcb200_surface_rates(mcb200_ctx *ctx, const mcb200_surface_params *params, const int32_t *eeff_direction);
+
+/* MultipleRefresh (src/MultipleRefresh.cpp:9-143): per cell and carrier,
+ * particles with |q| < 1e-30 are dropped and, unless the count is within a
+ * factor Rpar = 2 of desired and the charge spread within Rsqr = 2, the
+ * population is resampled to desired_e / desired_h particles with
+ * probability |q| / sum|q|, each carrying sum(q) / desired.  Within a cell
+ * particles are taken in uid order; each (cell, carrier) draws from stream
+ * (seed, cell, step, 0x4d520000 + carrier); resampled particles get fresh
+ * uids.  *generated receives the change in particle count (mr_gen_num). */
+int mcb200_multiple_refresh(mcb200_ctx *ctx, const int32_t *desired_e, const int32_t *desired_h, uint32_t step,
+                            uint64_t seed, int64_t *generated);
+
+/* Copy a device array to the host: "rho", "e_rough", "e_phonon", "h_rough",
+ * "h_phonon", "efield", "hfield" (3 per cell),
  * "cell_charge_e", "cell_charge_h", "cell_volume" (per cell);
  * "node_density", "node_volume", "node_doping", "vadd", "rhs", "potential"
  * (per node); "stencil" (7 per node). */

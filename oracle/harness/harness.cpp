@@ -413,6 +413,36 @@ int orc_poisson_stencil(double *out) {
   return A->NumMyRows();
 }
 
+/* MultipleRefresh (src/MultipleRefresh.cpp:60-143) cell by cell, with the
+ * reference's own gen_new_par_mr (:9-58) doing the resampling.  The loop is
+ * restated here only to fix the two things the engine defines: a cell's
+ * particles are taken in uid order, and each (cell, carrier) draws from
+ * stream (seed, cell, step, 0x4d520000 + carrier). */
+int orc_multiple_refresh(uint32_t step) {
+  MeshQuantities *mq = g_mq;
+  int *e_num, *h_num;
+  mq->c_desired_electron_number->ExtractView(&e_num);
+  mq->c_desired_hole_number->ExtractView(&h_num);
+  for (size_t c = 0; c < mq->par_list.size(); ++c) {
+    std::list<Particle> &lst = mq->par_list[c];
+    std::vector<Particle> all(lst.begin(), lst.end());
+    std::stable_sort(all.begin(), all.end(),
+                     [](const Particle &a, const Particle &b) { return (uint32_t)a.par_id < (uint32_t)b.par_id; });
+    std::vector<Particle> vec[2], fresh[2];
+    for (const Particle &p : all)
+      if (fabs(p.charge) >= mq->pckill) vec[p.par_type == PELEC ? 0 : 1].push_back(p);
+    const size_t before = lst.size();
+    lst.clear();
+    for (int t = 0; t < 2; ++t) {
+      set_stream((uint32_t)c, step, 0x4d520000u + (uint32_t)t);
+      const bool redone = mq->gen_new_par_mr(vec[t], t == 0 ? e_num[c] : h_num[c], fresh[t]);
+      for (const Particle &p : redone ? fresh[t] : vec[t]) lst.push_back(p);
+    }
+    mq->mr_gen_num += (int)lst.size() - (int)before;
+  }
+  return mq->mr_gen_num;
+}
+
 /* Reference charge bookkeeping used by the flight (Rho = screening density):
  * src/mcmodel.cpp:2664-2712. */
 int orc_compute_cell_charge() {

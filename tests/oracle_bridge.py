@@ -151,6 +151,10 @@ class Oracle:
     def reset_tallies(self):
         self.lib.orc_reset_tallies()
 
+    def multiple_refresh(self, step: int) -> int:
+        self.lib.orc_multiple_refresh.argtypes = [ctypes.c_uint32]
+        return int(self.lib.orc_multiple_refresh(step))
+
     def density_and_field(self):
         """particle_to_density -> compute_field (Poisson + pot2field) -> compute_cell_charge."""
         self.lib.orc_density_and_field()
