@@ -4,20 +4,25 @@
 One JSON line on rank 0.  A "step" is one transport step (mcb200_step:
 flight of every particle over dt, mid-step copies, removal, counting sort by
 cell) of the bulk n-Si box: 40x20x20 cells of 5 nm, N_D = 1e17 cm^-3, 300 K,
-frozen uniform E_x = 10 kV/cm, dt = 1 fs, FP64, REFLECT on every face (the
-reference's config-1 physics), with the electron ensemble scaled so the
-particle store (80 B / particle) exceeds the 126 MB L2.
+frozen uniform E_x = 10 kV/cm, dt = 1 fs, REFLECT on every face (the
+reference's bulk physics), with the electron ensemble scaled so the
+particle store exceeds the 126 MB L2.  The same workload is timed twice:
+plain FP64 flight (80 B / particle, the reference's arithmetic) and FP32
+flight (56 B / particle, float kinematics and rate lookups, FP64 energy and
+time bookkeeping).
 
-  value     particle-steps/s of the whole job, state resident in HBM,
-            device time of the timed steps (CUDA events on the engine stream)
-  e2e       the same metric through the C ABI with host buffers: each step
-            uploads the step's cell fields from pinned memory and reads the
-            tallies back
-  roofline  flight kernel: 160 algorithmic bytes per particle-step (read +
-            write of the 80-byte FP64 state) / measured kernel time, against
-            the measured HBM copy bandwidth
+  value       FP32-flight particle-steps/s of the whole job, state resident
+              in HBM, device time of the timed steps (CUDA events on the
+              engine stream); fp64_plain.value is the FP64 arm, and
+              fp32_over_fp64 their ratio
+  e2e         the same metric through the C ABI with host buffers: each
+              step uploads the step's cell fields from pinned memory and
+              reads the tallies back
+  roofline    flight kernel: 112 (FP32) / 160 (FP64) algorithmic bytes per
+              particle-step (read + write of the state) / measured kernel
+              time, against the measured HBM copy bandwidth
   cpu_baseline  the reference's own update_particle() (CPU oracle, one core)
-            on a bounded sample of the same box
+              on a bounded sample of the same box
 
 --impl reference times the reference's CPU implementation (the oracle built
 from its sources) on all host cores, one process per core.
@@ -40,9 +45,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "c-mc_electron_b200"))
 
 METRIC = "particle-steps/s"
-BOX = dict(nx=40, ny=20, nz=20, cell_nm=5.0, donor_m3=1e23, field_v_per_m=1e6, dt_s=1e-15, kelvin=300.0)
-BYTES_PER_PARTICLE_STEP_FP64 = 160  # read + write of the 80-byte FP64 particle state
-PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "flight_fp64_bulk_traffic.json")
+from mcb200.workloads import BULK_BOX as BOX  # noqa: E402
+
+# read + write of the particle state: 80 B (FP64 plain), 56 B (FP32 flight)
+BYTES_PER_PARTICLE_STEP = {"fp64": 160, "fp32": 112}
+PROFILE_TRAFFIC = {p: os.path.join(ROOT, "profiles", f"flight_{p}_bulk_traffic.json") for p in ("fp64", "fp32")}
 
 
 def measured_peaks():
@@ -102,53 +109,15 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------- engine arm
-def build_bulk_engine(particles: int, seed: int, device: int):
+def measure_precision(args, rank: int, world: int, device: int, precision: str):
+    """Warm-up, timed steps and e2e steps of one flight precision on the bulk
+    box; returns the measurements of this rank (maxima / sums over ranks)."""
     import mcb200
-
-    eng = mcb200.Engine(table_dir=mcb200.DEFAULT_TABLE_DIR, kelvin=BOX["kelvin"], device=device,
-                        max_particles=particles + particles // 8 + 4096)
-    u = eng.units()
-    nx, ny, nz = BOX["nx"], BOX["ny"], BOX["nz"]
-    h = BOX["cell_nm"] * 1e-9 / u["spr0"]
-    eng.set_mesh(np.arange(nx + 1) * h, np.arange(ny + 1) * h, np.arange(nz + 1) * h)
-    cells = nx * ny * nz
-    # PASS inside, REFLECT on the six outer faces (UP, DOWN, LEFT, RIGHT, FRONT, BACK)
-    mr = np.full((nx, ny, nz, 6), 1, dtype=np.int32)  # indexed [i, j, k, face]
-    mr[0, :, :, 0] = 2
-    mr[nx - 1, :, :, 1] = 2
-    mr[:, 0, :, 2] = 2
-    mr[:, ny - 1, :, 3] = 2
-    mr[:, :, 0, 4] = 2
-    mr[:, :, nz - 1, 5] = 2
-    mr = np.ascontiguousarray(mr.transpose(1, 0, 2, 3)).reshape(-1)  # cell index (j*nx + i)*nz + k
-    doping = BOX["donor_m3"] / u["conc0"]
-    eng.set_cells(mr, np.full(cells, doping))
-    fields = fields_for(eng)
-    eng.set_fields(*fields)
-    per_cell = particles // cells
-    vol = h ** 3
-    cell_of = np.repeat(np.arange(cells, dtype=np.int32), per_cell)
-    charge = np.full(cell_of.size, -doping * vol / per_cell)
-    eng.seed(cell_of, charge, 0, seed)
-    dt = BOX["dt_s"] / u["time0"]
-    return eng, dt, fields
-
-
-def fields_for(eng):
-    u = eng.units()
-    cells = eng.mesh.ncells
-    e = np.zeros((cells, 3))
-    e[:, 0] = -BOX["field_v_per_m"] / u["field0"]  # electron-felt field: ChargeSign = -1
-    hfield = -e
-    rho = np.full(cells, BOX["donor_m3"] / u["conc0"])  # |q| density of a neutral box = N_D
-    return e.ravel(), hfield.ravel(), rho
-
-
-def engine_arm(args, rank: int, world: int, device: int):
-    import mcb200
+    from mcb200.workloads import bulk_box_engine
 
     seed = 1 + rank
-    eng, dt, fields = build_bulk_engine(args.particles, seed, device)
+    prec = mcb200.FLIGHT_FP32 if precision == "fp32" else mcb200.FLIGHT_FP64
+    eng, dt, fields = bulk_box_engine(args.particles, seed, device, precision=prec)
     n0 = eng.num_particles()
     for s in range(args.warmup):
         eng.step(s, seed, dt)
@@ -168,7 +137,6 @@ def engine_arm(args, rank: int, world: int, device: int):
     flight_ms_per_launch = tim["flight_ms"] / max(tim["flight_launches"], 1)
     tallies = eng.tallies()
     total_ps = dist_sum(tim["particles_flown"], world)
-    value = total_ps / (step_ms * 1e-3)
     # e2e: the public C ABI with host buffers; per step: pinned H2D of the
     # cell fields, one step, D2H of the tallies.
     try:
@@ -187,42 +155,60 @@ def engine_arm(args, rank: int, world: int, device: int):
     for s in range(base, base + e2e_steps):
         eng.set_fields(e_h, h_h, rho_h)
         eng.step(s, seed, dt)
-        t = eng.tallies()
+        eng.tallies()
         d2h = 8 * (16 + 16 * 6 + 2 * (eng.mesh.ny + 1) + 2 * eng.mesh.nnodes)
     e2e_wall = dist_max(time.perf_counter() - t0, world)
     e2e_ps = dist_sum(float(eng.num_particles()) * e2e_steps, world)
-    peak, peak_kind = measured_peaks()
-    achieved = BYTES_PER_PARTICLE_STEP_FP64 * (tim["particles_flown"] / max(tim["flight_launches"], 1)) / (
-        flight_ms_per_launch * 1e-3) / 1e9
+    bytes_ps = BYTES_PER_PARTICLE_STEP[precision]
+    per_launch = tim["particles_flown"] / max(tim["flight_launches"], 1)
+    achieved = bytes_ps * per_launch / (flight_ms_per_launch * 1e-3) / 1e9
     traffic = None
     try:
-        with open(PROFILE_TRAFFIC) as f:
-            prof = json.load(f)
-        traffic = prof["dram_bytes_per_particle_step"] * tim["particles_flown"] / max(tim["flight_launches"], 1)
+        with open(PROFILE_TRAFFIC[precision]) as f:
+            traffic = json.load(f)["dram_bytes_per_particle_step"] * per_launch
     except Exception:
         pass
-    out = {
-        "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": step_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"bulk n-Si box {BOX['nx']}x{BOX['ny']}x{BOX['nz']} cells of 5 nm, N_D=1e17 cm^-3, "
-                               f"E_x=10 kV/cm frozen, 300 K, dt=1 fs, FP64 flight, {n0} electrons per GPU",
-                   "particles_per_gpu": n0, "precision": "fp64-plain",
-                   "l2": "particle store larger than L2 (80 B x particles)", "parallelism": f"replicas{world}"},
-        "e2e": {"value": e2e_ps / e2e_wall, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic,
-                     "kernel": "flight_kernel", "peak_kind": peak_kind,
-                     "bytes_per_unit": BYTES_PER_PARTICLE_STEP_FP64},
-        "gpu_launches": int(tim["launches"]),
-        "clocks": clocks.summary(),
-        "flight_ms_per_launch": flight_ms_per_launch,
-        "wall_s": wall,
-        "events_per_particle_step": tallies["events"] / max(tim["particles_flown"], 1),
-    }
+    out = dict(n0=n0, value=total_ps / (step_ms * 1e-3), step_ms=step_ms, wall=wall,
+               flight_ms_per_launch=flight_ms_per_launch, launches=int(tim["launches"]),
+               clocks=clocks.summary(), e2e=e2e_ps / e2e_wall, h2d=h2d, d2h=d2h, achieved=achieved,
+               traffic=traffic, bytes=bytes_ps,
+               events=tallies["events"] / max(tim["particles_flown"], 1), caught=tallies["caught"],
+               zero_time=tallies["zero_time"])
     eng.close()
     return out
+
+
+def engine_arm(args, rank: int, world: int, device: int):
+    fp64 = measure_precision(args, rank, world, device, "fp64")
+    fp32 = measure_precision(args, rank, world, device, "fp32")
+    peak, peak_kind = measured_peaks()
+    box = f"bulk n-Si box {BOX['nx']}x{BOX['ny']}x{BOX['nz']} cells of 5 nm, N_D=1e17 cm^-3, E_x=10 kV/cm frozen, " \
+          f"300 K, dt=1 fs, {fp32['n0']} electrons per GPU"
+    roof = lambda m: {"bound": "hbm", "achieved": m["achieved"], "peak": peak, "unit": "GB/s",
+                      "frac": m["achieved"] / peak, "traffic": m["traffic"], "kernel": "flight_kernel",
+                      "peak_kind": peak_kind, "bytes_per_unit": m["bytes"]}
+    return {
+        "metric": METRIC, "value": fp32["value"], "unit": "particle-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": fp32["step_ms"] / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": box + "; FP32 flight (FP64 energy/time bookkeeping) vs plain FP64 flight",
+                   "particles_per_gpu": fp32["n0"], "precision": "fp32-flight",
+                   "l2": "particle store larger than L2 (56 B / 80 B x particles)",
+                   "parallelism": f"replicas{world}"},
+        "e2e": {"value": fp32["e2e"], "unit": "particle-steps/s", "h2d_bytes_per_step": fp32["h2d"],
+                "d2h_bytes_per_step": fp32["d2h"]},
+        "roofline": roof(fp32),
+        "gpu_launches": fp32["launches"],
+        "clocks": fp32["clocks"],
+        "fp64_plain": {"value": fp64["value"], "ms_per_step": fp64["step_ms"] / args.steps, "dtype": "f64",
+                       "e2e": fp64["e2e"], "roofline": roof(fp64), "gpu_launches": fp64["launches"],
+                       "clocks": fp64["clocks"], "events_per_particle_step": fp64["events"]},
+        "fp32_over_fp64": fp32["value"] / fp64["value"],
+        "flight_ms_per_launch": fp32["flight_ms_per_launch"],
+        "events_per_particle_step": fp32["events"],
+        "fp32_zero_time_catches": fp32["zero_time"],
+        "wall_s": fp32["wall"] + fp64["wall"],
+    }
 
 
 # ------------------------------------------------------------ reference (CPU)

@@ -58,10 +58,11 @@ struct Decision {
   double tot;    // their total charge
 };
 
-__device__ void order_cell_by_uid(DevParticles P, int b, int e) {
+template <typename R>
+__device__ void order_cell_by_uid(DevParticlesT<R> P, int b, int e) {
   for (int i = b + 1; i < e; ++i) {  // insertion sort on uid, moving whole particles
     const uint32_t u = P.uid[i];
-    const double x = P.x[i], y = P.y[i], z = P.z[i], kx = P.kx[i], ky = P.ky[i], kz = P.kz[i];
+    const R x = P.x[i], y = P.y[i], z = P.z[i], kx = P.kx[i], ky = P.ky[i], kz = P.kz[i];
     const double en = P.energy[i], ch = P.charge[i];
     const uint32_t cl = P.cell[i], me = P.meta[i];
     const int32_t it = P.itet[i];
@@ -81,7 +82,8 @@ __device__ void order_cell_by_uid(DevParticles P, int b, int e) {
 }
 
 // gen_new_par_mr's test (src/MultipleRefresh.cpp:18-33) for one carrier type.
-__device__ Decision decide(const DevParticles &P, int b, int e, int type, int new_num, const RefreshParams &r) {
+template <typename R>
+__device__ Decision decide(const DevParticlesT<R> &P, int b, int e, int type, int new_num, const RefreshParams &r) {
   Decision d{1, 0, 0.0};
   double tmp = 0;
   for (int i = b; i < e; ++i) {
@@ -98,7 +100,8 @@ __device__ Decision decide(const DevParticles &P, int b, int e, int type, int ne
   return d;
 }
 
-__global__ void refresh_count_kernel(DevParticles P, const unsigned int *cell_end, const unsigned int *cell_count,
+template <typename R>
+__global__ void refresh_count_kernel(DevParticlesT<R> P, const unsigned int *cell_end, const unsigned int *cell_count,
                                      int cells, const int *desired_e, const int *desired_h, RefreshParams r,
                                      unsigned int *out_count, unsigned int *new_count) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -119,10 +122,11 @@ __global__ void refresh_count_kernel(DevParticles P, const unsigned int *cell_en
   new_count[c] = fresh;
 }
 
-__global__ void refresh_emit_kernel(DevParticles P, const unsigned int *cell_end, const unsigned int *cell_count,
+template <typename R>
+__global__ void refresh_emit_kernel(DevParticlesT<R> P, const unsigned int *cell_end, const unsigned int *cell_count,
                                     int cells, const int *desired_e, const int *desired_h, RefreshParams r,
                                     const unsigned int *out_offset, const unsigned int *uid_offset, uint32_t uid0,
-                                    DevParticles dst, unsigned long long *mr_gen) {
+                                    DevParticlesT<R> dst, unsigned long long *mr_gen) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= cells) return;
   const int e = (int)cell_end[c], b = e - (int)cell_count[c];
@@ -178,18 +182,32 @@ void launch_surface_rates(int cells, const SurfaceRateParams &q, const double *f
   surface_rates_kernel<<<(cells + 255) / 256, 256, 0, s>>>(cells, q, field, rho, eeff_dir, e_rough, e_phon, h_rough,
                                                            h_phon);
 }
-void launch_refresh_count(const DevParticles &P, const unsigned int *cell_end, const unsigned int *cell_count,
+template <typename R>
+void launch_refresh_count(const DevParticlesT<R> &P, const unsigned int *cell_end, const unsigned int *cell_count,
                           int cells, const int *desired_e, const int *desired_h, const RefreshParams &r,
                           unsigned int *out_count, unsigned int *new_count, cudaStream_t s) {
-  refresh_count_kernel<<<(cells + 127) / 128, 128, 0, s>>>(P, cell_end, cell_count, cells, desired_e, desired_h, r,
+  refresh_count_kernel<R><<<(cells + 127) / 128, 128, 0, s>>>(P, cell_end, cell_count, cells, desired_e, desired_h, r,
                                                            out_count, new_count);
 }
-void launch_refresh_emit(const DevParticles &P, const unsigned int *cell_end, const unsigned int *cell_count,
+template <typename R>
+void launch_refresh_emit(const DevParticlesT<R> &P, const unsigned int *cell_end, const unsigned int *cell_count,
                          int cells, const int *desired_e, const int *desired_h, const RefreshParams &r,
                          const unsigned int *out_offset, const unsigned int *uid_offset, uint32_t uid0,
-                         const DevParticles &dst, unsigned long long *mr_gen, cudaStream_t s) {
-  refresh_emit_kernel<<<(cells + 127) / 128, 128, 0, s>>>(P, cell_end, cell_count, cells, desired_e, desired_h, r,
+                         const DevParticlesT<R> &dst, unsigned long long *mr_gen, cudaStream_t s) {
+  refresh_emit_kernel<R><<<(cells + 127) / 128, 128, 0, s>>>(P, cell_end, cell_count, cells, desired_e, desired_h, r,
                                                           out_offset, uid_offset, uid0, dst, mr_gen);
 }
+
+#define MCB200_INSTANTIATE(R)                                                                                 \
+  template void launch_refresh_count<R>(const DevParticlesT<R> &, const unsigned int *, const unsigned int *, \
+                                        int, const int *, const int *, const RefreshParams &, unsigned int *, \
+                                        unsigned int *, cudaStream_t);                                        \
+  template void launch_refresh_emit<R>(const DevParticlesT<R> &, const unsigned int *, const unsigned int *,  \
+                                       int, const int *, const int *, const RefreshParams &,                 \
+                                       const unsigned int *, const unsigned int *, uint32_t,                 \
+                                       const DevParticlesT<R> &, unsigned long long *, cudaStream_t);
+MCB200_INSTANTIATE(double)
+MCB200_INSTANTIATE(float)
+#undef MCB200_INSTANTIATE
 
 }  // namespace mcb200

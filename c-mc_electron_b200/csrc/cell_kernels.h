@@ -29,12 +29,14 @@ struct RefreshParams {
 void launch_surface_rates(int cells, const SurfaceRateParams &q, const double *field, const double *rho,
                           const int *eeff_dir, double *e_rough, double *e_phon, double *h_rough, double *h_phon,
                           cudaStream_t s);
-void launch_refresh_count(const DevParticles &P, const unsigned int *cell_end, const unsigned int *cell_count,
+template <typename R>
+void launch_refresh_count(const DevParticlesT<R> &P, const unsigned int *cell_end, const unsigned int *cell_count,
                           int cells, const int *desired_e, const int *desired_h, const RefreshParams &r,
                           unsigned int *out_count, unsigned int *new_count, cudaStream_t s);
-void launch_refresh_emit(const DevParticles &P, const unsigned int *cell_end, const unsigned int *cell_count,
+template <typename R>
+void launch_refresh_emit(const DevParticlesT<R> &P, const unsigned int *cell_end, const unsigned int *cell_count,
                          int cells, const int *desired_e, const int *desired_h, const RefreshParams &r,
                          const unsigned int *out_offset, const unsigned int *uid_offset, uint32_t uid0,
-                         const DevParticles &dst, unsigned long long *mr_gen, cudaStream_t s);
+                         const DevParticlesT<R> &dst, unsigned long long *mr_gen, cudaStream_t s);
 
 }  // namespace mcb200

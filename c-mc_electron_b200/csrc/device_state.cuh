@@ -25,17 +25,32 @@ enum MotionRule : int { kPass = 1, kReflect = 2, kScattOx = 3, kPeriod = 4, kGen
 enum Dir : int { kUp = 0, kDown = 1, kLeft = 2, kRight = 3, kFront = 4, kBack = 5 };
 
 // Full-band tables in device memory.  Per-tetrahedron data the free flight
-// touches on every event is packed into one 160-byte record so a tet's
-// geometry arrives in two 128-byte lines from L2 (the whole table, ~9 MB,
-// stays L2-resident on B200).
-struct TetFlight {
-  double n[4][4];  // face f: inward normal (n[f][0..2]) and offset n[f][3]
-  double v[4];     // group velocity (v[0..2]) and base energy v[3]
+// touches on every event is packed into one record so a tet's geometry
+// arrives in whole 32-byte sectors from L2 (the table stays L2-resident on
+// B200: 160 B x 55320 tets = 8.9 MB in FP64, half that in FP32).  R is the
+// arithmetic type of the flight kinematics: double for the plain path,
+// float for the FP32-flight path.
+template <typename R>
+struct TetFlightT {
+  R n[4][4];  // face f: inward normal (n[f][0..2]) and offset n[f][3]
+  R v[4];     // group velocity (v[0..2]) and base energy v[3]
 };
-struct TetShape {
-  double e[4];     // node energies, ascending
-  double fac[3];   // FASTSURF coefficients (low, medium, high)
-  double vgt;      // |v|
+template <typename R>
+struct TetShapeT {
+  R e[4];     // node energies, ascending
+  R fac[3];   // FASTSURF coefficients (low, medium, high)
+  R vgt;      // |v|
+};
+using TetFlight = TetFlightT<double>;
+using TetShape = TetShapeT<double>;
+
+// FP32 copies of the tables the FP32 flight reads (built from the FP64
+// tables by rounding each entry once).
+struct DevTables32 {
+  const TetFlightT<float> *tf;
+  const TetShapeT<float> *ts;
+  const float4 *knode;
+  const float *gamtet, *energy, *sumscatt, *scatte, *dose, *scattiie, *scatth, *dosh, *scattiih, *dostetmax;
 };
 
 struct DevTables {
@@ -86,6 +101,7 @@ struct DevTables {
   const double *bz;           // [3][5][48]  (xbz, ybz, zbz)
   const int *indmat;          // [729]
   const int *reflect_isym;    // [3][48]: isym after mirroring k_x / k_y / k_z
+  DevTables32 f32;            // FP32 flight tables (null until a context selects FP32 flight)
 };
 
 // Mesh in the reference's normalised units; cell (i, j, k) has linear index
@@ -94,6 +110,7 @@ struct DevMesh {
   int nx, ny, nz;               // cells per axis
   const double *lx, *ly, *lz;   // node coordinates [n+1]
   const double *dx, *dy, *dz;   // cell widths [n]
+  const float *dxf, *dyf, *dzf; // cell widths rounded to float (FP32 flight: cell-relative positions)
   const int *motion;            // [cells][6]
   const int *contact;           // [cells] attached contact, 1-based, 0 = none
   const int *in_surf;           // [cells]
@@ -109,16 +126,26 @@ struct DevMesh {
   int heat;                     // flag_heat: phonon events deposit heat
 };
 
-// Particle store: structure of arrays, one entry per particle (80 bytes).
-struct DevParticles {
-  double *x, *y, *z;
-  double *kx, *ky, *kz;
+// Particle store: structure of arrays, one entry per particle.  R = double:
+// absolute positions, 80 bytes per particle.  R = float (FP32 flight):
+// positions relative to the low corner of the particle's cell, 56 bytes.
+// Energy and charge stay FP64 in both.
+template <typename R>
+struct DevParticlesT {
+  R *x, *y, *z;
+  R *kx, *ky, *kz;
   double *energy, *charge;
   uint32_t *cell;       // packed i | j << 10 | k << 20
   int32_t *itet;
   uint32_t *meta;       // isym | type << 8 | flags << 16
   uint32_t *uid;
 };
+using DevParticles = DevParticlesT<double>;
+using DevParticles32 = DevParticlesT<float>;
+
+// Bytes of one particle in the store.
+template <typename R>
+constexpr int particle_bytes() { return 6 * (int)sizeof(R) + 2 * 8 + 4 * 4; }
 
 // Fixed-point scales of the order-independent int64 tallies.
 constexpr double kChargeScale = 1099511627776.0;  // 2^40 per unit normalised charge
@@ -144,12 +171,15 @@ enum TallyCounter : int {
   kCntTooManyEvents = 6,
   kCntChildOverflow = 7,
   kCntNoTet = 8,       // Getisym found no tetrahedron (particle caught)
+  kCntZeroTime = 9,    // FP32 flight: too many consecutive zero-length events (particle caught)
   kCntNumCounters = 16
 };
 
 // A copy made mid-step by GENERATE / GENREF, to be flown for the rest of the step.
-struct DevChildren {
-  double *x, *y, *z, *kx, *ky, *kz, *energy, *charge, *left_time;
+template <typename R>
+struct DevChildrenT {
+  R *x, *y, *z, *kx, *ky, *kz;
+  double *energy, *charge, *left_time;
   uint32_t *cell;
   int32_t *itet;
   uint32_t *meta;
@@ -157,6 +187,7 @@ struct DevChildren {
   unsigned int *count;
   int capacity;
 };
+using DevChildren = DevChildrenT<double>;
 
 inline __host__ __device__ uint32_t pack_cell(int i, int j, int k) {
   return (uint32_t)i | ((uint32_t)j << 10) | ((uint32_t)k << 20);

@@ -21,6 +21,9 @@ namespace {
 struct CudaError : std::runtime_error {
   using std::runtime_error::runtime_error;
 };
+struct CapacityError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
 
 void ck(cudaError_t e, const char *what) {
   if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
@@ -41,30 +44,37 @@ T *dupload(const std::vector<T> &v, std::vector<void *> &owned) {
   return p;
 }
 
-struct ParticleBuffers {
-  DevParticles d{};
-  void alloc(size_t cap, std::vector<void *> &owned) {
-    d.x = dalloc<double>(cap, owned); d.y = dalloc<double>(cap, owned); d.z = dalloc<double>(cap, owned);
-    d.kx = dalloc<double>(cap, owned); d.ky = dalloc<double>(cap, owned); d.kz = dalloc<double>(cap, owned);
-    d.energy = dalloc<double>(cap, owned); d.charge = dalloc<double>(cap, owned);
-    d.cell = dalloc<uint32_t>(cap, owned); d.itet = dalloc<int32_t>(cap, owned);
-    d.meta = dalloc<uint32_t>(cap, owned); d.uid = dalloc<uint32_t>(cap, owned);
-  }
-};
+template <typename R>
+void alloc_particles(DevParticlesT<R> &d, size_t cap, std::vector<void *> &owned) {
+  d.x = dalloc<R>(cap, owned); d.y = dalloc<R>(cap, owned); d.z = dalloc<R>(cap, owned);
+  d.kx = dalloc<R>(cap, owned); d.ky = dalloc<R>(cap, owned); d.kz = dalloc<R>(cap, owned);
+  d.energy = dalloc<double>(cap, owned); d.charge = dalloc<double>(cap, owned);
+  d.cell = dalloc<uint32_t>(cap, owned); d.itet = dalloc<int32_t>(cap, owned);
+  d.meta = dalloc<uint32_t>(cap, owned); d.uid = dalloc<uint32_t>(cap, owned);
+}
 
+template <typename R>
+void alloc_children(DevChildrenT<R> &d, int cap, std::vector<void *> &owned) {
+  d.x = dalloc<R>(cap, owned); d.y = dalloc<R>(cap, owned); d.z = dalloc<R>(cap, owned);
+  d.kx = dalloc<R>(cap, owned); d.ky = dalloc<R>(cap, owned); d.kz = dalloc<R>(cap, owned);
+  d.energy = dalloc<double>(cap, owned); d.charge = dalloc<double>(cap, owned);
+  d.left_time = dalloc<double>(cap, owned);
+  d.cell = dalloc<uint32_t>(cap, owned); d.itet = dalloc<int32_t>(cap, owned);
+  d.meta = dalloc<uint32_t>(cap, owned);
+  d.parent_uid = dalloc<uint32_t>(cap, owned); d.sub = dalloc<uint32_t>(cap, owned);
+  d.count = dalloc<unsigned int>(1, owned);
+  d.capacity = cap;
+}
+
+// One particle buffer / one child generation, in the context's flight
+// precision (only the matching member is allocated).
+struct ParticleBuffers {
+  DevParticlesT<double> d{};
+  DevParticlesT<float> f{};
+};
 struct ChildBuffers {
-  DevChildren d{};
-  void alloc(int cap, std::vector<void *> &owned) {
-    d.x = dalloc<double>(cap, owned); d.y = dalloc<double>(cap, owned); d.z = dalloc<double>(cap, owned);
-    d.kx = dalloc<double>(cap, owned); d.ky = dalloc<double>(cap, owned); d.kz = dalloc<double>(cap, owned);
-    d.energy = dalloc<double>(cap, owned); d.charge = dalloc<double>(cap, owned);
-    d.left_time = dalloc<double>(cap, owned);
-    d.cell = dalloc<uint32_t>(cap, owned); d.itet = dalloc<int32_t>(cap, owned);
-    d.meta = dalloc<uint32_t>(cap, owned);
-    d.parent_uid = dalloc<uint32_t>(cap, owned); d.sub = dalloc<uint32_t>(cap, owned);
-    d.count = dalloc<unsigned int>(1, owned);
-    d.capacity = cap;
-  }
+  DevChildrenT<double> d{};
+  DevChildrenT<float> f{};
 };
 
 }  // namespace
@@ -81,6 +91,8 @@ struct mcb200_ctx {
   bool mesh_set = false, cells_set = false, fields_set = false;
   std::vector<double> hlx, hly, hlz;
   // particles: two buffers, the store ping-pongs through the cell sort
+  int precision = MCB200_FLIGHT_FP64;
+  std::vector<void *> store_owned;  // particle and child buffers (reallocated on a precision change)
   size_t capacity = 0;
   ParticleBuffers pb[2];
   int cur = 0;
@@ -117,6 +129,7 @@ struct mcb200_ctx {
     for (cudaEvent_t e : ev)
       if (e) cudaEventDestroy(e);
     for (void *p : mesh_owned) cudaFree(p);
+    for (void *p : store_owned) cudaFree(p);
     for (void *p : owned) cudaFree(p);
     if (h_pinned) cudaFreeHost(h_pinned);
     if (h_scratch) cudaFreeHost(h_scratch);
@@ -129,6 +142,33 @@ namespace {
 int fail(mcb200_ctx *c, int code, const std::string &msg) {
   if (c) c->error = msg;
   return code;
+}
+
+template <typename R>
+DevParticlesT<R> &store(mcb200_ctx *c, int i) {
+  if constexpr (sizeof(R) == 8) return c->pb[i].d;
+  else return c->pb[i].f;
+}
+template <typename R>
+DevChildrenT<R> &children(mcb200_ctx *c, int g) {
+  if constexpr (sizeof(R) == 8) return c->cb[g].d;
+  else return c->cb[g].f;
+}
+
+// Particle and child buffers for the context's precision.
+void alloc_stores(mcb200_ctx *c) {
+  for (void *p : c->store_owned) cudaFree(p);
+  c->store_owned.clear();
+  for (int i = 0; i < 2; ++i) c->pb[i] = ParticleBuffers{};
+  for (int g = 0; g < mcb200_ctx::kGenerations; ++g) c->cb[g] = ChildBuffers{};
+  for (int i = 0; i < 2; ++i) {
+    if (c->precision == MCB200_FLIGHT_FP32) alloc_particles(c->pb[i].f, c->capacity, c->store_owned);
+    else alloc_particles(c->pb[i].d, c->capacity, c->store_owned);
+  }
+  for (int g = 0; g < mcb200_ctx::kGenerations; ++g) {
+    if (c->precision == MCB200_FLIGHT_FP32) alloc_children(c->cb[g].f, c->child_cap, c->store_owned);
+    else alloc_children(c->cb[g].d, c->child_cap, c->store_owned);
+  }
 }
 
 // Uniform k-space locator for the tetrahedron search (see flight_physics.cuh).
@@ -212,6 +252,50 @@ void build_kgrid(mcb200_ctx *c, int g) {
   c->dt.seed_grid = dupload(seed, c->owned);
 }
 
+template <typename T>
+std::vector<float> to_float(const std::vector<T> &v) {
+  return std::vector<float>(v.begin(), v.end());
+}
+
+// FP32 copies of the flight tables.  Face planes are scaled to unit normals
+// (the sign of every face test and every drift-time ratio is unchanged), so
+// the FP32 containment tolerance is a k-space distance.
+void upload_tables32(mcb200_ctx *c, const std::vector<TetFlight> &tf, const std::vector<TetShape> &ts,
+                     const std::vector<double4> &kn) {
+  const FullBandTables &t = c->tab;
+  DevTables32 &d = c->dt.f32;
+  std::vector<TetFlightT<float>> tf32(tf.size());
+  std::vector<TetShapeT<float>> ts32(ts.size());
+  for (size_t it = 0; it < tf.size(); ++it) {
+    for (int f = 0; f < 4; ++f) {
+      const double *n = tf[it].n[f];
+      const double len = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+      const double sc = len > 0 ? 1.0 / len : 1.0;
+      for (int cc = 0; cc < 4; ++cc) tf32[it].n[f][cc] = (float)(n[cc] * sc);
+    }
+    for (int cc = 0; cc < 4; ++cc) tf32[it].v[cc] = (float)tf[it].v[cc];
+    for (int v = 0; v < 4; ++v) ts32[it].e[v] = (float)ts[it].e[v];
+    for (int v = 0; v < 3; ++v) ts32[it].fac[v] = (float)ts[it].fac[v];
+    ts32[it].vgt = (float)ts[it].vgt;
+  }
+  std::vector<float4> kn32(kn.size());
+  for (size_t i = 0; i < kn.size(); ++i)
+    kn32[i] = make_float4((float)kn[i].x, (float)kn[i].y, (float)kn[i].z, (float)kn[i].w);
+  d.tf = dupload(tf32, c->owned);
+  d.ts = dupload(ts32, c->owned);
+  d.knode = dupload(kn32, c->owned);
+  d.gamtet = dupload(to_float(t.gamtet), c->owned);
+  d.energy = dupload(to_float(t.energy), c->owned);
+  d.sumscatt = dupload(to_float(t.sumscatt), c->owned);
+  d.scatte = dupload(to_float(t.scatte), c->owned);
+  d.dose = dupload(to_float(t.dose), c->owned);
+  d.scattiie = dupload(to_float(t.scattiie), c->owned);
+  d.scatth = dupload(to_float(t.scatth), c->owned);
+  d.dosh = dupload(to_float(t.dosh), c->owned);
+  d.scattiih = dupload(to_float(t.scattiih), c->owned);
+  d.dostetmax = dupload(to_float(t.dostetmax), c->owned);
+}
+
 void upload_tables(mcb200_ctx *c) {
   const FullBandTables &t = c->tab;
   DevTables &d = c->dt;
@@ -288,6 +372,7 @@ void upload_tables(mcb200_ctx *c) {
   d.indmat = dupload(indmat, c->owned);
   d.reflect_isym = dupload(refl, c->owned);
   build_kgrid(c, 40);
+  upload_tables32(c, tf, ts, kn);
 }
 
 template <typename T>
@@ -306,6 +391,68 @@ void free_mesh(mcb200_ctx *c) {
   for (void *p : c->mesh_owned) cudaFree(p);
   c->mesh_owned.clear();
 }
+
+// Host particles (absolute FP64 positions) into store 0 of precision R;
+// an FP32 store keeps positions relative to the cell's low corner.
+template <typename R>
+void upload_store(mcb200_ctx *c, size_t n, const mcb200_particles *p, const std::vector<uint32_t> &cell,
+                  const std::vector<uint32_t> &meta) {
+  const DevParticlesT<R> &d = store<R>(c, 0);
+  auto put = [&](void *dst, const void *src, size_t sz) {
+    ck(cudaMemcpyAsync(dst, src, n * sz, cudaMemcpyHostToDevice, c->stream), "upload particles");
+  };
+  std::vector<float> h[6];
+  if constexpr (sizeof(R) == 8) {
+    put(d.x, p->x, 8); put(d.y, p->y, 8); put(d.z, p->z, 8);
+    put(d.kx, p->kx, 8); put(d.ky, p->ky, 8); put(d.kz, p->kz, 8);
+  } else {
+    for (auto &v : h) v.resize(n);
+    for (size_t q = 0; q < n; ++q) {
+      h[0][q] = (float)(p->x[q] - c->hlx[p->i[q]]);
+      h[1][q] = (float)(p->y[q] - c->hly[p->j[q]]);
+      h[2][q] = (float)(p->z[q] - c->hlz[p->k[q]]);
+      h[3][q] = (float)p->kx[q]; h[4][q] = (float)p->ky[q]; h[5][q] = (float)p->kz[q];
+    }
+    put(d.x, h[0].data(), 4); put(d.y, h[1].data(), 4); put(d.z, h[2].data(), 4);
+    put(d.kx, h[3].data(), 4); put(d.ky, h[4].data(), 4); put(d.kz, h[5].data(), 4);
+  }
+  put(d.energy, p->energy, 8); put(d.charge, p->charge, 8);
+  put(d.cell, cell.data(), 4); put(d.itet, p->itet, 4); put(d.meta, meta.data(), 4); put(d.uid, p->uid, 4);
+  ck(cudaStreamSynchronize(c->stream), "sync");
+}
+
+// The current store back to host particles (absolute FP64 positions).
+template <typename R>
+void download_store(mcb200_ctx *c, size_t n, mcb200_particles *p, std::vector<uint32_t> &cell,
+                    std::vector<uint32_t> &meta) {
+  const DevParticlesT<R> &d = store<R>(c, c->cur);
+  auto get = [&](void *dst, const void *src, size_t sz) {
+    ck(cudaMemcpyAsync(dst, src, n * sz, cudaMemcpyDeviceToHost, c->stream), "download particles");
+  };
+  std::vector<float> h[6];
+  if constexpr (sizeof(R) == 8) {
+    get(p->x, d.x, 8); get(p->y, d.y, 8); get(p->z, d.z, 8);
+    get(p->kx, d.kx, 8); get(p->ky, d.ky, 8); get(p->kz, d.kz, 8);
+  } else {
+    for (auto &v : h) v.resize(n);
+    get(h[0].data(), d.x, 4); get(h[1].data(), d.y, 4); get(h[2].data(), d.z, 4);
+    get(h[3].data(), d.kx, 4); get(h[4].data(), d.ky, 4); get(h[5].data(), d.kz, 4);
+  }
+  get(p->energy, d.energy, 8); get(p->charge, d.charge, 8);
+  get(cell.data(), d.cell, 4); get(p->itet, d.itet, 4); get(meta.data(), d.meta, 4); get(p->uid, d.uid, 4);
+  ck(cudaStreamSynchronize(c->stream), "sync");
+  if constexpr (sizeof(R) == 4) {
+    for (size_t q = 0; q < n; ++q) {
+      p->x[q] = c->hlx[cell[q] & 1023] + (double)h[0][q];
+      p->y[q] = c->hly[(cell[q] >> 10) & 1023] + (double)h[1][q];
+      p->z[q] = c->hlz[(cell[q] >> 20) & 1023] + (double)h[2][q];
+      p->kx[q] = h[3][q]; p->ky[q] = h[4][q]; p->kz[q] = h[5][q];
+    }
+  }
+}
+
+template <typename R>
+void step_impl(mcb200_ctx *c, uint32_t step, uint64_t seed, double dt);
 
 }  // namespace
 
@@ -334,10 +481,8 @@ int mcb200_create(const char *table_dir, double kelvin, int device, size_t max_p
     ck(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device), "device attribute");
     upload_tables(c);
     c->capacity = max_particles;
-    c->pb[0].alloc(max_particles, c->owned);
-    c->pb[1].alloc(max_particles, c->owned);
     c->child_cap = (int)std::min<size_t>(std::max<size_t>(max_particles / 8, 4096), 1u << 22);
-    for (int g = 0; g < mcb200_ctx::kGenerations; ++g) c->cb[g].alloc(c->child_cap, c->owned);
+    alloc_stores(c);
     const size_t all_children = (size_t)c->child_cap * mcb200_ctx::kGenerations;
     c->child_keys = dalloc<uint64_t>(all_children, c->owned);
     c->child_alive = dalloc<uint8_t>(all_children, c->owned);
@@ -360,6 +505,25 @@ int mcb200_create(const char *table_dir, double kelvin, int device, size_t max_p
 }
 
 void mcb200_destroy(mcb200_ctx *ctx) { delete ctx; }
+
+int mcb200_set_flight_precision(mcb200_ctx *c, int precision) {
+  if (!c || (precision != MCB200_FLIGHT_FP64 && precision != MCB200_FLIGHT_FP32)) return MCB200_ERR_ARG;
+  if (c->device < 0) return fail(c, MCB200_ERR_STATE, "host-only context");
+  if (c->n != 0) return fail(c, MCB200_ERR_STATE, "flight precision can only change while the store is empty");
+  if (precision == c->precision) return MCB200_OK;
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    ck(cudaStreamSynchronize(c->stream), "sync");
+    c->precision = precision;
+    c->cur = 0;
+    alloc_stores(c);
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_get_flight_precision(const mcb200_ctx *c) { return c ? c->precision : -1; }
 
 const char *mcb200_last_error(const mcb200_ctx *ctx) { return ctx ? ctx->error.c_str() : "null context"; }
 
@@ -442,6 +606,9 @@ int mcb200_set_mesh(mcb200_ctx *c, int nx, int ny, int nz, const double *lx, con
     m.nx = nx; m.ny = ny; m.nz = nz;
     m.lx = dupload(c->hlx, c->mesh_owned); m.ly = dupload(c->hly, c->mesh_owned); m.lz = dupload(c->hlz, c->mesh_owned);
     m.dx = dupload(dx, c->mesh_owned); m.dy = dupload(dy, c->mesh_owned); m.dz = dupload(dz, c->mesh_owned);
+    m.dxf = dupload(to_float(dx), c->mesh_owned);
+    m.dyf = dupload(to_float(dy), c->mesh_owned);
+    m.dzf = dupload(to_float(dz), c->mesh_owned);
     const size_t cells = (size_t)nx * ny * nz, nodes = (size_t)(nx + 1) * (ny + 1) * (nz + 1);
     c->ncells = (int)cells;
     m.motion = dalloc<int>(cells * 6, c->mesh_owned);
@@ -560,15 +727,9 @@ int mcb200_upload_particles(mcb200_ctx *c, size_t n, const mcb200_particles *p) 
       meta[q] = (uint32_t)p->isym[q] | ((uint32_t)p->type[q] << 8);
       maxuid = std::max(maxuid, p->uid[q] + 1);
     }
-    const DevParticles &d = c->pb[0].d;
     c->cur = 0;
-    auto put = [&](void *dst, const void *src, size_t sz) {
-      ck(cudaMemcpyAsync(dst, src, n * sz, cudaMemcpyHostToDevice, c->stream), "upload particles");
-    };
-    put(d.x, p->x, 8); put(d.y, p->y, 8); put(d.z, p->z, 8);
-    put(d.kx, p->kx, 8); put(d.ky, p->ky, 8); put(d.kz, p->kz, 8);
-    put(d.energy, p->energy, 8); put(d.charge, p->charge, 8);
-    put(d.cell, cell.data(), 4); put(d.itet, p->itet, 4); put(d.meta, meta.data(), 4); put(d.uid, p->uid, 4);
+    if (c->precision == MCB200_FLIGHT_FP32) upload_store<float>(c, n, p, cell, meta);
+    else upload_store<double>(c, n, p, cell, meta);
     ck(cudaStreamSynchronize(c->stream), "sync");
     c->n = n;
     c->next_uid = maxuid;
@@ -586,15 +747,8 @@ int mcb200_download_particles(mcb200_ctx *c, mcb200_particles *p, size_t capacit
     ck(cudaSetDevice(c->device), "cudaSetDevice");
     const size_t n = c->n;
     std::vector<uint32_t> cell(n), meta(n);
-    const DevParticles &d = c->pb[c->cur].d;
-    auto get = [&](void *dst, const void *src, size_t sz) {
-      ck(cudaMemcpyAsync(dst, src, n * sz, cudaMemcpyDeviceToHost, c->stream), "download particles");
-    };
-    get(p->x, d.x, 8); get(p->y, d.y, 8); get(p->z, d.z, 8);
-    get(p->kx, d.kx, 8); get(p->ky, d.ky, 8); get(p->kz, d.kz, 8);
-    get(p->energy, d.energy, 8); get(p->charge, d.charge, 8);
-    get(cell.data(), d.cell, 4); get(p->itet, d.itet, 4); get(meta.data(), d.meta, 4); get(p->uid, d.uid, 4);
-    ck(cudaStreamSynchronize(c->stream), "sync");
+    if (c->precision == MCB200_FLIGHT_FP32) download_store<float>(c, n, p, cell, meta);
+    else download_store<double>(c, n, p, cell, meta);
     for (size_t q = 0; q < n; ++q) {
       p->i[q] = cell[q] & 1023;
       p->j[q] = (cell[q] >> 10) & 1023;
@@ -629,12 +783,16 @@ int mcb200_seed_particles(mcb200_ctx *c, size_t n, const int32_t *cell_of, const
     F.T = c->dt;
     F.M = c->mesh;
     F.Y = c->y;
-    F.C = c->cb[0].d;
-    F.C.capacity = 0;
+    F.C = DevChildren{};
     F.dt = 0;
     F.seed = seed;
     F.step = kSeedStreamStep;
-    launch_seed(F, c->pb[c->cur].d, (int)c->n, (int)n, dcell, dq, type, c->next_uid, grid_for(c, n, 256), c->stream);
+    if (c->precision == MCB200_FLIGHT_FP32)
+      launch_seed(F, store<float>(c, c->cur), (int)c->n, (int)n, dcell, dq, type, c->next_uid, grid_for(c, n, 256),
+                  c->stream);
+    else
+      launch_seed(F, store<double>(c, c->cur), (int)c->n, (int)n, dcell, dq, type, c->next_uid, grid_for(c, n, 256),
+                  c->stream);
     ck(cudaGetLastError(), "seed kernel");
     ck(cudaStreamSynchronize(c->stream), "sync");
     for (void *p : tmp) cudaFree(p);
@@ -652,91 +810,11 @@ int mcb200_step(mcb200_ctx *c, uint32_t step, uint64_t seed, double dt) {
     return fail(c, MCB200_ERR_STATE, "mcb200_step needs mesh, cells and fields");
   try {
     ck(cudaSetDevice(c->device), "cudaSetDevice");
-    cudaStream_t s = c->stream;
-    FlightCtx F;
-    F.T = c->dt;
-    F.M = c->mesh;
-    F.Y = c->y;
-    F.dt = dt;
-    F.seed = seed;
-    F.step = step;
-    const int block = 256;
-    if (c->timing) ck(cudaEventRecord(c->ev[0], s), "event");
-    // 1. main flight; copies go to generation 0
-    ck(cudaMemsetAsync(c->cb[0].d.count, 0, sizeof(unsigned int), s), "memset");
-    F.C = c->cb[0].d;
-    if (c->timing) ck(cudaEventRecord(c->ev[1], s), "event");
-    launch_flight(F, c->pb[c->cur].d, (int)c->n, grid_for(c, c->n, block), block, s);
-    ck(cudaGetLastError(), "flight kernel");
-    if (c->timing) ck(cudaEventRecord(c->ev[2], s), "event");
-    const size_t flown = c->n;
-    c->launches += c->n > 0 ? 1 : 0;
-    // 2. copies fly the rest of the step, generation by generation
-    unsigned int counts[mcb200_ctx::kGenerations] = {0, 0, 0, 0};
-    int gens = 0;
-    for (int g = 0; g < mcb200_ctx::kGenerations; ++g) {
-      ck(cudaMemcpyAsync(c->h_pinned, c->cb[g].d.count, sizeof(unsigned int), cudaMemcpyDeviceToHost, s), "count");
-      ck(cudaStreamSynchronize(s), "sync");
-      counts[g] = std::min<unsigned int>(c->h_pinned[0], (unsigned int)c->child_cap);
-      if (counts[g] == 0) break;
-      gens = g + 1;
-      if (g + 1 < mcb200_ctx::kGenerations) {
-        ck(cudaMemsetAsync(c->cb[g + 1].d.count, 0, sizeof(unsigned int), s), "memset");
-        F.C = c->cb[g + 1].d;
-      } else {
-        F.C = c->cb[g].d;  // a fifth generation would overflow: counted, not flown
-        F.C.capacity = 0;
-      }
-      launch_child_flight(F, c->cb[g].d, grid_for(c, counts[g], block), block, s);
-      ck(cudaGetLastError(), "child flight kernel");
-      c->launches += 1;
-    }
-    // 3. uids for surviving copies, then append them to the store
-    size_t total_children = 0;
-    for (int g = 0; g < gens; ++g) {
-      launch_child_keys(c->cb[g].d, counts[g], c->child_keys + total_children, c->child_alive + total_children, s);
-      total_children += counts[g];
-    }
-    size_t n_all = c->n;
-    if (total_children > 0) {
-      if (c->n + total_children > c->capacity) return fail(c, MCB200_ERR_CAPACITY, "particle store full after GENERATE");
-      launch_child_rank(c->child_keys, c->child_alive, (int)total_children, c->next_uid, c->child_uids, s);
-      ck(cudaMemsetAsync(c->append_count, 0, sizeof(unsigned int), s), "memset");
-      size_t off = 0;
-      for (int g = 0; g < gens; ++g) {
-        launch_children_to_particles(c->cb[g].d, counts[g], c->child_uids + off, c->child_alive + off,
-                                     c->pb[c->cur].d, (int)c->n, c->append_count, s);
-        off += counts[g];
-      }
-      ck(cudaMemcpyAsync(c->h_pinned, c->append_count, sizeof(unsigned int), cudaMemcpyDeviceToHost, s), "count");
-      ck(cudaStreamSynchronize(s), "sync");
-      const unsigned int appended = c->h_pinned[0];
-      n_all = c->n + appended;
-      c->next_uid += appended;
-      c->launches += 2 * gens + 1;
-    }
-    // 4. drop caught particles and counting-sort the store by cell
-    const int other = 1 - c->cur;
-    launch_cell_sort(c->pb[c->cur].d, (int)n_all, c->pb[other].d, c->ncells, c->mesh.nx, c->mesh.nz, c->hist,
-                     c->offsets, c->tile_sums, c->total, grid_for(c, n_all, 256), s);
-    ck(cudaGetLastError(), "cell sort");
-    c->launches += n_all > 0 ? 5 : 3;
-    ck(cudaMemcpyAsync(c->h_pinned, c->total, sizeof(unsigned int), cudaMemcpyDeviceToHost, s), "count");
-    if (c->timing) ck(cudaEventRecord(c->ev[3], s), "event");
-    ck(cudaStreamSynchronize(s), "sync");
-    c->n = c->h_pinned[0];
-    c->cur = other;
-    if (c->timing) {
-      float ms_flight = 0, ms_step = 0;
-      ck(cudaEventElapsedTime(&ms_flight, c->ev[1], c->ev[2]), "elapsed");
-      ck(cudaEventElapsedTime(&ms_step, c->ev[0], c->ev[3]), "elapsed");
-      c->flight_ms += ms_flight;
-      c->step_ms += ms_step;
-      c->flight_launches += flown > 0 ? 1 : 0;
-      c->particles_flown += flown;
-      c->steps += 1;
-    }
+    if (c->precision == MCB200_FLIGHT_FP32) step_impl<float>(c, step, seed, dt);
+    else step_impl<double>(c, step, seed, dt);
     return MCB200_OK;
+  } catch (const CapacityError &e) {
+    return fail(c, MCB200_ERR_CAPACITY, e.what());
   } catch (const std::exception &e) {
     return fail(c, MCB200_ERR_CUDA, e.what());
   }
@@ -897,9 +975,10 @@ int mcb200_deposit(mcb200_ctx *c) {
   try {
     ck(cudaSetDevice(c->device), "cudaSetDevice");
     cudaStream_t s = c->stream;
-    const DevParticles &P = c->pb[c->cur].d;
     const int grid = grid_for(c, c->n, 256);
-    launch_charge_bounds(P, (int)c->n, c->fb.abs_sum, grid, s);
+    const bool fp32 = c->precision == MCB200_FLIGHT_FP32;
+    if (fp32) launch_charge_bounds(store<float>(c, c->cur), (int)c->n, c->fb.abs_sum, grid, s);
+    else launch_charge_bounds(store<double>(c, c->cur), (int)c->n, c->fb.abs_sum, grid, s);
     ck(cudaMemcpyAsync(c->h_scratch, c->fb.abs_sum, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
        "copy");
     ck(cudaStreamSynchronize(s), "sync");
@@ -914,7 +993,8 @@ int mcb200_deposit(mcb200_ctx *c) {
     };
     const double be = (double)b[2] * qmax[0], bh = (double)b[3] * qmax[1];
     const DepositScales S{{unit(be), unit(bh), unit(be + bh)}};
-    launch_deposit(P, (int)c->n, c->mesh, c->fb, S, grid, s);
+    if (fp32) launch_deposit(store<float>(c, c->cur), (int)c->n, c->mesh, c->fb, S, grid, s);
+    else launch_deposit(store<double>(c, c->cur), (int)c->n, c->mesh, c->fb, S, grid, s);
     ck(cudaGetLastError(), "deposit");
     ck(cudaStreamSynchronize(s), "sync");
     c->fields_set = true;
@@ -996,15 +1076,20 @@ int mcb200_multiple_refresh(mcb200_ctx *c, const int32_t *desired_e, const int32
     // group the store by cell into the other buffer (hist = counts, offsets =
     // cell ends); the refreshed population then goes back to this buffer
     const int sorted = 1 - c->cur, other = c->cur;
-    launch_cell_sort(c->pb[c->cur].d, (int)c->n, c->pb[sorted].d, cells, c->mesh.nx, c->mesh.nz, c->hist,
-                     c->offsets, c->tile_sums, c->total, grid_for(c, c->n, 256), s);
     const RefreshParams r{seed, step, 2.0, 2.0, 1.0e-30};  // Rpar, Rsqr, pckill: src/mcmodel.cpp:3878-3880
-    const DevParticles &P = c->pb[sorted].d;
-    launch_refresh_count(P, c->offsets, c->hist, cells, de, dh, r, out_count, new_count, s);
-    launch_exclusive_scan(out_count, out_off, tiles, tot, cells, s);
-    launch_exclusive_scan(new_count, uid_off, tiles, tot + 1, cells, s);
-    launch_refresh_emit(P, c->offsets, c->hist, cells, de, dh, r, out_off, uid_off, c->next_uid, c->pb[other].d, gen,
-                        s);
+    auto refresh = [&](auto tag) {
+      using R = decltype(tag);
+      launch_cell_sort(store<R>(c, c->cur), (int)c->n, store<R>(c, sorted), cells, c->mesh.nx, c->mesh.nz, c->hist,
+                       c->offsets, c->tile_sums, c->total, grid_for(c, c->n, 256), s);
+      const DevParticlesT<R> &P = store<R>(c, sorted);
+      launch_refresh_count(P, c->offsets, c->hist, cells, de, dh, r, out_count, new_count, s);
+      launch_exclusive_scan(out_count, out_off, tiles, tot, cells, s);
+      launch_exclusive_scan(new_count, uid_off, tiles, tot + 1, cells, s);
+      launch_refresh_emit(P, c->offsets, c->hist, cells, de, dh, r, out_off, uid_off, c->next_uid, store<R>(c, other),
+                          gen, s);
+    };
+    if (c->precision == MCB200_FLIGHT_FP32) refresh(float{});
+    else refresh(double{});
     ck(cudaGetLastError(), "refresh");
     unsigned int totals[2];
     long long g = 0;
@@ -1059,3 +1144,98 @@ int mcb200_get_array(mcb200_ctx *c, const char *name, double *out, size_t n) {
 }
 
 }  // extern "C"
+
+namespace {
+
+// One step of the store in precision R: main flight, mid-step copies
+// generation by generation, uids and append, then removal of caught
+// particles and the counting sort by cell.
+template <typename R>
+void step_impl(mcb200_ctx *c, uint32_t step, uint64_t seed, double dt) {
+  cudaStream_t s = c->stream;
+  FlightCtxT<R> F;
+  F.T = c->dt;
+  F.M = c->mesh;
+  F.Y = c->y;
+  F.dt = dt;
+  F.seed = seed;
+  F.step = step;
+  const int block = 256;
+  if (c->timing) ck(cudaEventRecord(c->ev[0], s), "event");
+  // 1. main flight; copies go to generation 0
+  ck(cudaMemsetAsync(children<R>(c, 0).count, 0, sizeof(unsigned int), s), "memset");
+  F.C = children<R>(c, 0);
+  if (c->timing) ck(cudaEventRecord(c->ev[1], s), "event");
+  launch_flight(F, store<R>(c, c->cur), (int)c->n, grid_for(c, c->n, block), block, s);
+  ck(cudaGetLastError(), "flight kernel");
+  if (c->timing) ck(cudaEventRecord(c->ev[2], s), "event");
+  const size_t flown = c->n;
+  c->launches += c->n > 0 ? 1 : 0;
+  // 2. copies fly the rest of the step, generation by generation
+  unsigned int counts[mcb200_ctx::kGenerations] = {0, 0, 0, 0};
+  int gens = 0;
+  for (int g = 0; g < mcb200_ctx::kGenerations; ++g) {
+    ck(cudaMemcpyAsync(c->h_pinned, children<R>(c, g).count, sizeof(unsigned int), cudaMemcpyDeviceToHost, s), "count");
+    ck(cudaStreamSynchronize(s), "sync");
+    counts[g] = std::min<unsigned int>(c->h_pinned[0], (unsigned int)c->child_cap);
+    if (counts[g] == 0) break;
+    gens = g + 1;
+    if (g + 1 < mcb200_ctx::kGenerations) {
+      ck(cudaMemsetAsync(children<R>(c, g + 1).count, 0, sizeof(unsigned int), s), "memset");
+      F.C = children<R>(c, g + 1);
+    } else {
+      F.C = children<R>(c, g);  // a fifth generation would overflow: counted, not flown
+      F.C.capacity = 0;
+    }
+    launch_child_flight(F, children<R>(c, g), grid_for(c, counts[g], block), block, s);
+    ck(cudaGetLastError(), "child flight kernel");
+    c->launches += 1;
+  }
+  // 3. uids for surviving copies, then append them to the store
+  size_t total_children = 0;
+  for (int g = 0; g < gens; ++g) {
+    launch_child_keys(children<R>(c, g), counts[g], c->child_keys + total_children, c->child_alive + total_children, s);
+    total_children += counts[g];
+  }
+  size_t n_all = c->n;
+  if (total_children > 0) {
+    if (c->n + total_children > c->capacity) throw CapacityError("particle store full after GENERATE");
+    launch_child_rank(c->child_keys, c->child_alive, (int)total_children, c->next_uid, c->child_uids, s);
+    ck(cudaMemsetAsync(c->append_count, 0, sizeof(unsigned int), s), "memset");
+    size_t off = 0;
+    for (int g = 0; g < gens; ++g) {
+      launch_children_to_particles(children<R>(c, g), counts[g], c->child_uids + off, c->child_alive + off,
+                                   store<R>(c, c->cur), (int)c->n, c->append_count, s);
+      off += counts[g];
+    }
+    ck(cudaMemcpyAsync(c->h_pinned, c->append_count, sizeof(unsigned int), cudaMemcpyDeviceToHost, s), "count");
+    ck(cudaStreamSynchronize(s), "sync");
+    const unsigned int appended = c->h_pinned[0];
+    n_all = c->n + appended;
+    c->next_uid += appended;
+    c->launches += 2 * gens + 1;
+  }
+  // 4. drop caught particles and counting-sort the store by cell
+  const int other = 1 - c->cur;
+  launch_cell_sort(store<R>(c, c->cur), (int)n_all, store<R>(c, other), c->ncells, c->mesh.nx, c->mesh.nz, c->hist,
+                   c->offsets, c->tile_sums, c->total, grid_for(c, n_all, 256), s);
+  ck(cudaGetLastError(), "cell sort");
+  c->launches += n_all > 0 ? 5 : 3;
+  ck(cudaMemcpyAsync(c->h_pinned, c->total, sizeof(unsigned int), cudaMemcpyDeviceToHost, s), "count");
+  if (c->timing) ck(cudaEventRecord(c->ev[3], s), "event");
+  ck(cudaStreamSynchronize(s), "sync");
+  c->n = c->h_pinned[0];
+  c->cur = other;
+  if (c->timing) {
+    float ms_flight = 0, ms_step = 0;
+    ck(cudaEventElapsedTime(&ms_flight, c->ev[1], c->ev[2]), "elapsed");
+    ck(cudaEventElapsedTime(&ms_step, c->ev[0], c->ev[3]), "elapsed");
+    c->flight_ms += ms_flight;
+    c->step_ms += ms_step;
+    c->flight_launches += flown > 0 ? 1 : 0;
+    c->particles_flown += flown;
+    c->steps += 1;
+  }
+}
+
+}  // namespace

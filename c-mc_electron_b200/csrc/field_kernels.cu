@@ -52,7 +52,8 @@ __device__ __forceinline__ void fx_add(long long *p, double v, double scale) {
 }
 
 // scale[0]: electron cell sums, [1]: hole cell sums, [2]: |q| and node sums.
-__global__ void deposit_kernel(DevParticles P, int n, DevMesh M, DepositScales S, long long *cell_e,
+template <typename R>
+__global__ void deposit_kernel(DevParticlesT<R> P, int n, DevMesh M, DepositScales S, long long *cell_e,
                                long long *cell_h, long long *cell_abs, long long *node_q) {
   const int px = M.nx + 1, pz = M.nz + 1;
   const double scale = S.s[2];
@@ -66,9 +67,16 @@ __global__ void deposit_kernel(DevParticles P, int n, DevMesh M, DepositScales S
     if (((meta >> 8) & 255) == 0) fx_add(cell_e + cell, cc, S.s[0]);
     else fx_add(cell_h + cell, cc, S.s[1]);
     fx_add(cell_abs + cell, fabs(cc), scale);
-    const double rx = (P.x[p] - M.lx[i]) / M.dx[i];
-    const double ry = (P.y[p] - M.ly[j]) / M.dy[j];
-    const double rz = (P.z[p] - M.lz[k]) / M.dz[k];
+    double rx, ry, rz;
+    if constexpr (sizeof(R) == 4) {  // FP32 store: positions relative to the cell's low corner
+      rx = (double)P.x[p] / M.dx[i];
+      ry = (double)P.y[p] / M.dy[j];
+      rz = (double)P.z[p] / M.dz[k];
+    } else {
+      rx = (P.x[p] - M.lx[i]) / M.dx[i];
+      ry = (P.y[p] - M.ly[j]) / M.dy[j];
+      rz = (P.z[p] - M.lz[k]) / M.dz[k];
+    }
     auto node = [&](int a, int b, int d) { return node_q + ((size_t)b * px + a) * pz + d; };
     fx_add(node(i, j, k), cc * (1 - ry) * (1 - rx) * (1 - rz), scale);
     fx_add(node(i + 1, j, k), cc * (1 - ry) * rx * (1 - rz), scale);
@@ -265,24 +273,34 @@ __global__ void pot2field_kernel(DevMesh M, const double *pot, double *efield, d
 // ---------------------------------------------------------------------------
 static inline int blocks(long long n, int b) { return (int)((n + b - 1) / b); }
 
-void launch_charge_bounds(const DevParticles &P, int n, unsigned long long *out, int grid, cudaStream_t s) {
+template <typename R>
+void launch_charge_bounds(const DevParticlesT<R> &P, int n, unsigned long long *out, int grid, cudaStream_t s) {
   cudaMemsetAsync(out, 0, 4 * sizeof(unsigned long long), s);
   if (n > 0) charge_bounds_kernel<<<grid, 256, 0, s>>>(P.charge, P.meta, n, out);
 }
 
-void launch_deposit(const DevParticles &P, int n, const DevMesh &M, const FieldBuffers &f, const DepositScales &S,
+template <typename R>
+void launch_deposit(const DevParticlesT<R> &P, int n, const DevMesh &M, const FieldBuffers &f, const DepositScales &S,
                     int grid, cudaStream_t s) {
   const int cells = M.nx * M.ny * M.nz, nodes = (M.nx + 1) * (M.ny + 1) * (M.nz + 1);
   cudaMemsetAsync(f.acc_cell, 0, sizeof(long long) * 3 * (size_t)cells, s);
   cudaMemsetAsync(f.acc_node, 0, sizeof(long long) * (size_t)nodes, s);
   if (n > 0)
-    deposit_kernel<<<grid, 256, 0, s>>>(P, n, M, S, f.acc_cell, f.acc_cell + cells, f.acc_cell + 2 * (size_t)cells,
+    deposit_kernel<R><<<grid, 256, 0, s>>>(P, n, M, S, f.acc_cell, f.acc_cell + cells, f.acc_cell + 2 * (size_t)cells,
                                          f.acc_node);
   deposit_cells_kernel<<<blocks(cells, 256), 256, 0, s>>>(cells, S, f.acc_cell, f.acc_cell + cells,
                                                            f.acc_cell + 2 * (size_t)cells, f.cvol, M.da, f.cell_e,
                                                            f.cell_h, const_cast<double *>(M.rho));
   deposit_nodes_kernel<<<blocks(nodes, 256), 256, 0, s>>>(nodes, S.s[2], f.acc_node, f.pvol, f.density);
 }
+
+template void launch_charge_bounds<double>(const DevParticlesT<double> &, int, unsigned long long *, int,
+                                           cudaStream_t);
+template void launch_charge_bounds<float>(const DevParticlesT<float> &, int, unsigned long long *, int, cudaStream_t);
+template void launch_deposit<double>(const DevParticlesT<double> &, int, const DevMesh &, const FieldBuffers &,
+                                     const DepositScales &, int, cudaStream_t);
+template void launch_deposit<float>(const DevParticlesT<float> &, int, const DevMesh &, const FieldBuffers &,
+                                    const DepositScales &, int, cudaStream_t);
 
 void launch_rhs(int nodes, const FieldBuffers &f, cudaStream_t s) {
   rhs_kernel<<<blocks(nodes, 256), 256, 0, s>>>(nodes, f.density, f.pvol, f.pdop, f.dirichlet, f.bc_vapp, f.vadd,

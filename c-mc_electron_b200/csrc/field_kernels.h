@@ -33,8 +33,10 @@ struct DepositScales {
 };
 
 // out[4] = {max |q| bits of electrons, of holes, electron count, hole count}
-void launch_charge_bounds(const DevParticles &P, int n, unsigned long long *out, int grid, cudaStream_t s);
-void launch_deposit(const DevParticles &P, int n, const DevMesh &M, const FieldBuffers &f, const DepositScales &S,
+template <typename R>
+void launch_charge_bounds(const DevParticlesT<R> &P, int n, unsigned long long *out, int grid, cudaStream_t s);
+template <typename R>
+void launch_deposit(const DevParticlesT<R> &P, int n, const DevMesh &M, const FieldBuffers &f, const DepositScales &S,
                     int grid, cudaStream_t s);
 void launch_rhs(int nodes, const FieldBuffers &f, cudaStream_t s);
 // Returns 0 on success; host_scratch must hold 8 doubles (pinned).

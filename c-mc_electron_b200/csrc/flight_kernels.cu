@@ -20,21 +20,23 @@ namespace mcb200 {
 constexpr uint32_t kMetaDead = 1u << 16;
 constexpr uint32_t kMetaUnfinished = 1u << 17;
 
-__device__ void load_sym(SymSmem &S, const DevTables &T) {
+template <typename R>
+__device__ void load_sym(SymSmemT<R> &S, const DevTables &T) {
   for (int i = threadIdx.x; i < 48 * 6; i += blockDim.x) S.symi[i] = T.symi[i];
   for (int i = threadIdx.x; i < 5 * 48; i += blockDim.x) S.newisym[i] = T.newisym[i];
-  for (int i = threadIdx.x; i < 3 * 5 * 48; i += blockDim.x) S.bz[i] = T.bz[i];
+  for (int i = threadIdx.x; i < 3 * 5 * 48; i += blockDim.x) S.bz[i] = (R)T.bz[i];
   for (int i = threadIdx.x; i < 3 * 48; i += blockDim.x) S.refl[i] = T.reflect_isym[i];
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(256, 2) flight_kernel(FlightCtx F, DevParticles P, int n) {
-  __shared__ SymSmem S;
+template <typename R>
+__global__ void __launch_bounds__(256, 2) flight_kernel(FlightCtxT<R> F, DevParticlesT<R> P, int n) {
+  __shared__ SymSmemT<R> S;
   load_sym(S, F.T);
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
     const uint32_t meta = P.meta[p];
     if (meta & kMetaDead) continue;
-    Flyer f(F, S);
+    FlyerT<R> f(F, S);
     f.x = P.x[p]; f.y = P.y[p]; f.z = P.z[p];
     f.kx = P.kx[p]; f.ky = P.ky[p]; f.kz = P.kz[p];
     f.energy = P.energy[p];
@@ -44,9 +46,7 @@ __global__ void __launch_bounds__(256, 2) flight_kernel(FlightCtx F, DevParticle
     f.itet = P.itet[p];
     f.isym = meta & 255;
     f.type = (meta >> 8) & 255;
-    f.uid = P.uid[p];
-    f.sub = 0;
-    f.n = 0;
+    f.start_stream(P.uid[p], 0);
     f.nchild = 0;
     f.left_time = F.dt;
     const int r = f.fly();
@@ -64,12 +64,13 @@ __global__ void __launch_bounds__(256, 2) flight_kernel(FlightCtx F, DevParticle
 
 // Copies made during the previous pass (buffer `in`) fly the rest of their
 // step; copies they make go to `F.C`.
-__global__ void __launch_bounds__(256, 2) child_flight_kernel(FlightCtx F, DevChildren in) {
-  __shared__ SymSmem S;
+template <typename R>
+__global__ void __launch_bounds__(256, 2) child_flight_kernel(FlightCtxT<R> F, DevChildrenT<R> in) {
+  __shared__ SymSmemT<R> S;
   load_sym(S, F.T);
   const int n = min((int)*in.count, in.capacity);
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
-    Flyer f(F, S);
+    FlyerT<R> f(F, S);
     f.x = in.x[p]; f.y = in.y[p]; f.z = in.z[p];
     f.kx = in.kx[p]; f.ky = in.ky[p]; f.kz = in.kz[p];
     f.energy = in.energy[p];
@@ -79,9 +80,7 @@ __global__ void __launch_bounds__(256, 2) child_flight_kernel(FlightCtx F, DevCh
     f.itet = in.itet[p];
     f.isym = in.meta[p] & 255;
     f.type = (in.meta[p] >> 8) & 255;
-    f.uid = in.parent_uid[p];
-    f.sub = in.sub[p];
-    f.n = 0;
+    f.start_stream(in.parent_uid[p], in.sub[p]);
     f.nchild = 0;
     f.left_time = in.left_time[p];
     const int r = f.fly();
@@ -163,7 +162,8 @@ __global__ void scan_add(unsigned int *out, const unsigned int *tile_sums, int n
   if (i < n) out[i] += tile_sums[blockIdx.x];
 }
 
-__global__ void cell_scatter(DevParticles src, int n, DevParticles dst, unsigned int *cursor, int nx, int nz) {
+template <typename R>
+__global__ void cell_scatter(DevParticlesT<R> src, int n, DevParticlesT<R> dst, unsigned int *cursor, int nx, int nz) {
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
     const uint32_t m = src.meta[p];
     if (m & kMetaDead) continue;
@@ -179,8 +179,9 @@ __global__ void cell_scatter(DevParticles src, int n, DevParticles dst, unsigned
 }
 
 // Append surviving copies (already flown) to the particle store, with uids.
-__global__ void children_to_particles(DevChildren c, int n, const uint32_t *uids, const uint8_t *alive,
-                                      DevParticles dst, int dst_offset, unsigned int *dst_count) {
+template <typename R>
+__global__ void children_to_particles(DevChildrenT<R> c, int n, const uint32_t *uids, const uint8_t *alive,
+                                      DevParticlesT<R> dst, int dst_offset, unsigned int *dst_count) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || !alive[i]) return;
   const unsigned int q = dst_offset + atomicAdd(dst_count, 1u);
@@ -193,7 +194,8 @@ __global__ void children_to_particles(DevChildren c, int n, const uint32_t *uids
   dst.uid[q] = uids[i];
 }
 
-__global__ void child_keys(DevChildren c, int n, uint64_t *keys, uint8_t *alive) {
+template <typename R>
+__global__ void child_keys(DevChildrenT<R> c, int n, uint64_t *keys, uint8_t *alive) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   keys[i] = ((uint64_t)c.parent_uid[i] << 32) | c.sub[i];
@@ -207,8 +209,12 @@ __global__ void child_keys(DevChildren c, int n, uint64_t *keys, uint8_t *alive)
 // (src/mcmodel.cpp:3006-3057): energy from the Boltzmann distribution,
 // accepted against the DOS, band by the DOS share, k uniform on the
 // iso-energy surface.  Draws: stream (seed, uid, kSeedStreamStep, 0).
+// The sampling runs in FP64 for both stores, so an FP32 store starts from
+// the same ensemble as an FP64 one (rounded once, positions made
+// cell-relative).
 
-__global__ void __launch_bounds__(256) seed_kernel(FlightCtx F, DevParticles P, int offset, int n,
+template <typename R>
+__global__ void __launch_bounds__(256) seed_kernel(FlightCtx F, DevParticlesT<R> P, int offset, int n,
                                                    const int *cell_of, const double *charge, int type,
                                                    uint32_t uid0) {
   __shared__ SymSmem S;
@@ -221,9 +227,7 @@ __global__ void __launch_bounds__(256) seed_kernel(FlightCtx F, DevParticles P, 
     const int kc = c % F.M.nz, ic = (c / F.M.nz) % F.M.nx, jc = c / (F.M.nz * F.M.nx);
     f.ic = ic; f.jc = jc; f.kc = kc;
     f.type = type;
-    f.uid = uid0 + q;
-    f.sub = 0;
-    f.n = 0;
+    f.start_stream(uid0 + q, 0);
     double lamda = f.Random();
     f.x = lamda * F.M.lx[ic] + (1 - lamda) * F.M.lx[ic + 1];
     lamda = f.Random();
@@ -252,8 +256,12 @@ __global__ void __launch_bounds__(256) seed_kernel(FlightCtx F, DevParticles P, 
     }
     if (!ok) count(F.Y, kCntNoTet);
     const int o = offset + q;
-    P.x[o] = f.x; P.y[o] = f.y; P.z[o] = f.z;
-    P.kx[o] = f.kx; P.ky[o] = f.ky; P.kz[o] = f.kz;
+    if constexpr (FlightReal<R>::kCellRelative) {
+      P.x[o] = (R)(f.x - F.M.lx[ic]); P.y[o] = (R)(f.y - F.M.ly[jc]); P.z[o] = (R)(f.z - F.M.lz[kc]);
+    } else {
+      P.x[o] = f.x; P.y[o] = f.y; P.z[o] = f.z;
+    }
+    P.kx[o] = (R)f.kx; P.ky[o] = (R)f.ky; P.kz[o] = (R)f.kz;
     P.energy[o] = f.energy;
     P.charge[o] = charge[q];
     P.cell[o] = pack_cell(ic, jc, kc);
@@ -264,26 +272,33 @@ __global__ void __launch_bounds__(256) seed_kernel(FlightCtx F, DevParticles P, 
 }
 
 // ---- host-side launchers ----------------------------------------------------
-void launch_seed(const FlightCtx &F, const DevParticles &P, int offset, int n, const int *cell_of,
+template <typename R>
+void launch_seed(const FlightCtx &F, const DevParticlesT<R> &P, int offset, int n, const int *cell_of,
                  const double *charge, int type, uint32_t uid0, int grid, cudaStream_t s) {
-  if (n > 0) seed_kernel<<<grid, 256, 0, s>>>(F, P, offset, n, cell_of, charge, type, uid0);
+  if (n > 0) seed_kernel<R><<<grid, 256, 0, s>>>(F, P, offset, n, cell_of, charge, type, uid0);
 }
-void launch_flight(const FlightCtx &F, const DevParticles &P, int n, int grid, int block, cudaStream_t s) {
-  if (n > 0) flight_kernel<<<grid, block, 0, s>>>(F, P, n);
+template <typename R>
+void launch_flight(const FlightCtxT<R> &F, const DevParticlesT<R> &P, int n, int grid, int block, cudaStream_t s) {
+  if (n > 0) flight_kernel<R><<<grid, block, 0, s>>>(F, P, n);
 }
-void launch_child_flight(const FlightCtx &F, const DevChildren &in, int grid, int block, cudaStream_t s) {
-  child_flight_kernel<<<grid, block, 0, s>>>(F, in);
+template <typename R>
+void launch_child_flight(const FlightCtxT<R> &F, const DevChildrenT<R> &in, int grid, int block, cudaStream_t s) {
+  child_flight_kernel<R><<<grid, block, 0, s>>>(F, in);
 }
-void launch_child_keys(const DevChildren &c, int n, uint64_t *keys, uint8_t *alive, cudaStream_t s) {
-  if (n > 0) child_keys<<<(n + 255) / 256, 256, 0, s>>>(c, n, keys, alive);
+template <typename R>
+void launch_child_keys(const DevChildrenT<R> &c, int n, uint64_t *keys, uint8_t *alive, cudaStream_t s) {
+  if (n > 0) child_keys<R><<<(n + 255) / 256, 256, 0, s>>>(c, n, keys, alive);
 }
 void launch_child_rank(const uint64_t *keys, const uint8_t *alive, int n, uint32_t next_uid, uint32_t *uid_out,
                        cudaStream_t s) {
   if (n > 0) child_rank_kernel<<<(n + 255) / 256, 256, 0, s>>>(keys, alive, n, next_uid, uid_out);
 }
-void launch_children_to_particles(const DevChildren &c, int n, const uint32_t *uids, const uint8_t *alive,
-                                  const DevParticles &dst, int dst_offset, unsigned int *dst_count, cudaStream_t s) {
-  if (n > 0) children_to_particles<<<(n + 255) / 256, 256, 0, s>>>(c, n, uids, alive, dst, dst_offset, dst_count);
+template <typename R>
+void launch_children_to_particles(const DevChildrenT<R> &c, int n, const uint32_t *uids, const uint8_t *alive,
+                                  const DevParticlesT<R> &dst, int dst_offset, unsigned int *dst_count,
+                                  cudaStream_t s) {
+  if (n > 0)
+    children_to_particles<R><<<(n + 255) / 256, 256, 0, s>>>(c, n, uids, alive, dst, dst_offset, dst_count);
 }
 void launch_exclusive_scan(const unsigned int *in, unsigned int *out, unsigned int *tile_sums, unsigned int *total,
                            int n, cudaStream_t s) {
@@ -292,7 +307,8 @@ void launch_exclusive_scan(const unsigned int *in, unsigned int *out, unsigned i
   scan_tile_sums<<<1, 32, 0, s>>>(tile_sums, tiles, total);
   scan_add<<<tiles, 1024, 0, s>>>(out, tile_sums, n);
 }
-void launch_cell_sort(const DevParticles &src, int n, const DevParticles &dst, int ncells, int nx, int nz,
+template <typename R>
+void launch_cell_sort(const DevParticlesT<R> &src, int n, const DevParticlesT<R> &dst, int ncells, int nx, int nz,
                       unsigned int *hist, unsigned int *offsets, unsigned int *tile_sums, unsigned int *total,
                       int grid, cudaStream_t s) {
   cudaMemsetAsync(hist, 0, sizeof(unsigned int) * ncells, s);
@@ -301,7 +317,23 @@ void launch_cell_sort(const DevParticles &src, int n, const DevParticles &dst, i
   scan_tiles<<<tiles, 1024, 0, s>>>(hist, offsets, tile_sums, ncells);
   scan_tile_sums<<<1, 32, 0, s>>>(tile_sums, tiles, total);
   scan_add<<<tiles, 1024, 0, s>>>(offsets, tile_sums, ncells);
-  if (n > 0) cell_scatter<<<grid, 256, 0, s>>>(src, n, dst, offsets, nx, nz);
+  if (n > 0) cell_scatter<R><<<grid, 256, 0, s>>>(src, n, dst, offsets, nx, nz);
 }
+
+#define MCB200_INSTANTIATE(R)                                                                                   \
+  template void launch_seed<R>(const FlightCtx &, const DevParticlesT<R> &, int, int, const int *,            \
+                               const double *, int, uint32_t, int, cudaStream_t);                             \
+  template void launch_flight<R>(const FlightCtxT<R> &, const DevParticlesT<R> &, int, int, int, cudaStream_t); \
+  template void launch_child_flight<R>(const FlightCtxT<R> &, const DevChildrenT<R> &, int, int, cudaStream_t); \
+  template void launch_child_keys<R>(const DevChildrenT<R> &, int, uint64_t *, uint8_t *, cudaStream_t);       \
+  template void launch_children_to_particles<R>(const DevChildrenT<R> &, int, const uint32_t *,               \
+                                                const uint8_t *, const DevParticlesT<R> &, int,                 \
+                                                unsigned int *, cudaStream_t);                                  \
+  template void launch_cell_sort<R>(const DevParticlesT<R> &, int, const DevParticlesT<R> &, int, int, int,    \
+                                    unsigned int *, unsigned int *, unsigned int *, unsigned int *, int,        \
+                                    cudaStream_t);
+MCB200_INSTANTIATE(double)
+MCB200_INSTANTIATE(float)
+#undef MCB200_INSTANTIATE
 
 }  // namespace mcb200

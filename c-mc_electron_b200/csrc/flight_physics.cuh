@@ -17,6 +17,14 @@
 //    TOO_MANY_LOOPS (src/mcmodel.cpp:2156);
 //  * surface-phonon mechanism choice uses drand = Random() * sum(rates): the
 //    reference reads an uninitialised local there (src/ParSurfaceScatter.cpp:94,149);
+//  * FP32 flight (R = float) runs the same event loop with float kinematics:
+//    positions relative to the cell's low corner, k, velocities, fields,
+//    event times and rate lookups in float; energy, charge and the
+//    remaining step time stay double.  Its own random stream (four float
+//    uniforms per Philox block, mcb200_uniform_f32) and a rounding-tolerant
+//    event clock (a zero event time is taken as an event now, not as the
+//    reference's "Tf < MY_ZERO" catch) make it statistically, not bitwise,
+//    equal to the FP64 path;
 //  * the tetrahedron search after an impurity event (Getisym,
 //    src/ParticleUtils.cpp:395-625) walks the mesh from the current
 //    tetrahedron through face neighbours, falling back to a uniform k-grid
@@ -33,109 +41,229 @@ namespace mcb200 {
 constexpr double kMyZero = 1e-13;          // MY_ZERO, include/defs.h
 constexpr double kPiD = 3.141592653589793238462643e0;
 constexpr int kMaxEvents = 1000000;
+// FP32 flight: consecutive zero-length events after which a particle is
+// taken as stuck (counted in kCntZeroTime and caught).
+constexpr int kMaxZeroTimeEvents = 64;
 
-// Symmetry tables staged in shared memory (one copy per block).
-struct SymSmem {
-  int symi[48 * 6];   // matsym[c][s] at s*6+c
-  int newisym[5 * 48];
-  double bz[3 * 5 * 48];
-  int refl[3 * 48];
+// Arithmetic of the two flight precisions.
+template <typename R> struct FlightReal;
+template <> struct FlightReal<double> {
+  using V4 = double4;
+  static constexpr bool kCellRelative = false;  // absolute positions, reference arithmetic
+  static constexpr double kContain = kMyZero;   // face test d >= -kContain (unnormalised faces)
+  static constexpr double kBig = 1e99;
+};
+template <> struct FlightReal<float> {
+  using V4 = float4;
+  static constexpr bool kCellRelative = true;   // positions relative to the cell's low corner
+  static constexpr float kContain = 2e-5f;      // unit face normals: a k-space distance, ~10 float ulps at the BZ edge
+  static constexpr float kBig = 1e30f;
 };
 
-struct FlightCtx {
+__device__ __forceinline__ double m_abs(double v) { return fabs(v); }
+__device__ __forceinline__ float m_abs(float v) { return fabsf(v); }
+__device__ __forceinline__ double m_sqrt(double v) { return sqrt(v); }
+__device__ __forceinline__ float m_sqrt(float v) { return sqrtf(v); }
+__device__ __forceinline__ double m_log(double v) { return log(v); }
+__device__ __forceinline__ float m_log(float v) { return logf(v); }
+__device__ __forceinline__ double m_floor(double v) { return floor(v); }
+__device__ __forceinline__ float m_floor(float v) { return floorf(v); }
+__device__ __forceinline__ void m_sincos(double v, double *s, double *c) { *s = sin(v); *c = cos(v); }
+__device__ __forceinline__ void m_sincos(float v, float *s, float *c) { sincosf(v, s, c); }
+
+// Table views per precision (the FP64 tables or their FP32 copies).
+template <typename R> struct Tab;
+template <> struct Tab<double> {
+  static __device__ __forceinline__ const TetFlightT<double> *tf(const DevTables &T) { return T.tf; }
+  static __device__ __forceinline__ const TetShapeT<double> *ts(const DevTables &T) { return T.ts; }
+  static __device__ __forceinline__ const double4 *knode(const DevTables &T) { return T.knode; }
+  static __device__ __forceinline__ const double *gamtet(const DevTables &T) { return T.gamtet; }
+  static __device__ __forceinline__ const double *energy(const DevTables &T) { return T.energy; }
+  static __device__ __forceinline__ const double *sumscatt(const DevTables &T) { return T.sumscatt; }
+  static __device__ __forceinline__ const double *scatte(const DevTables &T) { return T.scatte; }
+  static __device__ __forceinline__ const double *dose(const DevTables &T) { return T.dose; }
+  static __device__ __forceinline__ const double *scattiie(const DevTables &T) { return T.scattiie; }
+  static __device__ __forceinline__ const double *scatth(const DevTables &T) { return T.scatth; }
+  static __device__ __forceinline__ const double *dosh(const DevTables &T) { return T.dosh; }
+  static __device__ __forceinline__ const double *scattiih(const DevTables &T) { return T.scattiih; }
+  static __device__ __forceinline__ const double *dostetmax(const DevTables &T) { return T.dostetmax; }
+};
+template <> struct Tab<float> {
+  static __device__ __forceinline__ const TetFlightT<float> *tf(const DevTables &T) { return T.f32.tf; }
+  static __device__ __forceinline__ const TetShapeT<float> *ts(const DevTables &T) { return T.f32.ts; }
+  static __device__ __forceinline__ const float4 *knode(const DevTables &T) { return T.f32.knode; }
+  static __device__ __forceinline__ const float *gamtet(const DevTables &T) { return T.f32.gamtet; }
+  static __device__ __forceinline__ const float *energy(const DevTables &T) { return T.f32.energy; }
+  static __device__ __forceinline__ const float *sumscatt(const DevTables &T) { return T.f32.sumscatt; }
+  static __device__ __forceinline__ const float *scatte(const DevTables &T) { return T.f32.scatte; }
+  static __device__ __forceinline__ const float *dose(const DevTables &T) { return T.f32.dose; }
+  static __device__ __forceinline__ const float *scattiie(const DevTables &T) { return T.f32.scattiie; }
+  static __device__ __forceinline__ const float *scatth(const DevTables &T) { return T.f32.scatth; }
+  static __device__ __forceinline__ const float *dosh(const DevTables &T) { return T.f32.dosh; }
+  static __device__ __forceinline__ const float *scattiih(const DevTables &T) { return T.f32.scattiih; }
+  static __device__ __forceinline__ const float *dostetmax(const DevTables &T) { return T.f32.dostetmax; }
+};
+
+// Symmetry tables staged in shared memory (one copy per block).
+template <typename R>
+struct SymSmemT {
+  int symi[48 * 6];   // matsym[c][s] at s*6+c
+  int newisym[5 * 48];
+  R bz[3 * 5 * 48];
+  int refl[3 * 48];
+};
+using SymSmem = SymSmemT<double>;
+
+template <typename R>
+struct FlightCtxT {
   DevTables T;
   DevMesh M;
   DevTallies Y;
-  DevChildren C;
+  DevChildrenT<R> C;
   double dt;
   uint64_t seed;
   uint32_t step;
 };
+using FlightCtx = FlightCtxT<double>;
 
 __device__ __forceinline__ void tally_add_i64(long long *p, double v, double scale) {
   atomicAdd(reinterpret_cast<unsigned long long *>(p), (unsigned long long)__double2ll_rn(v * scale));
 }
 __device__ __forceinline__ void count(const DevTallies &Y, int which) { atomicAdd(&Y.counters[which], 1ull); }
 
-struct Flyer {
-  const FlightCtx &F;
-  const SymSmem &S;
-  // random stream
+template <typename R>
+struct FlyerT {
+  using Real = FlightReal<R>;
+  using V4 = typename Real::V4;
+  using TB = Tab<R>;
+  const FlightCtxT<R> &F;
+  const SymSmemT<R> &S;
+  // random stream and the cached Philox block (index rblk, words rw0..rw3)
   uint32_t uid, sub, n;
+  uint32_t rblk, rw0, rw1, rw2, rw3;
   // particle registers (MeshQuantities members, include/mcmodel.h:215-233)
-  double x, y, z, kx, ky, kz, energy, charge, left_time;
+  R x, y, z, kx, ky, kz;
+  double energy, charge, left_time;
   int ic, jc, kc, itet, isym, type, iband;
-  double Ex, Ey, Ez, Rho, DA, vx, vy, vz;
+  R Ex, Ey, Ez, vx, vy, vz;
+  double Rho, DA;                                // FP64: cell screening and doping densities
+  R imp_a, imp_b, imp_ecut, imp_emax, imp_beta;  // FP32: the cell's Brooks-Herring constants
   int itetdir, idir;
   bool catch_, self;
-  double rough_rate, sphon_rate, surf_gamma, imp_gamma;
+  R rough_rate, sphon_rate, surf_gamma, imp_gamma;
   int nchild;
 
-  __device__ Flyer(const FlightCtx &f, const SymSmem &s) : F(f), S(s) {}
+  __device__ FlyerT(const FlightCtxT<R> &f, const SymSmemT<R> &s) : F(f), S(s) {}
 
-  __device__ __forceinline__ double Random() { return mcb200_uniform(F.seed, uid, F.step, sub, n++); }
+  __device__ __forceinline__ void start_stream(uint32_t u, uint32_t sb) {
+    uid = u;
+    sub = sb;
+    n = 0;
+    rblk = 0xffffffffu;
+  }
+
+  // Draw n of the particle's stream (include/mcb200_rng.h).  FP64: the
+  // 52-bit uniforms of mcb200_uniform, two per Philox block; FP32: the
+  // 23-bit uniforms of mcb200_uniform_f32, four per block.  A block is
+  // computed once and kept for the draws that follow.
+  __device__ __forceinline__ R Random() {
+    if constexpr (sizeof(R) == 8) {
+      const uint32_t b = n >> 1;
+      double u;
+      if ((n & 1u) && b == rblk) {
+        u = mcb200_bits_to_unit(rw3, rw2);
+      } else {
+        const mcb200_philox_block w =
+            mcb200_philox4x32_10(b, uid, F.step, sub, (uint32_t)F.seed, (uint32_t)(F.seed >> 32));
+        rblk = b;
+        rw2 = w.w[2];
+        rw3 = w.w[3];
+        u = (n & 1u) ? mcb200_bits_to_unit(w.w[3], w.w[2]) : mcb200_bits_to_unit(w.w[1], w.w[0]);
+      }
+      ++n;
+      return u;
+    } else {
+      const uint32_t b = n >> 2;
+      if (b != rblk) {
+        const mcb200_philox_block w =
+            mcb200_philox4x32_10(b, uid, F.step, sub, (uint32_t)F.seed, (uint32_t)(F.seed >> 32));
+        rblk = b;
+        rw0 = w.w[0];
+        rw1 = w.w[1];
+        rw2 = w.w[2];
+        rw3 = w.w[3];
+      }
+      const uint32_t q = n & 3u;
+      const uint32_t w = q == 0 ? rw0 : (q == 1 ? rw1 : (q == 2 ? rw2 : rw3));
+      ++n;
+      return mcb200_bits_to_unit_f32(w);
+    }
+  }
 
   __device__ __forceinline__ int ms(int c, int s) const { return S.symi[s * 6 + c]; }
   __device__ __forceinline__ int cell_index() const { return (jc * F.M.nx + ic) * F.M.nz + kc; }
   __device__ __forceinline__ int cell_index(int i, int j, int k) const { return (j * F.M.nx + i) * F.M.nz + k; }
+  __device__ __forceinline__ const TetFlightT<R> &tf(int it) const { return TB::tf(F.T)[it]; }
+  __device__ __forceinline__ const TetShapeT<R> &ts(int it) const { return TB::ts(F.T)[it]; }
 
   // in_wedge, src/ParticleUtils.cpp:295-305: BZ vector -> irreducible wedge of isym.
-  __device__ __forceinline__ void in_wedge(double &xo, double &yo, double &zo, double xi, double yi, double zi) const {
+  __device__ __forceinline__ void in_wedge(R &xo, R &yo, R &zo, R xi, R yi, R zi) const {
     const int p0 = ms(0, isym) - 1, p1 = ms(1, isym) - 1;
-    const double a = xi * (double)ms(3, isym), b = yi * (double)ms(4, isym), c = zi * (double)ms(5, isym);
+    const R a = xi * (R)ms(3, isym), b = yi * (R)ms(4, isym), c = zi * (R)ms(5, isym);
     xo = p0 == 0 ? a : (p1 == 0 ? b : c);
     yo = p0 == 1 ? a : (p1 == 1 ? b : c);
     zo = p0 == 2 ? a : (p1 == 2 ? b : c);
   }
   // Band::OutWedge, src/Band.cpp:555-570: wedge vector -> BZ.
-  __device__ __forceinline__ void out_wedge(double &xo, double &yo, double &zo, double xi, double yi, double zi) const {
+  __device__ __forceinline__ void out_wedge(R &xo, R &yo, R &zo, R xi, R yi, R zi) const {
     const int p0 = ms(0, isym) - 1, p1 = ms(1, isym) - 1, p2 = ms(2, isym) - 1;
-    xo = (p0 == 0 ? xi : (p0 == 1 ? yi : zi)) * (double)ms(3, isym);
-    yo = (p1 == 0 ? xi : (p1 == 1 ? yi : zi)) * (double)ms(4, isym);
-    zo = (p2 == 0 ? xi : (p2 == 1 ? yi : zi)) * (double)ms(5, isym);
+    xo = (p0 == 0 ? xi : (p0 == 1 ? yi : zi)) * (R)ms(3, isym);
+    yo = (p1 == 0 ? xi : (p1 == 1 ? yi : zi)) * (R)ms(4, isym);
+    zo = (p2 == 0 ? xi : (p2 == 1 ? yi : zi)) * (R)ms(5, isym);
   }
   // GetV, src/ParticleUtils.cpp:307-313.
   __device__ __forceinline__ void GetV() {
-    const double4 v = *reinterpret_cast<const double4 *>(F.T.tf[itet].v);
+    const V4 v = *reinterpret_cast<const V4 *>(tf(itet).v);
     out_wedge(vx, vy, vz, v.x, v.y, v.z);
   }
   // GetEnergy, src/ParticleUtils.cpp:315-329.
   __device__ void GetEnergy() {
-    double dx, dy, dz;
+    R dx, dy, dz;
     in_wedge(dx, dy, dz, kx, ky, kz);
-    const double4 k0 = F.T.knode[F.T.tnode[itet].x];
+    const V4 k0 = TB::knode(F.T)[F.T.tnode[itet].x];
     dx -= k0.x;
     dy -= k0.y;
     dz -= k0.z;
-    const double *v = F.T.tf[itet].v;
+    const R *v = tf(itet).v;
     energy = v[3] + v[0] * dx + v[1] * dy + v[2] * dz;
   }
-  __device__ __forceinline__ double face_dist(int it, int f, double a, double b, double c) const {
-    const double *nn = F.T.tf[it].n[f];
+  __device__ __forceinline__ R face_dist(int it, int f, R a, R b, R c) const {
+    const R *nn = tf(it).n[f];
     return nn[0] * a + nn[1] * b + nn[2] * c - nn[3];
   }
-  __device__ __forceinline__ bool tet_contains(int it, double a, double b, double c) const {
-    return face_dist(it, 0, a, b, c) >= -kMyZero && face_dist(it, 1, a, b, c) >= -kMyZero &&
-           face_dist(it, 2, a, b, c) >= -kMyZero && face_dist(it, 3, a, b, c) >= -kMyZero;
+  __device__ __forceinline__ bool tet_contains(int it, R a, R b, R c) const {
+    const R tol = -Real::kContain;
+    return face_dist(it, 0, a, b, c) >= tol && face_dist(it, 1, a, b, c) >= tol &&
+           face_dist(it, 2, a, b, c) >= tol && face_dist(it, 3, a, b, c) >= tol;
   }
 
   // TetTime, src/TetHit.cpp:4-106: time to the tet face the drift reaches first.
-  __device__ double TetTime() {
-    double xkl, ykl, zkl, xfl, yfl, zfl;
+  __device__ R TetTime() {
+    R xkl, ykl, zkl, xfl, yfl, zfl;
     in_wedge(xkl, ykl, zkl, kx, ky, kz);
     in_wedge(xfl, yfl, zfl, Ex, Ey, Ez);
-    const TetFlight &t = F.T.tf[itet];
-    double best = 0;
+    const TetFlightT<R> &t = tf(itet);
+    R best = 0;
     itetdir = 0;
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
-      const double nf = t.n[f][0] * xfl + t.n[f][1] * yfl + t.n[f][2] * zfl;
-      double tfp;
+      const R nf = t.n[f][0] * xfl + t.n[f][1] * yfl + t.n[f][2] * zfl;
+      R tfp;
       if (nf < 0) {
         tfp = (t.n[f][3] - (t.n[f][0] * xkl + t.n[f][1] * ykl + t.n[f][2] * zkl)) / nf;
         if (tfp < 0) tfp = 0;
       } else {
-        tfp = 1e99;
+        tfp = Real::kBig;
       }
       if (f == 0) best = tfp;
       else if (tfp < best) {
@@ -146,37 +274,55 @@ struct Flyer {
     return best;
   }
 
-  // CellTime, src/CellHit.cpp:4-93: time to the real-space cell face.
-  __device__ double CellTime() {
+  // CellTime, src/CellHit.cpp:4-93: time to the real-space cell face.  FP32
+  // positions are offsets from the cell's low corner, so the gaps are
+  // (width - x) and x.
+  __device__ R CellTime() {
     const DevMesh &M = F.M;
     int idx, idy, idz;
-    double tx, ty, tz;
-    if (vx > 0) { idx = kDown; tx = (M.lx[ic + 1] - x) / vx; }
-    else if (vx < 0) { idx = kUp; tx = -(x - M.lx[ic]) / vx; }
-    else { idx = kUp; tx = 1e99; }
-    if (vy > 0) { idy = kRight; ty = (M.ly[jc + 1] - y) / vy; }
-    else if (vy < 0) { idy = kLeft; ty = -(y - M.ly[jc]) / vy; }
-    else { idy = kRight; ty = 1e99; }
-    if (vz > 0) { idz = kBack; tz = (M.lz[kc + 1] - z) / vz; }
-    else if (vz < 0) { idz = kFront; tz = -(z - M.lz[kc]) / vz; }
-    else { idz = kFront; tz = 1e99; }
+    R tx, ty, tz;
+    if constexpr (Real::kCellRelative) {
+      if (vx > 0) { idx = kDown; tx = (M.dxf[ic] - x) / vx; }
+      else if (vx < 0) { idx = kUp; tx = -x / vx; }
+      else { idx = kUp; tx = Real::kBig; }
+      if (vy > 0) { idy = kRight; ty = (M.dyf[jc] - y) / vy; }
+      else if (vy < 0) { idy = kLeft; ty = -y / vy; }
+      else { idy = kRight; ty = Real::kBig; }
+      if (vz > 0) { idz = kBack; tz = (M.dzf[kc] - z) / vz; }
+      else if (vz < 0) { idz = kFront; tz = -z / vz; }
+      else { idz = kFront; tz = Real::kBig; }
+    } else {
+      if (vx > 0) { idx = kDown; tx = (M.lx[ic + 1] - x) / vx; }
+      else if (vx < 0) { idx = kUp; tx = -(x - M.lx[ic]) / vx; }
+      else { idx = kUp; tx = Real::kBig; }
+      if (vy > 0) { idy = kRight; ty = (M.ly[jc + 1] - y) / vy; }
+      else if (vy < 0) { idy = kLeft; ty = -(y - M.ly[jc]) / vy; }
+      else { idy = kRight; ty = Real::kBig; }
+      if (vz > 0) { idz = kBack; tz = (M.lz[kc + 1] - z) / vz; }
+      else if (vz < 0) { idz = kFront; tz = -(z - M.lz[kc]) / vz; }
+      else { idz = kFront; tz = Real::kBig; }
+    }
     idir = idx;
-    double t = tx;
+    R t = tx;
     if (ty < t) { idir = idy; t = ty; }
     if (tz < t) { idir = idz; t = tz; }
-    if (t < -kMyZero) t = 0;
+    if constexpr (Real::kCellRelative) {
+      if (t < 0) t = 0;  // a position rounded just past the face
+    } else {
+      if (t < -kMyZero) t = 0;
+    }
     return t;
   }
 
   // Band::CONFBZ, src/Band.cpp:573-616: fold k back into the first BZ.
-  __device__ void CONFBZ(double &a, double &b, double &c) const {
-    const double p = F.T.a0pi;
+  __device__ void CONFBZ(R &a, R &b, R &c) const {
+    const R p = (R)F.T.a0pi;
     for (int guard = 0; guard < 64; ++guard) {
-      bool out = fabs(a) > p || fabs(b) > p || fabs(c) > p || fabs(a) + fabs(b) + fabs(c) > 1.50 * p;
+      bool out = m_abs(a) > p || m_abs(b) > p || m_abs(c) > p || m_abs(a) + m_abs(b) + m_abs(c) > (R)1.50 * p;
       if (!out) return;
-      a = a > 0.0 ? a - p : a + p;
-      b = b > 0.0 ? b - p : b + p;
-      c = c > 0.0 ? c - p : c + p;
+      a = a > (R)0 ? a - p : a + p;
+      b = b > (R)0 ? b - p : b + p;
+      c = c > (R)0 ? c - p : c + p;
     }
   }
 
@@ -185,14 +331,14 @@ struct Flyer {
   // until every face test passes (the reference's containment test,
   // d >= -MY_ZERO).  Returns -1 when the walk reaches a wedge boundary or
   // does not settle within the step cap; the caller then uses the k-grid.
-  __device__ int walk_to(int start, double a, double b, double c) const {
+  __device__ int walk_to(int start, R a, R b, R c) const {
     int it = start;
     for (int s = 0; s < 64; ++s) {
       int fmin = -1;
-      double dmin = -kMyZero;
+      R dmin = -Real::kContain;
 #pragma unroll
       for (int f = 0; f < 4; ++f) {
-        const double d = face_dist(it, f, a, b, c);
+        const R d = face_dist(it, f, a, b, c);
         if (d < dmin) {
           dmin = d;
           fmin = f;
@@ -210,32 +356,39 @@ struct Flyer {
   // band iband that contains the wedge vector (k-grid lookup, see file note).
   __device__ void Getisym() {
     int mink, maxk;
-    double tmin, tmax;
-    if (fabs(kx) > fabs(ky)) { tmin = fabs(ky); tmax = fabs(kx); mink = 1; maxk = 0; }
-    else { tmin = fabs(kx); tmax = fabs(ky); mink = 0; maxk = 1; }
-    if (fabs(kz) < tmin) mink = 2;
-    else if (fabs(kz) > tmax) maxk = 2;
+    R tmin, tmax;
+    if (m_abs(kx) > m_abs(ky)) { tmin = m_abs(ky); tmax = m_abs(kx); mink = 1; maxk = 0; }
+    else { tmin = m_abs(kx); tmax = m_abs(ky); mink = 0; maxk = 1; }
+    if (m_abs(kz) < tmin) mink = 2;
+    else if (m_abs(kz) > tmax) maxk = 2;
     // pos[mink] = 2, pos[maxk] = 0, else 1 (mink != maxk always)
     const int p0 = maxk == 0 ? 0 : (mink == 0 ? 2 : 1);
     const int p1 = maxk == 1 ? 0 : (mink == 1 ? 2 : 1);
     const int p2 = maxk == 2 ? 0 : (mink == 2 ? 2 : 1);
-    auto sgn = [](double v) { return (int)(fabs(v) / v); };  // utils.cpp sign()
-    const int sx = sgn(kx) + 1, sy = sgn(ky) + 1, sz = sgn(kz) + 1;
+    int sx, sy, sz;
+    if constexpr (sizeof(R) == 8) {
+      auto sgn = [](double v) { return (int)(fabs(v) / v); };  // utils.cpp sign()
+      sx = sgn(kx) + 1; sy = sgn(ky) + 1; sz = sgn(kz) + 1;
+    } else {
+      // a component rounded to exactly zero lies on a wedge plane: either
+      // side's wedge contains it, take the positive one
+      sx = kx < 0 ? 0 : 2; sy = ky < 0 ? 0 : 2; sz = kz < 0 ? 0 : 2;
+    }
     if (sx < 0 || sx > 2 || sy < 0 || sy > 2 || sz < 0 || sz > 2) {  // a zero component: sign() is NaN in the reference
       count(F.Y, kCntNoTet);
       catch_ = true;
       return;
     }
     isym = F.T.indmat[((((sx * 3 + sy) * 3 + sz) * 3 + p0) * 3 + p1) * 3 + p2];
-    double a, b, c;
+    R a, b, c;
     in_wedge(a, b, c, kx, ky, kz);
     if (iband == F.T.ibt[itet] && tet_contains(itet, a, b, c)) return;
     int start = iband == F.T.ibt[itet] ? itet : -1;
     if (iband == F.T.bandof[0]) {  // lowest conduction band: start next to the point
       const int sg = kSeedGridN;
-      const int si = min(max((int)floor((a - F.T.grid_lo[0]) * F.T.seed_inv[0]), 0), sg - 1);
-      const int sj = min(max((int)floor((b - F.T.grid_lo[1]) * F.T.seed_inv[1]), 0), sg - 1);
-      const int sk = min(max((int)floor((c - F.T.grid_lo[2]) * F.T.seed_inv[2]), 0), sg - 1);
+      const int si = min(max((int)m_floor((a - (R)F.T.grid_lo[0]) * (R)F.T.seed_inv[0]), 0), sg - 1);
+      const int sj = min(max((int)m_floor((b - (R)F.T.grid_lo[1]) * (R)F.T.seed_inv[1]), 0), sg - 1);
+      const int sk = min(max((int)m_floor((c - (R)F.T.grid_lo[2]) * (R)F.T.seed_inv[2]), 0), sg - 1);
       const int s0 = F.T.seed_grid[((size_t)si * sg + sj) * sg + sk];
       if (s0 >= 0) start = s0;
     }
@@ -247,9 +400,9 @@ struct Flyer {
       }
     }
     const int g = F.T.grid_n;
-    int gi = (int)floor((a - F.T.grid_lo[0]) * F.T.grid_inv[0]);
-    int gj = (int)floor((b - F.T.grid_lo[1]) * F.T.grid_inv[1]);
-    int gk = (int)floor((c - F.T.grid_lo[2]) * F.T.grid_inv[2]);
+    int gi = (int)m_floor((a - (R)F.T.grid_lo[0]) * (R)F.T.grid_inv[0]);
+    int gj = (int)m_floor((b - (R)F.T.grid_lo[1]) * (R)F.T.grid_inv[1]);
+    int gk = (int)m_floor((c - (R)F.T.grid_lo[2]) * (R)F.T.grid_inv[2]);
     gi = min(max(gi, 0), g - 1);
     gj = min(max(gj, 0), g - 1);
     gk = min(max(gk, 0), g - 1);
@@ -269,7 +422,7 @@ struct Flyer {
   // GetisymBZ, src/ParticleUtils.cpp:331-392: after a BZ-boundary crossing,
   // search the BZ-surface tets of the particle's energy bin.
   __device__ void GetisymBZ() {
-    double a, b, c;
+    R a, b, c;
     in_wedge(a, b, c, kx, ky, kz);
     if (iband == F.T.ibt[itet] && tet_contains(itet, a, b, c)) return;
     int ie = (int)(energy * F.T.dlist);
@@ -310,74 +463,74 @@ struct Flyer {
   // the drawn index (1..4); an index of 5 (u*4+1 rounding up to 5, possible
   // only for u within 2^-51 of 1) reads past the reference's table and is
   // clamped to 4 here.
-  __device__ __forceinline__ int talend_index() { return min((int)(Random() * 4.0 + 1.0), 4); }
+  __device__ __forceinline__ int talend_index() { return min((int)(Random() * (R)4.0 + (R)1.0), 4); }
   __device__ void TALIND(int ityp) {
     int ital = 1;
-    const double ax = fabs(kx), ay = fabs(ky), az = fabs(kz);
+    const R ax = m_abs(kx), ay = m_abs(ky), az = m_abs(kz);
     if (ax >= ay && ax >= az) {
-      if (kx >= 0.0) {
+      if (kx >= (R)0) {
         if (ityp == 1) ital = 1;
         if (ityp == 2) ital = 2;
         if (ityp == 3) ital = talend_index() + 2;  // {3,4,5,6}
       }
-      if (kx < 0.0) {
+      if (kx < (R)0) {
         if (ityp == 1) ital = 2;
         if (ityp == 2) ital = 1;
         if (ityp == 3) ital = talend_index() + 2;
       }
     }
     if (ay >= az && ay >= ax) {
-      if (ky >= 0.0) {
+      if (ky >= (R)0) {
         if (ityp == 1) ital = 3;
         if (ityp == 2) ital = 4;
         if (ityp == 3) { const int i = talend_index(); ital = i <= 2 ? i : i + 2; }  // {1,2,5,6}
       }
-      if (ky < 0.0) {
+      if (ky < (R)0) {
         if (ityp == 1) ital = 4;
         if (ityp == 2) ital = 3;
         if (ityp == 3) { const int i = talend_index(); ital = i <= 2 ? i : i + 2; }
       }
     }
     if (az > ay && az > ax) {
-      if (kz >= 0.0) {
+      if (kz >= (R)0) {
         if (ityp == 1) ital = 5;
         if (ityp == 2) ital = 6;
         if (ityp == 3) ital = talend_index();  // {1,2,3,4}
       }
-      if (kz < 0.0) {
+      if (kz < (R)0) {
         if (ityp == 1) ital = 6;
         if (ityp == 2) ital = 5;
         if (ityp == 3) ital = talend_index();
       }
     }
-    isym = (int)(Random() * 8.0) + 8 * (ital - 1);
+    isym = (int)(Random() * (R)8.0) + 8 * (ital - 1);
   }
 
   // Band::CALDOSTETMAX, src/Band.cpp:2298-2320.
-  __device__ double CALDOSTETMAX(double eed, int ib) const {
-    const double *d = F.T.dostetmax + (size_t)ib * kNT;
-    if (eed <= 0.0) return d[0];
-    if (eed >= F.T.emax) return d[kNT - 1];
-    const int itab = min((int)(eed / F.T.dtable), kNT - 2);  // eed just below emax may round to the last point
+  __device__ R CALDOSTETMAX(R eed, int ib) const {
+    const R *d = TB::dostetmax(F.T) + (size_t)ib * kNT;
+    if (eed <= (R)0) return d[0];
+    if (eed >= (R)F.T.emax) return d[kNT - 1];
+    const int itab = min((int)(eed / (R)F.T.dtable), kNT - 2);  // eed just below emax may round to the last point
     return d[itab] > d[itab + 1] ? d[itab] : d[itab + 1];
   }
 
   // Band::SURF, src/Band.cpp:194-332 (only reached by FASTSURF for
   // tetrahedra whose two lowest nodes are degenerate).
-  __device__ double SURF(double eps, int it) const;
+  __device__ R SURF(R eps, int it) const;
   // Band::FASTSURF, src/Band.cpp:665-704.
-  __device__ double FASTSURF(double eps, int it) const {
-    const TetShape &s = F.T.ts[it];
-    const double e0 = s.e[0], e1 = s.e[1], e2 = s.e[2], e3 = s.e[3];
+  __device__ R FASTSURF(R eps, int it) const {
+    const TetShapeT<R> &s = ts(it);
+    const R e0 = s.e[0], e1 = s.e[1], e2 = s.e[2], e3 = s.e[3];
     if (eps > e0 && eps < e3) {
       if (eps <= e1) return s.fac[0] * (eps - e0) * (eps - e0);
       if (eps < e2) {
-        if (e1 - e0 > 1e-10) return s.fac[0] * (eps - e0) * (eps - e0) - s.fac[1] * (eps - e1) * (eps - e1);
+        if (e1 - e0 > (R)1e-10) return s.fac[0] * (eps - e0) * (eps - e0) - s.fac[1] * (eps - e1) * (eps - e1);
         return SURF(eps, it);
       }
       return s.fac[2] * (eps - e3) * (eps - e3);
     }
-    return 0.0;
+    return 0;
   }
 
   // get_state, src/ParticleUtils.cpp:48-120: random final state on the
@@ -387,11 +540,12 @@ struct Flyer {
       self = true;
       return;
     }
-    const double maxdostet = CALDOSTETMAX(energy, iband);
-    int itab = (int)(energy * F.T.dlists);
+    const R e = (R)energy;
+    const R maxdostet = CALDOSTETMAX(e, iband);
+    int itab = (int)(e * (R)F.T.dlists);
     bool small_ = itab < kMWLES;
     if (!small_) {
-      itab = (int)(energy * F.T.dlist);
+      itab = (int)(e * (R)F.T.dlist);
       if (itab >= kMWLE) itab = kMWLE - 1;
     }
     const int nted = small_ ? F.T.ntlists[itab * kMNB + iband] : F.T.ntlist[itab * kMNB + iband];
@@ -403,11 +557,13 @@ struct Flyer {
     }
     int count2 = 0;
     for (;;) {
-      itet = lst[(int)(nted * Random()) + base];
+      int pick = (int)(nted * Random());
+      if constexpr (sizeof(R) == 4) pick = min(pick, nted - 1);
+      itet = lst[pick + base];
       count2++;
-      const TetShape &s = F.T.ts[itet];
-      if ((count2 < 10000) && !((s.e[0] < energy) && (s.e[3] > energy))) continue;
-      const double dostet = FASTSURF(energy, itet) / s.vgt;
+      const TetShapeT<R> &s = ts(itet);
+      if ((count2 < 10000) && !((s.e[0] < e) && (s.e[3] > e))) continue;
+      const R dostet = FASTSURF(e, itet) / s.vgt;
       if (((Random() * maxdostet) > dostet) && (count2 < 10000)) continue;
       break;
     }
@@ -424,29 +580,37 @@ struct Flyer {
   __device__ void getK();
 
   // Band::CALSCATTSUM, src/Band.cpp:1999-2033.
-  __device__ double CALSCATTSUM(double eed, int ib) const {
-    const double *s = F.T.sumscatt;
-    if (eed <= 0.0) return s[ib];
-    if (eed >= F.T.emax) return s[(size_t)(kNT - 1) * kMNB + ib];
-    const int itab = min((int)(eed / F.T.dtable), kNT - 2);
-    const double intp = (eed - F.T.energy[itab]) / (F.T.energy[itab + 1] - F.T.energy[itab]);
+  __device__ R CALSCATTSUM(R eed, int ib) const {
+    const R *s = TB::sumscatt(F.T);
+    const R *E = TB::energy(F.T);
+    if (eed <= (R)0) return s[ib];
+    if (eed >= (R)F.T.emax) return s[(size_t)(kNT - 1) * kMNB + ib];
+    const int itab = min((int)(eed / (R)F.T.dtable), kNT - 2);
+    const R intp = (eed - E[itab]) / (E[itab + 1] - E[itab]);
     return s[(size_t)itab * kMNB + ib] + intp * (s[(size_t)(itab + 1) * kMNB + ib] - s[(size_t)itab * kMNB + ib]);
   }
 
   // Electron mechanism choice by a running sum over Band::CALSCATTE
   // (src/Band.cpp:2165-2231) entries, without materialising the 56-entry
   // array: returns the chosen index or -1 (self-scattering).
-  __device__ int pick_electron_mechanism(double drand) const;
-  __device__ double electron_rate_sum() const;
-  __device__ int pick_hole_mechanism(double drand) const;
-  __device__ double hole_rate_sum() const;
+  __device__ int pick_electron_mechanism(R drand) const;
+  __device__ R electron_rate_sum() const;
+  __device__ int pick_hole_mechanism(R drand) const;
+  __device__ R hole_rate_sum() const;
 
   // heat_to_point, src/heat.cpp:169-196 (CIC onto the cell's 8 nodes).
   __device__ void heat_to_point(double e, long long *heat) const {
     const DevMesh &M = F.M;
-    const double rx = (x - M.lx[ic]) / M.dx[ic];
-    const double ry = (y - M.ly[jc]) / M.dy[jc];
-    const double rz = (z - M.lz[kc]) / M.dz[kc];
+    R rx, ry, rz;
+    if constexpr (Real::kCellRelative) {
+      rx = x / M.dxf[ic];
+      ry = y / M.dyf[jc];
+      rz = z / M.dzf[kc];
+    } else {
+      rx = (x - M.lx[ic]) / M.dx[ic];
+      ry = (y - M.ly[jc]) / M.dy[jc];
+      rz = (z - M.lz[kc]) / M.dz[kc];
+    }
     const int px = M.nx + 1, pz = M.nz + 1;
     auto node = [&](int i, int j, int k) { return ((size_t)j * px + i) * pz + k; };
     tally_add_i64(heat + node(ic, jc, kc), e * (1 - ry) * (1 - rx) * (1 - rz), kEnergyScale);
@@ -461,7 +625,8 @@ struct Flyer {
 
   // EPSCAT, src/ElectronPhononScatter.cpp:98-195 (Flag_QuantumCorrection = 0).
   __device__ void EPSCAT(int iscat) {
-    const double eeold = energy, xkold = kx, ykold = ky, zkold = kz;
+    const double eeold = energy;
+    const R xkold = kx, ykold = ky, zkold = kz;
     const int ibold = iband, itetold = itet, isymold = isym;
     const DevTables &T = F.T;
     iband = iscat / T.scpre + T.bandof[0];
@@ -491,11 +656,12 @@ struct Flyer {
 
   // ESCATII, src/ElectronPhononScatter.cpp:406-497 (secondary generation off: seciifl = false).
   __device__ void ESCATII(int iscat) {
-    const double eeold = energy, xkold = kx, ykold = ky, zkold = kz;
+    const double eeold = energy;
+    const R xkold = kx, ykold = ky, zkold = kz;
     const int ibold = iband, itetold = itet, isymold = isym;
     iband = iscat / F.T.scpre + F.T.bandof[0];
     energy = (energy - F.T.sieg) / 3.0;
-    isym = ((int)(48 * Random()) % 48);
+    isym = ((int)((R)48 * Random()) % 48);
     get_state();
     if (self) {
       energy = eeold; kx = xkold; ky = ykold; kz = zkold;
@@ -505,9 +671,9 @@ struct Flyer {
 
   // ElectronPhononScatter, src/ElectronPhononScatter.cpp:5-95.
   __device__ void ElectronPhononScatter() {
-    const double scasum = CALSCATTSUM(energy, iband);
-    const double g = F.T.gamtet[itet];
-    const double drand = scasum > g ? Random() * scasum : Random() * g;
+    const R scasum = CALSCATTSUM((R)energy, iband);
+    const R g = TB::gamtet(F.T)[itet];
+    const R drand = scasum > g ? Random() * scasum : Random() * g;
     if (scasum < drand) {
       self = true;
       return;
@@ -524,7 +690,8 @@ struct Flyer {
 
   // HPSCAT, src/HolePhononScatter.cpp:86-146.
   __device__ void HPSCAT(int iscat) {
-    const double eeold = energy, xkold = kx, ykold = ky, zkold = kz;
+    const double eeold = energy;
+    const R xkold = kx, ykold = ky, zkold = kz;
     const int ibold = iband, itetold = itet, isymold = isym;
     iband = iscat / F.T.scprh + F.T.bandof[1];
     switch (iscat % F.T.scprh) {
@@ -532,7 +699,7 @@ struct Flyer {
       case 2: energy = energy - F.T.temphop; break;
       default: break;
     }
-    isym = ((int)(48 * Random()) % 48);
+    isym = ((int)((R)48 * Random()) % 48);
     get_state();
     if (self) {
       energy = eeold; kx = xkold; ky = ykold; kz = zkold;
@@ -543,11 +710,12 @@ struct Flyer {
 
   // HSCATII, src/HolePhononScatter.cpp:149-234 (seciifl = false).
   __device__ void HSCATII(int iscat) {
-    const double eeold = energy, xkold = kx, ykold = ky, zkold = kz;
+    const double eeold = energy;
+    const R xkold = kx, ykold = ky, zkold = kz;
     const int ibold = iband, itetold = itet, isymold = isym;
     iband = iscat / F.T.scprh + F.T.bandof[1];
     energy = (energy - F.T.sieg) / 3.0;
-    isym = ((int)(48 * Random()) % 48);
+    isym = ((int)((R)48 * Random()) % 48);
     get_state();
     if (self) {
       energy = eeold; kx = xkold; ky = ykold; kz = zkold;
@@ -557,9 +725,9 @@ struct Flyer {
 
   // HolePhononScatter, src/HolePhononScatter.cpp:4-83.
   __device__ void HolePhononScatter() {
-    const double scasum = CALSCATTSUM(energy, iband);
-    const double g = F.T.gamtet[itet];
-    const double drand = scasum > g ? Random() * scasum : Random() * g;
+    const R scasum = CALSCATTSUM((R)energy, iband);
+    const R g = TB::gamtet(F.T)[itet];
+    const R drand = scasum > g ? Random() * scasum : Random() * g;
     if (scasum < drand) {
       self = true;
       return;
@@ -574,34 +742,42 @@ struct Flyer {
     else HPSCAT(iscat);
   }
 
-  // GetImpScRate, src/ElectronImpurityScatter.cpp:62-126 (Brooks-Herring, bhmrtfl = false).
-  __device__ double GetImpScRate(double eel) const {
-    const DevTables &T = F.T;
-    if ((eel * T.eV0 < 0.120) && (DA * T.conc0 >= 1e22)) {
-      const double eebeta = T.frickel * 4 * kPiD * Rho / (2.0 * T.meld * T.eps_si);
-      if (F.M.surface_scatter && F.M.surface_impurity && F.M.in_surf[cell_index()]) {
-        // The reference's surface-impurity formula is commented out there and
-        // leaves the rate unset; the engine treats it as zero.
-        return 0.0;
+  // GetImpScRate, src/ElectronImpurityScatter.cpp:62-126 (Brooks-Herring,
+  // bhmrtfl = false).  FP32: the same rate written as
+  // imp_a * sqrt(e) / (1 + imp_b * e) with the cell's constants (load_cell_fields).
+  __device__ R GetImpScRate(R eel) const {
+    if constexpr (sizeof(R) == 4) {
+      return eel < imp_ecut ? imp_a * m_sqrt(eel) / ((R)1 + imp_b * eel) : (R)0;
+    } else {
+      const DevTables &T = F.T;
+      if ((eel * T.eV0 < 0.120) && (DA * T.conc0 >= 1e22)) {
+        const double eebeta = T.frickel * 4 * kPiD * Rho / (2.0 * T.meld * T.eps_si);
+        if (F.M.surface_scatter && F.M.surface_impurity && F.M.in_surf[cell_index()]) {
+          // The reference's surface-impurity formula is commented out there and
+          // leaves the rate unset; the engine treats it as zero.
+          return 0.0;
+        }
+        const double fr = T.frickel * Rho;
+        return DA * T.meld * sqrt(2.0 * T.meld * eel) /
+               (kPiD * (fr * fr) * (1.0 + 4.0 * eel * T.melt / (eebeta * T.meld)));
       }
-      const double fr = T.frickel * Rho;
-      return DA * T.meld * sqrt(2.0 * T.meld * eel) /
-             (kPiD * (fr * fr) * (1.0 + 4.0 * eel * T.melt / (eebeta * T.meld)));
+      return 0.0;
     }
-    return 0.0;
   }
 
   // GetImpScGamma, src/ElectronImpurityScatter.cpp:6-59: majorant of the
   // BH rate over the tet's energy span.
-  __device__ double GetImpScGamma() const {
+  __device__ R GetImpScGamma() const {
     const DevTables &T = F.T;
-    const double eemax = T.frickel * 4 * kPiD * Rho / (8.0 * T.melt * T.eps_si);
-    const TetShape &s = T.ts[itet];
-    double gammax;
+    R eemax;
+    if constexpr (sizeof(R) == 4) eemax = imp_emax;
+    else eemax = T.frickel * 4 * kPiD * Rho / (8.0 * T.melt * T.eps_si);
+    const TetShapeT<R> &s = ts(itet);
+    R gammax;
     if (eemax < s.e[0]) gammax = GetImpScRate(s.e[0]);
     else if (eemax > s.e[3]) gammax = GetImpScRate(s.e[3]);
     else gammax = GetImpScRate(eemax);
-    const double floor_ = 1.0 / T.scrt0;
+    const R floor_ = (R)(1.0 / T.scrt0);
     return gammax > floor_ ? gammax : floor_;
   }
 
@@ -610,7 +786,7 @@ struct Flyer {
 
   // ElectronImpurityScatter, src/ElectronImpurityScatter.cpp:128-185.
   __device__ void ElectronImpurityScatter() {
-    const double gamimp = GetImpScRate(energy);
+    const R gamimp = GetImpScRate((R)energy);
     if (gamimp < Random() * imp_gamma) {
       self = true;
     } else {
@@ -621,8 +797,8 @@ struct Flyer {
   // GetSurfScRate, src/ParSurfaceScatter.cpp:3-45.
   __device__ void GetSurfScRate() {
     const int c = cell_index();
-    if (type == 0) { rough_rate = F.M.e_rough[c]; sphon_rate = F.M.e_sphon[c]; }
-    else { rough_rate = F.M.h_rough[c]; sphon_rate = F.M.h_sphon[c]; }
+    if (type == 0) { rough_rate = (R)F.M.e_rough[c]; sphon_rate = (R)F.M.e_sphon[c]; }
+    else { rough_rate = (R)F.M.h_rough[c]; sphon_rate = (R)F.M.h_sphon[c]; }
     surf_gamma = rough_rate + sphon_rate;
   }
 
@@ -655,32 +831,60 @@ struct Flyer {
       return;
     }
     const DevMesh &M = F.M;
-    switch (idir) {
-      case kUp: x = M.lx[ic]; ic--; break;
-      case kDown: x = M.lx[ic + 1]; ic++; break;
-      case kRight:
-        y = M.ly[jc + 1];
-        jc++;
-        tally_add_i64(F.Y.rcurrent + jc, charge, kChargeScale);
-        break;
-      case kLeft:
-        y = M.ly[jc];
-        tally_add_i64(F.Y.lcurrent + jc, charge, kChargeScale);
-        jc--;
-        break;
-      case kFront: z = M.lz[kc]; kc--; break;
-      case kBack: z = M.lz[kc + 1]; kc++; break;
+    if constexpr (Real::kCellRelative) {  // the face, in the new cell's frame
+      switch (idir) {
+        case kUp: x = M.dxf[ic - 1]; ic--; break;
+        case kDown: x = 0; ic++; break;
+        case kRight:
+          y = 0;
+          jc++;
+          tally_add_i64(F.Y.rcurrent + jc, charge, kChargeScale);
+          break;
+        case kLeft:
+          y = M.dyf[jc - 1];
+          tally_add_i64(F.Y.lcurrent + jc, charge, kChargeScale);
+          jc--;
+          break;
+        case kFront: z = M.dzf[kc - 1]; kc--; break;
+        case kBack: z = 0; kc++; break;
+      }
+    } else {
+      switch (idir) {
+        case kUp: x = M.lx[ic]; ic--; break;
+        case kDown: x = M.lx[ic + 1]; ic++; break;
+        case kRight:
+          y = M.ly[jc + 1];
+          jc++;
+          tally_add_i64(F.Y.rcurrent + jc, charge, kChargeScale);
+          break;
+        case kLeft:
+          y = M.ly[jc];
+          tally_add_i64(F.Y.lcurrent + jc, charge, kChargeScale);
+          jc--;
+          break;
+        case kFront: z = M.lz[kc]; kc--; break;
+        case kBack: z = M.lz[kc + 1]; kc++; break;
+      }
     }
   }
   // Period, src/CellHit.cpp:416-432.
   __device__ void Period() {
     const DevMesh &M = F.M;
-    if (idir == kUp) x = M.lx[ic + 1];
-    else if (idir == kDown) x = M.lx[ic];
-    else if (idir == kLeft) y = M.ly[jc + 1];
-    else if (idir == kRight) y = M.ly[jc];
-    else if (idir == kFront) z = M.lz[kc + 1];
-    else if (idir == kBack) z = M.lz[kc];
+    if constexpr (Real::kCellRelative) {
+      if (idir == kUp) x = M.dxf[ic];
+      else if (idir == kDown) x = 0;
+      else if (idir == kLeft) y = M.dyf[jc];
+      else if (idir == kRight) y = 0;
+      else if (idir == kFront) z = M.dzf[kc];
+      else if (idir == kBack) z = 0;
+    } else {
+      if (idir == kUp) x = M.lx[ic + 1];
+      else if (idir == kDown) x = M.lx[ic];
+      else if (idir == kLeft) y = M.ly[jc + 1];
+      else if (idir == kRight) y = M.ly[jc];
+      else if (idir == kFront) z = M.lz[kc + 1];
+      else if (idir == kBack) z = M.lz[kc];
+    }
   }
   __device__ void neighbour(int &i, int &j, int &k) const {
     i = ic; j = jc; k = kc;
@@ -715,14 +919,26 @@ struct Flyer {
       count(F.Y, kCntUnfinished);
       return;
     }
-    const DevChildren &C = F.C;
+    const DevChildrenT<R> &C = F.C;
     const unsigned slot = atomicAdd(C.count, 1u);
     const uint32_t csub = sub * 16u + 1u + (uint32_t)nchild++;
     if ((int)slot >= C.capacity) {
       count(F.Y, kCntChildOverflow);
       return;
     }
-    C.x[slot] = x; C.y[slot] = y; C.z[slot] = z;
+    R cx = x, cy = y, cz = z;
+    if constexpr (Real::kCellRelative) {  // the same point in the neighbour cell's frame
+      const DevMesh &M = F.M;
+      switch (idir) {
+        case kUp: cx = x + M.dxf[i]; break;
+        case kDown: cx = x - M.dxf[ic]; break;
+        case kLeft: cy = y + M.dyf[j]; break;
+        case kRight: cy = y - M.dyf[jc]; break;
+        case kFront: cz = z + M.dzf[k]; break;
+        case kBack: cz = z - M.dzf[kc]; break;
+      }
+    }
+    C.x[slot] = cx; C.y[slot] = cy; C.z[slot] = cz;
     C.kx[slot] = kx; C.ky[slot] = ky; C.kz[slot] = kz;
     C.energy[slot] = energy; C.charge[slot] = charge; C.left_time[slot] = left_time;
     C.cell[slot] = pack_cell(i, j, k);
@@ -748,12 +964,28 @@ struct Flyer {
   }
   __device__ void load_cell_fields() {
     const int c = cell_index();
-    Rho = F.M.rho[c];
-    DA = F.M.da[c];
-    const double *f = (type == 0 ? F.M.efield : F.M.hfield) + 3 * (size_t)c;
-    Ex = f[0];
-    Ey = f[1];
-    Ez = f[2];
+    const DevMesh &M = F.M;
+    const double *f = (type == 0 ? M.efield : M.hfield) + 3 * (size_t)c;
+    Ex = (R)f[0];
+    Ey = (R)f[1];
+    Ez = (R)f[2];
+    if constexpr (sizeof(R) == 8) {
+      Rho = M.rho[c];
+      DA = M.da[c];
+    } else if (type == 0) {
+      // GetImpScRate / GetImpScGamma / EleImpScUpdateK's cell-dependent
+      // factors, evaluated once per cell in FP64
+      const DevTables &T = F.T;
+      const double rho = M.rho[c], da = M.da[c];
+      const bool on = (da * T.conc0 >= 1e22) && !(M.surface_scatter && M.surface_impurity && M.in_surf[c]);
+      const double eebeta = T.frickel * 4 * kPiD * rho / (2.0 * T.meld * T.eps_si);
+      const double fr = T.frickel * rho;
+      imp_a = on ? (R)(da * T.meld * sqrt(2.0 * T.meld) / (kPiD * (fr * fr))) : (R)0;
+      imp_b = on ? (R)(4.0 * T.melt / (eebeta * T.meld)) : (R)0;
+      imp_ecut = (R)(0.120 / T.eV0);
+      imp_emax = (R)(T.frickel * 4 * kPiD * rho / (8.0 * T.melt * T.eps_si));
+      imp_beta = (R)(T.frickel * 4 * kPiD * rho / T.eps_si);
+    }
   }
   // HitCell, src/CellHit.cpp:96-211.  Returns false when the particle would
   // leave the device through a PASS / GENERATE face on the outer y boundary.
@@ -767,7 +999,7 @@ struct Flyer {
     else if (imot == kScattOx) {
       if (F.M.surface_scatter) Reflect();
       else {
-        if (Random() > F.T.difpr[type]) Reflect();
+        if (Random() > (R)F.T.difpr[type]) Reflect();
         else Diffuse();
       }
     } else if (imot == kPeriod) Period();
@@ -797,13 +1029,13 @@ struct Flyer {
     }
     self = false;
     if (type == 0) {
-      const double drand = Random() * electron_rate_sum();
+      const R drand = Random() * electron_rate_sum();
       const int iscat = pick_electron_mechanism(drand);
       if (iscat < 0) { self = true; return; }
       if (((iscat % F.T.scpre) + 1) == F.T.scpre) ESCATII(iscat);
       else EPSCAT(iscat);
     } else {
-      const double drand = Random() * hole_rate_sum();
+      const R drand = Random() * hole_rate_sum();
       const int iscat = pick_hole_mechanism(drand);
       if (iscat < 0) { self = true; return; }
       if (((iscat % F.T.scprh) + 1) == F.T.scprh) HSCATII(iscat);
@@ -816,14 +1048,15 @@ struct Flyer {
   __device__ int fly() {
     catch_ = false;
     bool get_tet = true, get_cell = true, get_ph = true, get_imp = true, get_surf = true;
-    double ssnl = 0, imprnl = 0, phrnl = 0;
-    double TetTf = 0, CellTf = 0, PhScTf, ImpScTf, SurfScTf, Tf;
+    R ssnl = 0, imprnl = 0, phrnl = 0;
+    R TetTf = 0, CellTf = 0, PhScTf, ImpScTf, SurfScTf, Tf;
     bool too_far = false;
+    int zero_run = 0;
     load_cell_fields();
     iband = F.T.ibt[itet];
     GetV();
     int loop = 0;
-    const double dt = F.dt;
+    const R two_dt = (R)(2 * F.dt);
     surf_gamma = 0;
     imp_gamma = 0;
     while (left_time > 0) {
@@ -835,23 +1068,23 @@ struct Flyer {
       }
       if (get_tet) { TetTf = TetTime(); get_tet = false; }
       if (get_cell) { CellTf = CellTime(); get_cell = false; }
-      if (get_ph) { phrnl = -log(Random()); get_ph = false; }
-      const double g = F.T.gamtet[itet];
+      if (get_ph) { phrnl = -m_log(Random()); get_ph = false; }
+      const R g = TB::gamtet(F.T)[itet];
       PhScTf = phrnl / g;
       if (iband == F.T.bandof[0]) {
-        if (get_imp) { imprnl = -log(Random()); get_imp = false; }
+        if (get_imp) { imprnl = -m_log(Random()); get_imp = false; }
         imp_gamma = GetImpScGamma();
         ImpScTf = imprnl / imp_gamma;
       } else {
-        ImpScTf = 2 * dt;
-        imp_gamma = 1.0 / F.T.scrt0;
+        ImpScTf = two_dt;
+        imp_gamma = (R)(1.0 / F.T.scrt0);
       }
       if (F.M.surface_scatter && F.M.in_surf[cell_index()]) {
-        if (get_surf) { ssnl = -log(Random()); get_surf = false; }
+        if (get_surf) { ssnl = -m_log(Random()); get_surf = false; }
         GetSurfScRate();
-        SurfScTf = (surf_gamma > 0 && ssnl > 0) ? ssnl / surf_gamma : 2 * dt;
+        SurfScTf = (surf_gamma > 0 && ssnl > 0) ? ssnl / surf_gamma : two_dt;
       } else {
-        SurfScTf = 2 * dt;
+        SurfScTf = two_dt;
       }
       // Min(..., flag), src/Constant_GlobalVariable_MathFunction.cpp:92-118
       int flag = 1;
@@ -860,17 +1093,32 @@ struct Flyer {
       if (Tf > PhScTf) { Tf = PhScTf; flag = 3; }
       if (Tf > ImpScTf) { Tf = ImpScTf; flag = 4; }
       if (Tf > SurfScTf) { Tf = SurfScTf; flag = 5; }
-      if (Tf > left_time) { Tf = left_time; flag = 6; }
-      if (Tf < kMyZero) {
-        catch_ = true;
-        break;
+      if ((double)Tf > left_time) { Tf = (R)left_time; flag = 6; }
+      if constexpr (sizeof(R) == 8) {
+        if (Tf < kMyZero) {
+          catch_ = true;
+          break;
+        }
+      } else {
+        // float event times that round to zero (or below) are events now
+        if (!(Tf > (R)0)) {
+          Tf = 0;
+          if (++zero_run > kMaxZeroTimeEvents) {
+            count(F.Y, kCntZeroTime);
+            catch_ = true;
+            break;
+          }
+        } else {
+          zero_run = 0;
+        }
       }
       TetTf -= Tf;
       CellTf -= Tf;
       PhScTf -= Tf;
       ImpScTf -= Tf;
       SurfScTf -= Tf;
-      left_time -= Tf;
+      if (flag == 6) left_time = 0;  // Tf == left_time: the step is used up
+      else left_time -= Tf;
       phrnl -= g * Tf;
       imprnl -= imp_gamma * Tf;
       ssnl -= surf_gamma * Tf;
@@ -950,5 +1198,6 @@ struct Flyer {
     return 0;
   }
 };
+using Flyer = FlyerT<double>;
 
 }  // namespace mcb200

@@ -21,12 +21,14 @@ DEFAULT_TABLE_DIR = os.path.join(PKG_DIR, "tables")
 OK = 0
 COUNTER_NAMES = [
     "phonon", "impurity", "caught", "generated", "events", "unfinished", "too_many_events",
-    "child_overflow", "no_tet",
+    "child_overflow", "no_tet", "zero_time",
 ]
 NUM_COUNTERS = 16
 FLAG_SURFACE_SCATTER = 1
 FLAG_SURFACE_IMPURITY = 2
 FLAG_HEAT = 4
+FLIGHT_FP64 = 0
+FLIGHT_FP32 = 1
 UNIT_NAMES = ["T0", "eV0", "spr0", "time0", "conc0", "field0", "scrt0", "pot0", "a0pi", "sieg",
               "eps_silicon", "eps_oxide", "curr0", "dens0"]
 
@@ -94,6 +96,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mcb200_seed_particles.argtypes = [vp, c.c_size_t, i32p, dp, c.c_int, c.c_uint64]
     lib.mcb200_set_timing.argtypes = [vp, c.c_int]
     lib.mcb200_get_timing.argtypes = [vp, dp, c.c_int]
+    lib.mcb200_set_flight_precision.argtypes = [vp, c.c_int]
+    lib.mcb200_get_flight_precision.argtypes = [vp]
     return lib
 
 
@@ -135,7 +139,7 @@ class Engine:
     """One engine context: full-band tables, mesh, particles, tallies on one GPU."""
 
     def __init__(self, table_dir: str = DEFAULT_TABLE_DIR, kelvin: float = 300.0, device: int = 0,
-                 max_particles: int = 1 << 20):
+                 max_particles: int = 1 << 20, precision: int = FLIGHT_FP64):
         self._lib = lib()
         self._ctx = ctypes.c_void_p()
         rc = self._lib.mcb200_create(table_dir.encode(), kelvin, device, max_particles, ctypes.byref(self._ctx))
@@ -146,6 +150,8 @@ class Engine:
                 self._ctx = ctypes.c_void_p()
             raise EngineError(f"mcb200_create failed ({rc}): {msg}")
         self.mesh: Mesh | None = None
+        if precision != FLIGHT_FP64:
+            self.set_flight_precision(precision)
 
     def close(self):
         if self._ctx:
@@ -161,6 +167,15 @@ class Engine:
     def _check(self, rc: int, what: str):
         if rc != OK:
             raise EngineError(f"{what} failed ({rc}): {self._lib.mcb200_last_error(self._ctx).decode()}")
+
+    def set_flight_precision(self, precision: int):
+        """FLIGHT_FP64 (reference arithmetic) or FLIGHT_FP32 (float kinematics,
+        56-byte store); only while the store is empty."""
+        self._check(self._lib.mcb200_set_flight_precision(self._ctx, precision), "mcb200_set_flight_precision")
+
+    @property
+    def precision(self) -> int:
+        return self._lib.mcb200_get_flight_precision(self._ctx)
 
     def units(self) -> dict:
         out = np.zeros(len(UNIT_NAMES))

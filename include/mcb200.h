@@ -66,6 +66,7 @@ typedef struct {
 #define MCB200_CNT_TOO_MANY 6      /* particles over the per-step event cap */
 #define MCB200_CNT_CHILD_OVERFLOW 7
 #define MCB200_CNT_NO_TET 8        /* tetrahedron search failed (particle caught) */
+#define MCB200_CNT_ZERO_TIME 9     /* FP32 flight: stuck on zero-length events (particle caught) */
 #define MCB200_NUM_COUNTERS 16
 
 /* Build the full-band tables from `table_dir` (the reference's input/
@@ -78,6 +79,23 @@ typedef struct {
 int mcb200_create(const char *table_dir, double kelvin, int device, size_t max_particles, mcb200_ctx **out);
 void mcb200_destroy(mcb200_ctx *ctx);
 const char *mcb200_last_error(const mcb200_ctx *ctx);
+
+/* Flight precision of the context's particle store.
+ *  MCB200_FLIGHT_FP64: the reference's arithmetic (IEEE double, reference
+ *    operand order; 80 bytes per particle).  The default.
+ *  MCB200_FLIGHT_FP32: flight kinematics and rate lookups in float --
+ *    positions relative to the cell's low corner, k, velocities, fields,
+ *    event times, band and rate tables -- with energy, charge and the
+ *    remaining step time in double and the tallies in int64 fixed point
+ *    (56 bytes per particle).  Draws come from the float stream of
+ *    include/mcb200_rng.h, so results agree with FP64 statistically.
+ * No counterpart in the reference (it flies in double only).  Only allowed
+ * while the store is empty (before upload / seed); the particle buffers are
+ * reallocated.  Host-side particle arrays stay FP64 in both precisions. */
+#define MCB200_FLIGHT_FP64 0
+#define MCB200_FLIGHT_FP32 1
+int mcb200_set_flight_precision(mcb200_ctx *ctx, int precision);
+int mcb200_get_flight_precision(const mcb200_ctx *ctx);
 
 /* Normalisation scales (MeshQuantities::init_phpysical_parameter,
  * src/mcmodel.cpp:4007-4122): out[0..n) = T0, eV0, spr0, time0, conc0,

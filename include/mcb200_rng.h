@@ -18,6 +18,12 @@
  *   bits    = ((hi << 32) | lo) >> 12                 (52 bits)
  *   u       = (bits + 0.5) * 2^-52                    in (0, 1), never 0 or 1
  *
+ * The FP32 flight path draws floats from the same blocks, four per block:
+ *   block   = Philox4x32-10({ n >> 2, uid, step, sub }, key)
+ *   w       = word (n & 3) of the block
+ *   u       = ((w >> 9) + 0.5) * 2^-23                in (0, 1), never 0 or 1
+ * (23 random bits; every value is exactly representable as a float).
+ *
  * `sub` separates streams of the same particle within one step: 0 for the
  * particle's own flight, other values for particles created mid-step and for
  * the per-cell refresh draws.  Everything here is integer arithmetic plus one
@@ -88,6 +94,19 @@ MCB200_HD double mcb200_uniform(uint64_t seed, uint32_t uid, uint32_t step, uint
   mcb200_philox_block b = mcb200_philox4x32_10(n >> 1, uid, step, sub, (uint32_t)seed,
                                                (uint32_t)(seed >> 32));
   return (n & 1u) ? mcb200_bits_to_unit(b.w[3], b.w[2]) : mcb200_bits_to_unit(b.w[1], b.w[0]);
+}
+
+/* One 32-bit word -> a float in (0,1): 23 random bits centred in their bin. */
+MCB200_HD float mcb200_bits_to_unit_f32(uint32_t w) {
+  return ((float)(w >> 9) + 0.5f) * (1.0f / 8388608.0f); /* 2^-23 */
+}
+
+/* Draw number n of the FP32 stream (seed, uid, step, sub). */
+MCB200_HD float mcb200_uniform_f32(uint64_t seed, uint32_t uid, uint32_t step, uint32_t sub,
+                                   uint32_t n) {
+  mcb200_philox_block b = mcb200_philox4x32_10(n >> 2, uid, step, sub, (uint32_t)seed,
+                                               (uint32_t)(seed >> 32));
+  return mcb200_bits_to_unit_f32(b.w[n & 3u]);
 }
 
 #endif /* MCB200_RNG_H */
