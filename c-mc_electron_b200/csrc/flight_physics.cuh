@@ -152,6 +152,18 @@ struct FlyerT {
   bool catch_, self;
   R rough_rate, sphon_rate, surf_gamma, imp_gamma;
   int nchild;
+  // Work left by an event handler for the shared tails of the event loop
+  // (one call site each for the mechanism search, the final-state draw and
+  // the k-point search; see run_pick / run_final_state / run_locate).
+  bool pick_pending;
+  R pick_drand;
+  int fs_kind, fs_tal;  // pending final-state draw: kind and wedge rule
+  double fs_eeold;      // state before the draw (restored on self-scattering)
+  R fs_kx, fs_ky, fs_kz;
+  int fs_ib, fs_it, fs_is;
+  int loc_mode;         // pending k-point search
+  enum : int { kFsNone = 0, kFsPhonon = 1, kFsIonize = 2, kFsDiffuse = 3 };
+  enum : int { kLocNone = 0, kLocBZ = 1, kLocImpurity = 2 };
 
   __device__ FlyerT(const FlightCtxT<R> &f, const SymSmemT<R> &s) : F(f), S(s) {}
 
@@ -419,12 +431,13 @@ struct FlyerT {
     catch_ = true;
   }
 
-  // GetisymBZ, src/ParticleUtils.cpp:331-392: after a BZ-boundary crossing,
-  // search the BZ-surface tets of the particle's energy bin.
-  __device__ void GetisymBZ() {
+  // GetisymBZ, src/ParticleUtils.cpp:331-392, first part: after a
+  // BZ-boundary crossing, the current tet or one of the BZ-surface tets of
+  // the particle's energy bin; false leaves the search to Getisym.
+  __device__ bool bz_surface_search() {
     R a, b, c;
     in_wedge(a, b, c, kx, ky, kz);
-    if (iband == F.T.ibt[itet] && tet_contains(itet, a, b, c)) return;
+    if (iband == F.T.ibt[itet] && tet_contains(itet, a, b, c)) return true;
     int ie = (int)(energy * F.T.dlist);
     if (ie < 0) ie = 0;
     if (ie >= kMWLE) ie = kMWLE - 1;
@@ -433,13 +446,14 @@ struct FlyerT {
       const int it = F.T.slist[itl];
       if (iband == F.T.ibt[it] && tet_contains(it, a, b, c)) {
         itet = it;
-        return;
+        return true;
       }
     }
-    Getisym();
+    return false;
   }
 
-  // HitTet, src/TetHit.cpp:109-142.
+  // HitTet, src/TetHit.cpp:109-142.  After a BZ-boundary crossing the tet
+  // search and GetEnergy run in run_locate.
   __device__ void HitTet() {
     const int nb = (&F.T.tneib[itet].x)[itetdir];
     if (nb >= 0) {
@@ -450,12 +464,22 @@ struct FlyerT {
       ky = ky + S.bz[(1 * 5 + ii) * 48 + isym];
       kz = kz + S.bz[(2 * 5 + ii) * 48 + isym];
       isym = S.newisym[ii * 48 + isym];
-      GetisymBZ();
-      if (catch_) return;
-      GetEnergy();
+      loc_mode = kLocBZ;
     } else {
       isym = S.newisym[(-nb - 2) * 48 + isym];
     }
+  }
+
+  // The k-point search after a BZ crossing (GetisymBZ, then GetEnergy unless
+  // the particle was caught: src/TetHit.cpp:129-134) or after an accepted
+  // impurity event (Getisym, then GetEnergy:
+  // src/ElectronImpurityScatter.cpp:291-296).
+  __device__ void run_locate() {
+    const bool bz = loc_mode == kLocBZ;
+    loc_mode = kLocNone;
+    if (!(bz && bz_surface_search())) Getisym();
+    if (bz && catch_) return;
+    GetEnergy();
   }
 
   // TALIND, src/ParticleUtils.cpp:626-748: final valley (and a random wedge
@@ -623,54 +647,131 @@ struct FlyerT {
     tally_add_i64(heat + node(ic + 1, jc + 1, kc + 1), e * ry * rx * rz, kEnergyScale);
   }
 
-  // EPSCAT, src/ElectronPhononScatter.cpp:98-195 (Flag_QuantumCorrection = 0).
-  __device__ void EPSCAT(int iscat) {
-    const double eeold = energy;
-    const R xkold = kx, ykold = ky, zkold = kz;
-    const int ibold = iband, itetold = itet, isymold = isym;
+  // ---- final states ----------------------------------------------------
+  // The reference draws a final state inside EPSCAT / ESCATII (electrons),
+  // HPSCAT / HSCATII (holes) and Diffuse.  Here the event handlers set up the
+  // mechanism's band, energy and wedge rule (request_scatter,
+  // request_diffuse) and one shared tail, run_final_state, makes the draws
+  // in the reference's order (the wedge: TALIND or a random isym; then
+  // get_state) and applies the routine's epilogue.  One call site of
+  // get_state / TALIND / getK keeps the event loop small enough for the
+  // instruction cache.
+  __device__ void save_old() {
+    fs_eeold = energy;
+    fs_kx = kx; fs_ky = ky; fs_kz = kz;
+    fs_ib = iband; fs_it = itet; fs_is = isym;
+  }
+  __device__ void restore_k() {
+    kx = fs_kx; ky = fs_ky; kz = fs_kz;
+    iband = fs_ib; itet = fs_it; isym = fs_is;
+  }
+
+  // Set-up of EPSCAT (src/ElectronPhononScatter.cpp:98-195,
+  // Flag_QuantumCorrection = 0), ESCATII (:406-497, seciifl = false), HPSCAT
+  // (src/HolePhononScatter.cpp:86-146) and HSCATII (:149-234) for mechanism
+  // iscat: the final band and energy, and the wedge rule of the draw
+  // (fs_tal: 1..3 = TALIND(ityp), 0 = a random isym, -1 = none).
+  __device__ void request_scatter(int iscat) {
+    save_old();
     const DevTables &T = F.T;
-    iband = iscat / T.scpre + T.bandof[0];
-    switch (iscat % T.scpre) {
-      case 0: TALIND(1); break;
-      case 1: energy = energy + T.temptag; TALIND(2); break;
-      case 2: energy = energy - T.temptag; TALIND(2); break;
-      case 3: energy = energy + T.templag; TALIND(2); break;
-      case 4: energy = energy - T.templag; TALIND(2); break;
-      case 5: energy = energy + T.templog; TALIND(2); break;
-      case 6: energy = energy - T.templog; TALIND(2); break;
-      case 7: energy = energy + T.temptaf; TALIND(3); break;
-      case 8: energy = energy - T.temptaf; TALIND(3); break;
-      case 9: energy = energy + T.templaf; TALIND(3); break;
-      case 10: energy = energy - T.templaf; TALIND(3); break;
-      case 11: energy = energy + T.temptof; TALIND(3); break;
-      case 12: energy = energy - T.temptof; TALIND(3); break;
-      default: break;
+    if (type == 0) {
+      iband = iscat / T.scpre + T.bandof[0];
+      const int m = iscat % T.scpre;
+      if (m + 1 == T.scpre) {  // ESCATII
+        fs_kind = kFsIonize;
+        fs_tal = 0;
+        energy = (energy - T.sieg) / 3.0;
+        return;
+      }
+      fs_kind = kFsPhonon;
+      switch (m) {
+        case 0: fs_tal = 1; break;
+        case 1: energy = energy + T.temptag; fs_tal = 2; break;
+        case 2: energy = energy - T.temptag; fs_tal = 2; break;
+        case 3: energy = energy + T.templag; fs_tal = 2; break;
+        case 4: energy = energy - T.templag; fs_tal = 2; break;
+        case 5: energy = energy + T.templog; fs_tal = 2; break;
+        case 6: energy = energy - T.templog; fs_tal = 2; break;
+        case 7: energy = energy + T.temptaf; fs_tal = 3; break;
+        case 8: energy = energy - T.temptaf; fs_tal = 3; break;
+        case 9: energy = energy + T.templaf; fs_tal = 3; break;
+        case 10: energy = energy - T.templaf; fs_tal = 3; break;
+        case 11: energy = energy + T.temptof; fs_tal = 3; break;
+        case 12: energy = energy - T.temptof; fs_tal = 3; break;
+        default: fs_tal = -1; break;
+      }
+    } else {
+      iband = iscat / T.scprh + T.bandof[1];
+      const int m = iscat % T.scprh;
+      fs_tal = 0;
+      if (m + 1 == T.scprh) {  // HSCATII
+        fs_kind = kFsIonize;
+        energy = (energy - T.sieg) / 3.0;
+        return;
+      }
+      fs_kind = kFsPhonon;
+      if (m == 1) energy = energy + T.temphop;
+      else if (m == 2) energy = energy - T.temphop;
     }
+  }
+  // Set-up of Diffuse, src/CellHit.cpp:243-386 (TALIND(1), get_state, then
+  // the mirror that points the velocity back into the device).
+  __device__ void request_diffuse() {
+    save_old();
+    fs_kind = kFsDiffuse;
+    fs_tal = 1;
+  }
+  // The draws and epilogue of the pending final state.
+  __device__ void run_final_state() {
+    const int kind = fs_kind;
+    fs_kind = kFsNone;
+    if (fs_tal == 0) isym = ((int)((R)48 * Random()) % 48);
+    else if (fs_tal > 0) TALIND(fs_tal);
     get_state();
-    if (self) {
-      energy = eeold; kx = xkold; ky = ykold; kz = zkold;
-      iband = ibold; itet = itetold; isym = isymold;
+    if (kind == kFsDiffuse) {
+      if (self) restore_k();
+      GetV();
+      switch (idir) {
+        case kUp:
+          if (vx == (R)0) restore_k();
+          if (vx < (R)0) reflect_axis(0);
+          break;
+        case kRight:
+          if (vy == (R)0) restore_k();
+          if (vy > (R)0) reflect_axis(1);
+          break;
+        case kDown:
+          if (vx == (R)0) restore_k();
+          if (vx > (R)0) reflect_axis(0);
+          break;
+        case kLeft:
+          if (vy == (R)0) restore_k();
+          if (vy < (R)0) reflect_axis(1);
+          break;
+        case kFront:
+          if (vz == (R)0) restore_k();
+          if (vz < (R)0) reflect_axis(2);
+          break;
+        case kBack:
+          if (vz == (R)0) restore_k();
+          if (vz > (R)0) reflect_axis(2);
+          break;
+      }
+      return;
     }
-    if (F.M.heat) heat_to_point((energy - eeold) * fabs(charge), F.Y.heat_e);
+    if (self) {
+      energy = fs_eeold;
+      restore_k();
+    }
+    if (kind == kFsPhonon && F.M.heat)
+      heat_to_point((energy - fs_eeold) * fabs(charge), type == 0 ? F.Y.heat_e : F.Y.heat_h);
   }
 
-  // ESCATII, src/ElectronPhononScatter.cpp:406-497 (secondary generation off: seciifl = false).
-  __device__ void ESCATII(int iscat) {
-    const double eeold = energy;
-    const R xkold = kx, ykold = ky, zkold = kz;
-    const int ibold = iband, itetold = itet, isymold = isym;
-    iband = iscat / F.T.scpre + F.T.bandof[0];
-    energy = (energy - F.T.sieg) / 3.0;
-    isym = ((int)((R)48 * Random()) % 48);
-    get_state();
-    if (self) {
-      energy = eeold; kx = xkold; ky = ykold; kz = zkold;
-      iband = ibold; itet = itetold; isym = isymold;
-    }
-  }
-
-  // ElectronPhononScatter, src/ElectronPhononScatter.cpp:5-95.
-  __device__ void ElectronPhononScatter() {
+  // ElectronPhononScatter (src/ElectronPhononScatter.cpp:5-95) and
+  // HolePhononScatter (src/HolePhononScatter.cpp:4-83): real or
+  // self-scattering against the variable-gamma majorant; a real event
+  // leaves the mechanism search to run_pick.
+  __device__ void phonon_event() {
     const R scasum = CALSCATTSUM((R)energy, iband);
     const R g = TB::gamtet(F.T)[itet];
     const R drand = scasum > g ? Random() * scasum : Random() * g;
@@ -679,67 +780,19 @@ struct FlyerT {
       return;
     }
     self = false;
-    const int iscat = pick_electron_mechanism(drand);
+    pick_drand = drand;
+    pick_pending = true;
+  }
+  // The mechanism search of ElectronPhononScatter / HolePhononScatter
+  // (src/ElectronPhononScatter.cpp:47-63, src/HolePhononScatter.cpp:49-66).
+  __device__ void run_pick() {
+    pick_pending = false;
+    const int iscat = type == 0 ? pick_electron_mechanism(pick_drand) : pick_hole_mechanism(pick_drand);
     if (iscat < 0) {
       self = true;
       return;
     }
-    if (((iscat % F.T.scpre) + 1) == F.T.scpre) ESCATII(iscat);
-    else EPSCAT(iscat);
-  }
-
-  // HPSCAT, src/HolePhononScatter.cpp:86-146.
-  __device__ void HPSCAT(int iscat) {
-    const double eeold = energy;
-    const R xkold = kx, ykold = ky, zkold = kz;
-    const int ibold = iband, itetold = itet, isymold = isym;
-    iband = iscat / F.T.scprh + F.T.bandof[1];
-    switch (iscat % F.T.scprh) {
-      case 1: energy = energy + F.T.temphop; break;
-      case 2: energy = energy - F.T.temphop; break;
-      default: break;
-    }
-    isym = ((int)((R)48 * Random()) % 48);
-    get_state();
-    if (self) {
-      energy = eeold; kx = xkold; ky = ykold; kz = zkold;
-      iband = ibold; itet = itetold; isym = isymold;
-    }
-    if (F.M.heat) heat_to_point((energy - eeold) * fabs(charge), F.Y.heat_h);
-  }
-
-  // HSCATII, src/HolePhononScatter.cpp:149-234 (seciifl = false).
-  __device__ void HSCATII(int iscat) {
-    const double eeold = energy;
-    const R xkold = kx, ykold = ky, zkold = kz;
-    const int ibold = iband, itetold = itet, isymold = isym;
-    iband = iscat / F.T.scprh + F.T.bandof[1];
-    energy = (energy - F.T.sieg) / 3.0;
-    isym = ((int)((R)48 * Random()) % 48);
-    get_state();
-    if (self) {
-      energy = eeold; kx = xkold; ky = ykold; kz = zkold;
-      iband = ibold; itet = itetold; isym = isymold;
-    }
-  }
-
-  // HolePhononScatter, src/HolePhononScatter.cpp:4-83.
-  __device__ void HolePhononScatter() {
-    const R scasum = CALSCATTSUM((R)energy, iband);
-    const R g = TB::gamtet(F.T)[itet];
-    const R drand = scasum > g ? Random() * scasum : Random() * g;
-    if (scasum < drand) {
-      self = true;
-      return;
-    }
-    self = false;
-    const int iscat = pick_hole_mechanism(drand);
-    if (iscat < 0) {
-      self = true;
-      return;
-    }
-    if (((iscat % F.T.scprh) + 1) == F.T.scprh) HSCATII(iscat);
-    else HPSCAT(iscat);
+    request_scatter(iscat);
   }
 
   // GetImpScRate, src/ElectronImpurityScatter.cpp:62-126 (Brooks-Herring,
@@ -814,8 +867,6 @@ struct FlyerT {
     else if (idir == kRight || idir == kLeft) reflect_axis(1);
     else if (idir == kFront || idir == kBack) reflect_axis(2);
   }
-  // Diffuse, src/CellHit.cpp:243-386.
-  __device__ void Diffuse();
   __device__ bool inside_mesh(int i, int j, int k) const {
     return i >= 0 && j >= 0 && k >= 0 && i < F.M.nx && j < F.M.ny && k < F.M.nz;
   }
@@ -1000,7 +1051,7 @@ struct FlyerT {
       if (F.M.surface_scatter) Reflect();
       else {
         if (Random() > (R)F.T.difpr[type]) Reflect();
-        else Diffuse();
+        else request_diffuse();
       }
     } else if (imot == kPeriod) Period();
     else if (imot == kGenerate || imot == kGenRef) {
@@ -1021,32 +1072,24 @@ struct FlyerT {
   }
   // ParticleSurfaceScatter, src/ParSurfaceScatter.cpp:48-61, with the
   // surface-phonon branches' drand defined (see file note).
-  __device__ void ParticleSurfaceScatter() {
+  __device__ void surface_event() {
     if (Random() * surf_gamma < rough_rate) {
       idir = F.M.surface_dir[min(max(F.M.nearest_surf[cell_index()], 0), kMaxSurfaces - 1)];
-      Diffuse();
+      request_diffuse();
       return;
     }
     self = false;
-    if (type == 0) {
-      const R drand = Random() * electron_rate_sum();
-      const int iscat = pick_electron_mechanism(drand);
-      if (iscat < 0) { self = true; return; }
-      if (((iscat % F.T.scpre) + 1) == F.T.scpre) ESCATII(iscat);
-      else EPSCAT(iscat);
-    } else {
-      const R drand = Random() * hole_rate_sum();
-      const int iscat = pick_hole_mechanism(drand);
-      if (iscat < 0) { self = true; return; }
-      if (((iscat % F.T.scprh) + 1) == F.T.scprh) HSCATII(iscat);
-      else HPSCAT(iscat);
-    }
+    pick_drand = Random() * (type == 0 ? electron_rate_sum() : hole_rate_sum());
+    pick_pending = true;
   }
 
   // One particle, one step: particle_fly, src/mcmodel.cpp:1874-2161.
   // Returns 0 done, 1 caught, 2 unfinished (outer-boundary PASS).
   __device__ int fly() {
     catch_ = false;
+    pick_pending = false;
+    fs_kind = kFsNone;
+    loc_mode = kLocNone;
     bool get_tet = true, get_cell = true, get_ph = true, get_imp = true, get_surf = true;
     R ssnl = 0, imprnl = 0, phrnl = 0;
     R TetTf = 0, CellTf = 0, PhScTf, ImpScTf, SurfScTf, Tf;
@@ -1157,32 +1200,39 @@ struct FlyerT {
           }
           break;
         case 3:
-          if (type == 0) ElectronPhononScatter();
-          else HolePhononScatter();
-          if (!self) {
-            get_tet = true;
-            get_cell = true;
-            count(F.Y, kCntPhonon);
-          }
-          get_ph = true;
+          phonon_event();
           break;
         case 4:
           if (type == 0) ElectronImpurityScatter();
-          if (!self) {
-            get_tet = true;
-            get_cell = true;
-            count(F.Y, kCntImpurity);
-          }
-          get_imp = true;
           break;
         case 5:
-          ParticleSurfaceScatter();
-          if (!self) {
-            get_tet = true;
-            get_cell = true;
-          }
-          get_surf = true;
+          surface_event();
           break;
+      }
+      // shared tails: mechanism search, final-state draw, k-point search
+      if (pick_pending) run_pick();
+      if (fs_kind != kFsNone) run_final_state();
+      if (loc_mode != kLocNone) run_locate();
+      if (flag == 3) {
+        if (!self) {
+          get_tet = true;
+          get_cell = true;
+          count(F.Y, kCntPhonon);
+        }
+        get_ph = true;
+      } else if (flag == 4) {
+        if (!self) {
+          get_tet = true;
+          get_cell = true;
+          count(F.Y, kCntImpurity);
+        }
+        get_imp = true;
+      } else if (flag == 5) {
+        if (!self) {
+          get_tet = true;
+          get_cell = true;
+        }
+        get_surf = true;
       }
       if (too_far || catch_) break;
     }

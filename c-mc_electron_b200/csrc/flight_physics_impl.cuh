@@ -274,53 +274,10 @@ __device__ void FlyerT<R>::EleImpScUpdateK() {
     xkl = xkl + (R)0.85 * (R)T.a0pi;
     out_wedge(kx, ky, kz, xkl, ykl, zkl);
     CONFBZ(kx, ky, kz);
-    Getisym();
-    GetEnergy();
+    loc_mode = kLocImpurity;  // Getisym + GetEnergy in run_locate
     self = false;
   } else {
     self = true;
-  }
-}
-
-// Diffuse, src/CellHit.cpp:243-386: random state on the iso-energy surface,
-// then mirrored so the velocity points back into the device.
-template <typename R>
-__device__ void FlyerT<R>::Diffuse() {
-  const int ibandold = iband, itetold = itet, isymold = isym;
-  const R xkold = kx, ykold = ky, zkold = kz;
-  TALIND(1);
-  get_state();
-  auto restore = [&]() {
-    iband = ibandold; itet = itetold; isym = isymold;
-    kx = xkold; ky = ykold; kz = zkold;
-  };
-  if (self) restore();
-  GetV();
-  switch (idir) {
-    case kUp:
-      if (vx == (R)0) restore();
-      if (vx < (R)0) reflect_axis(0);
-      break;
-    case kRight:
-      if (vy == (R)0) restore();
-      if (vy > (R)0) reflect_axis(1);
-      break;
-    case kDown:
-      if (vx == (R)0) restore();
-      if (vx > (R)0) reflect_axis(0);
-      break;
-    case kLeft:
-      if (vy == (R)0) restore();
-      if (vy < (R)0) reflect_axis(1);
-      break;
-    case kFront:
-      if (vz == (R)0) restore();
-      if (vz < (R)0) reflect_axis(2);
-      break;
-    case kBack:
-      if (vz == (R)0) restore();
-      if (vz > (R)0) reflect_axis(2);
-      break;
   }
 }
 

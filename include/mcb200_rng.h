@@ -62,6 +62,12 @@ MCB200_HD void mcb200_mulhilo32(uint32_t a, uint32_t b, uint32_t *hi, uint32_t *
 MCB200_HD mcb200_philox_block mcb200_philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2,
                                                    uint32_t c3, uint32_t k0, uint32_t k1) {
   mcb200_philox_block r;
+#if defined(__CUDA_ARCH__)
+  /* kept rolled on the device: the block is computed at many call sites of
+     the flight loop, and ten unrolled rounds at each would crowd the
+     instruction cache */
+#pragma unroll 1
+#endif
   for (int round = 0; round < 10; ++round) {
     uint32_t hi0, lo0, hi1, lo1;
     mcb200_mulhilo32(MCB200_PHILOX_M0, c0, &hi0, &lo0);
