@@ -120,6 +120,10 @@ struct DevMesh {
   const double *rho;            // [cells] screening density |q|/vol (compute_cell_charge)
   const double *da;             // [cells] ionised doping density
   const double *e_rough, *e_sphon, *h_rough, *h_sphon;  // [cells] surface rates
+  // FP32 flight: per cell, (electron-felt field, bh_a), (hole-felt field,
+  // bh_b), (bh_emax, bh_beta, bh_ecut, 0) -- the fields and the
+  // Brooks-Herring factors in float, rebuilt before each FP32 step
+  const float4 *cell32;         // [cells][3]
   int surface_dir[kMaxSurfaces];
   int surface_scatter;          // Flag_SurfaceScatter
   int surface_impurity;         // Flag_SurfaceImpurityScatter

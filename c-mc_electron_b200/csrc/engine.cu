@@ -106,6 +106,8 @@ struct mcb200_ctx {
   uint8_t *child_alive = nullptr;
   uint32_t *child_uids = nullptr;
   unsigned int *append_count = nullptr;
+  unsigned int *tickets = nullptr;  // work counters of the persistent flight launches (main + generations)
+  float4 *cell32 = nullptr;         // FP32 flight's per-cell records (mesh-sized)
   // tallies
   DevTallies y{};
   // sort scratch
@@ -488,6 +490,7 @@ int mcb200_create(const char *table_dir, double kelvin, int device, size_t max_p
     c->child_alive = dalloc<uint8_t>(all_children, c->owned);
     c->child_uids = dalloc<uint32_t>(all_children, c->owned);
     c->append_count = dalloc<unsigned int>(1, c->owned);
+    c->tickets = dalloc<unsigned int>(1 + mcb200_ctx::kGenerations, c->owned);
     c->y.counters = dalloc<unsigned long long>(kCntNumCounters, c->owned);
     c->y.contact = dalloc<long long>(kMaxContacts * 6, c->owned);
     c->total = dalloc<unsigned int>(1, c->owned);
@@ -629,6 +632,8 @@ int mcb200_set_mesh(mcb200_ctx *c, int nx, int ny, int nz, const double *lx, con
     c->y.rcurrent = dalloc<long long>(ny + 1, c->mesh_owned);
     c->y.heat_e = dalloc<long long>(nodes, c->mesh_owned);
     c->y.heat_h = dalloc<long long>(nodes, c->mesh_owned);
+    c->cell32 = dalloc<float4>(cells * 3, c->mesh_owned);
+    m.cell32 = c->cell32;
     c->hist = dalloc<unsigned int>(cells, c->mesh_owned);
     c->offsets = dalloc<unsigned int>(cells, c->mesh_owned);
     c->tile_sums = dalloc<unsigned int>((cells + 1023) / 1024 + 1, c->mesh_owned);
@@ -1160,13 +1165,17 @@ void step_impl(mcb200_ctx *c, uint32_t step, uint64_t seed, double dt) {
   F.dt = dt;
   F.seed = seed;
   F.step = step;
-  const int block = 256;
   if (c->timing) ck(cudaEventRecord(c->ev[0], s), "event");
+  ck(cudaMemsetAsync(c->tickets, 0, sizeof(unsigned int) * (1 + mcb200_ctx::kGenerations), s), "memset");
+  if constexpr (sizeof(R) == 4) {  // FP32 flight reads the fields as per-cell float records
+    launch_cell_records32(c->dt, c->mesh, c->cell32, c->ncells, s);
+    c->launches += 1;
+  }
   // 1. main flight; copies go to generation 0
   ck(cudaMemsetAsync(children<R>(c, 0).count, 0, sizeof(unsigned int), s), "memset");
   F.C = children<R>(c, 0);
   if (c->timing) ck(cudaEventRecord(c->ev[1], s), "event");
-  launch_flight(F, store<R>(c, c->cur), (int)c->n, grid_for(c, c->n, block), block, s);
+  launch_flight(F, store<R>(c, c->cur), (int)c->n, c->tickets, c->sm_count, s);
   ck(cudaGetLastError(), "flight kernel");
   if (c->timing) ck(cudaEventRecord(c->ev[2], s), "event");
   const size_t flown = c->n;
@@ -1187,7 +1196,7 @@ void step_impl(mcb200_ctx *c, uint32_t step, uint64_t seed, double dt) {
       F.C = children<R>(c, g);  // a fifth generation would overflow: counted, not flown
       F.C.capacity = 0;
     }
-    launch_child_flight(F, children<R>(c, g), grid_for(c, counts[g], block), block, s);
+    launch_child_flight(F, children<R>(c, g), (int)counts[g], c->tickets + 1 + g, c->sm_count, s);
     ck(cudaGetLastError(), "child flight kernel");
     c->launches += 1;
   }

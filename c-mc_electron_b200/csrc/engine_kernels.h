@@ -13,10 +13,16 @@ template <typename R>
 struct FlightCtxT;
 using FlightCtx = FlightCtxT<double>;
 
+// Persistent flight launches: `ticket` is a zeroed device counter the blocks
+// take particle indices from; n_hint bounds the children a generation holds.
 template <typename R>
-void launch_flight(const FlightCtxT<R> &F, const DevParticlesT<R> &P, int n, int grid, int block, cudaStream_t s);
+void launch_flight(const FlightCtxT<R> &F, const DevParticlesT<R> &P, int n, unsigned int *ticket, int sm_count,
+                   cudaStream_t s);
 template <typename R>
-void launch_child_flight(const FlightCtxT<R> &F, const DevChildrenT<R> &in, int grid, int block, cudaStream_t s);
+void launch_child_flight(const FlightCtxT<R> &F, const DevChildrenT<R> &in, int n_hint, unsigned int *ticket,
+                         int sm_count, cudaStream_t s);
+// FP32 flight's per-cell records (DevMesh::cell32), [cells][3] float4.
+void launch_cell_records32(const DevTables &T, const DevMesh &M, float4 *out, int cells, cudaStream_t s);
 template <typename R>
 void launch_child_keys(const DevChildrenT<R> &c, int n, uint64_t *keys, uint8_t *alive, cudaStream_t s);
 void launch_child_rank(const uint64_t *keys, const uint8_t *alive, int n, uint32_t next_uid, uint32_t *uid_out,

@@ -11,11 +11,24 @@
 //   3. child_rank_kernel: copies get uids next_uid + rank of (parent, sub).
 //   4. cell_histogram / cell_scan / cell_scatter: survivors and copies are
 //      counting-sorted by cell into the second particle buffer.
+#include <algorithm>
+
 #include "engine_kernels.h"
 #include "flight_physics.cuh"
 #include "flight_physics_impl.cuh"
 
 namespace mcb200 {
+
+// Resident blocks of 256 threads per SM the flight kernels are compiled for
+// (the register budget per thread follows: 2 -> 128, 3 -> 80).
+#ifndef MCB200_FLIGHT_BLOCKS_F32
+#define MCB200_FLIGHT_BLOCKS_F32 2
+#endif
+#ifndef MCB200_FLIGHT_BLOCKS_F64
+#define MCB200_FLIGHT_BLOCKS_F64 2
+#endif
+template <typename R>
+constexpr int kFlightBlocks = sizeof(R) == 4 ? MCB200_FLIGHT_BLOCKS_F32 : MCB200_FLIGHT_BLOCKS_F64;
 
 constexpr uint32_t kMetaDead = 1u << 16;
 constexpr uint32_t kMetaUnfinished = 1u << 17;
@@ -29,14 +42,15 @@ __device__ void load_sym(SymSmemT<R> &S, const DevTables &T) {
   __syncthreads();
 }
 
+// Loading and storing the flown particles of the main store (StoreIO) and
+// of a child generation (ChildIO).
 template <typename R>
-__global__ void __launch_bounds__(256, 2) flight_kernel(FlightCtxT<R> F, DevParticlesT<R> P, int n) {
-  __shared__ SymSmemT<R> S;
-  load_sym(S, F.T);
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+struct StoreIO {
+  DevParticlesT<R> P;
+  double dt;
+  __device__ bool load(int p, FlyerT<R> &f) const {
     const uint32_t meta = P.meta[p];
-    if (meta & kMetaDead) continue;
-    FlyerT<R> f(F, S);
+    if (meta & kMetaDead) return false;
     f.x = P.x[p]; f.y = P.y[p]; f.z = P.z[p];
     f.kx = P.kx[p]; f.ky = P.ky[p]; f.kz = P.kz[p];
     f.energy = P.energy[p];
@@ -48,8 +62,10 @@ __global__ void __launch_bounds__(256, 2) flight_kernel(FlightCtxT<R> F, DevPart
     f.type = (meta >> 8) & 255;
     f.start_stream(P.uid[p], 0);
     f.nchild = 0;
-    f.left_time = F.dt;
-    const int r = f.fly();
+    f.left_time = dt;
+    return true;
+  }
+  __device__ void store(int p, const FlyerT<R> &f, int r) const {
     P.x[p] = f.x; P.y[p] = f.y; P.z[p] = f.z;
     P.kx[p] = f.kx; P.ky[p] = f.ky; P.kz[p] = f.kz;
     P.energy[p] = f.energy;
@@ -60,40 +76,121 @@ __global__ void __launch_bounds__(256, 2) flight_kernel(FlightCtxT<R> F, DevPart
     if (r == 2) m |= kMetaUnfinished;
     P.meta[p] = m;
   }
+};
+template <typename R>
+struct ChildIO {
+  DevChildrenT<R> C;
+  __device__ bool load(int p, FlyerT<R> &f) const {
+    f.x = C.x[p]; f.y = C.y[p]; f.z = C.z[p];
+    f.kx = C.kx[p]; f.ky = C.ky[p]; f.kz = C.kz[p];
+    f.energy = C.energy[p];
+    f.charge = C.charge[p];
+    const uint32_t c = C.cell[p];
+    f.ic = c & 1023; f.jc = (c >> 10) & 1023; f.kc = (c >> 20) & 1023;
+    f.itet = C.itet[p];
+    f.isym = C.meta[p] & 255;
+    f.type = (C.meta[p] >> 8) & 255;
+    f.start_stream(C.parent_uid[p], C.sub[p]);
+    f.nchild = 0;
+    f.left_time = C.left_time[p];
+    return true;
+  }
+  __device__ void store(int p, const FlyerT<R> &f, int r) const {
+    C.x[p] = f.x; C.y[p] = f.y; C.z[p] = f.z;
+    C.kx[p] = f.kx; C.ky[p] = f.ky; C.kz[p] = f.kz;
+    C.energy[p] = f.energy;
+    C.cell[p] = pack_cell(f.ic, f.jc, f.kc);
+    C.itet[p] = f.itet;
+    uint32_t m = (uint32_t)f.isym | ((uint32_t)f.type << 8);
+    if (r == 1) m |= kMetaDead;
+    if (r == 2) m |= kMetaUnfinished;
+    C.meta[p] = m;
+  }
+};
+
+// Persistent flight: each lane holds one particle at a time and advances it
+// one event per pass; a lane whose particle has finished its step stores it
+// and takes the next particle index from `ticket` (one atomic per warp for
+// all lanes that need work).  Lanes therefore stay busy while the warp's
+// other particles finish, instead of idling until the slowest one is done.
+// Every particle's draws come from its own stream, so the result does not
+// depend on which lane flies it or when.
+template <typename R, class IO>
+__device__ __forceinline__ void fly_interleaved(const FlightCtxT<R> &F, const SymSmemT<R> &S, const IO &io, int n,
+                                                unsigned int *ticket) {
+  FlyerT<R> f(F, S);
+  const unsigned lane = threadIdx.x & 31u;
+  int p = -1;
+  bool exhausted = false;
+  for (;;) {
+    if (!exhausted) {
+      const unsigned need = __ballot_sync(0xffffffffu, p < 0);
+      if (need) {
+        const int leader = __ffs(need) - 1;
+        unsigned base = 0;
+        if ((int)lane == leader) base = atomicAdd(ticket, (unsigned)__popc(need));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if ((unsigned long long)base + __popc(need) >= (unsigned long long)n) exhausted = true;
+        if (p < 0) {
+          const unsigned q = base + __popc(need & ((1u << lane) - 1u));
+          if (q < (unsigned)n && io.load((int)q, f)) {
+            p = (int)q;
+            f.begin();
+            if (!(f.left_time > 0)) {
+              io.store(p, f, f.finish());
+              p = -1;
+            }
+          }
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, p >= 0)) {
+      if (exhausted) break;
+      continue;
+    }
+    if (p >= 0 && f.iterate()) {
+      io.store(p, f, f.finish());
+      p = -1;
+    }
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256, kFlightBlocks<R>) flight_kernel(FlightCtxT<R> F, DevParticlesT<R> P, int n,
+                                                        unsigned int *ticket) {
+  __shared__ SymSmemT<R> S;
+  load_sym(S, F.T);
+  fly_interleaved(F, S, StoreIO<R>{P, F.dt}, n, ticket);
 }
 
 // Copies made during the previous pass (buffer `in`) fly the rest of their
 // step; copies they make go to `F.C`.
 template <typename R>
-__global__ void __launch_bounds__(256, 2) child_flight_kernel(FlightCtxT<R> F, DevChildrenT<R> in) {
+__global__ void __launch_bounds__(256, kFlightBlocks<R>) child_flight_kernel(FlightCtxT<R> F, DevChildrenT<R> in,
+                                                              unsigned int *ticket) {
   __shared__ SymSmemT<R> S;
   load_sym(S, F.T);
-  const int n = min((int)*in.count, in.capacity);
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
-    FlyerT<R> f(F, S);
-    f.x = in.x[p]; f.y = in.y[p]; f.z = in.z[p];
-    f.kx = in.kx[p]; f.ky = in.ky[p]; f.kz = in.kz[p];
-    f.energy = in.energy[p];
-    f.charge = in.charge[p];
-    const uint32_t c = in.cell[p];
-    f.ic = c & 1023; f.jc = (c >> 10) & 1023; f.kc = (c >> 20) & 1023;
-    f.itet = in.itet[p];
-    f.isym = in.meta[p] & 255;
-    f.type = (in.meta[p] >> 8) & 255;
-    f.start_stream(in.parent_uid[p], in.sub[p]);
-    f.nchild = 0;
-    f.left_time = in.left_time[p];
-    const int r = f.fly();
-    in.x[p] = f.x; in.y[p] = f.y; in.z[p] = f.z;
-    in.kx[p] = f.kx; in.ky[p] = f.ky; in.kz[p] = f.kz;
-    in.energy[p] = f.energy;
-    in.cell[p] = pack_cell(f.ic, f.jc, f.kc);
-    in.itet[p] = f.itet;
-    uint32_t m = (uint32_t)f.isym | ((uint32_t)f.type << 8);
-    if (r == 1) m |= kMetaDead;
-    if (r == 2) m |= kMetaUnfinished;
-    in.meta[p] = m;
-  }
+  fly_interleaved(F, S, ChildIO<R>{in}, min((int)*in.count, in.capacity), ticket);
+}
+
+// FP32 flight's per-cell records (DevMesh::cell32): the fields in float and
+// the Brooks-Herring factors of GetImpScRate / GetImpScGamma /
+// EleImpScUpdateK (src/ElectronImpurityScatter.cpp:6-306) evaluated once per
+// cell in FP64 from the cell's screening density and doping.
+__global__ void cell_records32_kernel(DevTables T, DevMesh M, float4 *out, int cells) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cells) return;
+  const double rho = M.rho[c], da = M.da[c];
+  const bool on = (da * T.conc0 >= 1e22) && !(M.surface_scatter && M.surface_impurity && M.in_surf[c]);
+  const double eebeta = T.frickel * 4 * kPiD * rho / (2.0 * T.meld * T.eps_si);
+  const double fr = T.frickel * rho;
+  const float bh_a = on ? (float)(da * T.meld * sqrt(2.0 * T.meld) / (kPiD * (fr * fr))) : 0.0f;
+  const float bh_b = on ? (float)(4.0 * T.melt / (eebeta * T.meld)) : 0.0f;
+  const double *e = M.efield + 3 * (size_t)c, *h = M.hfield + 3 * (size_t)c;
+  out[3 * (size_t)c + 0] = make_float4((float)e[0], (float)e[1], (float)e[2], bh_a);
+  out[3 * (size_t)c + 1] = make_float4((float)h[0], (float)h[1], (float)h[2], bh_b);
+  out[3 * (size_t)c + 2] = make_float4((float)(T.frickel * 4 * kPiD * rho / (8.0 * T.melt * T.eps_si)),
+                                       (float)(T.frickel * 4 * kPiD * rho / T.eps_si), (float)(0.120 / T.eV0), 0.0f);
 }
 
 // uid of each surviving copy: next_uid + number of surviving copies with a
@@ -277,13 +374,32 @@ void launch_seed(const FlightCtx &F, const DevParticlesT<R> &P, int offset, int 
                  const double *charge, int type, uint32_t uid0, int grid, cudaStream_t s) {
   if (n > 0) seed_kernel<R><<<grid, 256, 0, s>>>(F, P, offset, n, cell_of, charge, type, uid0);
 }
+// Blocks of the persistent flight kernels: enough to fill every SM at the
+// kernel's occupancy, fewer when there are fewer particles than threads.
 template <typename R>
-void launch_flight(const FlightCtxT<R> &F, const DevParticlesT<R> &P, int n, int grid, int block, cudaStream_t s) {
-  if (n > 0) flight_kernel<R><<<grid, block, 0, s>>>(F, P, n);
+int flight_grid(int n, int block, int sm_count) {
+  static int per_sm = 0;
+  if (per_sm == 0) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, flight_kernel<R>, block, 0) != cudaSuccess || b < 1) b = 1;
+    per_sm = b;
+  }
+  const long long want = ((long long)n + block - 1) / block;
+  return (int)std::max<long long>(1, std::min<long long>(want, (long long)per_sm * sm_count));
+}
+
+template <typename R>
+void launch_flight(const FlightCtxT<R> &F, const DevParticlesT<R> &P, int n, unsigned int *ticket, int sm_count,
+                   cudaStream_t s) {
+  if (n > 0) flight_kernel<R><<<flight_grid<R>(n, 256, sm_count), 256, 0, s>>>(F, P, n, ticket);
 }
 template <typename R>
-void launch_child_flight(const FlightCtxT<R> &F, const DevChildrenT<R> &in, int grid, int block, cudaStream_t s) {
-  child_flight_kernel<R><<<grid, block, 0, s>>>(F, in);
+void launch_child_flight(const FlightCtxT<R> &F, const DevChildrenT<R> &in, int n_hint, unsigned int *ticket,
+                         int sm_count, cudaStream_t s) {
+  child_flight_kernel<R><<<flight_grid<R>(n_hint, 256, sm_count), 256, 0, s>>>(F, in, ticket);
+}
+void launch_cell_records32(const DevTables &T, const DevMesh &M, float4 *out, int cells, cudaStream_t s) {
+  if (cells > 0) cell_records32_kernel<<<(cells + 255) / 256, 256, 0, s>>>(T, M, out, cells);
 }
 template <typename R>
 void launch_child_keys(const DevChildrenT<R> &c, int n, uint64_t *keys, uint8_t *alive, cudaStream_t s) {
@@ -323,8 +439,10 @@ void launch_cell_sort(const DevParticlesT<R> &src, int n, const DevParticlesT<R>
 #define MCB200_INSTANTIATE(R)                                                                                   \
   template void launch_seed<R>(const FlightCtx &, const DevParticlesT<R> &, int, int, const int *,            \
                                const double *, int, uint32_t, int, cudaStream_t);                             \
-  template void launch_flight<R>(const FlightCtxT<R> &, const DevParticlesT<R> &, int, int, int, cudaStream_t); \
-  template void launch_child_flight<R>(const FlightCtxT<R> &, const DevChildrenT<R> &, int, int, cudaStream_t); \
+  template void launch_flight<R>(const FlightCtxT<R> &, const DevParticlesT<R> &, int, unsigned int *, int,    \
+                                 cudaStream_t);                                                                 \
+  template void launch_child_flight<R>(const FlightCtxT<R> &, const DevChildrenT<R> &, int, unsigned int *, int, \
+                                       cudaStream_t);                                                           \
   template void launch_child_keys<R>(const DevChildrenT<R> &, int, uint64_t *, uint8_t *, cudaStream_t);       \
   template void launch_children_to_particles<R>(const DevChildrenT<R> &, int, const uint32_t *,               \
                                                 const uint8_t *, const DevParticlesT<R> &, int,                 \

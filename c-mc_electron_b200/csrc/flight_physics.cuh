@@ -1016,26 +1016,27 @@ struct FlyerT {
   __device__ void load_cell_fields() {
     const int c = cell_index();
     const DevMesh &M = F.M;
-    const double *f = (type == 0 ? M.efield : M.hfield) + 3 * (size_t)c;
-    Ex = (R)f[0];
-    Ey = (R)f[1];
-    Ez = (R)f[2];
     if constexpr (sizeof(R) == 8) {
+      const double *f = (type == 0 ? M.efield : M.hfield) + 3 * (size_t)c;
+      Ex = f[0];
+      Ey = f[1];
+      Ez = f[2];
       Rho = M.rho[c];
       DA = M.da[c];
-    } else if (type == 0) {
-      // GetImpScRate / GetImpScGamma / EleImpScUpdateK's cell-dependent
-      // factors, evaluated once per cell in FP64
-      const DevTables &T = F.T;
-      const double rho = M.rho[c], da = M.da[c];
-      const bool on = (da * T.conc0 >= 1e22) && !(M.surface_scatter && M.surface_impurity && M.in_surf[c]);
-      const double eebeta = T.frickel * 4 * kPiD * rho / (2.0 * T.meld * T.eps_si);
-      const double fr = T.frickel * rho;
-      imp_a = on ? (R)(da * T.meld * sqrt(2.0 * T.meld) / (kPiD * (fr * fr))) : (R)0;
-      imp_b = on ? (R)(4.0 * T.melt / (eebeta * T.meld)) : (R)0;
-      imp_ecut = (R)(0.120 / T.eV0);
-      imp_emax = (R)(T.frickel * 4 * kPiD * rho / (8.0 * T.melt * T.eps_si));
-      imp_beta = (R)(T.frickel * 4 * kPiD * rho / T.eps_si);
+    } else {
+      const float4 *r = M.cell32 + 3 * (size_t)c;
+      if (type == 0) {
+        const float4 a = r[0], b = r[1], m = r[2];
+        Ex = a.x; Ey = a.y; Ez = a.z;
+        imp_a = a.w;
+        imp_b = b.w;
+        imp_emax = m.x;
+        imp_beta = m.y;
+        imp_ecut = m.z;
+      } else {
+        const float4 b = r[1];
+        Ex = b.x; Ey = b.y; Ez = b.z;
+      }
     }
   }
   // HitCell, src/CellHit.cpp:96-211.  Returns false when the particle would
@@ -1083,159 +1084,172 @@ struct FlyerT {
     pick_pending = true;
   }
 
-  // One particle, one step: particle_fly, src/mcmodel.cpp:1874-2161.
-  // Returns 0 done, 1 caught, 2 unfinished (outer-boundary PASS).
-  __device__ int fly() {
+  // One particle, one step: particle_fly, src/mcmodel.cpp:1874-2161, split
+  // into begin (the set-up before the event loop), iterate (one pass of the
+  // loop; true when the particle's step is over) and finish (the tallies
+  // after the loop), so a kernel can interleave particles on one lane.
+  // Loop state (particle_fly's locals):
+  bool get_tet, get_cell, get_ph, get_imp, get_surf, too_far;
+  R ssnl, imprnl, phrnl, TetTf, CellTf;
+  int loop, zero_run;
+
+  __device__ void begin() {
     catch_ = false;
     pick_pending = false;
     fs_kind = kFsNone;
     loc_mode = kLocNone;
-    bool get_tet = true, get_cell = true, get_ph = true, get_imp = true, get_surf = true;
-    R ssnl = 0, imprnl = 0, phrnl = 0;
-    R TetTf = 0, CellTf = 0, PhScTf, ImpScTf, SurfScTf, Tf;
-    bool too_far = false;
-    int zero_run = 0;
+    get_tet = get_cell = get_ph = get_imp = get_surf = true;
+    ssnl = imprnl = phrnl = 0;
+    TetTf = CellTf = 0;
+    too_far = false;
+    zero_run = 0;
     load_cell_fields();
     iband = F.T.ibt[itet];
     GetV();
-    int loop = 0;
-    const R two_dt = (R)(2 * F.dt);
+    loop = 0;
     surf_gamma = 0;
     imp_gamma = 0;
-    while (left_time > 0) {
-      GetV();
-      if (++loop > kMaxEvents) {
-        count(F.Y, kCntTooManyEvents);
-        catch_ = true;
-        break;
-      }
-      if (get_tet) { TetTf = TetTime(); get_tet = false; }
-      if (get_cell) { CellTf = CellTime(); get_cell = false; }
-      if (get_ph) { phrnl = -m_log(Random()); get_ph = false; }
-      const R g = TB::gamtet(F.T)[itet];
-      PhScTf = phrnl / g;
-      if (iband == F.T.bandof[0]) {
-        if (get_imp) { imprnl = -m_log(Random()); get_imp = false; }
-        imp_gamma = GetImpScGamma();
-        ImpScTf = imprnl / imp_gamma;
-      } else {
-        ImpScTf = two_dt;
-        imp_gamma = (R)(1.0 / F.T.scrt0);
-      }
-      if (F.M.surface_scatter && F.M.in_surf[cell_index()]) {
-        if (get_surf) { ssnl = -m_log(Random()); get_surf = false; }
-        GetSurfScRate();
-        SurfScTf = (surf_gamma > 0 && ssnl > 0) ? ssnl / surf_gamma : two_dt;
-      } else {
-        SurfScTf = two_dt;
-      }
-      // Min(..., flag), src/Constant_GlobalVariable_MathFunction.cpp:92-118
-      int flag = 1;
-      Tf = TetTf;
-      if (Tf > CellTf) { Tf = CellTf; flag = 2; }
-      if (Tf > PhScTf) { Tf = PhScTf; flag = 3; }
-      if (Tf > ImpScTf) { Tf = ImpScTf; flag = 4; }
-      if (Tf > SurfScTf) { Tf = SurfScTf; flag = 5; }
-      if ((double)Tf > left_time) { Tf = (R)left_time; flag = 6; }
-      if constexpr (sizeof(R) == 8) {
-        if (Tf < kMyZero) {
-          catch_ = true;
-          break;
-        }
-      } else {
-        // float event times that round to zero (or below) are events now
-        if (!(Tf > (R)0)) {
-          Tf = 0;
-          if (++zero_run > kMaxZeroTimeEvents) {
-            count(F.Y, kCntZeroTime);
-            catch_ = true;
-            break;
-          }
-        } else {
-          zero_run = 0;
-        }
-      }
-      TetTf -= Tf;
-      CellTf -= Tf;
-      PhScTf -= Tf;
-      ImpScTf -= Tf;
-      SurfScTf -= Tf;
-      if (flag == 6) left_time = 0;  // Tf == left_time: the step is used up
-      else left_time -= Tf;
-      phrnl -= g * Tf;
-      imprnl -= imp_gamma * Tf;
-      ssnl -= surf_gamma * Tf;
-      kx += Ex * Tf;
-      ky += Ey * Tf;
-      kz += Ez * Tf;
-      energy += (vx * Ex + vy * Ey + vz * Ez) * Tf;
-      x += vx * Tf;
-      y += vy * Tf;
-      z += vz * Tf;
-      if (energy < 0) {
-        catch_ = true;
-        break;
-      }
-      switch (flag) {
-        case 1:
-          HitTet();
-          get_tet = true;
-          get_cell = true;
-          break;
-        case 2:
-          if (HitCell()) {
-            get_tet = true;
-            get_cell = true;
-          } else {
-            // trace_back, src/mcmodel.cpp:1774-1783
-            kx -= Ex * Tf;
-            ky -= Ey * Tf;
-            kz -= Ez * Tf;
-            energy -= (vx * Ex + vy * Ey + vz * Ez) * Tf;
-            x -= vx * Tf;
-            y -= vy * Tf;
-            z -= vz * Tf;
-            left_time += Tf;
-            too_far = true;
-          }
-          break;
-        case 3:
-          phonon_event();
-          break;
-        case 4:
-          if (type == 0) ElectronImpurityScatter();
-          break;
-        case 5:
-          surface_event();
-          break;
-      }
-      // shared tails: mechanism search, final-state draw, k-point search
-      if (pick_pending) run_pick();
-      if (fs_kind != kFsNone) run_final_state();
-      if (loc_mode != kLocNone) run_locate();
-      if (flag == 3) {
-        if (!self) {
-          get_tet = true;
-          get_cell = true;
-          count(F.Y, kCntPhonon);
-        }
-        get_ph = true;
-      } else if (flag == 4) {
-        if (!self) {
-          get_tet = true;
-          get_cell = true;
-          count(F.Y, kCntImpurity);
-        }
-        get_imp = true;
-      } else if (flag == 5) {
-        if (!self) {
-          get_tet = true;
-          get_cell = true;
-        }
-        get_surf = true;
-      }
-      if (too_far || catch_) break;
+  }
+
+  __device__ bool iterate() {
+    GetV();
+    if (++loop > kMaxEvents) {
+      count(F.Y, kCntTooManyEvents);
+      catch_ = true;
+      return true;
     }
+    if (get_tet) { TetTf = TetTime(); get_tet = false; }
+    if (get_cell) { CellTf = CellTime(); get_cell = false; }
+    if (get_ph) { phrnl = -m_log(Random()); get_ph = false; }
+    const R g = TB::gamtet(F.T)[itet];
+    R PhScTf, ImpScTf, SurfScTf, Tf;
+    PhScTf = phrnl / g;
+    if (iband == F.T.bandof[0]) {
+      if (get_imp) { imprnl = -m_log(Random()); get_imp = false; }
+      imp_gamma = GetImpScGamma();
+      ImpScTf = imprnl / imp_gamma;
+    } else {
+      ImpScTf = (R)(2 * F.dt);
+      imp_gamma = (R)(1.0 / F.T.scrt0);
+    }
+    if (F.M.surface_scatter && F.M.in_surf[cell_index()]) {
+      if (get_surf) { ssnl = -m_log(Random()); get_surf = false; }
+      GetSurfScRate();
+      SurfScTf = (surf_gamma > 0 && ssnl > 0) ? ssnl / surf_gamma : (R)(2 * F.dt);
+    } else {
+      SurfScTf = (R)(2 * F.dt);
+    }
+    // Min(..., flag), src/Constant_GlobalVariable_MathFunction.cpp:92-118
+    int flag = 1;
+    Tf = TetTf;
+    if (Tf > CellTf) { Tf = CellTf; flag = 2; }
+    if (Tf > PhScTf) { Tf = PhScTf; flag = 3; }
+    if (Tf > ImpScTf) { Tf = ImpScTf; flag = 4; }
+    if (Tf > SurfScTf) { Tf = SurfScTf; flag = 5; }
+    if ((double)Tf > left_time) { Tf = (R)left_time; flag = 6; }
+    if constexpr (sizeof(R) == 8) {
+      if (Tf < kMyZero) {
+        catch_ = true;
+        return true;
+      }
+    } else {
+      // float event times that round to zero (or below) are events now
+      if (!(Tf > (R)0)) {
+        Tf = 0;
+        if (++zero_run > kMaxZeroTimeEvents) {
+          count(F.Y, kCntZeroTime);
+          catch_ = true;
+          return true;
+        }
+      } else {
+        zero_run = 0;
+      }
+    }
+    TetTf -= Tf;
+    CellTf -= Tf;
+    PhScTf -= Tf;
+    ImpScTf -= Tf;
+    SurfScTf -= Tf;
+    if (flag == 6) left_time = 0;  // Tf == left_time: the step is used up
+    else left_time -= Tf;
+    phrnl -= g * Tf;
+    imprnl -= imp_gamma * Tf;
+    ssnl -= surf_gamma * Tf;
+    kx += Ex * Tf;
+    ky += Ey * Tf;
+    kz += Ez * Tf;
+    energy += (vx * Ex + vy * Ey + vz * Ez) * Tf;
+    x += vx * Tf;
+    y += vy * Tf;
+    z += vz * Tf;
+    if (energy < 0) {
+      catch_ = true;
+      return true;
+    }
+    switch (flag) {
+      case 1:
+        HitTet();
+        get_tet = true;
+        get_cell = true;
+        break;
+      case 2:
+        if (HitCell()) {
+          get_tet = true;
+          get_cell = true;
+        } else {
+          // trace_back, src/mcmodel.cpp:1774-1783
+          kx -= Ex * Tf;
+          ky -= Ey * Tf;
+          kz -= Ez * Tf;
+          energy -= (vx * Ex + vy * Ey + vz * Ez) * Tf;
+          x -= vx * Tf;
+          y -= vy * Tf;
+          z -= vz * Tf;
+          left_time += Tf;
+          too_far = true;
+        }
+        break;
+      case 3:
+        phonon_event();
+        break;
+      case 4:
+        if (type == 0) ElectronImpurityScatter();
+        break;
+      case 5:
+        surface_event();
+        break;
+    }
+    // shared tails: mechanism search, final-state draw, k-point search
+    if (pick_pending) run_pick();
+    if (fs_kind != kFsNone) run_final_state();
+    if (loc_mode != kLocNone) run_locate();
+    if (flag == 3) {
+      if (!self) {
+        get_tet = true;
+        get_cell = true;
+        count(F.Y, kCntPhonon);
+      }
+      get_ph = true;
+    } else if (flag == 4) {
+      if (!self) {
+        get_tet = true;
+        get_cell = true;
+        count(F.Y, kCntImpurity);
+      }
+      get_imp = true;
+    } else if (flag == 5) {
+      if (!self) {
+        get_tet = true;
+        get_cell = true;
+      }
+      get_surf = true;
+    }
+    if (too_far || catch_) return true;
+    return !(left_time > 0);
+  }
+
+  // Returns 0 done, 1 caught, 2 unfinished (outer-boundary PASS).
+  __device__ int finish() {
     atomicAdd(&F.Y.counters[kCntEvents], (unsigned long long)loop);
     if (catch_) {
       count(F.Y, kCntCaught);
@@ -1246,6 +1260,14 @@ struct FlyerT {
       return 2;
     }
     return 0;
+  }
+
+  __device__ int fly() {
+    begin();
+    if (left_time > 0)
+      while (!iterate()) {
+      }
+    return finish();
   }
 };
 using Flyer = FlyerT<double>;

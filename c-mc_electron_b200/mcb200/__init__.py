@@ -15,7 +15,8 @@ from dataclasses import dataclass
 import numpy as np
 
 PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-LIB_PATH = os.path.join(PKG_DIR, "libmcb200.so")
+# MCB200_LIBRARY selects another build of the engine library (a tuning variant).
+LIB_PATH = os.environ.get("MCB200_LIBRARY", os.path.join(PKG_DIR, "libmcb200.so"))
 DEFAULT_TABLE_DIR = os.path.join(PKG_DIR, "tables")
 
 OK = 0
