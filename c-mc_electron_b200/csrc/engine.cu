@@ -559,6 +559,7 @@ int mcb200_copy_table(const mcb200_ctx *c, const char *name, void *out, size_t b
   if (n == "ykk") { copy_vec(t.ykk, out, bytes, needed); return 0; }
   if (n == "zkk") { copy_vec(t.zkk, out, bytes, needed); return 0; }
   if (n == "eek") { copy_vec(t.eek, out, bytes, needed); return 0; }
+  if (n == "ni") { copy_vec(std::vector<double>{t.ni}, out, bytes, needed); return 0; }
   if (n == "ntlist") { copy_vec(t.ntlist, out, bytes, needed); return 0; }
   if (n == "ptlist") { copy_vec(t.ptlist, out, bytes, needed); return 0; }
   if (n == "tlist") { copy_vec(t.tlist, out, bytes, needed); return 0; }

@@ -62,6 +62,17 @@ PARTICLE_FIELDS = {
 }
 
 
+class DeckInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ("nx", "ny", "nz", "total_step", "electron_number", "hole_number",
+                                            "stat_step", "stat_heat_step", "heat_steps", "mr_step")] + \
+               [("temperature", ctypes.c_double), ("dt_s", ctypes.c_double)] + \
+               [(n, ctypes.c_int) for n in ("flag_multiple_refresh", "flag_compute_potential", "flag_compute_heat",
+                                            "flag_surface_scatter", "flag_surface_roughness", "flag_surface_phonon",
+                                            "flag_surface_impurity", "flag_restart", "n_contacts", "n_planes",
+                                            "n_surfaces", "default_electrons", "default_holes")] + \
+               [("output_dir", ctypes.c_char * 512), ("prepared", ctypes.c_int), ("dt", ctypes.c_double)]
+
+
 def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     if not os.path.exists(path):
         raise EngineError(f"{path} is missing: build it with `make -C c-mc_electron_b200` "
@@ -97,6 +108,16 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mcb200_seed_particles.argtypes = [vp, c.c_size_t, i32p, dp, c.c_int, c.c_uint64]
     lib.mcb200_set_timing.argtypes = [vp, c.c_int]
     lib.mcb200_get_timing.argtypes = [vp, dp, c.c_int]
+    lib.mcb200_deck_load.argtypes = [c.c_char_p, c.POINTER(vp)]
+    lib.mcb200_deck_free.argtypes = [vp]
+    lib.mcb200_deck_error.argtypes = [vp]
+    lib.mcb200_deck_error.restype = c.c_char_p
+    lib.mcb200_deck_get_info.argtypes = [vp, c.POINTER(DeckInfo)]
+    lib.mcb200_deck_int_array.argtypes = [vp, c.c_char_p, i32p, c.c_size_t, c.POINTER(c.c_size_t)]
+    lib.mcb200_deck_double_array.argtypes = [vp, c.c_char_p, dp, c.c_size_t, c.POINTER(c.c_size_t)]
+    lib.mcb200_deck_prepare.argtypes = [vp, vp]
+    lib.mcb200_apply_deck.argtypes = [vp, vp]
+    lib.mcb200_seed_deck.argtypes = [vp, vp, c.c_uint64]
     lib.mcb200_set_flight_precision.argtypes = [vp, c.c_int]
     lib.mcb200_get_flight_precision.argtypes = [vp]
     return lib
@@ -332,3 +353,68 @@ class Engine:
 
     def reset_tallies(self):
         self._check(self._lib.mcb200_reset_tallies(self._ctx), "reset_tallies")
+
+
+class Deck:
+    """A reference input deck (input.txt + lgrid.txt + ldg.txt) read by the
+    engine library's own parser (mcb200_deck_load)."""
+
+    def __init__(self, input_path: str):
+        self._lib = lib()
+        self._deck = ctypes.c_void_p()
+        rc = self._lib.mcb200_deck_load(os.fspath(input_path).encode(), ctypes.byref(self._deck))
+        if rc != OK:
+            msg = self._lib.mcb200_deck_error(self._deck).decode() if self._deck else "no deck"
+            self.close()
+            raise EngineError(f"mcb200_deck_load failed ({rc}): {msg}")
+
+    def close(self):
+        if self._deck:
+            self._lib.mcb200_deck_free(self._deck)
+            self._deck = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, what: str):
+        if rc != OK:
+            raise EngineError(f"{what} failed ({rc}): {self._lib.mcb200_deck_error(self._deck).decode()}")
+
+    def info(self) -> dict:
+        inf = DeckInfo()
+        self._check(self._lib.mcb200_deck_get_info(self._deck, ctypes.byref(inf)), "mcb200_deck_get_info")
+        out = {name: getattr(inf, name) for name, _ in DeckInfo._fields_}
+        out["output_dir"] = inf.output_dir.decode()
+        return out
+
+    def int_array(self, name: str) -> np.ndarray:
+        need = ctypes.c_size_t()
+        self._check(self._lib.mcb200_deck_int_array(self._deck, name.encode(), None, 0, ctypes.byref(need)), name)
+        out = np.empty(need.value, dtype=np.int32)
+        self._check(self._lib.mcb200_deck_int_array(self._deck, name.encode(), _ptr(out, ctypes.c_int32), out.size,
+                                                    ctypes.byref(need)), name)
+        return out
+
+    def double_array(self, name: str) -> np.ndarray:
+        need = ctypes.c_size_t()
+        self._check(self._lib.mcb200_deck_double_array(self._deck, name.encode(), None, 0, ctypes.byref(need)), name)
+        out = np.empty(need.value, dtype=np.float64)
+        self._check(self._lib.mcb200_deck_double_array(self._deck, name.encode(), _ptr(out, ctypes.c_double),
+                                                       out.size, ctypes.byref(need)), name)
+        return out
+
+    def prepare(self, engine: "Engine"):
+        self._check(self._lib.mcb200_deck_prepare(self._deck, engine._ctx), "mcb200_deck_prepare")
+
+    def apply(self, engine: "Engine"):
+        """Mesh, cells and device of the deck into `engine`."""
+        self._check(self._lib.mcb200_apply_deck(engine._ctx, self._deck), "mcb200_apply_deck")
+        lx, ly, lz = (self.double_array(n) for n in ("lx", "ly", "lz"))
+        engine.mesh = Mesh(len(lx) - 1, len(ly) - 1, len(lz) - 1, lx, ly, lz)
+
+    def seed(self, engine: "Engine", seed: int):
+        """The deck's initial ensemble (init_particle_data) into `engine`."""
+        self._check(self._lib.mcb200_seed_deck(engine._ctx, self._deck, seed), "mcb200_seed_deck")

@@ -106,3 +106,106 @@ def bulk_box(dirpath: str, nx=40, ny=20, nz=20, cell_nm=5.0, donor_m3=1e23, elec
                 ElectronNumber=electrons, HoleNumber=holes)
     return dict(input=os.path.join(dirpath, "input.txt"), grid=os.path.join(dirpath, "lgrid.txt"),
                 device=os.path.join(dirpath, "ldg.txt"))
+
+
+def finfet_grid():
+    """Node coordinates (nm) of the FinFET mesh: 80 x 50 x 40 cells.
+    x (height): 1 nm gate oxide in 0.5 nm cells, the 30 nm fin in 0.5 nm
+    cells, the substrate in 2 nm cells; y (transport): 10 nm source and
+    drain in 2 nm cells, the 20 nm channel in 0.5 nm cells; z (width): the
+    10 nm fin and its 1 nm oxides in 0.5 nm cells, 16 nm either side in 2 nm
+    cells."""
+    x = np.concatenate([[-1.0, -0.5], np.arange(0.0, 30.0001, 0.5), np.arange(32.0, 66.0001, 2.0)])
+    y = np.concatenate([np.arange(-20.0, -10.0, 2.0), np.arange(-10.0, 10.0001, 0.5), np.arange(12.0, 20.0001, 2.0)])
+    z = np.concatenate([np.arange(-17.0, -1.0, 2.0), [-1.0, -0.5], np.arange(0.0, 10.0001, 0.5), [10.5, 11.0],
+                        np.arange(13.0, 27.0001, 2.0)])
+    return x, y, z
+
+
+def finfet(dirpath: str, electrons=300000, holes=50000, vd=0.7, vg=0.8, phims=-0.46, dt=2e-16, total_step=7000,
+           heat_steps=3000, stat_step=1000, mr_step=50, surface_scatter=True, compute_heat=True,
+           delta_nm=0.4, lambda_nm=1.5, kelvin=300.0) -> dict:
+    """The n-FinFET of the self-consistent workload, in the reference's deck
+    language and with the reference FinFET's topology (finfet/ldg.txt):
+    fin 30 nm tall (x) and 10 nm wide (z), gate length 20 nm (y), 1 nm SiO2
+    on the top and both sides of the gated fin, oxide beside the fin's foot,
+    a silicon substrate below; source / drain 1e20 cm^-3 donors rolling off
+    at 2 nm per decade into a 1e15 cm^-3 p-type channel as 0.5 nm stair-step
+    donor boxes; CATCH / GENERATE planes one cell inside the source, drain
+    and substrate contacts, REFLECT at the fin ends, SCATTOX on every
+    Si/SiO2 or outer face; contacts: source 0 V, drain vd, substrate 0 V,
+    a three-plane gate at vg with work-function difference phims.  Doping
+    values are in m^-3 as the reference reads them.  The surface-roughness
+    parameters go to input.txt as surface_roughness_delta_nm /
+    surface_roughness_lambda_nm (keys the reference does not read)."""
+    os.makedirs(dirpath, exist_ok=True)
+    x, y, z = finfet_grid()
+    write_grid(os.path.join(dirpath, "lgrid.txt"), x, y, z)
+    g = lambda v: f"{v:g}"
+    L = [
+        "default_par_number 3 1",
+        "region -1 66 -20 20 -17 27 VACUUM",
+        "region 0 30 -20 20 0 10 SILICON",
+        "region 30 66 -20 20 -17 27 SILICON",
+        "region -1 0 -20 20 -1 11 OXIDE",
+        "region 0 24 -20 20 -1 0 OXIDE",
+        "region 0 24 -20 20 10 11 OXIDE",
+        "region 24 30 -20 20 -17 0 OXIDE",
+        "region 24 30 -20 20 10 27 OXIDE",
+        "donor -1 66 -20 20 -17 27 0",
+        "donor 0 24 -20 -10 0 10 1e+26",
+        "donor 0 24 10 20 0 10 1e+26",
+    ]
+    for s_ in range(20):  # 2 nm / decade roll-off on the 0.5 nm channel grid
+        conc = 1e26 * 10.0 ** (-(0.5 * s_ + 0.25) / 2.0)
+        y0, y1 = -10.0 + 0.5 * s_, -10.0 + 0.5 * (s_ + 1)
+        L.append(f"donor 0 24 {g(y0)} {g(y1)} 0 10 {conc:.6g}")
+        L.append(f"donor 0 24 {g(-y1)} {g(-y0)} 0 10 {conc:.6g}")
+    L += [
+        "acceptor -1 66 -20 20 -17 27 0",
+        "acceptor 0 30 -10 10 0 10 1e+21",
+        "acceptor 24 30 -20 20 0 10 1e+21",
+        "acceptor 30 66 -20 20 -17 27 1e+21",
+        "motioncube -1 66 -20 20 -17 27 PASS PASS PASS PASS PASS PASS",
+        "motionplane 0 24 -18 -18 0 10 LEFT CATCH",
+        "motionplane 0 24 -18 -18 0 10 RIGHT GENERATE",
+        "motionplane 0 30 -20 -20 0 10 LEFT REFLECT",
+        "motionplane 0 24 18 18 0 10 RIGHT CATCH",
+        "motionplane 0 24 18 18 0 10 LEFT GENERATE",
+        "motionplane 0 30 20 20 0 10 RIGHT REFLECT",
+        "motionplane 0 0 -20 20 0 10 UP SCATTOX",
+        "motionplane 0 30 -20 20 0 0 FRONT SCATTOX",
+        "motionplane 0 30 -20 20 10 10 BACK SCATTOX",
+        "motionplane 30 30 -20 20 -17 0 UP SCATTOX",
+        "motionplane 30 30 -20 20 10 27 UP SCATTOX",
+        "motionplane 30 66 -20 -20 -17 27 LEFT SCATTOX",
+        "motionplane 30 66 20 20 -17 27 RIGHT SCATTOX",
+        "motionplane 30 66 -20 20 -17 -17 FRONT SCATTOX",
+        "motionplane 30 66 -20 20 27 27 BACK SCATTOX",
+        "motionplane 66 66 -20 20 -17 27 DOWN SCATTOX",
+        "motionplane 64 64 -20 20 -17 27 UP GENERATE",
+        "motionplane 64 64 -20 20 -17 27 DOWN CATCH",
+        "attachcontact 0 30 -20 20 0 10 0",
+        "attachcontact 0 24 -20 -16 0 10 1",
+        "attachcontact 0 24 16 20 0 10 2",
+        "attachcontact 60 66 -20 20 -17 27 3",
+        "surfaces 3",
+        "0 0 0",
+        "2 0 4",
+        "2 10 5",
+        "surface_scatter_range 0 24 -20 20 0 10",
+        "contact", "1 0", "0 24 -20 -20 0 10", "0",
+        "contact", "1 0", f"0 24 20 20 0 10", g(vd),
+        "contact", "1 0", "66 66 -20 20 -17 27", "0",
+        "contact", f"3 {g(phims)}", "-1 -1 -10 10 -1 11", "-1 24 -10 10 -1 -1", "-1 24 -10 10 11 11", g(vg),
+        "end",
+    ]
+    with open(os.path.join(dirpath, "ldg.txt"), "w") as f:
+        f.write("\n".join(L) + "\n")
+    write_input(os.path.join(dirpath, "input.txt"), dt=dt, Temperature=kelvin, total_step=total_step,
+                ElectronNumber=electrons, HoleNumber=holes, Flag_SurfaceScatter=int(surface_scatter),
+                Flag_MultipleRefresh=1, mr_step=mr_step, Flag_compute_heat=int(compute_heat), heat_steps=heat_steps,
+                stat_step=stat_step, stat_heat_step=stat_step, surface_roughness_delta_nm=delta_nm,
+                surface_roughness_lambda_nm=lambda_nm)
+    return dict(input=os.path.join(dirpath, "input.txt"), grid=os.path.join(dirpath, "lgrid.txt"),
+                device=os.path.join(dirpath, "ldg.txt"))

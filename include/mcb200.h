@@ -276,6 +276,67 @@ typedef struct {
 int mcb200_sort_particles_static(const mcb200_device_particles *in, size_t n, int nx, int ny, int nz,
                                  const mcb200_device_particles *out, size_t *n_out, void *stream);
 
+/* ---- input decks ---------------------------------------------------------
+ * The reference's decks read on the host, with its own semantics:
+ * input.txt key = value (MeshQuantities::getInputData,
+ * src/mcmodel.cpp:3824-3992; '#' starts a comment), the node coordinates of
+ * lgrid.txt in micrometres (read_grid_file, :4595-4693) and the device
+ * script ldg.txt (read_device_file, :4190-4479; region, donor, acceptor,
+ * motioncube, motionplane, attachcontact, contact, parnumber,
+ * default_par_number, ScatterArea, surfaces, surface_scatter_range,
+ * quantumRegion, VsVdVg, vgrange, ep_parm, end) applied to the cells as
+ * init_by_user_input / SetMRCube / SetMRPlane do (src/mcmodel.cpp:3065-3153,
+ * src/set_user_defined_data.cpp).  The grid and device files are looked up
+ * relative to the directory of input.txt.  A coordinate off the grid lines
+ * (where the reference exits) is MCB200_ERR_IO with the reason in
+ * mcb200_deck_error(). */
+typedef struct mcb200_deck mcb200_deck;
+
+typedef struct {
+  int nx, ny, nz;
+  int total_step, electron_number, hole_number, stat_step, stat_heat_step, heat_steps, mr_step;
+  double temperature, dt_s;
+  int flag_multiple_refresh, flag_compute_potential, flag_compute_heat, flag_surface_scatter,
+      flag_surface_roughness, flag_surface_phonon, flag_surface_impurity, flag_restart;
+  int n_contacts, n_planes, n_surfaces, default_electrons, default_holes;
+  char output_dir[512];
+  int prepared;  /* mcb200_deck_prepare has run */
+  double dt;     /* dt / time0 once prepared */
+} mcb200_deck_info;
+
+/* On failure *out may still hold a deck whose mcb200_deck_error() says why. */
+int mcb200_deck_load(const char *input_path, mcb200_deck **out);
+void mcb200_deck_free(mcb200_deck *deck);
+const char *mcb200_deck_error(const mcb200_deck *deck);
+int mcb200_deck_get_info(const mcb200_deck *deck, mcb200_deck_info *info);
+/* Named arrays; *needed receives the length (out may be NULL to ask).
+ * Per cell, index (j * nx + i) * nz + k: int "material", "desired_electrons",
+ * "desired_holes", "attached_contact", "scatter_type", "in_surf_region",
+ * "quantum_region", "motion_rule" (6 per cell); "contact_planes" (7 per
+ * plane: contact, i0, i1, j0, j1, k0, k1 node indices), "surface_type",
+ * "surface_dir"; double "lx_m", "ly_m", "lz_m" (metres), "donor_m3",
+ * "acceptor_m3", "contact_vapp_v", "contact_phims_v", "surface_pos_nm".
+ * After mcb200_deck_prepare, normalised: double "lx", "ly", "lz", "dx",
+ * "dy", "dz" (scaling, :4125-4166), "donor", "acceptor", "volume", "da",
+ * "init_electron_charge", "init_hole_charge" (init_cell_data, :3187-3270),
+ * "contact_vapp", "contact_phims", "surface_pos"; int "nearest_surf",
+ * "eeff_direction" (init_surface_roughness, :3155-3185), "electron_num",
+ * "hole_num", "refresh_electrons", "refresh_holes" (compute_par_num,
+ * src/particle_init.cpp:17-74). */
+int mcb200_deck_int_array(const mcb200_deck *deck, const char *name, int32_t *out, size_t n, size_t *needed);
+int mcb200_deck_double_array(const mcb200_deck *deck, const char *name, double *out, size_t n, size_t *needed);
+/* Normalise the deck with the context's units and intrinsic density; the
+ * context's tables must be built at the deck's Temperature. */
+int mcb200_deck_prepare(mcb200_deck *deck, const mcb200_ctx *ctx);
+/* mcb200_set_mesh + mcb200_set_cells + mcb200_set_device from the deck
+ * (prepares it first if needed). */
+int mcb200_apply_deck(mcb200_ctx *ctx, mcb200_deck *deck);
+/* The initial ensemble of init_particle_data (src/particle_init.cpp:112-219):
+ * electron_num / hole_num carriers per silicon cell sharing the cell's
+ * neutral charge, electrons first, cells in (i, k, j) order, each sampled by
+ * mcb200_seed_particles. */
+int mcb200_seed_deck(mcb200_ctx *ctx, mcb200_deck *deck, uint64_t seed);
+
 #ifdef __cplusplus
 }
 #endif

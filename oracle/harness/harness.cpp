@@ -185,6 +185,19 @@ double orc_scalar(const char *name) {
   if (n == "flag_surface_impurity") return mq->Flag_SurfaceImpurityScatter;
   if (n == "num_contact") return (double)mq->contact.size();
   if (n == "num_surface") return mq->NumSurface;
+  if (n == "total_step") return mq->total_step;
+  if (n == "electron_number") return mq->electron_number;
+  if (n == "hole_number") return mq->hole_number;
+  if (n == "stat_step") return mq->stat_step;
+  if (n == "mr_step") return mq->mr_step;
+  if (n == "heat_steps") return mq->heat_steps;
+  if (n == "default_electron_num") return mq->default_electron_num;
+  if (n == "default_hole_num") return mq->default_hole_num;
+  if (n == "sum_charge_e") return mq->sum_charge[PELEC];
+  if (n == "sum_charge_h") return mq->sum_charge[PHOLE];
+  if (n == "par_num") return mq->par_num;
+  if (n == "flag_mr") return mq->Flag_MultipleRefresh;
+  if (n == "flag_compute_heat") return mq->Flag_compute_heat;
   if (n == "draws") return (double)g_draws;
   return NAN;
 }
@@ -214,6 +227,8 @@ static Epetra_Vector *cell_vec(const std::string &n) {
   if (n == "c_h_roughnessRate") return mq->c_h_roughnessRate;
   if (n == "c_h_surfPhononRate") return mq->c_h_surfPhononRate;
   if (n == "c_donor") return mq->c_donor;
+  if (n == "c_init_electron_charge") return mq->c_init_electron_charge;
+  if (n == "c_init_hole_charge") return mq->c_init_hole_charge;
   if (n == "c_acceptor") return mq->c_acceptor;
   if (n == "p_electron_heat") return mq->p_electron_heat;
   if (n == "p_hole_heat") return mq->p_hole_heat;
@@ -233,6 +248,8 @@ static Epetra_IntVector *cell_ivec(const std::string &n) {
   if (n == "c_nearestSurf") return mq->c_nearestSurf;
   if (n == "c_EeffDirection") return mq->c_EeffDirection;
   if (n == "c_material") return mq->c_material;
+  if (n == "c_scatter_type") return mq->c_scatter_type;
+  if (n == "c_quantumRegion") return mq->c_quantumRegion;
   if (n == "c_desired_electron_number") return mq->c_desired_electron_number;
   if (n == "c_desired_hole_number") return mq->c_desired_hole_number;
   if (n == "c_electron_num") return mq->c_electron_num;
@@ -249,7 +266,7 @@ int orc_array_len(const char *name) {
   if (n == "dx") return (int)dx.size();
   if (n == "dy") return (int)dy.size();
   if (n == "dz") return (int)dz.size();
-  if (n == "SurfaceDir") return MNSurface;
+  if (n == "SurfaceDir" || n == "SurfaceType" || n == "SurfacePosition") return MNSurface;
   if (n == "lcurrent" || n == "rcurrent") return p_numy;
   if (Epetra_Vector *v = cell_vec(n)) return v->MyLength();
   if (Epetra_IntVector *v = cell_ivec(n)) return v->MyLength();
@@ -266,6 +283,8 @@ int orc_get_array(const char *name, double *out) {
   if (n == "dz") g = &dz;
   if (g) { std::copy(g->begin(), g->end(), out); return 0; }
   if (n == "SurfaceDir") { for (int i = 0; i < MNSurface; ++i) out[i] = g_mq->SurfaceDir[i]; return 0; }
+  if (n == "SurfaceType") { for (int i = 0; i < MNSurface; ++i) out[i] = g_mq->SurfaceType[i]; return 0; }
+  if (n == "SurfacePosition") { for (int i = 0; i < MNSurface; ++i) out[i] = g_mq->SurfacePosition[i]; return 0; }
   if (n == "lcurrent") { std::copy(g_mq->lcurrent, g_mq->lcurrent + p_numy, out); return 0; }
   if (n == "rcurrent") { std::copy(g_mq->rcurrent, g_mq->rcurrent + p_numy, out); return 0; }
   if (Epetra_Vector *v = cell_vec(n)) { for (int i = 0; i < v->MyLength(); ++i) out[i] = (*v)[i]; return 0; }
