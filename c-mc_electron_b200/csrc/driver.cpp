@@ -1,0 +1,395 @@
+// driver.cpp -- the self-consistent simulation behind `main input.txt`:
+// MeshQuantities::run / density (src/mcmodel.cpp:499-566, :424-467) and
+// compute_heat / heat_density (src/heat.cpp:48-160) over the engine's C ABI,
+// with the reference's data/ outputs (output_stat, current_scatter_info,
+// output_for_restart; src/mcmodel.cpp:756-1161).
+//
+// Per transport step, as density() orders it: statistics of the store
+// (statistic), charge deposition (particle_to_density + compute_cell_charge),
+// the Poisson solve and cell fields (compute_field; every poisson_every
+// steps, 1 = every step as the reference), surface rates when surface
+// scattering is on (GetSurfRoughnessPhononScRate), then the carrier step
+// (update_particle).  MultipleRefresh every mr_step steps; outputs every
+// stat_step steps, appended to the per-step files as the reference opens
+// them (section_current and the first `current` are truncated).
+#include <sys/stat.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "mcb200.h"
+
+namespace {
+
+struct RunError : std::runtime_error {
+  int code;
+  RunError(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+void ok(int rc, mcb200_ctx *c, const char *what) {
+  if (rc != MCB200_OK) throw RunError(rc, std::string(what) + ": " + (c ? mcb200_last_error(c) : ""));
+}
+void deck_ok(int rc, mcb200_deck *d, const char *what) {
+  if (rc != MCB200_OK) throw RunError(rc, std::string(what) + ": " + (d ? mcb200_deck_error(d) : ""));
+}
+
+std::vector<int32_t> deck_ints(mcb200_deck *d, const char *name) {
+  size_t n = 0;
+  deck_ok(mcb200_deck_int_array(d, name, nullptr, 0, &n), d, name);
+  std::vector<int32_t> v(n);
+  deck_ok(mcb200_deck_int_array(d, name, v.data(), n, &n), d, name);
+  return v;
+}
+std::vector<double> deck_doubles(mcb200_deck *d, const char *name) {
+  size_t n = 0;
+  deck_ok(mcb200_deck_double_array(d, name, nullptr, 0, &n), d, name);
+  std::vector<double> v(n);
+  deck_ok(mcb200_deck_double_array(d, name, v.data(), n, &n), d, name);
+  return v;
+}
+
+// input.txt keys the reference does not read: run-time choices of this engine.
+struct Extras {
+  double delta_nm = 0.1126755, lambda_nm = 2.0;  // surface roughness (the reference's hard-coded values)
+  int poisson_every = 1;
+};
+Extras read_extras(const std::string &path) {
+  Extras e;
+  std::ifstream in(path);
+  std::string line;
+  while (std::getline(in, line)) {
+    const size_t hash = line.find('#');
+    if (hash != std::string::npos) line = line.substr(0, hash);
+    const size_t eq = line.find('=');
+    if (eq == std::string::npos) continue;
+    std::string k = line.substr(0, eq), v = line.substr(eq + 1);
+    k.erase(0, k.find_first_not_of(" \t"));
+    k.erase(k.find_last_not_of(" \t\r") + 1);
+    if (k == "surface_roughness_delta_nm") e.delta_nm = std::atof(v.c_str());
+    else if (k == "surface_roughness_lambda_nm") e.lambda_nm = std::atof(v.c_str());
+    else if (k == "poisson_step") e.poisson_every = std::max(1, std::atoi(v.c_str()));
+  }
+  return e;
+}
+
+struct Run {
+  mcb200_ctx *ctx = nullptr;
+  mcb200_deck *deck = nullptr;
+  mcb200_deck_info info{};
+  mcb200_run_options opt{};
+  mcb200_run_report *rep = nullptr;
+  std::string data_dir;
+  double u[14];
+  int nx = 0, ny = 0, nz = 0, cells = 0, nodes = 0;
+  std::vector<int32_t> refresh_e, refresh_h, eeff;
+  std::vector<double> node_volume, saved_e_charge, saved_h_charge, pot_avg;
+  mcb200_surface_params surf{};
+  int poisson_every = 1;
+  uint64_t seed = 1;
+  bool heat = false;
+
+  double T0() const { return u[0]; }
+  double spr0() const { return u[2]; }
+  double time0() const { return u[3]; }
+  double conc0() const { return u[4]; }
+  double pot0() const { return u[7]; }
+  double curr0() const { return u[12]; }
+
+  std::string file(const char *prefix, int step) const {
+    std::ostringstream os;
+    os << data_dir << "/" << prefix << step;
+    return os.str();
+  }
+
+  // One step of density() (heat == false) or heat_density() (heat == true).
+  void density(int step) {
+    ok(mcb200_stat_accumulate(ctx), ctx, "mcb200_stat_accumulate");
+    ok(mcb200_deposit(ctx), ctx, "mcb200_deposit");
+    if (!heat && info.flag_compute_potential && step % poisson_every == 0) {
+      int it = 0;
+      double res = 0;
+      ok(mcb200_solve_poisson(ctx, opt.poisson_rel_tol > 0 ? opt.poisson_rel_tol : 1e-10, 20000, &it, &res), ctx,
+         "mcb200_solve_poisson");
+      rep->poisson_solves += 1;
+      rep->poisson_iterations += it;
+      rep->poisson_max_residual = std::max(rep->poisson_max_residual, res);
+    }
+    if (info.flag_surface_scatter) ok(mcb200_surface_rates(ctx, &surf, eeff.data()), ctx, "mcb200_surface_rates");
+    ok(mcb200_step(ctx, (uint32_t)(heat ? 0x80000000u + step : step), seed, info.dt), ctx, "mcb200_step");
+    rep->particle_steps += mcb200_num_particles(ctx);
+  }
+
+  void refresh(int step) {
+    if (!info.flag_multiple_refresh || step % info.mr_step != info.mr_step - 1) return;
+    int64_t gen = 0;
+    ok(mcb200_multiple_refresh(ctx, refresh_e.data(), refresh_h.data(), (uint32_t)(heat ? 0x80000000u + step : step),
+                               seed, &gen),
+       ctx, "mcb200_multiple_refresh");
+    rep->refreshes += 1;
+  }
+
+  // output_stat + current_scatter_info + output_for_restart for the window
+  // that ends at `step` (stat_step steps), then a new window.
+  void output(int step, int window) {
+    if (opt.write_outputs) write_outputs(step, window);
+    ok(mcb200_reset_tallies(ctx), ctx, "mcb200_reset_tallies");
+    ok(mcb200_stat_begin(ctx, window), ctx, "mcb200_stat_begin");
+  }
+
+  void write_outputs(int step, int window) {
+    const double dt = info.dt, pot0v = pot0(), curr0v = curr0(), velo0 = spr0() / time0(), conc0v = conc0();
+    std::vector<uint64_t> counters(MCB200_NUM_COUNTERS);
+    std::vector<double> contact(16 * 6), lcur(ny + 1), rcur(ny + 1), he(nodes), hh(nodes);
+    ok(mcb200_get_tallies(ctx, counters.data(), contact.data(), lcur.data(), rcur.data(), he.data(), hh.data()), ctx,
+       "mcb200_get_tallies");
+    {  // current (appended per window) and section_current<step>
+      std::ofstream f(data_dir + "/current", std::ios::app);
+      f << "step = " << step << "\n";
+      for (int c = 0; c < info.n_contacts; ++c) {
+        const double *t = &contact[6 * c];
+        f << "icont = " << c << "\n"
+          << "CharGen = " << t[1] << ' ' << "NumParGen = " << (long long)t[0] << ' ' << "CharCatch = " << t[4] << ' '
+          << "NumParCatch = " << (long long)t[3] << "\n"
+          << "EnergyGen= " << t[2] << "\n"
+          << "EnergyCatch= " << t[5] << "\n"
+          << "EnergyCurrent= " << (t[5] - t[2]) / (dt * window) * pot0v << "\n"
+          << "Current = " << (t[1] - t[4]) / (dt * window) * curr0v * 1e-2 << "\n";
+      }
+      f << "times of phonon scatter : " << counters[MCB200_CNT_PHONON] << "\n"
+        << "times of impurity scatter : " << counters[MCB200_CNT_IMPURITY] << "\n";
+      std::ofstream s(file("section_current", step));
+      for (int j = 0; j <= ny; ++j)
+        s << j << ' ' << rcur[j] / (dt * window) * curr0v << ' ' << lcur[j] / (dt * window) * curr0v << ' '
+          << (rcur[j] - lcur[j]) / (dt * window) * curr0v << "\n";
+    }
+    auto stat = [&](const char *name, size_t n) {
+      std::vector<double> v(n);
+      ok(mcb200_stat_get(ctx, name, v.data(), n), ctx, name);
+      return v;
+    };
+    const std::vector<double> count = stat("cell_count", cells), pot = stat("pot_sum", nodes);
+    auto cidx = [&](int i, int j, int k) { return ((size_t)j * nx + i) * nz + k; };
+    auto nidx = [&](int i, int j, int k) { return ((size_t)j * (nx + 1) + i) * (nz + 1) + k; };
+    {
+      std::ofstream f(file("electron_num", step), std::ios::app);
+      for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j)
+          for (int k = 0; k < nz; ++k) f << i << ' ' << j << ' ' << k << ' ' << count[cidx(i, j, k)] / window << "\n";
+    }
+    pot_avg.assign(nodes, 0.0);
+    {
+      std::ofstream f(file("pot", step), std::ios::app), q(file("qc_pot", step), std::ios::app);
+      for (int i = 0; i <= nx; ++i)
+        for (int k = 0; k <= nz; ++k)
+          for (int j = 0; j <= ny; ++j) {
+            const size_t p = nidx(i, j, k);
+            pot_avg[p] = pot[p] / window;
+            f << i << ' ' << j << ' ' << k << ' ' << pot_avg[p] * pot0v << "\n";
+            q << i << ' ' << j << ' ' << k << ' ' << pot_avg[p] * pot0v << "\n";  // no quantum correction
+          }
+    }
+    const char *names[2] = {"Electron", "Hole"};
+    const char *pre[2] = {"electron_", "hole_"};
+    std::vector<double> qsum[2];
+    for (int t = 0; t < 2; ++t) {
+      const std::string p(pre[t]);
+      const std::vector<double> qvx = stat((p + "qvx").c_str(), nodes), qvy = stat((p + "qvy").c_str(), nodes),
+                                qvz = stat((p + "qvz").c_str(), nodes), qe = stat((p + "qe").c_str(), nodes);
+      qsum[t] = stat((p + "q").c_str(), nodes);
+      std::vector<double> &saved = t == 0 ? saved_e_charge : saved_h_charge;
+      saved.assign(nodes, 0.0);
+      std::ofstream f(file(names[t], step), std::ios::app);
+      for (int i = 0; i <= nx; ++i)
+        for (int k = 0; k <= nz; ++k)
+          for (int j = 0; j <= ny; ++j) {
+            const size_t n = nidx(i, j, k);
+            const double q = qsum[t][n], aq = std::fabs(q);
+            double vx = 0, vy = 0, vz = 0, en = 0;
+            if (aq > 1e-13) {
+              vx = qvx[n] / aq * velo0;
+              vy = qvy[n] / aq * velo0;
+              vz = qvz[n] / aq * velo0;
+              en = qe[n] / aq * pot0v;
+            }
+            const double dens = node_volume[n] > 1e-13 ? q / node_volume[n] / window * conc0v : 0.0;
+            saved[n] = dens;
+            f << i << ' ' << j << ' ' << k << ' ' << vx << ' ' << vy << ' ' << vz << ' ' << en << ' ' << dens << "\n";
+          }
+    }
+    if (heat) {
+      std::ofstream f(file("heat", step), std::ios::app);
+      for (int i = 0; i <= nx; ++i)
+        for (int k = 0; k <= nz; ++k)
+          for (int j = 0; j <= ny; ++j) {
+            const size_t n = nidx(i, j, k);
+            const double v1 = std::fabs(qsum[0][n]) > 1e-13 ? he[n] * pot0v / qsum[0][n] : 0.0;
+            const double v2 = std::fabs(qsum[1][n]) > 1e-13 ? hh[n] * pot0v / qsum[1][n] : 0.0;
+            f << i << ' ' << j << ' ' << k << ' ' << v1 << ' ' << v1 * saved_e_charge[n] << ' ' << v2 << ' '
+              << v2 * saved_h_charge[n] << "\n";
+          }
+      double total = 0;
+      for (int n = 0; n < nodes; ++n) total += he[n] + hh[n];
+      rep->heat_total += total;
+    }
+    {  // par_info_restart<step>: per cell |q| and count of each carrier type
+      const size_t n = mcb200_num_particles(ctx);
+      std::vector<double> pd[8];
+      std::vector<int32_t> pi[6];
+      std::vector<uint32_t> uid(n);
+      for (auto &v : pd) v.resize(n);
+      for (auto &v : pi) v.resize(n);
+      mcb200_particles hp{pd[0].data(), pd[1].data(), pd[2].data(), pd[3].data(), pd[4].data(), pd[5].data(),
+                          pd[6].data(), pd[7].data(), pi[0].data(), pi[1].data(), pi[2].data(), pi[3].data(),
+                          pi[4].data(), pi[5].data(), uid.data()};
+      size_t got = 0;
+      ok(mcb200_download_particles(ctx, &hp, n, &got), ctx, "mcb200_download_particles");
+      std::vector<double> ec(cells, 0.0), hc(cells, 0.0);
+      std::vector<int> en(cells, 0), hn(cells, 0);
+      for (size_t q = 0; q < got; ++q) {
+        const size_t c = cidx(pi[0][q], pi[1][q], pi[2][q]);
+        if (pi[5][q] == 0) { ec[c] += std::fabs(pd[6][q]); en[c]++; }
+        else { hc[c] += std::fabs(pd[6][q]); hn[c]++; }
+      }
+      std::ofstream f(file("par_info_restart", step), std::ios::app);
+      for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j)
+          for (int k = 0; k < nz; ++k) {
+            const size_t c = cidx(i, j, k);
+            f << i << ' ' << j << ' ' << k << ' ' << ec[c] << ' ' << en[c] << ' ' << hc[c] << ' ' << hn[c] << "\n";
+          }
+      f << "-1 -1 -1\n";
+    }
+    // drain current of the window: contact 1 when there are several, else 0
+    const int drain = info.n_contacts > 1 ? 1 : 0;
+    if (info.n_contacts > 0)
+      rep->last_current[0] = (contact[6 * drain + 1] - contact[6 * drain + 4]) / (dt * window) * curr0v * 1e-2;
+    rep->windows += 1;
+  }
+
+  void go(const char *input_path, int device) {
+    deck_ok(mcb200_deck_load(input_path, &deck), deck, "mcb200_deck_load");
+    deck_ok(mcb200_deck_get_info(deck, &info), deck, "mcb200_deck_get_info");
+    const Extras ex = read_extras(input_path);
+    poisson_every = opt.poisson_every > 0 ? opt.poisson_every : ex.poisson_every;
+    seed = opt.seed ? opt.seed : 1;
+    // tables and context
+    const char *tables = opt.table_dir;
+    if (!tables) throw RunError(MCB200_ERR_ARG, "no table directory");
+    mcb200_ctx *probe = nullptr;
+    if (int rc = mcb200_create(tables, info.temperature, -1, 1, &probe)) {
+      const std::string m = probe ? mcb200_last_error(probe) : "";
+      mcb200_destroy(probe);
+      throw RunError(rc, "tables: " + m);
+    }
+    deck_ok(mcb200_deck_prepare(deck, probe), deck, "mcb200_deck_prepare");
+    mcb200_destroy(probe);
+    deck_ok(mcb200_deck_get_info(deck, &info), deck, "mcb200_deck_get_info");
+    const std::vector<int32_t> en = deck_ints(deck, "electron_num"), hn = deck_ints(deck, "hole_num");
+    refresh_e = deck_ints(deck, "refresh_electrons");
+    refresh_h = deck_ints(deck, "refresh_holes");
+    eeff = deck_ints(deck, "eeff_direction");
+    size_t start = 0, target = 0;
+    for (size_t c = 0; c < en.size(); ++c) {
+      start += (size_t)en[c] + hn[c];
+      target += (size_t)refresh_e[c] + refresh_h[c];
+    }
+    const size_t capacity = std::max(start, target) + std::max(start, target) / 4 + 65536;
+    ok(mcb200_create(tables, info.temperature, device, capacity, &ctx), ctx, "mcb200_create");
+    if (opt.flight_precision) ok(mcb200_set_flight_precision(ctx, opt.flight_precision), ctx, "precision");
+    ok(mcb200_units(ctx, u, 14), ctx, "mcb200_units");
+    deck_ok(mcb200_apply_deck(ctx, deck), deck, "mcb200_apply_deck");
+    nx = info.nx; ny = info.ny; nz = info.nz;
+    cells = nx * ny * nz;
+    nodes = (nx + 1) * (ny + 1) * (nz + 1);
+    node_volume.resize(nodes);
+    ok(mcb200_get_array(ctx, "node_volume", node_volume.data(), nodes), ctx, "node_volume");
+    deck_ok(mcb200_seed_deck(ctx, deck, seed), deck, "mcb200_seed_deck");
+    rep->initial_particles = mcb200_num_particles(ctx);
+    surf.delta = ex.delta_nm * 1e-9 / spr0();
+    surf.ail = ex.lambda_nm * 1e-9 / spr0();
+    surf.xiph = 12.0; surf.theta = 2.857703; surf.gama = 1.5; surf.nbmod = 2.0;
+    surf.npf = -0.6; surf.pft = 0.7; surf.pfn = 0.3; surf.kpha = 3600e-4;
+    surf.roughness = info.flag_surface_roughness;
+    surf.phonon = info.flag_surface_phonon;
+    data_dir = opt.data_dir ? opt.data_dir : "./data";
+    if (opt.write_outputs) {
+      ::mkdir(data_dir.c_str(), 0755);
+      std::ofstream(data_dir + "/current", std::ios::trunc);
+    }
+    // the first fields: deposit and solve before the first step
+    ok(mcb200_deposit(ctx), ctx, "mcb200_deposit");
+    if (info.flag_compute_potential) {
+      int it = 0;
+      double res = 0;
+      ok(mcb200_solve_poisson(ctx, 1e-10, 20000, &it, &res), ctx, "mcb200_solve_poisson");
+    }
+    ok(mcb200_set_timing(ctx, 1), ctx, "mcb200_set_timing");
+    const int steps = opt.max_steps > 0 ? std::min(opt.max_steps, info.total_step) : info.total_step;
+    ok(mcb200_stat_begin(ctx, info.stat_step), ctx, "mcb200_stat_begin");
+    const auto t0 = std::chrono::steady_clock::now();
+    heat = false;
+    for (int step = 0; step < steps; ++step) {
+      density(step);
+      refresh(step);
+      if (step % info.stat_step == info.stat_step - 1) output(step, info.stat_step);
+      if (opt.verbose && step % std::max(1, info.stat_step / 10) == 0)
+        std::printf("step %d: %zu particles\n", step, mcb200_num_particles(ctx));
+    }
+    rep->steps_done = steps;
+    // heat phase: the last window's mean potential, frozen
+    const int hsteps = !info.flag_compute_heat ? 0
+                       : (opt.max_heat_steps >= 0 ? std::min(opt.max_heat_steps, info.heat_steps) : info.heat_steps);
+    if (hsteps > 0) {
+      if (!pot_avg.empty()) ok(mcb200_set_potential(ctx, pot_avg.data()), ctx, "mcb200_set_potential");
+      heat = true;
+      ok(mcb200_set_heat_tally(ctx, 1), ctx, "mcb200_set_heat_tally");
+      const int window = info.stat_heat_step > 0 ? info.stat_heat_step : info.stat_step;
+      ok(mcb200_reset_tallies(ctx), ctx, "mcb200_reset_tallies");
+      ok(mcb200_stat_begin(ctx, window), ctx, "mcb200_stat_begin");
+      for (int step = 0; step < hsteps; ++step) {
+        density(step);
+        refresh(step);
+        if (step % window == window - 1) output(step, window);
+      }
+      rep->heat_steps_done = hsteps;
+    }
+    ok(mcb200_sync(ctx), ctx, "mcb200_sync");
+    rep->wall_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    double tim[6];
+    ok(mcb200_get_timing(ctx, tim, 6), ctx, "mcb200_get_timing");
+    rep->flight_ms = tim[0];
+    rep->step_ms = tim[2];
+    rep->final_particles = mcb200_num_particles(ctx);
+  }
+};
+
+}  // namespace
+
+extern "C" int mcb200_run_deck(const char *input_path, int device, const mcb200_run_options *options,
+                               mcb200_run_report *report, char *error, size_t error_len) {
+  if (!input_path || !options || !report) return MCB200_ERR_ARG;
+  std::memset(report, 0, sizeof(*report));
+  Run r;
+  r.opt = *options;
+  r.rep = report;
+  int rc = MCB200_OK;
+  try {
+    r.go(input_path, device);
+  } catch (const RunError &e) {
+    rc = e.code ? e.code : MCB200_ERR_STATE;
+    if (error && error_len) std::snprintf(error, error_len, "%s", e.what());
+  } catch (const std::exception &e) {
+    rc = MCB200_ERR_STATE;
+    if (error && error_len) std::snprintf(error, error_len, "%s", e.what());
+  }
+  if (r.ctx) mcb200_destroy(r.ctx);
+  if (r.deck) mcb200_deck_free(r.deck);
+  return rc;
+}

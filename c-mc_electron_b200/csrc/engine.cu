@@ -13,6 +13,7 @@
 #include "fullband_tables.h"
 #include "mcb200.h"
 #include "poisson_setup.h"
+#include "stat_kernels.h"
 
 using namespace mcb200;
 
@@ -119,6 +120,13 @@ struct mcb200_ctx {
   FieldBuffers fb{};
   bool device_set = false;
   double *h_scratch = nullptr;  // pinned, 8 doubles
+  // window statistics (mcb200_stat_*)
+  StatBuffers sb{};
+  StatScales ss{};
+  unsigned long long *stat_bounds = nullptr;
+  int stat_steps = 0;
+  bool stat_open = false;
+  double vmax = 0;  // largest group-velocity component of the band tables
   // CUDA-event timing on the context's stream (mcb200_timing)
   bool timing = false;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -375,6 +383,9 @@ void upload_tables(mcb200_ctx *c) {
   d.reflect_isym = dupload(refl, c->owned);
   build_kgrid(c, 40);
   upload_tables32(c, tf, ts, kn);
+  c->vmax = 0;
+  for (size_t q = 0; q < t.vt.size(); ++q)
+    if (q % 4 != 3) c->vmax = std::max(c->vmax, std::fabs(t.vt[q]));
 }
 
 template <typename T>
@@ -634,6 +645,12 @@ int mcb200_set_mesh(mcb200_ctx *c, int nx, int ny, int nz, const double *lx, con
     c->y.heat_e = dalloc<long long>(nodes, c->mesh_owned);
     c->y.heat_h = dalloc<long long>(nodes, c->mesh_owned);
     c->cell32 = dalloc<float4>(cells * 3, c->mesh_owned);
+    c->sb.nodes = (int)nodes;
+    c->sb.node = dalloc<long long>(nodes * 10, c->mesh_owned);
+    c->sb.cell_count = dalloc<unsigned long long>(cells, c->mesh_owned);
+    c->sb.pot_sum = dalloc<double>(nodes, c->mesh_owned);
+    c->stat_bounds = dalloc<unsigned long long>(4, c->mesh_owned);
+    c->stat_open = false;
     m.cell32 = c->cell32;
     c->hist = dalloc<unsigned int>(cells, c->mesh_owned);
     c->offsets = dalloc<unsigned int>(cells, c->mesh_owned);
@@ -1108,6 +1125,133 @@ int mcb200_multiple_refresh(mcb200_ctx *c, const int32_t *desired_e, const int32
     c->next_uid += totals[1];
     if (generated) *generated = g;
     return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_set_potential(mcb200_ctx *c, const double *potential) {
+  if (!c || !potential) return MCB200_ERR_ARG;
+  if (!c->device_set) return fail(c, MCB200_ERR_STATE, "mcb200_set_potential needs mcb200_set_device");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    const size_t nodes = (size_t)(c->mesh.nx + 1) * (c->mesh.ny + 1) * (c->mesh.nz + 1);
+    ck(cudaMemcpyAsync(c->fb.potential, potential, nodes * sizeof(double), cudaMemcpyHostToDevice, c->stream),
+       "copy");
+    launch_pot2field(c->mesh, c->fb.potential, c->stream);
+    ck(cudaGetLastError(), "pot2field");
+    ck(cudaStreamSynchronize(c->stream), "sync");
+    c->fields_set = true;
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_set_heat_tally(mcb200_ctx *c, int enable) {
+  if (!c) return MCB200_ERR_ARG;
+  if (!c->cells_set) return fail(c, MCB200_ERR_STATE, "mcb200_set_heat_tally before mcb200_set_cells");
+  c->mesh.heat = enable ? 1 : 0;
+  return MCB200_OK;
+}
+
+int mcb200_stat_begin(mcb200_ctx *c, int window_steps) {
+  if (!c || window_steps <= 0) return MCB200_ERR_ARG;
+  if (!c->mesh_set) return fail(c, MCB200_ERR_STATE, "mcb200_stat_begin before mcb200_set_mesh");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    cudaStream_t s = c->stream;
+    const int grid = grid_for(c, c->n, 256);
+    if (c->precision == MCB200_FLIGHT_FP32) launch_charge_bounds(store<float>(c, c->cur), (int)c->n, c->stat_bounds, grid, s);
+    else launch_charge_bounds(store<double>(c, c->cur), (int)c->n, c->stat_bounds, grid, s);
+    ck(cudaMemcpyAsync(c->h_scratch, c->stat_bounds, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
+       "copy");
+    ck(cudaStreamSynchronize(s), "sync");
+    unsigned long long b[4];
+    std::memcpy(b, c->h_scratch, sizeof(b));
+    const double emax = std::max(c->tab.emax, 1.0) * 2.0;
+    for (int t = 0; t < 2; ++t) {
+      double qmax;
+      std::memcpy(&qmax, &b[t], 8);
+      const double bound = std::max((double)b[2 + t] * qmax * window_steps * 4.0, 1e-300);
+      auto unit = [](double bnd) { return std::ldexp(1.0, 62 - (int)std::ceil(std::log2(bnd))); };
+      c->ss.q[t] = unit(bound);
+      c->ss.v[t] = unit(bound * std::max(c->vmax, 1e-300));
+      c->ss.e[t] = unit(bound * emax);
+    }
+    const size_t nodes = (size_t)c->sb.nodes;
+    ck(cudaMemsetAsync(c->sb.node, 0, sizeof(long long) * nodes * 10, s), "memset");
+    ck(cudaMemsetAsync(c->sb.cell_count, 0, sizeof(unsigned long long) * c->ncells, s), "memset");
+    ck(cudaMemsetAsync(c->sb.pot_sum, 0, sizeof(double) * nodes, s), "memset");
+    ck(cudaStreamSynchronize(s), "sync");
+    c->stat_steps = 0;
+    c->stat_open = true;
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_stat_accumulate(mcb200_ctx *c) {
+  if (!c) return MCB200_ERR_ARG;
+  if (!c->stat_open) return fail(c, MCB200_ERR_STATE, "mcb200_stat_accumulate before mcb200_stat_begin");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    cudaStream_t s = c->stream;
+    const int grid = grid_for(c, c->n, 256);
+    if (c->precision == MCB200_FLIGHT_FP32)
+      launch_statistic(store<float>(c, c->cur), (int)c->n, c->mesh, c->dt, c->ss, c->sb, grid, s);
+    else
+      launch_statistic(store<double>(c, c->cur), (int)c->n, c->mesh, c->dt, c->ss, c->sb, grid, s);
+    if (c->device_set) launch_add_potential(c->sb.nodes, c->fb.potential, c->sb.pot_sum, s);
+    ck(cudaGetLastError(), "statistic");
+    c->stat_steps += 1;
+    c->launches += 1 + (c->device_set ? 1 : 0);
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_stat_get(mcb200_ctx *c, const char *name, double *out, size_t n) {
+  if (!c || !name || !out) return MCB200_ERR_ARG;
+  if (!c->stat_open) return fail(c, MCB200_ERR_STATE, "no statistics window");
+  const std::string nm(name);
+  const size_t nodes = (size_t)c->sb.nodes, cells = (size_t)c->ncells;
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    ck(cudaStreamSynchronize(c->stream), "sync");
+    if (nm == "steps") {
+      if (n < 1) return fail(c, MCB200_ERR_CAPACITY, "output too small");
+      out[0] = c->stat_steps;
+      return MCB200_OK;
+    }
+    if (nm == "cell_count") {
+      if (n < cells) return fail(c, MCB200_ERR_CAPACITY, "output too small");
+      std::vector<unsigned long long> h(cells);
+      ck(cudaMemcpy(h.data(), c->sb.cell_count, cells * 8, cudaMemcpyDeviceToHost), "copy");
+      for (size_t q = 0; q < cells; ++q) out[q] = (double)h[q];
+      return MCB200_OK;
+    }
+    if (nm == "pot_sum") {
+      if (n < nodes) return fail(c, MCB200_ERR_CAPACITY, "output too small");
+      ck(cudaMemcpy(out, c->sb.pot_sum, nodes * 8, cudaMemcpyDeviceToHost), "copy");
+      return MCB200_OK;
+    }
+    // electron_* / hole_*: qvx, qvy, qvz, q, qe per node
+    static const char *fields[5] = {"qvx", "qvy", "qvz", "q", "qe"};
+    for (int t = 0; t < 2; ++t)
+      for (int f = 0; f < 5; ++f)
+        if (nm == std::string(t == 0 ? "electron_" : "hole_") + fields[f]) {
+          if (n < nodes) return fail(c, MCB200_ERR_CAPACITY, "output too small");
+          std::vector<long long> h(nodes);
+          ck(cudaMemcpy(h.data(), c->sb.node + ((size_t)t * 5 + f) * nodes, nodes * 8, cudaMemcpyDeviceToHost),
+             "copy");
+          const double scale = f < 3 ? c->ss.v[t] : (f == 3 ? c->ss.q[t] : c->ss.e[t]);
+          for (size_t q = 0; q < nodes; ++q) out[q] = (double)h[q] / scale;
+          return MCB200_OK;
+        }
+    return fail(c, MCB200_ERR_ARG, "unknown statistic " + nm);
   } catch (const std::exception &e) {
     return fail(c, MCB200_ERR_CUDA, e.what());
   }

@@ -73,6 +73,22 @@ class DeckInfo(ctypes.Structure):
                [("output_dir", ctypes.c_char * 512), ("prepared", ctypes.c_int), ("dt", ctypes.c_double)]
 
 
+class RunOptions(ctypes.Structure):
+    _fields_ = [("table_dir", ctypes.c_char_p), ("data_dir", ctypes.c_char_p), ("flight_precision", ctypes.c_int),
+                ("poisson_every", ctypes.c_int), ("poisson_rel_tol", ctypes.c_double), ("max_steps", ctypes.c_int),
+                ("max_heat_steps", ctypes.c_int), ("write_outputs", ctypes.c_int), ("seed", ctypes.c_uint64),
+                ("verbose", ctypes.c_int)]
+
+
+class RunReport(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ("steps_done", "heat_steps_done", "windows", "refreshes")] + \
+               [("initial_particles", ctypes.c_size_t), ("final_particles", ctypes.c_size_t),
+                ("particle_steps", ctypes.c_uint64), ("wall_s", ctypes.c_double), ("flight_ms", ctypes.c_double),
+                ("step_ms", ctypes.c_double), ("poisson_solves", ctypes.c_int),
+                ("poisson_iterations", ctypes.c_longlong), ("poisson_max_residual", ctypes.c_double),
+                ("last_current", ctypes.c_double * 1), ("heat_total", ctypes.c_double)]
+
+
 def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     if not os.path.exists(path):
         raise EngineError(f"{path} is missing: build it with `make -C c-mc_electron_b200` "
@@ -118,6 +134,13 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mcb200_deck_prepare.argtypes = [vp, vp]
     lib.mcb200_apply_deck.argtypes = [vp, vp]
     lib.mcb200_seed_deck.argtypes = [vp, vp, c.c_uint64]
+    lib.mcb200_run_deck.argtypes = [c.c_char_p, c.c_int, c.POINTER(RunOptions), c.POINTER(RunReport), c.c_char_p,
+                                    c.c_size_t]
+    lib.mcb200_stat_begin.argtypes = [vp, c.c_int]
+    lib.mcb200_stat_accumulate.argtypes = [vp]
+    lib.mcb200_stat_get.argtypes = [vp, c.c_char_p, dp, c.c_size_t]
+    lib.mcb200_set_potential.argtypes = [vp, dp]
+    lib.mcb200_set_heat_tally.argtypes = [vp, c.c_int]
     lib.mcb200_set_flight_precision.argtypes = [vp, c.c_int]
     lib.mcb200_get_flight_precision.argtypes = [vp]
     return lib
@@ -418,3 +441,23 @@ class Deck:
     def seed(self, engine: "Engine", seed: int):
         """The deck's initial ensemble (init_particle_data) into `engine`."""
         self._check(self._lib.mcb200_seed_deck(engine._ctx, self._deck, seed), "mcb200_seed_deck")
+
+
+def run_deck(input_path: str, device: int = 0, data_dir: str | None = None, precision: int = FLIGHT_FP64,
+             max_steps: int = 0, max_heat_steps: int = -1, poisson_every: int = 0, seed: int = 1,
+             write_outputs: bool = True, table_dir: str = DEFAULT_TABLE_DIR, verbose: bool = False) -> dict:
+    """The self-consistent simulation of a deck (mcb200_run_deck, the engine's
+    `main input.txt`).  Returns the run report as a dict."""
+    opt = RunOptions(table_dir=table_dir.encode(), data_dir=data_dir.encode() if data_dir else None,
+                     flight_precision=precision, poisson_every=poisson_every, poisson_rel_tol=0.0,
+                     max_steps=max_steps, max_heat_steps=max_heat_steps, write_outputs=int(write_outputs),
+                     seed=seed, verbose=int(verbose))
+    rep = RunReport()
+    err = ctypes.create_string_buffer(1024)
+    rc = lib().mcb200_run_deck(os.fspath(input_path).encode(), device, ctypes.byref(opt), ctypes.byref(rep), err,
+                               len(err))
+    if rc != OK:
+        raise EngineError(f"mcb200_run_deck failed ({rc}): {err.value.decode()}")
+    out = {name: getattr(rep, name) for name, _ in RunReport._fields_}
+    out["last_current"] = rep.last_current[0]
+    return out

@@ -276,6 +276,29 @@ typedef struct {
 int mcb200_sort_particles_static(const mcb200_device_particles *in, size_t n, int nx, int ny, int nz,
                                  const mcb200_device_particles *out, size_t *n_out, void *stream);
 
+/* Node potential (normalised, node layout) set from outside, then the cell
+ * fields from it (pot2field): the fixed potential of the reference's heat
+ * phase (compute_heat / heat_field, src/heat.cpp:100-128). */
+int mcb200_set_potential(mcb200_ctx *ctx, const double *potential);
+/* Phonon events tally heat (flag_heat, src/heat.cpp:108-160) while enabled. */
+int mcb200_set_heat_tally(mcb200_ctx *ctx, int enable);
+
+/* ---- window statistics ----------------------------------------------------
+ * The sums the reference accumulates every step for its stat_step outputs
+ * (MeshQuantities::statistic, src/mcmodel.cpp:1167-1408): per node and
+ * carrier type the CIC-weighted |q| v_x, |q| v_y, |q| v_z, |q| and |q| E of
+ * every particle, per cell the particle count, per node the potential.
+ * mcb200_stat_begin opens a window of `window_steps` steps (zeroes the sums
+ * and fixes their int64 fixed-point units from the store's charges);
+ * mcb200_stat_accumulate adds the current store and potential (call it once
+ * per step); mcb200_stat_get reads a sum as doubles: "electron_qvx",
+ * "electron_qvy", "electron_qvz", "electron_q", "electron_qe", "hole_..."
+ * (per node, normalised units), "cell_count" (per cell), "pot_sum" (per
+ * node), "steps" (1 value). */
+int mcb200_stat_begin(mcb200_ctx *ctx, int window_steps);
+int mcb200_stat_accumulate(mcb200_ctx *ctx);
+int mcb200_stat_get(mcb200_ctx *ctx, const char *name, double *out, size_t n);
+
 /* ---- input decks ---------------------------------------------------------
  * The reference's decks read on the host, with its own semantics:
  * input.txt key = value (MeshQuantities::getInputData,
@@ -336,6 +359,49 @@ int mcb200_apply_deck(mcb200_ctx *ctx, mcb200_deck *deck);
  * neutral charge, electrons first, cells in (i, k, j) order, each sampled by
  * mcb200_seed_particles. */
 int mcb200_seed_deck(mcb200_ctx *ctx, mcb200_deck *deck, uint64_t seed);
+
+/* ---- the self-consistent simulation (`main input.txt`) --------------------
+ * MeshQuantities::run and compute_heat (src/mcmodel.cpp:499-566,
+ * src/heat.cpp:108-160) over this ABI: load and apply the deck, seed the
+ * initial ensemble, then total_step transport steps (statistics,
+ * deposition, Poisson + fields every poisson_every steps, surface rates,
+ * carrier step; MultipleRefresh every mr_step; outputs every stat_step) and,
+ * with Flag_compute_heat, heat_steps steps at the last window's mean
+ * potential with heat tallies on.  Outputs go to data_dir in the
+ * reference's formats: current, section_current<step>, electron_num<step>,
+ * pot<step>, qc_pot<step>, Electron<step>, Hole<step>, heat<step>,
+ * par_info_restart<step>.  input.txt may also carry keys the reference
+ * ignores: poisson_step (solve every N steps), surface_roughness_delta_nm,
+ * surface_roughness_lambda_nm. */
+typedef struct {
+  const char *table_dir;     /* band tables (bs.si.asc, ...) */
+  const char *data_dir;      /* NULL: "./data" as the reference */
+  int flight_precision;      /* MCB200_FLIGHT_FP64 / MCB200_FLIGHT_FP32 */
+  int poisson_every;         /* 0: input.txt's poisson_step, else 1 */
+  double poisson_rel_tol;    /* 0: 1e-10 */
+  int max_steps;             /* 0: the deck's total_step */
+  int max_heat_steps;        /* -1: the deck's heat_steps (when Flag_compute_heat) */
+  int write_outputs;
+  uint64_t seed;             /* 0: 1 */
+  int verbose;
+} mcb200_run_options;
+
+typedef struct {
+  int steps_done, heat_steps_done, windows, refreshes;
+  size_t initial_particles, final_particles;
+  uint64_t particle_steps;        /* particles flown, summed over steps */
+  double wall_s;                  /* host wall time of the step loops */
+  double flight_ms, step_ms;      /* device time of the flight kernels / of mcb200_step */
+  int poisson_solves;
+  long long poisson_iterations;
+  double poisson_max_residual;
+  double last_current[1];         /* drain current (A/cm) of the last window */
+  double heat_total;              /* sum of the heat tallies over the heat windows (kT x charge) */
+} mcb200_run_report;
+
+/* `error` (may be NULL) receives a message on failure. */
+int mcb200_run_deck(const char *input_path, int device, const mcb200_run_options *options,
+                    mcb200_run_report *report, char *error, size_t error_len);
 
 #ifdef __cplusplus
 }
