@@ -108,10 +108,22 @@ struct Run {
     return os.str();
   }
 
+  using clock = std::chrono::steady_clock;
+  clock::time_point mark = clock::now();
+  // wall time since the last lap into report->phase_s[phase]
+  void lap(int phase) {
+    const clock::time_point now = clock::now();
+    rep->phase_s[phase] += std::chrono::duration<double>(now - mark).count();
+    mark = now;
+  }
+
   // One step of density() (heat == false) or heat_density() (heat == true).
   void density(int step) {
+    mark = clock::now();
     ok(mcb200_stat_accumulate(ctx), ctx, "mcb200_stat_accumulate");
+    lap(0);
     ok(mcb200_deposit(ctx), ctx, "mcb200_deposit");
+    lap(1);
     if (!heat && info.flag_compute_potential && step % poisson_every == 0) {
       int it = 0;
       double res = 0;
@@ -121,26 +133,33 @@ struct Run {
       rep->poisson_iterations += it;
       rep->poisson_max_residual = std::max(rep->poisson_max_residual, res);
     }
+    lap(2);
     if (info.flag_surface_scatter) ok(mcb200_surface_rates(ctx, &surf, eeff.data()), ctx, "mcb200_surface_rates");
+    lap(3);
     ok(mcb200_step(ctx, (uint32_t)(heat ? 0x80000000u + step : step), seed, info.dt), ctx, "mcb200_step");
     rep->particle_steps += mcb200_num_particles(ctx);
+    lap(4);
   }
 
   void refresh(int step) {
     if (!info.flag_multiple_refresh || step % info.mr_step != info.mr_step - 1) return;
+    mark = clock::now();
     int64_t gen = 0;
     ok(mcb200_multiple_refresh(ctx, refresh_e.data(), refresh_h.data(), (uint32_t)(heat ? 0x80000000u + step : step),
                                seed, &gen),
        ctx, "mcb200_multiple_refresh");
     rep->refreshes += 1;
+    lap(5);
   }
 
   // output_stat + current_scatter_info + output_for_restart for the window
   // that ends at `step` (stat_step steps), then a new window.
   void output(int step, int window) {
+    mark = clock::now();
     if (opt.write_outputs) write_outputs(step, window);
     ok(mcb200_reset_tallies(ctx), ctx, "mcb200_reset_tallies");
     ok(mcb200_stat_begin(ctx, window), ctx, "mcb200_stat_begin");
+    lap(6);
   }
 
   void write_outputs(int step, int window) {

@@ -118,12 +118,15 @@ struct mcb200_ctx {
   int sm_count = 148;
   // deposition / Poisson (mcb200_set_device)
   FieldBuffers fb{};
+  CgPlan cg_plan;
   bool device_set = false;
-  double *h_scratch = nullptr;  // pinned, 8 doubles
+  double *h_scratch = nullptr;  // pinned, 16 doubles
   // window statistics (mcb200_stat_*)
   StatBuffers sb{};
   StatScales ss{};
   unsigned long long *stat_bounds = nullptr;
+  int *eeff_dev = nullptr;           // surface-normal field component per cell (mcb200_surface_rates)
+  std::vector<int> eeff_host;
   int stat_steps = 0;
   bool stat_open = false;
   double vmax = 0;  // largest group-velocity component of the band tables
@@ -650,6 +653,8 @@ int mcb200_set_mesh(mcb200_ctx *c, int nx, int ny, int nz, const double *lx, con
     c->sb.cell_count = dalloc<unsigned long long>(cells, c->mesh_owned);
     c->sb.pot_sum = dalloc<double>(nodes, c->mesh_owned);
     c->stat_bounds = dalloc<unsigned long long>(4, c->mesh_owned);
+    c->eeff_dev = dalloc<int>(cells, c->mesh_owned);
+    c->eeff_host.clear();
     c->stat_open = false;
     m.cell32 = c->cell32;
     c->hist = dalloc<unsigned int>(cells, c->mesh_owned);
@@ -659,6 +664,7 @@ int mcb200_set_mesh(mcb200_ctx *c, int nx, int ny, int nz, const double *lx, con
     c->mesh_set = true;
     c->cells_set = c->fields_set = c->device_set = false;
     c->fb = FieldBuffers{};
+    c->cg_plan = CgPlan{};
     return mcb200_reset_tallies(c);
   } catch (const std::exception &e) {
     return fail(c, MCB200_ERR_CUDA, e.what());
@@ -978,13 +984,15 @@ int mcb200_set_device(mcb200_ctx *c, const int32_t *material, const double *dono
     f.cg_r = dalloc<double>(nodes, c->mesh_owned);
     f.cg_z = dalloc<double>(nodes, c->mesh_owned);
     f.cg_p = dalloc<double>(nodes, c->mesh_owned);
+    f.cg_p1 = dalloc<double>(nodes, c->mesh_owned);
     f.cg_q = dalloc<double>(nodes, c->mesh_owned);
-    f.cg_part = dalloc<double>(512, c->mesh_owned);
-    f.cg_scalars = dalloc<double>(8, c->mesh_owned);
+    f.cg_part = dalloc<double>(3 * kCgMaxGrid, c->mesh_owned);  // the persistent CG's partial sums
+    f.cg_scalars = dalloc<double>(16, c->mesh_owned);  // the CG scalars sc[0..9]
     f.abs_sum = dalloc<unsigned long long>(4, c->mesh_owned);
     ck(cudaMemset(f.potential, 0, nodes * sizeof(double)), "memset");
     ck(cudaMemset(f.density, 0, nodes * sizeof(double)), "memset");
-    if (!c->h_scratch) ck(cudaMallocHost(&c->h_scratch, 8 * sizeof(double)), "cudaMallocHost");
+    if (!c->h_scratch) ck(cudaMallocHost(&c->h_scratch, 16 * sizeof(double)), "cudaMallocHost");
+    c->cg_plan = CgPlan{};
     c->device_set = true;
     return MCB200_OK;
   } catch (const std::exception &e) {
@@ -1035,7 +1043,7 @@ int mcb200_solve_poisson(mcb200_ctx *c, double rel_tol, int max_iter, int *itera
     cudaStream_t s = c->stream;
     const int nodes = (c->mesh.nx + 1) * (c->mesh.ny + 1) * (c->mesh.nz + 1);
     launch_rhs(nodes, c->fb, s);
-    if (cg_solve(c->mesh, c->fb, rel_tol, max_iter, s, c->h_scratch, iterations, rel_residual))
+    if (cg_solve(c->mesh, c->fb, rel_tol, max_iter, s, c->h_scratch, iterations, rel_residual, c->cg_plan))
       return fail(c, MCB200_ERR_CUDA, "Poisson solve failed");
     launch_pot2field(c->mesh, c->fb.potential, s);
     ck(cudaGetLastError(), "pot2field");
@@ -1060,16 +1068,19 @@ int mcb200_surface_rates(mcb200_ctx *c, const mcb200_surface_params *p, const in
     q.eps_si = u.eps_silicon; q.eps_ox = u.eps_oxide; q.Tn = u.Tn; q.T0 = u.T0; q.boltz = 8.617343e-5;
     q.field0 = u.field0; q.em0 = u.em0; q.ec0 = u.ec0; q.hq0 = u.hq0; q.conc0 = u.conc0; q.sirho = u.sirho;
     q.scrt0 = u.scrt0;
-    std::vector<void *> tmp;
-    int *dir = dalloc<int>(c->ncells, tmp);
-    ck(cudaMemcpyAsync(dir, eeff_direction, sizeof(int) * c->ncells, cudaMemcpyHostToDevice, c->stream), "copy");
+    // the direction array stays on the device; it is uploaded when it changes
+    if (c->eeff_host.size() != (size_t)c->ncells ||
+        std::memcmp(c->eeff_host.data(), eeff_direction, sizeof(int) * c->ncells) != 0) {
+      c->eeff_host.assign(eeff_direction, eeff_direction + c->ncells);
+      ck(cudaMemcpyAsync(c->eeff_dev, c->eeff_host.data(), sizeof(int) * c->ncells, cudaMemcpyHostToDevice, c->stream),
+         "copy");
+    }
     const DevMesh &m = c->mesh;
-    launch_surface_rates(c->ncells, q, m.hfield, m.rho, dir, const_cast<double *>(m.e_rough),
+    launch_surface_rates(c->ncells, q, m.hfield, m.rho, c->eeff_dev, const_cast<double *>(m.e_rough),
                          const_cast<double *>(m.e_sphon), const_cast<double *>(m.h_rough),
                          const_cast<double *>(m.h_sphon), c->stream);
     ck(cudaGetLastError(), "surface rates");
-    ck(cudaStreamSynchronize(c->stream), "sync");
-    for (void *q2 : tmp) cudaFree(q2);
+    c->launches += 1;
     return MCB200_OK;
   } catch (const std::exception &e) {
     return fail(c, MCB200_ERR_CUDA, e.what());

@@ -13,10 +13,16 @@
 //    reductions, so a solve is bit-reproducible.
 //  * pot2field (:2776-2855): cell field from the 8 corner potentials,
 //    stored as felt by each carrier (ChargeSign applied).
+#include <cooperative_groups.h>
+
+#include <algorithm>
+
 #include "device_state.cuh"
 #include "field_kernels.h"
 
 namespace mcb200 {
+
+namespace cg = cooperative_groups;
 
 constexpr uint32_t kDeadBit = 1u << 16;
 
@@ -190,26 +196,8 @@ __global__ void __launch_bounds__(kRedBlock) dot_final(const double *part, doubl
   if (threadIdx.x == 0) *out = s;
 }
 
-// CG scalars live in device memory: [0] rz, [1] pq, [2] rz_new, [3] rr, [4] alpha, [5] beta
-__global__ void cg_alpha(double *sc) { sc[4] = sc[0] / sc[1]; }
-__global__ void cg_beta(double *sc) {
-  sc[5] = sc[2] / sc[0];
-  sc[0] = sc[2];
-}
-__global__ void cg_update_xr(int n, const double *sc, const double *p, const double *q, double *x, double *r,
-                             const double *diag_inv, double *z, const uint8_t *dir) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || dir[i]) return;
-  const double alpha = sc[4];
-  x[i] += alpha * p[i];
-  r[i] -= alpha * q[i];
-  z[i] = r[i] * diag_inv[i];
-}
-__global__ void cg_update_p(int n, const double *sc, const double *z, double *p, const uint8_t *dir) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || dir[i]) return;
-  p[i] = z[i] + sc[5] * p[i];
-}
+// CG scalars in device memory: [0] rz, [3] rr, [6] ||b||^2, [7] converged,
+// [8] iterations, [9] (rel_tol ||b||)^2
 __global__ void cg_init(int n, const double *r, const double *diag_inv, double *z, double *p, const uint8_t *dir,
                         const double *rhs, double *x) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -244,6 +232,106 @@ __global__ void folded_rhs(int nodes, Grid3 g, const double *st, const uint8_t *
 __global__ void set_dirichlet(int nodes, const uint8_t *dir, const double *rhs, double *x) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p < nodes && dir[p]) x[p] = rhs[p];
+}
+
+// ---- persistent CG -----------------------------------------------------------
+// One cooperative launch runs every iteration of a solve.  Per iteration two
+// grid-wide barriers: (A) p_new = z + beta p_old, computed on the fly for the
+// node and its neighbours (p ping-pongs between two buffers), q = A p_new and
+// the block partials of p.q; (B) alpha, the x / r / z update and the
+// partials of r.z and r.r.  After each barrier every block sums all partials
+// itself, in the same fixed order, so every block takes the same scalars and
+// the same convergence decision, and a solve is bit-reproducible for a given
+// grid.
+__device__ __forceinline__ double sum_partials(const double *part, int n) {
+  double v = 0.0;
+  for (int i = threadIdx.x; i < n; i += kRedBlock) v += part[i];
+  return block_sum<kRedBlock>(v);
+}
+
+__global__ void __launch_bounds__(kRedBlock) cg_persistent(int nodes, Grid3 g, const double *st, const uint8_t *dir,
+                                                           const double *diag_inv, double *x, double *r, double *z,
+                                                           double *p0, double *p1, double *q, double *part,
+                                                           double *sc, int max_iter) {
+  cg::grid_group grid = cg::this_grid();
+  const int nblk = gridDim.x;
+  double *part_pq = part, *part_rz = part + nblk, *part_rr = part + 2 * nblk;
+  double rz = sc[0], rr = sc[3], beta = 0.0;  // p0 holds z: the first p is z
+  const double tol2 = sc[9];
+  bool done = sc[7] != 0.0;
+  int it = 0;
+  const double *pin = p0;
+  double *pout = p1;
+  const int stride = nblk * kRedBlock;
+  while (!done && it < max_iter) {
+    double v = 0.0;
+    for (int n = blockIdx.x * kRedBlock + threadIdx.x; n < nodes; n += stride) {
+      if (dir[n]) {
+        q[n] = 0.0;
+        pout[n] = 0.0;
+        continue;
+      }
+      int i, j, k;
+      node_ijk(n, g, i, j, k);
+      const double *a = st + (size_t)n * 7;
+      const double pn = z[n] + beta * pin[n];
+      pout[n] = pn;
+      double acc = a[6] * pn;
+      const int nb[6] = {i > 0 ? n - g.pz : -1, i + 1 < g.px ? n + g.pz : -1, j > 0 ? n - g.px * g.pz : -1,
+                         j + 1 < g.py ? n + g.px * g.pz : -1, k > 0 ? n - 1 : -1, k + 1 < g.pz ? n + 1 : -1};
+#pragma unroll
+      for (int s = 0; s < 6; ++s) {
+        const int m = nb[s];
+        if (m < 0 || a[s] == 0.0 || dir[m]) continue;
+        acc += a[s] * (z[m] + beta * pin[m]);
+      }
+      q[n] = acc;
+      v += pn * acc;
+    }
+    const double bs = block_sum<kRedBlock>(v);
+    if (threadIdx.x == 0) part_pq[blockIdx.x] = bs;
+    grid.sync();
+    const double alpha = rz / sum_partials(part_pq, nblk);
+    double a1 = 0.0, a2 = 0.0;
+    for (int n = blockIdx.x * kRedBlock + threadIdx.x; n < nodes; n += stride) {
+      if (dir[n]) continue;
+      x[n] += alpha * pout[n];
+      const double rn = r[n] - alpha * q[n];
+      r[n] = rn;
+      const double zn = rn * diag_inv[n];
+      z[n] = zn;
+      a1 += rn * zn;
+      a2 += rn * rn;
+    }
+    const double b1 = block_sum<kRedBlock>(a1);
+    const double b2 = block_sum<kRedBlock>(a2);
+    if (threadIdx.x == 0) {
+      part_rz[blockIdx.x] = b1;
+      part_rr[blockIdx.x] = b2;
+    }
+    grid.sync();
+    const double rz_new = sum_partials(part_rz, nblk);
+    rr = sum_partials(part_rr, nblk);
+    beta = rz_new / rz;
+    rz = rz_new;
+    ++it;
+    done = rr <= tol2;
+    const double *t = pout;
+    pout = const_cast<double *>(pin);
+    pin = t;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    sc[0] = rz;
+    sc[3] = rr;
+    sc[8] = it;
+  }
+}
+
+// sc[9] = (rel_tol * ||b||)^2; converged already when the warm start meets it
+__global__ void cg_setup(double *sc, double rel_tol2) {
+  sc[9] = rel_tol2 * sc[6];
+  sc[7] = sc[3] <= sc[9] ? 1.0 : 0.0;
+  sc[8] = 0.0;
 }
 
 // pot2field / pot2field_for_hole, src/mcmodel.cpp:2732-2855 (no quantum
@@ -313,7 +401,7 @@ static void dot(int n, const double *a, const double *b, double *part, double *o
 }
 
 int cg_solve(const DevMesh &M, const FieldBuffers &f, double rel_tol, int max_iter, cudaStream_t s,
-             double *host_scratch, int *iterations, double *rel_residual) {
+             double *host_scratch, int *iterations, double *rel_residual, CgPlan &plan) {
   const int nodes = (M.nx + 1) * (M.ny + 1) * (M.nz + 1);
   const Grid3 g{M.nx + 1, M.ny + 1, M.nz + 1};
   const int nb = blocks(nodes, 256);
@@ -327,28 +415,31 @@ int cg_solve(const DevMesh &M, const FieldBuffers &f, double rel_tol, int max_it
   cg_init<<<nb, 256, 0, s>>>(nodes, f.cg_r, f.diag_inv, f.cg_z, f.cg_p, f.dirichlet, f.rhs, f.potential);
   dot(nodes, f.cg_r, f.cg_z, f.cg_part, sc + 0, s);
   dot(nodes, f.cg_r, f.cg_r, f.cg_part, sc + 3, s);
-  cudaMemcpyAsync(host_scratch, sc, 8 * sizeof(double), cudaMemcpyDeviceToHost, s);
-  if (cudaStreamSynchronize(s) != cudaSuccess) return 1;
-  const double bnorm = sqrt(host_scratch[6]) > 0 ? sqrt(host_scratch[6]) : 1.0;
-  double res = sqrt(host_scratch[3]) / bnorm;
-  int it = 0;
-  const int check = 8;
-  while (res > rel_tol && it < max_iter) {
-    for (int q = 0; q < check && it < max_iter; ++q, ++it) {
-      stencil_apply<<<nb, 256, 0, s>>>(nodes, g, f.stencil, f.dirichlet, f.cg_p, nullptr, f.cg_q);
-      dot(nodes, f.cg_p, f.cg_q, f.cg_part, sc + 1, s);
-      cg_alpha<<<1, 1, 0, s>>>(sc);
-      cg_update_xr<<<nb, 256, 0, s>>>(nodes, sc, f.cg_p, f.cg_q, f.potential, f.cg_r, f.diag_inv, f.cg_z,
-                                      f.dirichlet);
-      dot(nodes, f.cg_r, f.cg_z, f.cg_part, sc + 2, s);
-      cg_beta<<<1, 1, 0, s>>>(sc);
-      cg_update_p<<<nb, 256, 0, s>>>(nodes, sc, f.cg_z, f.cg_p, f.dirichlet);
-    }
-    dot(nodes, f.cg_r, f.cg_r, f.cg_part, sc + 3, s);
-    cudaMemcpyAsync(host_scratch, sc, 8 * sizeof(double), cudaMemcpyDeviceToHost, s);
-    if (cudaStreamSynchronize(s) != cudaSuccess) return 1;
-    res = sqrt(host_scratch[3]) / bnorm;
+  cg_setup<<<1, 1, 0, s>>>(sc, rel_tol * rel_tol);
+  // every iteration in one cooperative launch (cg_persistent)
+  if (plan.grid == 0) {
+    int dev = 0, sms = 0, per_sm = 0, coop = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    if (!coop || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_persistent, kRedBlock, 0) != cudaSuccess ||
+        per_sm < 1)
+      return 1;
+    plan.grid = std::min(per_sm * sms, kCgMaxGrid);
   }
+  int nodes_arg = nodes, max_arg = max_iter;
+  Grid3 g_arg = g;
+  const double *st = f.stencil, *dinv = f.diag_inv;
+  const uint8_t *dirp = f.dirichlet;
+  double *x = f.potential, *r = f.cg_r, *z = f.cg_z, *p0 = f.cg_p, *p1 = f.cg_p1, *q = f.cg_q, *part = f.cg_part;
+  void *args[] = {&nodes_arg, &g_arg, &st, &dirp, &dinv, &x, &r, &z, &p0, &p1, &q, &part, &sc, &max_arg};
+  if (cudaLaunchCooperativeKernel((const void *)cg_persistent, plan.grid, kRedBlock, args, 0, s) != cudaSuccess)
+    return 1;
+  plan.launches += 1;
+  cudaMemcpyAsync(host_scratch, sc, 10 * sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return 1;
+  const int it = (int)host_scratch[8];
+  const double bnorm = sqrt(host_scratch[6]) > 0 ? sqrt(host_scratch[6]) : 1.0;
   // true residual of the final iterate
   stencil_apply<<<nb, 256, 0, s>>>(nodes, g, f.stencil, f.dirichlet, f.potential, f.rhs, f.cg_r);
   dot(nodes, f.cg_r, f.cg_r, f.cg_part, sc + 3, s);

@@ -21,7 +21,7 @@ struct FieldBuffers {
   double *density = nullptr;                    // p_par_charge (charge / node volume)
   // Poisson
   double *rhs = nullptr, *potential = nullptr;
-  double *cg_r = nullptr, *cg_z = nullptr, *cg_p = nullptr, *cg_q = nullptr, *cg_part = nullptr,
+  double *cg_r = nullptr, *cg_z = nullptr, *cg_p = nullptr, *cg_p1 = nullptr, *cg_q = nullptr, *cg_part = nullptr,
          *cg_scalars = nullptr;
   unsigned long long *abs_sum = nullptr;
 };
@@ -39,9 +39,16 @@ template <typename R>
 void launch_deposit(const DevParticlesT<R> &P, int n, const DevMesh &M, const FieldBuffers &f, const DepositScales &S,
                     int grid, cudaStream_t s);
 void launch_rhs(int nodes, const FieldBuffers &f, cudaStream_t s);
-// Returns 0 on success; host_scratch must hold 8 doubles (pinned).
+// The CG iterations of one solve run in one cooperative launch; its grid
+// (blocks) is fixed per context on first use, so the reduction order is too.
+constexpr int kCgMaxGrid = 1024;
+struct CgPlan {
+  int grid = 0;
+  unsigned long long launches = 0;
+};
+// Returns 0 on success; host_scratch must hold 10 doubles (pinned).
 int cg_solve(const DevMesh &M, const FieldBuffers &f, double rel_tol, int max_iter, cudaStream_t s,
-             double *host_scratch, int *iterations, double *rel_residual);
+             double *host_scratch, int *iterations, double *rel_residual, CgPlan &plan);
 void launch_pot2field(const DevMesh &M, const double *pot, cudaStream_t s);
 
 }  // namespace mcb200

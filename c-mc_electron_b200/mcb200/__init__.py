@@ -86,7 +86,8 @@ class RunReport(ctypes.Structure):
                 ("particle_steps", ctypes.c_uint64), ("wall_s", ctypes.c_double), ("flight_ms", ctypes.c_double),
                 ("step_ms", ctypes.c_double), ("poisson_solves", ctypes.c_int),
                 ("poisson_iterations", ctypes.c_longlong), ("poisson_max_residual", ctypes.c_double),
-                ("last_current", ctypes.c_double * 1), ("heat_total", ctypes.c_double)]
+                ("last_current", ctypes.c_double * 1), ("heat_total", ctypes.c_double),
+                ("phase_s", ctypes.c_double * 8)]
 
 
 def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
@@ -460,4 +461,6 @@ def run_deck(input_path: str, device: int = 0, data_dir: str | None = None, prec
         raise EngineError(f"mcb200_run_deck failed ({rc}): {err.value.decode()}")
     out = {name: getattr(rep, name) for name, _ in RunReport._fields_}
     out["last_current"] = rep.last_current[0]
+    out["phase_s"] = dict(zip(("statistics", "deposition", "poisson", "surface_rates", "step", "refresh", "outputs"),
+                              list(rep.phase_s)[:7]))
     return out

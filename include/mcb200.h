@@ -397,6 +397,8 @@ typedef struct {
   double poisson_max_residual;
   double last_current[1];         /* drain current (A/cm) of the last window */
   double heat_total;              /* sum of the heat tallies over the heat windows (kT x charge) */
+  double phase_s[8];              /* host wall time per phase: statistics, deposition, Poisson + fields,
+                                     surface rates, carrier step, refresh, outputs, (unused) */
 } mcb200_run_report;
 
 /* `error` (may be NULL) receives a message on failure. */
