@@ -351,15 +351,53 @@ struct Run {
     }
     ok(mcb200_set_timing(ctx, 1), ctx, "mcb200_set_timing");
     const int steps = opt.max_steps > 0 ? std::min(opt.max_steps, info.total_step) : info.total_step;
+    const int warm = std::max(0, std::min(opt.warmup_steps, steps));
     ok(mcb200_stat_begin(ctx, info.stat_step), ctx, "mcb200_stat_begin");
     const auto t0 = std::chrono::steady_clock::now();
+    auto timed_t0 = t0;
+    uint64_t ps0 = 0;
     heat = false;
+    std::vector<double> readback(16 * 6);
+    double flushed_ms = 0;  // device time of the timed steps when each follows an L2 eviction
     for (int step = 0; step < steps; ++step) {
+      if (step == warm) {  // the timed region starts: device event + engine timing reset
+        ok(mcb200_sync(ctx), ctx, "mcb200_sync");
+        ok(mcb200_set_timing(ctx, 1), ctx, "mcb200_set_timing");
+        ok(mcb200_mark(ctx, 0), ctx, "mcb200_mark");
+        timed_t0 = std::chrono::steady_clock::now();
+        ps0 = rep->particle_steps;
+      }
+      const bool flush = opt.flush_l2_bytes > 0 && step >= warm;
+      if (flush) {
+        ok(mcb200_flush_l2(ctx, opt.flush_l2_bytes), ctx, "mcb200_flush_l2");
+        ok(mcb200_mark(ctx, 2), ctx, "mcb200_mark");
+      }
       density(step);
       refresh(step);
+      if (flush) {
+        double ms = 0;
+        ok(mcb200_mark(ctx, 3), ctx, "mcb200_mark");
+        ok(mcb200_elapsed_ms(ctx, 2, 3, &ms), ctx, "mcb200_elapsed_ms");
+        flushed_ms += ms;
+      }
+      if (opt.readback_every_step)
+        ok(mcb200_get_tallies(ctx, nullptr, readback.data(), nullptr, nullptr, nullptr, nullptr), ctx, "tallies");
       if (step % info.stat_step == info.stat_step - 1) output(step, info.stat_step);
       if (opt.verbose && step % std::max(1, info.stat_step / 10) == 0)
         std::printf("step %d: %zu particles\n", step, mcb200_num_particles(ctx));
+    }
+    if (steps > warm) {
+      ok(mcb200_mark(ctx, 1), ctx, "mcb200_mark");
+      ok(mcb200_elapsed_ms(ctx, 0, 1, &rep->timed_device_ms), ctx, "mcb200_elapsed_ms");
+      if (opt.flush_l2_bytes > 0) rep->timed_device_ms = flushed_ms;  // the evictions are not timed
+      rep->timed_wall_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - timed_t0).count();
+      rep->timed_particle_steps = rep->particle_steps - ps0;
+      rep->timed_steps = steps - warm;
+      double tt[6];
+      ok(mcb200_get_timing(ctx, tt, 6), ctx, "mcb200_get_timing");
+      rep->timed_flight_ms = tt[0];
+      rep->timed_flight_launches = (uint64_t)tt[1];
+      rep->timed_launches = (uint64_t)tt[5];
     }
     rep->steps_done = steps;
     // heat phase: the last window's mean potential, frozen

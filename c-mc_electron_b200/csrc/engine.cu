@@ -133,6 +133,9 @@ struct mcb200_ctx {
   // CUDA-event timing on the context's stream (mcb200_timing)
   bool timing = false;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t marks[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  void *flush_buf = nullptr;  // mcb200_flush_l2 scratch
+  size_t flush_bytes = 0;
   double flight_ms = 0, step_ms = 0;
   uint64_t flight_launches = 0, steps = 0, particles_flown = 0, launches = 0;
 
@@ -141,9 +144,12 @@ struct mcb200_ctx {
     cudaSetDevice(device);
     for (cudaEvent_t e : ev)
       if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : marks)
+      if (e) cudaEventDestroy(e);
     for (void *p : mesh_owned) cudaFree(p);
     for (void *p : store_owned) cudaFree(p);
     for (void *p : owned) cudaFree(p);
+    if (flush_buf) cudaFree(flush_buf);
     if (h_pinned) cudaFreeHost(h_pinned);
     if (h_scratch) cudaFreeHost(h_scratch);
     if (stream) cudaStreamDestroy(stream);
@@ -865,6 +871,53 @@ int mcb200_set_timing(mcb200_ctx *c, int enable) {
   }
 }
 
+int mcb200_flush_l2(mcb200_ctx *c, size_t bytes) {
+  if (!c || bytes == 0) return MCB200_ERR_ARG;
+  if (c->device < 0) return fail(c, MCB200_ERR_STATE, "host-only context");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    if (c->flush_bytes < bytes) {
+      if (c->flush_buf) cudaFree(c->flush_buf);
+      c->flush_buf = nullptr;
+      c->flush_bytes = 0;
+      ck(cudaMalloc(&c->flush_buf, bytes), "cudaMalloc");
+      c->flush_bytes = bytes;
+    }
+    ck(cudaMemsetAsync(c->flush_buf, c->launches & 0xff, bytes, c->stream), "memset");
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_mark(mcb200_ctx *c, int slot) {
+  if (!c || slot < 0 || slot >= 8) return MCB200_ERR_ARG;
+  if (c->device < 0) return fail(c, MCB200_ERR_STATE, "host-only context");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    if (!c->marks[slot]) ck(cudaEventCreate(&c->marks[slot]), "cudaEventCreate");
+    ck(cudaEventRecord(c->marks[slot], c->stream), "cudaEventRecord");
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_elapsed_ms(mcb200_ctx *c, int from, int to, double *ms) {
+  if (!c || !ms || from < 0 || from >= 8 || to < 0 || to >= 8) return MCB200_ERR_ARG;
+  if (!c->marks[from] || !c->marks[to]) return fail(c, MCB200_ERR_STATE, "mark not recorded");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    ck(cudaEventSynchronize(c->marks[to]), "cudaEventSynchronize");
+    float f = 0;
+    ck(cudaEventElapsedTime(&f, c->marks[from], c->marks[to]), "cudaEventElapsedTime");
+    *ms = f;
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
 int mcb200_get_timing(const mcb200_ctx *c, double *out, int n) {
   if (!c || !out) return MCB200_ERR_ARG;
   const double v[6] = {c->flight_ms, (double)c->flight_launches, c->step_ms, (double)c->steps,
@@ -1026,6 +1079,7 @@ int mcb200_deposit(mcb200_ctx *c) {
     const DepositScales S{{unit(be), unit(bh), unit(be + bh)}};
     if (fp32) launch_deposit(store<float>(c, c->cur), (int)c->n, c->mesh, c->fb, S, grid, s);
     else launch_deposit(store<double>(c, c->cur), (int)c->n, c->mesh, c->fb, S, grid, s);
+    c->launches += c->n > 0 ? 4 : 2;  // charge bounds, particle deposit, cell and node passes
     ck(cudaGetLastError(), "deposit");
     ck(cudaStreamSynchronize(s), "sync");
     c->fields_set = true;
@@ -1048,6 +1102,7 @@ int mcb200_solve_poisson(mcb200_ctx *c, double rel_tol, int max_iter, int *itera
     launch_pot2field(c->mesh, c->fb.potential, s);
     ck(cudaGetLastError(), "pot2field");
     ck(cudaStreamSynchronize(s), "sync");
+    c->launches += 17;  // rhs, 15 of the solve (set-up, dots, persistent CG, true residual), pot2field
     c->fields_set = true;
     return MCB200_OK;
   } catch (const std::exception &e) {
@@ -1124,6 +1179,7 @@ int mcb200_multiple_refresh(mcb200_ctx *c, const int32_t *desired_e, const int32
     };
     if (c->precision == MCB200_FLIGHT_FP32) refresh(float{});
     else refresh(double{});
+    c->launches += c->n > 0 ? 13 : 11;  // cell sort, count, two scans, emit
     ck(cudaGetLastError(), "refresh");
     unsigned int totals[2];
     long long g = 0;
@@ -1152,6 +1208,7 @@ int mcb200_set_potential(mcb200_ctx *c, const double *potential) {
     launch_pot2field(c->mesh, c->fb.potential, c->stream);
     ck(cudaGetLastError(), "pot2field");
     ck(cudaStreamSynchronize(c->stream), "sync");
+    c->launches += 1;
     c->fields_set = true;
     return MCB200_OK;
   } catch (const std::exception &e) {

@@ -77,7 +77,8 @@ class RunOptions(ctypes.Structure):
     _fields_ = [("table_dir", ctypes.c_char_p), ("data_dir", ctypes.c_char_p), ("flight_precision", ctypes.c_int),
                 ("poisson_every", ctypes.c_int), ("poisson_rel_tol", ctypes.c_double), ("max_steps", ctypes.c_int),
                 ("max_heat_steps", ctypes.c_int), ("write_outputs", ctypes.c_int), ("seed", ctypes.c_uint64),
-                ("verbose", ctypes.c_int)]
+                ("verbose", ctypes.c_int), ("warmup_steps", ctypes.c_int), ("readback_every_step", ctypes.c_int),
+                ("flush_l2_bytes", ctypes.c_size_t)]
 
 
 class RunReport(ctypes.Structure):
@@ -87,7 +88,10 @@ class RunReport(ctypes.Structure):
                 ("step_ms", ctypes.c_double), ("poisson_solves", ctypes.c_int),
                 ("poisson_iterations", ctypes.c_longlong), ("poisson_max_residual", ctypes.c_double),
                 ("last_current", ctypes.c_double * 1), ("heat_total", ctypes.c_double),
-                ("phase_s", ctypes.c_double * 8)]
+                ("phase_s", ctypes.c_double * 8), ("timed_device_ms", ctypes.c_double),
+                ("timed_wall_s", ctypes.c_double), ("timed_particle_steps", ctypes.c_uint64),
+                ("timed_steps", ctypes.c_int), ("timed_flight_ms", ctypes.c_double),
+                ("timed_flight_launches", ctypes.c_uint64), ("timed_launches", ctypes.c_uint64)]
 
 
 def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
@@ -138,6 +142,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mcb200_run_deck.argtypes = [c.c_char_p, c.c_int, c.POINTER(RunOptions), c.POINTER(RunReport), c.c_char_p,
                                     c.c_size_t]
     lib.mcb200_stat_begin.argtypes = [vp, c.c_int]
+    lib.mcb200_mark.argtypes = [vp, c.c_int]
+    lib.mcb200_flush_l2.argtypes = [vp, c.c_size_t]
+    lib.mcb200_elapsed_ms.argtypes = [vp, c.c_int, c.c_int, dp]
     lib.mcb200_stat_accumulate.argtypes = [vp]
     lib.mcb200_stat_get.argtypes = [vp, c.c_char_p, dp, c.c_size_t]
     lib.mcb200_set_potential.argtypes = [vp, dp]
@@ -446,13 +453,15 @@ class Deck:
 
 def run_deck(input_path: str, device: int = 0, data_dir: str | None = None, precision: int = FLIGHT_FP64,
              max_steps: int = 0, max_heat_steps: int = -1, poisson_every: int = 0, seed: int = 1,
-             write_outputs: bool = True, table_dir: str = DEFAULT_TABLE_DIR, verbose: bool = False) -> dict:
+             write_outputs: bool = True, table_dir: str = DEFAULT_TABLE_DIR, verbose: bool = False,
+             warmup_steps: int = 0, readback_every_step: bool = False, flush_l2_bytes: int = 0) -> dict:
     """The self-consistent simulation of a deck (mcb200_run_deck, the engine's
     `main input.txt`).  Returns the run report as a dict."""
     opt = RunOptions(table_dir=table_dir.encode(), data_dir=data_dir.encode() if data_dir else None,
                      flight_precision=precision, poisson_every=poisson_every, poisson_rel_tol=0.0,
                      max_steps=max_steps, max_heat_steps=max_heat_steps, write_outputs=int(write_outputs),
-                     seed=seed, verbose=int(verbose))
+                     seed=seed, verbose=int(verbose), warmup_steps=warmup_steps,
+                     readback_every_step=int(readback_every_step), flush_l2_bytes=flush_l2_bytes)
     rep = RunReport()
     err = ctypes.create_string_buffer(1024)
     rc = lib().mcb200_run_deck(os.fspath(input_path).encode(), device, ctypes.byref(opt), ctypes.byref(rep), err,

@@ -235,6 +235,15 @@ int mcb200_sync(mcb200_ctx *ctx);
 int mcb200_set_timing(mcb200_ctx *ctx, int enable);
 int mcb200_get_timing(const mcb200_ctx *ctx, double *out, int n);
 
+/* CUDA events on the context's stream: mcb200_mark records event `slot`
+ * (0..7); mcb200_elapsed_ms waits for `to` and returns the device time
+ * between two recorded marks. */
+int mcb200_mark(mcb200_ctx *ctx, int slot);
+/* Overwrite a scratch buffer of `bytes` (allocated on first use, held by the
+ * context) on the context's stream: evicts the L2 between timed steps. */
+int mcb200_flush_l2(mcb200_ctx *ctx, size_t bytes);
+int mcb200_elapsed_ms(mcb200_ctx *ctx, int from, int to, double *ms);
+
 /* Tallies since the last reset.  Any output may be NULL.
  * counters[MCB200_NUM_COUNTERS]; contact[16*6] per contact {NumParGen,
  * CharGen, EnergyGen, NumParCatch, CharCatch, EnergyCatch};
@@ -384,6 +393,9 @@ typedef struct {
   int write_outputs;
   uint64_t seed;             /* 0: 1 */
   int verbose;
+  int warmup_steps;          /* transport steps run before the timed ones (counted in max_steps) */
+  int readback_every_step;   /* read the tallies back to the host after every step */
+  size_t flush_l2_bytes;     /* >0: before every timed step write this many bytes (L2 eviction), timed apart */
 } mcb200_run_options;
 
 typedef struct {
@@ -399,6 +411,13 @@ typedef struct {
   double heat_total;              /* sum of the heat tallies over the heat windows (kT x charge) */
   double phase_s[8];              /* host wall time per phase: statistics, deposition, Poisson + fields,
                                      surface rates, carrier step, refresh, outputs, (unused) */
+  /* the timed transport steps (after warmup_steps): device time between
+     CUDA events on the context's stream, host wall time, particles flown */
+  double timed_device_ms, timed_wall_s;
+  uint64_t timed_particle_steps;
+  int timed_steps;
+  double timed_flight_ms;         /* flight-kernel device time within them */
+  uint64_t timed_flight_launches, timed_launches;
 } mcb200_run_report;
 
 /* `error` (may be NULL) receives a message on failure. */
