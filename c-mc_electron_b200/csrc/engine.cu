@@ -27,7 +27,10 @@ struct CapacityError : std::runtime_error {
 };
 
 void ck(cudaError_t e, const char *what) {
-  if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // clear the latched error so the next call does not report this one
+    throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+  }
 }
 
 template <typename T>
@@ -515,6 +518,7 @@ int mcb200_create(const char *table_dir, double kelvin, int device, size_t max_p
     c->y.contact = dalloc<long long>(kMaxContacts * 6, c->owned);
     c->total = dalloc<unsigned int>(1, c->owned);
     ck(cudaMallocHost(&c->h_pinned, 64 * sizeof(unsigned int)), "cudaMallocHost");
+    ck(cudaMallocHost(&c->h_scratch, 16 * sizeof(double)), "cudaMallocHost");
     ck(cudaMemsetAsync(c->y.counters, 0, sizeof(unsigned long long) * kCntNumCounters, c->stream), "memset");
     ck(cudaMemsetAsync(c->y.contact, 0, sizeof(long long) * kMaxContacts * 6, c->stream), "memset");
     ck(cudaStreamSynchronize(c->stream), "sync");
@@ -1044,7 +1048,6 @@ int mcb200_set_device(mcb200_ctx *c, const int32_t *material, const double *dono
     f.abs_sum = dalloc<unsigned long long>(4, c->mesh_owned);
     ck(cudaMemset(f.potential, 0, nodes * sizeof(double)), "memset");
     ck(cudaMemset(f.density, 0, nodes * sizeof(double)), "memset");
-    if (!c->h_scratch) ck(cudaMallocHost(&c->h_scratch, 16 * sizeof(double)), "cudaMallocHost");
     c->cg_plan = CgPlan{};
     c->device_set = true;
     return MCB200_OK;

@@ -1,0 +1,136 @@
+"""FP32-flight error report: each ensemble observable of the bulk n-Si
+velocity-field sweep (the frozen-field bulk box, 1 / 3 / 10 / 30 / 100 kV/cm)
+from FP32 flight against the all-FP64 run (the FP64 path is bit-exact with
+the reference's routines, so it stands for the CPU oracle too).
+
+The box is the bulk workload's (N_D = 1e17 cm^-3, 300 K, dt = 1 fs, 5 nm
+cells, REFLECT on every face) stretched to 1 um along the field (200 x 10 x
+10 cells) so that within the 0.8 ps measured few electrons reach the far
+wall.  Per field and precision: warm-up steps, then `blocks` windows of
+`block_steps` steps, each averaged with the window statistics
+(statistic(), src/mcmodel.cpp:1167-1408): drift velocity
+<v_x> = sum |q| v_x / sum |q| (m/s), mean energy sum |q| E / sum |q| (eV);
+from the store at the end: valley occupation (isym / 8); from the tallies:
+real phonon and impurity events per particle-step.  Standard errors are
+batch means over the windows (velocity, energy), binomial (valleys) and
+Poisson (event counts).
+
+    python -m mcb200.precision [--electrons 100000] [--json out.json]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+
+import numpy as np
+
+from . import FLIGHT_FP32, FLIGHT_FP64, lib
+from .workloads import bulk_box_engine
+
+FIELDS_KV_CM = (1.0, 3.0, 10.0, 30.0, 100.0)
+
+
+def _stat(eng, name: str, n: int) -> np.ndarray:
+    out = np.zeros(n)
+    eng._check(lib().mcb200_stat_get(eng._ctx, name.encode(), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                     n), f"mcb200_stat_get {name}")
+    return out
+
+
+SWEEP_BOX = dict(nx=200, ny=10, nz=10)
+
+
+def run_field(field_kv_cm: float, precision: int, electrons: int = 100000, warmup: int = 300, blocks: int = 5,
+              block_steps: int = 100, seed: int = 11, device: int = 0) -> dict:
+    eng, dt, _ = bulk_box_engine(electrons, seed, device, precision=precision, field_v_per_m=field_kv_cm * 1e5,
+                                 **SWEEP_BOX)
+    u = eng.units()
+    velo0 = u["spr0"] / u["time0"]
+    nodes = (eng.mesh.nx + 1) * (eng.mesh.ny + 1) * (eng.mesh.nz + 1)
+    step = 0
+    for _ in range(warmup):
+        eng.step(step, seed, dt)
+        step += 1
+    eng.reset_tallies()
+    flown = 0
+    v_blocks, e_blocks = [], []
+    for _ in range(blocks):
+        eng._check(lib().mcb200_stat_begin(eng._ctx, block_steps), "mcb200_stat_begin")
+        for _ in range(block_steps):
+            eng._check(lib().mcb200_stat_accumulate(eng._ctx), "mcb200_stat_accumulate")
+            n = eng.num_particles()
+            eng.step(step, seed, dt)
+            flown += n
+            step += 1
+        q = _stat(eng, "electron_q", nodes).sum()
+        v_blocks.append(_stat(eng, "electron_qvx", nodes).sum() / q * velo0)
+        e_blocks.append(_stat(eng, "electron_qe", nodes).sum() / q * u["eV0"])
+    t = eng.tallies()
+    p = eng.download()
+    eng.close()
+    valley = np.bincount(p["isym"] // 8, minlength=6) / len(p["isym"])
+    vb, eb = np.array(v_blocks), np.array(e_blocks)
+    return {
+        "field_kv_cm": field_kv_cm, "electrons": len(p["isym"]),
+        "drift_velocity_m_s": float(vb.mean()), "drift_velocity_se": float(vb.std(ddof=1) / np.sqrt(len(vb))),
+        "mean_energy_ev": float(eb.mean()), "mean_energy_se": float(eb.std(ddof=1) / np.sqrt(len(eb))),
+        "valley": valley.tolist(), "valley_se": np.sqrt(valley * (1 - valley) / len(p["isym"])).tolist(),
+        "phonon_per_particle_step": t["phonon"] / flown, "phonon_se": np.sqrt(t["phonon"]) / flown,
+        "impurity_per_particle_step": t["impurity"] / flown, "impurity_se": np.sqrt(t["impurity"]) / flown,
+        "caught": t["caught"], "zero_time": t["zero_time"],
+    }
+
+
+def compare(fp64: dict, fp32: dict) -> dict:
+    """Relative error of every FP32 observable against FP64, and the same in
+    combined standard errors."""
+    out = {}
+    for key, se in (("drift_velocity_m_s", "drift_velocity_se"), ("mean_energy_ev", "mean_energy_se"),
+                    ("phonon_per_particle_step", "phonon_se"), ("impurity_per_particle_step", "impurity_se")):
+        a, b = fp64[key], fp32[key]
+        sig = float(np.hypot(fp64[se], fp32[se]))
+        out[key] = {"fp64": a, "fp32": b, "rel_error": (b - a) / a if a else 0.0,
+                    "sigmas": (b - a) / sig if sig > 0 else 0.0}
+    va, vb = np.array(fp64["valley"]), np.array(fp32["valley"])
+    sa, sb = np.array(fp64["valley_se"]), np.array(fp32["valley_se"])
+    out["valley_max_sigmas"] = float(np.max(np.abs(vb - va) / np.hypot(sa, sb)))
+    out["valley_max_abs_error"] = float(np.max(np.abs(vb - va)))
+    return out
+
+
+def sweep(electrons: int = 100000, warmup: int = 300, blocks: int = 5, block_steps: int = 100,
+          fields=FIELDS_KV_CM, device: int = 0) -> list:
+    rows = []
+    for f in fields:
+        r64 = run_field(f, FLIGHT_FP64, electrons, warmup, blocks, block_steps, device=device)
+        r32 = run_field(f, FLIGHT_FP32, electrons, warmup, blocks, block_steps, device=device)
+        rows.append({"field_kv_cm": f, "fp64": r64, "fp32": r32, "error": compare(r64, r32)})
+    return rows
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--electrons", type=int, default=100000)
+    ap.add_argument("--warmup", type=int, default=300)
+    ap.add_argument("--blocks", type=int, default=5)
+    ap.add_argument("--block-steps", type=int, default=100)
+    ap.add_argument("--json", default=None)
+    a = ap.parse_args()
+    rows = sweep(a.electrons, a.warmup, a.blocks, a.block_steps)
+    print(f"{'E kV/cm':>8} {'vd FP64 m/s':>12} {'vd FP32':>12} {'rel':>8} {'sig':>5}  "
+          f"{'E FP64 eV':>9} {'E FP32':>9} {'rel':>8} {'sig':>5}  {'imp rel':>8} {'ph rel':>8} {'valley sig':>10}")
+    for r in rows:
+        e = r["error"]
+        v, en = e["drift_velocity_m_s"], e["mean_energy_ev"]
+        print(f"{r['field_kv_cm']:8.0f} {v['fp64']:12.4g} {v['fp32']:12.4g} {v['rel_error']:8.1e} {v['sigmas']:5.1f}  "
+              f"{en['fp64']:9.4f} {en['fp32']:9.4f} {en['rel_error']:8.1e} {en['sigmas']:5.1f}  "
+              f"{e['impurity_per_particle_step']['rel_error']:8.1e} {e['phonon_per_particle_step']['rel_error']:8.1e} "
+              f"{e['valley_max_sigmas']:10.1f}")
+    if a.json:
+        with open(a.json, "w") as f:
+            json.dump(rows, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()
