@@ -203,7 +203,7 @@ def finfet_run(args, device: int, precision: str, readback: bool = False) -> dic
 
 def engine_arm(args, rank: int, world: int, device: int):
     runs = {p: finfet_run(args, device, p) for p in ("fp64", "fp32")}
-    e2e = finfet_run(args, device, "fp32", readback=True)
+    e2e = finfet_run(args, device, "fp32", readback=True) if args.workload == "all" else runs["fp32"]
     peak, peak_kind = measured_peaks()
     value = {}
     for p, r in runs.items():
@@ -232,7 +232,7 @@ def engine_arm(args, rank: int, world: int, device: int):
     cg = {"solves": r32["poisson_solves"], "iterations": r32["poisson_iterations"],
           "max_rel_residual": r32["poisson_max_residual"]}
     bulk = {}
-    for p in ("fp64", "fp32"):
+    for p in (("fp64", "fp32") if args.workload == "all" else ()):
         m = measure_precision(args, rank, world, device, p)
         bulk[p] = {"value": m["value"], "flight_ms_per_launch": m["flight_ms_per_launch"],
                    "roofline_frac": m["achieved"] / peak, "achieved_gbs": m["achieved"],
@@ -265,7 +265,7 @@ def engine_arm(args, rank: int, world: int, device: int):
         "poisson": cg,
         "phase_s_fp32": r32["phase_s"], "phase_s_fp64": r64["phase_s"],
         "bulk": bulk,
-        "bulk_fp32_over_fp64": bulk["fp32"]["value"] / bulk["fp64"]["value"],
+        "bulk_fp32_over_fp64": bulk["fp32"]["value"] / bulk["fp64"]["value"] if bulk else None,
     }
 
 
@@ -384,6 +384,8 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--particles", type=int, default=2_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="all", choices=["all", "finfet"],
+                    help="finfet: only the two FinFET arms (no e2e rerun, no bulk box): for profiling")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
