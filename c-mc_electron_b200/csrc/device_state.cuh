@@ -24,16 +24,22 @@ enum MotionRule : int { kPass = 1, kReflect = 2, kScattOx = 3, kPeriod = 4, kGen
 // Face directions, same header :204.
 enum Dir : int { kUp = 0, kDown = 1, kLeft = 2, kRight = 3, kFront = 4, kBack = 5 };
 
-// Full-band tables in device memory.  Per-tetrahedron data the free flight
-// touches on every event is packed into one record so a tet's geometry
-// arrives in whole 32-byte sectors from L2 (the table stays L2-resident on
-// B200: 160 B x 55320 tets = 8.9 MB in FP64, half that in FP32).  R is the
+// Full-band tables in device memory.  Everything the free flight reads about
+// a tetrahedron on an event (face planes, velocity, neighbours, majorant,
+// energy span, band) is packed into one record: one 128-byte L2 line in
+// FP32, two in FP64 (55320 tets: 7 MB / 14 MB, L2-resident on B200).  R is the
 // arithmetic type of the flight kinematics: double for the plain path,
 // float for the FP32-flight path.
 template <typename R>
 struct TetFlightT {
-  R n[4][4];  // face f: inward normal (n[f][0..2]) and offset n[f][3]
-  R v[4];     // group velocity (v[0..2]) and base energy v[3]
+  R n[4][4];    // face f: inward normal (n[f][0..2]) and offset n[f][3]
+  R v[4];       // group velocity (v[0..2]) and base energy v[3]
+  int neib[4];  // NeibrTet per face (>= 0 tet, < 0 wedge / BZ code)
+  R gam;        // gamtet: the variable-gamma phonon majorant
+  R e0, e3;     // lowest and highest node energy
+  int band;     // ibt
+  int node0;    // the first (lowest) node, the base of GetEnergy
+  int pad[sizeof(R) == 4 ? 3 : 12];  // one 128-byte line (FP32) / two (FP64)
 };
 template <typename R>
 struct TetShapeT {

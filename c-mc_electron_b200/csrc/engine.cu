@@ -159,6 +159,9 @@ struct mcb200_ctx {
   }
 };
 
+static_assert(sizeof(TetFlightT<float>) == 128, "FP32 tet record: one 128-byte line");
+static_assert(sizeof(TetFlightT<double>) == 256, "FP64 tet record: two 128-byte lines");
+
 namespace {
 
 int fail(mcb200_ctx *c, int code, const std::string &msg) {
@@ -286,7 +289,7 @@ void upload_tables32(mcb200_ctx *c, const std::vector<TetFlight> &tf, const std:
                      const std::vector<double4> &kn) {
   const FullBandTables &t = c->tab;
   DevTables32 &d = c->dt.f32;
-  std::vector<TetFlightT<float>> tf32(tf.size());
+  std::vector<TetFlightT<float>> tf32(tf.size(), TetFlightT<float>{});
   std::vector<TetShapeT<float>> ts32(ts.size());
   for (size_t it = 0; it < tf.size(); ++it) {
     for (int f = 0; f < 4; ++f) {
@@ -296,6 +299,12 @@ void upload_tables32(mcb200_ctx *c, const std::vector<TetFlight> &tf, const std:
       for (int cc = 0; cc < 4; ++cc) tf32[it].n[f][cc] = (float)(n[cc] * sc);
     }
     for (int cc = 0; cc < 4; ++cc) tf32[it].v[cc] = (float)tf[it].v[cc];
+    for (int f = 0; f < 4; ++f) tf32[it].neib[f] = tf[it].neib[f];
+    tf32[it].gam = (float)tf[it].gam;
+    tf32[it].e0 = (float)tf[it].e0;
+    tf32[it].e3 = (float)tf[it].e3;
+    tf32[it].band = tf[it].band;
+    tf32[it].node0 = tf[it].node0;
     for (int v = 0; v < 4; ++v) ts32[it].e[v] = (float)ts[it].e[v];
     for (int v = 0; v < 3; ++v) ts32[it].fac[v] = (float)ts[it].fac[v];
     ts32[it].vgt = (float)ts[it].vgt;
@@ -330,13 +339,19 @@ void upload_tables(mcb200_ctx *c) {
   d.mell = t.mell; d.melt = t.melt; d.meld = t.meld;
   d.a0pi = t.u.a0pi; d.sieg = t.u.sieg; d.eV0 = t.u.eV0; d.conc0 = t.u.conc0; d.scrt0 = t.u.scrt0;
   d.eps_si = t.u.eps_silicon; d.frickel = t.u.frickel;
-  std::vector<TetFlight> tf(t.nt);
+  std::vector<TetFlight> tf(t.nt, TetFlight{});
   std::vector<TetShape> ts(t.nt);
   std::vector<int4> tn(t.nt), tb(t.nt);
   for (int it = 0; it < t.nt; ++it) {
     for (int f = 0; f < 4; ++f)
       for (int cc = 0; cc < 4; ++cc) tf[it].n[f][cc] = t.D(cc, f, it);
     for (int cc = 0; cc < 4; ++cc) tf[it].v[cc] = t.vt[(size_t)4 * it + cc];
+    for (int f = 0; f < 4; ++f) tf[it].neib[f] = t.N(f, it);
+    tf[it].gam = t.gamtet[it];
+    tf[it].e0 = t.eek[t.T(0, it)];
+    tf[it].e3 = t.eek[t.T(3, it)];
+    tf[it].band = t.ibt[it];
+    tf[it].node0 = t.T(0, it);
     for (int v = 0; v < 4; ++v) ts[it].e[v] = t.eek[t.T(v, it)];
     ts[it].fac[0] = t.faclow[it]; ts[it].fac[1] = t.facmedium[it]; ts[it].fac[2] = t.fachigh[it];
     ts[it].vgt = t.vgt[it];

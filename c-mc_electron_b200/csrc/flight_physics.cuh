@@ -242,11 +242,12 @@ struct FlyerT {
   __device__ void GetEnergy() {
     R dx, dy, dz;
     in_wedge(dx, dy, dz, kx, ky, kz);
-    const V4 k0 = TB::knode(F.T)[F.T.tnode[itet].x];
+    const TetFlightT<R> &t = tf(itet);
+    const V4 k0 = TB::knode(F.T)[t.node0];
     dx -= k0.x;
     dy -= k0.y;
     dz -= k0.z;
-    const R *v = tf(itet).v;
+    const R *v = t.v;
     energy = v[3] + v[0] * dx + v[1] * dy + v[2] * dz;
   }
   __device__ __forceinline__ R face_dist(int it, int f, R a, R b, R c) const {
@@ -357,7 +358,7 @@ struct FlyerT {
         }
       }
       if (fmin < 0) return it;
-      const int nb = (&F.T.tneib[it].x)[fmin];
+      const int nb = tf(it).neib[fmin];
       if (nb < 0) return -1;
       it = nb;
     }
@@ -394,8 +395,9 @@ struct FlyerT {
     isym = F.T.indmat[((((sx * 3 + sy) * 3 + sz) * 3 + p0) * 3 + p1) * 3 + p2];
     R a, b, c;
     in_wedge(a, b, c, kx, ky, kz);
-    if (iband == F.T.ibt[itet] && tet_contains(itet, a, b, c)) return;
-    int start = iband == F.T.ibt[itet] ? itet : -1;
+    const bool same_band = iband == tf(itet).band;
+    if (same_band && tet_contains(itet, a, b, c)) return;
+    int start = same_band ? itet : -1;
     if (iband == F.T.bandof[0]) {  // lowest conduction band: start next to the point
       const int sg = kSeedGridN;
       const int si = min(max((int)m_floor((a - (R)F.T.grid_lo[0]) * (R)F.T.seed_inv[0]), 0), sg - 1);
@@ -437,14 +439,14 @@ struct FlyerT {
   __device__ bool bz_surface_search() {
     R a, b, c;
     in_wedge(a, b, c, kx, ky, kz);
-    if (iband == F.T.ibt[itet] && tet_contains(itet, a, b, c)) return true;
+    if (iband == tf(itet).band && tet_contains(itet, a, b, c)) return true;
     int ie = (int)(energy * F.T.dlist);
     if (ie < 0) ie = 0;
     if (ie >= kMWLE) ie = kMWLE - 1;
     const int p = F.T.pslist[ie * kMNB + iband], cnt = F.T.nslist[ie * kMNB + iband];
     for (int itl = p; itl <= p + cnt - 1; ++itl) {
       const int it = F.T.slist[itl];
-      if (iband == F.T.ibt[it] && tet_contains(it, a, b, c)) {
+      if (iband == tf(it).band && tet_contains(it, a, b, c)) {
         itet = it;
         return true;
       }
@@ -455,7 +457,7 @@ struct FlyerT {
   // HitTet, src/TetHit.cpp:109-142.  After a BZ-boundary crossing the tet
   // search and GetEnergy run in run_locate.
   __device__ void HitTet() {
-    const int nb = (&F.T.tneib[itet].x)[itetdir];
+    const int nb = tf(itet).neib[itetdir];
     if (nb >= 0) {
       itet = nb;
     } else if (nb == -5 || nb == -6) {
@@ -773,7 +775,7 @@ struct FlyerT {
   // leaves the mechanism search to run_pick.
   __device__ void phonon_event() {
     const R scasum = CALSCATTSUM((R)energy, iband);
-    const R g = TB::gamtet(F.T)[itet];
+    const R g = tf(itet).gam;
     const R drand = scasum > g ? Random() * scasum : Random() * g;
     if (scasum < drand) {
       self = true;
@@ -825,10 +827,10 @@ struct FlyerT {
     R eemax;
     if constexpr (sizeof(R) == 4) eemax = imp_emax;
     else eemax = T.frickel * 4 * kPiD * Rho / (8.0 * T.melt * T.eps_si);
-    const TetShapeT<R> &s = ts(itet);
+    const TetFlightT<R> &s = tf(itet);
     R gammax;
-    if (eemax < s.e[0]) gammax = GetImpScRate(s.e[0]);
-    else if (eemax > s.e[3]) gammax = GetImpScRate(s.e[3]);
+    if (eemax < s.e0) gammax = GetImpScRate(s.e0);
+    else if (eemax > s.e3) gammax = GetImpScRate(s.e3);
     else gammax = GetImpScRate(eemax);
     const R floor_ = (R)(1.0 / T.scrt0);
     return gammax > floor_ ? gammax : floor_;
@@ -1104,7 +1106,7 @@ struct FlyerT {
     too_far = false;
     zero_run = 0;
     load_cell_fields();
-    iband = F.T.ibt[itet];
+    iband = tf(itet).band;
     GetV();
     loop = 0;
     surf_gamma = 0;
@@ -1121,7 +1123,7 @@ struct FlyerT {
     if (get_tet) { TetTf = TetTime(); get_tet = false; }
     if (get_cell) { CellTf = CellTime(); get_cell = false; }
     if (get_ph) { phrnl = -m_log(Random()); get_ph = false; }
-    const R g = TB::gamtet(F.T)[itet];
+    const R g = tf(itet).gam;
     R PhScTf, ImpScTf, SurfScTf, Tf;
     PhScTf = phrnl / g;
     if (iband == F.T.bandof[0]) {
