@@ -12,6 +12,7 @@
 #include "flight_physics.cuh"
 #include "fullband_tables.h"
 #include "mcb200.h"
+#include "mg_setup.h"
 #include "poisson_setup.h"
 #include "stat_kernels.h"
 
@@ -122,6 +123,8 @@ struct mcb200_ctx {
   // deposition / Poisson (mcb200_set_device)
   FieldBuffers fb{};
   CgPlan cg_plan;
+  MgDevice mg{};                            // multigrid hierarchy of the Poisson stencil (mcb200_set_device)
+  int cg_method = kCgAuto, cg_blocks = 0;   // mcb200_set_poisson_solver
   bool device_set = false;
   double *h_scratch = nullptr;  // pinned, 16 doubles
   // window statistics (mcb200_stat_*)
@@ -690,6 +693,8 @@ int mcb200_set_mesh(mcb200_ctx *c, int nx, int ny, int nz, const double *lx, con
     c->cells_set = c->fields_set = c->device_set = false;
     c->fb = FieldBuffers{};
     c->cg_plan = CgPlan{};
+    c->cg_plan.method = c->cg_method;
+    c->cg_plan.blocks = c->cg_blocks;
     return mcb200_reset_tallies(c);
   } catch (const std::exception &e) {
     return fail(c, MCB200_ERR_CUDA, e.what());
@@ -1063,7 +1068,27 @@ int mcb200_set_device(mcb200_ctx *c, const int32_t *material, const double *dono
     f.abs_sum = dalloc<unsigned long long>(4, c->mesh_owned);
     ck(cudaMemset(f.potential, 0, nodes * sizeof(double)), "memset");
     ck(cudaMemset(f.density, 0, nodes * sizeof(double)), "memset");
+    {  // multigrid hierarchy of the stencil, node coordinates from the cell widths
+      std::vector<double> X(m.nx + 1, 0.0), Y(m.ny + 1, 0.0), Z(m.nz + 1, 0.0);
+      for (int i = 0; i < m.nx; ++i) X[i + 1] = X[i] + dx[i];
+      for (int j = 0; j < m.ny; ++j) Y[j + 1] = Y[j] + dy[j];
+      for (int k = 0; k < m.nz; ++k) Z[k + 1] = Z[k] + dz[k];
+      bool built = false;
+      MgHierarchy h;
+      try {
+        h = MgHierarchy::build(m.nx + 1, m.ny + 1, m.nz + 1, X, Y, Z, s.stencil, s.dirichlet);
+        built = true;
+      } catch (const std::logic_error &) {  // a mesh that does not coarsen: Jacobi preconditioning
+      } catch (const std::runtime_error &) {
+      }
+      if (built) {
+        c->mg = mg_upload(h, c->mesh_owned);
+        f.mg = &c->mg;
+      }
+    }
     c->cg_plan = CgPlan{};
+    c->cg_plan.method = c->cg_method;
+    c->cg_plan.blocks = c->cg_blocks;
     c->device_set = true;
     return MCB200_OK;
   } catch (const std::exception &e) {
@@ -1120,12 +1145,35 @@ int mcb200_solve_poisson(mcb200_ctx *c, double rel_tol, int max_iter, int *itera
     launch_pot2field(c->mesh, c->fb.potential, s);
     ck(cudaGetLastError(), "pot2field");
     ck(cudaStreamSynchronize(s), "sync");
-    c->launches += 17;  // rhs, 15 of the solve (set-up, dots, persistent CG, true residual), pot2field
+    // rhs, the solve's set-up / dots / persistent CG / true residual (15 with
+    // Jacobi preconditioning, 12 with multigrid: no Jacobi z0 or r.z0), pot2field
+    c->launches += c->cg_plan.used == kCgMultigrid ? 14 : 17;
     c->fields_set = true;
     return MCB200_OK;
   } catch (const std::exception &e) {
     return fail(c, MCB200_ERR_CUDA, e.what());
   }
+}
+
+int mcb200_set_poisson_solver(mcb200_ctx *c, int method, int blocks) {
+  if (!c || method < MCB200_POISSON_AUTO || method > MCB200_POISSON_MULTIGRID || blocks < 0 || blocks > kCgMaxGrid)
+    return c ? fail(c, MCB200_ERR_ARG, "mcb200_set_poisson_solver: bad arguments") : MCB200_ERR_ARG;
+  if (method == MCB200_POISSON_MULTIGRID && c->device_set && !c->fb.mg)
+    return fail(c, MCB200_ERR_STATE, "mcb200_set_poisson_solver: no multigrid hierarchy for this device");
+  c->cg_method = method;
+  c->cg_blocks = blocks;
+  c->cg_plan.method = method;
+  c->cg_plan.blocks = blocks;
+  c->cg_plan.grid = 0;  // re-planned by the next solve
+  return MCB200_OK;
+}
+
+int mcb200_get_poisson_solver(mcb200_ctx *c, int *method_used, int *blocks, int *levels) {
+  if (!c) return MCB200_ERR_ARG;
+  if (method_used) *method_used = c->cg_plan.used;
+  if (blocks) *blocks = c->cg_plan.grid;
+  if (levels) *levels = c->fb.mg ? c->mg.levels : 0;
+  return MCB200_OK;
 }
 
 int mcb200_surface_rates(mcb200_ctx *c, const mcb200_surface_params *p, const int32_t *eeff_direction) {

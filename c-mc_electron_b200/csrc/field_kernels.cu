@@ -19,6 +19,7 @@
 
 #include "device_state.cuh"
 #include "field_kernels.h"
+#include "poisson_common.cuh"
 
 namespace mcb200 {
 
@@ -127,15 +128,6 @@ __global__ void rhs_kernel(int nodes, const double *density, const double *pvol,
   else rhs[p] = fabs(density[p]) > 0 ? density[p] * pvol[p] + pdop[p] : 0.0;
 }
 
-struct Grid3 {
-  int px, py, pz;
-};
-__device__ __forceinline__ void node_ijk(int p, const Grid3 &g, int &i, int &j, int &k) {
-  k = p % g.pz;
-  const int t = p / g.pz;
-  i = t % g.px;
-  j = t / g.px;
-}
 
 // y = A_ff x on free nodes (Dirichlet neighbours excluded); Dirichlet rows: y = 0.
 // With `rhs`, writes b_ff - A x instead, where b_ff folds the Dirichlet values
@@ -165,22 +157,7 @@ __global__ void stencil_apply(int nodes, Grid3 g, const double *st, const uint8_
   y[p] = rhs ? (rhs[p] - fold) - acc : acc;
 }
 
-// Fixed-order block partial sums of a[i]*b[i] (first stage of a dot product).
-template <int B>
-__device__ double block_sum(double v) {
-  __shared__ double s[B];
-  s[threadIdx.x] = v;
-  __syncthreads();
-  for (int o = B / 2; o > 0; o >>= 1) {
-    if (threadIdx.x < o) s[threadIdx.x] += s[threadIdx.x + o];
-    __syncthreads();
-  }
-  const double r = s[0];
-  __syncthreads();
-  return r;
-}
 
-constexpr int kRedBlock = 256;
 constexpr int kRedGrid = 296;  // 2 x 148 SMs; fixed so the reduction order is fixed
 
 __global__ void __launch_bounds__(kRedBlock) dot_partial(int n, const double *a, const double *b, double *part) {
@@ -243,11 +220,6 @@ __global__ void set_dirichlet(int nodes, const uint8_t *dir, const double *rhs, 
 // itself, in the same fixed order, so every block takes the same scalars and
 // the same convergence decision, and a solve is bit-reproducible for a given
 // grid.
-__device__ __forceinline__ double sum_partials(const double *part, int n) {
-  double v = 0.0;
-  for (int i = threadIdx.x; i < n; i += kRedBlock) v += part[i];
-  return block_sum<kRedBlock>(v);
-}
 
 __global__ void __launch_bounds__(kRedBlock) cg_persistent(int nodes, Grid3 g, const double *st, const uint8_t *dir,
                                                            const double *diag_inv, double *x, double *r, double *z,
@@ -405,6 +377,8 @@ int cg_solve(const DevMesh &M, const FieldBuffers &f, double rel_tol, int max_it
   const int nodes = (M.nx + 1) * (M.ny + 1) * (M.nz + 1);
   const Grid3 g{M.nx + 1, M.ny + 1, M.nz + 1};
   const int nb = blocks(nodes, 256);
+  const bool use_mg = f.mg && plan.method != kCgJacobi;
+  if (plan.method == kCgMultigrid && !f.mg) return 1;
   double *sc = f.cg_scalars;
   // ||b_free|| with the Dirichlet values folded in
   set_dirichlet<<<nb, 256, 0, s>>>(nodes, f.dirichlet, f.rhs, f.potential);
@@ -412,29 +386,43 @@ int cg_solve(const DevMesh &M, const FieldBuffers &f, double rel_tol, int max_it
   dot(nodes, f.cg_q, f.cg_q, f.cg_part, sc + 6, s);
   // r = b - A x (x: the previous potential, a warm start)
   stencil_apply<<<nb, 256, 0, s>>>(nodes, g, f.stencil, f.dirichlet, f.potential, f.rhs, f.cg_r);
-  cg_init<<<nb, 256, 0, s>>>(nodes, f.cg_r, f.diag_inv, f.cg_z, f.cg_p, f.dirichlet, f.rhs, f.potential);
-  dot(nodes, f.cg_r, f.cg_z, f.cg_part, sc + 0, s);
+  if (!use_mg) {
+    cg_init<<<nb, 256, 0, s>>>(nodes, f.cg_r, f.diag_inv, f.cg_z, f.cg_p, f.dirichlet, f.rhs, f.potential);
+    dot(nodes, f.cg_r, f.cg_z, f.cg_part, sc + 0, s);
+  }
   dot(nodes, f.cg_r, f.cg_r, f.cg_part, sc + 3, s);
   cg_setup<<<1, 1, 0, s>>>(sc, rel_tol * rel_tol);
-  // every iteration in one cooperative launch (cg_persistent)
-  if (plan.grid == 0) {
-    int dev = 0, sms = 0, per_sm = 0, coop = 0;
+  // every iteration in one cooperative launch (cg_persistent / cg_mg_persistent)
+  if (plan.grid == 0 || plan.used != (use_mg ? kCgMultigrid : kCgJacobi)) {
+    int dev = 0, sms = 0, per_sm = 0, coop = 0, most = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-    if (!coop || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_persistent, kRedBlock, 0) != cudaSuccess ||
-        per_sm < 1)
-      return 1;
-    plan.grid = std::min(per_sm * sms, kCgMaxGrid);
+    if (use_mg) {
+      most = cg_mg_max_grid();
+    } else if (coop &&
+               cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_persistent, kRedBlock, 0) == cudaSuccess) {
+      most = per_sm * sms;
+    }
+    if (most < 1) return 1;
+    most = std::min(most, kCgMaxGrid);
+    plan.grid = plan.blocks > 0 ? std::min(plan.blocks, most) : most;
+    plan.used = use_mg ? kCgMultigrid : kCgJacobi;
   }
-  int nodes_arg = nodes, max_arg = max_iter;
-  Grid3 g_arg = g;
-  const double *st = f.stencil, *dinv = f.diag_inv;
-  const uint8_t *dirp = f.dirichlet;
   double *x = f.potential, *r = f.cg_r, *z = f.cg_z, *p0 = f.cg_p, *p1 = f.cg_p1, *q = f.cg_q, *part = f.cg_part;
-  void *args[] = {&nodes_arg, &g_arg, &st, &dirp, &dinv, &x, &r, &z, &p0, &p1, &q, &part, &sc, &max_arg};
-  if (cudaLaunchCooperativeKernel((const void *)cg_persistent, plan.grid, kRedBlock, args, 0, s) != cudaSuccess)
-    return 1;
+  if (use_mg) {
+    if (launch_cg_mg(nodes, g, f.stencil, f.dirichlet, x, r, z, p0, p1, q, part, sc, max_iter, *f.mg, plan.grid, s) !=
+        cudaSuccess)
+      return 1;
+  } else {
+    int nodes_arg = nodes, max_arg = max_iter;
+    Grid3 g_arg = g;
+    const double *st = f.stencil, *dinv = f.diag_inv;
+    const uint8_t *dirp = f.dirichlet;
+    void *args[] = {&nodes_arg, &g_arg, &st, &dirp, &dinv, &x, &r, &z, &p0, &p1, &q, &part, &sc, &max_arg};
+    if (cudaLaunchCooperativeKernel((const void *)cg_persistent, plan.grid, kRedBlock, args, 0, s) != cudaSuccess)
+      return 1;
+  }
   plan.launches += 1;
   cudaMemcpyAsync(host_scratch, sc, 10 * sizeof(double), cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return 1;

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include "device_state.cuh"
+#include "mg_kernels.h"
 
 namespace mcb200 {
 
@@ -24,6 +25,7 @@ struct FieldBuffers {
   double *cg_r = nullptr, *cg_z = nullptr, *cg_p = nullptr, *cg_p1 = nullptr, *cg_q = nullptr, *cg_part = nullptr,
          *cg_scalars = nullptr;
   unsigned long long *abs_sum = nullptr;
+  const MgDevice *mg = nullptr;  // multigrid hierarchy of the stencil (null: Jacobi preconditioning only)
 };
 
 // Fixed-point units (powers of two) of the deposition sums: electron cell
@@ -42,8 +44,12 @@ void launch_rhs(int nodes, const FieldBuffers &f, cudaStream_t s);
 // The CG iterations of one solve run in one cooperative launch; its grid
 // (blocks) is fixed per context on first use, so the reduction order is too.
 constexpr int kCgMaxGrid = 1024;
+enum CgMethod { kCgAuto = 0, kCgJacobi = 1, kCgMultigrid = 2 };
 struct CgPlan {
-  int grid = 0;
+  int method = kCgAuto;  // kCgAuto: multigrid when the hierarchy exists
+  int blocks = 0;        // requested grid (0: the largest co-resident grid, at most kCgMaxGrid)
+  int grid = 0;          // grid in use (0 until the first solve)
+  int used = 0;          // kCgJacobi or kCgMultigrid, set by the last solve
   unsigned long long launches = 0;
 };
 // Returns 0 on success; host_scratch must hold 10 doubles (pinned).

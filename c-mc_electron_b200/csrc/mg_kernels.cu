@@ -1,0 +1,427 @@
+// mg_kernels.cu -- conjugate gradients preconditioned by one geometric
+// multigrid V-cycle, every iteration of a solve in one cooperative launch.
+//
+// The reference factorises its finite-volume Poisson matrix with KLU and
+// solves it every step (MeshQuantities::linear_poisson_solver,
+// src/mcmodel.cpp:2714-2730).  Here the Dirichlet contact rows are
+// eliminated and the remaining SPD system is solved by CG in FP64 to a
+// relative residual; the preconditioner is a symmetric V-cycle over the
+// hierarchy of mg_setup.h: damped Jacobi (nu sweeps before and after the
+// coarse correction, weight 1.6 / rho(D^-1 A) per level), residual
+// restriction by P^T (gather over the 3 x 3 x 3 fine neighbourhood of each
+// coarse node), the exact dense inverse on the coarsest level, trilinear
+// prolongation.  Every phase is a grid-stride pass over one level's nodes
+// separated by grid-wide barriers; nothing is accumulated with atomics and
+// the dot products use fixed-order reductions, so a solve is
+// bit-reproducible for a given grid.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <stdexcept>
+
+#include "mg_kernels.h"
+#include "poisson_common.cuh"
+
+namespace mcb200 {
+
+namespace cg = cooperative_groups;
+
+namespace {
+
+__device__ __forceinline__ double axis_weight(const int2 *cm, const double2 *wm, int i, int c) {
+  const int2 cc = cm[i];
+  const double2 w = wm[i];
+  double v = 0.0;
+  if (cc.x == c) v += w.x;
+  if (cc.y == c && cc.y != cc.x) v += w.y;
+  return v;
+}
+
+// (A x)[n] with the 7-point stencil of the CG (-x, +x, -y, +y, -z, +z,
+// diagonal).  x is zero on Dirichlet nodes and isolated nodes have no
+// couplings, so no neighbour needs masking.
+__device__ __forceinline__ double apply7(const double *st7, const Grid3 &g, const double *x, int n) {
+  int i, j, k;
+  node_ijk(n, g, i, j, k);
+  const double *a = st7 + (size_t)n * 7;
+  double acc = a[6] * x[n];
+  if (i > 0) acc += a[0] * x[n - g.pz];
+  if (i + 1 < g.px) acc += a[1] * x[n + g.pz];
+  if (j > 0) acc += a[2] * x[n - g.px * g.pz];
+  if (j + 1 < g.py) acc += a[3] * x[n + g.px * g.pz];
+  if (k > 0) acc += a[4] * x[n - 1];
+  if (k + 1 < g.pz) acc += a[5] * x[n + 1];
+  return acc;
+}
+
+// (A x)[n] with a level's 27-point Galerkin stencil, entry ((di+1)*3 + (dj+1))*3 + (dk+1).
+__device__ __forceinline__ double apply27(const MgDevLevel &L, const double *x, int n) {
+  int i, j, k;
+  node_ijk(n, Grid3{L.px, L.py, L.pz}, i, j, k);
+  const double *a = L.st + (size_t)n * 27;
+  double acc = 0.0;
+  for (int di = -1; di <= 1; ++di) {
+    const int i2 = i + di;
+    if (i2 < 0 || i2 >= L.px) continue;
+    for (int dj = -1; dj <= 1; ++dj) {
+      const int j2 = j + dj;
+      if (j2 < 0 || j2 >= L.py) continue;
+      const double *ar = a + ((di + 1) * 3 + (dj + 1)) * 3;
+      const int base = (j2 * L.px + i2) * L.pz + k;
+      if (k > 0) acc += ar[0] * x[base - 1];
+      acc += ar[1] * x[base];
+      if (k + 1 < L.pz) acc += ar[2] * x[base + 1];
+    }
+  }
+  return acc;
+}
+
+struct Solve {
+  const MgDevice &mg;
+  const double *st7;
+  Grid3 g0;
+  int tid, stride;
+  unsigned cur;  // bit l: level l's iterate is in xb (else xa)
+
+  __device__ double *X(int l) const { return (cur >> l) & 1u ? mg.L[l].xb : mg.L[l].xa; }
+  __device__ double *Xo(int l) const { return (cur >> l) & 1u ? mg.L[l].xa : mg.L[l].xb; }
+  __device__ double A(int l, const double *x, int n) const {
+    return l == 0 ? apply7(st7, g0, x, n) : apply27(mg.L[l], x, n);
+  }
+
+  // First sweep from a zero iterate: x = omega D^-1 b (level 0's isolated
+  // rows: D^-1 b), for node n.
+  __device__ void first(int l, int n, double b) const {
+    const MgDevLevel &L = mg.L[l];
+    X(l)[n] = L.dir[n] ? (l == 0 ? L.dinv[n] * b : 0.0) : L.omega * L.dinv[n] * b;
+  }
+  // One damped-Jacobi sweep into the other buffer; returns sum b.x_new of
+  // this thread's nodes when `dot`.
+  __device__ double sweep(int l, bool dot) {
+    const MgDevLevel &L = mg.L[l];
+    const double *xc = X(l), *b = L.b;
+    double *xn = Xo(l);
+    double acc = 0.0;
+    for (int n = tid; n < L.n; n += stride) {
+      double v;
+      if (L.dir[n]) v = l == 0 ? L.dinv[n] * b[n] : 0.0;
+      else v = xc[n] + L.omega * L.dinv[n] * (b[n] - A(l, xc, n));
+      xn[n] = v;
+      if (dot) acc += b[n] * v;
+    }
+    cur ^= 1u << l;
+    return acc;
+  }
+  __device__ void residual(int l) const {
+    const MgDevLevel &L = mg.L[l];
+    const double *x = X(l);
+    for (int n = tid; n < L.n; n += stride) L.r[n] = L.dir[n] ? 0.0 : L.b[n] - A(l, x, n);
+  }
+  // b_{l+1} = P^T r_l, and the first sweep of level l+1 unless it is the coarsest.
+  __device__ void restrict_to(int l) const {
+    const MgDevLevel &F = mg.L[l], &C = mg.L[l + 1];
+    const bool smooth = l + 2 < mg.levels;
+    const Grid3 gc{C.px, C.py, C.pz};
+    for (int c = tid; c < C.n; c += stride) {
+      if (C.dir[c]) {
+        C.b[c] = 0.0;
+        if (smooth) X(l + 1)[c] = 0.0;
+        continue;
+      }
+      int ci, cj, ck;
+      node_ijk(c, gc, ci, cj, ck);
+      const int fi = F.keep[0][ci], fj = F.keep[1][cj], fk = F.keep[2][ck];
+      double acc = 0.0;
+      for (int dj = -1; dj <= 1; ++dj) {
+        const int j = fj + dj;
+        if (j < 0 || j >= F.py) continue;
+        const double wy = axis_weight(F.cmap[1], F.wmap[1], j, cj);
+        if (wy == 0.0) continue;
+        for (int di = -1; di <= 1; ++di) {
+          const int i = fi + di;
+          if (i < 0 || i >= F.px) continue;
+          const double wx = axis_weight(F.cmap[0], F.wmap[0], i, ci);
+          if (wx == 0.0) continue;
+          for (int dk = -1; dk <= 1; ++dk) {
+            const int k = fk + dk;
+            if (k < 0 || k >= F.pz) continue;
+            const double wz = axis_weight(F.cmap[2], F.wmap[2], k, ck);
+            if (wz == 0.0) continue;
+            acc += wx * wy * wz * F.r[(j * F.px + i) * F.pz + k];
+          }
+        }
+      }
+      C.b[c] = acc;
+      if (smooth) first(l + 1, c, acc);
+    }
+  }
+  // x_l += P x_{l+1} on the free rows.
+  __device__ void prolong(int l) const {
+    const MgDevLevel &F = mg.L[l], &C = mg.L[l + 1];
+    const double *xc = X(l + 1);
+    double *x = X(l);
+    const Grid3 gf{F.px, F.py, F.pz};
+    for (int n = tid; n < F.n; n += stride) {
+      if (F.dir[n]) continue;
+      int i, j, k;
+      node_ijk(n, gf, i, j, k);
+      const int2 cx = F.cmap[0][i], cy = F.cmap[1][j], cz = F.cmap[2][k];
+      const double2 wx = F.wmap[0][i], wy = F.wmap[1][j], wz = F.wmap[2][k];
+      double acc = 0.0;
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        const double wb = b ? wy.y : wy.x;
+        if (wb == 0.0) continue;
+        const int cj = b ? cy.y : cy.x;
+#pragma unroll
+        for (int a = 0; a < 2; ++a) {
+          const double wa = a ? wx.y : wx.x;
+          if (wa == 0.0) continue;
+          const int ci = a ? cx.y : cx.x;
+#pragma unroll
+          for (int d = 0; d < 2; ++d) {
+            const double wd = d ? wz.y : wz.x;
+            if (wd == 0.0) continue;
+            const int ck = d ? cz.y : cz.x;
+            acc += wa * wb * wd * xc[(cj * C.px + ci) * C.pz + ck];
+          }
+        }
+      }
+      x[n] += acc;
+    }
+  }
+  // x = C^-1 b on the coarsest level, one warp per row; returns sum b.x of
+  // the rows this thread's warp finished (lane 0 only).
+  __device__ double dense(int l) const {
+    const MgDevLevel &L = mg.L[l];
+    const int lane = threadIdx.x & 31, warp = tid >> 5, warps = stride >> 5;
+    double *x = X(l);
+    double acc = 0.0;
+    for (int row = warp; row < L.n; row += warps) {
+      const double *m = mg.coarse_inv + (size_t)row * L.n;
+      double s = 0.0;
+      for (int c = lane; c < L.n; c += 32) s += m[c] * L.b[c];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (lane == 0) {
+        x[row] = s;
+        acc += L.b[row] * s;
+      }
+    }
+    return acc;
+  }
+
+  // z = M r.  On entry level 0's first sweep is in X(0) (levels > 1); on
+  // exit X(0) holds z, part_rz the block partials of r.z, and the grid has
+  // synchronised.
+  __device__ void vcycle(cg::grid_group &grid, double *part_rz) {
+    const int L = mg.levels;
+    double rz = 0.0;
+    if (L == 1) {
+      rz = dense(0);
+    } else {
+      for (int l = 0; l + 1 < L; ++l) {
+        for (int s = 1; s < mg.nu; ++s) {
+          sweep(l, false);
+          grid.sync();
+        }
+        residual(l);
+        grid.sync();
+        restrict_to(l);
+        grid.sync();
+      }
+      dense(L - 1);
+      grid.sync();
+      for (int l = L - 2; l >= 0; --l) {
+        prolong(l);
+        grid.sync();
+        for (int s = 0; s < mg.nu; ++s) {
+          const bool last = l == 0 && s + 1 == mg.nu;
+          const double v = sweep(l, last);
+          if (last) rz = v;
+          if (!last) grid.sync();
+        }
+      }
+    }
+    const double bs = block_sum<kRedBlock>(rz);
+    if (threadIdx.x == 0) part_rz[blockIdx.x] = bs;
+    grid.sync();
+  }
+};
+
+// CG scalars as in the Jacobi solve: [0] rz, [3] rr, [6] ||b||^2, [7]
+// converged, [8] iterations, [9] (rel_tol ||b||)^2.  z = M r for the
+// initial residual is computed here.
+__global__ void __launch_bounds__(kRedBlock) cg_mg_persistent(int nodes, Grid3 g, const double *st7,
+                                                              const uint8_t *dirichlet, double *x, double *r,
+                                                              double *p0, double *p1, double *q, double *part,
+                                                              double *sc, int max_iter,
+                                                              const __grid_constant__ MgDevice mg) {
+  cg::grid_group grid = cg::this_grid();
+  const int nblk = gridDim.x;
+  double *part_pq = part, *part_rz = part + nblk, *part_rr = part + 2 * nblk;
+  Solve S{mg, st7, g, (int)(blockIdx.x * blockDim.x + threadIdx.x), (int)(gridDim.x * blockDim.x), 0u};
+  const double tol2 = sc[9];
+  bool done = sc[7] != 0.0;
+  double rr = sc[3], rz = 0.0, beta = 0.0;
+  int it = 0;
+  if (!done) {
+    if (mg.levels > 1) {
+      for (int n = S.tid; n < nodes; n += S.stride) S.first(0, n, r[n]);
+      grid.sync();
+    }
+    S.vcycle(grid, part_rz);
+    rz = sum_partials(part_rz, nblk);
+  }
+  const double *pin = p0;
+  double *pout = p1;
+  while (!done && it < max_iter) {
+    const double *z = S.X(0);
+    double v = 0.0;
+    for (int n = S.tid; n < nodes; n += S.stride) {
+      if (dirichlet[n]) {
+        q[n] = 0.0;
+        pout[n] = 0.0;
+        continue;
+      }
+      int i, j, k;
+      node_ijk(n, g, i, j, k);
+      const double *a = st7 + (size_t)n * 7;
+      const double pn = it == 0 ? z[n] : z[n] + beta * pin[n];
+      pout[n] = pn;
+      double acc = a[6] * pn;
+      const int nb[6] = {i > 0 ? n - g.pz : -1, i + 1 < g.px ? n + g.pz : -1, j > 0 ? n - g.px * g.pz : -1,
+                         j + 1 < g.py ? n + g.px * g.pz : -1, k > 0 ? n - 1 : -1, k + 1 < g.pz ? n + 1 : -1};
+#pragma unroll
+      for (int s = 0; s < 6; ++s) {
+        const int m = nb[s];
+        if (m < 0 || a[s] == 0.0 || dirichlet[m]) continue;
+        acc += a[s] * (it == 0 ? z[m] : z[m] + beta * pin[m]);
+      }
+      q[n] = acc;
+      v += pn * acc;
+    }
+    const double bs = block_sum<kRedBlock>(v);
+    if (threadIdx.x == 0) part_pq[blockIdx.x] = bs;
+    grid.sync();
+    const double alpha = rz / sum_partials(part_pq, nblk);
+    double a2 = 0.0;
+    for (int n = S.tid; n < nodes; n += S.stride) {
+      if (dirichlet[n]) {
+        if (mg.levels > 1) S.X(0)[n] = 0.0;
+        continue;
+      }
+      x[n] += alpha * pout[n];
+      const double rn = r[n] - alpha * q[n];
+      r[n] = rn;
+      a2 += rn * rn;
+      if (mg.levels > 1) S.first(0, n, rn);
+    }
+    const double b2 = block_sum<kRedBlock>(a2);
+    if (threadIdx.x == 0) part_rr[blockIdx.x] = b2;
+    grid.sync();
+    rr = sum_partials(part_rr, nblk);
+    ++it;
+    done = rr <= tol2;
+    if (done) break;
+    S.vcycle(grid, part_rz);
+    const double rz_new = sum_partials(part_rz, nblk);
+    beta = rz_new / rz;
+    rz = rz_new;
+    const double *t = pout;
+    pout = const_cast<double *>(pin);
+    pin = t;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    sc[0] = rz;
+    sc[3] = rr;
+    sc[8] = it;
+  }
+}
+
+template <typename T>
+T *upload(const std::vector<T> &v, std::vector<void *> &owned) {
+  if (v.empty()) return nullptr;
+  void *p = nullptr;
+  if (cudaMalloc(&p, v.size() * sizeof(T)) != cudaSuccess) throw std::runtime_error("multigrid: cudaMalloc failed");
+  owned.push_back(p);
+  if (cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+    throw std::runtime_error("multigrid: upload failed");
+  return static_cast<T *>(p);
+}
+double *scratch(size_t n, std::vector<void *> &owned) {
+  void *p = nullptr;
+  if (cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(double)) != cudaSuccess)
+    throw std::runtime_error("multigrid: cudaMalloc failed");
+  owned.push_back(p);
+  cudaMemset(p, 0, std::max<size_t>(n, 1) * sizeof(double));
+  return static_cast<double *>(p);
+}
+
+}  // namespace
+
+MgDevice mg_upload(const MgHierarchy &h, std::vector<void *> &owned) {
+  MgDevice d;
+  d.levels = (int)h.levels.size();
+  if (d.levels < 1 || d.levels > kMgMaxLevels) throw std::runtime_error("multigrid: bad level count");
+  for (int l = 0; l < d.levels; ++l) {
+    const MgLevel &s = h.levels[l];
+    MgDevLevel &L = d.L[l];
+    L.px = s.px;
+    L.py = s.py;
+    L.pz = s.pz;
+    L.n = s.nodes();
+    L.omega = s.omega;
+    L.st = upload(s.st, owned);
+    L.dinv = upload(s.dinv, owned);
+    L.dir = upload(s.dir, owned);
+    if (l > 0) {
+      L.b = scratch(L.n, owned);
+      L.xa = scratch(L.n, owned);
+    }
+    L.xb = scratch(L.n, owned);
+    L.r = scratch(L.n, owned);
+    if (l + 1 < d.levels) {
+      const MgAxis *ax[3] = {&s.ax, &s.ay, &s.az};
+      const std::vector<int> *kp[3] = {&s.kx, &s.ky, &s.kz};
+      for (int a = 0; a < 3; ++a) {
+        const size_t m = ax[a]->c0.size();
+        std::vector<int2> cm(m);
+        std::vector<double2> wm(m);
+        for (size_t i = 0; i < m; ++i) {
+          cm[i] = make_int2(ax[a]->c0[i], ax[a]->c1[i]);
+          wm[i] = make_double2(ax[a]->w0[i], ax[a]->w1[i]);
+        }
+        L.cmap[a] = upload(cm, owned);
+        L.wmap[a] = upload(wm, owned);
+        L.keep[a] = upload(*kp[a], owned);
+      }
+    }
+  }
+  d.coarse_inv = upload(h.coarse_inv, owned);
+  return d;
+}
+
+int cg_mg_max_grid() {
+  int dev = 0, sms = 0, per_sm = 0, coop = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+  if (!coop || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_mg_persistent, kRedBlock, 0) != cudaSuccess)
+    return 0;
+  return per_sm * sms;
+}
+
+cudaError_t launch_cg_mg(int nodes, const Grid3 &g, const double *st7, const uint8_t *dirichlet, double *x, double *r,
+                         double *z, double *p0, double *p1, double *q, double *part, double *sc, int max_iter,
+                         const MgDevice &mg_in, int grid, cudaStream_t s) {
+  MgDevice mg = mg_in;
+  mg.L[0].b = r;
+  mg.L[0].xa = z;
+  int nodes_arg = nodes, max_arg = max_iter;
+  Grid3 g_arg = g;
+  void *args[] = {&nodes_arg, &g_arg, &st7, &dirichlet, &x, &r, &p0, &p1, &q, &part, &sc, &max_arg, &mg};
+  return cudaLaunchCooperativeKernel((const void *)cg_mg_persistent, grid, kRedBlock, args, 0, s);
+}
+
+}  // namespace mcb200

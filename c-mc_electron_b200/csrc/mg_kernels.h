@@ -1,0 +1,51 @@
+// mg_kernels.h -- the multigrid-preconditioned CG Poisson solve on the GPU
+// (mg_kernels.cu): device copy of an MgHierarchy and its launcher.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "mg_setup.h"
+
+namespace mcb200 {
+
+struct MgDevLevel {
+  int px = 0, py = 0, pz = 0, n = 0;
+  double omega = 0.0;
+  const double *st = nullptr;    // [n][27] Galerkin stencil (levels >= 1)
+  const double *dinv = nullptr;  // [n] 1 / diagonal, 0 on Dirichlet rows
+  const uint8_t *dir = nullptr;  // [n] decoupled rows
+  double *b = nullptr, *xa = nullptr, *xb = nullptr, *r = nullptr;  // right side, iterate (ping-pong), residual
+  // interpolation from the next coarser level into this one, per axis:
+  // (c0, c1) coarse indices and (w0, w1) weights of each fine index, and the
+  // fine index of each coarse node
+  const int2 *cmap[3] = {nullptr, nullptr, nullptr};
+  const double2 *wmap[3] = {nullptr, nullptr, nullptr};
+  const int *keep[3] = {nullptr, nullptr, nullptr};
+};
+
+struct MgDevice {
+  int levels = 0;
+  int nu = 1;                          // smoothing sweeps before and after the coarse correction
+  const double *coarse_inv = nullptr;  // [n][n] dense inverse of the coarsest operator
+  MgDevLevel L[kMgMaxLevels];
+};
+
+// Copies the hierarchy to the device.  Level 0's b and xa are left null: the
+// solve binds them to the CG residual and preconditioned residual.  Every
+// allocation is appended to `owned` (freed by the caller with cudaFree).
+MgDevice mg_upload(const MgHierarchy &h, std::vector<void *> &owned);
+
+// The CG iterations of one solve with the V-cycle as preconditioner, in one
+// cooperative launch of `grid` blocks; the CG vectors and scalars are those
+// of the Jacobi solve (field_kernels.cu).  Returns the cudaError_t of the
+// launch.
+struct Grid3;
+cudaError_t launch_cg_mg(int nodes, const Grid3 &g, const double *st7, const uint8_t *dirichlet, double *x, double *r,
+                         double *z, double *p0, double *p1, double *q, double *part, double *sc, int max_iter,
+                         const MgDevice &mg, int grid, cudaStream_t s);
+// Largest cooperative grid of the MG kernel on the current device (blocks per SM x SMs); 0 if unavailable.
+int cg_mg_max_grid();
+
+}  // namespace mcb200

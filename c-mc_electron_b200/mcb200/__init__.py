@@ -30,6 +30,10 @@ FLAG_SURFACE_IMPURITY = 2
 FLAG_HEAT = 4
 FLIGHT_FP64 = 0
 FLIGHT_FP32 = 1
+# Poisson preconditioners (mcb200_set_poisson_solver)
+POISSON_AUTO = 0
+POISSON_JACOBI = 1
+POISSON_MULTIGRID = 2
 UNIT_NAMES = ["T0", "eV0", "spr0", "time0", "conc0", "field0", "scrt0", "pot0", "a0pi", "sieg",
               "eps_silicon", "eps_oxide", "curr0", "dens0"]
 
@@ -112,6 +116,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mcb200_set_device.argtypes = [vp, i32p, dp, dp, c.c_int, dp, dp, c.c_int, i32p]
     lib.mcb200_deposit.argtypes = [vp]
     lib.mcb200_solve_poisson.argtypes = [vp, c.c_double, c.c_int, c.POINTER(c.c_int), dp]
+    lib.mcb200_set_poisson_solver.argtypes = [vp, c.c_int, c.c_int]
+    lib.mcb200_get_poisson_solver.argtypes = [vp, c.POINTER(c.c_int), c.POINTER(c.c_int), c.POINTER(c.c_int)]
     lib.mcb200_get_array.argtypes = [vp, c.c_char_p, dp, c.c_size_t]
     lib.mcb200_surface_rates.argtypes = [vp, c.POINTER(SurfaceParams), i32p]
     lib.mcb200_multiple_refresh.argtypes = [vp, i32p, i32p, c.c_uint32, c.c_uint64, c.POINTER(c.c_int64)]
@@ -289,6 +295,24 @@ class Engine:
         self._check(self._lib.mcb200_solve_poisson(self._ctx, rel_tol, max_iter, ctypes.byref(it),
                                                    ctypes.byref(res)), "solve_poisson")
         return it.value, res.value
+
+    def set_potential(self, potential):
+        """Node potential (normalised) and the cell fields derived from it."""
+        pot = np.ascontiguousarray(potential, dtype=np.float64)
+        assert pot.size == self.mesh.nnodes
+        self._check(self._lib.mcb200_set_potential(self._ctx, _ptr(pot, ctypes.c_double)), "set_potential")
+
+    def set_poisson_solver(self, method=POISSON_AUTO, blocks=0):
+        """Preconditioner of the following solves (POISSON_AUTO / _JACOBI /
+        _MULTIGRID) and their cooperative grid (0: the largest co-resident)."""
+        self._check(self._lib.mcb200_set_poisson_solver(self._ctx, method, blocks), "set_poisson_solver")
+
+    def poisson_solver(self):
+        """(preconditioner of the last solve, its grid, multigrid levels)."""
+        m, b, l = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(self._lib.mcb200_get_poisson_solver(self._ctx, ctypes.byref(m), ctypes.byref(b), ctypes.byref(l)),
+                    "poisson_solver")
+        return m.value, b.value, l.value
 
     def array(self, name: str) -> np.ndarray:
         m = self.mesh

@@ -140,10 +140,23 @@ int mcb200_set_device(mcb200_ctx *ctx, const int32_t *material, const double *do
 int mcb200_deposit(mcb200_ctx *ctx);
 
 /* Poisson solve from the last deposit (compute_rhs + linear_poisson_solver,
- * src/mcmodel.cpp:2714-2893): Jacobi-preconditioned CG in FP64, warm-started
- * from the previous potential, to ||b - Ax|| / ||b|| <= rel_tol; then the
- * cell fields of both carriers (pot2field, :2732-2855). */
+ * src/mcmodel.cpp:2714-2893; the reference factorises with KLU): CG in FP64
+ * on the system with the contact rows eliminated, warm-started from the
+ * previous potential, to ||b - Ax|| / ||b|| <= rel_tol; then the cell fields
+ * of both carriers (pot2field, :2732-2855).  The preconditioner is one
+ * geometric-multigrid V-cycle (the default) or Jacobi, selected with
+ * mcb200_set_poisson_solver. */
 int mcb200_solve_poisson(mcb200_ctx *ctx, double rel_tol, int max_iter, int *iterations, double *rel_residual);
+
+#define MCB200_POISSON_AUTO 0      /* multigrid when the mesh has a hierarchy, else Jacobi */
+#define MCB200_POISSON_JACOBI 1    /* Jacobi-preconditioned CG */
+#define MCB200_POISSON_MULTIGRID 2 /* V-cycle-preconditioned CG */
+/* Preconditioner and cooperative grid (blocks; 0 = the largest co-resident
+ * grid) of the following solves.  No counterpart in the reference. */
+int mcb200_set_poisson_solver(mcb200_ctx *ctx, int method, int blocks);
+/* Preconditioner (MCB200_POISSON_JACOBI / _MULTIGRID) and grid of the last
+ * solve, and the multigrid level count of the device (0: none). */
+int mcb200_get_poisson_solver(mcb200_ctx *ctx, int *method_used, int *blocks, int *levels);
 
 /* Surface scattering parameters (the SurfSc_* members set in
  * init_phpysical_parameter, src/mcmodel.cpp:4107-4121): delta and ail are the
