@@ -406,7 +406,11 @@ int cg_solve(const DevMesh &M, const FieldBuffers &f, double rel_tol, int max_it
     }
     if (most < 1) return 1;
     most = std::min(most, kCgMaxGrid);
-    plan.grid = plan.blocks > 0 ? std::min(plan.blocks, most) : most;
+    // the V-cycle's short phases are barrier-bound: two blocks per SM
+    // measured fastest on the FinFET mesh (fewer blocks arrive at each
+    // barrier; more would idle on its coarse levels)
+    const int fallback = use_mg ? std::min(most, 2 * sms) : most;
+    plan.grid = plan.blocks > 0 ? std::min(plan.blocks, most) : fallback;
     plan.used = use_mg ? kCgMultigrid : kCgJacobi;
   }
   double *x = f.potential, *r = f.cg_r, *z = f.cg_z, *p0 = f.cg_p, *p1 = f.cg_p1, *q = f.cg_q, *part = f.cg_part;

@@ -28,14 +28,24 @@ namespace cg = cooperative_groups;
 
 namespace {
 
-__device__ __forceinline__ double axis_weight(const int2 *cm, const double2 *wm, int i, int c) {
-  const int2 cc = cm[i];
-  const double2 w = wm[i];
-  double v = 0.0;
-  if (cc.x == c) v += w.x;
-  if (cc.y == c && cc.y != cc.x) v += w.y;
-  return v;
+#ifdef MCB200_MG_TRACE
+// Opt-in phase trace (build with -DMCB200_MG_TRACE): block 0 records
+// (phase id, %globaltimer) after every barrier of the first solve.
+constexpr int kTraceMax = 8192;
+__device__ unsigned long long g_trace[2 * kTraceMax];
+__device__ int g_trace_n;
+__device__ __forceinline__ void trace(int id) {
+  if (blockIdx.x == 0 && threadIdx.x == 0 && g_trace_n < kTraceMax) {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    g_trace[2 * g_trace_n] = id;
+    g_trace[2 * g_trace_n + 1] = t;
+    ++g_trace_n;
+  }
 }
+#else
+__device__ __forceinline__ void trace(int) {}
+#endif
 
 // (A x)[n] with the 7-point stencil of the CG (-x, +x, -y, +y, -z, +z,
 // diagonal).  x is zero on Dirichlet nodes and isolated nodes have no
@@ -103,11 +113,11 @@ struct Solve {
     double *xn = Xo(l);
     double acc = 0.0;
     for (int n = tid; n < L.n; n += stride) {
-      double v;
-      if (L.dir[n]) v = l == 0 ? L.dinv[n] * b[n] : 0.0;
-      else v = xc[n] + L.omega * L.dinv[n] * (b[n] - A(l, xc, n));
+      const double bn = b[n], dn = L.dinv[n], ax = A(l, xc, n), xn0 = xc[n];
+      double v = xn0 + L.omega * dn * (bn - ax);
+      if (L.dir[n]) v = l == 0 ? dn * bn : 0.0;
       xn[n] = v;
-      if (dot) acc += b[n] * v;
+      if (dot) acc += bn * v;
     }
     cur ^= 1u << l;
     return acc;
@@ -115,42 +125,45 @@ struct Solve {
   __device__ void residual(int l) const {
     const MgDevLevel &L = mg.L[l];
     const double *x = X(l);
-    for (int n = tid; n < L.n; n += stride) L.r[n] = L.dir[n] ? 0.0 : L.b[n] - A(l, x, n);
+    for (int n = tid; n < L.n; n += stride) {
+      const double v = L.b[n] - A(l, x, n);
+      L.r[n] = L.dir[n] ? 0.0 : v;
+    }
   }
-  // b_{l+1} = P^T r_l, and the first sweep of level l+1 unless it is the coarsest.
+  // b_{l+1} = P^T r_l, and the first sweep of level l+1 unless it is the
+  // coarsest.  The 27 taps of a coarse node are the products of its three
+  // per-axis tap triples; off-grid taps have weight 0 and a clamped index,
+  // so every load is independent of the others.
   __device__ void restrict_to(int l) const {
     const MgDevLevel &F = mg.L[l], &C = mg.L[l + 1];
     const bool smooth = l + 2 < mg.levels;
     const Grid3 gc{C.px, C.py, C.pz};
     for (int c = tid; c < C.n; c += stride) {
-      if (C.dir[c]) {
-        C.b[c] = 0.0;
-        if (smooth) X(l + 1)[c] = 0.0;
-        continue;
-      }
       int ci, cj, ck;
       node_ijk(c, gc, ci, cj, ck);
       const int fi = F.keep[0][ci], fj = F.keep[1][cj], fk = F.keep[2][ck];
-      double acc = 0.0;
-      for (int dj = -1; dj <= 1; ++dj) {
-        const int j = fj + dj;
-        if (j < 0 || j >= F.py) continue;
-        const double wy = axis_weight(F.cmap[1], F.wmap[1], j, cj);
-        if (wy == 0.0) continue;
-        for (int di = -1; di <= 1; ++di) {
-          const int i = fi + di;
-          if (i < 0 || i >= F.px) continue;
-          const double wx = axis_weight(F.cmap[0], F.wmap[0], i, ci);
-          if (wx == 0.0) continue;
-          for (int dk = -1; dk <= 1; ++dk) {
-            const int k = fk + dk;
-            if (k < 0 || k >= F.pz) continue;
-            const double wz = axis_weight(F.cmap[2], F.wmap[2], k, ck);
-            if (wz == 0.0) continue;
-            acc += wx * wy * wz * F.r[(j * F.px + i) * F.pz + k];
-          }
-        }
+      double wx[3], wy[3], wz[3];
+      int ix[3], jy[3], kz[3];
+#pragma unroll
+      for (int t = 0; t < 3; ++t) {
+        wx[t] = F.rtap[0][3 * ci + t];
+        wy[t] = F.rtap[1][3 * cj + t];
+        wz[t] = F.rtap[2][3 * ck + t];
+        ix[t] = min(max(fi - 1 + t, 0), F.px - 1);
+        jy[t] = min(max(fj - 1 + t, 0), F.py - 1);
+        kz[t] = min(max(fk - 1 + t, 0), F.pz - 1);
       }
+      double acc = 0.0;
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const double wab = wx[a] * wy[b];
+          const double *row = F.r + (jy[b] * F.px + ix[a]) * F.pz;
+#pragma unroll
+          for (int d = 0; d < 3; ++d) acc += wab * wz[d] * row[kz[d]];
+        }
+      if (C.dir[c]) acc = 0.0;
       C.b[c] = acc;
       if (smooth) first(l + 1, c, acc);
     }
@@ -224,28 +237,37 @@ struct Solve {
         for (int s = 1; s < mg.nu; ++s) {
           sweep(l, false);
           grid.sync();
+          trace(10 * l + 1);
         }
         residual(l);
         grid.sync();
+        trace(10 * l + 2);
         restrict_to(l);
         grid.sync();
+        trace(10 * l + 3);
       }
       dense(L - 1);
       grid.sync();
+      trace(10 * (L - 1) + 4);
       for (int l = L - 2; l >= 0; --l) {
         prolong(l);
         grid.sync();
+        trace(10 * l + 5);
         for (int s = 0; s < mg.nu; ++s) {
           const bool last = l == 0 && s + 1 == mg.nu;
           const double v = sweep(l, last);
           if (last) rz = v;
-          if (!last) grid.sync();
+          if (!last) {
+            grid.sync();
+            trace(10 * l + 6);
+          }
         }
       }
     }
     const double bs = block_sum<kRedBlock>(rz);
     if (threadIdx.x == 0) part_rz[blockIdx.x] = bs;
     grid.sync();
+    trace(7);
   }
 };
 
@@ -265,6 +287,7 @@ __global__ void __launch_bounds__(kRedBlock) cg_mg_persistent(int nodes, Grid3 g
   bool done = sc[7] != 0.0;
   double rr = sc[3], rz = 0.0, beta = 0.0;
   int it = 0;
+  trace(0);
   if (!done) {
     if (mg.levels > 1) {
       for (int n = S.tid; n < nodes; n += S.stride) S.first(0, n, r[n]);
@@ -284,26 +307,28 @@ __global__ void __launch_bounds__(kRedBlock) cg_mg_persistent(int nodes, Grid3 g
         pout[n] = 0.0;
         continue;
       }
+      // z and p vanish on Dirichlet nodes, so neighbours need no mask
       int i, j, k;
       node_ijk(n, g, i, j, k);
       const double *a = st7 + (size_t)n * 7;
-      const double pn = it == 0 ? z[n] : z[n] + beta * pin[n];
+      // (pin is not read in the first iteration: it holds no p yet)
+      auto P = [&](int m) { return it == 0 ? z[m] : z[m] + beta * pin[m]; };
+      const double pn = P(n);
       pout[n] = pn;
       double acc = a[6] * pn;
-      const int nb[6] = {i > 0 ? n - g.pz : -1, i + 1 < g.px ? n + g.pz : -1, j > 0 ? n - g.px * g.pz : -1,
-                         j + 1 < g.py ? n + g.px * g.pz : -1, k > 0 ? n - 1 : -1, k + 1 < g.pz ? n + 1 : -1};
-#pragma unroll
-      for (int s = 0; s < 6; ++s) {
-        const int m = nb[s];
-        if (m < 0 || a[s] == 0.0 || dirichlet[m]) continue;
-        acc += a[s] * (it == 0 ? z[m] : z[m] + beta * pin[m]);
-      }
+      if (i > 0) acc += a[0] * P(n - g.pz);
+      if (i + 1 < g.px) acc += a[1] * P(n + g.pz);
+      if (j > 0) acc += a[2] * P(n - g.px * g.pz);
+      if (j + 1 < g.py) acc += a[3] * P(n + g.px * g.pz);
+      if (k > 0) acc += a[4] * P(n - 1);
+      if (k + 1 < g.pz) acc += a[5] * P(n + 1);
       q[n] = acc;
       v += pn * acc;
     }
     const double bs = block_sum<kRedBlock>(v);
     if (threadIdx.x == 0) part_pq[blockIdx.x] = bs;
     grid.sync();
+    trace(100);
     const double alpha = rz / sum_partials(part_pq, nblk);
     double a2 = 0.0;
     for (int n = S.tid; n < nodes; n += S.stride) {
@@ -320,6 +345,7 @@ __global__ void __launch_bounds__(kRedBlock) cg_mg_persistent(int nodes, Grid3 g
     const double b2 = block_sum<kRedBlock>(a2);
     if (threadIdx.x == 0) part_rr[blockIdx.x] = b2;
     grid.sync();
+    trace(101);
     rr = sum_partials(part_rr, nblk);
     ++it;
     done = rr <= tol2;
@@ -395,12 +421,25 @@ MgDevice mg_upload(const MgHierarchy &h, std::vector<void *> &owned) {
         L.cmap[a] = upload(cm, owned);
         L.wmap[a] = upload(wm, owned);
         L.keep[a] = upload(*kp[a], owned);
+        L.rtap[a] = upload(a == 0 ? s.rx : a == 1 ? s.ry : s.rz, owned);
       }
     }
   }
   d.coarse_inv = upload(h.coarse_inv, owned);
   return d;
 }
+
+#ifdef MCB200_MG_TRACE
+extern "C" int mcb200_mg_trace_read(unsigned long long *out, int max_entries) {
+  int n = 0;
+  cudaMemcpyFromSymbol(&n, g_trace_n, sizeof(int));
+  n = std::min(n, max_entries);
+  cudaMemcpyFromSymbol(out, g_trace, 2 * n * sizeof(unsigned long long));
+  const int zero = 0;
+  cudaMemcpyToSymbol(g_trace_n, &zero, sizeof(int));
+  return n;
+}
+#endif
 
 int cg_mg_max_grid() {
   int dev = 0, sms = 0, per_sm = 0, coop = 0;

@@ -23,6 +23,7 @@ struct MgDevLevel {
   const int2 *cmap[3] = {nullptr, nullptr, nullptr};
   const double2 *wmap[3] = {nullptr, nullptr, nullptr};
   const int *keep[3] = {nullptr, nullptr, nullptr};
+  const double *rtap[3] = {nullptr, nullptr, nullptr};  // [3 * coarse] restriction taps (mg_setup.h)
 };
 
 struct MgDevice {

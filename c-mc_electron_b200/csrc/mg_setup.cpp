@@ -46,6 +46,25 @@ MgAxis make_axis(const std::vector<double> &x, const std::vector<int> &keep) {
   return a;
 }
 
+// Weight of coarse node c in the interpolation of fine index i.
+double tap(const MgAxis &a, int i, int c) {
+  double v = 0.0;
+  if (a.c0[i] == c) v += a.w0[i];
+  if (a.c1[i] == c && a.c1[i] != a.c0[i]) v += a.w1[i];
+  return v;
+}
+
+std::vector<double> restriction_taps(const MgAxis &a, const std::vector<int> &keep) {
+  const int n = (int)a.c0.size();
+  std::vector<double> r(3 * keep.size(), 0.0);
+  for (size_t c = 0; c < keep.size(); ++c)
+    for (int t = 0; t < 3; ++t) {
+      const int i = keep[c] - 1 + t;
+      if (i >= 0 && i < n) r[3 * c + t] = tap(a, i, (int)c);
+    }
+  return r;
+}
+
 double min_spacing(const std::vector<double> &x) {
   double h = 1e300;
   for (size_t i = 0; i + 1 < x.size(); ++i) h = std::min(h, x[i + 1] - x[i]);
@@ -222,6 +241,9 @@ MgHierarchy MgHierarchy::build(int px, int py, int pz, const std::vector<double>
     f.ax = make_axis(f.x, kx);
     f.ay = make_axis(f.y, ky);
     f.az = make_axis(f.z, kz);
+    f.rx = restriction_taps(f.ax, kx);
+    f.ry = restriction_taps(f.ay, ky);
+    f.rz = restriction_taps(f.az, kz);
     // a coarse node on a decoupled fine node is decoupled too: interpolation
     // then falls to zero at Dirichlet walls instead of reaching across them
     c.dir.assign(c.nodes(), 0);

@@ -36,6 +36,9 @@ struct MgLevel {
   std::vector<double> x, y, z;     // node coordinates
   MgAxis ax, ay, az;               // interpolation from level + 1 into this level (empty on the coarsest)
   std::vector<int> kx, ky, kz;     // fine index of each node of level + 1, per axis (empty on the coarsest)
+  // restriction taps per axis: for node c of level + 1, the weights of the
+  // fine indices kx[c] - 1, kx[c], kx[c] + 1 (0 off the grid) -- [3 * coarse]
+  std::vector<double> rx, ry, rz;
   int nodes() const { return px * py * pz; }
   int idx(int i, int j, int k) const { return (j * px + i) * pz + k; }
 };

@@ -151,8 +151,9 @@ int mcb200_solve_poisson(mcb200_ctx *ctx, double rel_tol, int max_iter, int *ite
 #define MCB200_POISSON_AUTO 0      /* multigrid when the mesh has a hierarchy, else Jacobi */
 #define MCB200_POISSON_JACOBI 1    /* Jacobi-preconditioned CG */
 #define MCB200_POISSON_MULTIGRID 2 /* V-cycle-preconditioned CG */
-/* Preconditioner and cooperative grid (blocks; 0 = the largest co-resident
- * grid) of the following solves.  No counterpart in the reference. */
+/* Preconditioner and cooperative grid (blocks; 0 = automatic: Jacobi the
+ * largest co-resident grid, multigrid two blocks per SM) of the following
+ * solves.  No counterpart in the reference. */
 int mcb200_set_poisson_solver(mcb200_ctx *ctx, int method, int blocks);
 /* Preconditioner (MCB200_POISSON_JACOBI / _MULTIGRID) and grid of the last
  * solve, and the multigrid level count of the device (0: none). */
