@@ -182,21 +182,26 @@ def measure_precision(args, rank: int, world: int, device: int, precision: str):
 
 
 FINFET_POISSON_EVERY = 10
+PHASE_PROFILE_STEPS = 60  # steps of the phase-split run (each phase waited for)
 FLUSH_BYTES = 256 << 20  # > 126 MB L2
 
 
-def finfet_run(args, device: int, precision: str, readback: bool = False) -> dict:
+def finfet_run(args, device: int, precision: str, readback: bool = False, profile_steps: int = 0) -> dict:
+    """One run of the FinFET deck.  profile_steps > 0: a short run that waits
+    for the GPU after every phase, for the per-phase device time split only."""
     import mcb200
     from mcb200 import decks
 
+    steps = profile_steps if profile_steps else args.steps
     with tempfile.TemporaryDirectory() as tmp:
-        d = decks.finfet(tmp, total_step=args.warmup + args.steps + 1, heat_steps=0, stat_step=100000)
+        d = decks.finfet(tmp, total_step=args.warmup + steps + 1, heat_steps=0, stat_step=100000)
         prec = mcb200.FLIGHT_FP32 if precision == "fp32" else mcb200.FLIGHT_FP64
         with ClockSampler(device) as clocks:
-            rep = mcb200.run_deck(d["input"], device=device, precision=prec, max_steps=args.warmup + args.steps,
+            rep = mcb200.run_deck(d["input"], device=device, precision=prec, max_steps=args.warmup + steps,
                                   warmup_steps=args.warmup, max_heat_steps=0, poisson_every=FINFET_POISSON_EVERY,
                                   write_outputs=False, readback_every_step=readback,
-                                  flush_l2_bytes=0 if readback else FLUSH_BYTES)
+                                  flush_l2_bytes=0 if (readback or profile_steps) else FLUSH_BYTES,
+                                  profile_phases=bool(profile_steps))
         rep["clocks"] = clocks.summary()
     return rep
 
@@ -204,6 +209,7 @@ def finfet_run(args, device: int, precision: str, readback: bool = False) -> dic
 def engine_arm(args, rank: int, world: int, device: int):
     runs = {p: finfet_run(args, device, p) for p in ("fp64", "fp32")}
     e2e = finfet_run(args, device, "fp32", readback=True) if args.workload == "all" else runs["fp32"]
+    phases = finfet_run(args, device, "fp32", profile_steps=PHASE_PROFILE_STEPS)
     peak, peak_kind = measured_peaks()
     value = {}
     for p, r in runs.items():
@@ -263,7 +269,7 @@ def engine_arm(args, rank: int, world: int, device: int):
                        "clocks": r64["clocks"]},
         "fp32_over_fp64": value["fp32"] / value["fp64"],
         "poisson": cg,
-        "phase_s_fp32": r32["phase_s"], "phase_s_fp64": r64["phase_s"],
+        "phase_s_fp32": phases["phase_s"], "phase_profile_steps": PHASE_PROFILE_STEPS + args.warmup,
         "bulk": bulk,
         "bulk_fp32_over_fp64": bulk["fp32"]["value"] / bulk["fp64"]["value"] if bulk else None,
     }

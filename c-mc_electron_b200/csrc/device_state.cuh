@@ -199,6 +199,38 @@ struct DevChildrenT {
 };
 using DevChildren = DevChildrenT<double>;
 
+// A particle count that lives in device memory: *a (+ *b), at most `max`
+// (with neither pointer: `max` itself, a count the host knows).  Per-step
+// kernels read their sizes through it, so the host never waits for a count
+// between launches.
+struct DevCount {
+  const unsigned int *a = nullptr, *b = nullptr;
+  int max = 0;
+  __device__ __forceinline__ int get() const {
+    if (!a && !b) return max;
+    const unsigned long long v = (unsigned long long)(a ? *a : 0u) + (b ? *b : 0u);
+    return (int)(v < (unsigned long long)max ? v : (unsigned long long)max);
+  }
+};
+
+// The child generations of one step (one buffer per generation).
+constexpr int kChildGenerations = 4;
+template <typename R>
+struct ChildSetT {
+  DevChildrenT<R> g[kChildGenerations];
+  // offset of generation `gen` in the concatenation and the total count
+  __device__ __forceinline__ int offset(int gen, int *total) const {
+    int off = 0, at = 0;
+#pragma unroll
+    for (int q = 0; q < kChildGenerations; ++q) {
+      if (q == gen) at = off;
+      off += min((int)*g[q].count, g[q].capacity);
+    }
+    if (total) *total = off;
+    return at;
+  }
+};
+
 inline __host__ __device__ uint32_t pack_cell(int i, int j, int k) {
   return (uint32_t)i | ((uint32_t)j << 10) | ((uint32_t)k << 20);
 }

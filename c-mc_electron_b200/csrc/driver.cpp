@@ -110,8 +110,10 @@ struct Run {
 
   using clock = std::chrono::steady_clock;
   clock::time_point mark = clock::now();
-  // wall time since the last lap into report->phase_s[phase]
+  // wall time since the last lap into report->phase_s[phase] (after the
+  // GPU has finished the phase when profiling phases)
   void lap(int phase) {
+    if (opt.profile_phases) ok(mcb200_sync(ctx), ctx, "mcb200_sync");
     const clock::time_point now = clock::now();
     rep->phase_s[phase] += std::chrono::duration<double>(now - mark).count();
     mark = now;
@@ -124,20 +126,13 @@ struct Run {
     lap(0);
     ok(mcb200_deposit(ctx), ctx, "mcb200_deposit");
     lap(1);
-    if (!heat && info.flag_compute_potential && step % poisson_every == 0) {
-      int it = 0;
-      double res = 0;
-      ok(mcb200_solve_poisson(ctx, opt.poisson_rel_tol > 0 ? opt.poisson_rel_tol : 1e-10, 20000, &it, &res), ctx,
-         "mcb200_solve_poisson");
-      rep->poisson_solves += 1;
-      rep->poisson_iterations += it;
-      rep->poisson_max_residual = std::max(rep->poisson_max_residual, res);
-    }
+    if (!heat && info.flag_compute_potential && step % poisson_every == 0)  // statistics stay on the device
+      ok(mcb200_solve_poisson(ctx, opt.poisson_rel_tol > 0 ? opt.poisson_rel_tol : 1e-10, 20000, nullptr, nullptr),
+         ctx, "mcb200_solve_poisson");
     lap(2);
     if (info.flag_surface_scatter) ok(mcb200_surface_rates(ctx, &surf, eeff.data()), ctx, "mcb200_surface_rates");
     lap(3);
     ok(mcb200_step(ctx, (uint32_t)(heat ? 0x80000000u + step : step), seed, info.dt), ctx, "mcb200_step");
-    rep->particle_steps += mcb200_num_particles(ctx);
     lap(4);
   }
 
@@ -348,7 +343,10 @@ struct Run {
       int it = 0;
       double res = 0;
       ok(mcb200_solve_poisson(ctx, 1e-10, 20000, &it, &res), ctx, "mcb200_solve_poisson");
+      ok(mcb200_poisson_stats(ctx, nullptr, nullptr, nullptr, 1), ctx, "mcb200_poisson_stats");  // the run's solves only
     }
+    uint64_t ps_start = 0;
+    ok(mcb200_particle_steps(ctx, &ps_start), ctx, "mcb200_particle_steps");
     ok(mcb200_set_timing(ctx, 1), ctx, "mcb200_set_timing");
     const int steps = opt.max_steps > 0 ? std::min(opt.max_steps, info.total_step) : info.total_step;
     const int warm = std::max(0, std::min(opt.warmup_steps, steps));
@@ -365,7 +363,7 @@ struct Run {
         ok(mcb200_set_timing(ctx, 1), ctx, "mcb200_set_timing");
         ok(mcb200_mark(ctx, 0), ctx, "mcb200_mark");
         timed_t0 = std::chrono::steady_clock::now();
-        ps0 = rep->particle_steps;
+        ok(mcb200_particle_steps(ctx, &ps0), ctx, "mcb200_particle_steps");
       }
       const bool flush = opt.flush_l2_bytes > 0 && step >= warm;
       if (flush) {
@@ -391,7 +389,9 @@ struct Run {
       ok(mcb200_elapsed_ms(ctx, 0, 1, &rep->timed_device_ms), ctx, "mcb200_elapsed_ms");
       if (opt.flush_l2_bytes > 0) rep->timed_device_ms = flushed_ms;  // the evictions are not timed
       rep->timed_wall_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - timed_t0).count();
-      rep->timed_particle_steps = rep->particle_steps - ps0;
+      uint64_t ps1 = 0;
+      ok(mcb200_particle_steps(ctx, &ps1), ctx, "mcb200_particle_steps");
+      rep->timed_particle_steps = ps1 - ps0;
       rep->timed_steps = steps - warm;
       double tt[6];
       ok(mcb200_get_timing(ctx, tt, 6), ctx, "mcb200_get_timing");
@@ -419,6 +419,15 @@ struct Run {
     }
     ok(mcb200_sync(ctx), ctx, "mcb200_sync");
     rep->wall_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    uint64_t ps_end = 0;
+    ok(mcb200_particle_steps(ctx, &ps_end), ctx, "mcb200_particle_steps");
+    rep->particle_steps = ps_end - ps_start;
+    if (info.flag_compute_potential) {
+      int64_t solves = 0, its = 0;
+      ok(mcb200_poisson_stats(ctx, &solves, &its, &rep->poisson_max_residual, 0), ctx, "mcb200_poisson_stats");
+      rep->poisson_solves = (int)solves;
+      rep->poisson_iterations = its;
+    }
     double tim[6];
     ok(mcb200_get_timing(ctx, tim, 6), ctx, "mcb200_get_timing");
     rep->flight_ms = tim[0];

@@ -104,7 +104,7 @@ struct mcb200_ctx {
   size_t n = 0;
   uint32_t next_uid = 0;
   // mid-step copies: one buffer per generation
-  static constexpr int kGenerations = 4;
+  static constexpr int kGenerations = kChildGenerations;
   ChildBuffers cb[kGenerations];
   int child_cap = 0;
   uint64_t *child_keys = nullptr;
@@ -136,9 +136,21 @@ struct mcb200_ctx {
   int stat_steps = 0;
   bool stat_open = false;
   double vmax = 0;  // largest group-velocity component of the band tables
-  // CUDA-event timing on the context's stream (mcb200_timing)
+  // device-resident counts: the step path never waits for them; `n` and
+  // `next_uid` above are host copies, valid while !n_stale
+  unsigned int *dev_counts = nullptr;         // [0] particles, [1] next uid, [2] store-full flag
+  unsigned long long *dev_psteps = nullptr;   // particle-steps flown (particles at the start of each step)
+  unsigned int *sink_count = nullptr;         // copies of the last child generation: counted, not stored
+  bool n_stale = false;
+  bool overflow_pending = false;              // a store-full flag seen, not yet reported
+  // CUDA-event timing on the context's stream (mcb200_timing): a ring of
+  // per-step event quadruples, read back when a slot is reused or on demand
   bool timing = false;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  static constexpr int kTimingRing = 64;
+  cudaEvent_t ev[kTimingRing][4] = {};
+  bool ev_pending[kTimingRing] = {};
+  int ev_head = 0;
+  unsigned long long psteps_at_timing = 0;
   cudaEvent_t marks[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   void *flush_buf = nullptr;  // mcb200_flush_l2 scratch
   size_t flush_bytes = 0;
@@ -148,8 +160,9 @@ struct mcb200_ctx {
   ~mcb200_ctx() {
     if (device < 0) return;
     cudaSetDevice(device);
-    for (cudaEvent_t e : ev)
-      if (e) cudaEventDestroy(e);
+    for (auto &q : ev)
+      for (cudaEvent_t e : q)
+        if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : marks)
       if (e) cudaEventDestroy(e);
     for (void *p : mesh_owned) cudaFree(p);
@@ -170,6 +183,57 @@ namespace {
 int fail(mcb200_ctx *c, int code, const std::string &msg) {
   if (c) c->error = msg;
   return code;
+}
+
+__global__ void set_counts_kernel(unsigned int *d, unsigned int n, unsigned int next_uid) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    d[0] = n;
+    d[1] = next_uid;
+  }
+}
+
+// Host copies of the device counts, after the stream has drained (only when
+// a step may have changed them).  A store-full flag raised by a step is
+// reported here, once.
+void pull_counts(mcb200_ctx *c) {
+  if (c->n_stale) {
+    ck(cudaMemcpyAsync(c->h_pinned + 32, c->dev_counts, 3 * sizeof(unsigned int), cudaMemcpyDeviceToHost, c->stream),
+       "count");
+    ck(cudaStreamSynchronize(c->stream), "sync");
+    c->n = c->h_pinned[32];
+    c->next_uid = c->h_pinned[33];
+    c->n_stale = false;
+    if (c->h_pinned[34]) {
+      ck(cudaMemsetAsync(c->dev_counts + 2, 0, sizeof(unsigned int), c->stream), "memset");
+      c->overflow_pending = true;
+    }
+  }
+  if (c->overflow_pending) {
+    c->overflow_pending = false;
+    throw CapacityError("particle store full: GENERATE copies beyond the context capacity were dropped");
+  }
+}
+
+// The host's counts into device memory (after the host changed the store).
+void push_counts(mcb200_ctx *c) {
+  set_counts_kernel<<<1, 32, 0, c->stream>>>(c->dev_counts, (unsigned int)c->n, c->next_uid);
+  ck(cudaGetLastError(), "set counts");
+  c->n_stale = false;
+}
+
+// Reads back the timing of ring slot q (its events are complete or the call waits for them).
+void harvest_timing(mcb200_ctx *c, int q) {
+  if (!c->ev_pending[q]) return;
+  ck(cudaEventSynchronize(c->ev[q][3]), "cudaEventSynchronize");
+  float ms_flight = 0, ms_step = 0;
+  ck(cudaEventElapsedTime(&ms_flight, c->ev[q][1], c->ev[q][2]), "elapsed");
+  ck(cudaEventElapsedTime(&ms_step, c->ev[q][0], c->ev[q][3]), "elapsed");
+  c->flight_ms += ms_flight;
+  c->step_ms += ms_step;
+  c->ev_pending[q] = false;
+}
+void harvest_all_timing(mcb200_ctx *c) {
+  for (int q = 0; q < mcb200_ctx::kTimingRing; ++q) harvest_timing(c, q);
 }
 
 template <typename R>
@@ -535,6 +599,11 @@ int mcb200_create(const char *table_dir, double kelvin, int device, size_t max_p
     c->y.counters = dalloc<unsigned long long>(kCntNumCounters, c->owned);
     c->y.contact = dalloc<long long>(kMaxContacts * 6, c->owned);
     c->total = dalloc<unsigned int>(1, c->owned);
+    c->dev_counts = dalloc<unsigned int>(4, c->owned);
+    c->dev_psteps = dalloc<unsigned long long>(1, c->owned);
+    c->sink_count = dalloc<unsigned int>(1, c->owned);
+    ck(cudaMemsetAsync(c->dev_counts, 0, 4 * sizeof(unsigned int), c->stream), "memset");
+    ck(cudaMemsetAsync(c->dev_psteps, 0, sizeof(unsigned long long), c->stream), "memset");
     ck(cudaMallocHost(&c->h_pinned, 64 * sizeof(unsigned int)), "cudaMallocHost");
     ck(cudaMallocHost(&c->h_scratch, 16 * sizeof(double)), "cudaMallocHost");
     ck(cudaMemsetAsync(c->y.counters, 0, sizeof(unsigned long long) * kCntNumCounters, c->stream), "memset");
@@ -554,6 +623,11 @@ void mcb200_destroy(mcb200_ctx *ctx) { delete ctx; }
 int mcb200_set_flight_precision(mcb200_ctx *c, int precision) {
   if (!c || (precision != MCB200_FLIGHT_FP64 && precision != MCB200_FLIGHT_FP32)) return MCB200_ERR_ARG;
   if (c->device < 0) return fail(c, MCB200_ERR_STATE, "host-only context");
+  try {
+    pull_counts(c);
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CAPACITY, e.what());
+  }
   if (c->n != 0) return fail(c, MCB200_ERR_STATE, "flight precision can only change while the store is empty");
   if (precision == c->precision) return MCB200_OK;
   try {
@@ -789,9 +863,12 @@ int mcb200_upload_particles(mcb200_ctx *c, size_t n, const mcb200_particles *p) 
     c->cur = 0;
     if (c->precision == MCB200_FLIGHT_FP32) upload_store<float>(c, n, p, cell, meta);
     else upload_store<double>(c, n, p, cell, meta);
-    ck(cudaStreamSynchronize(c->stream), "sync");
     c->n = n;
     c->next_uid = maxuid;
+    c->overflow_pending = false;
+    ck(cudaMemsetAsync(c->dev_counts + 2, 0, sizeof(unsigned int), c->stream), "memset");
+    push_counts(c);
+    ck(cudaStreamSynchronize(c->stream), "sync");
     return MCB200_OK;
   } catch (const std::exception &e) {
     return fail(c, MCB200_ERR_CUDA, e.what());
@@ -800,6 +877,14 @@ int mcb200_upload_particles(mcb200_ctx *c, size_t n, const mcb200_particles *p) 
 
 int mcb200_download_particles(mcb200_ctx *c, mcb200_particles *p, size_t capacity, size_t *n_out) {
   if (!c || !p) return MCB200_ERR_ARG;
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    pull_counts(c);
+  } catch (const CapacityError &e) {
+    return fail(c, MCB200_ERR_CAPACITY, e.what());
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
   if (n_out) *n_out = c->n;
   if (capacity < c->n) return fail(c, MCB200_ERR_CAPACITY, "host buffers smaller than the particle count");
   try {
@@ -821,12 +906,50 @@ int mcb200_download_particles(mcb200_ctx *c, mcb200_particles *p, size_t capacit
   }
 }
 
-size_t mcb200_num_particles(const mcb200_ctx *c) { return c ? c->n : 0; }
+size_t mcb200_num_particles(const mcb200_ctx *cc) {
+  if (!cc) return 0;
+  mcb200_ctx *c = const_cast<mcb200_ctx *>(cc);  // reading the device count updates the host copy
+  if (c->n_stale) {
+    try {
+      cudaSetDevice(c->device);
+      pull_counts(c);
+    } catch (const CapacityError &e) {
+      c->overflow_pending = true;  // reported by the next call that returns a status
+      c->error = e.what();
+    } catch (const std::exception &e) {
+      c->error = e.what();
+    }
+  }
+  return c->n;
+}
+
+int mcb200_particle_steps(mcb200_ctx *c, uint64_t *total) {
+  if (!c || !total) return MCB200_ERR_ARG;
+  if (c->device < 0) return fail(c, MCB200_ERR_STATE, "host-only context");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    ck(cudaMemcpyAsync(c->h_scratch, c->dev_psteps, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream),
+       "copy");
+    ck(cudaStreamSynchronize(c->stream), "sync");
+    std::memcpy(total, c->h_scratch, sizeof(uint64_t));
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
 
 int mcb200_seed_particles(mcb200_ctx *c, size_t n, const int32_t *cell_of, const double *charge, int type,
                           uint64_t seed) {
   if (!c || (n > 0 && (!cell_of || !charge)) || type < 0 || type > 1) return MCB200_ERR_ARG;
   if (!c->mesh_set || !c->cells_set) return fail(c, MCB200_ERR_STATE, "mcb200_seed_particles needs mesh and cells");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    pull_counts(c);
+  } catch (const CapacityError &e) {
+    return fail(c, MCB200_ERR_CAPACITY, e.what());
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
   if (c->n + n > c->capacity) return fail(c, MCB200_ERR_CAPACITY, "more particles than the context capacity");
   for (size_t q = 0; q < n; ++q)
     if (cell_of[q] < 0 || cell_of[q] >= c->ncells) return fail(c, MCB200_ERR_ARG, "cell index outside the mesh");
@@ -853,10 +976,11 @@ int mcb200_seed_particles(mcb200_ctx *c, size_t n, const int32_t *cell_of, const
       launch_seed(F, store<double>(c, c->cur), (int)c->n, (int)n, dcell, dq, type, c->next_uid, grid_for(c, n, 256),
                   c->stream);
     ck(cudaGetLastError(), "seed kernel");
-    ck(cudaStreamSynchronize(c->stream), "sync");
-    for (void *p : tmp) cudaFree(p);
     c->n += n;
     c->next_uid += (uint32_t)n;
+    push_counts(c);
+    ck(cudaStreamSynchronize(c->stream), "sync");
+    for (void *p : tmp) cudaFree(p);
     return MCB200_OK;
   } catch (const std::exception &e) {
     return fail(c, MCB200_ERR_CUDA, e.what());
@@ -867,6 +991,10 @@ int mcb200_step(mcb200_ctx *c, uint32_t step, uint64_t seed, double dt) {
   if (!c) return MCB200_ERR_ARG;
   if (!c->mesh_set || !c->cells_set || !c->fields_set)
     return fail(c, MCB200_ERR_STATE, "mcb200_step needs mesh, cells and fields");
+  if (c->overflow_pending) {
+    c->overflow_pending = false;
+    return fail(c, MCB200_ERR_CAPACITY, "particle store full: GENERATE copies beyond the context capacity were dropped");
+  }
   try {
     ck(cudaSetDevice(c->device), "cudaSetDevice");
     if (c->precision == MCB200_FLIGHT_FP32) step_impl<float>(c, step, seed, dt);
@@ -884,11 +1012,17 @@ int mcb200_set_timing(mcb200_ctx *c, int enable) {
   if (c->device < 0) return fail(c, MCB200_ERR_STATE, "host-only context");
   try {
     ck(cudaSetDevice(c->device), "cudaSetDevice");
-    for (cudaEvent_t &e : c->ev)
-      if (!e) ck(cudaEventCreate(&e), "cudaEventCreate");
+    for (auto &q : c->ev)
+      for (cudaEvent_t &e : q)
+        if (!e) ck(cudaEventCreate(&e), "cudaEventCreate");
+    harvest_all_timing(c);
     c->timing = enable != 0;
     c->flight_ms = c->step_ms = 0;
     c->flight_launches = c->steps = c->particles_flown = c->launches = 0;
+    ck(cudaMemcpyAsync(c->h_scratch, c->dev_psteps, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream),
+       "copy");
+    ck(cudaStreamSynchronize(c->stream), "sync");
+    std::memcpy(&c->psteps_at_timing, c->h_scratch, sizeof(unsigned long long));
     return MCB200_OK;
   } catch (const std::exception &e) {
     return fail(c, MCB200_ERR_CUDA, e.what());
@@ -942,8 +1076,23 @@ int mcb200_elapsed_ms(mcb200_ctx *c, int from, int to, double *ms) {
   }
 }
 
-int mcb200_get_timing(const mcb200_ctx *c, double *out, int n) {
-  if (!c || !out) return MCB200_ERR_ARG;
+int mcb200_get_timing(const mcb200_ctx *cc, double *out, int n) {
+  if (!cc || !out) return MCB200_ERR_ARG;
+  mcb200_ctx *c = const_cast<mcb200_ctx *>(cc);  // outstanding event pairs are read back first
+  if (c->device >= 0 && c->timing) {
+    try {
+      ck(cudaSetDevice(c->device), "cudaSetDevice");
+      harvest_all_timing(c);
+      ck(cudaMemcpyAsync(c->h_scratch, c->dev_psteps, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream),
+         "copy");
+      ck(cudaStreamSynchronize(c->stream), "sync");
+      unsigned long long now = 0;
+      std::memcpy(&now, c->h_scratch, sizeof(now));
+      c->particles_flown = now - c->psteps_at_timing;
+    } catch (const std::exception &e) {
+      return fail(c, MCB200_ERR_CUDA, e.what());
+    }
+  }
   const double v[6] = {c->flight_ms, (double)c->flight_launches, c->step_ms, (double)c->steps,
                        (double)c->particles_flown, (double)c->launches};
   for (int i = 0; i < n && i < 6; ++i) out[i] = v[i];
@@ -953,7 +1102,15 @@ int mcb200_get_timing(const mcb200_ctx *c, double *out, int n) {
 int mcb200_sync(mcb200_ctx *c) {
   if (!c) return MCB200_ERR_ARG;
   cudaError_t e = cudaStreamSynchronize(c->stream);
-  return e == cudaSuccess ? MCB200_OK : fail(c, MCB200_ERR_CUDA, cudaGetErrorString(e));
+  if (e != cudaSuccess) return fail(c, MCB200_ERR_CUDA, cudaGetErrorString(e));
+  try {
+    pull_counts(c);
+  } catch (const CapacityError &x) {
+    return fail(c, MCB200_ERR_CAPACITY, x.what());
+  } catch (const std::exception &x) {
+    return fail(c, MCB200_ERR_CUDA, x.what());
+  }
+  return MCB200_OK;
 }
 
 int mcb200_get_tallies(mcb200_ctx *c, uint64_t *counters, double *contact, double *lcurrent, double *rcurrent,
@@ -963,6 +1120,7 @@ int mcb200_get_tallies(mcb200_ctx *c, uint64_t *counters, double *contact, doubl
   try {
     ck(cudaSetDevice(c->device), "cudaSetDevice");
     ck(cudaStreamSynchronize(c->stream), "sync");
+    pull_counts(c);
     if (counters) ck(cudaMemcpy(counters, c->y.counters, sizeof(uint64_t) * kCntNumCounters, cudaMemcpyDeviceToHost), "copy");
     if (contact) {
       std::vector<long long> v(kMaxContacts * 6);
@@ -988,6 +1146,8 @@ int mcb200_get_tallies(mcb200_ctx *c, uint64_t *counters, double *contact, doubl
     get(heat_e, c->y.heat_e, nodes, kEnergyScale);
     get(heat_h, c->y.heat_h, nodes, kEnergyScale);
     return MCB200_OK;
+  } catch (const CapacityError &e) {
+    return fail(c, MCB200_ERR_CAPACITY, e.what());
   } catch (const std::exception &e) {
     return fail(c, MCB200_ERR_CUDA, e.what());
   }
@@ -1066,6 +1226,9 @@ int mcb200_set_device(mcb200_ctx *c, const int32_t *material, const double *dono
     f.cg_part = dalloc<double>(3 * kCgMaxGrid, c->mesh_owned);  // the persistent CG's partial sums
     f.cg_scalars = dalloc<double>(16, c->mesh_owned);  // the CG scalars sc[0..9]
     f.abs_sum = dalloc<unsigned long long>(4, c->mesh_owned);
+    f.dep_scales = dalloc<DepositScales>(1, c->mesh_owned);
+    f.poisson_stats = dalloc<double>(3, c->mesh_owned);
+    ck(cudaMemset(f.poisson_stats, 0, 3 * sizeof(double)), "memset");
     ck(cudaMemset(f.potential, 0, nodes * sizeof(double)), "memset");
     ck(cudaMemset(f.density, 0, nodes * sizeof(double)), "memset");
     {  // multigrid hierarchy of the stencil, node coordinates from the cell widths
@@ -1102,29 +1265,12 @@ int mcb200_deposit(mcb200_ctx *c) {
   try {
     ck(cudaSetDevice(c->device), "cudaSetDevice");
     cudaStream_t s = c->stream;
-    const int grid = grid_for(c, c->n, 256);
-    const bool fp32 = c->precision == MCB200_FLIGHT_FP32;
-    if (fp32) launch_charge_bounds(store<float>(c, c->cur), (int)c->n, c->fb.abs_sum, grid, s);
-    else launch_charge_bounds(store<double>(c, c->cur), (int)c->n, c->fb.abs_sum, grid, s);
-    ck(cudaMemcpyAsync(c->h_scratch, c->fb.abs_sum, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
-       "copy");
-    ck(cudaStreamSynchronize(s), "sync");
-    unsigned long long b[4];
-    std::memcpy(b, c->h_scratch, sizeof(b));
-    double qmax[2];
-    std::memcpy(&qmax[0], &b[0], 8);
-    std::memcpy(&qmax[1], &b[1], 8);
-    // count x max|q| bounds every sum of a type; each sum gets 61 bits of range
-    auto unit = [](double bound) {
-      return std::ldexp(1.0, 61 - (int)std::ceil(std::log2(std::max(bound, 1e-300))));
-    };
-    const double be = (double)b[2] * qmax[0], bh = (double)b[3] * qmax[1];
-    const DepositScales S{{unit(be), unit(bh), unit(be + bh)}};
-    if (fp32) launch_deposit(store<float>(c, c->cur), (int)c->n, c->mesh, c->fb, S, grid, s);
-    else launch_deposit(store<double>(c, c->cur), (int)c->n, c->mesh, c->fb, S, grid, s);
-    c->launches += c->n > 0 ? 4 : 2;  // charge bounds, particle deposit, cell and node passes
+    const int grid = grid_for(c, c->capacity, 256);
+    const DevCount n{c->dev_counts, nullptr, (int)c->capacity};
+    if (c->precision == MCB200_FLIGHT_FP32) launch_deposit(store<float>(c, c->cur), n, c->mesh, c->fb, grid, s);
+    else launch_deposit(store<double>(c, c->cur), n, c->mesh, c->fb, grid, s);
+    c->launches += 5;  // charge bounds, units, particle deposit, cell and node passes
     ck(cudaGetLastError(), "deposit");
-    ck(cudaStreamSynchronize(s), "sync");
     c->fields_set = true;
     return MCB200_OK;
   } catch (const std::exception &e) {
@@ -1144,11 +1290,29 @@ int mcb200_solve_poisson(mcb200_ctx *c, double rel_tol, int max_iter, int *itera
       return fail(c, MCB200_ERR_CUDA, "Poisson solve failed");
     launch_pot2field(c->mesh, c->fb.potential, s);
     ck(cudaGetLastError(), "pot2field");
-    ck(cudaStreamSynchronize(s), "sync");
-    // rhs, the solve's set-up / dots / persistent CG / true residual (15 with
-    // Jacobi preconditioning, 12 with multigrid: no Jacobi z0 or r.z0), pot2field
-    c->launches += c->cg_plan.used == kCgMultigrid ? 14 : 17;
+    // rhs, the solve's set-up / dots / persistent CG / true residual /
+    // statistics (16 with Jacobi preconditioning, 13 with multigrid: no
+    // Jacobi z0 or r.z0), pot2field
+    c->launches += c->cg_plan.used == kCgMultigrid ? 15 : 18;
     c->fields_set = true;
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_poisson_stats(mcb200_ctx *c, int64_t *solves, int64_t *iterations, double *max_rel_residual, int reset) {
+  if (!c) return MCB200_ERR_ARG;
+  if (!c->device_set) return fail(c, MCB200_ERR_STATE, "mcb200_poisson_stats needs mcb200_set_device");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    ck(cudaMemcpyAsync(c->h_scratch + 10, c->fb.poisson_stats, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
+       "copy");
+    ck(cudaStreamSynchronize(c->stream), "sync");
+    if (solves) *solves = (int64_t)c->h_scratch[10];
+    if (iterations) *iterations = (int64_t)c->h_scratch[11];
+    if (max_rel_residual) *max_rel_residual = c->h_scratch[12];
+    if (reset) ck(cudaMemsetAsync(c->fb.poisson_stats, 0, 3 * sizeof(double), c->stream), "memset");
     return MCB200_OK;
   } catch (const std::exception &e) {
     return fail(c, MCB200_ERR_CUDA, e.what());
@@ -1214,6 +1378,7 @@ int mcb200_multiple_refresh(mcb200_ctx *c, const int32_t *desired_e, const int32
   if (!c->mesh_set) return fail(c, MCB200_ERR_STATE, "mcb200_multiple_refresh before mcb200_set_mesh");
   try {
     ck(cudaSetDevice(c->device), "cudaSetDevice");
+    pull_counts(c);
     cudaStream_t s = c->stream;
     const int cells = c->ncells;
     size_t want = 0;
@@ -1234,8 +1399,9 @@ int mcb200_multiple_refresh(mcb200_ctx *c, const int32_t *desired_e, const int32
     const RefreshParams r{seed, step, 2.0, 2.0, 1.0e-30};  // Rpar, Rsqr, pckill: src/mcmodel.cpp:3878-3880
     auto refresh = [&](auto tag) {
       using R = decltype(tag);
-      launch_cell_sort(store<R>(c, c->cur), (int)c->n, store<R>(c, sorted), cells, c->mesh.nx, c->mesh.nz, c->hist,
-                       c->offsets, c->tile_sums, c->total, grid_for(c, c->n, 256), s);
+      launch_cell_sort(store<R>(c, c->cur), DevCount{nullptr, nullptr, (int)c->n}, store<R>(c, sorted), cells,
+                       c->mesh.nx, c->mesh.nz, c->hist, c->offsets, c->tile_sums, c->total,
+                       grid_for(c, c->n, 256), s);
       const DevParticlesT<R> &P = store<R>(c, sorted);
       launch_refresh_count(P, c->offsets, c->hist, cells, de, dh, r, out_count, new_count, s);
       launch_exclusive_scan(out_count, out_off, tiles, tot, cells, s);
@@ -1245,7 +1411,7 @@ int mcb200_multiple_refresh(mcb200_ctx *c, const int32_t *desired_e, const int32
     };
     if (c->precision == MCB200_FLIGHT_FP32) refresh(float{});
     else refresh(double{});
-    c->launches += c->n > 0 ? 13 : 11;  // cell sort, count, two scans, emit
+    c->launches += 13;  // cell sort, count, two scans, emit, count update
     ck(cudaGetLastError(), "refresh");
     unsigned int totals[2];
     long long g = 0;
@@ -1256,8 +1422,11 @@ int mcb200_multiple_refresh(mcb200_ctx *c, const int32_t *desired_e, const int32
     c->cur = other;
     c->n = totals[0];
     c->next_uid += totals[1];
+    push_counts(c);
     if (generated) *generated = g;
     return MCB200_OK;
+  } catch (const CapacityError &e) {
+    return fail(c, MCB200_ERR_CAPACITY, e.what());
   } catch (const std::exception &e) {
     return fail(c, MCB200_ERR_CUDA, e.what());
   }
@@ -1295,9 +1464,10 @@ int mcb200_stat_begin(mcb200_ctx *c, int window_steps) {
   try {
     ck(cudaSetDevice(c->device), "cudaSetDevice");
     cudaStream_t s = c->stream;
-    const int grid = grid_for(c, c->n, 256);
-    if (c->precision == MCB200_FLIGHT_FP32) launch_charge_bounds(store<float>(c, c->cur), (int)c->n, c->stat_bounds, grid, s);
-    else launch_charge_bounds(store<double>(c, c->cur), (int)c->n, c->stat_bounds, grid, s);
+    const int grid = grid_for(c, c->capacity, 256);
+    const DevCount n{c->dev_counts, nullptr, (int)c->capacity};
+    if (c->precision == MCB200_FLIGHT_FP32) launch_charge_bounds(store<float>(c, c->cur), n, c->stat_bounds, grid, s);
+    else launch_charge_bounds(store<double>(c, c->cur), n, c->stat_bounds, grid, s);
     ck(cudaMemcpyAsync(c->h_scratch, c->stat_bounds, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
        "copy");
     ck(cudaStreamSynchronize(s), "sync");
@@ -1332,11 +1502,12 @@ int mcb200_stat_accumulate(mcb200_ctx *c) {
   try {
     ck(cudaSetDevice(c->device), "cudaSetDevice");
     cudaStream_t s = c->stream;
-    const int grid = grid_for(c, c->n, 256);
+    const int grid = grid_for(c, c->capacity, 256);
+    const DevCount n{c->dev_counts, nullptr, (int)c->capacity};
     if (c->precision == MCB200_FLIGHT_FP32)
-      launch_statistic(store<float>(c, c->cur), (int)c->n, c->mesh, c->dt, c->ss, c->sb, grid, s);
+      launch_statistic(store<float>(c, c->cur), n, c->mesh, c->dt, c->ss, c->sb, grid, s);
     else
-      launch_statistic(store<double>(c, c->cur), (int)c->n, c->mesh, c->dt, c->ss, c->sb, grid, s);
+      launch_statistic(store<double>(c, c->cur), n, c->mesh, c->dt, c->ss, c->sb, grid, s);
     if (c->device_set) launch_add_potential(c->sb.nodes, c->fb.potential, c->sb.pot_sum, s);
     ck(cudaGetLastError(), "statistic");
     c->stat_steps += 1;
@@ -1436,6 +1607,8 @@ namespace {
 // particles and the counting sort by cell.
 template <typename R>
 void step_impl(mcb200_ctx *c, uint32_t step, uint64_t seed, double dt) {
+  // Every size is read on the device (DevCount, child counts), so the step
+  // is enqueued without waiting for the GPU.
   cudaStream_t s = c->stream;
   FlightCtxT<R> F;
   F.T = c->dt;
@@ -1444,7 +1617,16 @@ void step_impl(mcb200_ctx *c, uint32_t step, uint64_t seed, double dt) {
   F.dt = dt;
   F.seed = seed;
   F.step = step;
-  if (c->timing) ck(cudaEventRecord(c->ev[0], s), "event");
+  cudaEvent_t *ev = nullptr;
+  if (c->timing) {
+    const int q = c->ev_head;
+    c->ev_head = (q + 1) % mcb200_ctx::kTimingRing;
+    harvest_timing(c, q);  // a slot is reused only after its step has finished
+    ev = c->ev[q];
+    c->ev_pending[q] = true;
+    ck(cudaEventRecord(ev[0], s), "event");
+  }
+  const int cap = (int)c->capacity;
   ck(cudaMemsetAsync(c->tickets, 0, sizeof(unsigned int) * (1 + mcb200_ctx::kGenerations), s), "memset");
   if constexpr (sizeof(R) == 4) {  // FP32 flight reads the fields as per-cell float records
     launch_cell_records32(c->dt, c->mesh, c->cell32, c->ncells, s);
@@ -1453,75 +1635,50 @@ void step_impl(mcb200_ctx *c, uint32_t step, uint64_t seed, double dt) {
   // 1. main flight; copies go to generation 0
   ck(cudaMemsetAsync(children<R>(c, 0).count, 0, sizeof(unsigned int), s), "memset");
   F.C = children<R>(c, 0);
-  if (c->timing) ck(cudaEventRecord(c->ev[1], s), "event");
-  launch_flight(F, store<R>(c, c->cur), (int)c->n, c->tickets, c->sm_count, s);
+  if (ev) ck(cudaEventRecord(ev[1], s), "event");
+  launch_flight(F, store<R>(c, c->cur), DevCount{c->dev_counts, nullptr, cap}, c->tickets, c->sm_count, s);
   ck(cudaGetLastError(), "flight kernel");
-  if (c->timing) ck(cudaEventRecord(c->ev[2], s), "event");
-  const size_t flown = c->n;
-  c->launches += c->n > 0 ? 1 : 0;
-  // 2. copies fly the rest of the step, generation by generation
-  unsigned int counts[mcb200_ctx::kGenerations] = {0, 0, 0, 0};
-  int gens = 0;
+  if (ev) ck(cudaEventRecord(ev[2], s), "event");
+  c->launches += 1;
+  // 2. copies fly the rest of the step, generation by generation (a
+  //    generation with no copies returns at once); copies of the last
+  //    generation are counted in a sink, not flown
   for (int g = 0; g < mcb200_ctx::kGenerations; ++g) {
-    ck(cudaMemcpyAsync(c->h_pinned, children<R>(c, g).count, sizeof(unsigned int), cudaMemcpyDeviceToHost, s), "count");
-    ck(cudaStreamSynchronize(s), "sync");
-    counts[g] = std::min<unsigned int>(c->h_pinned[0], (unsigned int)c->child_cap);
-    if (counts[g] == 0) break;
-    gens = g + 1;
     if (g + 1 < mcb200_ctx::kGenerations) {
       ck(cudaMemsetAsync(children<R>(c, g + 1).count, 0, sizeof(unsigned int), s), "memset");
       F.C = children<R>(c, g + 1);
     } else {
-      F.C = children<R>(c, g);  // a fifth generation would overflow: counted, not flown
+      ck(cudaMemsetAsync(c->sink_count, 0, sizeof(unsigned int), s), "memset");
+      F.C = children<R>(c, g);
+      F.C.count = c->sink_count;
       F.C.capacity = 0;
     }
-    launch_child_flight(F, children<R>(c, g), (int)counts[g], c->tickets + 1 + g, c->sm_count, s);
+    launch_child_flight(F, children<R>(c, g), c->child_cap, c->tickets + 1 + g, c->sm_count, s);
     ck(cudaGetLastError(), "child flight kernel");
     c->launches += 1;
   }
   // 3. uids for surviving copies, then append them to the store
-  size_t total_children = 0;
-  for (int g = 0; g < gens; ++g) {
-    launch_child_keys(children<R>(c, g), counts[g], c->child_keys + total_children, c->child_alive + total_children, s);
-    total_children += counts[g];
-  }
-  size_t n_all = c->n;
-  if (total_children > 0) {
-    if (c->n + total_children > c->capacity) throw CapacityError("particle store full after GENERATE");
-    launch_child_rank(c->child_keys, c->child_alive, (int)total_children, c->next_uid, c->child_uids, s);
-    ck(cudaMemsetAsync(c->append_count, 0, sizeof(unsigned int), s), "memset");
-    size_t off = 0;
-    for (int g = 0; g < gens; ++g) {
-      launch_children_to_particles(children<R>(c, g), counts[g], c->child_uids + off, c->child_alive + off,
-                                   store<R>(c, c->cur), (int)c->n, c->append_count, s);
-      off += counts[g];
-    }
-    ck(cudaMemcpyAsync(c->h_pinned, c->append_count, sizeof(unsigned int), cudaMemcpyDeviceToHost, s), "count");
-    ck(cudaStreamSynchronize(s), "sync");
-    const unsigned int appended = c->h_pinned[0];
-    n_all = c->n + appended;
-    c->next_uid += appended;
-    c->launches += 2 * gens + 1;
-  }
-  // 4. drop caught particles and counting-sort the store by cell
+  ChildSetT<R> set;
+  for (int g = 0; g < mcb200_ctx::kGenerations; ++g) set.g[g] = children<R>(c, g);
+  launch_append_children(set, c->child_keys, c->child_alive, c->child_uids, c->dev_counts + 1, store<R>(c, c->cur),
+                         c->dev_counts, cap, c->append_count, c->dev_counts + 2,
+                         grid_for(c, (size_t)c->child_cap * mcb200_ctx::kGenerations, 256), s);
+  ck(cudaGetLastError(), "append children");
+  c->launches += 3;
+  // 4. drop caught particles and counting-sort the store by cell; the
+  //    sorted count becomes the particle count
   const int other = 1 - c->cur;
-  launch_cell_sort(store<R>(c, c->cur), (int)n_all, store<R>(c, other), c->ncells, c->mesh.nx, c->mesh.nz, c->hist,
-                   c->offsets, c->tile_sums, c->total, grid_for(c, n_all, 256), s);
+  launch_cell_sort(store<R>(c, c->cur), DevCount{c->dev_counts, c->append_count, cap}, store<R>(c, other), c->ncells,
+                   c->mesh.nx, c->mesh.nz, c->hist, c->offsets, c->tile_sums, c->total, grid_for(c, c->capacity, 256),
+                   s);
+  launch_step_finish(c->dev_counts, c->total, c->dev_counts + 1, c->append_count, c->dev_psteps, s);
   ck(cudaGetLastError(), "cell sort");
-  c->launches += n_all > 0 ? 5 : 3;
-  ck(cudaMemcpyAsync(c->h_pinned, c->total, sizeof(unsigned int), cudaMemcpyDeviceToHost, s), "count");
-  if (c->timing) ck(cudaEventRecord(c->ev[3], s), "event");
-  ck(cudaStreamSynchronize(s), "sync");
-  c->n = c->h_pinned[0];
+  c->launches += 6;
+  if (ev) ck(cudaEventRecord(ev[3], s), "event");
   c->cur = other;
+  c->n_stale = true;
   if (c->timing) {
-    float ms_flight = 0, ms_step = 0;
-    ck(cudaEventElapsedTime(&ms_flight, c->ev[1], c->ev[2]), "elapsed");
-    ck(cudaEventElapsedTime(&ms_step, c->ev[0], c->ev[3]), "elapsed");
-    c->flight_ms += ms_flight;
-    c->step_ms += ms_step;
-    c->flight_launches += flown > 0 ? 1 : 0;
-    c->particles_flown += flown;
+    c->flight_launches += 1;
     c->steps += 1;
   }
 }

@@ -14,31 +14,38 @@ struct FlightCtxT;
 using FlightCtx = FlightCtxT<double>;
 
 // Persistent flight launches: `ticket` is a zeroed device counter the blocks
-// take particle indices from; n_hint bounds the children a generation holds.
+// take particle indices from; the main flight reads its particle count from
+// device memory (n.max sizes the grid), a child generation its own count;
+// n_hint bounds the copies a generation holds.
 template <typename R>
-void launch_flight(const FlightCtxT<R> &F, const DevParticlesT<R> &P, int n, unsigned int *ticket, int sm_count,
+void launch_flight(const FlightCtxT<R> &F, const DevParticlesT<R> &P, DevCount n, unsigned int *ticket, int sm_count,
                    cudaStream_t s);
 template <typename R>
 void launch_child_flight(const FlightCtxT<R> &F, const DevChildrenT<R> &in, int n_hint, unsigned int *ticket,
                          int sm_count, cudaStream_t s);
 // FP32 flight's per-cell records (DevMesh::cell32), [cells][3] float4.
 void launch_cell_records32(const DevTables &T, const DevMesh &M, float4 *out, int cells, cudaStream_t s);
+// The step's surviving copies (all generations) ranked by (parent uid, sub),
+// given uids from *next_uid on, and appended to `dst` after its *n
+// particles; *appended = surviving copies, *overflow set if the store is full.
 template <typename R>
-void launch_child_keys(const DevChildrenT<R> &c, int n, uint64_t *keys, uint8_t *alive, cudaStream_t s);
-void launch_child_rank(const uint64_t *keys, const uint8_t *alive, int n, uint32_t next_uid, uint32_t *uid_out,
-                       cudaStream_t s);
-template <typename R>
-void launch_children_to_particles(const DevChildrenT<R> &c, int n, const uint32_t *uids, const uint8_t *alive,
-                                  const DevParticlesT<R> &dst, int dst_offset, unsigned int *dst_count,
-                                  cudaStream_t s);
+void launch_append_children(const ChildSetT<R> &set, uint64_t *keys, uint8_t *alive, uint32_t *uids,
+                            unsigned int *next_uid, const DevParticlesT<R> &dst, const unsigned int *n, int capacity,
+                            unsigned int *appended, unsigned int *overflow, int grid, cudaStream_t s);
+// *particle_steps += *n; *n = *sorted_total; *next_uid += *appended.
+void launch_step_finish(unsigned int *n, const unsigned int *sorted_total, unsigned int *next_uid,
+                        const unsigned int *appended, unsigned long long *particle_steps, cudaStream_t s);
 template <typename R>
 void launch_seed(const FlightCtx &F, const DevParticlesT<R> &P, int offset, int n, const int *cell_of,
                  const double *charge, int type, uint32_t uid0, int grid, cudaStream_t s);
 void launch_exclusive_scan(const unsigned int *in, unsigned int *out, unsigned int *tile_sums, unsigned int *total,
                            int n, cudaStream_t s);
+// Counting sort of the live particles among the first n (device count) of
+// `src` by cell into `dst`; *total = live particles, offsets = cell starts
+// (after the scatter: cell ends).
 template <typename R>
-void launch_cell_sort(const DevParticlesT<R> &src, int n, const DevParticlesT<R> &dst, int ncells, int nx, int nz,
-                      unsigned int *hist, unsigned int *offsets, unsigned int *tile_sums, unsigned int *total,
+void launch_cell_sort(const DevParticlesT<R> &src, DevCount n, const DevParticlesT<R> &dst, int ncells, int nx,
+                      int nz, unsigned int *hist, unsigned int *offsets, unsigned int *tile_sums, unsigned int *total,
                       int grid, cudaStream_t s);
 
 }  // namespace mcb200

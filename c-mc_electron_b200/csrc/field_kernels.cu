@@ -31,7 +31,9 @@ constexpr uint32_t kDeadBit = 1u << 16;
 // like the value for non-negative doubles) and the particle count.  count x
 // max |q| bounds every cell or node sum of that type, exactly and
 // independently of thread order.  out = {max_e bits, max_h bits, n_e, n_h}.
-__global__ void charge_bounds_kernel(const double *charge, const uint32_t *meta, int n, unsigned long long *out) {
+__global__ void charge_bounds_kernel(const double *charge, const uint32_t *meta, DevCount count,
+                                     unsigned long long *out) {
+  const int n = count.get();
   unsigned long long mx[2] = {0, 0}, cnt[2] = {0, 0};
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
     const uint32_t m = meta[p];
@@ -58,10 +60,30 @@ __device__ __forceinline__ void fx_add(long long *p, double v, double scale) {
   atomicAdd(reinterpret_cast<unsigned long long *>(p), (unsigned long long)__double2ll_rn(v * scale));
 }
 
+// Fixed-point units from the bounds of charge_bounds_kernel: a sum whose
+// magnitude is below 2^e gets the unit 2^(61 - e) (61 bits of range);
+// empty sums get 1.
+__device__ double fixed_unit(double bound) {
+  if (!(bound > 0.0)) return 1.0;
+  int e = 0;
+  frexp(bound, &e);  // bound < 2^e
+  return ldexp(1.0, 61 - e);
+}
+__global__ void deposit_scales_kernel(const unsigned long long *b, DepositScales *out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double qe = __longlong_as_double((long long)b[0]), qh = __longlong_as_double((long long)b[1]);
+  const double be = (double)b[2] * qe, bh = (double)b[3] * qh;
+  out->s[0] = fixed_unit(be);
+  out->s[1] = fixed_unit(bh);
+  out->s[2] = fixed_unit(be + bh);
+}
+
 // scale[0]: electron cell sums, [1]: hole cell sums, [2]: |q| and node sums.
 template <typename R>
-__global__ void deposit_kernel(DevParticlesT<R> P, int n, DevMesh M, DepositScales S, long long *cell_e,
-                               long long *cell_h, long long *cell_abs, long long *node_q) {
+__global__ void deposit_kernel(DevParticlesT<R> P, DevCount count, DevMesh M, const DepositScales *Sp,
+                               long long *cell_e, long long *cell_h, long long *cell_abs, long long *node_q) {
+  const int n = count.get();
+  const DepositScales S = *Sp;
   const int px = M.nx + 1, pz = M.nz + 1;
   const double scale = S.s[2];
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
@@ -97,11 +119,12 @@ __global__ void deposit_kernel(DevParticlesT<R> P, int n, DevMesh M, DepositScal
 }
 
 // compute_cell_charge's final loop (:2705-2710) and the per-cell sums.
-__global__ void deposit_cells_kernel(int cells, DepositScales S, const long long *cell_e, const long long *cell_h,
-                                     const long long *cell_abs, const double *cvol, const double *da, double *e_out,
-                                     double *h_out, double *rho_out) {
+__global__ void deposit_cells_kernel(int cells, const DepositScales *Sp, const long long *cell_e,
+                                     const long long *cell_h, const long long *cell_abs, const double *cvol,
+                                     const double *da, double *e_out, double *h_out, double *rho_out) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= cells) return;
+  const DepositScales S = *Sp;
   e_out[c] = (double)cell_e[c] / S.s[0];
   h_out[c] = (double)cell_h[c] / S.s[1];
   const double r = (double)cell_abs[c] / S.s[2] / cvol[c];
@@ -110,11 +133,11 @@ __global__ void deposit_cells_kernel(int cells, DepositScales S, const long long
 }
 
 // particle_to_density's volume division (:408-416).
-__global__ void deposit_nodes_kernel(int nodes, double scale, const long long *node_q, const double *pvol,
+__global__ void deposit_nodes_kernel(int nodes, const DepositScales *Sp, const long long *node_q, const double *pvol,
                                      double *density) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nodes) return;
-  const double q = (double)node_q[p] / scale;
+  const double q = (double)node_q[p] / Sp->s[2];
   density[p] = fabs(pvol[p]) > 0 ? q / pvol[p] : q;
 }
 
@@ -299,6 +322,17 @@ __global__ void __launch_bounds__(kRedBlock) cg_persistent(int nodes, Grid3 g, c
   }
 }
 
+// Running solve statistics: st[0] solves, st[1] iterations, st[2] the
+// largest relative true residual.  sc[3] holds the final ||b - Ax||^2 and
+// sc[6] ||b||^2.
+__global__ void poisson_stats_kernel(const double *sc, double *st) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double bnorm = sqrt(sc[6]) > 0 ? sqrt(sc[6]) : 1.0;
+  st[0] += 1.0;
+  st[1] += sc[8];
+  st[2] = fmax(st[2], sqrt(sc[3]) / bnorm);
+}
+
 // sc[9] = (rel_tol * ||b||)^2; converged already when the warm start meets it
 __global__ void cg_setup(double *sc, double rel_tol2) {
   sc[9] = rel_tol2 * sc[6];
@@ -334,33 +368,35 @@ __global__ void pot2field_kernel(DevMesh M, const double *pot, double *efield, d
 static inline int blocks(long long n, int b) { return (int)((n + b - 1) / b); }
 
 template <typename R>
-void launch_charge_bounds(const DevParticlesT<R> &P, int n, unsigned long long *out, int grid, cudaStream_t s) {
+void launch_charge_bounds(const DevParticlesT<R> &P, DevCount n, unsigned long long *out, int grid, cudaStream_t s) {
   cudaMemsetAsync(out, 0, 4 * sizeof(unsigned long long), s);
-  if (n > 0) charge_bounds_kernel<<<grid, 256, 0, s>>>(P.charge, P.meta, n, out);
+  charge_bounds_kernel<<<grid, 256, 0, s>>>(P.charge, P.meta, n, out);
 }
 
 template <typename R>
-void launch_deposit(const DevParticlesT<R> &P, int n, const DevMesh &M, const FieldBuffers &f, const DepositScales &S,
-                    int grid, cudaStream_t s) {
+void launch_deposit(const DevParticlesT<R> &P, DevCount n, const DevMesh &M, const FieldBuffers &f, int grid,
+                    cudaStream_t s) {
   const int cells = M.nx * M.ny * M.nz, nodes = (M.nx + 1) * (M.ny + 1) * (M.nz + 1);
+  launch_charge_bounds(P, n, f.abs_sum, grid, s);
+  deposit_scales_kernel<<<1, 32, 0, s>>>(f.abs_sum, f.dep_scales);
   cudaMemsetAsync(f.acc_cell, 0, sizeof(long long) * 3 * (size_t)cells, s);
   cudaMemsetAsync(f.acc_node, 0, sizeof(long long) * (size_t)nodes, s);
-  if (n > 0)
-    deposit_kernel<R><<<grid, 256, 0, s>>>(P, n, M, S, f.acc_cell, f.acc_cell + cells, f.acc_cell + 2 * (size_t)cells,
-                                         f.acc_node);
-  deposit_cells_kernel<<<blocks(cells, 256), 256, 0, s>>>(cells, S, f.acc_cell, f.acc_cell + cells,
+  deposit_kernel<R><<<grid, 256, 0, s>>>(P, n, M, f.dep_scales, f.acc_cell, f.acc_cell + cells,
+                                         f.acc_cell + 2 * (size_t)cells, f.acc_node);
+  deposit_cells_kernel<<<blocks(cells, 256), 256, 0, s>>>(cells, f.dep_scales, f.acc_cell, f.acc_cell + cells,
                                                            f.acc_cell + 2 * (size_t)cells, f.cvol, M.da, f.cell_e,
                                                            f.cell_h, const_cast<double *>(M.rho));
-  deposit_nodes_kernel<<<blocks(nodes, 256), 256, 0, s>>>(nodes, S.s[2], f.acc_node, f.pvol, f.density);
+  deposit_nodes_kernel<<<blocks(nodes, 256), 256, 0, s>>>(nodes, f.dep_scales, f.acc_node, f.pvol, f.density);
 }
 
-template void launch_charge_bounds<double>(const DevParticlesT<double> &, int, unsigned long long *, int,
+template void launch_charge_bounds<double>(const DevParticlesT<double> &, DevCount, unsigned long long *, int,
                                            cudaStream_t);
-template void launch_charge_bounds<float>(const DevParticlesT<float> &, int, unsigned long long *, int, cudaStream_t);
-template void launch_deposit<double>(const DevParticlesT<double> &, int, const DevMesh &, const FieldBuffers &,
-                                     const DepositScales &, int, cudaStream_t);
-template void launch_deposit<float>(const DevParticlesT<float> &, int, const DevMesh &, const FieldBuffers &,
-                                    const DepositScales &, int, cudaStream_t);
+template void launch_charge_bounds<float>(const DevParticlesT<float> &, DevCount, unsigned long long *, int,
+                                          cudaStream_t);
+template void launch_deposit<double>(const DevParticlesT<double> &, DevCount, const DevMesh &, const FieldBuffers &,
+                                     int, cudaStream_t);
+template void launch_deposit<float>(const DevParticlesT<float> &, DevCount, const DevMesh &, const FieldBuffers &,
+                                    int, cudaStream_t);
 
 void launch_rhs(int nodes, const FieldBuffers &f, cudaStream_t s) {
   rhs_kernel<<<blocks(nodes, 256), 256, 0, s>>>(nodes, f.density, f.pvol, f.pdop, f.dirichlet, f.bc_vapp, f.vadd,
@@ -428,16 +464,15 @@ int cg_solve(const DevMesh &M, const FieldBuffers &f, double rel_tol, int max_it
       return 1;
   }
   plan.launches += 1;
-  cudaMemcpyAsync(host_scratch, sc, 10 * sizeof(double), cudaMemcpyDeviceToHost, s);
-  if (cudaStreamSynchronize(s) != cudaSuccess) return 1;
-  const int it = (int)host_scratch[8];
-  const double bnorm = sqrt(host_scratch[6]) > 0 ? sqrt(host_scratch[6]) : 1.0;
-  // true residual of the final iterate
+  // true residual of the final iterate, and the running statistics
   stencil_apply<<<nb, 256, 0, s>>>(nodes, g, f.stencil, f.dirichlet, f.potential, f.rhs, f.cg_r);
   dot(nodes, f.cg_r, f.cg_r, f.cg_part, sc + 3, s);
-  cudaMemcpyAsync(host_scratch, sc, 8 * sizeof(double), cudaMemcpyDeviceToHost, s);
+  poisson_stats_kernel<<<1, 32, 0, s>>>(sc, f.poisson_stats);
+  if (!iterations && !rel_residual) return cudaGetLastError() == cudaSuccess ? 0 : 1;  // nothing waits
+  cudaMemcpyAsync(host_scratch, sc, 10 * sizeof(double), cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return 1;
-  if (iterations) *iterations = it;
+  const double bnorm = sqrt(host_scratch[6]) > 0 ? sqrt(host_scratch[6]) : 1.0;
+  if (iterations) *iterations = (int)host_scratch[8];
   if (rel_residual) *rel_residual = sqrt(host_scratch[3]) / bnorm;
   return 0;
 }

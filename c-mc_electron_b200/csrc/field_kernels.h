@@ -9,6 +9,12 @@
 
 namespace mcb200 {
 
+// Fixed-point units (powers of two) of the deposition sums: electron cell
+// charge, hole cell charge, |charge| and node charge.
+struct DepositScales {
+  double s[3];
+};
+
 struct FieldBuffers {
   // device description (poisson_setup.h), uploaded once
   double *cvol = nullptr, *pvol = nullptr, *pdop = nullptr, *vadd = nullptr;
@@ -24,22 +30,20 @@ struct FieldBuffers {
   double *rhs = nullptr, *potential = nullptr;
   double *cg_r = nullptr, *cg_z = nullptr, *cg_p = nullptr, *cg_p1 = nullptr, *cg_q = nullptr, *cg_part = nullptr,
          *cg_scalars = nullptr;
-  unsigned long long *abs_sum = nullptr;
+  unsigned long long *abs_sum = nullptr;   // charge bounds of the last deposit (charge_bounds_kernel)
+  DepositScales *dep_scales = nullptr;        // fixed-point units of the last deposit (device)
   const MgDevice *mg = nullptr;  // multigrid hierarchy of the stencil (null: Jacobi preconditioning only)
-};
-
-// Fixed-point units (powers of two) of the deposition sums: electron cell
-// charge, hole cell charge, |charge| and node charge.
-struct DepositScales {
-  double s[3];
+  double *poisson_stats = nullptr;  // [3] solves, iterations, largest relative residual (since the last reset)
 };
 
 // out[4] = {max |q| bits of electrons, of holes, electron count, hole count}
 template <typename R>
-void launch_charge_bounds(const DevParticlesT<R> &P, int n, unsigned long long *out, int grid, cudaStream_t s);
+void launch_charge_bounds(const DevParticlesT<R> &P, DevCount n, unsigned long long *out, int grid, cudaStream_t s);
+// Charge bounds, fixed-point units (f.dep_scales) and the deposition sums,
+// all on the device: nothing waits for the host.
 template <typename R>
-void launch_deposit(const DevParticlesT<R> &P, int n, const DevMesh &M, const FieldBuffers &f, const DepositScales &S,
-                    int grid, cudaStream_t s);
+void launch_deposit(const DevParticlesT<R> &P, DevCount n, const DevMesh &M, const FieldBuffers &f, int grid,
+                    cudaStream_t s);
 void launch_rhs(int nodes, const FieldBuffers &f, cudaStream_t s);
 // The CG iterations of one solve run in one cooperative launch; its grid
 // (blocks) is fixed per context on first use, so the reduction order is too.
@@ -52,7 +56,9 @@ struct CgPlan {
   int used = 0;          // kCgJacobi or kCgMultigrid, set by the last solve
   unsigned long long launches = 0;
 };
-// Returns 0 on success; host_scratch must hold 10 doubles (pinned).
+// Returns 0 on success; host_scratch must hold 10 doubles (pinned).  With
+// iterations and rel_residual both null nothing waits for the GPU (the
+// results only reach f.poisson_stats).
 int cg_solve(const DevMesh &M, const FieldBuffers &f, double rel_tol, int max_iter, cudaStream_t s,
              double *host_scratch, int *iterations, double *rel_residual, CgPlan &plan);
 void launch_pot2field(const DevMesh &M, const double *pot, cudaStream_t s);

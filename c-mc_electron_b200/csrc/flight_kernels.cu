@@ -156,11 +156,13 @@ __device__ __forceinline__ void fly_interleaved(const FlightCtxT<R> &F, const Sy
 }
 
 template <typename R>
-__global__ void __launch_bounds__(256, kFlightBlocks<R>) flight_kernel(FlightCtxT<R> F, DevParticlesT<R> P, int n,
-                                                        unsigned int *ticket) {
+__global__ void __launch_bounds__(256, kFlightBlocks<R>) flight_kernel(FlightCtxT<R> F, DevParticlesT<R> P,
+                                                                       DevCount n, unsigned int *ticket) {
+  const int count = n.get();
+  if (count == 0) return;
   __shared__ SymSmemT<R> S;
   load_sym(S, F.T);
-  fly_interleaved(F, S, StoreIO<R>{P, F.dt}, n, ticket);
+  fly_interleaved(F, S, StoreIO<R>{P, F.dt}, count, ticket);
 }
 
 // Copies made during the previous pass (buffer `in`) fly the rest of their
@@ -168,9 +170,11 @@ __global__ void __launch_bounds__(256, kFlightBlocks<R>) flight_kernel(FlightCtx
 template <typename R>
 __global__ void __launch_bounds__(256, kFlightBlocks<R>) child_flight_kernel(FlightCtxT<R> F, DevChildrenT<R> in,
                                                               unsigned int *ticket) {
+  const int count = min((int)*in.count, in.capacity);
+  if (count == 0) return;
   __shared__ SymSmemT<R> S;
   load_sym(S, F.T);
-  fly_interleaved(F, S, ChildIO<R>{in}, min((int)*in.count, in.capacity), ticket);
+  fly_interleaved(F, S, ChildIO<R>{in}, count, ticket);
 }
 
 // FP32 flight's per-cell records (DevMesh::cell32): the fields in float and
@@ -193,26 +197,33 @@ __global__ void cell_records32_kernel(DevTables T, DevMesh M, float4 *out, int c
                                        (float)(T.frickel * 4 * kPiD * rho / T.eps_si), (float)(0.120 / T.eV0), 0.0f);
 }
 
-// uid of each surviving copy: next_uid + number of surviving copies with a
-// smaller (parent uid, sub) key, over all copies of this step.  The key set
-// is the concatenation of the child generations (one buffer per generation).
-__global__ void child_rank_kernel(const uint64_t *keys, const uint8_t *alive, int n, uint32_t next_uid,
-                                  uint32_t *uid_out) {
+// uid of each surviving copy: *next_uid + number of surviving copies with a
+// smaller (parent uid, sub) key, over all copies of this step (the key set
+// is the concatenation of the child generations).  Blocks stride over the
+// copies; each block compares its 256 keys with all keys, 256 at a time.
+template <typename R>
+__global__ void child_rank_kernel(ChildSetT<R> set, const uint64_t *keys, const uint8_t *alive,
+                                  const unsigned int *next_uid, uint32_t *uid_out) {
   __shared__ uint64_t tile[256];
   __shared__ uint8_t tile_alive[256];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint64_t my = i < n ? keys[i] : 0;
-  uint32_t rank = 0;
-  for (int base = 0; base < n; base += 256) {
-    const int j = base + threadIdx.x;
-    tile[threadIdx.x] = j < n ? keys[j] : ~0ull;
-    tile_alive[threadIdx.x] = j < n ? alive[j] : 0;
-    __syncthreads();
-    const int m = min(256, n - base);
-    for (int q = 0; q < m; ++q) rank += (tile_alive[q] && tile[q] < my) ? 1u : 0u;
-    __syncthreads();
+  int n = 0;
+  set.offset(0, &n);
+  const uint32_t uid0 = *next_uid;
+  for (int base_i = blockIdx.x * 256; base_i < n; base_i += gridDim.x * 256) {
+    const int i = base_i + threadIdx.x;
+    const uint64_t my = i < n ? keys[i] : 0;
+    uint32_t rank = 0;
+    for (int base = 0; base < n; base += 256) {
+      const int j = base + threadIdx.x;
+      tile[threadIdx.x] = j < n ? keys[j] : ~0ull;
+      tile_alive[threadIdx.x] = j < n ? alive[j] : 0;
+      __syncthreads();
+      const int m = min(256, n - base);
+      for (int q = 0; q < m; ++q) rank += (tile_alive[q] && tile[q] < my) ? 1u : 0u;
+      __syncthreads();
+    }
+    if (i < n) uid_out[i] = uid0 + rank;
   }
-  if (i < n) uid_out[i] = next_uid + rank;
 }
 
 // ---- counting sort by cell ------------------------------------------------
@@ -220,8 +231,9 @@ __device__ __forceinline__ int cell_linear(uint32_t c, int nx, int nz) {
   return (int)((((c >> 10) & 1023) * nx + (c & 1023)) * nz + ((c >> 20) & 1023));
 }
 
-__global__ void cell_histogram(const uint32_t *cell, const uint32_t *meta, int n, int nx, int nz,
+__global__ void cell_histogram(const uint32_t *cell, const uint32_t *meta, DevCount count, int nx, int nz,
                                unsigned int *hist) {
+  const int n = count.get();
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
     if (!(meta[p] & kMetaDead)) atomicAdd(&hist[cell_linear(cell[p], nx, nz)], 1u);
 }
@@ -260,7 +272,9 @@ __global__ void scan_add(unsigned int *out, const unsigned int *tile_sums, int n
 }
 
 template <typename R>
-__global__ void cell_scatter(DevParticlesT<R> src, int n, DevParticlesT<R> dst, unsigned int *cursor, int nx, int nz) {
+__global__ void cell_scatter(DevParticlesT<R> src, DevCount count, DevParticlesT<R> dst, unsigned int *cursor, int nx,
+                             int nz) {
+  const int n = count.get();
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
     const uint32_t m = src.meta[p];
     if (m & kMetaDead) continue;
@@ -275,28 +289,76 @@ __global__ void cell_scatter(DevParticlesT<R> src, int n, DevParticlesT<R> dst, 
   }
 }
 
-// Append surviving copies (already flown) to the particle store, with uids.
+// Append the surviving copies (already flown) of every generation to the
+// particle store after its *n particles, with their uids.  `appended` counts
+// every surviving copy; one that would land beyond the store's capacity is
+// dropped and raises *overflow (the host reports it).
 template <typename R>
-__global__ void children_to_particles(DevChildrenT<R> c, int n, const uint32_t *uids, const uint8_t *alive,
-                                      DevParticlesT<R> dst, int dst_offset, unsigned int *dst_count) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || !alive[i]) return;
-  const unsigned int q = dst_offset + atomicAdd(dst_count, 1u);
-  dst.x[q] = c.x[i]; dst.y[q] = c.y[i]; dst.z[q] = c.z[i];
-  dst.kx[q] = c.kx[i]; dst.ky[q] = c.ky[i]; dst.kz[q] = c.kz[i];
-  dst.energy[q] = c.energy[i]; dst.charge[q] = c.charge[i];
-  dst.cell[q] = c.cell[i];
-  dst.itet[q] = c.itet[i];
-  dst.meta[q] = c.meta[i] & 0xffffu;
-  dst.uid[q] = uids[i];
+__global__ void children_to_particles(ChildSetT<R> set, const uint32_t *uids, const uint8_t *alive,
+                                      DevParticlesT<R> dst, const unsigned int *n, int capacity,
+                                      unsigned int *appended, unsigned int *overflow) {
+  int total = 0;
+  set.offset(0, &total);
+  const unsigned int n0 = *n;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    if (!alive[i]) continue;
+    int gen = 0, local = i;
+#pragma unroll
+    for (int q = 0; q + 1 < kChildGenerations; ++q) {
+      const int cnt = min((int)*set.g[gen].count, set.g[gen].capacity);
+      if (local >= cnt) {
+        local -= cnt;
+        ++gen;
+      }
+    }
+    const DevChildrenT<R> &c = set.g[gen];
+    const unsigned long long q = (unsigned long long)n0 + atomicAdd(appended, 1u);
+    if (q >= (unsigned long long)capacity) {
+      *overflow = 1u;
+      continue;
+    }
+    dst.x[q] = c.x[local]; dst.y[q] = c.y[local]; dst.z[q] = c.z[local];
+    dst.kx[q] = c.kx[local]; dst.ky[q] = c.ky[local]; dst.kz[q] = c.kz[local];
+    dst.energy[q] = c.energy[local]; dst.charge[q] = c.charge[local];
+    dst.cell[q] = c.cell[local];
+    dst.itet[q] = c.itet[local];
+    dst.meta[q] = c.meta[local] & 0xffffu;
+    dst.uid[q] = uids[i];
+  }
 }
 
+// Rank keys (parent uid, sub) and survival flags of the copies of every
+// generation, concatenated in generation order.
 template <typename R>
-__global__ void child_keys(DevChildrenT<R> c, int n, uint64_t *keys, uint8_t *alive) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  keys[i] = ((uint64_t)c.parent_uid[i] << 32) | c.sub[i];
-  alive[i] = (c.meta[i] & kMetaDead) ? 0 : 1;
+__global__ void child_keys(ChildSetT<R> set, uint64_t *keys, uint8_t *alive) {
+  int total = 0;
+  set.offset(0, &total);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    int gen = 0, local = i;
+#pragma unroll
+    for (int q = 0; q + 1 < kChildGenerations; ++q) {
+      const int cnt = min((int)*set.g[gen].count, set.g[gen].capacity);
+      if (local >= cnt) {
+        local -= cnt;
+        ++gen;
+      }
+    }
+    const DevChildrenT<R> &c = set.g[gen];
+    keys[i] = ((uint64_t)c.parent_uid[local] << 32) | c.sub[local];
+    alive[i] = (c.meta[local] & kMetaDead) ? 0 : 1;
+  }
+}
+
+// End of a step: the sorted store's count becomes the particle count, the
+// uid counter advances past this step's copies, and the particles flown this
+// step (the count at its start) are added to the particle-step total.
+__global__ void step_finish(unsigned int *n, const unsigned int *sorted_total, unsigned int *next_uid,
+                            const unsigned int *appended, unsigned long long *particle_steps) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    *particle_steps += *n;
+    *n = *sorted_total;
+    *next_uid += *appended;
+  }
 }
 
 // ---- initial ensemble ---------------------------------------------------------
@@ -389,9 +451,9 @@ int flight_grid(int n, int block, int sm_count) {
 }
 
 template <typename R>
-void launch_flight(const FlightCtxT<R> &F, const DevParticlesT<R> &P, int n, unsigned int *ticket, int sm_count,
+void launch_flight(const FlightCtxT<R> &F, const DevParticlesT<R> &P, DevCount n, unsigned int *ticket, int sm_count,
                    cudaStream_t s) {
-  if (n > 0) flight_kernel<R><<<flight_grid<R>(n, 256, sm_count), 256, 0, s>>>(F, P, n, ticket);
+  flight_kernel<R><<<flight_grid<R>(n.max, 256, sm_count), 256, 0, s>>>(F, P, n, ticket);
 }
 template <typename R>
 void launch_child_flight(const FlightCtxT<R> &F, const DevChildrenT<R> &in, int n_hint, unsigned int *ticket,
@@ -402,19 +464,17 @@ void launch_cell_records32(const DevTables &T, const DevMesh &M, float4 *out, in
   if (cells > 0) cell_records32_kernel<<<(cells + 255) / 256, 256, 0, s>>>(T, M, out, cells);
 }
 template <typename R>
-void launch_child_keys(const DevChildrenT<R> &c, int n, uint64_t *keys, uint8_t *alive, cudaStream_t s) {
-  if (n > 0) child_keys<R><<<(n + 255) / 256, 256, 0, s>>>(c, n, keys, alive);
+void launch_append_children(const ChildSetT<R> &set, uint64_t *keys, uint8_t *alive, uint32_t *uids,
+                            unsigned int *next_uid, const DevParticlesT<R> &dst, const unsigned int *n, int capacity,
+                            unsigned int *appended, unsigned int *overflow, int grid, cudaStream_t s) {
+  child_keys<R><<<grid, 256, 0, s>>>(set, keys, alive);
+  child_rank_kernel<R><<<grid, 256, 0, s>>>(set, keys, alive, next_uid, uids);
+  cudaMemsetAsync(appended, 0, sizeof(unsigned int), s);
+  children_to_particles<R><<<grid, 256, 0, s>>>(set, uids, alive, dst, n, capacity, appended, overflow);
 }
-void launch_child_rank(const uint64_t *keys, const uint8_t *alive, int n, uint32_t next_uid, uint32_t *uid_out,
-                       cudaStream_t s) {
-  if (n > 0) child_rank_kernel<<<(n + 255) / 256, 256, 0, s>>>(keys, alive, n, next_uid, uid_out);
-}
-template <typename R>
-void launch_children_to_particles(const DevChildrenT<R> &c, int n, const uint32_t *uids, const uint8_t *alive,
-                                  const DevParticlesT<R> &dst, int dst_offset, unsigned int *dst_count,
-                                  cudaStream_t s) {
-  if (n > 0)
-    children_to_particles<R><<<(n + 255) / 256, 256, 0, s>>>(c, n, uids, alive, dst, dst_offset, dst_count);
+void launch_step_finish(unsigned int *n, const unsigned int *sorted_total, unsigned int *next_uid,
+                        const unsigned int *appended, unsigned long long *particle_steps, cudaStream_t s) {
+  step_finish<<<1, 32, 0, s>>>(n, sorted_total, next_uid, appended, particle_steps);
 }
 void launch_exclusive_scan(const unsigned int *in, unsigned int *out, unsigned int *tile_sums, unsigned int *total,
                            int n, cudaStream_t s) {
@@ -424,30 +484,29 @@ void launch_exclusive_scan(const unsigned int *in, unsigned int *out, unsigned i
   scan_add<<<tiles, 1024, 0, s>>>(out, tile_sums, n);
 }
 template <typename R>
-void launch_cell_sort(const DevParticlesT<R> &src, int n, const DevParticlesT<R> &dst, int ncells, int nx, int nz,
-                      unsigned int *hist, unsigned int *offsets, unsigned int *tile_sums, unsigned int *total,
+void launch_cell_sort(const DevParticlesT<R> &src, DevCount n, const DevParticlesT<R> &dst, int ncells, int nx,
+                      int nz, unsigned int *hist, unsigned int *offsets, unsigned int *tile_sums, unsigned int *total,
                       int grid, cudaStream_t s) {
   cudaMemsetAsync(hist, 0, sizeof(unsigned int) * ncells, s);
-  if (n > 0) cell_histogram<<<grid, 256, 0, s>>>(src.cell, src.meta, n, nx, nz, hist);
+  cell_histogram<<<grid, 256, 0, s>>>(src.cell, src.meta, n, nx, nz, hist);
   const int tiles = (ncells + 1023) / 1024;
   scan_tiles<<<tiles, 1024, 0, s>>>(hist, offsets, tile_sums, ncells);
   scan_tile_sums<<<1, 32, 0, s>>>(tile_sums, tiles, total);
   scan_add<<<tiles, 1024, 0, s>>>(offsets, tile_sums, ncells);
-  if (n > 0) cell_scatter<R><<<grid, 256, 0, s>>>(src, n, dst, offsets, nx, nz);
+  cell_scatter<R><<<grid, 256, 0, s>>>(src, n, dst, offsets, nx, nz);
 }
 
 #define MCB200_INSTANTIATE(R)                                                                                   \
   template void launch_seed<R>(const FlightCtx &, const DevParticlesT<R> &, int, int, const int *,            \
                                const double *, int, uint32_t, int, cudaStream_t);                             \
-  template void launch_flight<R>(const FlightCtxT<R> &, const DevParticlesT<R> &, int, unsigned int *, int,    \
+  template void launch_flight<R>(const FlightCtxT<R> &, const DevParticlesT<R> &, DevCount, unsigned int *, int, \
                                  cudaStream_t);                                                                 \
   template void launch_child_flight<R>(const FlightCtxT<R> &, const DevChildrenT<R> &, int, unsigned int *, int, \
                                        cudaStream_t);                                                           \
-  template void launch_child_keys<R>(const DevChildrenT<R> &, int, uint64_t *, uint8_t *, cudaStream_t);       \
-  template void launch_children_to_particles<R>(const DevChildrenT<R> &, int, const uint32_t *,               \
-                                                const uint8_t *, const DevParticlesT<R> &, int,                 \
-                                                unsigned int *, cudaStream_t);                                  \
-  template void launch_cell_sort<R>(const DevParticlesT<R> &, int, const DevParticlesT<R> &, int, int, int,    \
+  template void launch_append_children<R>(const ChildSetT<R> &, uint64_t *, uint8_t *, uint32_t *,             \
+                                          unsigned int *, const DevParticlesT<R> &, const unsigned int *, int,  \
+                                          unsigned int *, unsigned int *, int, cudaStream_t);                   \
+  template void launch_cell_sort<R>(const DevParticlesT<R> &, DevCount, const DevParticlesT<R> &, int, int, int, \
                                     unsigned int *, unsigned int *, unsigned int *, unsigned int *, int,        \
                                     cudaStream_t);
 MCB200_INSTANTIATE(double)

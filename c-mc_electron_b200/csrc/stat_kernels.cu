@@ -33,7 +33,9 @@ __device__ __forceinline__ void group_velocity(const DevTables &T, int itet, int
 }
 
 template <typename R>
-__global__ void statistic_kernel(DevParticlesT<R> P, int n, DevMesh M, DevTables T, StatScales S, StatBuffers B) {
+__global__ void statistic_kernel(DevParticlesT<R> P, DevCount count, DevMesh M, DevTables T, StatScales S,
+                                 StatBuffers B) {
+  const int n = count.get();
   const int px = M.nx + 1, pz = M.nz + 1;
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
     const uint32_t meta = P.meta[p];
@@ -86,17 +88,17 @@ __global__ void add_potential_kernel(int nodes, const double *pot, double *sum) 
 }
 
 template <typename R>
-void launch_statistic(const DevParticlesT<R> &P, int n, const DevMesh &M, const DevTables &T, const StatScales &S,
+void launch_statistic(const DevParticlesT<R> &P, DevCount n, const DevMesh &M, const DevTables &T, const StatScales &S,
                       const StatBuffers &B, int grid, cudaStream_t s) {
-  if (n > 0) statistic_kernel<R><<<grid, 256, 0, s>>>(P, n, M, T, S, B);
+  statistic_kernel<R><<<grid, 256, 0, s>>>(P, n, M, T, S, B);
 }
 void launch_add_potential(int nodes, const double *pot, double *sum, cudaStream_t s) {
   if (nodes > 0 && pot) add_potential_kernel<<<(nodes + 255) / 256, 256, 0, s>>>(nodes, pot, sum);
 }
 
-template void launch_statistic<double>(const DevParticlesT<double> &, int, const DevMesh &, const DevTables &,
+template void launch_statistic<double>(const DevParticlesT<double> &, DevCount, const DevMesh &, const DevTables &,
                                        const StatScales &, const StatBuffers &, int, cudaStream_t);
-template void launch_statistic<float>(const DevParticlesT<float> &, int, const DevMesh &, const DevTables &,
+template void launch_statistic<float>(const DevParticlesT<float> &, DevCount, const DevMesh &, const DevTables &,
                                       const StatScales &, const StatBuffers &, int, cudaStream_t);
 
 }  // namespace mcb200

@@ -21,7 +21,7 @@ struct StatBuffers {
 };
 
 template <typename R>
-void launch_statistic(const DevParticlesT<R> &P, int n, const DevMesh &M, const DevTables &T, const StatScales &S,
+void launch_statistic(const DevParticlesT<R> &P, DevCount n, const DevMesh &M, const DevTables &T, const StatScales &S,
                       const StatBuffers &B, int grid, cudaStream_t s);
 void launch_add_potential(int nodes, const double *pot, double *sum, cudaStream_t s);
 

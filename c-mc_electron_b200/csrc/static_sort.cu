@@ -82,7 +82,8 @@ extern "C" int mcb200_sort_particles_static(const mcb200_device_particles *in, s
   const int grid = (int)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, (size_t)sms * 8));
   // launch_cell_sort clears the histogram before counting; offsets, tile sums
   // and the total are fully overwritten by the scan.
-  launch_cell_sort(as_dev(*in), (int)n, as_dev(*out), (int)cells, nx, nz, hist, offsets, tiles, total, grid, st);
+  launch_cell_sort(as_dev(*in), DevCount{nullptr, nullptr, (int)n}, as_dev(*out), (int)cells, nx, nz, hist, offsets,
+                   tiles, total, grid, st);
   if (cudaGetLastError() != cudaSuccess) return MCB200_ERR_CUDA;
   if (n_out) {
     unsigned int kept = 0;

@@ -82,7 +82,7 @@ class RunOptions(ctypes.Structure):
                 ("poisson_every", ctypes.c_int), ("poisson_rel_tol", ctypes.c_double), ("max_steps", ctypes.c_int),
                 ("max_heat_steps", ctypes.c_int), ("write_outputs", ctypes.c_int), ("seed", ctypes.c_uint64),
                 ("verbose", ctypes.c_int), ("warmup_steps", ctypes.c_int), ("readback_every_step", ctypes.c_int),
-                ("flush_l2_bytes", ctypes.c_size_t)]
+                ("flush_l2_bytes", ctypes.c_size_t), ("profile_phases", ctypes.c_int)]
 
 
 class RunReport(ctypes.Structure):
@@ -117,6 +117,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mcb200_deposit.argtypes = [vp]
     lib.mcb200_solve_poisson.argtypes = [vp, c.c_double, c.c_int, c.POINTER(c.c_int), dp]
     lib.mcb200_set_poisson_solver.argtypes = [vp, c.c_int, c.c_int]
+    lib.mcb200_poisson_stats.argtypes = [vp, c.POINTER(c.c_int64), c.POINTER(c.c_int64), dp, c.c_int]
+    lib.mcb200_particle_steps.argtypes = [vp, c.POINTER(c.c_uint64)]
     lib.mcb200_get_poisson_solver.argtypes = [vp, c.POINTER(c.c_int), c.POINTER(c.c_int), c.POINTER(c.c_int)]
     lib.mcb200_get_array.argtypes = [vp, c.c_char_p, dp, c.c_size_t]
     lib.mcb200_surface_rates.argtypes = [vp, c.POINTER(SurfaceParams), i32p]
@@ -295,6 +297,23 @@ class Engine:
         self._check(self._lib.mcb200_solve_poisson(self._ctx, rel_tol, max_iter, ctypes.byref(it),
                                                    ctypes.byref(res)), "solve_poisson")
         return it.value, res.value
+
+    def solve_poisson_async(self, rel_tol=1e-10, max_iter=20000):
+        """A solve the host does not wait for (results in poisson_stats())."""
+        self._check(self._lib.mcb200_solve_poisson(self._ctx, rel_tol, max_iter, None, None), "solve_poisson")
+
+    def poisson_stats(self, reset=False):
+        """(solves, CG iterations, largest relative residual) since the last reset."""
+        n, it, res = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_double()
+        self._check(self._lib.mcb200_poisson_stats(self._ctx, ctypes.byref(n), ctypes.byref(it), ctypes.byref(res),
+                                                   1 if reset else 0), "poisson_stats")
+        return n.value, it.value, res.value
+
+    def particle_steps(self) -> int:
+        """Particle-steps flown since the context was created (device count)."""
+        v = ctypes.c_uint64()
+        self._check(self._lib.mcb200_particle_steps(self._ctx, ctypes.byref(v)), "particle_steps")
+        return v.value
 
     def set_potential(self, potential):
         """Node potential (normalised) and the cell fields derived from it."""
@@ -478,14 +497,16 @@ class Deck:
 def run_deck(input_path: str, device: int = 0, data_dir: str | None = None, precision: int = FLIGHT_FP64,
              max_steps: int = 0, max_heat_steps: int = -1, poisson_every: int = 0, seed: int = 1,
              write_outputs: bool = True, table_dir: str = DEFAULT_TABLE_DIR, verbose: bool = False,
-             warmup_steps: int = 0, readback_every_step: bool = False, flush_l2_bytes: int = 0) -> dict:
+             warmup_steps: int = 0, readback_every_step: bool = False, flush_l2_bytes: int = 0,
+             profile_phases: bool = False) -> dict:
     """The self-consistent simulation of a deck (mcb200_run_deck, the engine's
     `main input.txt`).  Returns the run report as a dict."""
     opt = RunOptions(table_dir=table_dir.encode(), data_dir=data_dir.encode() if data_dir else None,
                      flight_precision=precision, poisson_every=poisson_every, poisson_rel_tol=0.0,
                      max_steps=max_steps, max_heat_steps=max_heat_steps, write_outputs=int(write_outputs),
                      seed=seed, verbose=int(verbose), warmup_steps=warmup_steps,
-                     readback_every_step=int(readback_every_step), flush_l2_bytes=flush_l2_bytes)
+                     readback_every_step=int(readback_every_step), flush_l2_bytes=flush_l2_bytes,
+                     profile_phases=int(profile_phases))
     rep = RunReport()
     err = ctypes.create_string_buffer(1024)
     rc = lib().mcb200_run_deck(os.fspath(input_path).encode(), device, ctypes.byref(opt), ctypes.byref(rep), err,

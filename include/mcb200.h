@@ -147,6 +147,11 @@ int mcb200_deposit(mcb200_ctx *ctx);
  * geometric-multigrid V-cycle (the default) or Jacobi, selected with
  * mcb200_set_poisson_solver. */
 int mcb200_solve_poisson(mcb200_ctx *ctx, double rel_tol, int max_iter, int *iterations, double *rel_residual);
+/* With iterations and rel_residual both NULL, mcb200_solve_poisson does not
+ * wait for the GPU; every solve adds to statistics kept on the device:
+ * solves, CG iterations and the largest relative residual, read (and
+ * optionally reset) here. */
+int mcb200_poisson_stats(mcb200_ctx *ctx, int64_t *solves, int64_t *iterations, double *max_rel_residual, int reset);
 
 #define MCB200_POISSON_AUTO 0      /* multigrid when the mesh has a hierarchy, else Jacobi */
 #define MCB200_POISSON_JACOBI 1    /* Jacobi-preconditioned CG */
@@ -216,10 +221,15 @@ int mcb200_set_fields(mcb200_ctx *ctx, const double *efield_xyz, const double *h
 int mcb200_set_surface_rates(mcb200_ctx *ctx, const double *e_rough, const double *e_phonon,
                              const double *h_rough, const double *h_phonon);
 
-/* Particle store. */
+/* Particle store.  The particle count lives on the device (steps change it
+ * without the host waiting); mcb200_num_particles and mcb200_download_particles
+ * wait for the context's stream to read it. */
 int mcb200_upload_particles(mcb200_ctx *ctx, size_t n, const mcb200_particles *p);
 int mcb200_download_particles(mcb200_ctx *ctx, mcb200_particles *p, size_t capacity, size_t *n_out);
 size_t mcb200_num_particles(const mcb200_ctx *ctx);
+/* Particle-steps flown since the context was created (the particle count at
+ * the start of every step, summed on the device); waits for the stream. */
+int mcb200_particle_steps(mcb200_ctx *ctx, uint64_t *total);
 
 /* Append n particles of carrier `type` (0 electron, 1 hole) sampled on the
  * GPU the way the reference initialises them: cell_of[q] is the cell of new
@@ -236,10 +246,14 @@ int mcb200_seed_particles(mcb200_ctx *ctx, size_t n, const int32_t *cell_of, con
  * loop on its own random stream (seed, uid, step), copies made by
  * GENERATE / GENREF finish the step, caught particles are removed, copies
  * join with fresh uids, and the store is counting-sorted by cell.
- * Asynchronous on the context's stream; tallies accumulate. */
+ * Asynchronous on the context's stream (the host never waits inside it);
+ * tallies accumulate.  A store that fills up with copies drops the excess
+ * and the next call that reads the count (mcb200_sync, mcb200_get_tallies,
+ * mcb200_download_particles, the next mcb200_step) returns
+ * MCB200_ERR_CAPACITY. */
 int mcb200_step(mcb200_ctx *ctx, uint32_t step, uint64_t seed, double dt);
 
-/* Wait for the context's stream. */
+/* Wait for the context's stream (and report a full store, as above). */
 int mcb200_sync(mcb200_ctx *ctx);
 
 /* Device timing of mcb200_step with CUDA events on the context's own stream
@@ -410,6 +424,9 @@ typedef struct {
   int warmup_steps;          /* transport steps run before the timed ones (counted in max_steps) */
   int readback_every_step;   /* read the tallies back to the host after every step */
   size_t flush_l2_bytes;     /* >0: before every timed step write this many bytes (L2 eviction), timed apart */
+  int profile_phases;        /* wait for the GPU after every phase so that report->phase_s holds the
+                                device-side time per phase (slows the run; 0: phases are only enqueued
+                                and phase_s is host enqueue time) */
 } mcb200_run_options;
 
 typedef struct {
@@ -424,7 +441,8 @@ typedef struct {
   double last_current[1];         /* drain current (A/cm) of the last window */
   double heat_total;              /* sum of the heat tallies over the heat windows (kT x charge) */
   double phase_s[8];              /* host wall time per phase: statistics, deposition, Poisson + fields,
-                                     surface rates, carrier step, refresh, outputs, (unused) */
+                                     surface rates, carrier step, refresh, outputs, (unused); see
+                                     profile_phases */
   /* the timed transport steps (after warmup_steps): device time between
      CUDA events on the context's stream, host wall time, particles flown */
   double timed_device_ms, timed_wall_s;
