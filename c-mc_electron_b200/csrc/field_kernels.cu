@@ -20,6 +20,7 @@
 #include "device_state.cuh"
 #include "field_kernels.h"
 #include "poisson_common.cuh"
+#include "warp_segments.cuh"
 
 namespace mcb200 {
 
@@ -31,8 +32,11 @@ constexpr uint32_t kDeadBit = 1u << 16;
 // like the value for non-negative doubles) and the particle count.  count x
 // max |q| bounds every cell or node sum of that type, exactly and
 // independently of thread order.  out = {max_e bits, max_h bits, n_e, n_h}.
-__global__ void charge_bounds_kernel(const double *charge, const uint32_t *meta, DevCount count,
-                                     unsigned long long *out) {
+// Warp shuffles, then one shared-memory pass per block, then one atomic
+// per block and value.
+__global__ void __launch_bounds__(256) charge_bounds_kernel(const double *charge, const uint32_t *meta,
+                                                            DevCount count, unsigned long long *out) {
+  __shared__ unsigned long long red[4][8];
   const int n = count.get();
   unsigned long long mx[2] = {0, 0}, cnt[2] = {0, 0};
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
@@ -43,21 +47,29 @@ __global__ void charge_bounds_kernel(const double *charge, const uint32_t *meta,
     mx[t] = b > mx[t] ? b : mx[t];
     cnt[t] += 1;
   }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int t = 0; t < 2; ++t) {
     for (int o = 16; o > 0; o >>= 1) {
       const unsigned long long om = __shfl_down_sync(0xffffffffu, mx[t], o);
       mx[t] = om > mx[t] ? om : mx[t];
       cnt[t] += __shfl_down_sync(0xffffffffu, cnt[t], o);
     }
-    if ((threadIdx.x & 31) == 0) {
-      atomicMax(out + t, mx[t]);
-      atomicAdd(out + 2 + t, cnt[t]);
+    if (lane == 0) {
+      red[t][warp] = mx[t];
+      red[2 + t][warp] = cnt[t];
     }
   }
-}
-
-__device__ __forceinline__ void fx_add(long long *p, double v, double scale) {
-  atomicAdd(reinterpret_cast<unsigned long long *>(p), (unsigned long long)__double2ll_rn(v * scale));
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    const int v = threadIdx.x;
+    unsigned long long a = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) a = v < 2 ? (red[v][w] > a ? red[v][w] : a) : a + red[v][w];
+    if (v < 2) {
+      if (a) atomicMax(out + v, a);
+    } else if (a) {
+      atomicAdd(out + v, a);
+    }
+  }
 }
 
 // Fixed-point units from the bounds of charge_bounds_kernel: a sum whose
@@ -78,43 +90,73 @@ __global__ void deposit_scales_kernel(const unsigned long long *b, DepositScales
   out->s[2] = fixed_unit(be + bh);
 }
 
+__device__ __forceinline__ long long fx(double v, double scale) { return __double2ll_rn(v * scale); }
+__device__ __forceinline__ void fx_put(long long *p, long long v) {
+  atomicAdd(reinterpret_cast<unsigned long long *>(p), (unsigned long long)v);
+}
+
 // scale[0]: electron cell sums, [1]: hole cell sums, [2]: |q| and node sums.
+// Lanes of a warp walk consecutive particles; runs of particles of the same
+// cell and carrier type add their fixed-point terms before one atomic each.
 template <typename R>
-__global__ void deposit_kernel(DevParticlesT<R> P, DevCount count, DevMesh M, const DepositScales *Sp,
-                               long long *cell_e, long long *cell_h, long long *cell_abs, long long *node_q) {
+__global__ void __launch_bounds__(256) deposit_kernel(DevParticlesT<R> P, DevCount count, DevMesh M,
+                                                      const DepositScales *Sp, long long *cell_e, long long *cell_h,
+                                                      long long *cell_abs, long long *node_q) {
   const int n = count.get();
   const DepositScales S = *Sp;
   const int px = M.nx + 1, pz = M.nz + 1;
   const double scale = S.s[2];
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
-    const uint32_t meta = P.meta[p];
-    if (meta & kDeadBit) continue;
-    const uint32_t c = P.cell[p];
+  const unsigned lane = threadIdx.x & 31u;
+  for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += gridDim.x * blockDim.x) {
+    const int p = base + (int)lane;
+    const uint32_t meta = p < n ? P.meta[p] : kDeadBit;
+    const bool live = !(meta & kDeadBit);
+    const uint32_t c = live ? P.cell[p] : 0u;
+    const int type = ((meta >> 8) & 255) == 0 ? 0 : 1;
+    const WarpRuns runs(live ? (c | ((unsigned)type << 30)) : 0xffffffffu);
     const int i = c & 1023, j = (c >> 10) & 1023, k = (c >> 20) & 1023;
-    const int cell = (j * M.nx + i) * M.nz + k;
-    const double cc = P.charge[p];
-    if (((meta >> 8) & 255) == 0) fx_add(cell_e + cell, cc, S.s[0]);
-    else fx_add(cell_h + cell, cc, S.s[1]);
-    fx_add(cell_abs + cell, fabs(cc), scale);
-    double rx, ry, rz;
-    if constexpr (sizeof(R) == 4) {  // FP32 store: positions relative to the cell's low corner
-      rx = (double)P.x[p] / M.dx[i];
-      ry = (double)P.y[p] / M.dy[j];
-      rz = (double)P.z[p] / M.dz[k];
-    } else {
-      rx = (P.x[p] - M.lx[i]) / M.dx[i];
-      ry = (P.y[p] - M.ly[j]) / M.dy[j];
-      rz = (P.z[p] - M.lz[k]) / M.dz[k];
+    long long vc = 0, va = 0, vn[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (live) {
+      const double cc = P.charge[p];
+      vc = fx(cc, type == 0 ? S.s[0] : S.s[1]);
+      va = fx(fabs(cc), scale);
+      double rx, ry, rz;
+      if constexpr (sizeof(R) == 4) {  // FP32 store: positions relative to the cell's low corner
+        rx = (double)P.x[p] / M.dx[i];
+        ry = (double)P.y[p] / M.dy[j];
+        rz = (double)P.z[p] / M.dz[k];
+      } else {
+        rx = (P.x[p] - M.lx[i]) / M.dx[i];
+        ry = (P.y[p] - M.ly[j]) / M.dy[j];
+        rz = (P.z[p] - M.lz[k]) / M.dz[k];
+      }
+      vn[0] = fx(cc * (1 - ry) * (1 - rx) * (1 - rz), scale);
+      vn[1] = fx(cc * (1 - ry) * rx * (1 - rz), scale);
+      vn[2] = fx(cc * (1 - ry) * (1 - rx) * rz, scale);
+      vn[3] = fx(cc * (1 - ry) * rx * rz, scale);
+      vn[4] = fx(cc * ry * (1 - rx) * (1 - rz), scale);
+      vn[5] = fx(cc * ry * rx * (1 - rz), scale);
+      vn[6] = fx(cc * ry * (1 - rx) * rz, scale);
+      vn[7] = fx(cc * ry * rx * rz, scale);
     }
-    auto node = [&](int a, int b, int d) { return node_q + ((size_t)b * px + a) * pz + d; };
-    fx_add(node(i, j, k), cc * (1 - ry) * (1 - rx) * (1 - rz), scale);
-    fx_add(node(i + 1, j, k), cc * (1 - ry) * rx * (1 - rz), scale);
-    fx_add(node(i, j, k + 1), cc * (1 - ry) * (1 - rx) * rz, scale);
-    fx_add(node(i + 1, j, k + 1), cc * (1 - ry) * rx * rz, scale);
-    fx_add(node(i, j + 1, k), cc * ry * (1 - rx) * (1 - rz), scale);
-    fx_add(node(i + 1, j + 1, k), cc * ry * rx * (1 - rz), scale);
-    fx_add(node(i, j + 1, k + 1), cc * ry * (1 - rx) * rz, scale);
-    fx_add(node(i + 1, j + 1, k + 1), cc * ry * rx * rz, scale);
+    const long long sc = runs.sum(vc), sa = runs.sum(va);
+    long long sn[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) sn[q] = runs.sum(vn[q]);
+    if (live && runs.tail) {
+      const int cell = (j * M.nx + i) * M.nz + k;
+      fx_put((type == 0 ? cell_e : cell_h) + cell, sc);
+      fx_put(cell_abs + cell, sa);
+      auto node = [&](int a, int b, int d) { return node_q + ((size_t)b * px + a) * pz + d; };
+      fx_put(node(i, j, k), sn[0]);
+      fx_put(node(i + 1, j, k), sn[1]);
+      fx_put(node(i, j, k + 1), sn[2]);
+      fx_put(node(i + 1, j, k + 1), sn[3]);
+      fx_put(node(i, j + 1, k), sn[4]);
+      fx_put(node(i + 1, j + 1, k), sn[5]);
+      fx_put(node(i, j + 1, k + 1), sn[6]);
+      fx_put(node(i + 1, j + 1, k + 1), sn[7]);
+    }
   }
 }
 

@@ -11,13 +11,15 @@
 // largest group-velocity component of the band tables, |E| <= the energy
 // table's top.
 #include "stat_kernels.h"
+#include "warp_segments.cuh"
 
 namespace mcb200 {
 
 constexpr uint32_t kStatDead = 1u << 16;
 
-__device__ __forceinline__ void st_add(long long *p, double v, double scale) {
-  atomicAdd(reinterpret_cast<unsigned long long *>(p), (unsigned long long)__double2ll_rn(v * scale));
+__device__ __forceinline__ long long st_fx(double v, double scale) { return __double2ll_rn(v * scale); }
+__device__ __forceinline__ void st_put(long long *p, long long v) {
+  atomicAdd(reinterpret_cast<unsigned long long *>(p), (unsigned long long)v);
 }
 
 // GetV (src/ParticleUtils.cpp:307-313) from the FP64 tables: the wedge
@@ -32,41 +34,58 @@ __device__ __forceinline__ void group_velocity(const DevTables &T, int itet, int
   vz = (p2 == 0 ? v[0] : (p2 == 1 ? v[1] : v[2])) * (double)m[5];
 }
 
+// Lanes of a warp walk consecutive particles of the cell-sorted store; runs
+// of particles of the same cell and carrier type add their fixed-point
+// terms with shuffles before one atomic per run (warp_segments.cuh).
 template <typename R>
-__global__ void statistic_kernel(DevParticlesT<R> P, DevCount count, DevMesh M, DevTables T, StatScales S,
-                                 StatBuffers B) {
+__global__ void __launch_bounds__(256) statistic_kernel(DevParticlesT<R> P, DevCount count, DevMesh M, DevTables T,
+                                                        StatScales S, StatBuffers B) {
   const int n = count.get();
   const int px = M.nx + 1, pz = M.nz + 1;
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
-    const uint32_t meta = P.meta[p];
-    if (meta & kStatDead) continue;
-    const uint32_t c = P.cell[p];
-    const int i = c & 1023, j = (c >> 10) & 1023, k = (c >> 20) & 1023;
-    atomicAdd(B.cell_count + (j * M.nx + i) * M.nz + k, 1ull);
+  const unsigned lane = threadIdx.x & 31u;
+  for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += gridDim.x * blockDim.x) {
+    const int p = base + (int)lane;
+    const uint32_t meta = p < n ? P.meta[p] : kStatDead;
+    const bool live = !(meta & kStatDead);
+    const uint32_t c = live ? P.cell[p] : 0u;
     const int type = ((meta >> 8) & 255) == 0 ? 0 : 1;
-    double vx, vy, vz;
-    group_velocity(T, P.itet[p], meta & 255, vx, vy, vz);
-    double rx, ry, rz;
-    if constexpr (sizeof(R) == 4) {
-      rx = (double)P.x[p] / M.dx[i];
-      ry = (double)P.y[p] / M.dy[j];
-      rz = (double)P.z[p] / M.dz[k];
-    } else {
-      rx = (P.x[p] - M.lx[i]) / M.dx[i];
-      ry = (P.y[p] - M.ly[j]) / M.dy[j];
-      rz = (P.z[p] - M.lz[k]) / M.dz[k];
+    const WarpRuns runs(live ? (c | ((unsigned)type << 30)) : 0xffffffffu);
+    const int i = c & 1023, j = (c >> 10) & 1023, k = (c >> 20) & 1023;
+    double vx = 0, vy = 0, vz = 0, rx = 0, ry = 0, rz = 0, q = 0, e = 0;
+    if (live) {
+      group_velocity(T, P.itet[p], meta & 255, vx, vy, vz);
+      if constexpr (sizeof(R) == 4) {
+        rx = (double)P.x[p] / M.dx[i];
+        ry = (double)P.y[p] / M.dy[j];
+        rz = (double)P.z[p] / M.dz[k];
+      } else {
+        rx = (P.x[p] - M.lx[i]) / M.dx[i];
+        ry = (P.y[p] - M.ly[j]) / M.dy[j];
+        rz = (P.z[p] - M.lz[k]) / M.dz[k];
+      }
+      q = P.charge[p];
+      e = P.energy[p];
     }
-    const double q = P.charge[p], e = P.energy[p];
-    long long *base = B.node + (size_t)type * 5 * B.nodes;
-    const double sq = S.q[type], sv = S.v[type], se = S.e[type];
+    const long long cnt = runs.sum(live ? 1 : 0);
+    if (live && runs.tail)
+      atomicAdd(B.cell_count + (j * M.nx + i) * M.nz + k, (unsigned long long)cnt);
+    long long *basep = B.node + (size_t)type * 5 * B.nodes;
+    const double sq = type ? S.q[1] : S.q[0], sv = type ? S.v[1] : S.v[0], se = type ? S.e[1] : S.e[0];
     auto put = [&](int a, int b, int d, double w) {
-      const size_t node = ((size_t)b * px + a) * pz + d;
       const double aq = fabs(q * w);
-      st_add(base + 0 * (size_t)B.nodes + node, vx * aq, sv);
-      st_add(base + 1 * (size_t)B.nodes + node, vy * aq, sv);
-      st_add(base + 2 * (size_t)B.nodes + node, vz * aq, sv);
-      st_add(base + 3 * (size_t)B.nodes + node, aq, sq);
-      st_add(base + 4 * (size_t)B.nodes + node, aq * e, se);
+      const long long t0 = runs.sum(live ? st_fx(vx * aq, sv) : 0);
+      const long long t1 = runs.sum(live ? st_fx(vy * aq, sv) : 0);
+      const long long t2 = runs.sum(live ? st_fx(vz * aq, sv) : 0);
+      const long long t3 = runs.sum(live ? st_fx(aq, sq) : 0);
+      const long long t4 = runs.sum(live ? st_fx(aq * e, se) : 0);
+      if (live && runs.tail) {
+        const size_t node = ((size_t)b * px + a) * pz + d;
+        st_put(basep + 0 * (size_t)B.nodes + node, t0);
+        st_put(basep + 1 * (size_t)B.nodes + node, t1);
+        st_put(basep + 2 * (size_t)B.nodes + node, t2);
+        st_put(basep + 3 * (size_t)B.nodes + node, t3);
+        st_put(basep + 4 * (size_t)B.nodes + node, t4);
+      }
     };
     // the eight corners in the reference's order and weights
     put(i, j, k, (1 - rx) * (1 - ry) * (1 - rz));
