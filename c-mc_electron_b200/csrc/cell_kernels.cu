@@ -26,6 +26,13 @@ __global__ void surface_rates_kernel(int cells, SurfaceRateParams q, const doubl
   const double Rho = rho[c];
   double Eeff = fabs(field[3 * (size_t)c + min(max(eeff_dir[c], 0), 2)]);
   if (Eeff < 1e-20) Eeff = 1e-20;
+  // the per-cell powers, shared by both carrier types; the constant ones come from the host
+  double e_third = 0, Pf = 0, Wcl = 0;
+  if (q.phonon) {
+    e_third = pow(Eeff, -1.0 / 3.0);
+    Pf = q.pft * q.Tn + q.pfn * pow(Rho * q.conc0 / (1e17 * 1e6), q.npf) / q.Tn;
+    Wcl = q.tn_nbmod * q.boltz * q.T0 / (Eeff * q.field0);
+  }
   for (int t = 0; t < 2; ++t) {
     const double effmass = t == 0 ? 0.286 : 0.8;  // MASSeff, src/Constant_GlobalVariable_MathFunction.cpp:28
     double rough = 0, phon = 0;
@@ -34,13 +41,11 @@ __global__ void surface_rates_kernel(int cells, SurfaceRateParams q, const doubl
       rough = 2 * kPiC * effmass * (a * a);
     }
     if (q.phonon) {
-      const double Wcl = pow(q.Tn, q.nbmod) * q.boltz * q.T0 / (Eeff * q.field0);
-      const double Wq = pow(12.0 * effmass * q.em0 * (Eeff * q.field0) / q.ec0 / q.hq0 / q.hq0, -1.0 / 3.0);
-      const double Pf = q.pft * q.Tn + q.pfn * pow(Rho * q.conc0 / (1e17 * 1e6), q.npf) / q.Tn;
+      const double Wq = q.wq_c[t] * e_third;
       const double Wclq = (q.gama * Wcl + q.theta * Wq) / Pf;
       phon = effmass * q.em0 * q.boltz * q.T0 * q.xiph * q.xiph /
                  (q.hq0 * q.hq0 * q.hq0 * q.sirho * (9050.02 * 9050.02) * Wclq) / q.scrt0 +
-             q.ec0 / (effmass * q.em0 * q.kpha * pow(q.Tn, 2.24)) / q.scrt0;
+             q.ec0 / (effmass * q.em0 * q.kpha * q.tn_224) / q.scrt0;
     }
     if (t == 0) { e_rough[c] = rough; e_phon[c] = phon; }
     else { h_rough[c] = rough; h_phon[c] = phon; }

@@ -18,6 +18,9 @@ struct SurfaceRateParams {
   double delta, ail, xiph, theta, gama, nbmod, npf, pft, pfn, kpha;
   int roughness, phonon;
   double eps_si, eps_ox, Tn, T0, boltz, field0, em0, ec0, hq0, conc0, sirho, scrt0;
+  // derived on the host: Tn^nbmod, Tn^2.24 and, per carrier type,
+  // (12 m* em0 field0 / ec0 / hq0^2)^(-1/3) (the field-independent factor of Wq)
+  double tn_nbmod, tn_224, wq_c[2];
 };
 
 struct RefreshParams {

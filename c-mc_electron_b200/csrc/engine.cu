@@ -1353,6 +1353,12 @@ int mcb200_surface_rates(mcb200_ctx *c, const mcb200_surface_params *p, const in
     q.eps_si = u.eps_silicon; q.eps_ox = u.eps_oxide; q.Tn = u.Tn; q.T0 = u.T0; q.boltz = 8.617343e-5;
     q.field0 = u.field0; q.em0 = u.em0; q.ec0 = u.ec0; q.hq0 = u.hq0; q.conc0 = u.conc0; q.sirho = u.sirho;
     q.scrt0 = u.scrt0;
+    q.tn_nbmod = std::pow(q.Tn, q.nbmod);
+    q.tn_224 = std::pow(q.Tn, 2.24);
+    for (int t = 0; t < 2; ++t) {
+      const double effmass = t == 0 ? 0.286 : 0.8;
+      q.wq_c[t] = std::pow(12.0 * effmass * q.em0 * q.field0 / q.ec0 / q.hq0 / q.hq0, -1.0 / 3.0);
+    }
     // the direction array stays on the device; it is uploaded when it changes
     if (c->eeff_host.size() != (size_t)c->ncells ||
         std::memcmp(c->eeff_host.data(), eeff_direction, sizeof(int) * c->ncells) != 0) {

@@ -115,14 +115,17 @@ struct SymSmemT {
 using SymSmem = SymSmemT<double>;
 
 template <typename R>
-struct FlightCtxT {
-  DevTables T;
+struct FlightInstT {  // one simulation: its mesh and fields, tallies, copy buffer and step
   DevMesh M;
   DevTallies Y;
   DevChildrenT<R> C;
   double dt;
   uint64_t seed;
   uint32_t step;
+};
+template <typename R>
+struct FlightCtxT : FlightInstT<R> {  // plus the band tables, shared by every simulation
+  DevTables T;
 };
 using FlightCtx = FlightCtxT<double>;
 
@@ -136,8 +139,9 @@ struct FlyerT {
   using Real = FlightReal<R>;
   using V4 = typename Real::V4;
   using TB = Tab<R>;
-  const FlightCtxT<R> &F;
+  const FlightCtxT<R> &F;      // the tables (F.T)
   const SymSmemT<R> &S;
+  const FlightInstT<R> *I;     // the simulation of the current particle (F itself unless batched)
   // random stream and the cached Philox block (index rblk, words rw0..rw3)
   uint32_t uid, sub, n;
   uint32_t rblk, rw0, rw1, rw2, rw3;
@@ -165,7 +169,7 @@ struct FlyerT {
   enum : int { kFsNone = 0, kFsPhonon = 1, kFsIonize = 2, kFsDiffuse = 3 };
   enum : int { kLocNone = 0, kLocBZ = 1, kLocImpurity = 2 };
 
-  __device__ FlyerT(const FlightCtxT<R> &f, const SymSmemT<R> &s) : F(f), S(s) {}
+  __device__ FlyerT(const FlightCtxT<R> &f, const SymSmemT<R> &s) : F(f), S(s), I(&f) {}
 
   __device__ __forceinline__ void start_stream(uint32_t u, uint32_t sb) {
     uid = u;
@@ -186,7 +190,7 @@ struct FlyerT {
         u = mcb200_bits_to_unit(rw3, rw2);
       } else {
         const mcb200_philox_block w =
-            mcb200_philox4x32_10(b, uid, F.step, sub, (uint32_t)F.seed, (uint32_t)(F.seed >> 32));
+            mcb200_philox4x32_10(b, uid, I->step, sub, (uint32_t)I->seed, (uint32_t)(I->seed >> 32));
         rblk = b;
         rw2 = w.w[2];
         rw3 = w.w[3];
@@ -198,7 +202,7 @@ struct FlyerT {
       const uint32_t b = n >> 2;
       if (b != rblk) {
         const mcb200_philox_block w =
-            mcb200_philox4x32_10(b, uid, F.step, sub, (uint32_t)F.seed, (uint32_t)(F.seed >> 32));
+            mcb200_philox4x32_10(b, uid, I->step, sub, (uint32_t)I->seed, (uint32_t)(I->seed >> 32));
         rblk = b;
         rw0 = w.w[0];
         rw1 = w.w[1];
@@ -213,8 +217,8 @@ struct FlyerT {
   }
 
   __device__ __forceinline__ int ms(int c, int s) const { return S.symi[s * 6 + c]; }
-  __device__ __forceinline__ int cell_index() const { return (jc * F.M.nx + ic) * F.M.nz + kc; }
-  __device__ __forceinline__ int cell_index(int i, int j, int k) const { return (j * F.M.nx + i) * F.M.nz + k; }
+  __device__ __forceinline__ int cell_index() const { return (jc * I->M.nx + ic) * I->M.nz + kc; }
+  __device__ __forceinline__ int cell_index(int i, int j, int k) const { return (j * I->M.nx + i) * I->M.nz + k; }
   __device__ __forceinline__ const TetFlightT<R> &tf(int it) const { return TB::tf(F.T)[it]; }
   __device__ __forceinline__ const TetShapeT<R> &ts(int it) const { return TB::ts(F.T)[it]; }
 
@@ -291,7 +295,7 @@ struct FlyerT {
   // positions are offsets from the cell's low corner, so the gaps are
   // (width - x) and x.
   __device__ R CellTime() {
-    const DevMesh &M = F.M;
+    const DevMesh &M = I->M;
     int idx, idy, idz;
     R tx, ty, tz;
     if constexpr (Real::kCellRelative) {
@@ -388,7 +392,7 @@ struct FlyerT {
       sx = kx < 0 ? 0 : 2; sy = ky < 0 ? 0 : 2; sz = kz < 0 ? 0 : 2;
     }
     if (sx < 0 || sx > 2 || sy < 0 || sy > 2 || sz < 0 || sz > 2) {  // a zero component: sign() is NaN in the reference
-      count(F.Y, kCntNoTet);
+      count(I->Y, kCntNoTet);
       catch_ = true;
       return;
     }
@@ -429,7 +433,7 @@ struct FlyerT {
         return;
       }
     }
-    count(F.Y, kCntNoTet);
+    count(I->Y, kCntNoTet);
     catch_ = true;
   }
 
@@ -626,7 +630,7 @@ struct FlyerT {
 
   // heat_to_point, src/heat.cpp:169-196 (CIC onto the cell's 8 nodes).
   __device__ void heat_to_point(double e, long long *heat) const {
-    const DevMesh &M = F.M;
+    const DevMesh &M = I->M;
     R rx, ry, rz;
     if constexpr (Real::kCellRelative) {
       rx = x / M.dxf[ic];
@@ -765,8 +769,8 @@ struct FlyerT {
       energy = fs_eeold;
       restore_k();
     }
-    if (kind == kFsPhonon && F.M.heat)
-      heat_to_point((energy - fs_eeold) * fabs(charge), type == 0 ? F.Y.heat_e : F.Y.heat_h);
+    if (kind == kFsPhonon && I->M.heat)
+      heat_to_point((energy - fs_eeold) * fabs(charge), type == 0 ? I->Y.heat_e : I->Y.heat_h);
   }
 
   // ElectronPhononScatter (src/ElectronPhononScatter.cpp:5-95) and
@@ -807,7 +811,7 @@ struct FlyerT {
       const DevTables &T = F.T;
       if ((eel * T.eV0 < 0.120) && (DA * T.conc0 >= 1e22)) {
         const double eebeta = T.frickel * 4 * kPiD * Rho / (2.0 * T.meld * T.eps_si);
-        if (F.M.surface_scatter && F.M.surface_impurity && F.M.in_surf[cell_index()]) {
+        if (I->M.surface_scatter && I->M.surface_impurity && I->M.in_surf[cell_index()]) {
           // The reference's surface-impurity formula is commented out there and
           // leaves the rate unset; the engine treats it as zero.
           return 0.0;
@@ -852,8 +856,8 @@ struct FlyerT {
   // GetSurfScRate, src/ParSurfaceScatter.cpp:3-45.
   __device__ void GetSurfScRate() {
     const int c = cell_index();
-    if (type == 0) { rough_rate = (R)F.M.e_rough[c]; sphon_rate = (R)F.M.e_sphon[c]; }
-    else { rough_rate = (R)F.M.h_rough[c]; sphon_rate = (R)F.M.h_sphon[c]; }
+    if (type == 0) { rough_rate = (R)I->M.e_rough[c]; sphon_rate = (R)I->M.e_sphon[c]; }
+    else { rough_rate = (R)I->M.h_rough[c]; sphon_rate = (R)I->M.h_sphon[c]; }
     surf_gamma = rough_rate + sphon_rate;
   }
 
@@ -870,7 +874,7 @@ struct FlyerT {
     else if (idir == kFront || idir == kBack) reflect_axis(2);
   }
   __device__ bool inside_mesh(int i, int j, int k) const {
-    return i >= 0 && j >= 0 && k >= 0 && i < F.M.nx && j < F.M.ny && k < F.M.nz;
+    return i >= 0 && j >= 0 && k >= 0 && i < I->M.nx && j < I->M.ny && k < I->M.nz;
   }
   // Pass, src/CellHit.cpp:389-413.  A PASS rule on the outer x / z boundary
   // would move the particle off the mesh (the reference indexes out of its
@@ -879,11 +883,11 @@ struct FlyerT {
     int ni, nj, nk;
     neighbour(ni, nj, nk);
     if (!inside_mesh(ni, nj, nk)) {
-      count(F.Y, kCntUnfinished);
+      count(I->Y, kCntUnfinished);
       catch_ = true;
       return;
     }
-    const DevMesh &M = F.M;
+    const DevMesh &M = I->M;
     if constexpr (Real::kCellRelative) {  // the face, in the new cell's frame
       switch (idir) {
         case kUp: x = M.dxf[ic - 1]; ic--; break;
@@ -891,11 +895,11 @@ struct FlyerT {
         case kRight:
           y = 0;
           jc++;
-          tally_add_i64(F.Y.rcurrent + jc, charge, kChargeScale);
+          tally_add_i64(I->Y.rcurrent + jc, charge, kChargeScale);
           break;
         case kLeft:
           y = M.dyf[jc - 1];
-          tally_add_i64(F.Y.lcurrent + jc, charge, kChargeScale);
+          tally_add_i64(I->Y.lcurrent + jc, charge, kChargeScale);
           jc--;
           break;
         case kFront: z = M.dzf[kc - 1]; kc--; break;
@@ -908,11 +912,11 @@ struct FlyerT {
         case kRight:
           y = M.ly[jc + 1];
           jc++;
-          tally_add_i64(F.Y.rcurrent + jc, charge, kChargeScale);
+          tally_add_i64(I->Y.rcurrent + jc, charge, kChargeScale);
           break;
         case kLeft:
           y = M.ly[jc];
-          tally_add_i64(F.Y.lcurrent + jc, charge, kChargeScale);
+          tally_add_i64(I->Y.lcurrent + jc, charge, kChargeScale);
           jc--;
           break;
         case kFront: z = M.lz[kc]; kc--; break;
@@ -922,7 +926,7 @@ struct FlyerT {
   }
   // Period, src/CellHit.cpp:416-432.
   __device__ void Period() {
-    const DevMesh &M = F.M;
+    const DevMesh &M = I->M;
     if constexpr (Real::kCellRelative) {
       if (idir == kUp) x = M.dxf[ic];
       else if (idir == kDown) x = 0;
@@ -952,36 +956,36 @@ struct FlyerT {
   }
   __device__ void contact_add(int icont, int slot, double v, double scale) const {
     if (icont < 0 || icont >= kMaxContacts) return;
-    tally_add_i64(F.Y.contact + icont * 6 + slot, v, scale);
+    tally_add_i64(I->Y.contact + icont * 6 + slot, v, scale);
   }
   // Generate, src/CellHit.cpp:435-501: tally, then a copy of the particle
   // enters the neighbour cell and finishes the step there.
   __device__ void Generate() {
-    count(F.Y, kCntGenerated);
-    const int icont = F.M.contact[cell_index()] - 1;
+    count(I->Y, kCntGenerated);
+    const int icont = I->M.contact[cell_index()] - 1;
     if (icont >= 0) {
-      atomicAdd(reinterpret_cast<unsigned long long *>(F.Y.contact + icont * 6 + 0), 1ull);
+      atomicAdd(reinterpret_cast<unsigned long long *>(I->Y.contact + icont * 6 + 0), 1ull);
       contact_add(icont, 1, charge, kChargeScale);
       contact_add(icont, 2, energy, kEnergyScale);
     }
-    if (idir == kRight) tally_add_i64(F.Y.rcurrent + jc + 1, charge, kChargeScale);
-    if (idir == kLeft) tally_add_i64(F.Y.lcurrent + jc, charge, kChargeScale);
+    if (idir == kRight) tally_add_i64(I->Y.rcurrent + jc + 1, charge, kChargeScale);
+    if (idir == kLeft) tally_add_i64(I->Y.lcurrent + jc, charge, kChargeScale);
     int i, j, k;
     neighbour(i, j, k);
     if (!inside_mesh(i, j, k)) {
-      count(F.Y, kCntUnfinished);
+      count(I->Y, kCntUnfinished);
       return;
     }
-    const DevChildrenT<R> &C = F.C;
+    const DevChildrenT<R> &C = I->C;
     const unsigned slot = atomicAdd(C.count, 1u);
     const uint32_t csub = sub * 16u + 1u + (uint32_t)nchild++;
     if ((int)slot >= C.capacity) {
-      count(F.Y, kCntChildOverflow);
+      count(I->Y, kCntChildOverflow);
       return;
     }
     R cx = x, cy = y, cz = z;
     if constexpr (Real::kCellRelative) {  // the same point in the neighbour cell's frame
-      const DevMesh &M = F.M;
+      const DevMesh &M = I->M;
       switch (idir) {
         case kUp: cx = x + M.dxf[i]; break;
         case kDown: cx = x - M.dxf[ic]; break;
@@ -1004,20 +1008,20 @@ struct FlyerT {
   __device__ void Catch(bool with_current) {
     int i, j, k;
     neighbour(i, j, k);
-    const int icont = inside_mesh(i, j, k) ? F.M.contact[cell_index(i, j, k)] - 1 : -1;
+    const int icont = inside_mesh(i, j, k) ? I->M.contact[cell_index(i, j, k)] - 1 : -1;
     if (with_current) {
-      if (idir == kRight) tally_add_i64(F.Y.rcurrent + jc + 1, charge, kChargeScale);
-      if (idir == kLeft) tally_add_i64(F.Y.lcurrent + jc, charge, kChargeScale);
+      if (idir == kRight) tally_add_i64(I->Y.rcurrent + jc + 1, charge, kChargeScale);
+      if (idir == kLeft) tally_add_i64(I->Y.lcurrent + jc, charge, kChargeScale);
     }
     if (icont >= 0 && icont < kMaxContacts) {
-      atomicAdd(reinterpret_cast<unsigned long long *>(F.Y.contact + icont * 6 + 3), 1ull);
+      atomicAdd(reinterpret_cast<unsigned long long *>(I->Y.contact + icont * 6 + 3), 1ull);
       contact_add(icont, 4, charge, kChargeScale);
       contact_add(icont, 2, energy, kEnergyScale);  // the reference adds to EnergyGen here (src/CellHit.cpp:542)
     }
   }
   __device__ void load_cell_fields() {
     const int c = cell_index();
-    const DevMesh &M = F.M;
+    const DevMesh &M = I->M;
     if constexpr (sizeof(R) == 8) {
       const double *f = (type == 0 ? M.efield : M.hfield) + 3 * (size_t)c;
       Ex = f[0];
@@ -1044,14 +1048,14 @@ struct FlyerT {
   // HitCell, src/CellHit.cpp:96-211.  Returns false when the particle would
   // leave the device through a PASS / GENERATE face on the outer y boundary.
   __device__ bool HitCell() {
-    const int imot = F.M.motion[(size_t)cell_index() * 6 + idir];
+    const int imot = I->M.motion[(size_t)cell_index() * 6 + idir];
     if (imot == kPass || imot == kGenerate || imot == kGenRef) {
-      if ((idir == kLeft && jc == 0) || (idir == kRight && jc == F.M.ny - 1)) return false;
+      if ((idir == kLeft && jc == 0) || (idir == kRight && jc == I->M.ny - 1)) return false;
     }
     if (imot == kPass) Pass();
     else if (imot == kReflect) Reflect();
     else if (imot == kScattOx) {
-      if (F.M.surface_scatter) Reflect();
+      if (I->M.surface_scatter) Reflect();
       else {
         if (Random() > (R)F.T.difpr[type]) Reflect();
         else request_diffuse();
@@ -1068,7 +1072,7 @@ struct FlyerT {
       catch_ = true;
     } else {
       catch_ = true;  // no such rule: the reference exits
-      count(F.Y, kCntNoTet);
+      count(I->Y, kCntNoTet);
     }
     load_cell_fields();
     return true;
@@ -1077,7 +1081,7 @@ struct FlyerT {
   // surface-phonon branches' drand defined (see file note).
   __device__ void surface_event() {
     if (Random() * surf_gamma < rough_rate) {
-      idir = F.M.surface_dir[min(max(F.M.nearest_surf[cell_index()], 0), kMaxSurfaces - 1)];
+      idir = I->M.surface_dir[min(max(I->M.nearest_surf[cell_index()], 0), kMaxSurfaces - 1)];
       request_diffuse();
       return;
     }
@@ -1116,7 +1120,7 @@ struct FlyerT {
   __device__ bool iterate() {
     GetV();
     if (++loop > kMaxEvents) {
-      count(F.Y, kCntTooManyEvents);
+      count(I->Y, kCntTooManyEvents);
       catch_ = true;
       return true;
     }
@@ -1131,15 +1135,15 @@ struct FlyerT {
       imp_gamma = GetImpScGamma();
       ImpScTf = imprnl / imp_gamma;
     } else {
-      ImpScTf = (R)(2 * F.dt);
+      ImpScTf = (R)(2 * I->dt);
       imp_gamma = (R)(1.0 / F.T.scrt0);
     }
-    if (F.M.surface_scatter && F.M.in_surf[cell_index()]) {
+    if (I->M.surface_scatter && I->M.in_surf[cell_index()]) {
       if (get_surf) { ssnl = -m_log(Random()); get_surf = false; }
       GetSurfScRate();
-      SurfScTf = (surf_gamma > 0 && ssnl > 0) ? ssnl / surf_gamma : (R)(2 * F.dt);
+      SurfScTf = (surf_gamma > 0 && ssnl > 0) ? ssnl / surf_gamma : (R)(2 * I->dt);
     } else {
-      SurfScTf = (R)(2 * F.dt);
+      SurfScTf = (R)(2 * I->dt);
     }
     // Min(..., flag), src/Constant_GlobalVariable_MathFunction.cpp:92-118
     int flag = 1;
@@ -1159,7 +1163,7 @@ struct FlyerT {
       if (!(Tf > (R)0)) {
         Tf = 0;
         if (++zero_run > kMaxZeroTimeEvents) {
-          count(F.Y, kCntZeroTime);
+          count(I->Y, kCntZeroTime);
           catch_ = true;
           return true;
         }
@@ -1229,14 +1233,14 @@ struct FlyerT {
       if (!self) {
         get_tet = true;
         get_cell = true;
-        count(F.Y, kCntPhonon);
+        count(I->Y, kCntPhonon);
       }
       get_ph = true;
     } else if (flag == 4) {
       if (!self) {
         get_tet = true;
         get_cell = true;
-        count(F.Y, kCntImpurity);
+        count(I->Y, kCntImpurity);
       }
       get_imp = true;
     } else if (flag == 5) {
@@ -1252,13 +1256,13 @@ struct FlyerT {
 
   // Returns 0 done, 1 caught, 2 unfinished (outer-boundary PASS).
   __device__ int finish() {
-    atomicAdd(&F.Y.counters[kCntEvents], (unsigned long long)loop);
+    atomicAdd(&I->Y.counters[kCntEvents], (unsigned long long)loop);
     if (catch_) {
-      count(F.Y, kCntCaught);
+      count(I->Y, kCntCaught);
       return 1;
     }
     if (too_far) {
-      count(F.Y, kCntUnfinished);
+      count(I->Y, kCntUnfinished);
       return 2;
     }
     return 0;
