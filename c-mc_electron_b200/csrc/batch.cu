@@ -1,0 +1,321 @@
+// batch.cu -- many simulations stepped together (mcb200_batch_*).
+//
+// The reference runs one simulation per process.  Here independent
+// simulations of uneven size (bulk boxes, FinFETs at different biases,
+// different meshes and particle counts), each an mcb200_ctx made alike (the
+// same band tables), take their transport step together: their flights run
+// as ONE persistent launch over a per-simulation table (batch_flight_kernel,
+// flight_kernels.cu), likewise each generation of copies, while the work
+// before and after the flights (deposition, Poisson, fields, the counting
+// sort) stays on each simulation's own stream, where simulations overlap on
+// the device.  A particle's draws come from its own stream (seed, uid,
+// step), so each simulation steps exactly as it would alone.
+//
+// Ordering: a batch step waits (on the device) for the work already enqueued
+// on every member's stream, and every member's later work waits for the
+// batch step, so member calls and batch steps interleave freely.
+#include "engine_internal.h"
+
+struct mcb200_batch {
+  std::string error;
+  int device = 0, precision = MCB200_FLIGHT_FP64;
+  std::vector<mcb200_ctx *> m;
+  std::vector<mcb200_batch_member> cfg;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_flight = nullptr;
+  std::vector<cudaEvent_t> ev_member;
+  cudaEvent_t marks[8] = {};
+  void *tables = nullptr;          // device: [6][n] BatchInstT (main flight x 2 parities, 4 copy generations)
+  uint32_t *steps = nullptr;       // device: step number of each member
+  unsigned int *tickets = nullptr;  // device: work counters of the 5 batched launches
+  std::vector<unsigned char> snap;  // per member: DevMesh, DevTallies and store parity the tables were built for
+  uint64_t steps_done = 0, built_at = 0;
+  int blocks_per_sm = 0;  // batched flight grid (0: as many as fit); mcb200_batch_autotune
+  uint64_t launches = 0;
+
+  ~mcb200_batch() {
+    cudaSetDevice(device);
+    if (stream) cudaStreamSynchronize(stream);
+    if (tables) cudaFree(tables);
+    if (steps) cudaFree(steps);
+    if (tickets) cudaFree(tickets);
+    if (ev_flight) cudaEventDestroy(ev_flight);
+    for (cudaEvent_t e : ev_member)
+      if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : marks)
+      if (e) cudaEventDestroy(e);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace mcb200::eng {
+namespace {
+
+int bfail(mcb200_batch *b, int code, const std::string &msg) {
+  if (b) b->error = msg;
+  return code;
+}
+
+constexpr size_t kSnapBytes = sizeof(DevMesh) + sizeof(DevTallies) + sizeof(int);
+
+void snapshot(const mcb200_ctx *c, int parity, unsigned char *out) {
+  std::memcpy(out, &c->mesh, sizeof(DevMesh));
+  std::memcpy(out + sizeof(DevMesh), &c->y, sizeof(DevTallies));
+  std::memcpy(out + sizeof(DevMesh) + sizeof(DevTallies), &parity, sizeof(int));
+}
+
+// The six tables of the batch, for the members' current stores and meshes:
+// main flight at this step's store parity and at the next, then the four
+// copy generations (copies of generation g go to g + 1; the last
+// generation's copies are counted in the member's sink).
+template <typename R>
+void build_tables(mcb200_batch *b) {
+  const int n = (int)b->m.size();
+  std::vector<BatchInstT<R>> t(6 * (size_t)n);
+  for (int k = 0; k < n; ++k) {
+    mcb200_ctx *c = b->m[k];
+    BatchInstT<R> base{};
+    base.M = c->mesh;
+    base.Y = c->y;
+    base.dt = b->cfg[k].dt;
+    base.seed = b->cfg[k].seed;
+    base.step = 0;  // from b->steps at launch
+    base.n = c->dev_counts;
+    base.capacity = (int)c->capacity;
+    for (int par = 0; par < 2; ++par) {
+      BatchInstT<R> e = base;
+      e.P = store<R>(c, par == 0 ? c->cur : 1 - c->cur);
+      e.C = children<R>(c, 0);
+      t[(size_t)par * n + k] = e;
+    }
+    for (int g = 0; g < mcb200_ctx::kGenerations; ++g) {
+      BatchInstT<R> e = base;
+      e.in = children<R>(c, g);
+      if (g + 1 < mcb200_ctx::kGenerations) {
+        e.C = children<R>(c, g + 1);
+      } else {
+        e.C = children<R>(c, g);
+        e.C.count = c->sink_count;
+        e.C.capacity = 0;
+      }
+      t[(size_t)(2 + g) * n + k] = e;
+    }
+    snapshot(c, c->cur, &b->snap[(size_t)k * kSnapBytes]);
+  }
+  // the previous launches may still read the tables: replace them in order on the batch stream
+  ck(cudaStreamSynchronize(b->stream), "sync");
+  ck(cudaMemcpyAsync(b->tables, t.data(), t.size() * sizeof(BatchInstT<R>), cudaMemcpyHostToDevice, b->stream),
+     "upload batch tables");
+  ck(cudaStreamSynchronize(b->stream), "sync");
+  b->built_at = b->steps_done;
+}
+
+// True when every member still has the mesh, tallies and store parity the
+// tables assume for this step.
+bool tables_current(const mcb200_batch *b) {
+  const int flip = (int)((b->steps_done - b->built_at) & 1);
+  unsigned char now[kSnapBytes];
+  for (size_t k = 0; k < b->m.size(); ++k) {
+    const mcb200_ctx *c = b->m[k];
+    const unsigned char *was = &b->snap[k * kSnapBytes];
+    int built_cur = 0;
+    std::memcpy(&built_cur, was + sizeof(DevMesh) + sizeof(DevTallies), sizeof(int));
+    if (c->cur != (flip ? 1 - built_cur : built_cur)) return false;
+    snapshot(c, built_cur, now);
+    if (std::memcmp(now, was, kSnapBytes) != 0) return false;
+  }
+  return true;
+}
+
+__global__ void advance_steps(uint32_t *steps, int n) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) steps[k] += 1;
+}
+
+template <typename R>
+void batch_step_impl(mcb200_batch *b) {
+  const int n = (int)b->m.size();
+  if (!tables_current(b)) build_tables<R>(b);
+  // 1. every member: counters and records for the step, then the batch stream waits for it
+  for (int k = 0; k < n; ++k) {
+    mcb200_ctx *c = b->m[k];
+    step_prepare<R>(c);
+    ck(cudaEventRecord(b->ev_member[k], c->stream), "event");
+    ck(cudaStreamWaitEvent(b->stream, b->ev_member[k], 0), "wait");
+  }
+  // 2. the batched flights on the batch stream
+  FlightCtxT<R> F;
+  F.T = b->m[0]->ts->dt;
+  const int flip = (int)((b->steps_done - b->built_at) & 1);
+  const BatchInstT<R> *tab = static_cast<const BatchInstT<R> *>(b->tables);
+  ck(cudaMemsetAsync(b->tickets, 0, sizeof(unsigned int) * (1 + mcb200_ctx::kGenerations), b->stream), "memset");
+  const int sms = b->m[0]->sm_count;
+  if (launch_batch_flight<R>(F, tab + (size_t)flip * n, n, b->steps, false, b->tickets, b->blocks_per_sm, sms,
+                             b->stream))
+    throw std::runtime_error("batched flight launch failed");
+  for (int g = 0; g < mcb200_ctx::kGenerations; ++g)
+    if (launch_batch_flight<R>(F, tab + (size_t)(2 + g) * n, n, b->steps, true, b->tickets + 1 + g, b->blocks_per_sm,
+                               sms, b->stream))
+      throw std::runtime_error("batched copy flight launch failed");
+  advance_steps<<<(n + 63) / 64, 64, 0, b->stream>>>(b->steps, n);
+  ck(cudaGetLastError(), "advance steps");
+  ck(cudaEventRecord(b->ev_flight, b->stream), "event");
+  b->launches += 2 + mcb200_ctx::kGenerations;
+  // 3. every member: its tail after the flights, on its own stream
+  for (int k = 0; k < n; ++k) {
+    mcb200_ctx *c = b->m[k];
+    ck(cudaStreamWaitEvent(c->stream, b->ev_flight, 0), "wait");
+    step_tail<R>(c);
+  }
+  b->steps_done += 1;
+}
+
+// All members' streams joined into the batch stream.
+void join_members(mcb200_batch *b) {
+  for (size_t k = 0; k < b->m.size(); ++k) {
+    ck(cudaEventRecord(b->ev_member[k], b->m[k]->stream), "event");
+    ck(cudaStreamWaitEvent(b->stream, b->ev_member[k], 0), "wait");
+  }
+}
+
+}  // namespace
+}  // namespace mcb200::eng
+
+using namespace mcb200;
+using namespace mcb200::eng;
+
+extern "C" {
+
+int mcb200_batch_create(mcb200_ctx *const *ctxs, const mcb200_batch_member *members, int n, mcb200_batch **out) {
+  if (!out || !ctxs || !members || n < 1) return MCB200_ERR_ARG;
+  *out = nullptr;
+  if (n > kMaxBatch) return MCB200_ERR_CAPACITY;
+  mcb200_batch *b = new mcb200_batch;
+  *out = b;
+  const mcb200_ctx *first = ctxs[0];
+  if (!first || first->device < 0) return bfail(b, MCB200_ERR_STATE, "mcb200_batch_create: a member has no device");
+  b->device = first->device;
+  b->precision = first->precision;
+  for (int k = 0; k < n; ++k) {
+    mcb200_ctx *c = ctxs[k];
+    if (!c || c->device != b->device || c->ts != first->ts)
+      return bfail(b, MCB200_ERR_ARG, "mcb200_batch_create: members must share the device and the band tables "
+                                      "(mcb200_create_alike)");
+    if (c->precision != b->precision)
+      return bfail(b, MCB200_ERR_ARG, "mcb200_batch_create: members must share the flight precision");
+    if (!c->mesh_set || !c->cells_set)
+      return bfail(b, MCB200_ERR_STATE, "mcb200_batch_create: every member needs its mesh and cells");
+    for (int j = 0; j < k; ++j)
+      if (ctxs[j] == c) return bfail(b, MCB200_ERR_ARG, "mcb200_batch_create: a context appears twice");
+    b->m.push_back(c);
+    b->cfg.push_back(members[k]);
+  }
+  try {
+    ck(cudaSetDevice(b->device), "cudaSetDevice");
+    ck(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    ck(cudaEventCreateWithFlags(&b->ev_flight, cudaEventDisableTiming), "cudaEventCreate");
+    b->ev_member.assign(n, nullptr);
+    for (int k = 0; k < n; ++k) ck(cudaEventCreateWithFlags(&b->ev_member[k], cudaEventDisableTiming), "event");
+    const size_t entry = b->precision == MCB200_FLIGHT_FP32 ? sizeof(BatchInstT<float>) : sizeof(BatchInstT<double>);
+    ck(cudaMalloc(&b->tables, 6 * (size_t)n * entry), "cudaMalloc");
+    ck(cudaMalloc(&b->steps, (size_t)n * sizeof(uint32_t)), "cudaMalloc");
+    ck(cudaMalloc(&b->tickets, (1 + mcb200_ctx::kGenerations) * sizeof(unsigned int)), "cudaMalloc");
+    std::vector<uint32_t> first_steps(n);
+    for (int k = 0; k < n; ++k) first_steps[k] = members[k].first_step;
+    ck(cudaMemcpy(b->steps, first_steps.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice), "copy");
+    b->snap.assign((size_t)n * kSnapBytes, 0);
+    if (b->precision == MCB200_FLIGHT_FP32) build_tables<float>(b);
+    else build_tables<double>(b);
+  } catch (const std::exception &e) {
+    return bfail(b, MCB200_ERR_CUDA, e.what());
+  }
+  return MCB200_OK;
+}
+
+void mcb200_batch_destroy(mcb200_batch *b) { delete b; }
+
+const char *mcb200_batch_last_error(const mcb200_batch *b) { return b ? b->error.c_str() : "null batch"; }
+
+int mcb200_batch_step(mcb200_batch *b) {
+  if (!b) return MCB200_ERR_ARG;
+  for (mcb200_ctx *c : b->m) {
+    if (!c->fields_set) return bfail(b, MCB200_ERR_STATE, "mcb200_batch_step: a member has no fields");
+    if (c->precision != b->precision)
+      return bfail(b, MCB200_ERR_STATE, "mcb200_batch_step: a member changed its flight precision");
+    if (c->overflow_pending) {
+      c->overflow_pending = false;
+      return bfail(b, MCB200_ERR_CAPACITY, "particle store of a member full: GENERATE copies were dropped");
+    }
+  }
+  try {
+    ck(cudaSetDevice(b->device), "cudaSetDevice");
+    if (b->precision == MCB200_FLIGHT_FP32) batch_step_impl<float>(b);
+    else batch_step_impl<double>(b);
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return bfail(b, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_batch_sync(mcb200_batch *b) {
+  if (!b) return MCB200_ERR_ARG;
+  try {
+    ck(cudaSetDevice(b->device), "cudaSetDevice");
+    ck(cudaStreamSynchronize(b->stream), "sync");
+    for (mcb200_ctx *c : b->m) {
+      ck(cudaStreamSynchronize(c->stream), "sync");
+      pull_counts(c);
+    }
+    return MCB200_OK;
+  } catch (const CapacityError &e) {
+    return bfail(b, MCB200_ERR_CAPACITY, e.what());
+  } catch (const std::exception &e) {
+    return bfail(b, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_batch_set_grid(mcb200_batch *b, int blocks_per_sm) {
+  if (!b || blocks_per_sm < 0 || blocks_per_sm > 8) return MCB200_ERR_ARG;
+  b->blocks_per_sm = blocks_per_sm;
+  return MCB200_OK;
+}
+
+int mcb200_batch_mark(mcb200_batch *b, int slot) {
+  if (!b || slot < 0 || slot >= 8) return MCB200_ERR_ARG;
+  try {
+    ck(cudaSetDevice(b->device), "cudaSetDevice");
+    if (!b->marks[slot]) ck(cudaEventCreate(&b->marks[slot]), "cudaEventCreate");
+    join_members(b);
+    ck(cudaEventRecord(b->marks[slot], b->stream), "cudaEventRecord");
+    // members' later work follows the mark as well
+    for (mcb200_ctx *c : b->m) ck(cudaStreamWaitEvent(c->stream, b->marks[slot], 0), "wait");
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return bfail(b, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_batch_elapsed_ms(mcb200_batch *b, int from, int to, double *ms) {
+  if (!b || !ms || from < 0 || from >= 8 || to < 0 || to >= 8) return MCB200_ERR_ARG;
+  if (!b->marks[from] || !b->marks[to]) return bfail(b, MCB200_ERR_STATE, "mark not recorded");
+  try {
+    ck(cudaSetDevice(b->device), "cudaSetDevice");
+    ck(cudaEventSynchronize(b->marks[to]), "cudaEventSynchronize");
+    float f = 0;
+    ck(cudaEventElapsedTime(&f, b->marks[from], b->marks[to]), "cudaEventElapsedTime");
+    *ms = f;
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return bfail(b, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_batch_info(const mcb200_batch *b, int *members, uint64_t *steps_done, uint64_t *launches) {
+  if (!b) return MCB200_ERR_ARG;
+  if (members) *members = (int)b->m.size();
+  if (steps_done) *steps_done = b->steps_done;
+  if (launches) *launches = b->launches;
+  return MCB200_OK;
+}
+
+}  // extern "C"

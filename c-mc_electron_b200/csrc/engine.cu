@@ -6,179 +6,12 @@
 #include <string>
 #include <vector>
 
-#include "cell_kernels.h"
-#include "engine_kernels.h"
-#include "field_kernels.h"
-#include "flight_physics.cuh"
-#include "fullband_tables.h"
-#include "mcb200.h"
-#include "mg_setup.h"
-#include "poisson_setup.h"
-#include "stat_kernels.h"
+#include "engine_internal.h"
 
 using namespace mcb200;
+using namespace mcb200::eng;
 
-namespace {
-
-struct CudaError : std::runtime_error {
-  using std::runtime_error::runtime_error;
-};
-struct CapacityError : std::runtime_error {
-  using std::runtime_error::runtime_error;
-};
-
-void ck(cudaError_t e, const char *what) {
-  if (e != cudaSuccess) {
-    cudaGetLastError();  // clear the latched error so the next call does not report this one
-    throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
-  }
-}
-
-template <typename T>
-T *dalloc(size_t n, std::vector<void *> &owned) {
-  void *p = nullptr;
-  ck(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)), "cudaMalloc");
-  owned.push_back(p);
-  return static_cast<T *>(p);
-}
-
-template <typename T>
-T *dupload(const std::vector<T> &v, std::vector<void *> &owned) {
-  T *p = dalloc<T>(v.size(), owned);
-  if (!v.empty()) ck(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload table");
-  return p;
-}
-
-template <typename R>
-void alloc_particles(DevParticlesT<R> &d, size_t cap, std::vector<void *> &owned) {
-  d.x = dalloc<R>(cap, owned); d.y = dalloc<R>(cap, owned); d.z = dalloc<R>(cap, owned);
-  d.kx = dalloc<R>(cap, owned); d.ky = dalloc<R>(cap, owned); d.kz = dalloc<R>(cap, owned);
-  d.energy = dalloc<double>(cap, owned); d.charge = dalloc<double>(cap, owned);
-  d.cell = dalloc<uint32_t>(cap, owned); d.itet = dalloc<int32_t>(cap, owned);
-  d.meta = dalloc<uint32_t>(cap, owned); d.uid = dalloc<uint32_t>(cap, owned);
-}
-
-template <typename R>
-void alloc_children(DevChildrenT<R> &d, int cap, std::vector<void *> &owned) {
-  d.x = dalloc<R>(cap, owned); d.y = dalloc<R>(cap, owned); d.z = dalloc<R>(cap, owned);
-  d.kx = dalloc<R>(cap, owned); d.ky = dalloc<R>(cap, owned); d.kz = dalloc<R>(cap, owned);
-  d.energy = dalloc<double>(cap, owned); d.charge = dalloc<double>(cap, owned);
-  d.left_time = dalloc<double>(cap, owned);
-  d.cell = dalloc<uint32_t>(cap, owned); d.itet = dalloc<int32_t>(cap, owned);
-  d.meta = dalloc<uint32_t>(cap, owned);
-  d.parent_uid = dalloc<uint32_t>(cap, owned); d.sub = dalloc<uint32_t>(cap, owned);
-  d.count = dalloc<unsigned int>(1, owned);
-  d.capacity = cap;
-}
-
-// One particle buffer / one child generation, in the context's flight
-// precision (only the matching member is allocated).
-struct ParticleBuffers {
-  DevParticlesT<double> d{};
-  DevParticlesT<float> f{};
-};
-struct ChildBuffers {
-  DevChildrenT<double> d{};
-  DevChildrenT<float> f{};
-};
-
-}  // namespace
-
-struct mcb200_ctx {
-  std::string error;
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  std::vector<void *> owned;   // every cudaMalloc of the context
-  std::vector<void *> mesh_owned;
-  FullBandTables tab;
-  DevTables dt{};
-  DevMesh mesh{};
-  bool mesh_set = false, cells_set = false, fields_set = false;
-  std::vector<double> hlx, hly, hlz;
-  // particles: two buffers, the store ping-pongs through the cell sort
-  int precision = MCB200_FLIGHT_FP64;
-  std::vector<void *> store_owned;  // particle and child buffers (reallocated on a precision change)
-  size_t capacity = 0;
-  ParticleBuffers pb[2];
-  int cur = 0;
-  size_t n = 0;
-  uint32_t next_uid = 0;
-  // mid-step copies: one buffer per generation
-  static constexpr int kGenerations = kChildGenerations;
-  ChildBuffers cb[kGenerations];
-  int child_cap = 0;
-  uint64_t *child_keys = nullptr;
-  uint8_t *child_alive = nullptr;
-  uint32_t *child_uids = nullptr;
-  unsigned int *append_count = nullptr;
-  unsigned int *tickets = nullptr;  // work counters of the persistent flight launches (main + generations)
-  float4 *cell32 = nullptr;         // FP32 flight's per-cell records (mesh-sized)
-  // tallies
-  DevTallies y{};
-  // sort scratch
-  unsigned int *hist = nullptr, *offsets = nullptr, *tile_sums = nullptr, *total = nullptr;
-  int ncells = 0;
-  unsigned int *h_pinned = nullptr;  // small pinned readback area
-  int sm_count = 148;
-  // deposition / Poisson (mcb200_set_device)
-  FieldBuffers fb{};
-  CgPlan cg_plan;
-  MgDevice mg{};                            // multigrid hierarchy of the Poisson stencil (mcb200_set_device)
-  int cg_method = kCgAuto, cg_blocks = 0;   // mcb200_set_poisson_solver
-  bool device_set = false;
-  double *h_scratch = nullptr;  // pinned, 16 doubles
-  // window statistics (mcb200_stat_*)
-  StatBuffers sb{};
-  StatScales ss{};
-  unsigned long long *stat_bounds = nullptr;
-  int *eeff_dev = nullptr;           // surface-normal field component per cell (mcb200_surface_rates)
-  std::vector<int> eeff_host;
-  int stat_steps = 0;
-  bool stat_open = false;
-  double vmax = 0;  // largest group-velocity component of the band tables
-  // device-resident counts: the step path never waits for them; `n` and
-  // `next_uid` above are host copies, valid while !n_stale
-  unsigned int *dev_counts = nullptr;         // [0] particles, [1] next uid, [2] store-full flag
-  unsigned long long *dev_psteps = nullptr;   // particle-steps flown (particles at the start of each step)
-  unsigned int *sink_count = nullptr;         // copies of the last child generation: counted, not stored
-  bool n_stale = false;
-  bool overflow_pending = false;              // a store-full flag seen, not yet reported
-  // CUDA-event timing on the context's stream (mcb200_timing): a ring of
-  // per-step event quadruples, read back when a slot is reused or on demand
-  bool timing = false;
-  static constexpr int kTimingRing = 64;
-  cudaEvent_t ev[kTimingRing][4] = {};
-  bool ev_pending[kTimingRing] = {};
-  int ev_head = 0;
-  unsigned long long psteps_at_timing = 0;
-  cudaEvent_t marks[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-  void *flush_buf = nullptr;  // mcb200_flush_l2 scratch
-  size_t flush_bytes = 0;
-  double flight_ms = 0, step_ms = 0;
-  uint64_t flight_launches = 0, steps = 0, particles_flown = 0, launches = 0;
-
-  ~mcb200_ctx() {
-    if (device < 0) return;
-    cudaSetDevice(device);
-    for (auto &q : ev)
-      for (cudaEvent_t e : q)
-        if (e) cudaEventDestroy(e);
-    for (cudaEvent_t e : marks)
-      if (e) cudaEventDestroy(e);
-    for (void *p : mesh_owned) cudaFree(p);
-    for (void *p : store_owned) cudaFree(p);
-    for (void *p : owned) cudaFree(p);
-    if (flush_buf) cudaFree(flush_buf);
-    if (h_pinned) cudaFreeHost(h_pinned);
-    if (h_scratch) cudaFreeHost(h_scratch);
-    if (stream) cudaStreamDestroy(stream);
-  }
-};
-
-static_assert(sizeof(TetFlightT<float>) == 128, "FP32 tet record: one 128-byte line");
-static_assert(sizeof(TetFlightT<double>) == 256, "FP64 tet record: two 128-byte lines");
-
-namespace {
+namespace mcb200::eng {
 
 int fail(mcb200_ctx *c, int code, const std::string &msg) {
   if (c) c->error = msg;
@@ -236,16 +69,6 @@ void harvest_all_timing(mcb200_ctx *c) {
   for (int q = 0; q < mcb200_ctx::kTimingRing; ++q) harvest_timing(c, q);
 }
 
-template <typename R>
-DevParticlesT<R> &store(mcb200_ctx *c, int i) {
-  if constexpr (sizeof(R) == 8) return c->pb[i].d;
-  else return c->pb[i].f;
-}
-template <typename R>
-DevChildrenT<R> &children(mcb200_ctx *c, int g) {
-  if constexpr (sizeof(R) == 8) return c->cb[g].d;
-  else return c->cb[g].f;
-}
 
 // Particle and child buffers for the context's precision.
 void alloc_stores(mcb200_ctx *c) {
@@ -265,7 +88,7 @@ void alloc_stores(mcb200_ctx *c) {
 
 // Uniform k-space locator for the tetrahedron search (see flight_physics.cuh).
 void build_kgrid(mcb200_ctx *c, int g) {
-  const FullBandTables &t = c->tab;
+  const FullBandTables &t = c->ts->tab;
   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
   for (int i = 0; i < t.nk; ++i) {
     const double v[3] = {t.xkk[i], t.ykk[i], t.zkk[i]};
@@ -303,10 +126,10 @@ void build_kgrid(mcb200_ctx *c, int g) {
     }
     st[cells] = (int)tets.size();
   }
-  c->dt.grid_n = g;
-  for (int a = 0; a < 3; ++a) { c->dt.grid_lo[a] = lo[a]; c->dt.grid_inv[a] = inv[a]; }
-  c->dt.grid_start = dupload(start, c->owned);
-  c->dt.grid_tets = dupload(tets, c->owned);
+  c->ts->dt.grid_n = g;
+  for (int a = 0; a < 3; ++a) { c->ts->dt.grid_lo[a] = lo[a]; c->ts->dt.grid_inv[a] = inv[a]; }
+  c->ts->dt.grid_start = dupload(start, c->ts->owned);
+  c->ts->dt.grid_tets = dupload(tets, c->ts->owned);
 
   // Seed grid for the lowest conduction band (the band impurity scattering
   // lands in): per fine cell, a tetrahedron that contains the cell centre,
@@ -340,8 +163,8 @@ void build_kgrid(mcb200_ctx *c, int g) {
         }
         seed[((size_t)i * sg + j) * sg + k] = pick;
       }
-  for (int a = 0; a < 3; ++a) c->dt.seed_inv[a] = sg / (hi[a] - lo[a]);
-  c->dt.seed_grid = dupload(seed, c->owned);
+  for (int a = 0; a < 3; ++a) c->ts->dt.seed_inv[a] = sg / (hi[a] - lo[a]);
+  c->ts->dt.seed_grid = dupload(seed, c->ts->owned);
 }
 
 template <typename T>
@@ -354,8 +177,8 @@ std::vector<float> to_float(const std::vector<T> &v) {
 // the FP32 containment tolerance is a k-space distance.
 void upload_tables32(mcb200_ctx *c, const std::vector<TetFlight> &tf, const std::vector<TetShape> &ts,
                      const std::vector<double4> &kn) {
-  const FullBandTables &t = c->tab;
-  DevTables32 &d = c->dt.f32;
+  const FullBandTables &t = c->ts->tab;
+  DevTables32 &d = c->ts->dt.f32;
   std::vector<TetFlightT<float>> tf32(tf.size(), TetFlightT<float>{});
   std::vector<TetShapeT<float>> ts32(ts.size());
   for (size_t it = 0; it < tf.size(); ++it) {
@@ -379,24 +202,24 @@ void upload_tables32(mcb200_ctx *c, const std::vector<TetFlight> &tf, const std:
   std::vector<float4> kn32(kn.size());
   for (size_t i = 0; i < kn.size(); ++i)
     kn32[i] = make_float4((float)kn[i].x, (float)kn[i].y, (float)kn[i].z, (float)kn[i].w);
-  d.tf = dupload(tf32, c->owned);
-  d.ts = dupload(ts32, c->owned);
-  d.knode = dupload(kn32, c->owned);
-  d.gamtet = dupload(to_float(t.gamtet), c->owned);
-  d.energy = dupload(to_float(t.energy), c->owned);
-  d.sumscatt = dupload(to_float(t.sumscatt), c->owned);
-  d.scatte = dupload(to_float(t.scatte), c->owned);
-  d.dose = dupload(to_float(t.dose), c->owned);
-  d.scattiie = dupload(to_float(t.scattiie), c->owned);
-  d.scatth = dupload(to_float(t.scatth), c->owned);
-  d.dosh = dupload(to_float(t.dosh), c->owned);
-  d.scattiih = dupload(to_float(t.scattiih), c->owned);
-  d.dostetmax = dupload(to_float(t.dostetmax), c->owned);
+  d.tf = dupload(tf32, c->ts->owned);
+  d.ts = dupload(ts32, c->ts->owned);
+  d.knode = dupload(kn32, c->ts->owned);
+  d.gamtet = dupload(to_float(t.gamtet), c->ts->owned);
+  d.energy = dupload(to_float(t.energy), c->ts->owned);
+  d.sumscatt = dupload(to_float(t.sumscatt), c->ts->owned);
+  d.scatte = dupload(to_float(t.scatte), c->ts->owned);
+  d.dose = dupload(to_float(t.dose), c->ts->owned);
+  d.scattiie = dupload(to_float(t.scattiie), c->ts->owned);
+  d.scatth = dupload(to_float(t.scatth), c->ts->owned);
+  d.dosh = dupload(to_float(t.dosh), c->ts->owned);
+  d.scattiih = dupload(to_float(t.scattiih), c->ts->owned);
+  d.dostetmax = dupload(to_float(t.dostetmax), c->ts->owned);
 }
 
 void upload_tables(mcb200_ctx *c) {
-  const FullBandTables &t = c->tab;
-  DevTables &d = c->dt;
+  const FullBandTables &t = c->ts->tab;
+  DevTables &d = c->ts->dt;
   d.nt = t.nt; d.nk = t.nk; d.nbt = t.nbt;
   for (int i = 0; i < 3; ++i) { d.nband[i] = t.nband[i]; d.bandof[i] = t.bandof[i]; d.difpr[i] = t.difpr[i]; }
   d.scpre = t.scpre; d.scprh = t.scprh;
@@ -425,30 +248,30 @@ void upload_tables(mcb200_ctx *c) {
     tn[it] = make_int4(t.T(0, it), t.T(1, it), t.T(2, it), t.T(3, it));
     tb[it] = make_int4(t.N(0, it), t.N(1, it), t.N(2, it), t.N(3, it));
   }
-  d.tf = dupload(tf, c->owned);
-  d.ts = dupload(ts, c->owned);
-  d.tnode = dupload(tn, c->owned);
-  d.tneib = dupload(tb, c->owned);
-  d.ibt = dupload(t.ibt, c->owned);
-  d.gamtet = dupload(t.gamtet, c->owned);
+  d.tf = dupload(tf, c->ts->owned);
+  d.ts = dupload(ts, c->ts->owned);
+  d.tnode = dupload(tn, c->ts->owned);
+  d.tneib = dupload(tb, c->ts->owned);
+  d.ibt = dupload(t.ibt, c->ts->owned);
+  d.gamtet = dupload(t.gamtet, c->ts->owned);
   std::vector<double4> kn(t.nk);
   for (int i = 0; i < t.nk; ++i) kn[i] = make_double4(t.xkk[i], t.ykk[i], t.zkk[i], t.eek[i]);
-  d.knode = dupload(kn, c->owned);
-  d.energy = dupload(t.energy, c->owned);
-  d.sumscatt = dupload(t.sumscatt, c->owned);
-  d.scatte = dupload(t.scatte, c->owned);
-  d.dose = dupload(t.dose, c->owned);
-  d.scattiie = dupload(t.scattiie, c->owned);
-  d.scatth = dupload(t.scatth, c->owned);
-  d.dosh = dupload(t.dosh, c->owned);
-  d.scattiih = dupload(t.scattiih, c->owned);
-  d.dostetmax = dupload(t.dostetmax, c->owned);
-  d.dos = dupload(t.dos, c->owned);
-  d.sumdos = dupload(t.sumdos, c->owned);
+  d.knode = dupload(kn, c->ts->owned);
+  d.energy = dupload(t.energy, c->ts->owned);
+  d.sumscatt = dupload(t.sumscatt, c->ts->owned);
+  d.scatte = dupload(t.scatte, c->ts->owned);
+  d.dose = dupload(t.dose, c->ts->owned);
+  d.scattiie = dupload(t.scattiie, c->ts->owned);
+  d.scatth = dupload(t.scatth, c->ts->owned);
+  d.dosh = dupload(t.dosh, c->ts->owned);
+  d.scattiih = dupload(t.scattiih, c->ts->owned);
+  d.dostetmax = dupload(t.dostetmax, c->ts->owned);
+  d.dos = dupload(t.dos, c->ts->owned);
+  d.sumdos = dupload(t.sumdos, c->ts->owned);
   for (int i = 0; i < 3; ++i) d.dosmax[i] = t.dosmax[i];
-  d.ntlist = dupload(t.ntlist, c->owned); d.ptlist = dupload(t.ptlist, c->owned); d.tlist = dupload(t.tlist, c->owned);
-  d.nslist = dupload(t.nslist, c->owned); d.pslist = dupload(t.pslist, c->owned); d.slist = dupload(t.slist, c->owned);
-  d.ntlists = dupload(t.ntlists, c->owned); d.ptlists = dupload(t.ptlists, c->owned); d.tlists = dupload(t.tlists, c->owned);
+  d.ntlist = dupload(t.ntlist, c->ts->owned); d.ptlist = dupload(t.ptlist, c->ts->owned); d.tlist = dupload(t.tlist, c->ts->owned);
+  d.nslist = dupload(t.nslist, c->ts->owned); d.pslist = dupload(t.pslist, c->ts->owned); d.slist = dupload(t.slist, c->ts->owned);
+  d.ntlists = dupload(t.ntlists, c->ts->owned); d.ptlists = dupload(t.ptlists, c->ts->owned); d.tlists = dupload(t.tlists, c->ts->owned);
   std::vector<int> symi(48 * 6), newisym(5 * 48), indmat(t.indmat, t.indmat + 729), refl(3 * 48);
   std::vector<double> bz(3 * 5 * 48);
   for (int s = 0; s < 48; ++s)
@@ -470,16 +293,16 @@ void upload_tables(mcb200_ctx *c) {
                        (t.matsym[1][s] - 1)) * 3 + (t.matsym[2][s] - 1);
       refl[axis * 48 + s] = t.indmat[idx];
     }
-  d.symi = dupload(symi, c->owned);
-  d.newisym = dupload(newisym, c->owned);
-  d.bz = dupload(bz, c->owned);
-  d.indmat = dupload(indmat, c->owned);
-  d.reflect_isym = dupload(refl, c->owned);
+  d.symi = dupload(symi, c->ts->owned);
+  d.newisym = dupload(newisym, c->ts->owned);
+  d.bz = dupload(bz, c->ts->owned);
+  d.indmat = dupload(indmat, c->ts->owned);
+  d.reflect_isym = dupload(refl, c->ts->owned);
   build_kgrid(c, 40);
   upload_tables32(c, tf, ts, kn);
-  c->vmax = 0;
+  c->ts->vmax = 0;
   for (size_t q = 0; q < t.vt.size(); ++q)
-    if (q % 4 != 3) c->vmax = std::max(c->vmax, std::fabs(t.vt[q]));
+    if (q % 4 != 3) c->ts->vmax = std::max(c->ts->vmax, std::fabs(t.vt[q]));
 }
 
 template <typename T>
@@ -558,10 +381,39 @@ void download_store(mcb200_ctx *c, size_t n, mcb200_particles *p, std::vector<ui
   }
 }
 
+// Stream, particle store, copy buffers, tallies and counters of a context
+// on its device (the tables are already there).
+void init_device_context(mcb200_ctx *c, size_t max_particles) {
+  ck(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  ck(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device), "device attribute");
+  c->capacity = max_particles;
+  c->child_cap = (int)std::min<size_t>(std::max<size_t>(max_particles / 8, 4096), 1u << 22);
+  alloc_stores(c);
+  const size_t all_children = (size_t)c->child_cap * mcb200_ctx::kGenerations;
+  c->child_keys = dalloc<uint64_t>(all_children, c->owned);
+  c->child_alive = dalloc<uint8_t>(all_children, c->owned);
+  c->child_uids = dalloc<uint32_t>(all_children, c->owned);
+  c->append_count = dalloc<unsigned int>(1, c->owned);
+  c->tickets = dalloc<unsigned int>(1 + mcb200_ctx::kGenerations, c->owned);
+  c->y.counters = dalloc<unsigned long long>(kCntNumCounters, c->owned);
+  c->y.contact = dalloc<long long>(kMaxContacts * 6, c->owned);
+  c->total = dalloc<unsigned int>(1, c->owned);
+  c->dev_counts = dalloc<unsigned int>(4, c->owned);
+  c->dev_psteps = dalloc<unsigned long long>(1, c->owned);
+  c->sink_count = dalloc<unsigned int>(1, c->owned);
+  ck(cudaMemsetAsync(c->dev_counts, 0, 4 * sizeof(unsigned int), c->stream), "memset");
+  ck(cudaMemsetAsync(c->dev_psteps, 0, sizeof(unsigned long long), c->stream), "memset");
+  ck(cudaMallocHost(&c->h_pinned, 64 * sizeof(unsigned int)), "cudaMallocHost");
+  ck(cudaMallocHost(&c->h_scratch, 16 * sizeof(double)), "cudaMallocHost");
+  ck(cudaMemsetAsync(c->y.counters, 0, sizeof(unsigned long long) * kCntNumCounters, c->stream), "memset");
+  ck(cudaMemsetAsync(c->y.contact, 0, sizeof(long long) * kMaxContacts * 6, c->stream), "memset");
+  ck(cudaStreamSynchronize(c->stream), "sync");
+}
+
 template <typename R>
 void step_impl(mcb200_ctx *c, uint32_t step, uint64_t seed, double dt);
 
-}  // namespace
+}  // namespace mcb200::eng
 
 extern "C" {
 
@@ -570,51 +422,42 @@ int mcb200_create(const char *table_dir, double kelvin, int device, size_t max_p
   *out = nullptr;
   mcb200_ctx *c = new mcb200_ctx;
   c->device = device;
+  c->ts = std::make_shared<TableSet>();
   try {
-    c->tab = FullBandTables::build(table_dir, kelvin);
+    c->ts->tab = FullBandTables::build(table_dir, kelvin);
   } catch (const std::exception &e) {
     c->device = -1;
     int code = fail(c, MCB200_ERR_IO, e.what());
     *out = c;
     return code;
   }
-  if (device < 0) {  // host-only context: tables are built, nothing is uploaded
-    *out = c;
-    return MCB200_OK;
-  }
+  *out = c;
+  if (device < 0) return MCB200_OK;  // host-only context: tables are built, nothing is uploaded
   try {
     ck(cudaSetDevice(device), "cudaSetDevice");
-    ck(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
-    ck(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device), "device attribute");
+    c->ts->device = device;
     upload_tables(c);
-    c->capacity = max_particles;
-    c->child_cap = (int)std::min<size_t>(std::max<size_t>(max_particles / 8, 4096), 1u << 22);
-    alloc_stores(c);
-    const size_t all_children = (size_t)c->child_cap * mcb200_ctx::kGenerations;
-    c->child_keys = dalloc<uint64_t>(all_children, c->owned);
-    c->child_alive = dalloc<uint8_t>(all_children, c->owned);
-    c->child_uids = dalloc<uint32_t>(all_children, c->owned);
-    c->append_count = dalloc<unsigned int>(1, c->owned);
-    c->tickets = dalloc<unsigned int>(1 + mcb200_ctx::kGenerations, c->owned);
-    c->y.counters = dalloc<unsigned long long>(kCntNumCounters, c->owned);
-    c->y.contact = dalloc<long long>(kMaxContacts * 6, c->owned);
-    c->total = dalloc<unsigned int>(1, c->owned);
-    c->dev_counts = dalloc<unsigned int>(4, c->owned);
-    c->dev_psteps = dalloc<unsigned long long>(1, c->owned);
-    c->sink_count = dalloc<unsigned int>(1, c->owned);
-    ck(cudaMemsetAsync(c->dev_counts, 0, 4 * sizeof(unsigned int), c->stream), "memset");
-    ck(cudaMemsetAsync(c->dev_psteps, 0, sizeof(unsigned long long), c->stream), "memset");
-    ck(cudaMallocHost(&c->h_pinned, 64 * sizeof(unsigned int)), "cudaMallocHost");
-    ck(cudaMallocHost(&c->h_scratch, 16 * sizeof(double)), "cudaMallocHost");
-    ck(cudaMemsetAsync(c->y.counters, 0, sizeof(unsigned long long) * kCntNumCounters, c->stream), "memset");
-    ck(cudaMemsetAsync(c->y.contact, 0, sizeof(long long) * kMaxContacts * 6, c->stream), "memset");
-    ck(cudaStreamSynchronize(c->stream), "sync");
+    init_device_context(c, max_particles);
   } catch (const std::exception &e) {
-    int code = fail(c, MCB200_ERR_CUDA, e.what());
-    *out = c;
-    return code;
+    return fail(c, MCB200_ERR_CUDA, e.what());
   }
+  return MCB200_OK;
+}
+
+int mcb200_create_alike(const mcb200_ctx *like, size_t max_particles, mcb200_ctx **out) {
+  if (!out || !like || max_particles == 0) return MCB200_ERR_ARG;
+  *out = nullptr;
+  if (like->device < 0 || !like->ts || like->ts->device < 0) return MCB200_ERR_STATE;
+  mcb200_ctx *c = new mcb200_ctx;
+  c->device = like->device;
+  c->ts = like->ts;  // the same band tables, host and device
   *out = c;
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    init_device_context(c, max_particles);
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
   return MCB200_OK;
 }
 
@@ -648,7 +491,7 @@ const char *mcb200_last_error(const mcb200_ctx *ctx) { return ctx ? ctx->error.c
 
 int mcb200_units(const mcb200_ctx *c, double *out, int n) {
   if (!c || !out) return MCB200_ERR_ARG;
-  const Units &u = c->tab.u;
+  const Units &u = c->ts->tab.u;
   const double v[14] = {u.T0, u.eV0, u.spr0, u.time0, u.conc0, u.field0, u.scrt0,
                         u.pot0, u.a0pi, u.sieg, u.eps_silicon, u.eps_oxide, u.curr0, u.dens0};
   for (int i = 0; i < n && i < 14; ++i) out[i] = v[i];
@@ -657,7 +500,7 @@ int mcb200_units(const mcb200_ctx *c, double *out, int n) {
 
 int mcb200_copy_table(const mcb200_ctx *c, const char *name, void *out, size_t bytes, size_t *needed) {
   if (!c || !name || !needed) return MCB200_ERR_ARG;
-  const FullBandTables &t = c->tab;
+  const FullBandTables &t = c->ts->tab;
   const std::string n(name);
   std::vector<int> iv;
   std::vector<double> dv;
@@ -853,7 +696,7 @@ int mcb200_upload_particles(mcb200_ctx *c, size_t n, const mcb200_particles *p) 
       const int i = p->i[q], j = p->j[q], k = p->k[q];
       if (i < 0 || j < 0 || k < 0 || i >= c->mesh.nx || j >= c->mesh.ny || k >= c->mesh.nz)
         return fail(c, MCB200_ERR_ARG, "particle outside the mesh");
-      if (p->isym[q] < 0 || p->isym[q] > 47 || p->itet[q] < 0 || p->itet[q] >= c->tab.nt || p->type[q] < 0 ||
+      if (p->isym[q] < 0 || p->isym[q] > 47 || p->itet[q] < 0 || p->itet[q] >= c->ts->tab.nt || p->type[q] < 0 ||
           p->type[q] > 1)
         return fail(c, MCB200_ERR_ARG, "particle state out of range");
       cell[q] = pack_cell(i, j, k);
@@ -962,7 +805,7 @@ int mcb200_seed_particles(mcb200_ctx *c, size_t n, const int32_t *cell_of, const
     ck(cudaMemcpyAsync(dcell, cell_of, n * sizeof(int), cudaMemcpyHostToDevice, c->stream), "copy");
     ck(cudaMemcpyAsync(dq, charge, n * sizeof(double), cudaMemcpyHostToDevice, c->stream), "copy");
     FlightCtx F;
-    F.T = c->dt;
+    F.T = c->ts->dt;
     F.M = c->mesh;
     F.Y = c->y;
     F.C = DevChildren{};
@@ -1192,10 +1035,10 @@ int mcb200_set_device(mcb200_ctx *c, const int32_t *material, const double *dono
       const int32_t *r = planes + 7 * q;
       pl[q] = ContactPlane{r[0], r[1], r[2], r[3], r[4], r[5], r[6]};
     }
-    const Units &u = c->tab.u;
+    const Units &u = c->ts->tab.u;
     const double eps[6] = {0.0, u.eps_vacuum, u.eps_oxide, u.eps_silicon, 0.0, 0.0};
     const PoissonSetup s = PoissonSetup::build(m.nx, m.ny, m.nz, dx.data(), dy.data(), dz.data(), material, donor,
-                                               acceptor, c->tab.ni, eps, pl,
+                                               acceptor, c->ts->tab.ni, eps, pl,
                                                std::vector<double>(vapp, vapp + n_contacts),
                                                std::vector<double>(phims, phims + n_contacts));
     const size_t cells = (size_t)c->ncells, nodes = (size_t)s.nodes();
@@ -1345,7 +1188,7 @@ int mcb200_surface_rates(mcb200_ctx *c, const mcb200_surface_params *p, const in
   if (!c->mesh_set) return fail(c, MCB200_ERR_STATE, "mcb200_surface_rates before mcb200_set_mesh");
   try {
     ck(cudaSetDevice(c->device), "cudaSetDevice");
-    const Units &u = c->tab.u;
+    const Units &u = c->ts->tab.u;
     SurfaceRateParams q{};
     q.delta = p->delta; q.ail = p->ail; q.xiph = p->xiph; q.theta = p->theta; q.gama = p->gama;
     q.nbmod = p->nbmod; q.npf = p->npf; q.pft = p->pft; q.pfn = p->pfn; q.kpha = p->kpha;
@@ -1479,14 +1322,14 @@ int mcb200_stat_begin(mcb200_ctx *c, int window_steps) {
     ck(cudaStreamSynchronize(s), "sync");
     unsigned long long b[4];
     std::memcpy(b, c->h_scratch, sizeof(b));
-    const double emax = std::max(c->tab.emax, 1.0) * 2.0;
+    const double emax = std::max(c->ts->tab.emax, 1.0) * 2.0;
     for (int t = 0; t < 2; ++t) {
       double qmax;
       std::memcpy(&qmax, &b[t], 8);
       const double bound = std::max((double)b[2 + t] * qmax * window_steps * 4.0, 1e-300);
       auto unit = [](double bnd) { return std::ldexp(1.0, 62 - (int)std::ceil(std::log2(bnd))); };
       c->ss.q[t] = unit(bound);
-      c->ss.v[t] = unit(bound * std::max(c->vmax, 1e-300));
+      c->ss.v[t] = unit(bound * std::max(c->ts->vmax, 1e-300));
       c->ss.e[t] = unit(bound * emax);
     }
     const size_t nodes = (size_t)c->sb.nodes;
@@ -1511,9 +1354,9 @@ int mcb200_stat_accumulate(mcb200_ctx *c) {
     const int grid = grid_for(c, c->capacity, 256);
     const DevCount n{c->dev_counts, nullptr, (int)c->capacity};
     if (c->precision == MCB200_FLIGHT_FP32)
-      launch_statistic(store<float>(c, c->cur), n, c->mesh, c->dt, c->ss, c->sb, grid, s);
+      launch_statistic(store<float>(c, c->cur), n, c->mesh, c->ts->dt, c->ss, c->sb, grid, s);
     else
-      launch_statistic(store<double>(c, c->cur), n, c->mesh, c->dt, c->ss, c->sb, grid, s);
+      launch_statistic(store<double>(c, c->cur), n, c->mesh, c->ts->dt, c->ss, c->sb, grid, s);
     if (c->device_set) launch_add_potential(c->sb.nodes, c->fb.potential, c->sb.pot_sum, s);
     ck(cudaGetLastError(), "statistic");
     c->stat_steps += 1;
@@ -1606,18 +1449,58 @@ int mcb200_get_array(mcb200_ctx *c, const char *name, double *out, size_t n) {
 
 }  // extern "C"
 
-namespace {
+namespace mcb200::eng {
 
 // One step of the store in precision R: main flight, mid-step copies
 // generation by generation, uids and append, then removal of caught
 // particles and the counting sort by cell.
+// Before the flights of a step: work counters, the FP32 per-cell records,
+// and zeroed copy counters of every generation and of the sink.
+template <typename R>
+void step_prepare(mcb200_ctx *c) {
+  cudaStream_t s = c->stream;
+  ck(cudaMemsetAsync(c->tickets, 0, sizeof(unsigned int) * (1 + mcb200_ctx::kGenerations), s), "memset");
+  if constexpr (sizeof(R) == 4) {  // FP32 flight reads the fields as per-cell float records
+    launch_cell_records32(c->ts->dt, c->mesh, c->cell32, c->ncells, s);
+    c->launches += 1;
+  }
+  for (int g = 0; g < mcb200_ctx::kGenerations; ++g)
+    ck(cudaMemsetAsync(children<R>(c, g).count, 0, sizeof(unsigned int), s), "memset");
+  ck(cudaMemsetAsync(c->sink_count, 0, sizeof(unsigned int), s), "memset");
+}
+
+// After the flights of a step: uids for the surviving copies, which join the
+// store; caught particles are dropped and the store is counting-sorted by
+// cell; the sorted count becomes the particle count.
+template <typename R>
+void step_tail(mcb200_ctx *c) {
+  cudaStream_t s = c->stream;
+  const int cap = (int)c->capacity;
+  ChildSetT<R> set;
+  for (int g = 0; g < mcb200_ctx::kGenerations; ++g) set.g[g] = children<R>(c, g);
+  launch_append_children(set, c->child_keys, c->child_alive, c->child_uids, c->dev_counts + 1, store<R>(c, c->cur),
+                         c->dev_counts, cap, c->append_count, c->dev_counts + 2,
+                         grid_for(c, (size_t)c->child_cap * mcb200_ctx::kGenerations, 256), s);
+  ck(cudaGetLastError(), "append children");
+  c->launches += 3;
+  const int other = 1 - c->cur;
+  launch_cell_sort(store<R>(c, c->cur), DevCount{c->dev_counts, c->append_count, cap}, store<R>(c, other), c->ncells,
+                   c->mesh.nx, c->mesh.nz, c->hist, c->offsets, c->tile_sums, c->total, grid_for(c, c->capacity, 256),
+                   s);
+  launch_step_finish(c->dev_counts, c->total, c->dev_counts + 1, c->append_count, c->dev_psteps, s);
+  ck(cudaGetLastError(), "cell sort");
+  c->launches += 6;
+  c->cur = other;
+  c->n_stale = true;
+}
+
 template <typename R>
 void step_impl(mcb200_ctx *c, uint32_t step, uint64_t seed, double dt) {
   // Every size is read on the device (DevCount, child counts), so the step
   // is enqueued without waiting for the GPU.
   cudaStream_t s = c->stream;
   FlightCtxT<R> F;
-  F.T = c->dt;
+  F.T = c->ts->dt;
   F.M = c->mesh;
   F.Y = c->y;
   F.dt = dt;
@@ -1632,17 +1515,12 @@ void step_impl(mcb200_ctx *c, uint32_t step, uint64_t seed, double dt) {
     c->ev_pending[q] = true;
     ck(cudaEventRecord(ev[0], s), "event");
   }
-  const int cap = (int)c->capacity;
-  ck(cudaMemsetAsync(c->tickets, 0, sizeof(unsigned int) * (1 + mcb200_ctx::kGenerations), s), "memset");
-  if constexpr (sizeof(R) == 4) {  // FP32 flight reads the fields as per-cell float records
-    launch_cell_records32(c->dt, c->mesh, c->cell32, c->ncells, s);
-    c->launches += 1;
-  }
+  step_prepare<R>(c);
   // 1. main flight; copies go to generation 0
-  ck(cudaMemsetAsync(children<R>(c, 0).count, 0, sizeof(unsigned int), s), "memset");
   F.C = children<R>(c, 0);
   if (ev) ck(cudaEventRecord(ev[1], s), "event");
-  launch_flight(F, store<R>(c, c->cur), DevCount{c->dev_counts, nullptr, cap}, c->tickets, c->sm_count, s);
+  launch_flight(F, store<R>(c, c->cur), DevCount{c->dev_counts, nullptr, (int)c->capacity}, c->tickets, c->sm_count,
+                s);
   ck(cudaGetLastError(), "flight kernel");
   if (ev) ck(cudaEventRecord(ev[2], s), "event");
   c->launches += 1;
@@ -1651,10 +1529,8 @@ void step_impl(mcb200_ctx *c, uint32_t step, uint64_t seed, double dt) {
   //    generation are counted in a sink, not flown
   for (int g = 0; g < mcb200_ctx::kGenerations; ++g) {
     if (g + 1 < mcb200_ctx::kGenerations) {
-      ck(cudaMemsetAsync(children<R>(c, g + 1).count, 0, sizeof(unsigned int), s), "memset");
       F.C = children<R>(c, g + 1);
     } else {
-      ck(cudaMemsetAsync(c->sink_count, 0, sizeof(unsigned int), s), "memset");
       F.C = children<R>(c, g);
       F.C.count = c->sink_count;
       F.C.capacity = 0;
@@ -1663,30 +1539,18 @@ void step_impl(mcb200_ctx *c, uint32_t step, uint64_t seed, double dt) {
     ck(cudaGetLastError(), "child flight kernel");
     c->launches += 1;
   }
-  // 3. uids for surviving copies, then append them to the store
-  ChildSetT<R> set;
-  for (int g = 0; g < mcb200_ctx::kGenerations; ++g) set.g[g] = children<R>(c, g);
-  launch_append_children(set, c->child_keys, c->child_alive, c->child_uids, c->dev_counts + 1, store<R>(c, c->cur),
-                         c->dev_counts, cap, c->append_count, c->dev_counts + 2,
-                         grid_for(c, (size_t)c->child_cap * mcb200_ctx::kGenerations, 256), s);
-  ck(cudaGetLastError(), "append children");
-  c->launches += 3;
-  // 4. drop caught particles and counting-sort the store by cell; the
-  //    sorted count becomes the particle count
-  const int other = 1 - c->cur;
-  launch_cell_sort(store<R>(c, c->cur), DevCount{c->dev_counts, c->append_count, cap}, store<R>(c, other), c->ncells,
-                   c->mesh.nx, c->mesh.nz, c->hist, c->offsets, c->tile_sums, c->total, grid_for(c, c->capacity, 256),
-                   s);
-  launch_step_finish(c->dev_counts, c->total, c->dev_counts + 1, c->append_count, c->dev_psteps, s);
-  ck(cudaGetLastError(), "cell sort");
-  c->launches += 6;
+  // 3.-4. append the copies, sort by cell
+  step_tail<R>(c);
   if (ev) ck(cudaEventRecord(ev[3], s), "event");
-  c->cur = other;
-  c->n_stale = true;
   if (c->timing) {
     c->flight_launches += 1;
     c->steps += 1;
   }
 }
 
-}  // namespace
+template void step_prepare<float>(mcb200_ctx *);
+template void step_prepare<double>(mcb200_ctx *);
+template void step_tail<float>(mcb200_ctx *);
+template void step_tail<double>(mcb200_ctx *);
+
+}  // namespace mcb200::eng

@@ -1,0 +1,226 @@
+// engine_internal.h -- the engine context and the helpers its translation
+// units share (engine.cu, batch.cu).  Not part of the C ABI.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "cell_kernels.h"
+#include "engine_kernels.h"
+#include "field_kernels.h"
+#include "flight_physics.cuh"
+#include "fullband_tables.h"
+#include "mcb200.h"
+#include "mg_setup.h"
+#include "poisson_setup.h"
+#include "stat_kernels.h"
+
+namespace mcb200::eng {
+
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct CapacityError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+inline void ck(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // clear the latched error so the next call does not report this one
+    throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+  }
+}
+
+template <typename T>
+T *dalloc(size_t n, std::vector<void *> &owned) {
+  void *p = nullptr;
+  ck(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)), "cudaMalloc");
+  owned.push_back(p);
+  return static_cast<T *>(p);
+}
+
+template <typename T>
+T *dupload(const std::vector<T> &v, std::vector<void *> &owned) {
+  T *p = dalloc<T>(v.size(), owned);
+  if (!v.empty()) ck(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload table");
+  return p;
+}
+
+template <typename R>
+void alloc_particles(DevParticlesT<R> &d, size_t cap, std::vector<void *> &owned) {
+  d.x = dalloc<R>(cap, owned); d.y = dalloc<R>(cap, owned); d.z = dalloc<R>(cap, owned);
+  d.kx = dalloc<R>(cap, owned); d.ky = dalloc<R>(cap, owned); d.kz = dalloc<R>(cap, owned);
+  d.energy = dalloc<double>(cap, owned); d.charge = dalloc<double>(cap, owned);
+  d.cell = dalloc<uint32_t>(cap, owned); d.itet = dalloc<int32_t>(cap, owned);
+  d.meta = dalloc<uint32_t>(cap, owned); d.uid = dalloc<uint32_t>(cap, owned);
+}
+
+template <typename R>
+void alloc_children(DevChildrenT<R> &d, int cap, std::vector<void *> &owned) {
+  d.x = dalloc<R>(cap, owned); d.y = dalloc<R>(cap, owned); d.z = dalloc<R>(cap, owned);
+  d.kx = dalloc<R>(cap, owned); d.ky = dalloc<R>(cap, owned); d.kz = dalloc<R>(cap, owned);
+  d.energy = dalloc<double>(cap, owned); d.charge = dalloc<double>(cap, owned);
+  d.left_time = dalloc<double>(cap, owned);
+  d.cell = dalloc<uint32_t>(cap, owned); d.itet = dalloc<int32_t>(cap, owned);
+  d.meta = dalloc<uint32_t>(cap, owned);
+  d.parent_uid = dalloc<uint32_t>(cap, owned); d.sub = dalloc<uint32_t>(cap, owned);
+  d.count = dalloc<unsigned int>(1, owned);
+  d.capacity = cap;
+}
+
+// One particle buffer / one child generation, in the context's flight
+// precision (only the matching member is allocated).
+struct ParticleBuffers {
+  DevParticlesT<double> d{};
+  DevParticlesT<float> f{};
+};
+struct ChildBuffers {
+  DevChildrenT<double> d{};
+  DevChildrenT<float> f{};
+};
+
+// Band tables on the host and the device (mcb200_create): built once and
+// shared by every context created alike (mcb200_create_alike).
+struct TableSet {
+  FullBandTables tab;
+  DevTables dt{};
+  double vmax = 0;  // largest group-velocity component of the band tables
+  std::vector<void *> owned;
+  int device = -1;
+  ~TableSet() {
+    if (device < 0) return;
+    cudaSetDevice(device);
+    for (void *p : owned) cudaFree(p);
+  }
+};
+
+}  // namespace mcb200::eng
+
+using namespace mcb200;
+using namespace mcb200::eng;
+
+struct mcb200_ctx {
+  std::string error;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<void *> owned;   // every cudaMalloc of the context
+  std::vector<void *> mesh_owned;
+  std::shared_ptr<TableSet> ts;  // band tables (host and device), shared by contexts made alike
+  DevMesh mesh{};
+  bool mesh_set = false, cells_set = false, fields_set = false;
+  std::vector<double> hlx, hly, hlz;
+  // particles: two buffers, the store ping-pongs through the cell sort
+  int precision = MCB200_FLIGHT_FP64;
+  std::vector<void *> store_owned;  // particle and child buffers (reallocated on a precision change)
+  size_t capacity = 0;
+  ParticleBuffers pb[2];
+  int cur = 0;
+  size_t n = 0;
+  uint32_t next_uid = 0;
+  // mid-step copies: one buffer per generation
+  static constexpr int kGenerations = kChildGenerations;
+  ChildBuffers cb[kGenerations];
+  int child_cap = 0;
+  uint64_t *child_keys = nullptr;
+  uint8_t *child_alive = nullptr;
+  uint32_t *child_uids = nullptr;
+  unsigned int *append_count = nullptr;
+  unsigned int *tickets = nullptr;  // work counters of the persistent flight launches (main + generations)
+  float4 *cell32 = nullptr;         // FP32 flight's per-cell records (mesh-sized)
+  // tallies
+  DevTallies y{};
+  // sort scratch
+  unsigned int *hist = nullptr, *offsets = nullptr, *tile_sums = nullptr, *total = nullptr;
+  int ncells = 0;
+  unsigned int *h_pinned = nullptr;  // small pinned readback area
+  int sm_count = 148;
+  // deposition / Poisson (mcb200_set_device)
+  FieldBuffers fb{};
+  CgPlan cg_plan;
+  MgDevice mg{};                            // multigrid hierarchy of the Poisson stencil (mcb200_set_device)
+  int cg_method = kCgAuto, cg_blocks = 0;   // mcb200_set_poisson_solver
+  bool device_set = false;
+  double *h_scratch = nullptr;  // pinned, 16 doubles
+  // window statistics (mcb200_stat_*)
+  StatBuffers sb{};
+  StatScales ss{};
+  unsigned long long *stat_bounds = nullptr;
+  int *eeff_dev = nullptr;           // surface-normal field component per cell (mcb200_surface_rates)
+  std::vector<int> eeff_host;
+  int stat_steps = 0;
+  bool stat_open = false;
+  // device-resident counts: the step path never waits for them; `n` and
+  // `next_uid` above are host copies, valid while !n_stale
+  unsigned int *dev_counts = nullptr;         // [0] particles, [1] next uid, [2] store-full flag
+  unsigned long long *dev_psteps = nullptr;   // particle-steps flown (particles at the start of each step)
+  unsigned int *sink_count = nullptr;         // copies of the last child generation: counted, not stored
+  bool n_stale = false;
+  bool overflow_pending = false;              // a store-full flag seen, not yet reported
+  // CUDA-event timing on the context's stream (mcb200_timing): a ring of
+  // per-step event quadruples, read back when a slot is reused or on demand
+  bool timing = false;
+  static constexpr int kTimingRing = 64;
+  cudaEvent_t ev[kTimingRing][4] = {};
+  bool ev_pending[kTimingRing] = {};
+  int ev_head = 0;
+  unsigned long long psteps_at_timing = 0;
+  cudaEvent_t marks[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  void *flush_buf = nullptr;  // mcb200_flush_l2 scratch
+  size_t flush_bytes = 0;
+  double flight_ms = 0, step_ms = 0;
+  uint64_t flight_launches = 0, steps = 0, particles_flown = 0, launches = 0;
+
+  ~mcb200_ctx() {
+    if (device < 0) return;
+    cudaSetDevice(device);
+    for (auto &q : ev)
+      for (cudaEvent_t e : q)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : marks)
+      if (e) cudaEventDestroy(e);
+    for (void *p : mesh_owned) cudaFree(p);
+    for (void *p : store_owned) cudaFree(p);
+    for (void *p : owned) cudaFree(p);
+    if (flush_buf) cudaFree(flush_buf);
+    if (h_pinned) cudaFreeHost(h_pinned);
+    if (h_scratch) cudaFreeHost(h_scratch);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+static_assert(sizeof(TetFlightT<float>) == 128, "FP32 tet record: one 128-byte line");
+static_assert(sizeof(TetFlightT<double>) == 256, "FP64 tet record: two 128-byte lines");
+
+
+namespace mcb200::eng {
+
+template <typename R>
+DevParticlesT<R> &store(mcb200_ctx *c, int i) {
+  if constexpr (sizeof(R) == 8) return c->pb[i].d;
+  else return c->pb[i].f;
+}
+template <typename R>
+DevChildrenT<R> &children(mcb200_ctx *c, int g) {
+  if constexpr (sizeof(R) == 8) return c->cb[g].d;
+  else return c->cb[g].f;
+}
+
+int fail(mcb200_ctx *c, int code, const std::string &msg);
+// Host copies of the device counts (waits for the stream when a step may
+// have changed them); throws CapacityError once for a store-full flag.
+void pull_counts(mcb200_ctx *c);
+void push_counts(mcb200_ctx *c);
+int grid_for(const mcb200_ctx *c, size_t n, int block);
+// The parts of a transport step around its flights (engine.cu).
+template <typename R>
+void step_prepare(mcb200_ctx *c);
+template <typename R>
+void step_tail(mcb200_ctx *c);
+
+}  // namespace mcb200::eng

@@ -177,6 +177,85 @@ __global__ void __launch_bounds__(256, kFlightBlocks<R>) child_flight_kernel(Fli
   fly_interleaved(F, S, ChildIO<R>{in}, count, ticket);
 }
 
+// ---- batched flight ------------------------------------------------------
+// Many simulations in one persistent launch.  Each block copies the batch's
+// table of simulations (BatchInstT, one per simulation) into shared memory
+// and forms the prefix of their particle counts, read on the device; a lane
+// that takes ticket q flies particle q - prefix[k] of simulation k, the
+// largest k with prefix[k] <= q, with that simulation's mesh, fields,
+// tallies, copy buffer, dt, seed and step (FlyerT::I).  A particle's draws
+// still come from its own stream (seed, uid, step), so it flies exactly as
+// in a launch of its simulation alone.
+template <typename R, bool kChild>
+struct BatchIO {
+  const BatchInstT<R> *I;  // shared memory
+  const int *prefix;       // [ninst + 1], shared memory
+  int ninst;
+  __device__ __forceinline__ int find(int q) const {
+    int lo = 0, hi = ninst - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (prefix[mid] <= q) lo = mid;
+      else hi = mid - 1;
+    }
+    return lo;
+  }
+  __device__ bool load(int q, FlyerT<R> &f) const {
+    const int k = find(q);
+    const BatchInstT<R> &b = I[k];
+    f.I = &b;
+    const int p = q - prefix[k];
+    if constexpr (kChild) return ChildIO<R>{b.in}.load(p, f);
+    else return StoreIO<R>{b.P, b.dt}.load(p, f);
+  }
+  __device__ void store(int q, const FlyerT<R> &f, int r) const {
+    const BatchInstT<R> *b = static_cast<const BatchInstT<R> *>(f.I);
+    const int p = q - prefix[b - I];
+    if constexpr (kChild) ChildIO<R>{b->in}.store(p, f, r);
+    else StoreIO<R>{b->P, b->dt}.store(p, f, r);
+  }
+};
+
+// Dynamic shared memory of a batched launch over `ninst` simulations.
+template <typename R>
+constexpr size_t batch_smem_bytes(int ninst) {
+  return (size_t)ninst * sizeof(BatchInstT<R>) + (size_t)(ninst + 1) * sizeof(int);
+}
+
+// F holds the band tables (its per-simulation part is unused); steps[k] is
+// simulation k's step number (device memory, advanced between steps).
+template <typename R, bool kChild>
+__global__ void __launch_bounds__(256, kFlightBlocks<R>) batch_flight_kernel(const __grid_constant__ FlightCtxT<R> F,
+                                                                             const BatchInstT<R> *inst,
+                                                                             int ninst, const uint32_t *steps,
+                                                                             unsigned int *ticket) {
+  extern __shared__ __align__(16) unsigned char batch_smem[];
+  BatchInstT<R> *I = reinterpret_cast<BatchInstT<R> *>(batch_smem);
+  int *prefix = reinterpret_cast<int *>(I + ninst);
+  __shared__ SymSmemT<R> S;
+  {
+    static_assert(sizeof(BatchInstT<R>) % 8 == 0, "the table is copied in 8-byte words");
+    const unsigned long long *src = reinterpret_cast<const unsigned long long *>(inst);
+    unsigned long long *dst = reinterpret_cast<unsigned long long *>(I);
+    const int words = ninst * (int)(sizeof(BatchInstT<R>) / 8);
+    for (int w = threadIdx.x; w < words; w += blockDim.x) dst[w] = src[w];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int k = 0; k < ninst; ++k) {
+      I[k].step = steps[k];
+      prefix[k] = run;
+      run += kChild ? min((int)*I[k].in.count, I[k].in.capacity) : min((int)*I[k].n, I[k].capacity);
+    }
+    prefix[ninst] = run;
+  }
+  load_sym(S, F.T);  // ends with a barrier: the table and prefix are visible
+  const int total = prefix[ninst];
+  if (total == 0) return;
+  fly_interleaved(F, S, BatchIO<R, kChild>{I, prefix, ninst}, total, ticket);
+}
+
 // FP32 flight's per-cell records (DevMesh::cell32): the fields in float and
 // the Brooks-Herring factors of GetImpScRate / GetImpScGamma /
 // EleImpScUpdateK (src/ElectronImpurityScatter.cpp:6-306) evaluated once per
@@ -460,6 +539,26 @@ void launch_child_flight(const FlightCtxT<R> &F, const DevChildrenT<R> &in, int 
                          int sm_count, cudaStream_t s) {
   child_flight_kernel<R><<<flight_grid<R>(n_hint, 256, sm_count), 256, 0, s>>>(F, in, ticket);
 }
+template <typename R>
+int launch_batch_flight(const FlightCtxT<R> &F, const BatchInstT<R> *inst, int ninst, const uint32_t *steps,
+                        bool child, unsigned int *ticket, int blocks_per_sm, int sm_count, cudaStream_t s) {
+  if (ninst < 1 || ninst > kMaxBatch) return 1;
+  const size_t smem = batch_smem_bytes<R>(ninst);
+  auto kernel = child ? batch_flight_kernel<R, true> : batch_flight_kernel<R, false>;
+  static bool opted[2] = {false, false};
+  if (!opted[child ? 1 : 0]) {
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)batch_smem_bytes<R>(kMaxBatch)) != cudaSuccess)
+      return 1;
+    opted[child ? 1 : 0] = true;
+  }
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, smem) != cudaSuccess || per_sm < 1)
+    return 1;
+  if (blocks_per_sm > 0) per_sm = std::min(per_sm, blocks_per_sm);
+  kernel<<<per_sm * sm_count, 256, smem, s>>>(F, inst, ninst, steps, ticket);
+  return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
 void launch_cell_records32(const DevTables &T, const DevMesh &M, float4 *out, int cells, cudaStream_t s) {
   if (cells > 0) cell_records32_kernel<<<(cells + 255) / 256, 256, 0, s>>>(T, M, out, cells);
 }
@@ -506,6 +605,8 @@ void launch_cell_sort(const DevParticlesT<R> &src, DevCount n, const DevParticle
   template void launch_append_children<R>(const ChildSetT<R> &, uint64_t *, uint8_t *, uint32_t *,             \
                                           unsigned int *, const DevParticlesT<R> &, const unsigned int *, int,  \
                                           unsigned int *, unsigned int *, int, cudaStream_t);                   \
+  template int launch_batch_flight<R>(const FlightCtxT<R> &, const BatchInstT<R> *, int, const uint32_t *, bool, \
+                                      unsigned int *, int, int, cudaStream_t);                                  \
   template void launch_cell_sort<R>(const DevParticlesT<R> &, DevCount, const DevParticlesT<R> &, int, int, int, \
                                     unsigned int *, unsigned int *, unsigned int *, unsigned int *, int,        \
                                     cudaStream_t);

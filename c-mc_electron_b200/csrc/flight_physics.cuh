@@ -127,6 +127,19 @@ template <typename R>
 struct FlightCtxT : FlightInstT<R> {  // plus the band tables, shared by every simulation
   DevTables T;
 };
+
+// One simulation of a batched flight launch: its flight context, its
+// current particle store and device count (main flight), or the copies it
+// flies (child flights).
+template <typename R>
+struct BatchInstT : FlightInstT<R> {
+  DevParticlesT<R> P;
+  DevChildrenT<R> in;
+  const unsigned int *n;
+  int capacity;
+  int pad_;
+};
+constexpr int kMaxBatch = 64;  // simulations per batched launch (their table sits in shared memory)
 using FlightCtx = FlightCtxT<double>;
 
 __device__ __forceinline__ void tally_add_i64(long long *p, double v, double scale) {

@@ -77,6 +77,10 @@ class DeckInfo(ctypes.Structure):
                [("output_dir", ctypes.c_char * 512), ("prepared", ctypes.c_int), ("dt", ctypes.c_double)]
 
 
+class BatchMember(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_double), ("seed", ctypes.c_uint64), ("first_step", ctypes.c_uint32)]
+
+
 class RunOptions(ctypes.Structure):
     _fields_ = [("table_dir", ctypes.c_char_p), ("data_dir", ctypes.c_char_p), ("flight_precision", ctypes.c_int),
                 ("poisson_every", ctypes.c_int), ("poisson_rel_tol", ctypes.c_double), ("max_steps", ctypes.c_int),
@@ -106,6 +110,18 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     c = ctypes
     vp, i32p, dp = c.c_void_p, c.POINTER(c.c_int32), c.POINTER(c.c_double)
     lib.mcb200_create.argtypes = [c.c_char_p, c.c_double, c.c_int, c.c_size_t, c.POINTER(vp)]
+    lib.mcb200_create_alike.argtypes = [vp, c.c_size_t, c.POINTER(vp)]
+    lib.mcb200_batch_create.argtypes = [c.POINTER(vp), c.POINTER(BatchMember), c.c_int, c.POINTER(vp)]
+    lib.mcb200_batch_destroy.argtypes = [vp]
+    lib.mcb200_batch_destroy.restype = None
+    lib.mcb200_batch_last_error.argtypes = [vp]
+    lib.mcb200_batch_last_error.restype = c.c_char_p
+    lib.mcb200_batch_step.argtypes = [vp]
+    lib.mcb200_batch_sync.argtypes = [vp]
+    lib.mcb200_batch_set_grid.argtypes = [vp, c.c_int]
+    lib.mcb200_batch_mark.argtypes = [vp, c.c_int]
+    lib.mcb200_batch_elapsed_ms.argtypes = [vp, c.c_int, c.c_int, dp]
+    lib.mcb200_batch_info.argtypes = [vp, c.POINTER(c.c_int), c.POINTER(c.c_uint64), c.POINTER(c.c_uint64)]
     lib.mcb200_destroy.argtypes = [vp]
     lib.mcb200_destroy.restype = None
     lib.mcb200_last_error.argtypes = [vp]
@@ -200,10 +216,16 @@ class Engine:
     """One engine context: full-band tables, mesh, particles, tallies on one GPU."""
 
     def __init__(self, table_dir: str = DEFAULT_TABLE_DIR, kelvin: float = 300.0, device: int = 0,
-                 max_particles: int = 1 << 20, precision: int = FLIGHT_FP64):
+                 max_particles: int = 1 << 20, precision: int = FLIGHT_FP64, like: "Engine | None" = None):
+        """like: an engine whose device and band tables this one shares
+        (mcb200_create_alike; table_dir, kelvin and device are then unused)."""
         self._lib = lib()
         self._ctx = ctypes.c_void_p()
-        rc = self._lib.mcb200_create(table_dir.encode(), kelvin, device, max_particles, ctypes.byref(self._ctx))
+        self._like = like  # the shared tables live while a context uses them; keep the donor's wrapper alive
+        if like is not None:
+            rc = self._lib.mcb200_create_alike(like._ctx, max_particles, ctypes.byref(self._ctx))
+        else:
+            rc = self._lib.mcb200_create(table_dir.encode(), kelvin, device, max_particles, ctypes.byref(self._ctx))
         if rc != OK:
             msg = self._lib.mcb200_last_error(self._ctx).decode() if self._ctx else "no context"
             if self._ctx:
@@ -427,6 +449,62 @@ class Engine:
 
     def reset_tallies(self):
         self._check(self._lib.mcb200_reset_tallies(self._ctx), "reset_tallies")
+
+
+class Batch:
+    """Engines made alike stepped together (mcb200_batch_*): one persistent
+    flight launch over all members per step.  members: [(engine, dt, seed,
+    first_step)]."""
+
+    def __init__(self, members):
+        self._lib = lib()
+        self._b = ctypes.c_void_p()
+        self.engines = [m[0] for m in members]
+        ctxs = (ctypes.c_void_p * len(members))(*[m[0]._ctx.value for m in members])
+        cfg = (BatchMember * len(members))(*[BatchMember(m[1], m[2], m[3]) for m in members])
+        rc = self._lib.mcb200_batch_create(ctxs, cfg, len(members), ctypes.byref(self._b))
+        if rc != OK:
+            msg = self._lib.mcb200_batch_last_error(self._b).decode() if self._b else "no batch"
+            self.close()
+            raise EngineError(f"mcb200_batch_create failed ({rc}): {msg}")
+
+    def close(self):
+        if self._b:
+            self._lib.mcb200_batch_destroy(self._b)
+            self._b = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, what: str):
+        if rc != OK:
+            raise EngineError(f"{what} failed ({rc}): {self._lib.mcb200_batch_last_error(self._b).decode()}")
+
+    def step(self):
+        self._check(self._lib.mcb200_batch_step(self._b), "mcb200_batch_step")
+
+    def sync(self):
+        self._check(self._lib.mcb200_batch_sync(self._b), "mcb200_batch_sync")
+
+    def set_grid(self, blocks_per_sm: int):
+        self._check(self._lib.mcb200_batch_set_grid(self._b, blocks_per_sm), "mcb200_batch_set_grid")
+
+    def mark(self, slot: int):
+        self._check(self._lib.mcb200_batch_mark(self._b, slot), "mcb200_batch_mark")
+
+    def elapsed_ms(self, a: int, b: int) -> float:
+        v = ctypes.c_double()
+        self._check(self._lib.mcb200_batch_elapsed_ms(self._b, a, b, ctypes.byref(v)), "mcb200_batch_elapsed_ms")
+        return v.value
+
+    def info(self) -> dict:
+        n, st, la = ctypes.c_int(), ctypes.c_uint64(), ctypes.c_uint64()
+        self._check(self._lib.mcb200_batch_info(self._b, ctypes.byref(n), ctypes.byref(st), ctypes.byref(la)),
+                    "mcb200_batch_info")
+        return {"members": n.value, "steps": st.value, "launches": la.value}
 
 
 class Deck:

@@ -41,12 +41,14 @@ def uniform_fields(eng: Engine, field_v_per_m: float, donor_m3: float):
     return e.ravel(), (-e).ravel(), np.full(cells, donor_m3 / u["conc0"])
 
 
-def bulk_box_engine(particles: int, seed: int, device: int = 0, precision: int = FLIGHT_FP64, **overrides):
+def bulk_box_engine(particles: int, seed: int, device: int = 0, precision: int = FLIGHT_FP64, like=None,
+                    table_dir: str = DEFAULT_TABLE_DIR, **overrides):
     """Engine holding the bulk box with `particles` electrons (rounded down to
-    a multiple of the cell count).  Returns (engine, dt normalised, fields)."""
+    a multiple of the cell count); like: an engine to share band tables with.
+    Returns (engine, dt normalised, fields)."""
     box = dict(BULK_BOX, **overrides)
-    eng = Engine(table_dir=DEFAULT_TABLE_DIR, kelvin=box["kelvin"], device=device,
-                 max_particles=particles + particles // 8 + 4096, precision=precision)
+    eng = Engine(table_dir=table_dir, kelvin=box["kelvin"], device=device,
+                 max_particles=particles + particles // 8 + 4096, precision=precision, like=like)
     u = eng.units()
     nx, ny, nz = box["nx"], box["ny"], box["nz"]
     h = box["cell_nm"] * 1e-9 / u["spr0"]

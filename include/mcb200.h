@@ -77,6 +77,12 @@ typedef struct {
  * call then returns MCB200_ERR_STATE).  On failure *out may still hold a
  * context whose mcb200_last_error() says why; destroy it either way. */
 int mcb200_create(const char *table_dir, double kelvin, int device, size_t max_particles, mcb200_ctx **out);
+/* A new context on the same device with the same band tables as `like`
+ * (shared, not rebuilt or copied; they live until the last context using
+ * them is destroyed), its own stream, store of `max_particles`, mesh and
+ * tallies.  Contexts made alike can fly together in one batch.  No
+ * counterpart in the reference (one simulation per process). */
+int mcb200_create_alike(const mcb200_ctx *like, size_t max_particles, mcb200_ctx **out);
 void mcb200_destroy(mcb200_ctx *ctx);
 const char *mcb200_last_error(const mcb200_ctx *ctx);
 
@@ -255,6 +261,39 @@ int mcb200_step(mcb200_ctx *ctx, uint32_t step, uint64_t seed, double dt);
 
 /* Wait for the context's stream (and report a full store, as above). */
 int mcb200_sync(mcb200_ctx *ctx);
+
+/* ---- batches: many simulations stepped together ---------------------------
+ * No counterpart in the reference (one simulation per process).  Members
+ * are contexts made alike (mcb200_create_alike: one device, one set of band
+ * tables, one flight precision), each with its own mesh, fields, store and
+ * tallies, of any size.  mcb200_batch_step is mcb200_step for every member
+ * at once: the flights of all members run as one persistent launch over a
+ * per-member table, likewise each generation of GENERATE copies, and the
+ * rest of each member's step (copies joining the store, the cell sort) runs
+ * on the member's own stream.  Every particle draws from its own stream
+ * (seed, uid, step), so a member's result is the one mcb200_step would give
+ * it alone.  A batch step waits on the device for the work already enqueued
+ * on the members' streams and the members' later work waits for it; nothing
+ * waits on the host.  At most 64 members. */
+typedef struct mcb200_batch mcb200_batch;
+typedef struct {
+  double dt;            /* normalised time step, as mcb200_step */
+  uint64_t seed;        /* the member's random-stream key */
+  uint32_t first_step;  /* step number of the member's first batch step (+1 per batch step) */
+} mcb200_batch_member;
+int mcb200_batch_create(mcb200_ctx *const *ctxs, const mcb200_batch_member *members, int n, mcb200_batch **out);
+void mcb200_batch_destroy(mcb200_batch *batch);
+const char *mcb200_batch_last_error(const mcb200_batch *batch);
+int mcb200_batch_step(mcb200_batch *batch);
+/* Wait for the batch and every member; reports a member's full store. */
+int mcb200_batch_sync(mcb200_batch *batch);
+/* Resident blocks per SM of the batched flight launches (0: as many as fit). */
+int mcb200_batch_set_grid(mcb200_batch *batch, int blocks_per_sm);
+/* CUDA events after every member's enqueued work (mcb200_mark for a batch). */
+int mcb200_batch_mark(mcb200_batch *batch, int slot);
+int mcb200_batch_elapsed_ms(mcb200_batch *batch, int from, int to, double *ms);
+/* Members, batch steps taken, batched launches made. */
+int mcb200_batch_info(const mcb200_batch *batch, int *members, uint64_t *steps_done, uint64_t *launches);
 
 /* Device timing of mcb200_step with CUDA events on the context's own stream
  * (enable != 0 resets the accumulators and turns timing on).

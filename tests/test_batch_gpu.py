@@ -1,0 +1,111 @@
+"""Batched stepping (mcb200_batch_*): simulations of uneven size -- two
+frozen-field bulk boxes of different mesh, particle count and field, and a
+self-consistent FinFET with GENERATE / CATCH contacts whose copies go
+through every generation of the copy flights -- step together in one
+batched flight launch per step.  Each member must end bit-identical to a
+twin engine stepped alone with mcb200_step from the same state: every
+particle (matched by uid) and every tally.  Both flight precisions.
+"""
+import tempfile
+
+import numpy as np
+import pytest
+
+import mcb200
+from mcb200 import decks
+from mcb200.workloads import bulk_box_engine
+
+pytestmark = pytest.mark.gpu
+
+STEPS = 12
+POISSON_EVERY = 4
+BULK = [dict(particles=4000, seed=3, nx=10, ny=6, nz=6, field_v_per_m=1e6),
+        dict(particles=24000, seed=4, nx=20, ny=10, nz=8, field_v_per_m=5e6)]
+
+
+def finfet_engine(tmp, precision, like):
+    deck = mcb200.Deck(decks.finfet(tmp, electrons=20000, holes=3000, surface_scatter=False, compute_heat=False)
+                       ["input"])
+    eng = mcb200.Engine(table_dir=mcb200.DEFAULT_TABLE_DIR, kelvin=deck.info()["temperature"],
+                        max_particles=1 << 20, precision=precision, like=like)
+    deck.apply(eng)
+    deck.seed(eng, 11)
+    eng.deposit()
+    eng.solve_poisson(1e-10, 20000)
+    dt = deck.info()["dt"]
+    deck.close()
+    return eng, dt
+
+
+def build(tmp, precision, like=None):
+    """The three members; the first made from scratch unless `like` is given,
+    the others alike.  Returns [(engine, dt, seed, self_consistent)]."""
+    out = []
+    for spec in BULK:
+        eng, dt, _ = bulk_box_engine(spec["particles"], spec["seed"], 0, precision=precision,
+                                     like=like if like is not None else (out[0][0] if out else None),
+                                     **{k: v for k, v in spec.items() if k not in ("particles", "seed")})
+        out.append((eng, dt, 100 + spec["seed"], False))
+    eng, dt = finfet_engine(tmp, precision, out[0][0])
+    out.append((eng, dt, 200, True))
+    return out
+
+
+def density(eng, step, sc):
+    if sc:
+        eng.deposit()
+        if step % POISSON_EVERY == 0:
+            eng.solve_poisson_async(1e-10, 20000)
+
+
+def by_uid(eng):
+    d = eng.download()
+    order = np.argsort(d["uid"], kind="stable")
+    return {k: v[order] for k, v in d.items()}
+
+
+def same_tallies(a, b):
+    for k in a:
+        if isinstance(a[k], np.ndarray):
+            assert np.array_equal(a[k], b[k]), k
+        else:
+            assert a[k] == b[k], k
+
+
+@pytest.mark.parametrize("precision", [mcb200.FLIGHT_FP64, mcb200.FLIGHT_FP32])
+def test_batch_matches_members_alone(precision):
+    with tempfile.TemporaryDirectory() as t1, tempfile.TemporaryDirectory() as t2:
+        alone = build(t1, precision)
+        batched = build(t2, precision, like=alone[0][0])
+    for step in range(STEPS):
+        for eng, dt, seed, sc in alone:
+            density(eng, step, sc)
+            eng.step(step, seed, dt)
+    batch = mcb200.Batch([(eng, dt, seed, 0) for eng, dt, seed, _ in batched])
+    for step in range(STEPS):
+        for eng, _, _, sc in batched:
+            density(eng, step, sc)
+        batch.step()
+    batch.sync()
+    info = batch.info()
+    assert info["members"] == 3 and info["steps"] == STEPS and info["launches"] == STEPS * 6
+    for (ea, *_), (eb, *_) in zip(alone, batched):
+        a, b = by_uid(ea), by_uid(eb)
+        assert a["uid"].size > 0
+        for k in a:
+            assert np.array_equal(a[k], b[k]), k
+        same_tallies(ea.tallies(), eb.tallies())
+    # the FinFET member made copies, so the copy flights did work
+    assert batched[2][0].tallies()["generated"] > 0
+    batch.close()
+    for eng, *_ in batched + alone:
+        eng.close()
+
+
+def test_batch_rejects_mixed_tables():
+    a, dt, _ = bulk_box_engine(1000, 1, 0, nx=6, ny=5, nz=4)
+    b, _, _ = bulk_box_engine(1000, 2, 0, nx=6, ny=5, nz=4)  # its own tables, not alike
+    with pytest.raises(mcb200.EngineError):
+        mcb200.Batch([(a, dt, 1, 0), (b, dt, 2, 0)])
+    a.close()
+    b.close()
