@@ -14,6 +14,8 @@
 // Ordering: a batch step waits (on the device) for the work already enqueued
 // on every member's stream, and every member's later work waits for the
 // batch step, so member calls and batch steps interleave freely.
+#include <map>
+
 #include "engine_internal.h"
 
 struct mcb200_batch {
@@ -22,8 +24,19 @@ struct mcb200_batch {
   std::vector<mcb200_ctx *> m;
   std::vector<mcb200_batch_member> cfg;
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev_flight = nullptr;
+  cudaEvent_t ev_flight = nullptr, ev_fork = nullptr, ev_solved = nullptr;
   std::vector<cudaEvent_t> ev_member;
+  std::vector<uint32_t> member_step;  // host copy of each member's step number
+  // full timesteps replayed from CUDA graphs: one per (store parity, members
+  // solving Poisson), with the host-side effects of one step (launch counts)
+  bool use_graphs = false;
+  struct Graph {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<uint64_t> member_launches;
+    uint64_t batch_launches = 0;
+  };
+  std::map<std::pair<int, uint64_t>, Graph> graphs;
+  uint64_t graph_replays = 0, graph_captures = 0;
   cudaEvent_t marks[8] = {};
   void *tables = nullptr;          // device: [6][n] BatchInstT (main flight x 2 parities, 4 copy generations)
   uint32_t *steps = nullptr;       // device: step number of each member
@@ -33,9 +46,17 @@ struct mcb200_batch {
   int blocks_per_sm = 0;  // batched flight grid (0: as many as fit); mcb200_batch_autotune
   uint64_t launches = 0;
 
+  void drop_graphs() {
+    for (auto &g : graphs)
+      if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
+    graphs.clear();
+  }
   ~mcb200_batch() {
     cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
+    drop_graphs();
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_solved) cudaEventDestroy(ev_solved);
     if (tables) cudaFree(tables);
     if (steps) cudaFree(steps);
     if (tickets) cudaFree(tickets);
@@ -108,6 +129,7 @@ void build_tables(mcb200_batch *b) {
      "upload batch tables");
   ck(cudaStreamSynchronize(b->stream), "sync");
   b->built_at = b->steps_done;
+  b->drop_graphs();  // they hold the old tables' layout assumptions
 }
 
 // True when every member still has the mesh, tallies and store parity the
@@ -132,10 +154,13 @@ __global__ void advance_steps(uint32_t *steps, int n) {
   if (k < n) steps[k] += 1;
 }
 
+void join_members(mcb200_batch *b);
+
+// The transport part of a step (mcb200_step for every member): the tables
+// must be current.
 template <typename R>
-void batch_step_impl(mcb200_batch *b) {
+void batch_transport(mcb200_batch *b) {
   const int n = (int)b->m.size();
-  if (!tables_current(b)) build_tables<R>(b);
   // 1. every member: counters and records for the step, then the batch stream waits for it
   for (int k = 0; k < n; ++k) {
     mcb200_ctx *c = b->m[k];
@@ -168,6 +193,102 @@ void batch_step_impl(mcb200_batch *b) {
     step_tail<R>(c);
   }
   b->steps_done += 1;
+  for (uint32_t &st : b->member_step) ++st;
+}
+
+// Members that solve Poisson at this step (bit k).
+uint64_t poisson_due(const mcb200_batch *b) {
+  uint64_t due = 0;
+  for (size_t k = 0; k < b->m.size(); ++k) {
+    const mcb200_batch_member &m = b->cfg[k];
+    const uint32_t every = m.poisson_every > 0 ? (uint32_t)m.poisson_every : 1u;
+    if (m.self_consistent && b->m[k]->device_set && b->member_step[k] % every == 0) due |= 1ull << k;
+  }
+  return due;
+}
+
+// A full timestep of every member, as density() orders it: deposition,
+// Poisson + fields where due (solves one after another on the batch stream:
+// no two cooperative launches overlap), surface rates, then the transport
+// step.  Member streams fork from the batch stream and join it at the end,
+// so the step is one unit of work on the batch stream (and capturable).
+template <typename R>
+void batch_full_step(mcb200_batch *b, uint64_t due) {
+  const int n = (int)b->m.size();
+  ck(cudaEventRecord(b->ev_fork, b->stream), "event");
+  for (int k = 0; k < n; ++k) {
+    mcb200_ctx *c = b->m[k];
+    ck(cudaStreamWaitEvent(c->stream, b->ev_fork, 0), "wait");
+    if (b->cfg[k].self_consistent && c->device_set) deposit_enqueue(c, c->stream);
+  }
+  if (due) {
+    for (int k = 0; k < n; ++k) {
+      if (!((due >> k) & 1)) continue;
+      mcb200_ctx *c = b->m[k];
+      ck(cudaEventRecord(b->ev_member[k], c->stream), "event");
+      ck(cudaStreamWaitEvent(b->stream, b->ev_member[k], 0), "wait");
+      poisson_enqueue(c, b->stream, b->cfg[k].poisson_rel_tol > 0 ? b->cfg[k].poisson_rel_tol : 1e-10, 20000,
+                      nullptr, nullptr);
+    }
+    ck(cudaEventRecord(b->ev_solved, b->stream), "event");
+    for (int k = 0; k < n; ++k)
+      if ((due >> k) & 1) ck(cudaStreamWaitEvent(b->m[k]->stream, b->ev_solved, 0), "wait");
+  }
+  for (int k = 0; k < n; ++k) {
+    mcb200_ctx *c = b->m[k];
+    if (b->cfg[k].surface_rates && c->surf_cached) surface_rates_enqueue(c, c->stream);
+  }
+  batch_transport<R>(b);
+  join_members(b);
+}
+
+// One full timestep, replayed from (or first captured into) the graph of
+// its (store parity, Poisson members).
+template <typename R>
+void batch_graph_step(mcb200_batch *b, uint64_t due) {
+  const int n = (int)b->m.size();
+  const std::pair<int, uint64_t> key{b->m[0]->cur, due};
+  auto it = b->graphs.find(key);
+  if (it == b->graphs.end()) {
+    mcb200_batch::Graph g;
+    std::vector<uint64_t> before(n);
+    for (int k = 0; k < n; ++k) before[k] = b->m[k]->launches;
+    const uint64_t batch_before = b->launches;
+    cudaGraph_t graph = nullptr;
+    ck(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture");
+    try {
+      batch_full_step<R>(b, due);  // advances the host state by one step; the work runs at the launch below
+    } catch (...) {
+      cudaGraph_t broken = nullptr;
+      cudaStreamEndCapture(b->stream, &broken);
+      if (broken) cudaGraphDestroy(broken);
+      throw;
+    }
+    ck(cudaStreamEndCapture(b->stream, &graph), "cudaStreamEndCapture");
+    const cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    ck(e, "cudaGraphInstantiate");
+    g.member_launches.resize(n);
+    for (int k = 0; k < n; ++k) g.member_launches[k] = b->m[k]->launches - before[k];
+    g.batch_launches = b->launches - batch_before;
+    ck(cudaGraphLaunch(g.exec, b->stream), "cudaGraphLaunch");
+    b->graphs.emplace(key, std::move(g));
+    b->graph_captures += 1;
+    return;
+  }
+  ck(cudaGraphLaunch(it->second.exec, b->stream), "cudaGraphLaunch");
+  // the host-side effects of the step the graph holds
+  for (int k = 0; k < n; ++k) {
+    mcb200_ctx *c = b->m[k];
+    c->cur = 1 - c->cur;
+    c->n_stale = true;
+    c->launches += it->second.member_launches[k];
+    if (b->cfg[k].self_consistent && c->device_set) c->fields_set = true;
+  }
+  b->launches += it->second.batch_launches;
+  b->steps_done += 1;
+  for (uint32_t &st : b->member_step) ++st;
+  b->graph_replays += 1;
 }
 
 // All members' streams joined into the batch stream.
@@ -214,6 +335,8 @@ int mcb200_batch_create(mcb200_ctx *const *ctxs, const mcb200_batch_member *memb
     ck(cudaSetDevice(b->device), "cudaSetDevice");
     ck(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     ck(cudaEventCreateWithFlags(&b->ev_flight, cudaEventDisableTiming), "cudaEventCreate");
+    ck(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming), "cudaEventCreate");
+    ck(cudaEventCreateWithFlags(&b->ev_solved, cudaEventDisableTiming), "cudaEventCreate");
     b->ev_member.assign(n, nullptr);
     for (int k = 0; k < n; ++k) ck(cudaEventCreateWithFlags(&b->ev_member[k], cudaEventDisableTiming), "event");
     const size_t entry = b->precision == MCB200_FLIGHT_FP32 ? sizeof(BatchInstT<float>) : sizeof(BatchInstT<double>);
@@ -222,6 +345,7 @@ int mcb200_batch_create(mcb200_ctx *const *ctxs, const mcb200_batch_member *memb
     ck(cudaMalloc(&b->tickets, (1 + mcb200_ctx::kGenerations) * sizeof(unsigned int)), "cudaMalloc");
     std::vector<uint32_t> first_steps(n);
     for (int k = 0; k < n; ++k) first_steps[k] = members[k].first_step;
+    b->member_step = first_steps;
     ck(cudaMemcpy(b->steps, first_steps.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice), "copy");
     b->snap.assign((size_t)n * kSnapBytes, 0);
     if (b->precision == MCB200_FLIGHT_FP32) build_tables<float>(b);
@@ -249,12 +373,61 @@ int mcb200_batch_step(mcb200_batch *b) {
   }
   try {
     ck(cudaSetDevice(b->device), "cudaSetDevice");
-    if (b->precision == MCB200_FLIGHT_FP32) batch_step_impl<float>(b);
-    else batch_step_impl<double>(b);
+    if (b->precision == MCB200_FLIGHT_FP32) {
+      if (!tables_current(b)) build_tables<float>(b);
+      batch_transport<float>(b);
+    } else {
+      if (!tables_current(b)) build_tables<double>(b);
+      batch_transport<double>(b);
+    }
     return MCB200_OK;
   } catch (const std::exception &e) {
     return bfail(b, MCB200_ERR_CUDA, e.what());
   }
+}
+
+int mcb200_batch_run(mcb200_batch *b, int steps) {
+  if (!b || steps < 0) return MCB200_ERR_ARG;
+  for (size_t k = 0; k < b->m.size(); ++k) {
+    mcb200_ctx *c = b->m[k];
+    if (!c->fields_set && !(b->cfg[k].self_consistent && c->device_set))
+      return bfail(b, MCB200_ERR_STATE, "mcb200_batch_run: a member has no fields");
+    if (c->precision != b->precision)
+      return bfail(b, MCB200_ERR_STATE, "mcb200_batch_run: a member changed its flight precision");
+    if (c->overflow_pending) {
+      c->overflow_pending = false;
+      return bfail(b, MCB200_ERR_CAPACITY, "particle store of a member full: GENERATE copies were dropped");
+    }
+  }
+  try {
+    ck(cudaSetDevice(b->device), "cudaSetDevice");
+    for (int s = 0; s < steps; ++s) {
+      const uint64_t due = poisson_due(b);
+      if (b->precision == MCB200_FLIGHT_FP32) {
+        if (!tables_current(b)) build_tables<float>(b);
+        if (b->use_graphs) batch_graph_step<float>(b, due);
+        else batch_full_step<float>(b, due);
+      } else {
+        if (!tables_current(b)) build_tables<double>(b);
+        if (b->use_graphs) batch_graph_step<double>(b, due);
+        else batch_full_step<double>(b, due);
+      }
+    }
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return bfail(b, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_batch_use_graphs(mcb200_batch *b, int enable) {
+  if (!b) return MCB200_ERR_ARG;
+  b->use_graphs = enable != 0;
+  if (!b->use_graphs) {
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->stream);
+    b->drop_graphs();
+  }
+  return MCB200_OK;
 }
 
 int mcb200_batch_sync(mcb200_batch *b) {
@@ -310,11 +483,14 @@ int mcb200_batch_elapsed_ms(mcb200_batch *b, int from, int to, double *ms) {
   }
 }
 
-int mcb200_batch_info(const mcb200_batch *b, int *members, uint64_t *steps_done, uint64_t *launches) {
+int mcb200_batch_info(const mcb200_batch *b, int *members, uint64_t *steps_done, uint64_t *launches,
+                      uint64_t *graph_captures, uint64_t *graph_replays) {
   if (!b) return MCB200_ERR_ARG;
   if (members) *members = (int)b->m.size();
   if (steps_done) *steps_done = b->steps_done;
   if (launches) *launches = b->launches;
+  if (graph_captures) *graph_captures = b->graph_captures;
+  if (graph_replays) *graph_replays = b->graph_replays;
   return MCB200_OK;
 }
 

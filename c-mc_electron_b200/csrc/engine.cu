@@ -8,6 +8,8 @@
 
 #include "engine_internal.h"
 
+#include <mutex>
+
 using namespace mcb200;
 using namespace mcb200::eng;
 
@@ -600,6 +602,7 @@ int mcb200_set_mesh(mcb200_ctx *c, int nx, int ny, int nz, const double *lx, con
     c->stat_bounds = dalloc<unsigned long long>(4, c->mesh_owned);
     c->eeff_dev = dalloc<int>(cells, c->mesh_owned);
     c->eeff_host.clear();
+    c->surf_cached = false;
     c->stat_open = false;
     m.cell32 = c->cell32;
     c->hist = dalloc<unsigned int>(cells, c->mesh_owned);
@@ -1107,14 +1110,7 @@ int mcb200_deposit(mcb200_ctx *c) {
   if (!c->device_set || !c->cells_set) return fail(c, MCB200_ERR_STATE, "mcb200_deposit needs set_device and set_cells");
   try {
     ck(cudaSetDevice(c->device), "cudaSetDevice");
-    cudaStream_t s = c->stream;
-    const int grid = grid_for(c, c->capacity, 256);
-    const DevCount n{c->dev_counts, nullptr, (int)c->capacity};
-    if (c->precision == MCB200_FLIGHT_FP32) launch_deposit(store<float>(c, c->cur), n, c->mesh, c->fb, grid, s);
-    else launch_deposit(store<double>(c, c->cur), n, c->mesh, c->fb, grid, s);
-    c->launches += 5;  // charge bounds, units, particle deposit, cell and node passes
-    ck(cudaGetLastError(), "deposit");
-    c->fields_set = true;
+    deposit_enqueue(c, c->stream);
     return MCB200_OK;
   } catch (const std::exception &e) {
     return fail(c, MCB200_ERR_CUDA, e.what());
@@ -1126,18 +1122,16 @@ int mcb200_solve_poisson(mcb200_ctx *c, double rel_tol, int max_iter, int *itera
   if (!c->device_set) return fail(c, MCB200_ERR_STATE, "mcb200_solve_poisson needs mcb200_set_device");
   try {
     ck(cudaSetDevice(c->device), "cudaSetDevice");
-    cudaStream_t s = c->stream;
-    const int nodes = (c->mesh.nx + 1) * (c->mesh.ny + 1) * (c->mesh.nz + 1);
-    launch_rhs(nodes, c->fb, s);
-    if (cg_solve(c->mesh, c->fb, rel_tol, max_iter, s, c->h_scratch, iterations, rel_residual, c->cg_plan))
-      return fail(c, MCB200_ERR_CUDA, "Poisson solve failed");
-    launch_pot2field(c->mesh, c->fb.potential, s);
-    ck(cudaGetLastError(), "pot2field");
-    // rhs, the solve's set-up / dots / persistent CG / true residual /
-    // statistics (16 with Jacobi preconditioning, 13 with multigrid: no
-    // Jacobi z0 or r.z0), pot2field
-    c->launches += c->cg_plan.used == kCgMultigrid ? 15 : 18;
-    c->fields_set = true;
+    // cooperative launches of different contexts run one after another on the
+    // device (see poisson_enqueue); the chain is per device and process
+    static std::mutex chain_mutex;
+    static cudaEvent_t chain[64] = {};
+    std::lock_guard<std::mutex> lock(chain_mutex);
+    cudaEvent_t &last = chain[c->device & 63];
+    if (!last) ck(cudaEventCreateWithFlags(&last, cudaEventDisableTiming), "cudaEventCreate");
+    ck(cudaStreamWaitEvent(c->stream, last, 0), "wait");
+    poisson_enqueue(c, c->stream, rel_tol, max_iter, iterations, rel_residual);
+    ck(cudaEventRecord(last, c->stream), "event");
     return MCB200_OK;
   } catch (const std::exception &e) {
     return fail(c, MCB200_ERR_CUDA, e.what());
@@ -1209,12 +1203,9 @@ int mcb200_surface_rates(mcb200_ctx *c, const mcb200_surface_params *p, const in
       ck(cudaMemcpyAsync(c->eeff_dev, c->eeff_host.data(), sizeof(int) * c->ncells, cudaMemcpyHostToDevice, c->stream),
          "copy");
     }
-    const DevMesh &m = c->mesh;
-    launch_surface_rates(c->ncells, q, m.hfield, m.rho, c->eeff_dev, const_cast<double *>(m.e_rough),
-                         const_cast<double *>(m.e_sphon), const_cast<double *>(m.h_rough),
-                         const_cast<double *>(m.h_sphon), c->stream);
-    ck(cudaGetLastError(), "surface rates");
-    c->launches += 1;
+    c->surf_q = q;
+    c->surf_cached = true;
+    surface_rates_enqueue(c, c->stream);
     return MCB200_OK;
   } catch (const std::exception &e) {
     return fail(c, MCB200_ERR_CUDA, e.what());
@@ -1454,6 +1445,51 @@ namespace mcb200::eng {
 // One step of the store in precision R: main flight, mid-step copies
 // generation by generation, uids and append, then removal of caught
 // particles and the counting sort by cell.
+// The Poisson solve of context c on stream s: right-hand side from the last
+// deposit, CG (multigrid or Jacobi preconditioned; every iteration in one
+// cooperative launch), true residual and statistics, cell fields.  With
+// iterations and rel_residual null nothing waits for the GPU.  Two
+// cooperative launches must not run at the same time on a device (each
+// needs all its blocks resident at once, and two partly resident grids
+// could wait on each other for ever): callers enqueue solves in one order.
+void poisson_enqueue(mcb200_ctx *c, cudaStream_t s, double rel_tol, int max_iter, int *iterations,
+                     double *rel_residual) {
+  const int nodes = (c->mesh.nx + 1) * (c->mesh.ny + 1) * (c->mesh.nz + 1);
+  launch_rhs(nodes, c->fb, s);
+  if (cg_solve(c->mesh, c->fb, rel_tol, max_iter, s, c->h_scratch, iterations, rel_residual, c->cg_plan))
+    throw CudaError("Poisson solve failed");
+  launch_pot2field(c->mesh, c->fb.potential, s);
+  ck(cudaGetLastError(), "pot2field");
+  // rhs, the solve's set-up / dots / persistent CG / true residual /
+  // statistics (16 with Jacobi preconditioning, 13 with multigrid: no
+  // Jacobi z0 or r.z0), pot2field
+  c->launches += c->cg_plan.used == kCgMultigrid ? 15 : 18;
+  c->fields_set = true;
+}
+
+// Deposition of the current store (charge bounds, fixed-point units, cell
+// and node sums) on stream s; nothing waits for the GPU.
+void deposit_enqueue(mcb200_ctx *c, cudaStream_t s) {
+  const int grid = grid_for(c, c->capacity, 256);
+  const DevCount n{c->dev_counts, nullptr, (int)c->capacity};
+  if (c->precision == MCB200_FLIGHT_FP32) launch_deposit(store<float>(c, c->cur), n, c->mesh, c->fb, grid, s);
+  else launch_deposit(store<double>(c, c->cur), n, c->mesh, c->fb, grid, s);
+  c->launches += 5;  // charge bounds, units, particle deposit, cell and node passes
+  ck(cudaGetLastError(), "deposit");
+  c->fields_set = true;
+}
+
+// Surface roughness / phonon rates with the parameters of the context's last
+// mcb200_surface_rates call.
+void surface_rates_enqueue(mcb200_ctx *c, cudaStream_t s) {
+  const DevMesh &m = c->mesh;
+  launch_surface_rates(c->ncells, c->surf_q, m.hfield, m.rho, c->eeff_dev, const_cast<double *>(m.e_rough),
+                       const_cast<double *>(m.e_sphon), const_cast<double *>(m.h_rough),
+                       const_cast<double *>(m.h_sphon), s);
+  ck(cudaGetLastError(), "surface rates");
+  c->launches += 1;
+}
+
 // Before the flights of a step: work counters, the FP32 per-cell records,
 // and zeroed copy counters of every generation and of the sink.
 template <typename R>

@@ -153,6 +153,8 @@ struct mcb200_ctx {
   unsigned long long *stat_bounds = nullptr;
   int *eeff_dev = nullptr;           // surface-normal field component per cell (mcb200_surface_rates)
   std::vector<int> eeff_host;
+  bool surf_cached = false;          // surf_q holds the parameters of the last mcb200_surface_rates call
+  SurfaceRateParams surf_q{};
   int stat_steps = 0;
   bool stat_open = false;
   // device-resident counts: the step path never waits for them; `n` and
@@ -217,6 +219,10 @@ int fail(mcb200_ctx *c, int code, const std::string &msg);
 void pull_counts(mcb200_ctx *c);
 void push_counts(mcb200_ctx *c);
 int grid_for(const mcb200_ctx *c, size_t n, int block);
+void poisson_enqueue(mcb200_ctx *c, cudaStream_t s, double rel_tol, int max_iter, int *iterations,
+                     double *rel_residual);
+void surface_rates_enqueue(mcb200_ctx *c, cudaStream_t s);
+void deposit_enqueue(mcb200_ctx *c, cudaStream_t s);
 // The parts of a transport step around its flights (engine.cu).
 template <typename R>
 void step_prepare(mcb200_ctx *c);

@@ -78,7 +78,9 @@ class DeckInfo(ctypes.Structure):
 
 
 class BatchMember(ctypes.Structure):
-    _fields_ = [("dt", ctypes.c_double), ("seed", ctypes.c_uint64), ("first_step", ctypes.c_uint32)]
+    _fields_ = [("dt", ctypes.c_double), ("seed", ctypes.c_uint64), ("first_step", ctypes.c_uint32),
+                ("self_consistent", ctypes.c_int), ("poisson_every", ctypes.c_int),
+                ("poisson_rel_tol", ctypes.c_double), ("surface_rates", ctypes.c_int)]
 
 
 class RunOptions(ctypes.Structure):
@@ -121,7 +123,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mcb200_batch_set_grid.argtypes = [vp, c.c_int]
     lib.mcb200_batch_mark.argtypes = [vp, c.c_int]
     lib.mcb200_batch_elapsed_ms.argtypes = [vp, c.c_int, c.c_int, dp]
-    lib.mcb200_batch_info.argtypes = [vp, c.POINTER(c.c_int), c.POINTER(c.c_uint64), c.POINTER(c.c_uint64)]
+    lib.mcb200_batch_info.argtypes = [vp, c.POINTER(c.c_int), c.POINTER(c.c_uint64), c.POINTER(c.c_uint64),
+                                      c.POINTER(c.c_uint64), c.POINTER(c.c_uint64)]
+    lib.mcb200_batch_run.argtypes = [vp, c.c_int]
+    lib.mcb200_batch_use_graphs.argtypes = [vp, c.c_int]
     lib.mcb200_destroy.argtypes = [vp]
     lib.mcb200_destroy.restype = None
     lib.mcb200_last_error.argtypes = [vp]
@@ -454,14 +459,20 @@ class Engine:
 class Batch:
     """Engines made alike stepped together (mcb200_batch_*): one persistent
     flight launch over all members per step.  members: [(engine, dt, seed,
-    first_step)]."""
+    first_step)] or [(engine, dict of BatchMember fields)]."""
 
     def __init__(self, members):
         self._lib = lib()
         self._b = ctypes.c_void_p()
         self.engines = [m[0] for m in members]
         ctxs = (ctypes.c_void_p * len(members))(*[m[0]._ctx.value for m in members])
-        cfg = (BatchMember * len(members))(*[BatchMember(m[1], m[2], m[3]) for m in members])
+
+        def member(m):
+            if isinstance(m[1], dict):
+                return BatchMember(**m[1])
+            return BatchMember(m[1], m[2], m[3])
+
+        cfg = (BatchMember * len(members))(*[member(m) for m in members])
         rc = self._lib.mcb200_batch_create(ctxs, cfg, len(members), ctypes.byref(self._b))
         if rc != OK:
             msg = self._lib.mcb200_batch_last_error(self._b).decode() if self._b else "no batch"
@@ -486,6 +497,13 @@ class Batch:
     def step(self):
         self._check(self._lib.mcb200_batch_step(self._b), "mcb200_batch_step")
 
+    def run(self, steps: int):
+        """Full timesteps of every member (mcb200_batch_run)."""
+        self._check(self._lib.mcb200_batch_run(self._b, steps), "mcb200_batch_run")
+
+    def use_graphs(self, enable: bool = True):
+        self._check(self._lib.mcb200_batch_use_graphs(self._b, int(enable)), "mcb200_batch_use_graphs")
+
     def sync(self):
         self._check(self._lib.mcb200_batch_sync(self._b), "mcb200_batch_sync")
 
@@ -501,10 +519,11 @@ class Batch:
         return v.value
 
     def info(self) -> dict:
-        n, st, la = ctypes.c_int(), ctypes.c_uint64(), ctypes.c_uint64()
-        self._check(self._lib.mcb200_batch_info(self._b, ctypes.byref(n), ctypes.byref(st), ctypes.byref(la)),
-                    "mcb200_batch_info")
-        return {"members": n.value, "steps": st.value, "launches": la.value}
+        n, st, la, gc, gr = ctypes.c_int(), ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        self._check(self._lib.mcb200_batch_info(self._b, ctypes.byref(n), ctypes.byref(st), ctypes.byref(la),
+                                                ctypes.byref(gc), ctypes.byref(gr)), "mcb200_batch_info")
+        return {"members": n.value, "steps": st.value, "launches": la.value, "graph_captures": gc.value,
+                "graph_replays": gr.value}
 
 
 class Deck:

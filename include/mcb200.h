@@ -280,11 +280,25 @@ typedef struct {
   double dt;            /* normalised time step, as mcb200_step */
   uint64_t seed;        /* the member's random-stream key */
   uint32_t first_step;  /* step number of the member's first batch step (+1 per batch step) */
+  /* full timesteps (mcb200_batch_run) only: */
+  int self_consistent;  /* deposit every step and solve Poisson every poisson_every steps (needs set_device) */
+  int poisson_every;    /* 0: 1 (the member solves when its step number is a multiple) */
+  double poisson_rel_tol;  /* 0: 1e-10 */
+  int surface_rates;    /* recompute the surface rates every step with the member's last mcb200_surface_rates
+                           parameters */
 } mcb200_batch_member;
 int mcb200_batch_create(mcb200_ctx *const *ctxs, const mcb200_batch_member *members, int n, mcb200_batch **out);
 void mcb200_batch_destroy(mcb200_batch *batch);
 const char *mcb200_batch_last_error(const mcb200_batch *batch);
 int mcb200_batch_step(mcb200_batch *batch);
+/* `steps` full timesteps of every member, as density() orders them:
+ * deposition, Poisson + fields where due (the members' solves run one after
+ * another), surface rates, then the transport step of mcb200_batch_step.
+ * With graphs on, each step is replayed from a CUDA graph captured the first
+ * time its (store parity, solving members) occurs; graphs are dropped when
+ * a member's mesh, fields or store change outside the batch. */
+int mcb200_batch_run(mcb200_batch *batch, int steps);
+int mcb200_batch_use_graphs(mcb200_batch *batch, int enable);
 /* Wait for the batch and every member; reports a member's full store. */
 int mcb200_batch_sync(mcb200_batch *batch);
 /* Resident blocks per SM of the batched flight launches (0: as many as fit). */
@@ -292,8 +306,9 @@ int mcb200_batch_set_grid(mcb200_batch *batch, int blocks_per_sm);
 /* CUDA events after every member's enqueued work (mcb200_mark for a batch). */
 int mcb200_batch_mark(mcb200_batch *batch, int slot);
 int mcb200_batch_elapsed_ms(mcb200_batch *batch, int from, int to, double *ms);
-/* Members, batch steps taken, batched launches made. */
-int mcb200_batch_info(const mcb200_batch *batch, int *members, uint64_t *steps_done, uint64_t *launches);
+/* Members, batch steps taken, batched launches made, graphs captured and replayed. */
+int mcb200_batch_info(const mcb200_batch *batch, int *members, uint64_t *steps_done, uint64_t *launches,
+                      uint64_t *graph_captures, uint64_t *graph_replays);
 
 /* Device timing of mcb200_step with CUDA events on the context's own stream
  * (enable != 0 resets the accumulators and turns timing on).

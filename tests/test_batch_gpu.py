@@ -3,8 +3,11 @@ frozen-field bulk boxes of different mesh, particle count and field, and a
 self-consistent FinFET with GENERATE / CATCH contacts whose copies go
 through every generation of the copy flights -- step together in one
 batched flight launch per step.  Each member must end bit-identical to a
-twin engine stepped alone with mcb200_step from the same state: every
-particle (matched by uid) and every tally.  Both flight precisions.
+twin engine stepped alone (mcb200_deposit / mcb200_solve_poisson /
+mcb200_step) from the same state: every particle (matched by uid), every
+tally and the potential.  Both flight precisions; transport steps with the
+host's own density calls, and full timesteps run by the batch, with and
+without CUDA graphs.
 """
 import tempfile
 
@@ -97,6 +100,41 @@ def test_batch_matches_members_alone(precision):
         same_tallies(ea.tallies(), eb.tallies())
     # the FinFET member made copies, so the copy flights did work
     assert batched[2][0].tallies()["generated"] > 0
+    batch.close()
+    for eng, *_ in batched + alone:
+        eng.close()
+
+
+@pytest.mark.parametrize("precision,graphs", [(mcb200.FLIGHT_FP64, False), (mcb200.FLIGHT_FP64, True),
+                                              (mcb200.FLIGHT_FP32, True)])
+def test_batch_run_matches_members_alone(precision, graphs):
+    with tempfile.TemporaryDirectory() as t1, tempfile.TemporaryDirectory() as t2:
+        alone = build(t1, precision)
+        batched = build(t2, precision, like=alone[0][0])
+    first = [0, 3, 5]  # members start at different step numbers: different Poisson phases
+    for step in range(STEPS):
+        for (eng, dt, seed, sc), f in zip(alone, first):
+            density(eng, f + step, sc)
+            eng.step(f + step, seed, dt)
+    batch = mcb200.Batch([(eng, dict(dt=dt, seed=seed, first_step=f, self_consistent=int(sc),
+                                      poisson_every=POISSON_EVERY))
+                          for (eng, dt, seed, sc), f in zip(batched, first)])
+    batch.use_graphs(graphs)
+    batch.run(STEPS // 2)
+    batch.run(STEPS - STEPS // 2)
+    batch.sync()
+    info = batch.info()
+    assert info["steps"] == STEPS and info["launches"] == STEPS * 6
+    if graphs:
+        assert info["graph_captures"] >= 2 and info["graph_captures"] + info["graph_replays"] == STEPS
+    for (ea, *_), (eb, *_) in zip(alone, batched):
+        a, b = by_uid(ea), by_uid(eb)
+        for k in a:
+            assert np.array_equal(a[k], b[k]), k
+        same_tallies(ea.tallies(), eb.tallies())
+    pa, pb = alone[2][0].array("potential"), batched[2][0].array("potential")
+    assert np.array_equal(pa.view(np.uint64), pb.view(np.uint64))
+    assert alone[2][0].poisson_stats() == batched[2][0].poisson_stats()
     batch.close()
     for eng, *_ in batched + alone:
         eng.close()
