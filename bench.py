@@ -275,6 +275,64 @@ def engine_arm(args, rank: int, world: int, device: int):
     }
 
 
+# ------------------------------------------------------------ batching
+BATCH_MEMBERS = 64
+BATCH_STEPS = 40
+
+
+def batch_arm(args, device: int) -> dict:
+    """Many simulations at once: 64 seeded members, half frozen-field bulk
+    boxes (20^3 to 80x40x50 cells, E_x 1-100 kV/cm), half self-consistent
+    FinFETs (Lg 15/20/30 nm, Vg 0-0.8 V), particle counts log-uniform in
+    5k-500k, FP32 flight.  Full timesteps through the batch (one flight
+    launch per step for all members, steps replayed from CUDA graphs, launch
+    shapes from the autotuner) against the same members stepped one by one
+    on their own streams.  Device time between batch marks (every member's
+    stream joined), particle-steps from the members' device counters."""
+    import mcb200
+    from mcb200 import batching
+
+    t0 = time.perf_counter()
+    members, root = batching.build_mix(n=BATCH_MEMBERS, seed=4, precision=mcb200.FLIGHT_FP32)
+    setup_s = time.perf_counter() - t0
+    batch = mcb200.Batch([(m.eng, m.cfg) for m in members])
+    batch.use_graphs(True)
+    s0 = batch.info()["steps"]
+    tune = batch.autotune(10)
+    for m in members:
+        m.step += batch.info()["steps"] - s0
+
+    def timed(run):
+        run(10)  # warm-up
+        ps0 = batching.particle_steps(members)
+        batch.mark(0)
+        run(BATCH_STEPS)
+        batch.mark(1)
+        ms = batch.elapsed_ms(0, 1)
+        return (batching.particle_steps(members) - ps0) / (ms * 1e-3), ms / BATCH_STEPS
+
+    with ClockSampler(device) as clocks:
+        batched, ms_b = timed(lambda k: batching.run_batched(batch, members, k))
+        alone, ms_a = timed(lambda k: batching.run_alone(members, k))
+    info = batch.info()
+    kinds = [m.kind for m in members]
+    out = {"metric": "particle-steps/s", "members": len(members), "bulk": kinds.count("bulk"),
+           "finfet": kinds.count("finfet"), "particles": int(sum(m.desc["particles"] for m in members)),
+           "value": batched, "ms_per_step": ms_b, "unbatched_value": alone, "unbatched_ms_per_step": ms_a,
+           "batched_over_unbatched": batched / alone, "steps": BATCH_STEPS, "autotune": tune,
+           "graph_captures": info["graph_captures"], "graph_replays": info["graph_replays"],
+           "setup_s": setup_s, "clocks": clocks.summary(), "dtype": "f32", "data": "synthetic",
+           "config": "64 members (seed 4): bulk n-Si boxes 20^3-80x40x50 cells, E_x U[1,100] kV/cm, and "
+                     "self-consistent n-FinFETs Lg {15,20,30} nm, Vg U[0,0.8] V, Vd 0.7 V, surface scattering, "
+                     "Poisson every 10 steps (staggered), MultipleRefresh every 50; N log-uniform 5k-500k "
+                     "(FinFETs at least one electron per silicon cell); working set > L2"}
+    batch.close()
+    for m in members:
+        m.eng.close()
+    root.close()
+    return out
+
+
 # ------------------------------------------------------------ reference (CPU)
 def _oracle_sample(args):
     """One CPU process: the reference's routines on a reduced FinFET deck
@@ -390,16 +448,21 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--particles", type=int, default=2_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="all", choices=["all", "finfet"],
-                    help="finfet: only the two FinFET arms (no e2e rerun, no bulk box): for profiling")
+    ap.add_argument("--workload", default="all", choices=["all", "finfet", "batch"],
+                    help="finfet: only the two FinFET arms (no e2e rerun, no bulk box): for profiling; "
+                         "batch: only the batching arm")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     rank, world, local = dist_init()
     if args.impl == "reference":
         out = reference_arm(args, rank, world)
+    elif args.workload == "batch":
+        out = batch_arm(args, local)
     else:
         out = engine_arm(args, rank, world, local)
+        if args.workload == "all":
+            out["batch"] = batch_arm(args, local)
         if rank == 0 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline()
     if rank == 0 and out is not None:

@@ -242,6 +242,16 @@ void batch_full_step(mcb200_batch *b, uint64_t due) {
   join_members(b);
 }
 
+// A graph step on the batch stream, ordered with the members' own streams:
+// it follows the work already enqueued on them, and their later work (a
+// refresh, a download) follows it.
+void launch_graph(mcb200_batch *b, cudaGraphExec_t exec) {
+  join_members(b);
+  ck(cudaGraphLaunch(exec, b->stream), "cudaGraphLaunch");
+  ck(cudaEventRecord(b->ev_flight, b->stream), "event");
+  for (mcb200_ctx *c : b->m) ck(cudaStreamWaitEvent(c->stream, b->ev_flight, 0), "wait");
+}
+
 // One full timestep, replayed from (or first captured into) the graph of
 // its (store parity, Poisson members).
 template <typename R>
@@ -271,12 +281,12 @@ void batch_graph_step(mcb200_batch *b, uint64_t due) {
     g.member_launches.resize(n);
     for (int k = 0; k < n; ++k) g.member_launches[k] = b->m[k]->launches - before[k];
     g.batch_launches = b->launches - batch_before;
-    ck(cudaGraphLaunch(g.exec, b->stream), "cudaGraphLaunch");
+    launch_graph(b, g.exec);
     b->graphs.emplace(key, std::move(g));
     b->graph_captures += 1;
     return;
   }
-  ck(cudaGraphLaunch(it->second.exec, b->stream), "cudaGraphLaunch");
+  launch_graph(b, it->second.exec);
   // the host-side effects of the step the graph holds
   for (int k = 0; k < n; ++k) {
     mcb200_ctx *c = b->m[k];
@@ -417,6 +427,41 @@ int mcb200_batch_run(mcb200_batch *b, int steps) {
   } catch (const std::exception &e) {
     return bfail(b, MCB200_ERR_CUDA, e.what());
   }
+}
+
+int mcb200_batch_autotune(mcb200_batch *b, int trial_steps, mcb200_batch_tuning *best) {
+  if (!b || trial_steps < 1) return MCB200_ERR_ARG;
+  static const int flight_blocks[] = {1, 2};
+  static const int grid_per_sm[] = {2, 4, 8};
+  mcb200_batch_tuning win{0, 0, 0, 1e300, 0};
+  int tried = 0;
+  for (int fb : flight_blocks)
+    for (int gs : grid_per_sm) {
+      b->blocks_per_sm = fb;
+      for (mcb200_ctx *c : b->m) c->grid_per_sm = gs;
+      {
+        cudaSetDevice(b->device);
+        cudaStreamSynchronize(b->stream);
+        b->drop_graphs();  // the graphs hold the previous grids
+      }
+      // one untimed step (it captures the graphs of this setting), then the timed ones
+      if (int rc = mcb200_batch_run(b, 1)) return rc;
+      if (int rc = mcb200_batch_mark(b, 6)) return rc;
+      if (int rc = mcb200_batch_run(b, trial_steps)) return rc;
+      if (int rc = mcb200_batch_mark(b, 7)) return rc;
+      double ms = 0;
+      if (int rc = mcb200_batch_elapsed_ms(b, 6, 7, &ms)) return rc;
+      ms /= trial_steps;
+      ++tried;
+      if (ms < win.ms_per_step) win = mcb200_batch_tuning{fb, gs, 0, ms, 0};
+    }
+  win.candidates = tried;
+  b->blocks_per_sm = win.flight_blocks_per_sm;
+  for (mcb200_ctx *c : b->m) c->grid_per_sm = win.grid_per_sm;
+  cudaStreamSynchronize(b->stream);
+  b->drop_graphs();
+  if (best) *best = win;
+  return MCB200_OK;
 }
 
 int mcb200_batch_use_graphs(mcb200_batch *b, int enable) {

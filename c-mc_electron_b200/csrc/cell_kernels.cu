@@ -130,13 +130,13 @@ __global__ void refresh_count_kernel(DevParticlesT<R> P, const unsigned int *cel
 template <typename R>
 __global__ void refresh_emit_kernel(DevParticlesT<R> P, const unsigned int *cell_end, const unsigned int *cell_count,
                                     int cells, const int *desired_e, const int *desired_h, RefreshParams r,
-                                    const unsigned int *out_offset, const unsigned int *uid_offset, uint32_t uid0,
-                                    DevParticlesT<R> dst, unsigned long long *mr_gen) {
+                                    const unsigned int *out_offset, const unsigned int *uid_offset,
+                                    const unsigned int *uid0p, DevParticlesT<R> dst, unsigned long long *mr_gen) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= cells) return;
   const int e = (int)cell_end[c], b = e - (int)cell_count[c];
   unsigned int o = out_offset[c];
-  uint32_t uid = uid0 + uid_offset[c];
+  uint32_t uid = *uid0p + uid_offset[c];
   auto copy = [&](int from, unsigned int to) {
     dst.x[to] = P.x[from]; dst.y[to] = P.y[from]; dst.z[to] = P.z[from];
     dst.kx[to] = P.kx[from]; dst.ky[to] = P.ky[from]; dst.kz[to] = P.kz[from];
@@ -197,7 +197,7 @@ void launch_refresh_count(const DevParticlesT<R> &P, const unsigned int *cell_en
 template <typename R>
 void launch_refresh_emit(const DevParticlesT<R> &P, const unsigned int *cell_end, const unsigned int *cell_count,
                          int cells, const int *desired_e, const int *desired_h, const RefreshParams &r,
-                         const unsigned int *out_offset, const unsigned int *uid_offset, uint32_t uid0,
+                         const unsigned int *out_offset, const unsigned int *uid_offset, const unsigned int *uid0,
                          const DevParticlesT<R> &dst, unsigned long long *mr_gen, cudaStream_t s) {
   refresh_emit_kernel<R><<<(cells + 127) / 128, 128, 0, s>>>(P, cell_end, cell_count, cells, desired_e, desired_h, r,
                                                           out_offset, uid_offset, uid0, dst, mr_gen);
@@ -209,7 +209,7 @@ void launch_refresh_emit(const DevParticlesT<R> &P, const unsigned int *cell_end
                                         unsigned int *, cudaStream_t);                                        \
   template void launch_refresh_emit<R>(const DevParticlesT<R> &, const unsigned int *, const unsigned int *,  \
                                        int, const int *, const int *, const RefreshParams &,                 \
-                                       const unsigned int *, const unsigned int *, uint32_t,                 \
+                                       const unsigned int *, const unsigned int *, const unsigned int *,                 \
                                        const DevParticlesT<R> &, unsigned long long *, cudaStream_t);
 MCB200_INSTANTIATE(double)
 MCB200_INSTANTIATE(float)

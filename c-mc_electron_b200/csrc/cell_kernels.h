@@ -36,10 +36,11 @@ template <typename R>
 void launch_refresh_count(const DevParticlesT<R> &P, const unsigned int *cell_end, const unsigned int *cell_count,
                           int cells, const int *desired_e, const int *desired_h, const RefreshParams &r,
                           unsigned int *out_count, unsigned int *new_count, cudaStream_t s);
+// uid0: device word holding the first new uid (the context's uid counter).
 template <typename R>
 void launch_refresh_emit(const DevParticlesT<R> &P, const unsigned int *cell_end, const unsigned int *cell_count,
                          int cells, const int *desired_e, const int *desired_h, const RefreshParams &r,
-                         const unsigned int *out_offset, const unsigned int *uid_offset, uint32_t uid0,
+                         const unsigned int *out_offset, const unsigned int *uid_offset, const unsigned int *uid0,
                          const DevParticlesT<R> &dst, unsigned long long *mr_gen, cudaStream_t s);
 
 }  // namespace mcb200

@@ -20,6 +20,15 @@ int fail(mcb200_ctx *c, int code, const std::string &msg) {
   return code;
 }
 
+// After a refresh: the particle count is the emitted total, the uid counter
+// advances past the new particles (tot = {emitted, new uids}).
+__global__ void refresh_counts_kernel(unsigned int *d, const unsigned int *tot) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    d[0] = tot[0];
+    d[1] += tot[1];
+  }
+}
+
 __global__ void set_counts_kernel(unsigned int *d, unsigned int n, unsigned int next_uid) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     d[0] = n;
@@ -315,13 +324,14 @@ void copy_vec(const std::vector<T> &v, void *out, size_t bytes, size_t *needed) 
 
 int grid_for(const mcb200_ctx *c, size_t n, int block) {
   const size_t want = (n + block - 1) / block;
-  const size_t cap = (size_t)c->sm_count * 8;
+  const size_t cap = (size_t)c->sm_count * (size_t)c->grid_per_sm;
   return (int)std::max<size_t>(1, std::min(want, cap));
 }
 
 void free_mesh(mcb200_ctx *c) {
   for (void *p : c->mesh_owned) cudaFree(p);
   c->mesh_owned.clear();
+  c->mr = MrScratch{};
 }
 
 // Host particles (absolute FP64 positions) into store 0 of precision R;
@@ -1218,18 +1228,29 @@ int mcb200_multiple_refresh(mcb200_ctx *c, const int32_t *desired_e, const int32
   if (!c->mesh_set) return fail(c, MCB200_ERR_STATE, "mcb200_multiple_refresh before mcb200_set_mesh");
   try {
     ck(cudaSetDevice(c->device), "cudaSetDevice");
-    pull_counts(c);
     cudaStream_t s = c->stream;
     const int cells = c->ncells;
     size_t want = 0;
     for (int q = 0; q < cells; ++q) want += (size_t)std::max(desired_e[q], 0) + (size_t)std::max(desired_h[q], 0);
     if (want > c->capacity) return fail(c, MCB200_ERR_CAPACITY, "refresh targets exceed the particle capacity");
-    std::vector<void *> tmp;
-    int *de = dalloc<int>(cells, tmp), *dh = dalloc<int>(cells, tmp);
-    unsigned int *out_count = dalloc<unsigned int>(cells, tmp), *new_count = dalloc<unsigned int>(cells, tmp);
-    unsigned int *out_off = dalloc<unsigned int>(cells, tmp), *uid_off = dalloc<unsigned int>(cells, tmp);
-    unsigned int *tiles = dalloc<unsigned int>((cells + 1023) / 1024 + 1, tmp), *tot = dalloc<unsigned int>(2, tmp);
-    unsigned long long *gen = dalloc<unsigned long long>(1, tmp);
+    // scratch allocated with the mesh on first use (no device-wide cudaFree per refresh)
+    MrScratch &w = c->mr;
+    if (w.cells != cells) {
+      w.de = dalloc<int>(cells, c->mesh_owned);
+      w.dh = dalloc<int>(cells, c->mesh_owned);
+      w.out_count = dalloc<unsigned int>(cells, c->mesh_owned);
+      w.new_count = dalloc<unsigned int>(cells, c->mesh_owned);
+      w.out_off = dalloc<unsigned int>(cells, c->mesh_owned);
+      w.uid_off = dalloc<unsigned int>(cells, c->mesh_owned);
+      w.tiles = dalloc<unsigned int>((cells + 1023) / 1024 + 1, c->mesh_owned);
+      w.tot = dalloc<unsigned int>(2, c->mesh_owned);
+      w.gen = dalloc<unsigned long long>(1, c->mesh_owned);
+      w.cells = cells;
+    }
+    int *de = w.de, *dh = w.dh;
+    unsigned int *out_count = w.out_count, *new_count = w.new_count, *out_off = w.out_off, *uid_off = w.uid_off;
+    unsigned int *tiles = w.tiles, *tot = w.tot;
+    unsigned long long *gen = w.gen;
     ck(cudaMemcpyAsync(de, desired_e, sizeof(int) * cells, cudaMemcpyHostToDevice, s), "copy");
     ck(cudaMemcpyAsync(dh, desired_h, sizeof(int) * cells, cudaMemcpyHostToDevice, s), "copy");
     ck(cudaMemsetAsync(gen, 0, sizeof(unsigned long long), s), "memset");
@@ -1239,31 +1260,29 @@ int mcb200_multiple_refresh(mcb200_ctx *c, const int32_t *desired_e, const int32
     const RefreshParams r{seed, step, 2.0, 2.0, 1.0e-30};  // Rpar, Rsqr, pckill: src/mcmodel.cpp:3878-3880
     auto refresh = [&](auto tag) {
       using R = decltype(tag);
-      launch_cell_sort(store<R>(c, c->cur), DevCount{nullptr, nullptr, (int)c->n}, store<R>(c, sorted), cells,
-                       c->mesh.nx, c->mesh.nz, c->hist, c->offsets, c->tile_sums, c->total,
-                       grid_for(c, c->n, 256), s);
+      launch_cell_sort(store<R>(c, c->cur), DevCount{c->dev_counts, nullptr, (int)c->capacity}, store<R>(c, sorted),
+                       cells, c->mesh.nx, c->mesh.nz, c->hist, c->offsets, c->tile_sums, c->total,
+                       grid_for(c, c->capacity, 256), s);
       const DevParticlesT<R> &P = store<R>(c, sorted);
       launch_refresh_count(P, c->offsets, c->hist, cells, de, dh, r, out_count, new_count, s);
       launch_exclusive_scan(out_count, out_off, tiles, tot, cells, s);
       launch_exclusive_scan(new_count, uid_off, tiles, tot + 1, cells, s);
-      launch_refresh_emit(P, c->offsets, c->hist, cells, de, dh, r, out_off, uid_off, c->next_uid, store<R>(c, other),
-                          gen, s);
+      launch_refresh_emit(P, c->offsets, c->hist, cells, de, dh, r, out_off, uid_off, c->dev_counts + 1,
+                          store<R>(c, other), gen, s);
     };
     if (c->precision == MCB200_FLIGHT_FP32) refresh(float{});
     else refresh(double{});
-    c->launches += 13;  // cell sort, count, two scans, emit, count update
+    // the refreshed population's size and the uid counter, on the device
+    refresh_counts_kernel<<<1, 32, 0, s>>>(c->dev_counts, tot);
+    c->launches += 14;  // cell sort, count, two scans, emit, counts
     ck(cudaGetLastError(), "refresh");
-    unsigned int totals[2];
-    long long g = 0;
-    ck(cudaMemcpyAsync(totals, tot, sizeof(totals), cudaMemcpyDeviceToHost, s), "copy");
-    ck(cudaMemcpyAsync(&g, gen, sizeof(g), cudaMemcpyDeviceToHost, s), "copy");
-    ck(cudaStreamSynchronize(s), "sync");
-    for (void *q : tmp) cudaFree(q);
     c->cur = other;
-    c->n = totals[0];
-    c->next_uid += totals[1];
-    push_counts(c);
-    if (generated) *generated = g;
+    c->n_stale = true;
+    if (generated) {  // the only result that needs the host to wait
+      ck(cudaMemcpyAsync(c->h_scratch + 13, gen, sizeof(long long), cudaMemcpyDeviceToHost, s), "copy");
+      ck(cudaStreamSynchronize(s), "sync");
+      std::memcpy(generated, c->h_scratch + 13, sizeof(long long));
+    }
     return MCB200_OK;
   } catch (const CapacityError &e) {
     return fail(c, MCB200_ERR_CAPACITY, e.what());

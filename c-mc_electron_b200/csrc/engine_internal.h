@@ -85,6 +85,15 @@ struct ChildBuffers {
   DevChildrenT<float> f{};
 };
 
+// MultipleRefresh scratch, sized for the mesh (mcb200_multiple_refresh).
+struct MrScratch {
+  int cells = 0;
+  int *de = nullptr, *dh = nullptr;
+  unsigned int *out_count = nullptr, *new_count = nullptr, *out_off = nullptr, *uid_off = nullptr;
+  unsigned int *tiles = nullptr, *tot = nullptr;
+  unsigned long long *gen = nullptr;
+};
+
 // Band tables on the host and the device (mcb200_create): built once and
 // shared by every context created alike (mcb200_create_alike).
 struct TableSet {
@@ -139,7 +148,9 @@ struct mcb200_ctx {
   unsigned int *hist = nullptr, *offsets = nullptr, *tile_sums = nullptr, *total = nullptr;
   int ncells = 0;
   unsigned int *h_pinned = nullptr;  // small pinned readback area
+  MrScratch mr;                      // in mesh_owned
   int sm_count = 148;
+  int grid_per_sm = 8;  // blocks per SM of the grid-stride per-step kernels (sort, deposition, copies)
   // deposition / Poisson (mcb200_set_device)
   FieldBuffers fb{};
   CgPlan cg_plan;

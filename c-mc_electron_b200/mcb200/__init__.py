@@ -83,6 +83,11 @@ class BatchMember(ctypes.Structure):
                 ("poisson_rel_tol", ctypes.c_double), ("surface_rates", ctypes.c_int)]
 
 
+class BatchTuning(ctypes.Structure):
+    _fields_ = [("flight_blocks_per_sm", ctypes.c_int), ("grid_per_sm", ctypes.c_int), ("reserved", ctypes.c_int),
+                ("ms_per_step", ctypes.c_double), ("candidates", ctypes.c_int)]
+
+
 class RunOptions(ctypes.Structure):
     _fields_ = [("table_dir", ctypes.c_char_p), ("data_dir", ctypes.c_char_p), ("flight_precision", ctypes.c_int),
                 ("poisson_every", ctypes.c_int), ("poisson_rel_tol", ctypes.c_double), ("max_steps", ctypes.c_int),
@@ -126,6 +131,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mcb200_batch_info.argtypes = [vp, c.POINTER(c.c_int), c.POINTER(c.c_uint64), c.POINTER(c.c_uint64),
                                       c.POINTER(c.c_uint64), c.POINTER(c.c_uint64)]
     lib.mcb200_batch_run.argtypes = [vp, c.c_int]
+    lib.mcb200_batch_autotune.argtypes = [vp, c.c_int, c.POINTER(BatchTuning)]
     lib.mcb200_batch_use_graphs.argtypes = [vp, c.c_int]
     lib.mcb200_destroy.argtypes = [vp]
     lib.mcb200_destroy.restype = None
@@ -309,12 +315,15 @@ class Engine:
         self._check(self._lib.mcb200_surface_rates(self._ctx, ctypes.byref(sp), _ptr(d, ctypes.c_int32)),
                     "surface_rates")
 
-    def multiple_refresh(self, desired_e, desired_h, step: int, seed: int) -> int:
+    def multiple_refresh(self, desired_e, desired_h, step: int, seed: int, wait: bool = True):
+        """MultipleRefresh; returns the change in particle count, or None
+        without waiting for the GPU (wait=False)."""
         de, dh = (np.ascontiguousarray(a, dtype=np.int32) for a in (desired_e, desired_h))
         gen = ctypes.c_int64()
         self._check(self._lib.mcb200_multiple_refresh(self._ctx, _ptr(de, ctypes.c_int32), _ptr(dh, ctypes.c_int32),
-                                                      step, seed, ctypes.byref(gen)), "multiple_refresh")
-        return gen.value
+                                                      step, seed, ctypes.byref(gen) if wait else None),
+                    "multiple_refresh")
+        return gen.value if wait else None
 
     def deposit(self):
         self._check(self._lib.mcb200_deposit(self._ctx), "deposit")
@@ -500,6 +509,13 @@ class Batch:
     def run(self, steps: int):
         """Full timesteps of every member (mcb200_batch_run)."""
         self._check(self._lib.mcb200_batch_run(self._b, steps), "mcb200_batch_run")
+
+    def autotune(self, trial_steps: int) -> dict:
+        """Launch shapes picked by timing real steps (mcb200_batch_autotune)."""
+        t = BatchTuning()
+        self._check(self._lib.mcb200_batch_autotune(self._b, trial_steps, ctypes.byref(t)), "mcb200_batch_autotune")
+        return {"flight_blocks_per_sm": t.flight_blocks_per_sm, "grid_per_sm": t.grid_per_sm,
+                "ms_per_step": t.ms_per_step, "candidates": t.candidates}
 
     def use_graphs(self, enable: bool = True):
         self._check(self._lib.mcb200_batch_use_graphs(self._b, int(enable)), "mcb200_batch_use_graphs")

@@ -108,15 +108,17 @@ def bulk_box(dirpath: str, nx=40, ny=20, nz=20, cell_nm=5.0, donor_m3=1e23, elec
                 device=os.path.join(dirpath, "ldg.txt"))
 
 
-def finfet_grid():
-    """Node coordinates (nm) of the FinFET mesh: 80 x 50 x 40 cells.
-    x (height): 1 nm gate oxide in 0.5 nm cells, the 30 nm fin in 0.5 nm
-    cells, the substrate in 2 nm cells; y (transport): 10 nm source and
-    drain in 2 nm cells, the 20 nm channel in 0.5 nm cells; z (width): the
-    10 nm fin and its 1 nm oxides in 0.5 nm cells, 16 nm either side in 2 nm
-    cells."""
+def finfet_grid(lg_nm: float = 20.0):
+    """Node coordinates (nm) of the FinFET mesh: 80 x (30 + 2 lg_nm) x 40
+    cells (80 x 50 x 40 at the 20 nm gate).  x (height): 1 nm gate oxide in
+    0.5 nm cells, the 30 nm fin in 0.5 nm cells, the substrate in 2 nm cells;
+    y (transport): 10 nm source and drain in 2 nm cells, the channel of
+    length lg_nm in 0.5 nm cells; z (width): the 10 nm fin and its 1 nm
+    oxides in 0.5 nm cells, 16 nm either side in 2 nm cells."""
+    h = lg_nm / 2.0
+    e = h + 10.0
     x = np.concatenate([[-1.0, -0.5], np.arange(0.0, 30.0001, 0.5), np.arange(32.0, 66.0001, 2.0)])
-    y = np.concatenate([np.arange(-20.0, -10.0, 2.0), np.arange(-10.0, 10.0001, 0.5), np.arange(12.0, 20.0001, 2.0)])
+    y = np.concatenate([np.arange(-e, -h - 1e-9, 2.0), np.arange(-h, h + 1e-4, 0.5), np.arange(h + 2.0, e + 1e-4, 2.0)])
     z = np.concatenate([np.arange(-17.0, -1.0, 2.0), [-1.0, -0.5], np.arange(0.0, 10.0001, 0.5), [10.5, 11.0],
                         np.arange(13.0, 27.0001, 2.0)])
     return x, y, z
@@ -124,80 +126,87 @@ def finfet_grid():
 
 def finfet(dirpath: str, electrons=300000, holes=50000, vd=0.7, vg=0.8, phims=-0.46, dt=2e-16, total_step=7000,
            heat_steps=3000, stat_step=1000, mr_step=50, surface_scatter=True, compute_heat=True,
-           delta_nm=0.4, lambda_nm=1.5, kelvin=300.0) -> dict:
+           delta_nm=0.4, lambda_nm=1.5, kelvin=300.0, lg_nm=20.0, min_per_cell=(3, 1)) -> dict:
     """The n-FinFET of the self-consistent workload, in the reference's deck
     language and with the reference FinFET's topology (finfet/ldg.txt):
-    fin 30 nm tall (x) and 10 nm wide (z), gate length 20 nm (y), 1 nm SiO2
-    on the top and both sides of the gated fin, oxide beside the fin's foot,
-    a silicon substrate below; source / drain 1e20 cm^-3 donors rolling off
-    at 2 nm per decade into a 1e15 cm^-3 p-type channel as 0.5 nm stair-step
-    donor boxes; CATCH / GENERATE planes one cell inside the source, drain
-    and substrate contacts, REFLECT at the fin ends, SCATTOX on every
-    Si/SiO2 or outer face; contacts: source 0 V, drain vd, substrate 0 V,
-    a three-plane gate at vg with work-function difference phims.  Doping
-    values are in m^-3 as the reference reads them.  The surface-roughness
-    parameters go to input.txt as surface_roughness_delta_nm /
-    surface_roughness_lambda_nm (keys the reference does not read)."""
+    fin 30 nm tall (x) and 10 nm wide (z), gate length lg_nm (y; 20 nm by
+    default), 1 nm SiO2 on the top and both sides of the gated fin, oxide
+    beside the fin's foot, a silicon substrate below; source / drain 1e20
+    cm^-3 donors rolling off at 2 nm per decade into a 1e15 cm^-3 p-type
+    channel as 0.5 nm stair-step donor boxes; CATCH / GENERATE planes one
+    cell inside the source, drain and substrate contacts, REFLECT at the fin
+    ends, SCATTOX on every Si/SiO2 or outer face; contacts: source 0 V,
+    drain vd, substrate 0 V, a three-plane gate at vg with work-function
+    difference phims.  min_per_cell: the fewest electrons / holes of a
+    silicon cell (default_par_number).  Doping values are in m^-3 as the
+    reference reads them.  The surface-roughness parameters go to input.txt
+    as surface_roughness_delta_nm / surface_roughness_lambda_nm (keys the
+    reference does not read)."""
     os.makedirs(dirpath, exist_ok=True)
-    x, y, z = finfet_grid()
+    x, y, z = finfet_grid(lg_nm)
     write_grid(os.path.join(dirpath, "lgrid.txt"), x, y, z)
     g = lambda v: f"{v:g}"
+    h = lg_nm / 2.0
+    e = h + 10.0
+    Y = f"{g(-e)} {g(e)}"
     L = [
-        "default_par_number 3 1",
-        "region -1 66 -20 20 -17 27 VACUUM",
-        "region 0 30 -20 20 0 10 SILICON",
-        "region 30 66 -20 20 -17 27 SILICON",
-        "region -1 0 -20 20 -1 11 OXIDE",
-        "region 0 24 -20 20 -1 0 OXIDE",
-        "region 0 24 -20 20 10 11 OXIDE",
-        "region 24 30 -20 20 -17 0 OXIDE",
-        "region 24 30 -20 20 10 27 OXIDE",
-        "donor -1 66 -20 20 -17 27 0",
-        "donor 0 24 -20 -10 0 10 1e+26",
-        "donor 0 24 10 20 0 10 1e+26",
+        f"default_par_number {min_per_cell[0]} {min_per_cell[1]}",
+        f"region -1 66 {Y} -17 27 VACUUM",
+        f"region 0 30 {Y} 0 10 SILICON",
+        f"region 30 66 {Y} -17 27 SILICON",
+        f"region -1 0 {Y} -1 11 OXIDE",
+        f"region 0 24 {Y} -1 0 OXIDE",
+        f"region 0 24 {Y} 10 11 OXIDE",
+        f"region 24 30 {Y} -17 0 OXIDE",
+        f"region 24 30 {Y} 10 27 OXIDE",
+        f"donor -1 66 {Y} -17 27 0",
+        f"donor 0 24 {g(-e)} {g(-h)} 0 10 1e+26",
+        f"donor 0 24 {g(h)} {g(e)} 0 10 1e+26",
     ]
-    for s_ in range(20):  # 2 nm / decade roll-off on the 0.5 nm channel grid
+    for s_ in range(int(round(h / 0.5))):  # 2 nm / decade roll-off on the 0.5 nm channel grid
         conc = 1e26 * 10.0 ** (-(0.5 * s_ + 0.25) / 2.0)
-        y0, y1 = -10.0 + 0.5 * s_, -10.0 + 0.5 * (s_ + 1)
+        y0, y1 = -h + 0.5 * s_, -h + 0.5 * (s_ + 1)
         L.append(f"donor 0 24 {g(y0)} {g(y1)} 0 10 {conc:.6g}")
         L.append(f"donor 0 24 {g(-y1)} {g(-y0)} 0 10 {conc:.6g}")
+    c, r = e - 2.0, e - 4.0  # CATCH / GENERATE planes; contact-attached range
     L += [
-        "acceptor -1 66 -20 20 -17 27 0",
-        "acceptor 0 30 -10 10 0 10 1e+21",
-        "acceptor 24 30 -20 20 0 10 1e+21",
-        "acceptor 30 66 -20 20 -17 27 1e+21",
-        "motioncube -1 66 -20 20 -17 27 PASS PASS PASS PASS PASS PASS",
-        "motionplane 0 24 -18 -18 0 10 LEFT CATCH",
-        "motionplane 0 24 -18 -18 0 10 RIGHT GENERATE",
-        "motionplane 0 30 -20 -20 0 10 LEFT REFLECT",
-        "motionplane 0 24 18 18 0 10 RIGHT CATCH",
-        "motionplane 0 24 18 18 0 10 LEFT GENERATE",
-        "motionplane 0 30 20 20 0 10 RIGHT REFLECT",
-        "motionplane 0 0 -20 20 0 10 UP SCATTOX",
-        "motionplane 0 30 -20 20 0 0 FRONT SCATTOX",
-        "motionplane 0 30 -20 20 10 10 BACK SCATTOX",
-        "motionplane 30 30 -20 20 -17 0 UP SCATTOX",
-        "motionplane 30 30 -20 20 10 27 UP SCATTOX",
-        "motionplane 30 66 -20 -20 -17 27 LEFT SCATTOX",
-        "motionplane 30 66 20 20 -17 27 RIGHT SCATTOX",
-        "motionplane 30 66 -20 20 -17 -17 FRONT SCATTOX",
-        "motionplane 30 66 -20 20 27 27 BACK SCATTOX",
-        "motionplane 66 66 -20 20 -17 27 DOWN SCATTOX",
-        "motionplane 64 64 -20 20 -17 27 UP GENERATE",
-        "motionplane 64 64 -20 20 -17 27 DOWN CATCH",
-        "attachcontact 0 30 -20 20 0 10 0",
-        "attachcontact 0 24 -20 -16 0 10 1",
-        "attachcontact 0 24 16 20 0 10 2",
-        "attachcontact 60 66 -20 20 -17 27 3",
+        f"acceptor -1 66 {Y} -17 27 0",
+        f"acceptor 0 30 {g(-h)} {g(h)} 0 10 1e+21",
+        f"acceptor 24 30 {Y} 0 10 1e+21",
+        f"acceptor 30 66 {Y} -17 27 1e+21",
+        f"motioncube -1 66 {Y} -17 27 PASS PASS PASS PASS PASS PASS",
+        f"motionplane 0 24 {g(-c)} {g(-c)} 0 10 LEFT CATCH",
+        f"motionplane 0 24 {g(-c)} {g(-c)} 0 10 RIGHT GENERATE",
+        f"motionplane 0 30 {g(-e)} {g(-e)} 0 10 LEFT REFLECT",
+        f"motionplane 0 24 {g(c)} {g(c)} 0 10 RIGHT CATCH",
+        f"motionplane 0 24 {g(c)} {g(c)} 0 10 LEFT GENERATE",
+        f"motionplane 0 30 {g(e)} {g(e)} 0 10 RIGHT REFLECT",
+        f"motionplane 0 0 {Y} 0 10 UP SCATTOX",
+        f"motionplane 0 30 {Y} 0 0 FRONT SCATTOX",
+        f"motionplane 0 30 {Y} 10 10 BACK SCATTOX",
+        f"motionplane 30 30 {Y} -17 0 UP SCATTOX",
+        f"motionplane 30 30 {Y} 10 27 UP SCATTOX",
+        f"motionplane 30 66 {g(-e)} {g(-e)} -17 27 LEFT SCATTOX",
+        f"motionplane 30 66 {g(e)} {g(e)} -17 27 RIGHT SCATTOX",
+        f"motionplane 30 66 {Y} -17 -17 FRONT SCATTOX",
+        f"motionplane 30 66 {Y} 27 27 BACK SCATTOX",
+        f"motionplane 66 66 {Y} -17 27 DOWN SCATTOX",
+        f"motionplane 64 64 {Y} -17 27 UP GENERATE",
+        f"motionplane 64 64 {Y} -17 27 DOWN CATCH",
+        f"attachcontact 0 30 {Y} 0 10 0",
+        f"attachcontact 0 24 {g(-e)} {g(-r)} 0 10 1",
+        f"attachcontact 0 24 {g(r)} {g(e)} 0 10 2",
+        f"attachcontact 60 66 {Y} -17 27 3",
         "surfaces 3",
         "0 0 0",
         "2 0 4",
         "2 10 5",
-        "surface_scatter_range 0 24 -20 20 0 10",
-        "contact", "1 0", "0 24 -20 -20 0 10", "0",
-        "contact", "1 0", f"0 24 20 20 0 10", g(vd),
-        "contact", "1 0", "66 66 -20 20 -17 27", "0",
-        "contact", f"3 {g(phims)}", "-1 -1 -10 10 -1 11", "-1 24 -10 10 -1 -1", "-1 24 -10 10 11 11", g(vg),
+        f"surface_scatter_range 0 24 {Y} 0 10",
+        "contact", "1 0", f"0 24 {g(-e)} {g(-e)} 0 10", "0",
+        "contact", "1 0", f"0 24 {g(e)} {g(e)} 0 10", g(vd),
+        "contact", "1 0", f"66 66 {Y} -17 27", "0",
+        "contact", f"3 {g(phims)}", f"-1 -1 {g(-h)} {g(h)} -1 11", f"-1 24 {g(-h)} {g(h)} -1 -1",
+        f"-1 24 {g(-h)} {g(h)} 11 11", g(vg),
         "end",
     ]
     with open(os.path.join(dirpath, "ldg.txt"), "w") as f:

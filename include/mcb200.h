@@ -194,7 +194,9 @@ int mcb200_surface_rates(mcb200_ctx *ctx, const mcb200_surface_params *params, c
  * probability |q| / sum|q|, each carrying sum(q) / desired.  Within a cell
  * particles are taken in uid order; each (cell, carrier) draws from stream
  * (seed, cell, step, 0x4d520000 + carrier); resampled particles get fresh
- * uids.  *generated receives the change in particle count (mr_gen_num). */
+ * uids.  *generated receives the change in particle count (mr_gen_num);
+ * with generated NULL the refresh is only enqueued (its counts stay on the
+ * device, nothing waits for the GPU). */
 int mcb200_multiple_refresh(mcb200_ctx *ctx, const int32_t *desired_e, const int32_t *desired_h, uint32_t step,
                             uint64_t seed, int64_t *generated);
 
@@ -299,6 +301,17 @@ int mcb200_batch_step(mcb200_batch *batch);
  * a member's mesh, fields or store change outside the batch. */
 int mcb200_batch_run(mcb200_batch *batch, int steps);
 int mcb200_batch_use_graphs(mcb200_batch *batch, int enable);
+/* Launch shapes picked by measurement: for every candidate (batched-flight
+ * blocks per SM in {1, 2} x blocks per SM of the members' per-step kernels
+ * -- sort, deposition, copies -- in {2, 4, 8}) one untimed and `trial_steps`
+ * timed full timesteps (mcb200_batch_run: they advance the simulations like
+ * any other steps); the fastest by device time is kept and returned. */
+typedef struct {
+  int flight_blocks_per_sm, grid_per_sm, reserved;
+  double ms_per_step;  /* of the kept setting */
+  int candidates;
+} mcb200_batch_tuning;
+int mcb200_batch_autotune(mcb200_batch *batch, int trial_steps, mcb200_batch_tuning *best);
 /* Wait for the batch and every member; reports a member's full store. */
 int mcb200_batch_sync(mcb200_batch *batch);
 /* Resident blocks per SM of the batched flight launches (0: as many as fit). */
