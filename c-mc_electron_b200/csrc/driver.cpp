@@ -438,6 +438,25 @@ struct Run {
 
 }  // namespace
 
+extern "C" int mcb200_deck_surface_params(const char *input_path, mcb200_ctx *ctx, const mcb200_deck_info *info,
+                                          mcb200_surface_params *out, int *poisson_every) {
+  if (!input_path || !ctx || !info || !out) return MCB200_ERR_ARG;
+  const Extras ex = read_extras(input_path);
+  double u[14];
+  if (int rc = mcb200_units(ctx, u, 14)) return rc;
+  const double spr0 = u[2];
+  mcb200_surface_params s{};
+  s.delta = ex.delta_nm * 1e-9 / spr0;
+  s.ail = ex.lambda_nm * 1e-9 / spr0;
+  s.xiph = 12.0; s.theta = 2.857703; s.gama = 1.5; s.nbmod = 2.0;
+  s.npf = -0.6; s.pft = 0.7; s.pfn = 0.3; s.kpha = 3600e-4;
+  s.roughness = info->flag_surface_roughness;
+  s.phonon = info->flag_surface_phonon;
+  *out = s;
+  if (poisson_every) *poisson_every = ex.poisson_every;
+  return MCB200_OK;
+}
+
 extern "C" int mcb200_run_deck(const char *input_path, int device, const mcb200_run_options *options,
                                mcb200_run_report *report, char *error, size_t error_len) {
   if (!input_path || !options || !report) return MCB200_ERR_ARG;

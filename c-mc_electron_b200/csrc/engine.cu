@@ -779,6 +779,49 @@ size_t mcb200_num_particles(const mcb200_ctx *cc) {
   return c->n;
 }
 
+int mcb200_copy_ensemble(mcb200_ctx *dst, mcb200_ctx *src) {
+  if (!dst || !src || dst == src) return MCB200_ERR_ARG;
+  if (dst->device != src->device || dst->precision != src->precision || !dst->mesh_set || !src->mesh_set ||
+      dst->mesh.nx != src->mesh.nx || dst->mesh.ny != src->mesh.ny || dst->mesh.nz != src->mesh.nz)
+    return fail(dst, MCB200_ERR_ARG, "mcb200_copy_ensemble: contexts differ in device, precision or mesh");
+  try {
+    ck(cudaSetDevice(dst->device), "cudaSetDevice");
+    pull_counts(src);
+    ck(cudaStreamSynchronize(dst->stream), "sync");
+    if (src->n > dst->capacity) return fail(dst, MCB200_ERR_CAPACITY, "mcb200_copy_ensemble: too many particles");
+    const size_t n = src->n;
+    auto copy = [&](void *d, const void *s, size_t bytes) {
+      if (bytes) ck(cudaMemcpyAsync(d, s, bytes, cudaMemcpyDeviceToDevice, dst->stream), "copy ensemble");
+    };
+    auto move = [&](auto tag) {
+      using R = decltype(tag);
+      const DevParticlesT<R> &a = store<R>(src, src->cur), &b = store<R>(dst, 0);
+      copy(b.x, a.x, n * sizeof(R)); copy(b.y, a.y, n * sizeof(R)); copy(b.z, a.z, n * sizeof(R));
+      copy(b.kx, a.kx, n * sizeof(R)); copy(b.ky, a.ky, n * sizeof(R)); copy(b.kz, a.kz, n * sizeof(R));
+      copy(b.energy, a.energy, n * 8); copy(b.charge, a.charge, n * 8);
+      copy(b.cell, a.cell, n * 4); copy(b.itet, a.itet, n * 4); copy(b.meta, a.meta, n * 4); copy(b.uid, a.uid, n * 4);
+    };
+    if (dst->precision == MCB200_FLIGHT_FP32) move(float{});
+    else move(double{});
+    if (dst->device_set && src->device_set) {
+      const size_t nodes = (size_t)(dst->mesh.nx + 1) * (dst->mesh.ny + 1) * (dst->mesh.nz + 1);
+      copy(dst->fb.potential, src->fb.potential, nodes * sizeof(double));
+    }
+    dst->cur = 0;
+    dst->n = n;
+    dst->next_uid = src->next_uid;
+    dst->overflow_pending = false;
+    ck(cudaMemsetAsync(dst->dev_counts + 2, 0, sizeof(unsigned int), dst->stream), "memset");
+    push_counts(dst);
+    ck(cudaStreamSynchronize(dst->stream), "sync");
+    return MCB200_OK;
+  } catch (const CapacityError &e) {
+    return fail(dst, MCB200_ERR_CAPACITY, e.what());
+  } catch (const std::exception &e) {
+    return fail(dst, MCB200_ERR_CUDA, e.what());
+  }
+}
+
 int mcb200_particle_steps(mcb200_ctx *c, uint64_t *total) {
   if (!c || !total) return MCB200_ERR_ARG;
   if (c->device < 0) return fail(c, MCB200_ERR_STATE, "host-only context");

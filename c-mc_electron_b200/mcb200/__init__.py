@@ -88,6 +88,38 @@ class BatchTuning(ctypes.Structure):
                 ("ms_per_step", ctypes.c_double), ("candidates", ctypes.c_int)]
 
 
+class ServerOptions(ctypes.Structure):
+    _fields_ = [("table_dir", ctypes.c_char_p), ("kelvin", ctypes.c_double), ("device", ctypes.c_int),
+                ("flight_precision", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_size_t),
+                ("max_slots", ctypes.c_int), ("quantum_steps", ctypes.c_int), ("use_graphs", ctypes.c_int)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("input_path", ctypes.c_char_p), ("family", ctypes.c_char_p), ("bias", ctypes.c_double * 2),
+                ("target_rel_err", ctypes.c_double), ("min_windows", ctypes.c_int), ("max_steps", ctypes.c_int),
+                ("warm_windows_cold", ctypes.c_int), ("warm_windows_warm", ctypes.c_int),
+                ("warm_start", ctypes.c_int), ("poisson_every", ctypes.c_int), ("drain_contact", ctypes.c_int),
+                ("seed", ctypes.c_uint64), ("arrival_s", ctypes.c_double)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_uint64), ("status", ctypes.c_int), ("ids", ctypes.c_double),
+                ("ids_stderr", ctypes.c_double), ("windows", ctypes.c_int), ("steps", ctypes.c_int),
+                ("particle_steps", ctypes.c_uint64), ("arrival_s", ctypes.c_double), ("admit_s", ctypes.c_double),
+                ("done_s", ctypes.c_double), ("warm_from", ctypes.c_uint64), ("particles", ctypes.c_size_t),
+                ("bytes", ctypes.c_size_t)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("rounds", ctypes.c_uint64), ("particle_steps", ctypes.c_uint64), ("device_ms", ctypes.c_double),
+                ("active", ctypes.c_int), ("pending", ctypes.c_int), ("cached", ctypes.c_int),
+                ("bytes_in_use", ctypes.c_size_t)]
+
+
+SERVE_CONVERGED = 1
+SERVE_STEP_LIMIT = 2
+
+
 class RunOptions(ctypes.Structure):
     _fields_ = [("table_dir", ctypes.c_char_p), ("data_dir", ctypes.c_char_p), ("flight_precision", ctypes.c_int),
                 ("poisson_every", ctypes.c_int), ("poisson_rel_tol", ctypes.c_double), ("max_steps", ctypes.c_int),
@@ -131,6 +163,18 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mcb200_batch_info.argtypes = [vp, c.POINTER(c.c_int), c.POINTER(c.c_uint64), c.POINTER(c.c_uint64),
                                       c.POINTER(c.c_uint64), c.POINTER(c.c_uint64)]
     lib.mcb200_batch_run.argtypes = [vp, c.c_int]
+    lib.mcb200_server_create.argtypes = [c.POINTER(ServerOptions), c.POINTER(vp)]
+    lib.mcb200_server_destroy.argtypes = [vp]
+    lib.mcb200_server_destroy.restype = None
+    lib.mcb200_server_last_error.argtypes = [vp]
+    lib.mcb200_server_last_error.restype = c.c_char_p
+    lib.mcb200_server_now.argtypes = [vp]
+    lib.mcb200_server_now.restype = c.c_double
+    lib.mcb200_server_submit.argtypes = [vp, c.POINTER(Request), c.POINTER(c.c_uint64)]
+    lib.mcb200_server_round.argtypes = [vp, c.POINTER(c.c_int), c.POINTER(c.c_int)]
+    lib.mcb200_server_results.argtypes = [vp, c.POINTER(Result), c.c_int, c.POINTER(c.c_int)]
+    lib.mcb200_server_stats.argtypes = [vp, c.POINTER(ServerStats)]
+    lib.mcb200_copy_ensemble.argtypes = [vp, vp]
     lib.mcb200_batch_autotune.argtypes = [vp, c.c_int, c.POINTER(BatchTuning)]
     lib.mcb200_batch_use_graphs.argtypes = [vp, c.c_int]
     lib.mcb200_destroy.argtypes = [vp]
@@ -540,6 +584,75 @@ class Batch:
                                                 ctypes.byref(gc), ctypes.byref(gr)), "mcb200_batch_info")
         return {"members": n.value, "steps": st.value, "launches": la.value, "graph_captures": gc.value,
                 "graph_replays": gr.value}
+
+
+class Server:
+    """Bias-point requests served by continuous batching (mcb200_server_*)."""
+
+    def __init__(self, table_dir: str = DEFAULT_TABLE_DIR, device: int = 0, precision: int = FLIGHT_FP32,
+                 hbm_budget_bytes: int = 0, max_slots: int = 64, quantum_steps: int = 50, use_graphs: bool = True,
+                 kelvin: float = 300.0):
+        self._lib = lib()
+        self._s = ctypes.c_void_p()
+        self._table_dir = table_dir.encode()
+        opt = ServerOptions(self._table_dir, kelvin, device, precision, hbm_budget_bytes, max_slots, quantum_steps,
+                            int(use_graphs))
+        rc = self._lib.mcb200_server_create(ctypes.byref(opt), ctypes.byref(self._s))
+        if rc != OK:
+            msg = self._lib.mcb200_server_last_error(self._s).decode() if self._s else "no server"
+            self.close()
+            raise EngineError(f"mcb200_server_create failed ({rc}): {msg}")
+
+    def close(self):
+        if self._s:
+            self._lib.mcb200_server_destroy(self._s)
+            self._s = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, what: str):
+        if rc != OK:
+            raise EngineError(f"{what} failed ({rc}): {self._lib.mcb200_server_last_error(self._s).decode()}")
+
+    def now(self) -> float:
+        return self._lib.mcb200_server_now(self._s)
+
+    def submit(self, input_path: str, family: str, bias, seed: int, target_rel_err: float = 0.01,
+               min_windows: int = 5, max_steps: int = 0, warm_windows_cold: int = 10, warm_windows_warm: int = 1,
+               warm_start: bool = True, poisson_every: int = 0, drain_contact: int = 1, arrival_s=None) -> int:
+        req = Request(os.fspath(input_path).encode(), family.encode(), (ctypes.c_double * 2)(*bias), target_rel_err,
+                      min_windows, max_steps, warm_windows_cold, warm_windows_warm, int(warm_start), poisson_every,
+                      drain_contact, seed, self.now() if arrival_s is None else arrival_s)
+        rid = ctypes.c_uint64()
+        self._check(self._lib.mcb200_server_submit(self._s, ctypes.byref(req), ctypes.byref(rid)),
+                    "mcb200_server_submit")
+        return rid.value
+
+    def round(self):
+        """One scheduling round; returns (active, pending)."""
+        a, p = ctypes.c_int(), ctypes.c_int()
+        self._check(self._lib.mcb200_server_round(self._s, ctypes.byref(a), ctypes.byref(p)), "mcb200_server_round")
+        return a.value, p.value
+
+    def results(self) -> list:
+        out = []
+        buf = (Result * 64)()
+        while True:
+            n = ctypes.c_int()
+            self._check(self._lib.mcb200_server_results(self._s, buf, 64, ctypes.byref(n)), "mcb200_server_results")
+            for r in buf[:n.value]:
+                out.append({f: getattr(r, f) for f, _ in Result._fields_})
+            if n.value < 64:
+                return out
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        self._check(self._lib.mcb200_server_stats(self._s, ctypes.byref(st)), "mcb200_server_stats")
+        return {f: getattr(st, f) for f, _ in ServerStats._fields_}
 
 
 class Deck:

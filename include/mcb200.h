@@ -238,6 +238,11 @@ size_t mcb200_num_particles(const mcb200_ctx *ctx);
 /* Particle-steps flown since the context was created (the particle count at
  * the start of every step, summed on the device); waits for the stream. */
 int mcb200_particle_steps(mcb200_ctx *ctx, uint64_t *total);
+/* Warm start: the particles, uid counter and potential of `src` become those
+ * of `dst` (same device, flight precision and mesh dimensions; dst's store
+ * must hold them).  Waits for both contexts.  No counterpart in the
+ * reference. */
+int mcb200_copy_ensemble(mcb200_ctx *dst, mcb200_ctx *src);
 
 /* Append n particles of carrier `type` (0 electron, 1 hole) sampled on the
  * GPU the way the reference initialises them: cell_of[q] is the cell of new
@@ -518,6 +523,82 @@ typedef struct {
   double timed_flight_ms;         /* flight-kernel device time within them */
   uint64_t timed_flight_launches, timed_launches;
 } mcb200_run_report;
+
+/* The surface-scattering parameters mcb200_run_deck uses for a deck (the
+ * reference's constants; roughness delta / Lambda from input.txt's
+ * surface_roughness_delta_nm / _lambda_nm keys, else 0.1126755 nm / 2 nm)
+ * in ctx's units, and input.txt's poisson_step (1 without it). */
+int mcb200_deck_surface_params(const char *input_path, mcb200_ctx *ctx, const mcb200_deck_info *info,
+                               mcb200_surface_params *out, int *poisson_every);
+
+/* ---- serving bias-point requests (continuous batching) ---------------------
+ * No counterpart in the reference, which runs one bias point per process.
+ * A server owns one set of band tables on one device and serves requests,
+ * each a device deck (input.txt with its lgrid / ldg files) of a family
+ * (requests of a family share the mesh and may warm-start one another) at
+ * a bias.  Each mcb200_server_round: admits queued requests in arrival
+ * order while a slot (at most 64) is free and the HBM budget holds them
+ * (converged ensembles kept for warm starts are evicted least recently used
+ * first to make room), runs quantum_steps full timesteps of every active
+ * request as one batch (mcb200_batch_run), and retires the requests whose
+ * drain-current standard error -- one Ids sample per round, after the
+ * discarded transient windows -- is below target_rel_err of |Ids|, or that
+ * reached max_steps.  A request's steps, Poisson solves, refreshes and Ids
+ * windows count its own steps from admission, so a cold-started request has
+ * the same result alone or among others.  Calls are not thread-safe. */
+typedef struct mcb200_server mcb200_server;
+typedef struct {
+  const char *table_dir;
+  double kelvin;             /* lattice temperature of the tables (0: 300 K) */
+  int device;
+  int flight_precision;      /* MCB200_FLIGHT_FP64 / MCB200_FLIGHT_FP32 */
+  size_t hbm_budget_bytes;   /* device memory for requests and warm-start entries (0: 160 GB) */
+  int max_slots;             /* concurrent requests (0 or > 64: 64) */
+  int quantum_steps;         /* timesteps per round = steps per Ids window (0: 50) */
+  int use_graphs;            /* replay each round's steps from CUDA graphs */
+} mcb200_server_options;
+typedef struct {
+  const char *input_path;    /* the deck's input.txt (copied at submission) */
+  const char *family;        /* warm starts stay within a family (same mesh) */
+  double bias[2];            /* (Vg, Vd): the distance for nearest-bias warm starts */
+  double target_rel_err;     /* complete when stderr(Ids) <= target * |Ids| (0: 0.01) */
+  int min_windows;           /* kept Ids windows before completion (at least 2) */
+  int max_steps;             /* complete at this many steps regardless (0: no limit) */
+  int warm_windows_cold;     /* windows discarded as transient after a cold start */
+  int warm_windows_warm;     /* ... after a warm start */
+  int warm_start;            /* start from the nearest converged bias of the family, and keep this one */
+  int poisson_every;         /* 0: the deck's poisson_step */
+  int drain_contact;         /* 0-based contact whose current is Ids */
+  uint64_t seed;
+  double arrival_s;          /* arrival time on the server clock (mcb200_server_now), for latency */
+} mcb200_request;
+#define MCB200_SERVE_CONVERGED 1
+#define MCB200_SERVE_STEP_LIMIT 2
+typedef struct {
+  uint64_t id;
+  int status;                /* MCB200_SERVE_*, or a negative error code of the admission */
+  double ids, ids_stderr;    /* mean drain current (A/cm, as the reference's current file) and its stderr */
+  int windows, steps;
+  uint64_t particle_steps;
+  double arrival_s, admit_s, done_s;  /* server clock */
+  uint64_t warm_from;        /* request whose ensemble started this one (0: cold start) */
+  size_t particles, bytes;   /* final particles; device memory taken */
+} mcb200_result;
+typedef struct {
+  uint64_t rounds, particle_steps;
+  double device_ms;          /* device time of the rounds' steps */
+  int active, pending, cached;
+  size_t bytes_in_use;
+} mcb200_server_stats_t;
+int mcb200_server_create(const mcb200_server_options *opt, mcb200_server **out);
+void mcb200_server_destroy(mcb200_server *server);
+const char *mcb200_server_last_error(const mcb200_server *server);
+double mcb200_server_now(const mcb200_server *server);
+int mcb200_server_submit(mcb200_server *server, const mcb200_request *request, uint64_t *id);
+int mcb200_server_round(mcb200_server *server, int *active, int *pending);
+/* Moves up to `max` finished results out of the server. */
+int mcb200_server_results(mcb200_server *server, mcb200_result *out, int max, int *n);
+int mcb200_server_stats(const mcb200_server *server, mcb200_server_stats_t *stats);
 
 /* `error` (may be NULL) receives a message on failure. */
 int mcb200_run_deck(const char *input_path, int device, const mcb200_run_options *options,
