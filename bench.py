@@ -333,6 +333,47 @@ def batch_arm(args, device: int) -> dict:
     return out
 
 
+# ------------------------------------------------------------ serving
+SERVE_REQUESTS = 32
+SERVE_MAX_STEPS = 2000
+SERVE_QUANTUM = 50
+
+
+def serve_arm(args, device: int) -> dict:
+    """A 32-point bias sweep served by continuous batching: n-FinFET requests
+    (Vg 0-0.8 V in 0.05 V steps x Vd {0.05, 0.7} V x Lg {15, 20, 30} nm,
+    50k-1M particles log-uniform) arriving as a Poisson process of 4 req/s
+    (seed 5); FP32 flight, HBM budget 160 GB, one Ids window per 50-step
+    round (net flux through the middle third of the section planes), each
+    request done when stderr(Ids) < 1% of |Ids| after 6 transient windows
+    (2 after a warm start) or at 2000 steps.  Latency = completion - arrival
+    (server clock); throughput = particle-steps over the rounds' device time."""
+    import mcb200
+    from mcb200 import serving
+
+    with tempfile.TemporaryDirectory() as tmp:
+        reqs = serving.make_requests(tmp, n=SERVE_REQUESTS, seed=5, rate=4.0)
+        srv = mcb200.Server(device=device, precision=mcb200.FLIGHT_FP32, quantum_steps=SERVE_QUANTUM)
+        with ClockSampler(device) as clocks:
+            res, st, wall = serving.serve(srv, reqs, max_wall_s=900, max_steps=SERVE_MAX_STEPS, min_windows=5,
+                                          warm_windows_cold=6, warm_windows_warm=2, poisson_every=10,
+                                          target_rel_err=0.01, ids_sections=True)
+        srv.close()
+    lat = serving.latency_summary(res)
+    status = [r["status"] for r in res]
+    return {"metric": "bias-point latency", "unit": "s", "p50_s": lat.get("p50_s"), "p99_s": lat.get("p99_s"),
+            "mean_s": lat.get("mean_s"), "requests": SERVE_REQUESTS, "completed": len(res),
+            "converged": status.count(mcb200.SERVE_CONVERGED), "step_limited": status.count(mcb200.SERVE_STEP_LIMIT),
+            "warm_started": sum(1 for r in res if r["warm_from"]),
+            "throughput_particle_steps_per_s": st["particle_steps"] / (st["device_ms"] * 1e-3),
+            "particle_steps": st["particle_steps"], "rounds": st["rounds"], "wall_s": wall,
+            "median_rel_stderr": float(statistics.median(abs(r["ids_stderr"] / r["ids"]) for r in res if r["ids"]))
+            if res else None,
+            "clocks": clocks.summary(),
+            "config": "32 FinFET bias points, Poisson arrivals 4 req/s, 50k-1M particles, 160 GB budget, "
+                      "target 1% Ids stderr, 2000-step cap, 50-step rounds, FP32 flight"}
+
+
 # ------------------------------------------------------------ reference (CPU)
 def _oracle_sample(args):
     """One CPU process: the reference's routines on a reduced FinFET deck
@@ -448,7 +489,7 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--particles", type=int, default=2_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="all", choices=["all", "finfet", "batch"],
+    ap.add_argument("--workload", default="all", choices=["all", "finfet", "batch", "serve"],
                     help="finfet: only the two FinFET arms (no e2e rerun, no bulk box): for profiling; "
                          "batch: only the batching arm")
     args = ap.parse_args()
@@ -459,10 +500,15 @@ def main():
         out = reference_arm(args, rank, world)
     elif args.workload == "batch":
         out = batch_arm(args, local)
+    elif args.workload == "serve":
+        out = serve_arm(args, local)
     else:
         out = engine_arm(args, rank, world, local)
         if args.workload == "all":
             out["batch"] = batch_arm(args, local)
+            out["serving"] = serve_arm(args, local)
+            out["p50_latency_s"] = out["serving"]["p50_s"]
+            out["p99_latency_s"] = out["serving"]["p99_s"]
         if rank == 0 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline()
     if rank == 0 and out is not None:

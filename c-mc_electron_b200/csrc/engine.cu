@@ -1289,13 +1289,22 @@ int mcb200_multiple_refresh(mcb200_ctx *c, const int32_t *desired_e, const int32
       w.tot = dalloc<unsigned int>(2, c->mesh_owned);
       w.gen = dalloc<unsigned long long>(1, c->mesh_owned);
       w.cells = cells;
+      w.de_host.clear();
+      w.dh_host.clear();
     }
     int *de = w.de, *dh = w.dh;
     unsigned int *out_count = w.out_count, *new_count = w.new_count, *out_off = w.out_off, *uid_off = w.uid_off;
     unsigned int *tiles = w.tiles, *tot = w.tot;
     unsigned long long *gen = w.gen;
-    ck(cudaMemcpyAsync(de, desired_e, sizeof(int) * cells, cudaMemcpyHostToDevice, s), "copy");
-    ck(cudaMemcpyAsync(dh, desired_h, sizeof(int) * cells, cudaMemcpyHostToDevice, s), "copy");
+    // the targets stay on the device: a copy from pageable host memory would
+    // wait for the stream (and, in a batch, for every member's step)
+    if (w.de_host.size() != (size_t)cells || std::memcmp(w.de_host.data(), desired_e, sizeof(int) * cells) != 0 ||
+        std::memcmp(w.dh_host.data(), desired_h, sizeof(int) * cells) != 0) {
+      w.de_host.assign(desired_e, desired_e + cells);
+      w.dh_host.assign(desired_h, desired_h + cells);
+      ck(cudaMemcpyAsync(de, w.de_host.data(), sizeof(int) * cells, cudaMemcpyHostToDevice, s), "copy");
+      ck(cudaMemcpyAsync(dh, w.dh_host.data(), sizeof(int) * cells, cudaMemcpyHostToDevice, s), "copy");
+    }
     ck(cudaMemsetAsync(gen, 0, sizeof(unsigned long long), s), "memset");
     // group the store by cell into the other buffer (hist = counts, offsets =
     // cell ends); the refreshed population then goes back to this buffer

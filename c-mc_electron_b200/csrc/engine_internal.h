@@ -92,6 +92,7 @@ struct MrScratch {
   unsigned int *out_count = nullptr, *new_count = nullptr, *out_off = nullptr, *uid_off = nullptr;
   unsigned int *tiles = nullptr, *tot = nullptr;
   unsigned long long *gen = nullptr;
+  std::vector<int> de_host, dh_host;  // the targets last uploaded to de / dh
 };
 
 // Band tables on the host and the device (mcb200_create): built once and

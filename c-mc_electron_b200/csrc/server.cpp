@@ -131,14 +131,25 @@ size_t free_bytes(int device) {
   return f;
 }
 
-// Ids of the last window from the drain contact's tallies (the reference's
-// current_scatter_info: (CharGen - CharCatch) / (dt * steps) * curr0 * 1e-2),
-// then the tallies restart.
+// Ids of the last window, then the tallies restart.  Either the drain
+// contact's current (the reference's current_scatter_info: (CharGen -
+// CharCatch) / (dt * steps) * curr0 * 1e-2), or (ids_sections) the net
+// carrier flux through the y node planes (the reference's section_current,
+// (rcurrent - lcurrent) / (dt * steps) * curr0 * 1e-2) averaged over the
+// middle third of the planes: the same steady-state current with far less
+// noise per window, since every crossing of every plane counts.
 int read_window(Slot &s, int steps) {
-  std::vector<double> contact(16 * 6);
-  if (int rc = mcb200_get_tallies(s.ctx, nullptr, contact.data(), nullptr, nullptr, nullptr, nullptr)) return rc;
-  const int c = std::min(std::max(s.req.drain_contact, 0), 15);
-  const double ids = (contact[6 * c + 1] - contact[6 * c + 4]) / (s.info.dt * steps) * s.curr0 * 1e-2;
+  std::vector<double> contact(16 * 6), lc(s.info.ny + 1), rc(s.info.ny + 1);
+  if (int e = mcb200_get_tallies(s.ctx, nullptr, contact.data(), lc.data(), rc.data(), nullptr, nullptr)) return e;
+  double ids = 0;
+  if (s.req.ids_sections) {
+    const int ny = s.info.ny, j0 = ny / 3, j1 = std::max(j0 + 1, ny - ny / 3);
+    for (int j = j0; j < j1; ++j) ids += rc[j] - lc[j];
+    ids = ids / (j1 - j0) / (s.info.dt * steps) * s.curr0 * 1e-2;
+  } else {
+    const int c = std::min(std::max(s.req.drain_contact, 0), 15);
+    ids = (contact[6 * c + 1] - contact[6 * c + 4]) / (s.info.dt * steps) * s.curr0 * 1e-2;
+  }
   if (s.warm > 0) --s.warm;
   else s.windows.push_back(ids);
   return mcb200_reset_tallies(s.ctx);

@@ -99,7 +99,7 @@ class Request(ctypes.Structure):
                 ("target_rel_err", ctypes.c_double), ("min_windows", ctypes.c_int), ("max_steps", ctypes.c_int),
                 ("warm_windows_cold", ctypes.c_int), ("warm_windows_warm", ctypes.c_int),
                 ("warm_start", ctypes.c_int), ("poisson_every", ctypes.c_int), ("drain_contact", ctypes.c_int),
-                ("seed", ctypes.c_uint64), ("arrival_s", ctypes.c_double)]
+                ("ids_sections", ctypes.c_int), ("seed", ctypes.c_uint64), ("arrival_s", ctypes.c_double)]
 
 
 class Result(ctypes.Structure):
@@ -623,10 +623,11 @@ class Server:
 
     def submit(self, input_path: str, family: str, bias, seed: int, target_rel_err: float = 0.01,
                min_windows: int = 5, max_steps: int = 0, warm_windows_cold: int = 10, warm_windows_warm: int = 1,
-               warm_start: bool = True, poisson_every: int = 0, drain_contact: int = 1, arrival_s=None) -> int:
+               warm_start: bool = True, poisson_every: int = 0, drain_contact: int = 1, ids_sections: bool = False,
+               arrival_s=None) -> int:
         req = Request(os.fspath(input_path).encode(), family.encode(), (ctypes.c_double * 2)(*bias), target_rel_err,
                       min_windows, max_steps, warm_windows_cold, warm_windows_warm, int(warm_start), poisson_every,
-                      drain_contact, seed, self.now() if arrival_s is None else arrival_s)
+                      drain_contact, int(ids_sections), seed, self.now() if arrival_s is None else arrival_s)
         rid = ctypes.c_uint64()
         self._check(self._lib.mcb200_server_submit(self._s, ctypes.byref(req), ctypes.byref(rid)),
                     "mcb200_server_submit")

@@ -569,6 +569,8 @@ typedef struct {
   int warm_start;            /* start from the nearest converged bias of the family, and keep this one */
   int poisson_every;         /* 0: the deck's poisson_step */
   int drain_contact;         /* 0-based contact whose current is Ids */
+  int ids_sections;          /* 1: Ids from the net flux through the middle third of the y planes (section
+                                currents) instead of the contact's generate / catch balance */
   uint64_t seed;
   double arrival_s;          /* arrival time on the server clock (mcb200_server_now), for latency */
 } mcb200_request;
