@@ -24,7 +24,8 @@ struct mcb200_batch {
   std::vector<mcb200_ctx *> m;
   std::vector<mcb200_batch_member> cfg;
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev_flight = nullptr, ev_fork = nullptr, ev_solved = nullptr;
+  cudaStream_t side = nullptr;  // the flight of the members not solving Poisson, beside the solves
+  cudaEvent_t ev_flight = nullptr, ev_fork = nullptr, ev_solved = nullptr, ev_side = nullptr, ev_side0 = nullptr;
   std::vector<cudaEvent_t> ev_member;
   std::vector<uint32_t> member_step;  // host copy of each member's step number
   // full timesteps replayed from CUDA graphs: one per (store parity, members
@@ -40,7 +41,8 @@ struct mcb200_batch {
   cudaEvent_t marks[8] = {};
   void *tables = nullptr;          // device: [6][n] BatchInstT (main flight x 2 parities, 4 copy generations)
   uint32_t *steps = nullptr;       // device: step number of each member
-  unsigned int *tickets = nullptr;  // device: work counters of the 5 batched launches
+  unsigned int *tickets = nullptr;  // device: work counters of the batched launches (main, 4 copy generations, side)
+  bool overlap = true;              // fly the members not solving Poisson beside the solves
   std::vector<unsigned char> snap;  // per member: DevMesh, DevTallies and store parity the tables were built for
   uint64_t steps_done = 0, built_at = 0;
   int blocks_per_sm = 0;  // batched flight grid (0: as many as fit); mcb200_batch_autotune
@@ -57,6 +59,8 @@ struct mcb200_batch {
     drop_graphs();
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_solved) cudaEventDestroy(ev_solved);
+    if (ev_side) cudaEventDestroy(ev_side);
+    if (ev_side0) cudaEventDestroy(ev_side0);
     if (tables) cudaFree(tables);
     if (steps) cudaFree(steps);
     if (tickets) cudaFree(tickets);
@@ -65,6 +69,7 @@ struct mcb200_batch {
       if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : marks)
       if (e) cudaEventDestroy(e);
+    if (side) cudaStreamDestroy(side);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -156,36 +161,66 @@ __global__ void advance_steps(uint32_t *steps, int n) {
 
 void join_members(mcb200_batch *b);
 
+uint64_t all_members(const mcb200_batch *b) {
+  const size_t n = b->m.size();
+  return n >= 64 ? ~0ull : (1ull << n) - 1;
+}
+
 // The transport part of a step (mcb200_step for every member): the tables
-// must be current.
+// must be current.  The members in `early` (none of them waiting for work on
+// the batch stream) fly on the side stream as soon as their own streams are
+// ready, one block per SM (it fits beside the two blocks per SM of a
+// Poisson solve); the others fly in the main launch on the batch stream,
+// after which a helper launch on the batch stream draws from the side
+// launch's work counter with the room the solves left.  The copy
+// generations of all members follow.  A particle's flight does not depend
+// on the launch or block that carries it.
 template <typename R>
-void batch_transport(mcb200_batch *b) {
+void batch_transport(mcb200_batch *b, uint64_t early = 0) {
   const int n = (int)b->m.size();
-  // 1. every member: counters and records for the step, then the batch stream waits for it
+  const uint64_t all = all_members(b);
+  early &= all;
+  if (early == all) early = 0;  // one launch
+  // 1. every member: counters and records for the step, then the stream of its flight waits for it
   for (int k = 0; k < n; ++k) {
     mcb200_ctx *c = b->m[k];
     step_prepare<R>(c);
     ck(cudaEventRecord(b->ev_member[k], c->stream), "event");
-    ck(cudaStreamWaitEvent(b->stream, b->ev_member[k], 0), "wait");
+    ck(cudaStreamWaitEvent((early >> k) & 1 ? b->side : b->stream, b->ev_member[k], 0), "wait");
   }
-  // 2. the batched flights on the batch stream
+  // 2. the batched flights
   FlightCtxT<R> F;
   F.T = b->m[0]->ts->dt;
   const int flip = (int)((b->steps_done - b->built_at) & 1);
   const BatchInstT<R> *tab = static_cast<const BatchInstT<R> *>(b->tables);
-  ck(cudaMemsetAsync(b->tickets, 0, sizeof(unsigned int) * (1 + mcb200_ctx::kGenerations), b->stream), "memset");
   const int sms = b->m[0]->sm_count;
-  if (launch_batch_flight<R>(F, tab + (size_t)flip * n, n, b->steps, false, b->tickets, b->blocks_per_sm, sms,
-                             b->stream))
+  unsigned int *side_ticket = b->tickets + 1 + mcb200_ctx::kGenerations;
+  if (early) {
+    ck(cudaMemsetAsync(side_ticket, 0, sizeof(unsigned int), b->side), "memset");
+    ck(cudaEventRecord(b->ev_side0, b->side), "event");  // the side counter is reset
+    if (launch_batch_flight<R>(F, tab + (size_t)flip * n, n, early, b->steps, false, side_ticket, 1, sms, b->side))
+      throw std::runtime_error("batched flight launch failed");
+    ck(cudaEventRecord(b->ev_side, b->side), "event");
+  }
+  ck(cudaMemsetAsync(b->tickets, 0, sizeof(unsigned int) * (1 + mcb200_ctx::kGenerations), b->stream), "memset");
+  if (launch_batch_flight<R>(F, tab + (size_t)flip * n, n, all & ~early, b->steps, false, b->tickets,
+                             b->blocks_per_sm, sms, b->stream))
     throw std::runtime_error("batched flight launch failed");
-  for (int g = 0; g < mcb200_ctx::kGenerations; ++g)
-    if (launch_batch_flight<R>(F, tab + (size_t)(2 + g) * n, n, b->steps, true, b->tickets + 1 + g, b->blocks_per_sm,
+  if (early) {  // the helper, then the side launch's end
+    ck(cudaStreamWaitEvent(b->stream, b->ev_side0, 0), "wait");
+    if (launch_batch_flight<R>(F, tab + (size_t)flip * n, n, early, b->steps, false, side_ticket, b->blocks_per_sm,
                                sms, b->stream))
+      throw std::runtime_error("batched flight launch failed");
+    ck(cudaStreamWaitEvent(b->stream, b->ev_side, 0), "wait");
+  }
+  for (int g = 0; g < mcb200_ctx::kGenerations; ++g)
+    if (launch_batch_flight<R>(F, tab + (size_t)(2 + g) * n, n, all, b->steps, true, b->tickets + 1 + g,
+                               b->blocks_per_sm, sms, b->stream))
       throw std::runtime_error("batched copy flight launch failed");
   advance_steps<<<(n + 63) / 64, 64, 0, b->stream>>>(b->steps, n);
   ck(cudaGetLastError(), "advance steps");
   ck(cudaEventRecord(b->ev_flight, b->stream), "event");
-  b->launches += 2 + mcb200_ctx::kGenerations;
+  b->launches += 2 + mcb200_ctx::kGenerations + (early ? 2 : 0);
   // 3. every member: its tail after the flights, on its own stream
   for (int k = 0; k < n; ++k) {
     mcb200_ctx *c = b->m[k];
@@ -238,7 +273,7 @@ void batch_full_step(mcb200_batch *b, uint64_t due) {
     mcb200_ctx *c = b->m[k];
     if (b->cfg[k].surface_rates && c->surf_cached) surface_rates_enqueue(c, c->stream);
   }
-  batch_transport<R>(b);
+  batch_transport<R>(b, b->overlap ? all_members(b) & ~due : 0);
   join_members(b);
 }
 
@@ -344,6 +379,9 @@ int mcb200_batch_create(mcb200_ctx *const *ctxs, const mcb200_batch_member *memb
   try {
     ck(cudaSetDevice(b->device), "cudaSetDevice");
     ck(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    ck(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking), "cudaStreamCreate");
+    ck(cudaEventCreateWithFlags(&b->ev_side, cudaEventDisableTiming), "cudaEventCreate");
+    ck(cudaEventCreateWithFlags(&b->ev_side0, cudaEventDisableTiming), "cudaEventCreate");
     ck(cudaEventCreateWithFlags(&b->ev_flight, cudaEventDisableTiming), "cudaEventCreate");
     ck(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming), "cudaEventCreate");
     ck(cudaEventCreateWithFlags(&b->ev_solved, cudaEventDisableTiming), "cudaEventCreate");
@@ -352,7 +390,7 @@ int mcb200_batch_create(mcb200_ctx *const *ctxs, const mcb200_batch_member *memb
     const size_t entry = b->precision == MCB200_FLIGHT_FP32 ? sizeof(BatchInstT<float>) : sizeof(BatchInstT<double>);
     ck(cudaMalloc(&b->tables, 6 * (size_t)n * entry), "cudaMalloc");
     ck(cudaMalloc(&b->steps, (size_t)n * sizeof(uint32_t)), "cudaMalloc");
-    ck(cudaMalloc(&b->tickets, (1 + mcb200_ctx::kGenerations) * sizeof(unsigned int)), "cudaMalloc");
+    ck(cudaMalloc(&b->tickets, (2 + mcb200_ctx::kGenerations) * sizeof(unsigned int)), "cudaMalloc");
     std::vector<uint32_t> first_steps(n);
     for (int k = 0; k < n; ++k) first_steps[k] = members[k].first_step;
     b->member_step = first_steps;
@@ -435,31 +473,37 @@ int mcb200_batch_autotune(mcb200_batch *b, int trial_steps, mcb200_batch_tuning 
   static const int grid_per_sm[] = {2, 4, 8};
   mcb200_batch_tuning win{0, 0, 0, 1e300, 0};
   int tried = 0;
+  auto apply = [&](const mcb200_batch_tuning &t) {
+    b->blocks_per_sm = t.flight_blocks_per_sm;
+    b->overlap = t.overlap != 0;
+    for (mcb200_ctx *c : b->m) c->grid_per_sm = t.grid_per_sm;
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->stream);
+    b->drop_graphs();  // the graphs hold the previous launch shapes
+  };
+  auto trial = [&](mcb200_batch_tuning t) -> int {
+    apply(t);
+    // one untimed step (it captures the graphs of this setting), then the timed ones
+    if (int rc = mcb200_batch_run(b, 1)) return rc;
+    if (int rc = mcb200_batch_mark(b, 6)) return rc;
+    if (int rc = mcb200_batch_run(b, trial_steps)) return rc;
+    if (int rc = mcb200_batch_mark(b, 7)) return rc;
+    double ms = 0;
+    if (int rc = mcb200_batch_elapsed_ms(b, 6, 7, &ms)) return rc;
+    t.ms_per_step = ms / trial_steps;
+    ++tried;
+    if (t.ms_per_step < win.ms_per_step) win = t;
+    return MCB200_OK;
+  };
+  const int overlap0 = b->overlap ? 1 : 0;
   for (int fb : flight_blocks)
-    for (int gs : grid_per_sm) {
-      b->blocks_per_sm = fb;
-      for (mcb200_ctx *c : b->m) c->grid_per_sm = gs;
-      {
-        cudaSetDevice(b->device);
-        cudaStreamSynchronize(b->stream);
-        b->drop_graphs();  // the graphs hold the previous grids
-      }
-      // one untimed step (it captures the graphs of this setting), then the timed ones
-      if (int rc = mcb200_batch_run(b, 1)) return rc;
-      if (int rc = mcb200_batch_mark(b, 6)) return rc;
-      if (int rc = mcb200_batch_run(b, trial_steps)) return rc;
-      if (int rc = mcb200_batch_mark(b, 7)) return rc;
-      double ms = 0;
-      if (int rc = mcb200_batch_elapsed_ms(b, 6, 7, &ms)) return rc;
-      ms /= trial_steps;
-      ++tried;
-      if (ms < win.ms_per_step) win = mcb200_batch_tuning{fb, gs, 0, ms, 0};
-    }
+    for (int gs : grid_per_sm)
+      if (int rc = trial(mcb200_batch_tuning{fb, gs, overlap0, 0.0, 0})) return rc;
+  mcb200_batch_tuning other = win;
+  other.overlap = 1 - overlap0;
+  if (int rc = trial(other)) return rc;
   win.candidates = tried;
-  b->blocks_per_sm = win.flight_blocks_per_sm;
-  for (mcb200_ctx *c : b->m) c->grid_per_sm = win.grid_per_sm;
-  cudaStreamSynchronize(b->stream);
-  b->drop_graphs();
+  apply(win);
   if (best) *best = win;
   return MCB200_OK;
 }
@@ -495,6 +539,15 @@ int mcb200_batch_sync(mcb200_batch *b) {
 int mcb200_batch_set_grid(mcb200_batch *b, int blocks_per_sm) {
   if (!b || blocks_per_sm < 0 || blocks_per_sm > 8) return MCB200_ERR_ARG;
   b->blocks_per_sm = blocks_per_sm;
+  return MCB200_OK;
+}
+
+int mcb200_batch_set_overlap(mcb200_batch *b, int enable) {
+  if (!b) return MCB200_ERR_ARG;
+  cudaSetDevice(b->device);
+  cudaStreamSynchronize(b->stream);
+  b->overlap = enable != 0;
+  b->drop_graphs();
   return MCB200_OK;
 }
 

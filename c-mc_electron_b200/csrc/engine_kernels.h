@@ -24,14 +24,15 @@ template <typename R>
 void launch_child_flight(const FlightCtxT<R> &F, const DevChildrenT<R> &in, int n_hint, unsigned int *ticket,
                          int sm_count, cudaStream_t s);
 // One persistent launch flying the particles (child == false) or the copies
-// of one generation (child == true) of `ninst` simulations (inst: device
-// table of BatchInstT, steps: their step numbers); blocks_per_sm <= 0: as
-// many as fit.  Returns 0 on success.
+// of one generation (child == true) of the simulations k < ninst with bit k
+// of `members` set (inst: device table of BatchInstT, steps: their step
+// numbers); blocks_per_sm <= 0: as many as fit.  Returns 0 on success.
 template <typename R>
 struct BatchInstT;
 template <typename R>
-int launch_batch_flight(const FlightCtxT<R> &F, const BatchInstT<R> *inst, int ninst, const uint32_t *steps,
-                        bool child, unsigned int *ticket, int blocks_per_sm, int sm_count, cudaStream_t s);
+int launch_batch_flight(const FlightCtxT<R> &F, const BatchInstT<R> *inst, int ninst, uint64_t members,
+                        const uint32_t *steps, bool child, unsigned int *ticket, int blocks_per_sm, int sm_count,
+                        cudaStream_t s);
 // FP32 flight's per-cell records (DevMesh::cell32), [cells][3] float4.
 void launch_cell_records32(const DevTables &T, const DevMesh &M, float4 *out, int cells, cudaStream_t s);
 // The step's surviving copies (all generations) ranked by (parent uid, sub),

@@ -224,10 +224,12 @@ constexpr size_t batch_smem_bytes(int ninst) {
 
 // F holds the band tables (its per-simulation part is unused); steps[k] is
 // simulation k's step number (device memory, advanced between steps).
+// Simulations whose bit in `members` is clear contribute no particles.
 template <typename R, bool kChild>
 __global__ void __launch_bounds__(256, kFlightBlocks<R>) batch_flight_kernel(const __grid_constant__ FlightCtxT<R> F,
                                                                              const BatchInstT<R> *inst,
-                                                                             int ninst, const uint32_t *steps,
+                                                                             int ninst, uint64_t members,
+                                                                             const uint32_t *steps,
                                                                              unsigned int *ticket) {
   extern __shared__ __align__(16) unsigned char batch_smem[];
   BatchInstT<R> *I = reinterpret_cast<BatchInstT<R> *>(batch_smem);
@@ -246,7 +248,8 @@ __global__ void __launch_bounds__(256, kFlightBlocks<R>) batch_flight_kernel(con
     for (int k = 0; k < ninst; ++k) {
       I[k].step = steps[k];
       prefix[k] = run;
-      run += kChild ? min((int)*I[k].in.count, I[k].in.capacity) : min((int)*I[k].n, I[k].capacity);
+      if ((members >> k) & 1ull)
+        run += kChild ? min((int)*I[k].in.count, I[k].in.capacity) : min((int)*I[k].n, I[k].capacity);
     }
     prefix[ninst] = run;
   }
@@ -540,8 +543,9 @@ void launch_child_flight(const FlightCtxT<R> &F, const DevChildrenT<R> &in, int 
   child_flight_kernel<R><<<flight_grid<R>(n_hint, 256, sm_count), 256, 0, s>>>(F, in, ticket);
 }
 template <typename R>
-int launch_batch_flight(const FlightCtxT<R> &F, const BatchInstT<R> *inst, int ninst, const uint32_t *steps,
-                        bool child, unsigned int *ticket, int blocks_per_sm, int sm_count, cudaStream_t s) {
+int launch_batch_flight(const FlightCtxT<R> &F, const BatchInstT<R> *inst, int ninst, uint64_t members,
+                        const uint32_t *steps, bool child, unsigned int *ticket, int blocks_per_sm, int sm_count,
+                        cudaStream_t s) {
   if (ninst < 1 || ninst > kMaxBatch) return 1;
   const size_t smem = batch_smem_bytes<R>(ninst);
   auto kernel = child ? batch_flight_kernel<R, true> : batch_flight_kernel<R, false>;
@@ -556,7 +560,7 @@ int launch_batch_flight(const FlightCtxT<R> &F, const BatchInstT<R> *inst, int n
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, smem) != cudaSuccess || per_sm < 1)
     return 1;
   if (blocks_per_sm > 0) per_sm = std::min(per_sm, blocks_per_sm);
-  kernel<<<per_sm * sm_count, 256, smem, s>>>(F, inst, ninst, steps, ticket);
+  kernel<<<per_sm * sm_count, 256, smem, s>>>(F, inst, ninst, members, steps, ticket);
   return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 void launch_cell_records32(const DevTables &T, const DevMesh &M, float4 *out, int cells, cudaStream_t s) {
@@ -605,8 +609,8 @@ void launch_cell_sort(const DevParticlesT<R> &src, DevCount n, const DevParticle
   template void launch_append_children<R>(const ChildSetT<R> &, uint64_t *, uint8_t *, uint32_t *,             \
                                           unsigned int *, const DevParticlesT<R> &, const unsigned int *, int,  \
                                           unsigned int *, unsigned int *, int, cudaStream_t);                   \
-  template int launch_batch_flight<R>(const FlightCtxT<R> &, const BatchInstT<R> *, int, const uint32_t *, bool, \
-                                      unsigned int *, int, int, cudaStream_t);                                  \
+  template int launch_batch_flight<R>(const FlightCtxT<R> &, const BatchInstT<R> *, int, uint64_t,             \
+                                      const uint32_t *, bool, unsigned int *, int, int, cudaStream_t);          \
   template void launch_cell_sort<R>(const DevParticlesT<R> &, DevCount, const DevParticlesT<R> &, int, int, int, \
                                     unsigned int *, unsigned int *, unsigned int *, unsigned int *, int,        \
                                     cudaStream_t);

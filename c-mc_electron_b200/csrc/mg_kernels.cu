@@ -273,8 +273,10 @@ struct Solve {
 
 // CG scalars as in the Jacobi solve: [0] rz, [3] rr, [6] ||b||^2, [7]
 // converged, [8] iterations, [9] (rel_tol ||b||)^2.  z = M r for the
-// initial residual is computed here.
-__global__ void __launch_bounds__(kRedBlock) cg_mg_persistent(int nodes, Grid3 g, const double *st7,
+// initial residual is computed here.  At most 64 registers a thread: two
+// blocks of the solve and one 256-thread block of the flight kernels fit
+// in an SM's registers together, so a solve can run beside a flight.
+__global__ void __launch_bounds__(kRedBlock, 4) cg_mg_persistent(int nodes, Grid3 g, const double *st7,
                                                               const uint8_t *dirichlet, double *x, double *r,
                                                               double *p0, double *p1, double *q, double *part,
                                                               double *sc, int max_iter,
@@ -441,9 +443,23 @@ extern "C" int mcb200_mg_trace_read(unsigned long long *out, int max_entries) {
 }
 #endif
 
+// An SM's shared-memory carveout is fixed while blocks run on it; with the
+// driver's choice for this kernel (its blocks need 2 KB) a flight block
+// (about 56 KB for a batch of 64) could not join an SM running the solve.
+// Preferring half the maximum lets both share an SM.  Once per device.
+static void configure_solve_kernel(int dev) {
+  static unsigned long long done = 0;
+  if (dev < 0 || dev >= 64 || ((done >> dev) & 1ull)) return;
+  if (cudaFuncSetAttribute(cg_mg_persistent, cudaFuncAttributePreferredSharedMemoryCarveout, 50) == cudaSuccess)
+    done |= 1ull << dev;
+  else
+    cudaGetLastError();  // a hint only: the solve runs without it
+}
+
 int cg_mg_max_grid() {
   int dev = 0, sms = 0, per_sm = 0, coop = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  configure_solve_kernel(dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
   if (!coop || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_mg_persistent, kRedBlock, 0) != cudaSuccess)
@@ -460,6 +476,8 @@ cudaError_t launch_cg_mg(int nodes, const Grid3 &g, const double *st7, const uin
   int nodes_arg = nodes, max_arg = max_iter;
   Grid3 g_arg = g;
   void *args[] = {&nodes_arg, &g_arg, &st7, &dirichlet, &x, &r, &p0, &p1, &q, &part, &sc, &max_arg, &mg};
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) configure_solve_kernel(dev);
   return cudaLaunchCooperativeKernel((const void *)cg_mg_persistent, grid, kRedBlock, args, 0, s);
 }
 

@@ -308,11 +308,13 @@ int mcb200_batch_run(mcb200_batch *batch, int steps);
 int mcb200_batch_use_graphs(mcb200_batch *batch, int enable);
 /* Launch shapes picked by measurement: for every candidate (batched-flight
  * blocks per SM in {1, 2} x blocks per SM of the members' per-step kernels
- * -- sort, deposition, copies -- in {2, 4, 8}) one untimed and `trial_steps`
- * timed full timesteps (mcb200_batch_run: they advance the simulations like
- * any other steps); the fastest by device time is kept and returned. */
+ * -- sort, deposition, copies -- in {2, 4, 8}; then the fastest of those
+ * with overlap switched) one untimed and `trial_steps` timed full timesteps
+ * (mcb200_batch_run: they advance the simulations like any other steps);
+ * the fastest by device time is kept and returned. */
 typedef struct {
-  int flight_blocks_per_sm, grid_per_sm, reserved;
+  int flight_blocks_per_sm, grid_per_sm;
+  int overlap; /* mcb200_batch_set_overlap */
   double ms_per_step;  /* of the kept setting */
   int candidates;
 } mcb200_batch_tuning;
@@ -321,6 +323,13 @@ int mcb200_batch_autotune(mcb200_batch *batch, int trial_steps, mcb200_batch_tun
 int mcb200_batch_sync(mcb200_batch *batch);
 /* Resident blocks per SM of the batched flight launches (0: as many as fit). */
 int mcb200_batch_set_grid(mcb200_batch *batch, int blocks_per_sm);
+/* Overlap (default on): in a full timestep where some members solve Poisson,
+ * the members that do not fly in a launch of their own on a second stream
+ * while the solves run (a solve leaves most of the device idle: its passes
+ * are bound by grid barriers); the solving members fly after their solves,
+ * and a helper launch then takes over what is left of the first launch's
+ * particles.  The result is the same either way. */
+int mcb200_batch_set_overlap(mcb200_batch *batch, int enable);
 /* CUDA events after every member's enqueued work (mcb200_mark for a batch). */
 int mcb200_batch_mark(mcb200_batch *batch, int slot);
 int mcb200_batch_elapsed_ms(mcb200_batch *batch, int from, int to, double *ms);

@@ -1,14 +1,18 @@
 """Batched stepping (mcb200_batch_*): simulations of uneven size -- two
-frozen-field bulk boxes of different mesh, particle count and field, and a
-self-consistent FinFET with GENERATE / CATCH contacts whose copies go
-through every generation of the copy flights -- step together in one
-batched flight launch per step.  Each member must end bit-identical to a
+frozen-field bulk boxes of different mesh, particle count and field, and
+two self-consistent FinFETs (gate lengths 20 and 15 nm) with GENERATE /
+CATCH contacts whose copies go through every generation of the copy
+flights -- step together in one batched flight launch per step; in full
+timesteps where a FinFET solves Poisson, the members not solving fly beside
+the solve (overlap: a side launch plus a helper launch sharing its work
+counter).  Each member must end bit-identical to a
 twin engine stepped alone (mcb200_deposit / mcb200_solve_poisson /
 mcb200_step) from the same state: every particle (matched by uid), every
 tally and the potential.  Both flight precisions; transport steps with the
 host's own density calls, and full timesteps run by the batch, with and
 without CUDA graphs.
 """
+import os
 import tempfile
 
 import numpy as np
@@ -26,9 +30,9 @@ BULK = [dict(particles=4000, seed=3, nx=10, ny=6, nz=6, field_v_per_m=1e6),
         dict(particles=24000, seed=4, nx=20, ny=10, nz=8, field_v_per_m=5e6)]
 
 
-def finfet_engine(tmp, precision, like):
-    deck = mcb200.Deck(decks.finfet(tmp, electrons=20000, holes=3000, surface_scatter=False, compute_heat=False)
-                       ["input"])
+def finfet_engine(tmp, precision, like, lg_nm=20.0, vg=0.8):
+    deck = mcb200.Deck(decks.finfet(tmp, electrons=20000, holes=3000, surface_scatter=False, compute_heat=False,
+                                    lg_nm=lg_nm, vg=vg)["input"])
     eng = mcb200.Engine(table_dir=mcb200.DEFAULT_TABLE_DIR, kelvin=deck.info()["temperature"],
                         max_particles=1 << 20, precision=precision, like=like)
     deck.apply(eng)
@@ -41,7 +45,7 @@ def finfet_engine(tmp, precision, like):
 
 
 def build(tmp, precision, like=None):
-    """The three members; the first made from scratch unless `like` is given,
+    """The four members; the first made from scratch unless `like` is given,
     the others alike.  Returns [(engine, dt, seed, self_consistent)]."""
     out = []
     for spec in BULK:
@@ -49,8 +53,10 @@ def build(tmp, precision, like=None):
                                      like=like if like is not None else (out[0][0] if out else None),
                                      **{k: v for k, v in spec.items() if k not in ("particles", "seed")})
         out.append((eng, dt, 100 + spec["seed"], False))
-    eng, dt = finfet_engine(tmp, precision, out[0][0])
+    eng, dt = finfet_engine(os.path.join(tmp, "a"), precision, out[0][0])
     out.append((eng, dt, 200, True))
+    eng, dt = finfet_engine(os.path.join(tmp, "b"), precision, out[0][0], lg_nm=15.0, vg=0.5)
+    out.append((eng, dt, 300, True))
     return out
 
 
@@ -91,7 +97,7 @@ def test_batch_matches_members_alone(precision):
         batch.step()
     batch.sync()
     info = batch.info()
-    assert info["members"] == 3 and info["steps"] == STEPS and info["launches"] == STEPS * 6
+    assert info["members"] == 4 and info["steps"] == STEPS and info["launches"] == STEPS * 6
     for (ea, *_), (eb, *_) in zip(alone, batched):
         a, b = by_uid(ea), by_uid(eb)
         assert a["uid"].size > 0
@@ -105,13 +111,17 @@ def test_batch_matches_members_alone(precision):
         eng.close()
 
 
-@pytest.mark.parametrize("precision,graphs", [(mcb200.FLIGHT_FP64, False), (mcb200.FLIGHT_FP64, True),
-                                              (mcb200.FLIGHT_FP32, True)])
-def test_batch_run_matches_members_alone(precision, graphs):
+@pytest.mark.parametrize("precision,graphs,overlap", [(mcb200.FLIGHT_FP64, False, True),
+                                                      (mcb200.FLIGHT_FP64, True, True),
+                                                      (mcb200.FLIGHT_FP32, True, True),
+                                                      (mcb200.FLIGHT_FP64, True, False)])
+def test_batch_run_matches_members_alone(precision, graphs, overlap):
     with tempfile.TemporaryDirectory() as t1, tempfile.TemporaryDirectory() as t2:
         alone = build(t1, precision)
         batched = build(t2, precision, like=alone[0][0])
-    first = [0, 3, 5]  # members start at different step numbers: different Poisson phases
+    # members start at different step numbers: the FinFETs solve on different
+    # steps (t = 3, 7, 11 and 2, 6, 10), each flying beside the other's solve
+    first = [0, 3, 5, 2]
     for step in range(STEPS):
         for (eng, dt, seed, sc), f in zip(alone, first):
             density(eng, f + step, sc)
@@ -120,11 +130,13 @@ def test_batch_run_matches_members_alone(precision, graphs):
                                       poisson_every=POISSON_EVERY))
                           for (eng, dt, seed, sc), f in zip(batched, first)])
     batch.use_graphs(graphs)
+    batch.set_overlap(overlap)
     batch.run(STEPS // 2)
     batch.run(STEPS - STEPS // 2)
     batch.sync()
     info = batch.info()
-    assert info["steps"] == STEPS and info["launches"] == STEPS * 6
+    solving = 6  # steps with a solve: two more launches each (side flight and helper) with overlap
+    assert info["steps"] == STEPS and info["launches"] == STEPS * 6 + (2 * solving if overlap else 0)
     if graphs:
         assert info["graph_captures"] >= 2 and info["graph_captures"] + info["graph_replays"] == STEPS
     for (ea, *_), (eb, *_) in zip(alone, batched):
@@ -132,9 +144,10 @@ def test_batch_run_matches_members_alone(precision, graphs):
         for k in a:
             assert np.array_equal(a[k], b[k]), k
         same_tallies(ea.tallies(), eb.tallies())
-    pa, pb = alone[2][0].array("potential"), batched[2][0].array("potential")
-    assert np.array_equal(pa.view(np.uint64), pb.view(np.uint64))
-    assert alone[2][0].poisson_stats() == batched[2][0].poisson_stats()
+    for k in (2, 3):
+        pa, pb = alone[k][0].array("potential"), batched[k][0].array("potential")
+        assert np.array_equal(pa.view(np.uint64), pb.view(np.uint64))
+        assert alone[k][0].poisson_stats() == batched[k][0].poisson_stats()
     batch.close()
     for eng, *_ in batched + alone:
         eng.close()
