@@ -292,9 +292,11 @@ def batch_arm(args, device: int) -> dict:
     FinFETs (Lg 15/20/30 nm, Vg 0-0.8 V), particle counts log-uniform in
     5k-500k, FP32 flight.  Full timesteps through the batch (one flight
     launch per step for all members, steps replayed from CUDA graphs, launch
-    shapes from the autotuner) against the same members stepped one by one
-    on their own streams.  Device time between batch marks (every member's
-    stream joined), particle-steps from the members' device counters."""
+    shapes, overlap and solve pairing from the autotuner) against the same
+    members stepped one by one on their own streams, the two timed in
+    interleaved windows of 20 steps (batched, alone, alone, batched).  Device
+    time between batch marks (every member's stream joined), particle-steps
+    from the members' device counters."""
     import mcb200
     from mcb200 import batching
 
@@ -308,18 +310,29 @@ def batch_arm(args, device: int) -> dict:
     for m in members:
         m.step += batch.info()["steps"] - s0
 
-    def timed(run):
-        run(10)  # warm-up
+    def window(run, k):
         ps0 = batching.particle_steps(members)
         batch.mark(0)
-        run(BATCH_STEPS)
+        run(k)
         batch.mark(1)
-        ms = batch.elapsed_ms(0, 1)
-        return (batching.particle_steps(members) - ps0) / (ms * 1e-3), ms / BATCH_STEPS
+        return batching.particle_steps(members) - ps0, batch.elapsed_ms(0, 1)
 
+    run_b = lambda k: batching.run_batched(batch, members, k)  # noqa: E731
+    run_a = lambda k: batching.run_alone(members, k)  # noqa: E731
+    run_b(10)  # warm-ups: graphs of every step kind, first launches
+    run_a(10)
+    # The members' particle counts drift as they evolve, so the two arms are
+    # timed in interleaved windows (batched, alone, alone, batched, ...): a
+    # steady drift weighs on both alike.
+    tot = {"b": [0, 0.0], "a": [0, 0.0]}
+    order = ["b", "a", "a", "b"]
     with ClockSampler(device) as clocks:
-        batched, ms_b = timed(lambda k: batching.run_batched(batch, members, k))
-        alone, ms_a = timed(lambda k: batching.run_alone(members, k))
+        for arm in order:
+            ps, ms = window(run_b if arm == "b" else run_a, BATCH_STEPS // 2)
+            tot[arm][0] += ps
+            tot[arm][1] += ms
+    batched, ms_b = tot["b"][0] / (tot["b"][1] * 1e-3), tot["b"][1] / BATCH_STEPS
+    alone, ms_a = tot["a"][0] / (tot["a"][1] * 1e-3), tot["a"][1] / BATCH_STEPS
     info = batch.info()
     kinds = [m.kind for m in members]
     out = {"metric": "particle-steps/s", "members": len(members), "bulk": kinds.count("bulk"),

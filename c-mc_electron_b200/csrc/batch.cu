@@ -43,6 +43,7 @@ struct mcb200_batch {
   uint32_t *steps = nullptr;       // device: step number of each member
   unsigned int *tickets = nullptr;  // device: work counters of the batched launches (main, 4 copy generations, side)
   bool overlap = true;              // fly the members not solving Poisson beside the solves
+  bool pair_solves = true;          // two multigrid solves of the same shape per cooperative launch
   std::vector<unsigned char> snap;  // per member: DevMesh, DevTallies and store parity the tables were built for
   uint64_t steps_done = 0, built_at = 0;
   int blocks_per_sm = 0;  // batched flight grid (0: as many as fit); mcb200_batch_autotune
@@ -257,14 +258,46 @@ void batch_full_step(mcb200_batch *b, uint64_t due) {
     if (b->cfg[k].self_consistent && c->device_set) deposit_enqueue(c, c->stream);
   }
   if (due) {
+    // on the batch stream: every due member's set-up, the solves (two
+    // multigrid solves of the same shape share a launch when pairing is on),
+    // then the residuals and fields
+    std::vector<int> solving;
     for (int k = 0; k < n; ++k) {
       if (!((due >> k) & 1)) continue;
       mcb200_ctx *c = b->m[k];
       ck(cudaEventRecord(b->ev_member[k], c->stream), "event");
       ck(cudaStreamWaitEvent(b->stream, b->ev_member[k], 0), "wait");
-      poisson_enqueue(c, b->stream, b->cfg[k].poisson_rel_tol > 0 ? b->cfg[k].poisson_rel_tol : 1e-10, 20000,
-                      nullptr, nullptr);
+      poisson_prepare(c, b->stream, b->cfg[k].poisson_rel_tol > 0 ? b->cfg[k].poisson_rel_tol : 1e-10);
+      solving.push_back(k);
     }
+    constexpr int kMaxIter = 20000;
+    std::vector<char> launched(n, 0);
+    for (size_t i = 0; i < solving.size(); ++i) {
+      const int k0 = solving[i];
+      if (launched[k0]) continue;
+      mcb200_ctx *c0 = b->m[k0];
+      launched[k0] = 1;
+      int k1 = -1;
+      if (b->pair_solves && c0->cg_plan.used == kCgMultigrid && cg_mg_pair_fits(c0->cg_plan.grid))
+        for (size_t j = i + 1; j < solving.size() && k1 < 0; ++j) {
+          mcb200_ctx *c = b->m[solving[j]];
+          if (!launched[solving[j]] && c->cg_plan.used == kCgMultigrid && c->cg_plan.grid == c0->cg_plan.grid &&
+              c->fb.mg->levels == c0->fb.mg->levels && c->fb.mg->nu == c0->fb.mg->nu)
+            k1 = solving[j];
+        }
+      if (k1 >= 0) {
+        mcb200_ctx *c1 = b->m[k1];
+        launched[k1] = 1;
+        const MgSystem two[2] = {cg_mg_system(c0->mesh, c0->fb, kMaxIter), cg_mg_system(c1->mesh, c1->fb, kMaxIter)};
+        ck(launch_cg_mg_pair(two, c0->cg_plan.grid, b->stream), "paired Poisson solve");
+        c0->cg_plan.launches += 1;
+        c1->cg_plan.launches += 1;
+        b->launches += 1;
+      } else if (cg_launch(c0->mesh, c0->fb, kMaxIter, b->stream, c0->cg_plan)) {
+        throw CudaError("Poisson solve failed");
+      }
+    }
+    for (int k : solving) poisson_finish(b->m[k], b->stream, nullptr, nullptr);
     ck(cudaEventRecord(b->ev_solved, b->stream), "event");
     for (int k = 0; k < n; ++k)
       if ((due >> k) & 1) ck(cudaStreamWaitEvent(b->m[k]->stream, b->ev_solved, 0), "wait");
@@ -471,37 +504,64 @@ int mcb200_batch_autotune(mcb200_batch *b, int trial_steps, mcb200_batch_tuning 
   if (!b || trial_steps < 1) return MCB200_ERR_ARG;
   static const int flight_blocks[] = {1, 2};
   static const int grid_per_sm[] = {2, 4, 8};
-  mcb200_batch_tuning win{0, 0, 0, 1e300, 0};
+  mcb200_batch_tuning win{0, 0, 0, 1e300, 0, 0};
   int tried = 0;
   auto apply = [&](const mcb200_batch_tuning &t) {
     b->blocks_per_sm = t.flight_blocks_per_sm;
     b->overlap = t.overlap != 0;
+    b->pair_solves = t.pair_solves != 0;
     for (mcb200_ctx *c : b->m) c->grid_per_sm = t.grid_per_sm;
     cudaSetDevice(b->device);
     cudaStreamSynchronize(b->stream);
     b->drop_graphs();  // the graphs hold the previous launch shapes
   };
-  auto trial = [&](mcb200_batch_tuning t) -> int {
+  // ms per step of one setting: one untimed step (it captures the graphs of
+  // this setting), then the timed ones
+  auto measure = [&](const mcb200_batch_tuning &t, double &ms) -> int {
     apply(t);
-    // one untimed step (it captures the graphs of this setting), then the timed ones
     if (int rc = mcb200_batch_run(b, 1)) return rc;
     if (int rc = mcb200_batch_mark(b, 6)) return rc;
     if (int rc = mcb200_batch_run(b, trial_steps)) return rc;
     if (int rc = mcb200_batch_mark(b, 7)) return rc;
-    double ms = 0;
     if (int rc = mcb200_batch_elapsed_ms(b, 6, 7, &ms)) return rc;
-    t.ms_per_step = ms / trial_steps;
-    ++tried;
-    if (t.ms_per_step < win.ms_per_step) win = t;
+    ms /= trial_steps;
     return MCB200_OK;
   };
-  const int overlap0 = b->overlap ? 1 : 0;
+  // The simulations change while they are timed (particle counts drift), so
+  // the candidates of a stage are timed in order and again in reverse order
+  // and each keeps the mean of its two times: a linear drift cancels.
+  auto stage = [&](const std::vector<mcb200_batch_tuning> &cands) -> int {
+    std::vector<double> sum(cands.size(), 0.0);
+    for (int pass = 0; pass < 2; ++pass)
+      for (size_t i = 0; i < cands.size(); ++i) {
+        const size_t j = pass == 0 ? i : cands.size() - 1 - i;
+        double ms = 0;
+        if (int rc = measure(cands[j], ms)) return rc;
+        sum[j] += ms;
+      }
+    win.ms_per_step = 1e300;
+    for (size_t i = 0; i < cands.size(); ++i)
+      if (sum[i] / 2 < win.ms_per_step) {
+        win = cands[i];
+        win.ms_per_step = sum[i] / 2;
+      }
+    tried += (int)cands.size();
+    return MCB200_OK;
+  };
+  const int overlap0 = b->overlap ? 1 : 0, pair0 = b->pair_solves ? 1 : 0;
+  std::vector<mcb200_batch_tuning> shapes;
   for (int fb : flight_blocks)
-    for (int gs : grid_per_sm)
-      if (int rc = trial(mcb200_batch_tuning{fb, gs, overlap0, 0.0, 0})) return rc;
-  mcb200_batch_tuning other = win;
-  other.overlap = 1 - overlap0;
-  if (int rc = trial(other)) return rc;
+    for (int gs : grid_per_sm) shapes.push_back(mcb200_batch_tuning{fb, gs, overlap0, 0.0, 0, pair0});
+  if (int rc = stage(shapes)) return rc;
+  std::vector<mcb200_batch_tuning> modes;  // overlap and pairing, with the fastest launch shapes
+  for (int v = 0; v < 4; ++v) {
+    mcb200_batch_tuning t = win;
+    t.overlap = v & 1 ? 1 - overlap0 : overlap0;
+    t.pair_solves = v & 2 ? 1 - pair0 : pair0;
+    modes.push_back(t);
+  }
+  if (int rc = stage(modes)) return rc;
+  tried -= 1;  // the fastest shape was timed in both stages
   win.candidates = tried;
   apply(win);
   if (best) *best = win;
@@ -547,6 +607,15 @@ int mcb200_batch_set_overlap(mcb200_batch *b, int enable) {
   cudaSetDevice(b->device);
   cudaStreamSynchronize(b->stream);
   b->overlap = enable != 0;
+  b->drop_graphs();
+  return MCB200_OK;
+}
+
+int mcb200_batch_set_pairing(mcb200_batch *b, int enable) {
+  if (!b) return MCB200_ERR_ARG;
+  cudaSetDevice(b->device);
+  cudaStreamSynchronize(b->stream);
+  b->pair_solves = enable != 0;
   b->drop_graphs();
   return MCB200_OK;
 }

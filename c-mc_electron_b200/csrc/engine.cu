@@ -1523,12 +1523,21 @@ namespace mcb200::eng {
 // cooperative launches must not run at the same time on a device (each
 // needs all its blocks resident at once, and two partly resident grids
 // could wait on each other for ever): callers enqueue solves in one order.
-void poisson_enqueue(mcb200_ctx *c, cudaStream_t s, double rel_tol, int max_iter, int *iterations,
-                     double *rel_residual) {
+void poisson_prepare(mcb200_ctx *c, cudaStream_t s, double rel_tol) {
   const int nodes = (c->mesh.nx + 1) * (c->mesh.ny + 1) * (c->mesh.nz + 1);
   launch_rhs(nodes, c->fb, s);
-  if (cg_solve(c->mesh, c->fb, rel_tol, max_iter, s, c->h_scratch, iterations, rel_residual, c->cg_plan))
-    throw CudaError("Poisson solve failed");
+  if (cg_prepare(c->mesh, c->fb, rel_tol, s, c->cg_plan)) throw CudaError("Poisson solve failed");
+}
+
+void poisson_enqueue(mcb200_ctx *c, cudaStream_t s, double rel_tol, int max_iter, int *iterations,
+                     double *rel_residual) {
+  poisson_prepare(c, s, rel_tol);
+  if (cg_launch(c->mesh, c->fb, max_iter, s, c->cg_plan)) throw CudaError("Poisson solve failed");
+  poisson_finish(c, s, iterations, rel_residual);
+}
+
+void poisson_finish(mcb200_ctx *c, cudaStream_t s, int *iterations, double *rel_residual) {
+  if (cg_finish(c->mesh, c->fb, s, c->h_scratch, iterations, rel_residual)) throw CudaError("Poisson solve failed");
   launch_pot2field(c->mesh, c->fb.potential, s);
   ck(cudaGetLastError(), "pot2field");
   // rhs, the solve's set-up / dots / persistent CG / true residual /

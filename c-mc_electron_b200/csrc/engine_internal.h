@@ -233,6 +233,11 @@ void push_counts(mcb200_ctx *c);
 int grid_for(const mcb200_ctx *c, size_t n, int block);
 void poisson_enqueue(mcb200_ctx *c, cudaStream_t s, double rel_tol, int max_iter, int *iterations,
                      double *rel_residual);
+// poisson_enqueue around a caller's own launch of the solve: the right side
+// and the CG set-up (fixes c->cg_plan), then, after the launch, the true
+// residual, statistics and fields.
+void poisson_prepare(mcb200_ctx *c, cudaStream_t s, double rel_tol);
+void poisson_finish(mcb200_ctx *c, cudaStream_t s, int *iterations, double *rel_residual);
 void surface_rates_enqueue(mcb200_ctx *c, cudaStream_t s);
 void deposit_enqueue(mcb200_ctx *c, cudaStream_t s);
 // The parts of a transport step around its flights (engine.cu).

@@ -450,8 +450,7 @@ static void dot(int n, const double *a, const double *b, double *part, double *o
   dot_final<<<1, kRedBlock, 0, s>>>(part, out);
 }
 
-int cg_solve(const DevMesh &M, const FieldBuffers &f, double rel_tol, int max_iter, cudaStream_t s,
-             double *host_scratch, int *iterations, double *rel_residual, CgPlan &plan) {
+int cg_prepare(const DevMesh &M, const FieldBuffers &f, double rel_tol, cudaStream_t s, CgPlan &plan) {
   const int nodes = (M.nx + 1) * (M.ny + 1) * (M.nz + 1);
   const Grid3 g{M.nx + 1, M.ny + 1, M.nz + 1};
   const int nb = blocks(nodes, 256);
@@ -470,7 +469,7 @@ int cg_solve(const DevMesh &M, const FieldBuffers &f, double rel_tol, int max_it
   }
   dot(nodes, f.cg_r, f.cg_r, f.cg_part, sc + 3, s);
   cg_setup<<<1, 1, 0, s>>>(sc, rel_tol * rel_tol);
-  // every iteration in one cooperative launch (cg_persistent / cg_mg_persistent)
+  // the persistent launch's grid, fixed per context (so is the reduction order)
   if (plan.grid == 0 || plan.used != (use_mg ? kCgMultigrid : kCgJacobi)) {
     int dev = 0, sms = 0, per_sm = 0, coop = 0, most = 0;
     cudaGetDevice(&dev);
@@ -491,8 +490,29 @@ int cg_solve(const DevMesh &M, const FieldBuffers &f, double rel_tol, int max_it
     plan.grid = plan.blocks > 0 ? std::min(plan.blocks, most) : fallback;
     plan.used = use_mg ? kCgMultigrid : kCgJacobi;
   }
+  return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+MgSystem cg_mg_system(const DevMesh &M, const FieldBuffers &f, int max_iter) {
+  MgSystem y;
+  y.mg = *f.mg;
+  y.mg.L[0].b = f.cg_r;
+  y.mg.L[0].xa = f.cg_z;
+  y.st7 = f.stencil;
+  y.dirichlet = f.dirichlet;
+  y.x = f.potential; y.r = f.cg_r; y.p0 = f.cg_p; y.p1 = f.cg_p1; y.q = f.cg_q; y.part = f.cg_part;
+  y.sc = f.cg_scalars;
+  y.px = M.nx + 1; y.py = M.ny + 1; y.pz = M.nz + 1;
+  y.max_iter = max_iter;
+  return y;
+}
+
+int cg_launch(const DevMesh &M, const FieldBuffers &f, int max_iter, cudaStream_t s, CgPlan &plan) {
+  const int nodes = (M.nx + 1) * (M.ny + 1) * (M.nz + 1);
+  const Grid3 g{M.nx + 1, M.ny + 1, M.nz + 1};
   double *x = f.potential, *r = f.cg_r, *z = f.cg_z, *p0 = f.cg_p, *p1 = f.cg_p1, *q = f.cg_q, *part = f.cg_part;
-  if (use_mg) {
+  double *sc = f.cg_scalars;
+  if (plan.used == kCgMultigrid) {
     if (launch_cg_mg(nodes, g, f.stencil, f.dirichlet, x, r, z, p0, p1, q, part, sc, max_iter, *f.mg, plan.grid, s) !=
         cudaSuccess)
       return 1;
@@ -506,8 +526,17 @@ int cg_solve(const DevMesh &M, const FieldBuffers &f, double rel_tol, int max_it
       return 1;
   }
   plan.launches += 1;
+  return 0;
+}
+
+int cg_finish(const DevMesh &M, const FieldBuffers &f, cudaStream_t s, double *host_scratch, int *iterations,
+              double *rel_residual) {
+  const int nodes = (M.nx + 1) * (M.ny + 1) * (M.nz + 1);
+  const int nb = blocks(nodes, 256);
+  double *sc = f.cg_scalars;
   // true residual of the final iterate, and the running statistics
-  stencil_apply<<<nb, 256, 0, s>>>(nodes, g, f.stencil, f.dirichlet, f.potential, f.rhs, f.cg_r);
+  stencil_apply<<<nb, 256, 0, s>>>(nodes, Grid3{M.nx + 1, M.ny + 1, M.nz + 1}, f.stencil, f.dirichlet, f.potential,
+                                   f.rhs, f.cg_r);
   dot(nodes, f.cg_r, f.cg_r, f.cg_part, sc + 3, s);
   poisson_stats_kernel<<<1, 32, 0, s>>>(sc, f.poisson_stats);
   if (!iterations && !rel_residual) return cudaGetLastError() == cudaSuccess ? 0 : 1;  // nothing waits
@@ -517,6 +546,12 @@ int cg_solve(const DevMesh &M, const FieldBuffers &f, double rel_tol, int max_it
   if (iterations) *iterations = (int)host_scratch[8];
   if (rel_residual) *rel_residual = sqrt(host_scratch[3]) / bnorm;
   return 0;
+}
+
+int cg_solve(const DevMesh &M, const FieldBuffers &f, double rel_tol, int max_iter, cudaStream_t s,
+             double *host_scratch, int *iterations, double *rel_residual, CgPlan &plan) {
+  if (cg_prepare(M, f, rel_tol, s, plan) || cg_launch(M, f, max_iter, s, plan)) return 1;
+  return cg_finish(M, f, s, host_scratch, iterations, rel_residual);
 }
 
 void launch_pot2field(const DevMesh &M, const double *pot, cudaStream_t s) {

@@ -61,6 +61,16 @@ struct CgPlan {
 // results only reach f.poisson_stats).
 int cg_solve(const DevMesh &M, const FieldBuffers &f, double rel_tol, int max_iter, cudaStream_t s,
              double *host_scratch, int *iterations, double *rel_residual, CgPlan &plan);
+// cg_solve in three parts, for callers that launch several solves together:
+// the set-up (right side, residual, tolerances, the plan's grid), the
+// persistent launch, the true residual and statistics.  Each returns 0 on
+// success.  cg_mg_system: the multigrid launch's arguments (plan.used ==
+// kCgMultigrid, after cg_prepare) for launch_cg_mg_pair.
+int cg_prepare(const DevMesh &M, const FieldBuffers &f, double rel_tol, cudaStream_t s, CgPlan &plan);
+int cg_launch(const DevMesh &M, const FieldBuffers &f, int max_iter, cudaStream_t s, CgPlan &plan);
+int cg_finish(const DevMesh &M, const FieldBuffers &f, cudaStream_t s, double *host_scratch, int *iterations,
+              double *rel_residual);
+MgSystem cg_mg_system(const DevMesh &M, const FieldBuffers &f, int max_iter);
 void launch_pot2field(const DevMesh &M, const double *pot, cudaStream_t s);
 
 }  // namespace mcb200

@@ -225,38 +225,41 @@ struct Solve {
   }
 
   // z = M r.  On entry level 0's first sweep is in X(0) (levels > 1); on
-  // exit X(0) holds z, part_rz the block partials of r.z, and the grid has
-  // synchronised.
-  __device__ void vcycle(cg::grid_group &grid, double *part_rz) {
+  // exit X(0) holds z, part_rz the block partials of r.z (block vb of the
+  // solve), and the grid has synchronised.  Without `work` only the grid
+  // barriers are taken (a block of a finished solve sharing the launch).
+  __device__ void vcycle(cg::grid_group &grid, double *part_rz, int vb, bool work) {
     const int L = mg.levels;
     double rz = 0.0;
     if (L == 1) {
-      rz = dense(0);
+      if (work) rz = dense(0);
     } else {
       for (int l = 0; l + 1 < L; ++l) {
         for (int s = 1; s < mg.nu; ++s) {
-          sweep(l, false);
+          if (work) sweep(l, false);
           grid.sync();
           trace(10 * l + 1);
         }
-        residual(l);
+        if (work) residual(l);
         grid.sync();
         trace(10 * l + 2);
-        restrict_to(l);
+        if (work) restrict_to(l);
         grid.sync();
         trace(10 * l + 3);
       }
-      dense(L - 1);
+      if (work) dense(L - 1);
       grid.sync();
       trace(10 * (L - 1) + 4);
       for (int l = L - 2; l >= 0; --l) {
-        prolong(l);
+        if (work) prolong(l);
         grid.sync();
         trace(10 * l + 5);
         for (int s = 0; s < mg.nu; ++s) {
           const bool last = l == 0 && s + 1 == mg.nu;
-          const double v = sweep(l, last);
-          if (last) rz = v;
+          if (work) {
+            const double v = sweep(l, last);
+            if (last) rz = v;
+          }
           if (!last) {
             grid.sync();
             trace(10 * l + 6);
@@ -265,7 +268,7 @@ struct Solve {
       }
     }
     const double bs = block_sum<kRedBlock>(rz);
-    if (threadIdx.x == 0) part_rz[blockIdx.x] = bs;
+    if (threadIdx.x == 0 && work) part_rz[vb] = bs;
     grid.sync();
     trace(7);
   }
@@ -273,98 +276,156 @@ struct Solve {
 
 // CG scalars as in the Jacobi solve: [0] rz, [3] rr, [6] ||b||^2, [7]
 // converged, [8] iterations, [9] (rel_tol ||b||)^2.  z = M r for the
-// initial residual is computed here.  At most 64 registers a thread: two
-// blocks of the solve and one 256-thread block of the flight kernels fit
-// in an SM's registers together, so a solve can run beside a flight.
-__global__ void __launch_bounds__(kRedBlock, 4) cg_mg_persistent(int nodes, Grid3 g, const double *st7,
-                                                              const uint8_t *dirichlet, double *x, double *r,
-                                                              double *p0, double *p1, double *q, double *part,
-                                                              double *sc, int max_iter,
-                                                              const __grid_constant__ MgDevice mg) {
+// initial residual is computed here.
+//
+// K solves share the launch: block b works for solve b / grid on its own
+// grid of `grid` blocks (local block b % grid), so each solve runs as it
+// would alone.  Every block follows every solve's residual norm (each
+// computes the same fixed-order sums), so all blocks agree on when the
+// launch ends; a block whose solve has finished takes only the barriers.
+template <int K>
+struct MgGroup {
+  MgSystem s[K];
+  int grid;
+};
+
+template <int K>
+__device__ __forceinline__ void cg_mg_body(const MgGroup<K> &G) {
   cg::grid_group grid = cg::this_grid();
-  const int nblk = gridDim.x;
-  double *part_pq = part, *part_rz = part + nblk, *part_rr = part + 2 * nblk;
-  Solve S{mg, st7, g, (int)(blockIdx.x * blockDim.x + threadIdx.x), (int)(gridDim.x * blockDim.x), 0u};
-  const double tol2 = sc[9];
-  bool done = sc[7] != 0.0;
-  double rr = sc[3], rz = 0.0, beta = 0.0;
-  int it = 0;
+  const int nblk = G.grid;
+  const int me = K == 1 ? 0 : (int)blockIdx.x / nblk;
+  const int vb = (int)blockIdx.x - me * nblk;
+  const MgSystem &Y = G.s[me];
+  const Grid3 g{Y.px, Y.py, Y.pz};
+  const int nodes = g.px * g.py * g.pz;
+  const double *st7 = Y.st7;
+  const uint8_t *dirichlet = Y.dirichlet;
+  double *x = Y.x, *r = Y.r, *q = Y.q;
+  double *part_pq = Y.part, *part_rz = Y.part + nblk, *part_rr = Y.part + 2 * nblk;
+  Solve S{Y.mg, st7, g, vb * kRedBlock + (int)threadIdx.x, nblk * kRedBlock, 0u};
+  bool done[K];
+  int it[K];
+  bool any = false;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    done[k] = G.s[k].sc[7] != 0.0;
+    it[k] = 0;
+    any = any || !done[k];
+  }
+  double rr = Y.sc[3], rz = 0.0, beta = 0.0;
   trace(0);
-  if (!done) {
-    if (mg.levels > 1) {
-      for (int n = S.tid; n < nodes; n += S.stride) S.first(0, n, r[n]);
+  if (any) {
+    const bool work = !done[me];
+    if (Y.mg.levels > 1) {
+      if (work)
+        for (int n = S.tid; n < nodes; n += S.stride) S.first(0, n, r[n]);
       grid.sync();
     }
-    S.vcycle(grid, part_rz);
-    rz = sum_partials(part_rz, nblk);
+    S.vcycle(grid, part_rz, vb, work);
+    if (work) rz = sum_partials(part_rz, nblk);
   }
-  const double *pin = p0;
-  double *pout = p1;
-  while (!done && it < max_iter) {
+  const double *pin = Y.p0;
+  double *pout = Y.p1;
+  for (;;) {
+    bool act[K];
+    any = false;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      act[k] = !done[k] && it[k] < G.s[k].max_iter;
+      any = any || act[k];
+    }
+    if (!any) break;
+    const bool work = act[me];
     const double *z = S.X(0);
     double v = 0.0;
-    for (int n = S.tid; n < nodes; n += S.stride) {
-      if (dirichlet[n]) {
-        q[n] = 0.0;
-        pout[n] = 0.0;
-        continue;
+    if (work) {
+      const int first = it[me] == 0;
+      for (int n = S.tid; n < nodes; n += S.stride) {
+        if (dirichlet[n]) {
+          q[n] = 0.0;
+          pout[n] = 0.0;
+          continue;
+        }
+        // z and p vanish on Dirichlet nodes, so neighbours need no mask
+        int i, j, k;
+        node_ijk(n, g, i, j, k);
+        const double *a = st7 + (size_t)n * 7;
+        // (pin is not read in the first iteration: it holds no p yet)
+        auto P = [&](int m) { return first ? z[m] : z[m] + beta * pin[m]; };
+        const double pn = P(n);
+        pout[n] = pn;
+        double acc = a[6] * pn;
+        if (i > 0) acc += a[0] * P(n - g.pz);
+        if (i + 1 < g.px) acc += a[1] * P(n + g.pz);
+        if (j > 0) acc += a[2] * P(n - g.px * g.pz);
+        if (j + 1 < g.py) acc += a[3] * P(n + g.px * g.pz);
+        if (k > 0) acc += a[4] * P(n - 1);
+        if (k + 1 < g.pz) acc += a[5] * P(n + 1);
+        q[n] = acc;
+        v += pn * acc;
       }
-      // z and p vanish on Dirichlet nodes, so neighbours need no mask
-      int i, j, k;
-      node_ijk(n, g, i, j, k);
-      const double *a = st7 + (size_t)n * 7;
-      // (pin is not read in the first iteration: it holds no p yet)
-      auto P = [&](int m) { return it == 0 ? z[m] : z[m] + beta * pin[m]; };
-      const double pn = P(n);
-      pout[n] = pn;
-      double acc = a[6] * pn;
-      if (i > 0) acc += a[0] * P(n - g.pz);
-      if (i + 1 < g.px) acc += a[1] * P(n + g.pz);
-      if (j > 0) acc += a[2] * P(n - g.px * g.pz);
-      if (j + 1 < g.py) acc += a[3] * P(n + g.px * g.pz);
-      if (k > 0) acc += a[4] * P(n - 1);
-      if (k + 1 < g.pz) acc += a[5] * P(n + 1);
-      q[n] = acc;
-      v += pn * acc;
     }
     const double bs = block_sum<kRedBlock>(v);
-    if (threadIdx.x == 0) part_pq[blockIdx.x] = bs;
+    if (threadIdx.x == 0 && work) part_pq[vb] = bs;
     grid.sync();
     trace(100);
-    const double alpha = rz / sum_partials(part_pq, nblk);
     double a2 = 0.0;
-    for (int n = S.tid; n < nodes; n += S.stride) {
-      if (dirichlet[n]) {
-        if (mg.levels > 1) S.X(0)[n] = 0.0;
-        continue;
+    if (work) {
+      const double alpha = rz / sum_partials(part_pq, nblk);
+      for (int n = S.tid; n < nodes; n += S.stride) {
+        if (dirichlet[n]) {
+          if (Y.mg.levels > 1) S.X(0)[n] = 0.0;
+          continue;
+        }
+        x[n] += alpha * pout[n];
+        const double rn = r[n] - alpha * q[n];
+        r[n] = rn;
+        a2 += rn * rn;
+        if (Y.mg.levels > 1) S.first(0, n, rn);
       }
-      x[n] += alpha * pout[n];
-      const double rn = r[n] - alpha * q[n];
-      r[n] = rn;
-      a2 += rn * rn;
-      if (mg.levels > 1) S.first(0, n, rn);
     }
     const double b2 = block_sum<kRedBlock>(a2);
-    if (threadIdx.x == 0) part_rr[blockIdx.x] = b2;
+    if (threadIdx.x == 0 && work) part_rr[vb] = b2;
     grid.sync();
     trace(101);
-    rr = sum_partials(part_rr, nblk);
-    ++it;
-    done = rr <= tol2;
-    if (done) break;
-    S.vcycle(grid, part_rz);
-    const double rz_new = sum_partials(part_rz, nblk);
-    beta = rz_new / rz;
-    rz = rz_new;
-    const double *t = pout;
-    pout = const_cast<double *>(pin);
-    pin = t;
+    // every solve's |r|^2, each in its own order
+    bool more = false;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (!act[k]) continue;
+      const double rk = sum_partials(G.s[k].part + 2 * nblk, nblk);
+      if (k == me) rr = rk;
+      ++it[k];
+      done[k] = rk <= G.s[k].sc[9];
+      more = more || !done[k];
+    }
+    if (!more) break;
+    const bool cycle = work && !done[me];
+    S.vcycle(grid, part_rz, vb, cycle);
+    if (cycle) {
+      const double rz_new = sum_partials(part_rz, nblk);
+      beta = rz_new / rz;
+      rz = rz_new;
+      const double *t = pout;
+      pout = const_cast<double *>(pin);
+      pin = t;
+    }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    sc[0] = rz;
-    sc[3] = rr;
-    sc[8] = it;
+  if (vb == 0 && threadIdx.x == 0) {
+    Y.sc[0] = rz;
+    Y.sc[3] = rr;
+    Y.sc[8] = it[me];
   }
+}
+
+// At most 64 registers a thread: two blocks of a solve and one 256-thread
+// block of the flight kernels fit in an SM's registers together (a solve
+// can run beside a flight), and four blocks of the pair kernel fit alone.
+__global__ void __launch_bounds__(kRedBlock, 4) cg_mg_persistent(const __grid_constant__ MgGroup<1> G) {
+  cg_mg_body<1>(G);
+}
+__global__ void __launch_bounds__(kRedBlock, 4) cg_mg_pair(const __grid_constant__ MgGroup<2> G) {
+  cg_mg_body<2>(G);
 }
 
 template <typename T>
@@ -444,41 +505,66 @@ extern "C" int mcb200_mg_trace_read(unsigned long long *out, int max_entries) {
 #endif
 
 // An SM's shared-memory carveout is fixed while blocks run on it; with the
-// driver's choice for this kernel (its blocks need 2 KB) a flight block
-// (about 56 KB for a batch of 64) could not join an SM running the solve.
+// driver's choice for these kernels (their blocks need 2 KB) a flight block
+// (about 56 KB for a batch of 64) could not join an SM running a solve.
 // Preferring half the maximum lets both share an SM.  Once per device.
-static void configure_solve_kernel(int dev) {
+static void configure_solve_kernels(int dev) {
   static unsigned long long done = 0;
   if (dev < 0 || dev >= 64 || ((done >> dev) & 1ull)) return;
-  if (cudaFuncSetAttribute(cg_mg_persistent, cudaFuncAttributePreferredSharedMemoryCarveout, 50) == cudaSuccess)
+  if (cudaFuncSetAttribute(cg_mg_persistent, cudaFuncAttributePreferredSharedMemoryCarveout, 50) == cudaSuccess &&
+      cudaFuncSetAttribute(cg_mg_pair, cudaFuncAttributePreferredSharedMemoryCarveout, 50) == cudaSuccess)
     done |= 1ull << dev;
   else
-    cudaGetLastError();  // a hint only: the solve runs without it
+    cudaGetLastError();  // a hint only: the solves run without it
 }
 
-int cg_mg_max_grid() {
+static int co_resident(const void *kernel) {
   int dev = 0, sms = 0, per_sm = 0, coop = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return 0;
-  configure_solve_kernel(dev);
+  configure_solve_kernels(dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-  if (!coop || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_mg_persistent, kRedBlock, 0) != cudaSuccess)
+  if (!coop || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kRedBlock, 0) != cudaSuccess) {
+    cudaGetLastError();
     return 0;
+  }
   return per_sm * sms;
 }
 
+int cg_mg_max_grid() { return co_resident((const void *)cg_mg_persistent); }
+
+bool cg_mg_pair_fits(int grid) { return grid > 0 && 2 * grid <= co_resident((const void *)cg_mg_pair); }
+
 cudaError_t launch_cg_mg(int nodes, const Grid3 &g, const double *st7, const uint8_t *dirichlet, double *x, double *r,
                          double *z, double *p0, double *p1, double *q, double *part, double *sc, int max_iter,
-                         const MgDevice &mg_in, int grid, cudaStream_t s) {
-  MgDevice mg = mg_in;
-  mg.L[0].b = r;
-  mg.L[0].xa = z;
-  int nodes_arg = nodes, max_arg = max_iter;
-  Grid3 g_arg = g;
-  void *args[] = {&nodes_arg, &g_arg, &st7, &dirichlet, &x, &r, &p0, &p1, &q, &part, &sc, &max_arg, &mg};
+                         const MgDevice &mg, int grid, cudaStream_t s) {
+  if (nodes != g.px * g.py * g.pz) return cudaErrorInvalidValue;
+  MgGroup<1> G;
+  MgSystem &y = G.s[0];
+  y.mg = mg;
+  y.mg.L[0].b = r;
+  y.mg.L[0].xa = z;
+  y.st7 = st7;
+  y.dirichlet = dirichlet;
+  y.x = x; y.r = r; y.p0 = p0; y.p1 = p1; y.q = q; y.part = part; y.sc = sc;
+  y.px = g.px; y.py = g.py; y.pz = g.pz;
+  y.max_iter = max_iter;
+  G.grid = grid;
   int dev = 0;
-  if (cudaGetDevice(&dev) == cudaSuccess) configure_solve_kernel(dev);
+  if (cudaGetDevice(&dev) == cudaSuccess) configure_solve_kernels(dev);
+  void *args[] = {&G};
   return cudaLaunchCooperativeKernel((const void *)cg_mg_persistent, grid, kRedBlock, args, 0, s);
+}
+
+cudaError_t launch_cg_mg_pair(const MgSystem a[2], int grid, cudaStream_t s) {
+  if (a[0].mg.levels != a[1].mg.levels || a[0].mg.nu != a[1].mg.nu || !cg_mg_pair_fits(grid))
+    return cudaErrorInvalidValue;
+  MgGroup<2> G;
+  G.s[0] = a[0];
+  G.s[1] = a[1];
+  G.grid = grid;
+  void *args[] = {&G};
+  return cudaLaunchCooperativeKernel((const void *)cg_mg_pair, 2 * grid, kRedBlock, args, 0, s);
 }
 
 }  // namespace mcb200

@@ -49,4 +49,22 @@ cudaError_t launch_cg_mg(int nodes, const Grid3 &g, const double *st7, const uin
 // Largest cooperative grid of the MG kernel on the current device (blocks per SM x SMs); 0 if unavailable.
 int cg_mg_max_grid();
 
+// One solve's arguments, as launch_cg_mg takes them (mg with level 0's b and
+// xa bound to r and z).
+struct MgSystem {
+  MgDevice mg;
+  const double *st7 = nullptr;
+  const uint8_t *dirichlet = nullptr;
+  double *x = nullptr, *r = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr, *part = nullptr, *sc = nullptr;
+  int px = 0, py = 0, pz = 0, max_iter = 0;
+};
+// Two solves in one cooperative launch of 2 x `grid` blocks: blocks [0, grid)
+// solve a[0], the others a[1], each exactly as launch_cg_mg on `grid` blocks
+// (the same node-to-thread mapping and reduction order, so bit-identical
+// results), sharing one grid barrier per pass.  Both hierarchies must have
+// the same depth and smoothing (the pass sequence); cg_mg_pair_fits says
+// whether 2 x grid blocks are co-resident.
+cudaError_t launch_cg_mg_pair(const MgSystem a[2], int grid, cudaStream_t s);
+bool cg_mg_pair_fits(int grid);
+
 }  // namespace mcb200

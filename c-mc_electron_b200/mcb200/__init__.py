@@ -85,7 +85,7 @@ class BatchMember(ctypes.Structure):
 
 class BatchTuning(ctypes.Structure):
     _fields_ = [("flight_blocks_per_sm", ctypes.c_int), ("grid_per_sm", ctypes.c_int), ("overlap", ctypes.c_int),
-                ("ms_per_step", ctypes.c_double), ("candidates", ctypes.c_int)]
+                ("ms_per_step", ctypes.c_double), ("candidates", ctypes.c_int), ("pair_solves", ctypes.c_int)]
 
 
 class ServerOptions(ctypes.Structure):
@@ -159,6 +159,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mcb200_batch_sync.argtypes = [vp]
     lib.mcb200_batch_set_grid.argtypes = [vp, c.c_int]
     lib.mcb200_batch_set_overlap.argtypes = [vp, c.c_int]
+    lib.mcb200_batch_set_pairing.argtypes = [vp, c.c_int]
     lib.mcb200_batch_mark.argtypes = [vp, c.c_int]
     lib.mcb200_batch_elapsed_ms.argtypes = [vp, c.c_int, c.c_int, dp]
     lib.mcb200_batch_info.argtypes = [vp, c.POINTER(c.c_int), c.POINTER(c.c_uint64), c.POINTER(c.c_uint64),
@@ -560,7 +561,8 @@ class Batch:
         t = BatchTuning()
         self._check(self._lib.mcb200_batch_autotune(self._b, trial_steps, ctypes.byref(t)), "mcb200_batch_autotune")
         return {"flight_blocks_per_sm": t.flight_blocks_per_sm, "grid_per_sm": t.grid_per_sm,
-                "overlap": t.overlap, "ms_per_step": t.ms_per_step, "candidates": t.candidates}
+                "overlap": t.overlap, "pair_solves": t.pair_solves, "ms_per_step": t.ms_per_step,
+                "candidates": t.candidates}
 
     def use_graphs(self, enable: bool = True):
         self._check(self._lib.mcb200_batch_use_graphs(self._b, int(enable)), "mcb200_batch_use_graphs")
@@ -574,6 +576,10 @@ class Batch:
     def set_overlap(self, enable: bool = True):
         """Fly the members not solving Poisson beside the solves (default on)."""
         self._check(self._lib.mcb200_batch_set_overlap(self._b, int(bool(enable))), "mcb200_batch_set_overlap")
+
+    def set_pairing(self, enable: bool = True):
+        """Two due multigrid solves of the same shape per launch (default on)."""
+        self._check(self._lib.mcb200_batch_set_pairing(self._b, int(bool(enable))), "mcb200_batch_set_pairing")
 
     def mark(self, slot: int):
         self._check(self._lib.mcb200_batch_mark(self._b, slot), "mcb200_batch_mark")

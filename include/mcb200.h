@@ -309,14 +309,18 @@ int mcb200_batch_use_graphs(mcb200_batch *batch, int enable);
 /* Launch shapes picked by measurement: for every candidate (batched-flight
  * blocks per SM in {1, 2} x blocks per SM of the members' per-step kernels
  * -- sort, deposition, copies -- in {2, 4, 8}; then the fastest of those
- * with overlap switched) one untimed and `trial_steps` timed full timesteps
- * (mcb200_batch_run: they advance the simulations like any other steps);
- * the fastest by device time is kept and returned. */
+ * with overlap, pairing and both switched) one untimed and `trial_steps`
+ * timed full timesteps (mcb200_batch_run: they advance the simulations like
+ * any other steps).  The candidates of each of the two stages are timed in
+ * order and again in reverse order, so that a steady drift of the
+ * simulations (particle counts) cancels; the fastest mean device time is
+ * kept and returned. */
 typedef struct {
   int flight_blocks_per_sm, grid_per_sm;
   int overlap; /* mcb200_batch_set_overlap */
   double ms_per_step;  /* of the kept setting */
   int candidates;
+  int pair_solves; /* mcb200_batch_set_pairing */
 } mcb200_batch_tuning;
 int mcb200_batch_autotune(mcb200_batch *batch, int trial_steps, mcb200_batch_tuning *best);
 /* Wait for the batch and every member; reports a member's full store. */
@@ -330,6 +334,12 @@ int mcb200_batch_set_grid(mcb200_batch *batch, int blocks_per_sm);
  * and a helper launch then takes over what is left of the first launch's
  * particles.  The result is the same either way. */
 int mcb200_batch_set_overlap(mcb200_batch *batch, int enable);
+/* Pairing (default on): two due multigrid Poisson solves whose hierarchies
+ * have the same depth, smoothing and solve grid run in one cooperative
+ * launch of twice the grid (each on its own half, exactly as alone: the
+ * results are bit-identical), sharing the grid barriers that bound a solve.
+ * Each pair counts as one batched launch. */
+int mcb200_batch_set_pairing(mcb200_batch *batch, int enable);
 /* CUDA events after every member's enqueued work (mcb200_mark for a batch). */
 int mcb200_batch_mark(mcb200_batch *batch, int slot);
 int mcb200_batch_elapsed_ms(mcb200_batch *batch, int from, int to, double *ms);

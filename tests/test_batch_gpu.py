@@ -153,6 +153,53 @@ def test_batch_run_matches_members_alone(precision, graphs, overlap):
         eng.close()
 
 
+@pytest.mark.parametrize("precision", [mcb200.FLIGHT_FP64, mcb200.FLIGHT_FP32])
+def test_paired_solves_match_members_alone(precision):
+    """Two FinFETs on the same mesh (Vg 0.8 and 0.5) solving on the same
+    steps share one cooperative launch per solve (pairing); with a bulk box
+    flying beside the pair.  Potentials, solver statistics, particles and
+    tallies must equal those of twins stepped alone."""
+    def members(tmp, like=None):
+        bulk, dt0, _ = bulk_box_engine(4000, 3, 0, precision=precision, like=like, nx=10, ny=6, nz=6,
+                                       field_v_per_m=1e6)
+        out = [(bulk, dt0, 103, False)]
+        for name, vg, seed in (("a", 0.8, 200), ("b", 0.5, 300)):
+            eng, dt = finfet_engine(os.path.join(tmp, name), precision, bulk, vg=vg)
+            out.append((eng, dt, seed, True))
+        return out
+
+    with tempfile.TemporaryDirectory() as t1, tempfile.TemporaryDirectory() as t2:
+        alone = members(t1)
+        batched = members(t2, like=alone[0][0])
+    first = [0, 1, 1]  # the FinFETs solve together on t = 3, 7, 11
+    for step in range(STEPS):
+        for (eng, dt, seed, sc), f in zip(alone, first):
+            density(eng, f + step, sc)
+            eng.step(f + step, seed, dt)
+    batch = mcb200.Batch([(eng, dict(dt=dt, seed=seed, first_step=f, self_consistent=int(sc),
+                                      poisson_every=POISSON_EVERY))
+                          for (eng, dt, seed, sc), f in zip(batched, first)])
+    batch.use_graphs(True)
+    batch.set_pairing(True)
+    batch.run(STEPS)
+    batch.sync()
+    # 3 solving steps, each: one paired solve launch, the side flight and its helper
+    assert batch.info()["launches"] == STEPS * 6 + 3 * 3
+    for (ea, *_), (eb, *_) in zip(alone, batched):
+        a, b = by_uid(ea), by_uid(eb)
+        for k in a:
+            assert np.array_equal(a[k], b[k]), k
+        same_tallies(ea.tallies(), eb.tallies())
+    for k in (1, 2):
+        pa, pb = alone[k][0].array("potential"), batched[k][0].array("potential")
+        assert np.array_equal(pa.view(np.uint64), pb.view(np.uint64))
+        assert alone[k][0].poisson_stats() == batched[k][0].poisson_stats()
+    assert alone[1][0].poisson_stats() != alone[2][0].poisson_stats()  # two different systems
+    batch.close()
+    for eng, *_ in batched + alone:
+        eng.close()
+
+
 def test_batch_rejects_mixed_tables():
     a, dt, _ = bulk_box_engine(1000, 1, 0, nx=6, ny=5, nz=4)
     b, _, _ = bulk_box_engine(1000, 2, 0, nx=6, ny=5, nz=4)  # its own tables, not alike
