@@ -326,11 +326,14 @@ def batch_arm(args, device: int) -> dict:
     # steady drift weighs on both alike.
     tot = {"b": [0, 0.0], "a": [0, 0.0]}
     order = ["b", "a", "a", "b"]
+    windows = []
     with ClockSampler(device) as clocks:
         for arm in order:
             ps, ms = window(run_b if arm == "b" else run_a, BATCH_STEPS // 2)
             tot[arm][0] += ps
             tot[arm][1] += ms
+            windows.append({"arm": "batched" if arm == "b" else "alone", "ms_per_step": ms / (BATCH_STEPS // 2),
+                            "particles_per_step": ps / (BATCH_STEPS // 2)})
     batched, ms_b = tot["b"][0] / (tot["b"][1] * 1e-3), tot["b"][1] / BATCH_STEPS
     alone, ms_a = tot["a"][0] / (tot["a"][1] * 1e-3), tot["a"][1] / BATCH_STEPS
     info = batch.info()
@@ -338,7 +341,7 @@ def batch_arm(args, device: int) -> dict:
     out = {"metric": "particle-steps/s", "members": len(members), "bulk": kinds.count("bulk"),
            "finfet": kinds.count("finfet"), "particles": int(sum(m.desc["particles"] for m in members)),
            "value": batched, "ms_per_step": ms_b, "unbatched_value": alone, "unbatched_ms_per_step": ms_a,
-           "batched_over_unbatched": batched / alone, "steps": BATCH_STEPS, "autotune": tune,
+           "batched_over_unbatched": batched / alone, "steps": BATCH_STEPS, "windows": windows, "autotune": tune,
            "graph_captures": info["graph_captures"], "graph_replays": info["graph_replays"],
            "setup_s": setup_s, "clocks": clocks.summary(), "dtype": "f32", "data": "synthetic",
            "config": "64 members (seed 4): bulk n-Si boxes 20^3-80x40x50 cells, E_x U[1,100] kV/cm, and "

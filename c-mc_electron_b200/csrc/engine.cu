@@ -334,6 +334,46 @@ void free_mesh(mcb200_ctx *c) {
   c->mr = MrScratch{};
 }
 
+// The refresh targets stay on the device and are uploaded when they change,
+// on the upload stream: a copy from pageable host memory returns only when
+// its stream reaches it, and on the context's stream that means after every
+// step queued there (in a batch, the batched steps).  The upload follows the
+// last refresh that read the targets; the next refresh follows the upload.
+void upload_refresh_targets(mcb200_ctx *c, const int32_t *desired_e, const int32_t *desired_h) {
+  MrScratch &w = c->mr;
+  const int cells = c->ncells;
+  if (w.de_host.size() == (size_t)cells && std::memcmp(w.de_host.data(), desired_e, sizeof(int) * cells) == 0 &&
+      std::memcmp(w.dh_host.data(), desired_h, sizeof(int) * cells) == 0)
+    return;
+  w.de_host.assign(desired_e, desired_e + cells);
+  w.dh_host.assign(desired_h, desired_h + cells);
+  ck(cudaStreamWaitEvent(c->upload, c->ev_mr_used, 0), "wait");
+  ck(cudaMemcpyAsync(w.de, w.de_host.data(), sizeof(int) * cells, cudaMemcpyHostToDevice, c->upload), "copy");
+  ck(cudaMemcpyAsync(w.dh, w.dh_host.data(), sizeof(int) * cells, cudaMemcpyHostToDevice, c->upload), "copy");
+  ck(cudaEventRecord(c->ev_upload, c->upload), "event");
+  ck(cudaStreamWaitEvent(c->stream, c->ev_upload, 0), "wait");
+}
+
+// MultipleRefresh scratch for the mesh's cells, allocated with the cells
+// (an allocation at the first refresh would stall a running batch).
+void mr_scratch(mcb200_ctx *c) {
+  MrScratch &w = c->mr;
+  const int cells = c->ncells;
+  if (w.cells == cells) return;
+  w.de = dalloc<int>(cells, c->mesh_owned);
+  w.dh = dalloc<int>(cells, c->mesh_owned);
+  w.out_count = dalloc<unsigned int>(cells, c->mesh_owned);
+  w.new_count = dalloc<unsigned int>(cells, c->mesh_owned);
+  w.out_off = dalloc<unsigned int>(cells, c->mesh_owned);
+  w.uid_off = dalloc<unsigned int>(cells, c->mesh_owned);
+  w.tiles = dalloc<unsigned int>((cells + 1023) / 1024 + 1, c->mesh_owned);
+  w.tot = dalloc<unsigned int>(2, c->mesh_owned);
+  w.gen = dalloc<unsigned long long>(1, c->mesh_owned);
+  w.cells = cells;
+  w.de_host.clear();
+  w.dh_host.clear();
+}
+
 // Host particles (absolute FP64 positions) into store 0 of precision R;
 // an FP32 store keeps positions relative to the cell's low corner.
 template <typename R>
@@ -397,6 +437,9 @@ void download_store(mcb200_ctx *c, size_t n, mcb200_particles *p, std::vector<ui
 // on its device (the tables are already there).
 void init_device_context(mcb200_ctx *c, size_t max_particles) {
   ck(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  ck(cudaStreamCreateWithFlags(&c->upload, cudaStreamNonBlocking), "cudaStreamCreate");
+  ck(cudaEventCreateWithFlags(&c->ev_upload, cudaEventDisableTiming), "cudaEventCreate");
+  ck(cudaEventCreateWithFlags(&c->ev_mr_used, cudaEventDisableTiming), "cudaEventCreate");
   ck(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device), "device attribute");
   c->capacity = max_particles;
   c->child_cap = (int)std::min<size_t>(std::max<size_t>(max_particles / 8, 4096), 1u << 22);
@@ -655,6 +698,7 @@ int mcb200_set_cells(mcb200_ctx *c, const int32_t *motion_rule, const int32_t *a
     m.surface_scatter = (flags & MCB200_FLAG_SURFACE_SCATTER) ? 1 : 0;
     m.surface_impurity = (flags & MCB200_FLAG_SURFACE_IMPURITY) ? 1 : 0;
     m.heat = (flags & MCB200_FLAG_HEAT) ? 1 : 0;
+    mr_scratch(c);
     c->cells_set = true;
     return MCB200_OK;
   } catch (const std::exception &e) {
@@ -1276,35 +1320,13 @@ int mcb200_multiple_refresh(mcb200_ctx *c, const int32_t *desired_e, const int32
     size_t want = 0;
     for (int q = 0; q < cells; ++q) want += (size_t)std::max(desired_e[q], 0) + (size_t)std::max(desired_h[q], 0);
     if (want > c->capacity) return fail(c, MCB200_ERR_CAPACITY, "refresh targets exceed the particle capacity");
-    // scratch allocated with the mesh on first use (no device-wide cudaFree per refresh)
+    mr_scratch(c);  // allocated with the cells (mcb200_set_cells)
     MrScratch &w = c->mr;
-    if (w.cells != cells) {
-      w.de = dalloc<int>(cells, c->mesh_owned);
-      w.dh = dalloc<int>(cells, c->mesh_owned);
-      w.out_count = dalloc<unsigned int>(cells, c->mesh_owned);
-      w.new_count = dalloc<unsigned int>(cells, c->mesh_owned);
-      w.out_off = dalloc<unsigned int>(cells, c->mesh_owned);
-      w.uid_off = dalloc<unsigned int>(cells, c->mesh_owned);
-      w.tiles = dalloc<unsigned int>((cells + 1023) / 1024 + 1, c->mesh_owned);
-      w.tot = dalloc<unsigned int>(2, c->mesh_owned);
-      w.gen = dalloc<unsigned long long>(1, c->mesh_owned);
-      w.cells = cells;
-      w.de_host.clear();
-      w.dh_host.clear();
-    }
     int *de = w.de, *dh = w.dh;
     unsigned int *out_count = w.out_count, *new_count = w.new_count, *out_off = w.out_off, *uid_off = w.uid_off;
     unsigned int *tiles = w.tiles, *tot = w.tot;
     unsigned long long *gen = w.gen;
-    // the targets stay on the device: a copy from pageable host memory would
-    // wait for the stream (and, in a batch, for every member's step)
-    if (w.de_host.size() != (size_t)cells || std::memcmp(w.de_host.data(), desired_e, sizeof(int) * cells) != 0 ||
-        std::memcmp(w.dh_host.data(), desired_h, sizeof(int) * cells) != 0) {
-      w.de_host.assign(desired_e, desired_e + cells);
-      w.dh_host.assign(desired_h, desired_h + cells);
-      ck(cudaMemcpyAsync(de, w.de_host.data(), sizeof(int) * cells, cudaMemcpyHostToDevice, s), "copy");
-      ck(cudaMemcpyAsync(dh, w.dh_host.data(), sizeof(int) * cells, cudaMemcpyHostToDevice, s), "copy");
-    }
+    upload_refresh_targets(c, desired_e, desired_h);
     ck(cudaMemsetAsync(gen, 0, sizeof(unsigned long long), s), "memset");
     // group the store by cell into the other buffer (hist = counts, offsets =
     // cell ends); the refreshed population then goes back to this buffer
@@ -1324,6 +1346,7 @@ int mcb200_multiple_refresh(mcb200_ctx *c, const int32_t *desired_e, const int32
     };
     if (c->precision == MCB200_FLIGHT_FP32) refresh(float{});
     else refresh(double{});
+    ck(cudaEventRecord(c->ev_mr_used, s), "event");  // the targets are read
     // the refreshed population's size and the uid counter, on the device
     refresh_counts_kernel<<<1, 32, 0, s>>>(c->dev_counts, tot);
     c->launches += 14;  // cell sort, count, two scans, emit, counts
@@ -1338,6 +1361,24 @@ int mcb200_multiple_refresh(mcb200_ctx *c, const int32_t *desired_e, const int32
     return MCB200_OK;
   } catch (const CapacityError &e) {
     return fail(c, MCB200_ERR_CAPACITY, e.what());
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_set_refresh_targets(mcb200_ctx *c, const int32_t *desired_e, const int32_t *desired_h) {
+  if (!c || !desired_e || !desired_h) return MCB200_ERR_ARG;
+  if (!c->cells_set) return fail(c, MCB200_ERR_STATE, "mcb200_set_refresh_targets before mcb200_set_cells");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    size_t want = 0;
+    for (int q = 0; q < c->ncells; ++q)
+      want += (size_t)std::max(desired_e[q], 0) + (size_t)std::max(desired_h[q], 0);
+    if (want > c->capacity) return fail(c, MCB200_ERR_CAPACITY, "refresh targets exceed the particle capacity");
+    mr_scratch(c);
+    upload_refresh_targets(c, desired_e, desired_h);
+    ck(cudaStreamSynchronize(c->upload), "sync");
+    return MCB200_OK;
   } catch (const std::exception &e) {
     return fail(c, MCB200_ERR_CUDA, e.what());
   }

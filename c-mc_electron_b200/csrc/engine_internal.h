@@ -119,6 +119,10 @@ struct mcb200_ctx {
   std::string error;
   int device = 0;
   cudaStream_t stream = nullptr;
+  // uploads that must not wait for the work queued on `stream` (refresh
+  // targets from pageable memory); ev_mr_used: the last refresh's reads
+  cudaStream_t upload = nullptr;
+  cudaEvent_t ev_upload = nullptr, ev_mr_used = nullptr;
   std::vector<void *> owned;   // every cudaMalloc of the context
   std::vector<void *> mesh_owned;
   std::shared_ptr<TableSet> ts;  // band tables (host and device), shared by contexts made alike
@@ -204,6 +208,9 @@ struct mcb200_ctx {
     if (flush_buf) cudaFree(flush_buf);
     if (h_pinned) cudaFreeHost(h_pinned);
     if (h_scratch) cudaFreeHost(h_scratch);
+    if (ev_upload) cudaEventDestroy(ev_upload);
+    if (ev_mr_used) cudaEventDestroy(ev_mr_used);
+    if (upload) cudaStreamDestroy(upload);
     if (stream) cudaStreamDestroy(stream);
   }
 };

@@ -231,6 +231,9 @@ int admit(mcb200_server *v, Slot &s) {
   if (int rc = mcb200_deck_surface_params(s.input.c_str(), s.ctx, &s.info, &s.surf, &pe))
     return ctx_err(rc, "surface parameters");
   s.poisson_every = s.req.poisson_every > 0 ? s.req.poisson_every : pe;
+  // the refresh targets go to the device now, not at the first refresh inside a running batch
+  if (int rc = mcb200_set_refresh_targets(s.ctx, s.refresh_e.data(), s.refresh_h.data()))
+    return ctx_err(rc, "mcb200_set_refresh_targets");
   if (from) {
     if (int rc = mcb200_copy_ensemble(s.ctx, from->ctx)) return ctx_err(rc, "mcb200_copy_ensemble");
     // to this deck's carrier targets, as a refresh would

@@ -196,6 +196,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mcb200_get_array.argtypes = [vp, c.c_char_p, dp, c.c_size_t]
     lib.mcb200_surface_rates.argtypes = [vp, c.POINTER(SurfaceParams), i32p]
     lib.mcb200_multiple_refresh.argtypes = [vp, i32p, i32p, c.c_uint32, c.c_uint64, c.POINTER(c.c_int64)]
+    lib.mcb200_set_refresh_targets.argtypes = [vp, i32p, i32p]
     lib.mcb200_set_cells.argtypes = [vp, i32p, i32p, i32p, i32p, i32p, c.c_int, dp, c.c_int]
     lib.mcb200_set_fields.argtypes = [vp, dp, dp, dp]
     lib.mcb200_set_surface_rates.argtypes = [vp, dp, dp, dp, dp]
@@ -370,6 +371,12 @@ class Engine:
                                                       step, seed, ctypes.byref(gen) if wait else None),
                     "multiple_refresh")
         return gen.value if wait else None
+
+    def set_refresh_targets(self, desired_e, desired_h):
+        """Upload the MultipleRefresh targets now, not at the first refresh."""
+        de, dh = (np.ascontiguousarray(a, dtype=np.int32) for a in (desired_e, desired_h))
+        self._check(self._lib.mcb200_set_refresh_targets(self._ctx, _ptr(de, ctypes.c_int32), _ptr(dh, ctypes.c_int32)),
+                    "set_refresh_targets")
 
     def deposit(self):
         self._check(self._lib.mcb200_deposit(self._ctx), "deposit")

@@ -79,6 +79,7 @@ def finfet_member(like, tmp, lg_nm, vg, particles, seed, precision, first_step, 
                           phonon=info["flag_surface_phonon"]))
     eng.surface_rates(surface[0], **surface[1])
     refresh = (deck.int_array("refresh_electrons"), deck.int_array("refresh_holes"))
+    eng.set_refresh_targets(*refresh)  # not at the first refresh, inside a running batch
     cfg = dict(dt=info["dt"], seed=seed, first_step=first_step, self_consistent=1, poisson_every=POISSON_EVERY,
                surface_rates=1)
     deck.close()

@@ -199,6 +199,13 @@ int mcb200_surface_rates(mcb200_ctx *ctx, const mcb200_surface_params *params, c
  * device, nothing waits for the GPU). */
 int mcb200_multiple_refresh(mcb200_ctx *ctx, const int32_t *desired_e, const int32_t *desired_h, uint32_t step,
                             uint64_t seed, int64_t *generated);
+/* The refresh targets (c_desired_electron_number / c_desired_hole_number,
+ * one per cell) uploaded ahead of the first mcb200_multiple_refresh, which
+ * otherwise copies them (as it does whenever they change) from the caller's
+ * pageable memory: about a millisecond of host time per refresh-sized mesh,
+ * taken inside a running simulation.  Waits for the copy; no reference
+ * counterpart (the reference keeps the targets in MeshQuantities). */
+int mcb200_set_refresh_targets(mcb200_ctx *ctx, const int32_t *desired_e, const int32_t *desired_h);
 
 /* Copy a device array to the host: "rho", "e_rough", "e_phonon", "h_rough",
  * "h_phonon", "efield", "hfield" (3 per cell),

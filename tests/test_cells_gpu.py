@@ -45,7 +45,10 @@ def test_surface_rates():
     eng.close()
 
 
-def test_multiple_refresh():
+@pytest.mark.parametrize("preload", [False, True])
+def test_multiple_refresh(preload):
+    """MultipleRefresh against the oracle; preload: the targets uploaded
+    beforehand (mcb200_set_refresh_targets) instead of by the refresh."""
     with tempfile.TemporaryDirectory() as tmp:
         deck = decks.bulk_box(tmp, nx=6, ny=5, nz=4, electrons=2000, holes=400)
         orc = Oracle()
@@ -67,6 +70,8 @@ def test_multiple_refresh():
     after = orc.particles()
     eng = engine_from_oracle(orc, max_particles=1 << 14)
     eng.upload(p)
+    if preload:
+        eng.set_refresh_targets(de, dh)
     gen = eng.multiple_refresh(de, dh, step, seed=9)
     got = eng.download()
     assert gen == gen_ref
