@@ -44,12 +44,6 @@ import time
 
 import numpy as np
 
-# The batch arm drives 66 streams (one per member, the batch stream and its
-# side stream); with the default 8 hardware work queues a member stream that
-# waits for a Poisson solve holds back unrelated work queued behind it.  Read
-# when the CUDA context is created, so it is set before anything touches CUDA.
-os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
-
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "c-mc_electron_b200"))
 

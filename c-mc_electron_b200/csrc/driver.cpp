@@ -357,6 +357,18 @@ struct Run {
     heat = false;
     std::vector<double> readback(16 * 6);
     double flushed_ms = 0;  // device time of the timed steps when each follows an L2 eviction
+    // Each flushed step is bracketed by a pair of marks (slots 2-7: three
+    // pairs in turn); a pair is read only when it is about to be reused, so
+    // the host stays up to two steps ahead of the device and no step waits
+    // for its own launches to be enqueued.
+    bool pair_used[3] = {false, false, false};
+    auto settle = [&](int pair) {
+      if (!pair_used[pair]) return;
+      double ms = 0;
+      ok(mcb200_elapsed_ms(ctx, 2 + 2 * pair, 3 + 2 * pair, &ms), ctx, "mcb200_elapsed_ms");
+      flushed_ms += ms;
+      pair_used[pair] = false;
+    };
     for (int step = 0; step < steps; ++step) {
       if (step == warm) {  // the timed region starts: device event + engine timing reset
         ok(mcb200_sync(ctx), ctx, "mcb200_sync");
@@ -366,17 +378,17 @@ struct Run {
         ok(mcb200_particle_steps(ctx, &ps0), ctx, "mcb200_particle_steps");
       }
       const bool flush = opt.flush_l2_bytes > 0 && step >= warm;
+      const int pair = step % 3;
       if (flush) {
+        settle(pair);
         ok(mcb200_flush_l2(ctx, opt.flush_l2_bytes), ctx, "mcb200_flush_l2");
-        ok(mcb200_mark(ctx, 2), ctx, "mcb200_mark");
+        ok(mcb200_mark(ctx, 2 + 2 * pair), ctx, "mcb200_mark");
       }
       density(step);
       refresh(step);
       if (flush) {
-        double ms = 0;
-        ok(mcb200_mark(ctx, 3), ctx, "mcb200_mark");
-        ok(mcb200_elapsed_ms(ctx, 2, 3, &ms), ctx, "mcb200_elapsed_ms");
-        flushed_ms += ms;
+        ok(mcb200_mark(ctx, 3 + 2 * pair), ctx, "mcb200_mark");
+        pair_used[pair] = true;
       }
       if (opt.readback_every_step)
         ok(mcb200_get_tallies(ctx, nullptr, readback.data(), nullptr, nullptr, nullptr, nullptr), ctx, "tallies");
@@ -384,6 +396,7 @@ struct Run {
       if (opt.verbose && step % std::max(1, info.stat_step / 10) == 0)
         std::printf("step %d: %zu particles\n", step, mcb200_num_particles(ctx));
     }
+    for (int pair = 0; pair < 3; ++pair) settle(pair);
     if (steps > warm) {
       ok(mcb200_mark(ctx, 1), ctx, "mcb200_mark");
       ok(mcb200_elapsed_ms(ctx, 0, 1, &rep->timed_device_ms), ctx, "mcb200_elapsed_ms");

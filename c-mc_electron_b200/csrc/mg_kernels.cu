@@ -418,9 +418,20 @@ __device__ __forceinline__ void cg_mg_body(const MgGroup<K> &G) {
   }
 }
 
+// Preferred shared-memory carveout of the solve kernels, in per cent (-1:
+// the driver's choice).  An SM's carveout is fixed while blocks run on it;
+// with the driver's choice (the solve's blocks need 2 KB) a batched flight
+// block (about 56 KB for a batch of 64) cannot join an SM running a solve,
+// and 50 lets it.  Off by default: measured on the FinFET, 50 made the solve
+// 9 % slower (less L1) for a batch overlap gain within the noise.
+#ifndef MCB200_SOLVE_CARVEOUT
+#define MCB200_SOLVE_CARVEOUT -1
+#endif
 // At most 64 registers a thread: two blocks of a solve and one 256-thread
 // block of the flight kernels fit in an SM's registers together (a solve
 // can run beside a flight), and four blocks of the pair kernel fit alone.
+// (Measured on the FinFET: the cap costs the solo solve about 2 %; without
+// it the compiler's choice was slower still.)
 __global__ void __launch_bounds__(kRedBlock, 4) cg_mg_persistent(const __grid_constant__ MgGroup<1> G) {
   cg_mg_body<1>(G);
 }
@@ -504,15 +515,15 @@ extern "C" int mcb200_mg_trace_read(unsigned long long *out, int max_entries) {
 }
 #endif
 
-// An SM's shared-memory carveout is fixed while blocks run on it; with the
-// driver's choice for these kernels (their blocks need 2 KB) a flight block
-// (about 56 KB for a batch of 64) could not join an SM running a solve.
-// Preferring half the maximum lets both share an SM.  Once per device.
+// The carveout preference (MCB200_SOLVE_CARVEOUT), once per device.
 static void configure_solve_kernels(int dev) {
   static unsigned long long done = 0;
   if (dev < 0 || dev >= 64 || ((done >> dev) & 1ull)) return;
-  if (cudaFuncSetAttribute(cg_mg_persistent, cudaFuncAttributePreferredSharedMemoryCarveout, 50) == cudaSuccess &&
-      cudaFuncSetAttribute(cg_mg_pair, cudaFuncAttributePreferredSharedMemoryCarveout, 50) == cudaSuccess)
+  if (MCB200_SOLVE_CARVEOUT < 0 ||
+      (cudaFuncSetAttribute(cg_mg_persistent, cudaFuncAttributePreferredSharedMemoryCarveout, MCB200_SOLVE_CARVEOUT) ==
+           cudaSuccess &&
+       cudaFuncSetAttribute(cg_mg_pair, cudaFuncAttributePreferredSharedMemoryCarveout, MCB200_SOLVE_CARVEOUT) ==
+           cudaSuccess))
     done |= 1ull << dev;
   else
     cudaGetLastError();  // a hint only: the solves run without it
