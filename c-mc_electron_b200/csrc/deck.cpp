@@ -179,8 +179,12 @@ class DeviceScript {
           node_index(e, d_.lx_m); node_index(f, d_.lx_m);
           break;
         }
-        case 15:
-          for (int i = 0; i < 7; ++i) number<double>();  // quantum-correction parameters (off)
+        case 15:  // ep_parm: quantum-correction window (src/mcmodel.cpp:4549-4556)
+          for (int a = 0; a < 3; ++a) {
+            d_.qc_ratio[a] = number<double>();
+            d_.qc_theta_nm[a] = number<double>();
+          }
+          d_.qc_eb_v = number<double>();
           break;
         case 16:
           d_.num_surfaces = number<int>();
@@ -312,6 +316,7 @@ Deck Deck::load(const std::string &input_path) {
   d.flag_nonlinear_poisson = kv.get("NonLinearPoisson", false);
   d.flag_multiple_refresh = kv.get("Flag_MultipleRefresh", false);
   d.flag_quantum_correction = kv.get("Flag_QuantumCorrection", false);
+  d.quantum_start_step = kv.get("quantum_start_step", 20);
   d.flag_surface_scatter = kv.get("Flag_SurfaceScatter", true);
   d.flag_surface_roughness = kv.get("Flag_SurfaceRoughnessScatter", true);
   d.flag_surface_phonon = kv.get("Flag_SurfacePhononScatter", true);
@@ -392,6 +397,8 @@ DeckScaled DeckScaled::build(const Deck &d, const Units &u, double ni) {
     s.phims.push_back(c.phims_v / u.pot0);
   }
   for (int i = 0; i < d.num_surfaces; ++i) s.surface_pos[i] = d.surface_pos_nm[i] * 1e-9 / spr0;
+  for (int a = 0; a < 3; ++a) s.qc_theta[a] = d.qc_theta_nm[a] / (1e9 * spr0);
+  s.qc_eb = d.qc_eb_v / u.pot0;
   const int cells = d.cells();
   s.donor.resize(cells);
   s.acceptor.resize(cells);

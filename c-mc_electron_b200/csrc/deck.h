@@ -39,6 +39,9 @@ struct Deck {
   bool flag_surface_scatter = true, flag_surface_roughness = true, flag_surface_phonon = true;
   bool flag_surface_impurity = false, flag_restart = false, flag_nonlinear_poisson = false;
   bool flag_quantum_correction = false;
+  int quantum_start_step = 20;
+  // ep_parm (keyword 15): window ratio and theta (nm) per axis, barrier Eb (V)
+  double qc_ratio[3] = {0, 0, 0}, qc_theta_nm[3] = {0, 0, 0}, qc_eb_v = 0;
   // ---- lgrid.txt: node coordinates in metres (micrometres x 1e-6 as read)
   std::vector<double> lx_m, ly_m, lz_m;
   int nx = 0, ny = 0, nz = 0;
@@ -71,6 +74,7 @@ struct DeckScaled {
   std::vector<int> desired_e, desired_h;    // raised by compute_par_num
   std::vector<double> vapp, phims;          // per contact, / pot0
   double dt = 0;                            // / time0
+  double qc_theta[3] = {0, 0, 0}, qc_eb = 0;  // ep_parm: theta / (1e9 spr0), Eb / pot0 (:4549-4556)
 
   static DeckScaled build(const Deck &d, const Units &u, double ni);
 };

@@ -90,6 +90,8 @@ int mcb200_deck_get_info(const mcb200_deck *k, mcb200_deck_info *info) {
   info->flag_surface_phonon = d.flag_surface_phonon;
   info->flag_surface_impurity = d.flag_surface_impurity;
   info->flag_restart = d.flag_restart;
+  info->flag_quantum_correction = d.flag_quantum_correction;
+  info->quantum_start_step = d.quantum_start_step;
   info->n_contacts = (int)d.contacts.size();
   int planes = 0;
   for (const auto &c : d.contacts) planes += c.nplanes;
@@ -201,10 +203,21 @@ int mcb200_apply_deck(mcb200_ctx *ctx, mcb200_deck *k) {
                            s.dz.data());
   if (rc) return deck_fail(k, rc, std::string("mcb200_set_mesh: ") + mcb200_last_error(ctx));
   const int flags = (d.flag_surface_scatter ? MCB200_FLAG_SURFACE_SCATTER : 0) |
-                    (d.flag_surface_impurity ? MCB200_FLAG_SURFACE_IMPURITY : 0);
+                    (d.flag_surface_impurity ? MCB200_FLAG_SURFACE_IMPURITY : 0) |
+                    (d.flag_quantum_correction ? MCB200_FLAG_QUANTUM : 0);
   rc = mcb200_set_cells(ctx, d.motion.data(), d.attached_contact.data(), d.in_surf.data(), s.nearest_surf.data(),
                         d.surface_dir, d.num_surfaces, s.da.data(), flags);
   if (rc) return deck_fail(k, rc, std::string("mcb200_set_cells: ") + mcb200_last_error(ctx));
+  if (d.flag_quantum_correction) {  // set up now, on from quantum_start_step (mcb200_run_deck)
+    mcb200_quantum_params q{};
+    for (int a = 0; a < 3; ++a) {
+      q.ratio[a] = d.qc_ratio[a];
+      q.theta[a] = s.qc_theta[a];
+    }
+    q.eb = s.qc_eb;
+    rc = mcb200_set_quantum_correction(ctx, &q, d.material.data(), d.quantum_region.data(), 0);
+    if (rc) return deck_fail(k, rc, std::string("mcb200_set_quantum_correction: ") + mcb200_last_error(ctx));
+  }
   const std::vector<int32_t> planes = contact_planes(d);
   rc = mcb200_set_device(ctx, d.material.data(), s.donor.data(), s.acceptor.data(), (int)d.contacts.size(),
                          s.vapp.data(), s.phims.data(), (int)(planes.size() / 7), planes.data());

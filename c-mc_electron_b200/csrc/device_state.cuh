@@ -107,6 +107,9 @@ struct DevTables {
   const double *bz;           // [3][5][48]  (xbz, ybz, zbz)
   const int *indmat;          // [729]
   const int *reflect_isym;    // [3][48]: isym after mirroring k_x / k_y / k_z
+  // phonon dispersion tables (FullBandTables::dispersion; null when absent)
+  const double *disp;
+  int disp_off[6];
   DevTables32 f32;            // FP32 flight tables (null until a context selects FP32 flight)
 };
 
@@ -134,6 +137,7 @@ struct DevMesh {
   int surface_scatter;          // Flag_SurfaceScatter
   int surface_impurity;         // Flag_SurfaceImpurityScatter
   int heat;                     // flag_heat: phonon events deposit heat
+  int quantum;                  // Flag_QuantumCorrection: LO / TO / LA final energies from the dispersion tables
 };
 
 // Particle store: structure of arrays, one entry per particle.  R = double:

@@ -89,11 +89,12 @@ struct Run {
   double u[14];
   int nx = 0, ny = 0, nz = 0, cells = 0, nodes = 0;
   std::vector<int32_t> refresh_e, refresh_h, eeff;
-  std::vector<double> node_volume, saved_e_charge, saved_h_charge, pot_avg;
+  std::vector<double> node_volume, saved_e_charge, saved_h_charge, pot_avg, qc_avg;
   mcb200_surface_params surf{};
   int poisson_every = 1;
   uint64_t seed = 1;
   bool heat = false;
+  bool qc_on = false;  // the quantum correction has been switched on
 
   double T0() const { return u[0]; }
   double spr0() const { return u[2]; }
@@ -126,6 +127,11 @@ struct Run {
     lap(0);
     ok(mcb200_deposit(ctx), ctx, "mcb200_deposit");
     lap(1);
+    // compute_field applies the quantum correction from quantum_start_step on (src/mcmodel.cpp:2249)
+    if (!heat && info.flag_quantum_correction && !qc_on && step >= info.quantum_start_step) {
+      ok(mcb200_set_quantum_correction(ctx, nullptr, nullptr, nullptr, 1), ctx, "mcb200_set_quantum_correction");
+      qc_on = true;
+    }
     if (!heat && info.flag_compute_potential && step % poisson_every == 0)  // statistics stay on the device
       ok(mcb200_solve_poisson(ctx, opt.poisson_rel_tol > 0 ? opt.poisson_rel_tol : 1e-10, 20000, nullptr, nullptr),
          ctx, "mcb200_solve_poisson");
@@ -188,7 +194,8 @@ struct Run {
       ok(mcb200_stat_get(ctx, name, v.data(), n), ctx, name);
       return v;
     };
-    const std::vector<double> count = stat("cell_count", cells), pot = stat("pot_sum", nodes);
+    const std::vector<double> count = stat("cell_count", cells), pot = stat("pot_sum", nodes),
+                              qc_pot = stat("qc_pot_sum", nodes);
     auto cidx = [&](int i, int j, int k) { return ((size_t)j * nx + i) * nz + k; };
     auto nidx = [&](int i, int j, int k) { return ((size_t)j * (nx + 1) + i) * (nz + 1) + k; };
     {
@@ -198,6 +205,7 @@ struct Run {
           for (int k = 0; k < nz; ++k) f << i << ' ' << j << ' ' << k << ' ' << count[cidx(i, j, k)] / window << "\n";
     }
     pot_avg.assign(nodes, 0.0);
+    qc_avg.assign(nodes, 0.0);
     {
       std::ofstream f(file("pot", step), std::ios::app), q(file("qc_pot", step), std::ios::app);
       for (int i = 0; i <= nx; ++i)
@@ -205,8 +213,9 @@ struct Run {
           for (int j = 0; j <= ny; ++j) {
             const size_t p = nidx(i, j, k);
             pot_avg[p] = pot[p] / window;
+            qc_avg[p] = qc_pot[p] / window;
             f << i << ' ' << j << ' ' << k << ' ' << pot_avg[p] * pot0v << "\n";
-            q << i << ' ' << j << ' ' << k << ' ' << pot_avg[p] * pot0v << "\n";  // no quantum correction
+            q << i << ' ' << j << ' ' << k << ' ' << qc_avg[p] * pot0v << "\n";
           }
     }
     const char *names[2] = {"Electron", "Hole"};
@@ -417,7 +426,8 @@ struct Run {
     const int hsteps = !info.flag_compute_heat ? 0
                        : (opt.max_heat_steps >= 0 ? std::min(opt.max_heat_steps, info.heat_steps) : info.heat_steps);
     if (hsteps > 0) {
-      if (!pot_avg.empty()) ok(mcb200_set_potential(ctx, pot_avg.data()), ctx, "mcb200_set_potential");
+      if (!pot_avg.empty())  // heat_field, src/heat.cpp:100-105
+        ok(mcb200_set_potentials(ctx, pot_avg.data(), qc_avg.data()), ctx, "mcb200_set_potentials");
       heat = true;
       ok(mcb200_set_heat_tally(ctx, 1), ctx, "mcb200_set_heat_tally");
       const int window = info.stat_heat_step > 0 ? info.stat_heat_step : info.stat_step;

@@ -309,6 +309,8 @@ void upload_tables(mcb200_ctx *c) {
   d.bz = dupload(bz, c->ts->owned);
   d.indmat = dupload(indmat, c->ts->owned);
   d.reflect_isym = dupload(refl, c->ts->owned);
+  d.disp = t.dispersion.empty() ? nullptr : dupload(t.dispersion, c->ts->owned);
+  for (int i = 0; i < kDispTables; ++i) d.disp_off[i] = t.disp_off[i];
   build_kgrid(c, 40);
   upload_tables32(c, tf, ts, kn);
   c->ts->vmax = 0;
@@ -579,6 +581,7 @@ int mcb200_copy_table(const mcb200_ctx *c, const char *name, void *out, size_t b
   if (n == "tlist") { copy_vec(t.tlist, out, bytes, needed); return 0; }
   if (n == "nslist") { copy_vec(t.nslist, out, bytes, needed); return 0; }
   if (n == "pslist") { copy_vec(t.pslist, out, bytes, needed); return 0; }
+  if (n == "dispersion") { copy_vec(t.dispersion, out, bytes, needed); return 0; }
   if (n == "slist") { copy_vec(t.slist, out, bytes, needed); return 0; }
   if (n == "ntlists") { copy_vec(t.ntlists, out, bytes, needed); return 0; }
   if (n == "ptlists") { copy_vec(t.ptlists, out, bytes, needed); return 0; }
@@ -619,6 +622,9 @@ int mcb200_set_mesh(mcb200_ctx *c, int nx, int ny, int nz, const double *lx, con
     for (int i = 0; i < nx; ++i) dx[i] = wx ? wx[i] : c->hlx[i + 1] - c->hlx[i];
     for (int i = 0; i < ny; ++i) dy[i] = wy ? wy[i] : c->hly[i + 1] - c->hly[i];
     for (int i = 0; i < nz; ++i) dz[i] = wz ? wz[i] : c->hlz[i + 1] - c->hlz[i];
+    c->hdx = dx;
+    c->hdy = dy;
+    c->hdz = dz;
     DevMesh &m = c->mesh;
     m = DevMesh{};
     m.nx = nx; m.ny = ny; m.nz = nz;
@@ -652,6 +658,11 @@ int mcb200_set_mesh(mcb200_ctx *c, int nx, int ny, int nz, const double *lx, con
     c->sb.node = dalloc<long long>(nodes * 10, c->mesh_owned);
     c->sb.cell_count = dalloc<unsigned long long>(cells, c->mesh_owned);
     c->sb.pot_sum = dalloc<double>(nodes, c->mesh_owned);
+    c->sb.qc_pot_sum = dalloc<double>(nodes, c->mesh_owned);
+    c->qc = QuantumDevice{};
+    c->qc_pot = nullptr;
+    c->pot_scratch = nullptr;
+    c->qc_set = c->qc_on = false;
     c->stat_bounds = dalloc<unsigned long long>(4, c->mesh_owned);
     c->eeff_dev = dalloc<int>(cells, c->mesh_owned);
     c->eeff_host.clear();
@@ -698,6 +709,10 @@ int mcb200_set_cells(mcb200_ctx *c, const int32_t *motion_rule, const int32_t *a
     m.surface_scatter = (flags & MCB200_FLAG_SURFACE_SCATTER) ? 1 : 0;
     m.surface_impurity = (flags & MCB200_FLAG_SURFACE_IMPURITY) ? 1 : 0;
     m.heat = (flags & MCB200_FLAG_HEAT) ? 1 : 0;
+    m.quantum = (flags & MCB200_FLAG_QUANTUM) ? 1 : 0;
+    if (m.quantum && !c->ts->dt.disp)
+      return fail(c, MCB200_ERR_STATE, "quantum correction needs the phonon dispersion tables (kloem.txt, kloab.txt, "
+                                       "ktoem.txt, ktoab.txt, klaem.txt, klaab.txt in the table directory)");
     mr_scratch(c);
     c->cells_set = true;
     return MCB200_OK;
@@ -1366,6 +1381,87 @@ int mcb200_multiple_refresh(mcb200_ctx *c, const int32_t *desired_e, const int32
   }
 }
 
+int mcb200_set_quantum_correction(mcb200_ctx *c, const mcb200_quantum_params *p, const int32_t *material,
+                                  const int32_t *quantum_region, int enable) {
+  if (!c) return MCB200_ERR_ARG;
+  if (c->device < 0) return fail(c, MCB200_ERR_STATE, "host-only context");
+  if (!c->mesh_set) return fail(c, MCB200_ERR_STATE, "mcb200_set_quantum_correction before mcb200_set_mesh");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    if (p) {
+      if (!material || !quantum_region)
+        return fail(c, MCB200_ERR_ARG, "mcb200_set_quantum_correction: material and quantum_region are required");
+      QuantumParams q;
+      for (int a = 0; a < 3; ++a) {
+        q.ratio[a] = p->ratio[a];
+        q.theta[a] = p->theta[a];
+      }
+      q.eb = p->eb;
+      const DevMesh &m = c->mesh;
+      QuantumHost h;
+      try {
+        h = quantum_setup(m.nx, m.ny, m.nz, c->hlx.data(), c->hly.data(), c->hlz.data(), c->hdx.data(), c->hdy.data(),
+                          c->hdz.data(), material, quantum_region, q);
+      } catch (const std::invalid_argument &e) {
+        return fail(c, MCB200_ERR_ARG, e.what());
+      }
+      ck(cudaStreamSynchronize(c->stream), "sync");  // a running solve may read the previous set-up
+      QuantumDevice d;
+      d.px = m.nx + 1; d.py = m.ny + 1; d.pz = m.nz + 1;
+      d.n_list = (int)h.list.size();
+      d.list = h.list.empty() ? nullptr : dupload(h.list, c->mesh_owned);
+      d.inside = dupload(h.inside, c->mesh_owned);
+      d.eb = dupload(h.eb, c->mesh_owned);
+      d.range = dupload(h.range, c->mesh_owned);
+      d.qcl = dupload(h.qcl, c->mesh_owned);
+      std::vector<int2> win(h.lower.size());
+      for (size_t i = 0; i < win.size(); ++i) win[i] = make_int2(h.lower[i], h.upper[i]);
+      d.window = dupload(win, c->mesh_owned);
+      c->qc = d;
+      if (!c->qc_pot) c->qc_pot = dalloc<double>((size_t)d.px * d.py * d.pz, c->mesh_owned);
+      c->qc_set = true;
+    }
+    if (enable && !c->qc_set)
+      return fail(c, MCB200_ERR_STATE, "mcb200_set_quantum_correction: no set-up (params, material, region)");
+    const bool was = c->qc_on;
+    c->qc_on = enable != 0;
+    if (c->device_set && (c->qc_on != was || (p && c->qc_on))) {
+      // the current potential's fields, with or without the correction, so
+      // that the fields and the statistics agree before the next solve
+      if (c->qc_on) {
+        launch_effective_potential(c->qc, c->fb.potential, c->qc_pot, c->stream);
+        launch_pot2field(c->mesh, c->fb.potential, c->stream, c->qc_pot);
+      } else {
+        launch_pot2field(c->mesh, c->fb.potential, c->stream);
+      }
+      ck(cudaGetLastError(), "quantum correction");
+    }
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_quantum_potential(mcb200_ctx *c, const double *potential, double *out) {
+  if (!c || !potential || !out) return MCB200_ERR_ARG;
+  if (!c->qc_set) return fail(c, MCB200_ERR_STATE, "mcb200_quantum_potential needs mcb200_set_quantum_correction");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    const size_t nodes = (size_t)c->qc.px * c->qc.py * c->qc.pz;
+    if (!c->pot_scratch) c->pot_scratch = dalloc<double>(2 * nodes, c->mesh_owned);
+    ck(cudaMemcpyAsync(c->pot_scratch, potential, nodes * sizeof(double), cudaMemcpyHostToDevice, c->stream), "copy");
+    launch_effective_potential(c->qc, c->pot_scratch, c->pot_scratch + nodes, c->stream);
+    ck(cudaGetLastError(), "effective potential");
+    ck(cudaMemcpyAsync(out, c->pot_scratch + nodes, nodes * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
+       "copy");
+    ck(cudaStreamSynchronize(c->stream), "sync");
+    c->launches += 2;
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
 int mcb200_set_refresh_targets(mcb200_ctx *c, const int32_t *desired_e, const int32_t *desired_h) {
   if (!c || !desired_e || !desired_h) return MCB200_ERR_ARG;
   if (!c->cells_set) return fail(c, MCB200_ERR_STATE, "mcb200_set_refresh_targets before mcb200_set_cells");
@@ -1385,6 +1481,10 @@ int mcb200_set_refresh_targets(mcb200_ctx *c, const int32_t *desired_e, const in
 }
 
 int mcb200_set_potential(mcb200_ctx *c, const double *potential) {
+  return mcb200_set_potentials(c, potential, nullptr);
+}
+
+int mcb200_set_potentials(mcb200_ctx *c, const double *potential, const double *electron_potential) {
   if (!c || !potential) return MCB200_ERR_ARG;
   if (!c->device_set) return fail(c, MCB200_ERR_STATE, "mcb200_set_potential needs mcb200_set_device");
   try {
@@ -1392,7 +1492,15 @@ int mcb200_set_potential(mcb200_ctx *c, const double *potential) {
     const size_t nodes = (size_t)(c->mesh.nx + 1) * (c->mesh.ny + 1) * (c->mesh.nz + 1);
     ck(cudaMemcpyAsync(c->fb.potential, potential, nodes * sizeof(double), cudaMemcpyHostToDevice, c->stream),
        "copy");
-    launch_pot2field(c->mesh, c->fb.potential, c->stream);
+    const double *pot_e = nullptr;
+    if (electron_potential) {
+      if (!c->pot_scratch) c->pot_scratch = dalloc<double>(2 * nodes, c->mesh_owned);
+      ck(cudaMemcpyAsync(c->pot_scratch, electron_potential, nodes * sizeof(double), cudaMemcpyHostToDevice,
+                         c->stream),
+         "copy");
+      pot_e = c->pot_scratch;
+    }
+    launch_pot2field(c->mesh, c->fb.potential, c->stream, pot_e);
     ck(cudaGetLastError(), "pot2field");
     ck(cudaStreamSynchronize(c->stream), "sync");
     c->launches += 1;
@@ -1439,6 +1547,7 @@ int mcb200_stat_begin(mcb200_ctx *c, int window_steps) {
     ck(cudaMemsetAsync(c->sb.node, 0, sizeof(long long) * nodes * 10, s), "memset");
     ck(cudaMemsetAsync(c->sb.cell_count, 0, sizeof(unsigned long long) * c->ncells, s), "memset");
     ck(cudaMemsetAsync(c->sb.pot_sum, 0, sizeof(double) * nodes, s), "memset");
+    ck(cudaMemsetAsync(c->sb.qc_pot_sum, 0, sizeof(double) * nodes, s), "memset");
     ck(cudaStreamSynchronize(s), "sync");
     c->stat_steps = 0;
     c->stat_open = true;
@@ -1460,10 +1569,15 @@ int mcb200_stat_accumulate(mcb200_ctx *c) {
       launch_statistic(store<float>(c, c->cur), n, c->mesh, c->ts->dt, c->ss, c->sb, grid, s);
     else
       launch_statistic(store<double>(c, c->cur), n, c->mesh, c->ts->dt, c->ss, c->sb, grid, s);
-    if (c->device_set) launch_add_potential(c->sb.nodes, c->fb.potential, c->sb.pot_sum, s);
+    if (c->device_set) {
+      // statistic (src/mcmodel.cpp:1184-1199): the Poisson potential and the
+      // electrons' (quantum-corrected) one
+      launch_add_potential(c->sb.nodes, c->fb.potential, c->sb.pot_sum, s);
+      launch_add_potential(c->sb.nodes, c->qc_on ? c->qc_pot : c->fb.potential, c->sb.qc_pot_sum, s);
+    }
     ck(cudaGetLastError(), "statistic");
     c->stat_steps += 1;
-    c->launches += 1 + (c->device_set ? 1 : 0);
+    c->launches += 1 + (c->device_set ? 2 : 0);
     return MCB200_OK;
   } catch (const std::exception &e) {
     return fail(c, MCB200_ERR_CUDA, e.what());
@@ -1490,9 +1604,10 @@ int mcb200_stat_get(mcb200_ctx *c, const char *name, double *out, size_t n) {
       for (size_t q = 0; q < cells; ++q) out[q] = (double)h[q];
       return MCB200_OK;
     }
-    if (nm == "pot_sum") {
+    if (nm == "pot_sum" || nm == "qc_pot_sum") {
       if (n < nodes) return fail(c, MCB200_ERR_CAPACITY, "output too small");
-      ck(cudaMemcpy(out, c->sb.pot_sum, nodes * 8, cudaMemcpyDeviceToHost), "copy");
+      ck(cudaMemcpy(out, nm == "pot_sum" ? c->sb.pot_sum : c->sb.qc_pot_sum, nodes * 8, cudaMemcpyDeviceToHost),
+         "copy");
       return MCB200_OK;
     }
     // electron_* / hole_*: qvx, qvy, qvz, q, qe per node
@@ -1537,6 +1652,7 @@ int mcb200_get_array(mcb200_ctx *c, const char *name, double *out, size_t n) {
   else if (c->device_set && nm == "vadd") { src = c->fb.vadd; len = nodes; }
   else if (c->device_set && nm == "rhs") { src = c->fb.rhs; len = nodes; }
   else if (c->device_set && nm == "potential") { src = c->fb.potential; len = nodes; }
+  else if (c->qc_set && nm == "qc_potential") { src = c->qc_pot; len = nodes; }
   else if (c->device_set && nm == "stencil") { src = c->fb.stencil; len = 7 * nodes; }
   else return fail(c, MCB200_ERR_ARG, "unknown array " + nm);
   if (n < len) return fail(c, MCB200_ERR_CAPACITY, "output smaller than array " + nm);
@@ -1579,7 +1695,13 @@ void poisson_enqueue(mcb200_ctx *c, cudaStream_t s, double rel_tol, int max_iter
 
 void poisson_finish(mcb200_ctx *c, cudaStream_t s, int *iterations, double *rel_residual) {
   if (cg_finish(c->mesh, c->fb, s, c->h_scratch, iterations, rel_residual)) throw CudaError("Poisson solve failed");
-  launch_pot2field(c->mesh, c->fb.potential, s);
+  if (c->qc_on) {  // compute_field, src/mcmodel.cpp:2240-2262
+    launch_effective_potential(c->qc, c->fb.potential, c->qc_pot, s);
+    launch_pot2field(c->mesh, c->fb.potential, s, c->qc_pot);
+    c->launches += 2;
+  } else {
+    launch_pot2field(c->mesh, c->fb.potential, s);
+  }
   ck(cudaGetLastError(), "pot2field");
   // rhs, the solve's set-up / dots / persistent CG / true residual /
   // statistics (16 with Jacobi preconditioning, 13 with multigrid: no

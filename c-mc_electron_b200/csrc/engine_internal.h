@@ -13,6 +13,7 @@
 #include "cell_kernels.h"
 #include "engine_kernels.h"
 #include "field_kernels.h"
+#include "quantum_setup.h"
 #include "flight_physics.cuh"
 #include "fullband_tables.h"
 #include "mcb200.h"
@@ -129,6 +130,7 @@ struct mcb200_ctx {
   DevMesh mesh{};
   bool mesh_set = false, cells_set = false, fields_set = false;
   std::vector<double> hlx, hly, hlz;
+  std::vector<double> hdx, hdy, hdz;  // cell widths as given to mcb200_set_mesh
   // particles: two buffers, the store ping-pongs through the cell sort
   int precision = MCB200_FLIGHT_FP64;
   std::vector<void *> store_owned;  // particle and child buffers (reallocated on a precision change)
@@ -154,6 +156,12 @@ struct mcb200_ctx {
   int ncells = 0;
   unsigned int *h_pinned = nullptr;  // small pinned readback area
   MrScratch mr;                      // in mesh_owned
+  // effective-potential quantum correction (mcb200_set_quantum_correction);
+  // arrays in mesh_owned.  qc_on: solves give electrons the corrected field
+  QuantumDevice qc;
+  double *qc_pot = nullptr;
+  double *pot_scratch = nullptr;  // [2][nodes]: caller potentials (mcb200_set_potentials, mcb200_quantum_potential)
+  bool qc_set = false, qc_on = false;
   int sm_count = 148;
   int grid_per_sm = 8;  // blocks per SM of the grid-stride per-step kernels (sort, deposition, copies)
   // deposition / Poisson (mcb200_set_device)

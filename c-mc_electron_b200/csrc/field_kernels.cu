@@ -382,28 +382,36 @@ __global__ void cg_setup(double *sc, double rel_tol2) {
   sc[8] = 0.0;
 }
 
-// pot2field / pot2field_for_hole, src/mcmodel.cpp:2732-2855 (no quantum
-// correction): the same field for both carriers, stored as felt.
-__global__ void pot2field_kernel(DevMesh M, const double *pot, double *efield, double *hfield) {
+// pot2field / pot2field_for_hole, src/mcmodel.cpp:2732-2855: the field of
+// each cell from the averaged edge differences of its corner potentials,
+// stored as felt.  Holes take it from the Poisson potential, electrons from
+// pot_e: the same potential, or the quantum-corrected one (compute_field,
+// :2240-2262).
+__global__ void pot2field_kernel(DevMesh M, const double *pot, const double *pot_e, double *efield, double *hfield) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int cells = M.nx * M.ny * M.nz;
   if (c >= cells) return;
   const int k = c % M.nz, t = c / M.nz, i = t % M.nx, j = t / M.nx;
   const int px = M.nx + 1, pz = M.nz + 1;
-  auto P = [&](int a, int b, int d) { return pot[((size_t)b * px + a) * pz + d]; };
-  const double fx = -(P(i + 1, j, k) - P(i, j, k) + P(i + 1, j + 1, k) - P(i, j + 1, k) + P(i + 1, j, k + 1) -
-                      P(i, j, k + 1) + P(i + 1, j + 1, k + 1) - P(i, j + 1, k + 1)) / (4.0 * M.dx[i]);
-  const double fy = -(P(i, j + 1, k) + P(i + 1, j + 1, k) + P(i, j + 1, k + 1) + P(i + 1, j + 1, k + 1) -
-                      P(i, j, k) - P(i + 1, j, k) - P(i, j, k + 1) - P(i + 1, j, k + 1)) / (4.0 * M.dy[j]);
-  const double fz = -(P(i, j, k + 1) + P(i + 1, j, k + 1) + P(i, j + 1, k + 1) + P(i + 1, j + 1, k + 1) -
-                      P(i, j, k) - P(i + 1, j, k) - P(i, j + 1, k) - P(i + 1, j + 1, k)) / (4.0 * M.dz[k]);
+  auto field = [&](const double *v, double &fx, double &fy, double &fz) {
+    auto P = [&](int a, int b, int d) { return v[((size_t)b * px + a) * pz + d]; };
+    fx = -(P(i + 1, j, k) - P(i, j, k) + P(i + 1, j + 1, k) - P(i, j + 1, k) + P(i + 1, j, k + 1) - P(i, j, k + 1) +
+           P(i + 1, j + 1, k + 1) - P(i, j + 1, k + 1)) / (4.0 * M.dx[i]);
+    fy = -(P(i, j + 1, k) + P(i + 1, j + 1, k) + P(i, j + 1, k + 1) + P(i + 1, j + 1, k + 1) - P(i, j, k) -
+           P(i + 1, j, k) - P(i, j, k + 1) - P(i + 1, j, k + 1)) / (4.0 * M.dy[j]);
+    fz = -(P(i, j, k + 1) + P(i + 1, j, k + 1) + P(i, j + 1, k + 1) + P(i + 1, j + 1, k + 1) - P(i, j, k) -
+           P(i + 1, j, k) - P(i, j + 1, k) - P(i + 1, j + 1, k)) / (4.0 * M.dz[k]);
+  };
+  double fx, fy, fz;
+  field(pot, fx, fy, fz);
   // ChargeSign = {-1, +1} (src/Constant_GlobalVariable_MathFunction.cpp:18)
-  efield[3 * (size_t)c + 0] = -1.0 * fx;
-  efield[3 * (size_t)c + 1] = -1.0 * fy;
-  efield[3 * (size_t)c + 2] = -1.0 * fz;
   hfield[3 * (size_t)c + 0] = fx;
   hfield[3 * (size_t)c + 1] = fy;
   hfield[3 * (size_t)c + 2] = fz;
+  if (pot_e != pot) field(pot_e, fx, fy, fz);
+  efield[3 * (size_t)c + 0] = -1.0 * fx;
+  efield[3 * (size_t)c + 1] = -1.0 * fy;
+  efield[3 * (size_t)c + 2] = -1.0 * fz;
 }
 
 // ---------------------------------------------------------------------------
@@ -554,9 +562,9 @@ int cg_solve(const DevMesh &M, const FieldBuffers &f, double rel_tol, int max_it
   return cg_finish(M, f, s, host_scratch, iterations, rel_residual);
 }
 
-void launch_pot2field(const DevMesh &M, const double *pot, cudaStream_t s) {
+void launch_pot2field(const DevMesh &M, const double *pot, cudaStream_t s, const double *pot_e) {
   const int cells = M.nx * M.ny * M.nz;
-  pot2field_kernel<<<blocks(cells, 256), 256, 0, s>>>(M, pot, const_cast<double *>(M.efield),
+  pot2field_kernel<<<blocks(cells, 256), 256, 0, s>>>(M, pot, pot_e ? pot_e : pot, const_cast<double *>(M.efield),
                                                         const_cast<double *>(M.hfield));
 }
 

@@ -71,6 +71,7 @@ int cg_launch(const DevMesh &M, const FieldBuffers &f, int max_iter, cudaStream_
 int cg_finish(const DevMesh &M, const FieldBuffers &f, cudaStream_t s, double *host_scratch, int *iterations,
               double *rel_residual);
 MgSystem cg_mg_system(const DevMesh &M, const FieldBuffers &f, int max_iter);
-void launch_pot2field(const DevMesh &M, const double *pot, cudaStream_t s);
+// Fields of both carriers from pot; with pot_e, the electrons' from pot_e.
+void launch_pot2field(const DevMesh &M, const double *pot, cudaStream_t s, const double *pot_e = nullptr);
 
 }  // namespace mcb200

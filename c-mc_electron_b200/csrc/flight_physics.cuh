@@ -685,8 +685,87 @@ struct FlyerT {
     iband = fs_ib; itet = fs_it; isym = fs_is;
   }
 
-  // Set-up of EPSCAT (src/ElectronPhononScatter.cpp:98-195,
-  // Flag_QuantumCorrection = 0), ESCATII (:406-497, seciifl = false), HPSCAT
+  // FEKLOEM / FEKLOAB / FEKTOEM / FEKTOAB / FEKLAEM / FEKLAAB
+  // (src/ElectronPhononScatter.cpp:633-1022), table-driven: the final energy
+  // of an LO / TO / LA phonon event under quantum correction.  The energy in
+  // phonon quanta selects a column of the dispersion table (per-range
+  // offset, scale and spacing edeta); one draw walks the column's
+  // cumulative sum to a row i, and the final energy is the phonon energy
+  // shifted by +-(i / 2) steps of c * edeta.  Below one quantum the emission
+  // tables return at once, without a draw.  `which` follows kDispNames.
+  __device__ double fek(int which, double eet) {
+    const DevTables &T = F.T;
+    const bool emit = (which & 1) == 0;
+    const int phon = which >> 1;  // 0 LO, 1 TO, 2 LA
+    const double e = phon == 0 ? T.templog : (phon == 1 ? T.temptof : T.templaf);
+    const double ie = eet / e;
+    if (emit && ie < 1.0) return phon == 2 ? -1.0e-10 : 1.0e-10;
+    // energy ranges: upper bound, offset, scale, first column, edeta
+    double shift, mult, edeta;
+    int base;
+    bool last = false;
+    if (phon == 0 && emit) {  // FEKLOEM
+      if (ie < 3.05) { shift = 1.0; mult = 10.0; base = 0; edeta = 1.0; }
+      else if (ie < 5.625) { shift = 3.0; mult = 4.0; base = 20; edeta = 2.0; }
+      else if (ie < 13.25) { shift = 5.5; mult = 2.0; base = 30; edeta = 4.0; }
+      else if (ie < 28.5) { shift = 13.0; mult = 1.0; base = 45; edeta = 8.0; }
+      else { shift = 28.0; mult = 1.0; base = 60; edeta = 12.0; last = true; }
+    } else if (phon == 0) {  // FEKLOAB
+      if (ie < 1.05) { shift = 0.0; mult = 10.0; base = 0; edeta = 1.0; }
+      else if (ie < 3.625) { shift = 1.0; mult = 4.0; base = 10; edeta = 2.0; }
+      else if (ie < 11.25) { shift = 3.5; mult = 2.0; base = 20; edeta = 4.0; }
+      else if (ie < 26.5) { shift = 11.0; mult = 1.0; base = 35; edeta = 8.0; }
+      else { shift = 26.0; mult = 1.0; base = 50; edeta = 12.0; last = true; }
+    } else if (emit) {  // FEKTOEM, FEKLAEM
+      if (ie < 3.05) { shift = 1.0; mult = 10.0; base = 0; edeta = 0.25; }
+      else if (ie < 5.625) { shift = 3.0; mult = 4.0; base = 20; edeta = 0.5; }
+      else if (ie < 13.25) { shift = 5.5; mult = 2.0; base = 30; edeta = 0.5; }
+      else { shift = 13.0; mult = 1.0; base = 45; edeta = 1.0; last = true; }
+    } else {  // FEKTOAB, FEKLAAB
+      if (ie < 1.05) { shift = 0.0; mult = 10.0; base = 0; edeta = 0.25; }
+      else if (ie < 3.625) { shift = 1.0; mult = 4.0; base = 10; edeta = 0.25; }
+      else if (ie < 11.25) { shift = 3.5; mult = 2.0; base = 20; edeta = 0.5; }
+      else { shift = 11.0; mult = 1.0; base = 35; edeta = 1.0; last = true; }
+    }
+    int it = (int)((ie - shift) * mult + 0.5);
+    if (it < 1) it = 1;
+    if (last) {  // the last range's cap
+      if (phon == 0) { if (it > 60) it = 60; }
+      else if (emit) { if (it > 115) it = 115; }
+      else if (it > 60) it = 115;  // as the reference: past 60 the column jumps to 150
+    }
+    const int ei = base + it;
+    const int cols = phon == 0 ? (emit ? 120 : 110) : (emit ? 160 : 150);
+    const int rows = phon == 0 ? 201 : 51;
+    const double *tab = T.disp + T.disp_off[which] + (ei - 1);
+    const double ran = (double)Random();
+    int i = 0;
+    double ksum = 0.0;
+    if (which == 0) {  // FEKLOEM wraps before adding: rows 0..199
+      while (ksum < ran) {
+        ++i;
+        if (i == rows) { ksum = 1.1; i = 1; }
+        ksum += tab[(size_t)(i - 1) * cols];
+      }
+    } else {
+      while (ksum < ran) {
+        ++i;
+        ksum += tab[(size_t)(i - 1) * cols];
+        if (i == rows) { ksum = 1.1; i = 1; }
+      }
+    }
+    const int j = i % 2, k = i / 2;
+    const double c = phon == 0 ? 0.01 : 0.04;
+    double ef;
+    if (emit) ef = j == 1 ? eet - e * (1.0 - c * edeta * k) : eet - e * (1.0 + c * edeta * k);
+    else ef = j == 1 ? eet + e * (1.0 + c * edeta * k) : eet + e * (1.0 - c * edeta * k);
+    if (phon == 2 && ef <= 0.0) ef = 1.0e-5 * e;
+    return ef;
+  }
+
+  // Set-up of EPSCAT (src/ElectronPhononScatter.cpp:98-195; with
+  // Flag_QuantumCorrection the LO / LA / TO events take their final energy
+  // from fek, :152-167), ESCATII (:406-497, seciifl = false), HPSCAT
   // (src/HolePhononScatter.cpp:86-146) and HSCATII (:149-234) for mechanism
   // iscat: the final band and energy, and the wedge rule of the draw
   // (fs_tal: 1..3 = TALIND(ityp), 0 = a random isym, -1 = none).
@@ -718,6 +797,12 @@ struct FlyerT {
         case 11: energy = energy + T.temptof; fs_tal = 3; break;
         case 12: energy = energy - T.temptof; fs_tal = 3; break;
         default: fs_tal = -1; break;
+      }
+      if (I->M.quantum && (m == 5 || m == 6 || (m >= 9 && m <= 12))) {
+        // the dispersion table of the event: LO 5 / 6, LA 9 / 10, TO 11 / 12
+        // (absorption / emission); the energy before the event
+        static constexpr signed char kTable[13] = {-1, -1, -1, -1, -1, 1, 0, -1, -1, 5, 4, 3, 2};
+        energy = fek(kTable[m], fs_eeold);
       }
     } else {
       iband = iscat / T.scprh + T.bandof[1];

@@ -723,6 +723,30 @@ FullBandTables FullBandTables::build(const std::string &dir, double kelvin) {
     if (g == 0.0) g = t.sumscatt[(size_t)kMaxTab * kNumBandsMax + t.ibt[it]];
     t.gamtet[it] = g;
   }
+  // ------------------------------------------------------------ init_deep
+  // src/ParticleUtils.cpp:750-806: for each table, columns (energy bins)
+  // outer, rows inner.  All six or none.
+  {
+    std::vector<double> all;
+    bool ok = true;
+    for (int d = 0; d < kDispTables && ok; ++d) {
+      std::ifstream f(dir + "/" + kDispNames[d] + ".txt");
+      if (!f) {
+        ok = false;
+        break;
+      }
+      t.disp_off[d] = (int)all.size();
+      all.resize(all.size() + (size_t)kDispRows[d] * kDispCols[d]);
+      double *tab = all.data() + t.disp_off[d];
+      for (int col = 0; col < kDispCols[d] && ok; ++col)
+        for (int row = 0; row < kDispRows[d]; ++row)
+          if (!(f >> tab[(size_t)row * kDispCols[d] + col])) {
+            ok = false;
+            break;
+          }
+    }
+    if (ok) t.dispersion.swap(all);
+  }
   return t;
 }
 

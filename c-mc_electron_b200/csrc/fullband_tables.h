@@ -92,6 +92,13 @@ struct FullBandTables {
   double difpr[3];
   double mell, melt, meld;
   double ni = 0;         // intrinsic carrier density (GETINDENS), normalised
+  // --- phonon dispersion tables (init_deep, src/ParticleUtils.cpp:750-806):
+  // the final-energy distributions of the LO / TO / LA phonon events under
+  // quantum correction (FEK*, src/ElectronPhononScatter.cpp:633-1022).
+  // Table d is [kDispRows[d]][kDispCols[d]] at dispersion[disp_off[d]], in
+  // the order of kDispNames; `dispersion` stays empty when a file is absent.
+  std::vector<double> dispersion;
+  int disp_off[6] = {0, 0, 0, 0, 0, 0};
   bool seciifl = false;  // secondary particles from impact ionisation (off in the reference)
 
   // Build everything from a directory holding bs.si.asc and zd.si.asc.
@@ -111,5 +118,13 @@ struct FullBandTables {
 };
 
 double fii(double x1, double y1, double z1, double x2, double y2, double z2, double x3, double y3, double z3);
+
+// The six dispersion tables: LO emission / absorption, TO emission /
+// absorption, LA emission / absorption (files <name>.txt in the table
+// directory, read column by column as init_deep does).
+constexpr int kDispTables = 6;
+constexpr const char *kDispNames[kDispTables] = {"kloem", "kloab", "ktoem", "ktoab", "klaem", "klaab"};
+constexpr int kDispRows[kDispTables] = {201, 201, 51, 51, 51, 51};
+constexpr int kDispCols[kDispTables] = {120, 110, 160, 150, 160, 150};
 
 }  // namespace mcb200

@@ -17,6 +17,7 @@ struct StatBuffers {
   long long *node = nullptr;                 // [2 types][5: qvx qvy qvz q qE][nodes]
   unsigned long long *cell_count = nullptr;  // [cells]
   double *pot_sum = nullptr;                 // [nodes]
+  double *qc_pot_sum = nullptr;              // [nodes] the electrons' potential (quantum-corrected when on)
   int nodes = 0;
 };
 

@@ -28,6 +28,7 @@ NUM_COUNTERS = 16
 FLAG_SURFACE_SCATTER = 1
 FLAG_SURFACE_IMPURITY = 2
 FLAG_HEAT = 4
+FLAG_QUANTUM = 8
 FLIGHT_FP64 = 0
 FLIGHT_FP32 = 1
 # Poisson preconditioners (mcb200_set_poisson_solver)
@@ -74,7 +75,12 @@ class DeckInfo(ctypes.Structure):
                                             "flag_surface_scatter", "flag_surface_roughness", "flag_surface_phonon",
                                             "flag_surface_impurity", "flag_restart", "n_contacts", "n_planes",
                                             "n_surfaces", "default_electrons", "default_holes")] + \
-               [("output_dir", ctypes.c_char * 512), ("prepared", ctypes.c_int), ("dt", ctypes.c_double)]
+               [("output_dir", ctypes.c_char * 512), ("prepared", ctypes.c_int), ("dt", ctypes.c_double),
+                ("flag_quantum_correction", ctypes.c_int), ("quantum_start_step", ctypes.c_int)]
+
+
+class QuantumParams(ctypes.Structure):
+    _fields_ = [("ratio", ctypes.c_double * 3), ("theta", ctypes.c_double * 3), ("eb", ctypes.c_double)]
 
 
 class BatchMember(ctypes.Structure):
@@ -230,6 +236,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mcb200_stat_accumulate.argtypes = [vp]
     lib.mcb200_stat_get.argtypes = [vp, c.c_char_p, dp, c.c_size_t]
     lib.mcb200_set_potential.argtypes = [vp, dp]
+    lib.mcb200_set_potentials.argtypes = [vp, dp, dp]
+    lib.mcb200_set_quantum_correction.argtypes = [vp, vp, i32p, i32p, c.c_int]
+    lib.mcb200_quantum_potential.argtypes = [vp, dp, dp]
     lib.mcb200_set_heat_tally.argtypes = [vp, c.c_int]
     lib.mcb200_set_flight_precision.argtypes = [vp, c.c_int]
     lib.mcb200_get_flight_precision.argtypes = [vp]
@@ -409,6 +418,42 @@ class Engine:
         pot = np.ascontiguousarray(potential, dtype=np.float64)
         assert pot.size == self.mesh.nnodes
         self._check(self._lib.mcb200_set_potential(self._ctx, _ptr(pot, ctypes.c_double)), "set_potential")
+
+    def set_potentials(self, potential, electron_potential=None):
+        """The holes' field from `potential`, the electrons' from
+        `electron_potential` (default: the same) -- heat_field's pair of
+        mean potentials."""
+        pot = np.ascontiguousarray(potential, dtype=np.float64)
+        assert pot.size == self.mesh.nnodes
+        pe = None if electron_potential is None else np.ascontiguousarray(electron_potential, dtype=np.float64)
+        self._check(self._lib.mcb200_set_potentials(self._ctx, _ptr(pot, ctypes.c_double),
+                                                    None if pe is None else _ptr(pe, ctypes.c_double)),
+                    "set_potentials")
+
+    def set_quantum_correction(self, material=None, quantum_region=None, ratio=(0, 0, 0), theta=(0, 0, 0), eb=0.0,
+                               enable=False, setup=True):
+        """Effective-potential quantum correction (mcb200_set_quantum_correction):
+        with setup, built from per-cell material and quantum-region flags and
+        the normalised window (ratio, theta per axis, barrier eb); enable
+        switches it on for later Poisson solves."""
+        if setup:
+            p = QuantumParams((ctypes.c_double * 3)(*ratio), (ctypes.c_double * 3)(*theta), eb)
+            mat = np.ascontiguousarray(material, dtype=np.int32)
+            reg = np.ascontiguousarray(quantum_region, dtype=np.int32)
+            self._check(self._lib.mcb200_set_quantum_correction(self._ctx, ctypes.byref(p), _ptr(mat, ctypes.c_int32),
+                                                                _ptr(reg, ctypes.c_int32), int(bool(enable))),
+                        "set_quantum_correction")
+        else:
+            self._check(self._lib.mcb200_set_quantum_correction(self._ctx, None, None, None, int(bool(enable))),
+                        "set_quantum_correction")
+
+    def quantum_potential(self, potential) -> np.ndarray:
+        """The effective potential of `potential` (mcb200_quantum_potential)."""
+        pot = np.ascontiguousarray(potential, dtype=np.float64)
+        out = np.empty_like(pot)
+        self._check(self._lib.mcb200_quantum_potential(self._ctx, _ptr(pot, ctypes.c_double),
+                                                       _ptr(out, ctypes.c_double)), "quantum_potential")
+        return out
 
     def set_poisson_solver(self, method=POISSON_AUTO, blocks=0):
         """Preconditioner of the following solves (POISSON_AUTO / _JACOBI /

@@ -126,7 +126,7 @@ def finfet_grid(lg_nm: float = 20.0):
 
 def finfet(dirpath: str, electrons=300000, holes=50000, vd=0.7, vg=0.8, phims=-0.46, dt=2e-16, total_step=7000,
            heat_steps=3000, stat_step=1000, mr_step=50, surface_scatter=True, compute_heat=True,
-           delta_nm=0.4, lambda_nm=1.5, kelvin=300.0, lg_nm=20.0, min_per_cell=(3, 1)) -> dict:
+           delta_nm=0.4, lambda_nm=1.5, kelvin=300.0, lg_nm=20.0, min_per_cell=(3, 1), quantum=None) -> dict:
     """The n-FinFET of the self-consistent workload, in the reference's deck
     language and with the reference FinFET's topology (finfet/ldg.txt):
     fin 30 nm tall (x) and 10 nm wide (z), gate length lg_nm (y; 20 nm by
@@ -141,7 +141,10 @@ def finfet(dirpath: str, electrons=300000, holes=50000, vd=0.7, vg=0.8, phims=-0
     silicon cell (default_par_number).  Doping values are in m^-3 as the
     reference reads them.  The surface-roughness parameters go to input.txt
     as surface_roughness_delta_nm / surface_roughness_lambda_nm (keys the
-    reference does not read)."""
+    reference does not read).  quantum = (ratio, theta_nm, eb_v, start_step):
+    the effective-potential quantum correction on (Flag_QuantumCorrection,
+    quantum_start_step), with an ep_parm window of ratio * theta_nm on every
+    axis, oxide barrier eb_v, over the gated fin (quantumRegion)."""
     os.makedirs(dirpath, exist_ok=True)
     x, y, z = finfet_grid(lg_nm)
     write_grid(os.path.join(dirpath, "lgrid.txt"), x, y, z)
@@ -207,14 +210,18 @@ def finfet(dirpath: str, electrons=300000, holes=50000, vd=0.7, vg=0.8, phims=-0
         "contact", "1 0", f"66 66 {Y} -17 27", "0",
         "contact", f"3 {g(phims)}", f"-1 -1 {g(-h)} {g(h)} -1 11", f"-1 24 {g(-h)} {g(h)} -1 -1",
         f"-1 24 {g(-h)} {g(h)} 11 11", g(vg),
-        "end",
     ]
+    if quantum is not None:
+        r, t, eb = (g(v) for v in quantum[:3])
+        L += [f"ep_parm {r} {t} {r} {t} {r} {t} {eb}", f"quantumRegion 0 24 {Y} 0 10"]
+    L.append("end")
     with open(os.path.join(dirpath, "ldg.txt"), "w") as f:
         f.write("\n".join(L) + "\n")
     write_input(os.path.join(dirpath, "input.txt"), dt=dt, Temperature=kelvin, total_step=total_step,
                 ElectronNumber=electrons, HoleNumber=holes, Flag_SurfaceScatter=int(surface_scatter),
                 Flag_MultipleRefresh=1, mr_step=mr_step, Flag_compute_heat=int(compute_heat), heat_steps=heat_steps,
                 stat_step=stat_step, stat_heat_step=stat_step, surface_roughness_delta_nm=delta_nm,
-                surface_roughness_lambda_nm=lambda_nm)
+                surface_roughness_lambda_nm=lambda_nm,
+                **({} if quantum is None else dict(Flag_QuantumCorrection=1, quantum_start_step=int(quantum[3]))))
     return dict(input=os.path.join(dirpath, "input.txt"), grid=os.path.join(dirpath, "lgrid.txt"),
                 device=os.path.join(dirpath, "ldg.txt"))

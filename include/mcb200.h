@@ -207,6 +207,31 @@ int mcb200_multiple_refresh(mcb200_ctx *ctx, const int32_t *desired_e, const int
  * counterpart (the reference keeps the targets in MeshQuantities). */
 int mcb200_set_refresh_targets(mcb200_ctx *ctx, const int32_t *desired_e, const int32_t *desired_h);
 
+/* Effective-potential quantum correction (MeshQuantities::
+ * effective_potential / quantumPotential, src/mcmodel.cpp:2337-2403, with
+ * the set-up of init_effective_potential / init_p_mat / init_ep_range,
+ * :2406-2664).  At every node of the quantum region the potential is
+ * replaced, for electrons only, by its Gaussian average over a window of
+ * ratio * theta per axis (oxide nodes raised by the barrier eb); holes keep
+ * the Poisson potential's field (compute_field, :2240-2262).  With params,
+ * the set-up is (re)built from the cells' material (as mcb200_set_device)
+ * and quantum-region flags; enable switches the correction of every later
+ * Poisson solve on or off (the reference applies it from
+ * quantum_start_step on).  Lengths normalised like the mesh (nm / (1e9
+ * spr0)), eb in pot0.  mcb200_get_array "qc_potential": the corrected
+ * potential of the last solve. */
+typedef struct {
+  double ratio[3]; /* qc_{x,y,z}ratio */
+  double theta[3]; /* qc_{x,y,z}theta */
+  double eb;       /* Eb */
+} mcb200_quantum_params;
+int mcb200_set_quantum_correction(mcb200_ctx *ctx, const mcb200_quantum_params *params, const int32_t *material,
+                                  const int32_t *quantum_region, int enable);
+/* out = the effective potential of a caller's potential (every node; the
+ * quantum nodes corrected), as a solve with the correction on applies it.
+ * Waits for the result. */
+int mcb200_quantum_potential(mcb200_ctx *ctx, const double *potential, double *out);
+
 /* Copy a device array to the host: "rho", "e_rough", "e_phonon", "h_rough",
  * "h_phonon", "efield", "hfield" (3 per cell),
  * "cell_charge_e", "cell_charge_h", "cell_volume" (per cell);
@@ -217,6 +242,9 @@ int mcb200_get_array(mcb200_ctx *ctx, const char *name, double *out, size_t n);
 #define MCB200_FLAG_SURFACE_SCATTER 1   /* Flag_SurfaceScatter */
 #define MCB200_FLAG_SURFACE_IMPURITY 2  /* Flag_SurfaceImpurityScatter */
 #define MCB200_FLAG_HEAT 4              /* flag_heat: phonon events tally heat */
+#define MCB200_FLAG_QUANTUM 8           /* Flag_QuantumCorrection: LO / TO / LA phonon final energies drawn
+                                           from the dispersion tables (FEK*, src/ElectronPhononScatter.cpp:
+                                           152-167, 633-1022) */
 
 /* Per-cell data of the device (c_motion_rule: 6 ints per cell in face
  * order UP, DOWN, LEFT, RIGHT, FRONT, BACK; c_attached_contact (1-based);
@@ -415,6 +443,10 @@ int mcb200_sort_particles_static(const mcb200_device_particles *in, size_t n, in
  * fields from it (pot2field): the fixed potential of the reference's heat
  * phase (compute_heat / heat_field, src/heat.cpp:100-128). */
 int mcb200_set_potential(mcb200_ctx *ctx, const double *potential);
+/* The same with the electrons' field from electron_potential (NULL: from
+ * potential): heat_field takes the holes' field from the mean Poisson
+ * potential and the electrons' from the mean quantum-corrected one. */
+int mcb200_set_potentials(mcb200_ctx *ctx, const double *potential, const double *electron_potential);
 /* Phonon events tally heat (flag_heat, src/heat.cpp:108-160) while enabled. */
 int mcb200_set_heat_tally(mcb200_ctx *ctx, int enable);
 
@@ -460,6 +492,7 @@ typedef struct {
   char output_dir[512];
   int prepared;  /* mcb200_deck_prepare has run */
   double dt;     /* dt / time0 once prepared */
+  int flag_quantum_correction, quantum_start_step;
 } mcb200_deck_info;
 
 /* On failure *out may still hold a deck whose mcb200_deck_error() says why. */

@@ -199,6 +199,8 @@ double orc_scalar(const char *name) {
   if (n == "flag_mr") return mq->Flag_MultipleRefresh;
   if (n == "flag_compute_heat") return mq->Flag_compute_heat;
   if (n == "draws") return (double)g_draws;
+  if (n == "flag_quantum_correction") return mq->Flag_QuantumCorrection;
+  if (n == "quantum_start_step") return mq->quantum_start_step;
   return NAN;
 }
 int orc_set_scalar(const char *name, double v) {
@@ -206,6 +208,8 @@ int orc_set_scalar(const char *name, double v) {
   if (n == "flag_heat") { g_mq->flag_heat = v != 0; return 0; }
   if (n == "flag_surface_scatter") { g_mq->Flag_SurfaceScatter = v != 0; return 0; }
   if (n == "dt") { g_mq->dt = v; return 0; }
+  if (n == "flag_quantum_correction") { g_mq->Flag_QuantumCorrection = v != 0; return 0; }
+  if (n == "step") { g_mq->step = (int)v; return 0; }
   return 1;
 }
 
@@ -233,6 +237,7 @@ static Epetra_Vector *cell_vec(const std::string &n) {
   if (n == "p_electron_heat") return mq->p_electron_heat;
   if (n == "p_hole_heat") return mq->p_hole_heat;
   if (n == "p_poisson_pot") return mq->p_poisson_pot;
+  if (n == "p_poisson_pot_saved") return mq->p_poisson_pot_saved;
   if (n == "p_rhs") return mq->p_rhs;
   if (n == "p_par_charge") return mq->p_par_charge;
   if (n == "p_dop") return mq->p_dop;
@@ -380,6 +385,47 @@ int orc_density_and_field() {
   mq->particle_to_density(mq->p_par_charge, 2);
   mq->compute_field();
   mq->compute_cell_charge();
+  return 0;
+}
+
+/* The quantum-correction set-up of the reference's initialisation
+ * (src/mcmodel.cpp:136-140): init_effective_potential, init_p_mat,
+ * init_ep_range, from the deck's ep_parm and quantumRegion.  Once per
+ * orc_init. */
+int orc_init_quantum() {
+  g_mq->init_effective_potential();
+  g_mq->init_p_mat();
+  g_mq->init_ep_range();
+  return 0;
+}
+
+/* The phonon dispersion tables init_deep read (src/ParticleUtils.cpp:
+ * 750-806), as [rows][cols]: 0 kloem, 1 kloab, 2 ktoem, 3 ktoab, 4 klaem,
+ * 5 klaab. */
+int orc_dispersion(int which, double *out) {
+  static const int rows[6] = {201, 201, 51, 51, 51, 51}, cols[6] = {120, 110, 160, 150, 160, 150};
+  MeshQuantities *mq = g_mq;
+  if (which < 0 || which > 5) return 1;
+  for (int r = 0; r < rows[which]; ++r)
+    for (int c = 0; c < cols[which]; ++c) {
+      double v = 0;
+      switch (which) {
+        case 0: v = mq->kloem[r][c]; break;
+        case 1: v = mq->kloab[r][c]; break;
+        case 2: v = mq->ktoem[r][c]; break;
+        case 3: v = mq->ktoab[r][c]; break;
+        case 4: v = mq->klaem[r][c]; break;
+        default: v = mq->klaab[r][c]; break;
+      }
+      out[r * cols[which] + c] = v;
+    }
+  return 0;
+}
+
+/* quantumPotential (src/mcmodel.cpp:2378-2403): p_poisson_pot replaced by
+ * the effective potential at every quantum node. */
+int orc_quantum_potential() {
+  g_mq->quantumPotential();
   return 0;
 }
 

@@ -155,6 +155,21 @@ class Oracle:
         self.lib.orc_multiple_refresh.argtypes = [ctypes.c_uint32]
         return int(self.lib.orc_multiple_refresh(step))
 
+    def init_quantum(self):
+        """The reference's quantum-correction set-up (init_effective_potential,
+        init_p_mat, init_ep_range), from the deck's ep_parm and quantumRegion."""
+        self.lib.orc_init_quantum()
+
+    def dispersion(self, which: int, rows: int, cols: int) -> np.ndarray:
+        out = np.zeros(rows * cols)
+        self.lib.orc_dispersion.argtypes = [ctypes.c_int, ctypes.c_void_p]
+        assert self.lib.orc_dispersion(which, out.ctypes.data) == 0
+        return out
+
+    def quantum_potential(self):
+        """quantumPotential: p_poisson_pot corrected at the quantum nodes."""
+        self.lib.orc_quantum_potential()
+
     def density_and_field(self):
         """particle_to_density -> compute_field (Poisson + pot2field) -> compute_cell_charge."""
         self.lib.orc_density_and_field()

@@ -84,9 +84,11 @@ def compare(a: dict, b: dict) -> dict:
 
 
 def run_bulk_parity(n_particles: int = 2000, steps: int = 3, seed: int = 11, field_v_per_m: float = 1e6,
-                    cells=(8, 6, 6), heat: bool = False) -> dict:
+                    cells=(8, 6, 6), heat: bool = False, quantum: bool = False) -> dict:
     """Bulk n-Si box, frozen uniform field: `steps` transport steps through
-    both implementations from the oracle's own initial ensemble."""
+    both implementations from the oracle's own initial ensemble.  quantum:
+    Flag_QuantumCorrection on both sides (LO / TO / LA final energies from
+    the dispersion tables)."""
     nx, ny, nz = cells
     with tempfile.TemporaryDirectory() as tmp:
         deck = decks.bulk_box(tmp, nx=nx, ny=ny, nz=nz, electrons=n_particles, holes=n_particles // 4)
@@ -96,10 +98,13 @@ def run_bulk_parity(n_particles: int = 2000, steps: int = 3, seed: int = 11, fie
     orc.compute_cell_charge()
     if heat:
         orc.set_scalar("flag_heat", 1)
+    if quantum:
+        orc.set_scalar("flag_quantum_correction", 1)
     dt = orc.scalar("dt")
     p0 = orc.particles()
     n0 = len(p0["x"])
-    eng = engine_from_oracle(orc, max_particles=max(4 * n0, 4096), flags=mcb200.FLAG_HEAT if heat else 0)
+    flags = (mcb200.FLAG_HEAT if heat else 0) | (mcb200.FLAG_QUANTUM if quantum else 0)
+    eng = engine_from_oracle(orc, max_particles=max(4 * n0, 4096), flags=flags)
     eng.upload(p0)
     orc.reset_tallies()
     worst = {"mismatch": 0}
@@ -113,6 +118,7 @@ def run_bulk_parity(n_particles: int = 2000, steps: int = 3, seed: int = 11, fie
             break
         worst = res
     t = eng.tallies()
+    worst["energy_sum"] = float(np.sum(eng.download()["energy"]))
     worst.update(n_start=n0, phonon_engine=t["phonon"], phonon_oracle=int(orc.scalar("phonon_scatter")),
                  impurity_engine=t["impurity"], impurity_oracle=int(orc.scalar("impurity_scatter")),
                  events=t["events"], caught_engine=t["caught"], caught_oracle=int(orc.scalar("catch_par_num")))
