@@ -474,6 +474,33 @@ DeckScaled DeckScaled::build(const Deck &d, const Units &u, double ni) {
     if (s.desired_e[c] < d.default_e) s.desired_e[c] = d.default_e;
     if (s.desired_h[c] < d.default_h) s.desired_h[c] = d.default_h;
   }
+  // Flag_restart (init_particle_data, src/particle_init.cpp:130-134, with
+  // read_par_info_for_restart, src/mcmodel.cpp:853-889): the restart file's
+  // lines "i j k |q|_e n_e |q|_h n_h", ended by a negative i, replace the
+  // carrier counts of the cells they name (the refresh targets keep theirs)
+  // and give the charges a restarted silicon cell away from the contacts
+  // shares among its carriers.  Cells off the mesh are skipped.
+  if (d.flag_restart) {
+    const std::string path = resolve(d.base_dir, d.restart_file);
+    std::ifstream f(path);
+    if (!f) throw DeckError("cannot open the restart file " + path);
+    s.restart_e_charge.assign(cells, 0.0);
+    s.restart_h_charge.assign(cells, 0.0);
+    for (;;) {
+      int i = 0, j = 0, k = 0;
+      if (!(f >> i >> j >> k)) throw DeckError("restart file " + path + " ends before its -1 line");
+      if (i < 0) break;
+      double c1 = 0, c2 = 0;
+      int n1 = 0, n2 = 0;
+      if (!(f >> c1 >> n1 >> c2 >> n2)) throw DeckError("restart file " + path + ": short line");
+      if (i >= d.nx || j < 0 || j >= d.ny || k < 0 || k >= d.nz) continue;
+      const int c = d.cell(i, j, k);
+      s.restart_e_charge[c] = c1;
+      s.restart_h_charge[c] = c2;
+      s.electron_num[c] = n1;
+      s.hole_num[c] = n2;
+    }
+  }
   return s;
 }
 

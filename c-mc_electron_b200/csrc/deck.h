@@ -72,6 +72,8 @@ struct DeckScaled {
   double surface_pos[30] = {0};
   std::vector<int> electron_num, hole_num;  // compute_par_num, src/particle_init.cpp:17-74
   std::vector<int> desired_e, desired_h;    // raised by compute_par_num
+  // Flag_restart: per-cell |q| sums of the restart file (its counts replace electron_num / hole_num)
+  std::vector<double> restart_e_charge, restart_h_charge;
   std::vector<double> vapp, phims;          // per contact, / pot0
   double dt = 0;                            // / time0
   double qc_theta[3] = {0, 0, 0}, qc_eb = 0;  // ep_parm: theta / (1e9 spr0), Eb / pot0 (:4549-4556)

@@ -91,6 +91,7 @@ int mcb200_deck_get_info(const mcb200_deck *k, mcb200_deck_info *info) {
   info->flag_surface_impurity = d.flag_surface_impurity;
   info->flag_restart = d.flag_restart;
   info->flag_quantum_correction = d.flag_quantum_correction;
+  info->restart_step = d.restart_step;
   info->quantum_start_step = d.quantum_start_step;
   info->n_contacts = (int)d.contacts.size();
   int planes = 0;
@@ -242,7 +243,12 @@ int mcb200_seed_deck(mcb200_ctx *ctx, mcb200_deck *k, uint64_t seed) {
           const int c = d.cell(i, j, kk);
           if (d.material[c] != kMatSilicon) continue;
           const int pnum = type == 0 ? s.electron_num[c] : s.hole_num[c];
-          const double q = (type == 0 ? s.init_e_charge[c] : s.init_h_charge[c]) / pnum;
+          // restarted cells away from the contacts keep the file's charge
+          // (electrons negative), src/particle_init.cpp:157-178
+          const bool restarted = d.flag_restart && d.attached_contact[c] <= 0;
+          if (restarted && pnum == 0) continue;
+          const double q = restarted ? (type == 0 ? -s.restart_e_charge[c] : s.restart_h_charge[c]) / pnum
+                                     : (type == 0 ? s.init_e_charge[c] : s.init_h_charge[c]) / pnum;
           for (int p = 0; p < pnum; ++p) {
             cell_of.push_back(c);
             charge.push_back(q);

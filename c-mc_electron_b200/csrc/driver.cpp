@@ -357,7 +357,10 @@ struct Run {
     uint64_t ps_start = 0;
     ok(mcb200_particle_steps(ctx, &ps_start), ctx, "mcb200_particle_steps");
     ok(mcb200_set_timing(ctx, 1), ctx, "mcb200_set_timing");
-    const int steps = opt.max_steps > 0 ? std::min(opt.max_steps, info.total_step) : info.total_step;
+    // run(): from restart_step on with Flag_restart (src/mcmodel.cpp:507-518)
+    const int first = info.flag_restart ? std::max(0, info.restart_step) : 0;
+    const int remaining = std::max(0, info.total_step - first);
+    const int steps = opt.max_steps > 0 ? std::min(opt.max_steps, remaining) : remaining;
     const int warm = std::max(0, std::min(opt.warmup_steps, steps));
     ok(mcb200_stat_begin(ctx, info.stat_step), ctx, "mcb200_stat_begin");
     const auto t0 = std::chrono::steady_clock::now();
@@ -378,15 +381,15 @@ struct Run {
       flushed_ms += ms;
       pair_used[pair] = false;
     };
-    for (int step = 0; step < steps; ++step) {
-      if (step == warm) {  // the timed region starts: device event + engine timing reset
+    for (int step = first; step < first + steps; ++step) {
+      if (step == first + warm) {  // the timed region starts: device event + engine timing reset
         ok(mcb200_sync(ctx), ctx, "mcb200_sync");
         ok(mcb200_set_timing(ctx, 1), ctx, "mcb200_set_timing");
         ok(mcb200_mark(ctx, 0), ctx, "mcb200_mark");
         timed_t0 = std::chrono::steady_clock::now();
         ok(mcb200_particle_steps(ctx, &ps0), ctx, "mcb200_particle_steps");
       }
-      const bool flush = opt.flush_l2_bytes > 0 && step >= warm;
+      const bool flush = opt.flush_l2_bytes > 0 && step >= first + warm;
       const int pair = step % 3;
       if (flush) {
         settle(pair);

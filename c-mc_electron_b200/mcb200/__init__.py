@@ -76,7 +76,8 @@ class DeckInfo(ctypes.Structure):
                                             "flag_surface_impurity", "flag_restart", "n_contacts", "n_planes",
                                             "n_surfaces", "default_electrons", "default_holes")] + \
                [("output_dir", ctypes.c_char * 512), ("prepared", ctypes.c_int), ("dt", ctypes.c_double),
-                ("flag_quantum_correction", ctypes.c_int), ("quantum_start_step", ctypes.c_int)]
+                ("flag_quantum_correction", ctypes.c_int), ("quantum_start_step", ctypes.c_int),
+                ("restart_step", ctypes.c_int)]
 
 
 class QuantumParams(ctypes.Structure):

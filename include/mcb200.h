@@ -493,6 +493,7 @@ typedef struct {
   int prepared;  /* mcb200_deck_prepare has run */
   double dt;     /* dt / time0 once prepared */
   int flag_quantum_correction, quantum_start_step;
+  int restart_step; /* with flag_restart: the first step (mcb200_run_deck) */
 } mcb200_deck_info;
 
 /* On failure *out may still hold a deck whose mcb200_deck_error() says why. */

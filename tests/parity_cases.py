@@ -127,3 +127,34 @@ def run_bulk_parity(n_particles: int = 2000, steps: int = 3, seed: int = 11, fie
         worst["heat_oracle"] = orc.array("p_electron_heat")
     eng.close()
     return worst
+
+
+def make_restart(deck: dict, seed: int = 5, restart_step: int = 7) -> np.ndarray:
+    """A restart file for the deck (par_info_restart's format: i j k |q|_e
+    n_e |q|_h n_h, ended by -1 -1 -1) with seeded counts and charges, a few
+    cells left out and one line off the mesh; input.txt switched to restart
+    from it.  Returns the (nx, ny, nz) of the mesh."""
+    rng = np.random.default_rng(seed)
+    dk = mcb200.Deck(deck["input"])
+    info = dk.info()
+    dk.close()
+    nx, ny, nz = info["nx"], info["ny"], info["nz"]
+    lines = []
+    for i in range(nx):
+        for j in range(ny):
+            for k in range(nz):
+                if rng.random() < 0.1:
+                    continue  # not in the file: keeps the computed count and a zero charge
+                ne, nh = int(rng.integers(0, 6)), int(rng.integers(0, 3))
+                lines.append(f"{i} {j} {k} {rng.uniform(0.5, 2.0) * ne:.17g} {ne} {rng.uniform(0.1, 0.5) * nh:.17g} {nh}")
+    lines.insert(len(lines) // 2, f"{nx + 3} 0 0 1.0 9 1.0 9")  # off the mesh: skipped
+    lines.append("-1 -1 -1")
+    folder = os.path.dirname(deck["input"])
+    with open(os.path.join(folder, "restart.txt"), "w") as f:
+        f.write("\n".join(lines) + "\n")
+    with open(deck["input"]) as f:
+        kv = [l for l in f.read().splitlines() if not l.startswith(("Flag_restart", "restart_step", "restart_filename"))]
+    kv += ["Flag_restart=1", f"restart_step={restart_step}", "restart_filename=restart.txt"]
+    with open(deck["input"], "w") as f:
+        f.write("\n".join(kv) + "\n")
+    return np.array([nx, ny, nz])

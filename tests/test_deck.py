@@ -19,6 +19,7 @@ import pytest
 import mcb200
 from mcb200 import decks
 from oracle_bridge import ORACLE_TABLES, Oracle
+from parity_cases import make_restart
 
 REF_FINFET = "/root/reference/finfet"
 
@@ -83,6 +84,36 @@ def test_contact_bar_with_surfaces_deck():
     with tempfile.TemporaryDirectory() as tmp:
         d = decks.contact_bar(tmp, vd=0.4, electrons=3000, holes=500, surfaces=True)
         _compare(d["input"])
+
+
+def test_restart_deck():
+    """Flag_restart: the restart file's counts replace the computed ones
+    (contact cells included), as the reference's init_particle_data reads
+    them; the refresh targets keep the computed counts."""
+    with tempfile.TemporaryDirectory() as tmp:
+        d = decks.contact_bar(tmp, vd=0.4, electrons=3000, holes=500)
+        make_restart(d)
+        _compare(d["input"])
+        deck = mcb200.Deck(d["input"])
+        assert deck.info()["flag_restart"] == 1 and deck.info()["restart_step"] == 7
+        deck.close()
+
+
+def test_restart_deck_errors():
+    with tempfile.TemporaryDirectory() as tmp:
+        d = decks.contact_bar(tmp, electrons=300)
+        make_restart(d)
+        path = os.path.join(tmp, "restart.txt")
+        with open(path) as f:
+            body = f.read().splitlines()
+        with open(path, "w") as f:
+            f.write("\n".join(body[:-1]) + "\n")  # no -1 line
+        deck = mcb200.Deck(d["input"])
+        eng = mcb200.Engine(table_dir=ORACLE_TABLES, kelvin=deck.info()["temperature"], device=-1)
+        with pytest.raises(mcb200.EngineError, match="restart"):
+            deck.prepare(eng)
+        eng.close()
+        deck.close()
 
 
 def test_bulk_box_deck():

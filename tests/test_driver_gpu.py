@@ -25,7 +25,7 @@ import pytest
 import mcb200
 from mcb200 import decks
 from oracle_bridge import ORACLE_TABLES, Oracle
-from parity_cases import DISC_FIELDS
+from parity_cases import DISC_FIELDS, make_restart
 
 pytestmark = pytest.mark.gpu
 
@@ -166,3 +166,52 @@ def test_run_deck_finfet(precision):
         assert rep["final_particles"] > 0.5 * rep["initial_particles"]
         _check_outputs(data, 29, has_heat=True)
         assert np.isfinite(rep["heat_total"])
+
+
+def test_restart_seed_matches_oracle():
+    """Flag_restart seeding (init_particle_data with
+    read_par_info_for_restart): per cell and carrier type the same number of
+    particles as the reference, each with the same charge, bit for bit --
+    the file's charge shared away from the contacts, the neutral charge in
+    contact cells, nothing in a restarted cell with no carriers."""
+    with tempfile.TemporaryDirectory() as tmp:
+        d = decks.contact_bar(tmp, vd=0.4, electrons=3000, holes=500)
+        make_restart(d)
+        orc = Oracle()
+        orc.init(d["input"], seed=1)
+        ref = orc.particles()
+        deck = mcb200.Deck(d["input"])
+        eng = mcb200.Engine(table_dir=ORACLE_TABLES, kelvin=deck.info()["temperature"], max_particles=1 << 16)
+        deck.apply(eng)
+        deck.seed(eng, 1)
+        deck.close()
+    got = eng.download()
+    eng.close()
+
+    def canon(p):
+        order = np.lexsort((p["charge"], p["k"], p["j"], p["i"], p["type"]))
+        return {k: np.asarray(p[k])[order] for k in ("type", "i", "j", "k", "charge")}
+
+    a, b = canon(got), canon(ref)
+    assert len(a["charge"]) == len(b["charge"]) > 0
+    for k in ("type", "i", "j", "k"):
+        assert np.array_equal(a[k], b[k]), k
+    assert np.array_equal(a["charge"].view(np.uint64), b["charge"].view(np.uint64))
+
+
+def test_run_deck_from_restart():
+    """mcb200_run_deck on a restart deck: seeded from the file, stepped from
+    restart_step (7) on, outputs named by that step count."""
+    with tempfile.TemporaryDirectory() as tmp:
+        d = decks.contact_bar(tmp, vd=0.4, electrons=3000, holes=500)
+        make_restart(d, restart_step=7)
+        with open(d["input"]) as f:
+            kv = [l for l in f.read().splitlines() if not l.startswith("stat_step")]
+        with open(d["input"], "w") as f:
+            f.write("\n".join(kv + ["stat_step=3"]) + "\n")
+        data = os.path.join(tmp, "data")
+        rep = mcb200.run_deck(d["input"], data_dir=data, table_dir=ORACLE_TABLES, max_steps=4, max_heat_steps=0)
+        names = set(os.listdir(data))
+    assert rep["steps_done"] == 4
+    # steps 7..10: the window ends at step 8 (8 % 3 == 2)
+    assert "pot8" in names and "pot2" not in names, sorted(names)
