@@ -1573,11 +1573,12 @@ int mcb200_stat_accumulate(mcb200_ctx *c) {
       // statistic (src/mcmodel.cpp:1184-1199): the Poisson potential and the
       // electrons' (quantum-corrected) one
       launch_add_potential(c->sb.nodes, c->fb.potential, c->sb.pot_sum, s);
-      launch_add_potential(c->sb.nodes, c->qc_on ? c->qc_pot : c->fb.potential, c->sb.qc_pot_sum, s);
+      if (c->qc_set)  // without a quantum set-up the two sums are the same
+        launch_add_potential(c->sb.nodes, c->qc_on ? c->qc_pot : c->fb.potential, c->sb.qc_pot_sum, s);
     }
     ck(cudaGetLastError(), "statistic");
     c->stat_steps += 1;
-    c->launches += 1 + (c->device_set ? 2 : 0);
+    c->launches += 1 + (c->device_set ? (c->qc_set ? 2 : 1) : 0);
     return MCB200_OK;
   } catch (const std::exception &e) {
     return fail(c, MCB200_ERR_CUDA, e.what());
@@ -1606,8 +1607,8 @@ int mcb200_stat_get(mcb200_ctx *c, const char *name, double *out, size_t n) {
     }
     if (nm == "pot_sum" || nm == "qc_pot_sum") {
       if (n < nodes) return fail(c, MCB200_ERR_CAPACITY, "output too small");
-      ck(cudaMemcpy(out, nm == "pot_sum" ? c->sb.pot_sum : c->sb.qc_pot_sum, nodes * 8, cudaMemcpyDeviceToHost),
-         "copy");
+      const bool qc = nm == "qc_pot_sum" && c->qc_set;
+      ck(cudaMemcpy(out, qc ? c->sb.qc_pot_sum : c->sb.pot_sum, nodes * 8, cudaMemcpyDeviceToHost), "copy");
       return MCB200_OK;
     }
     // electron_* / hole_*: qvx, qvy, qvz, q, qe per node
