@@ -213,9 +213,7 @@ def engine_arm(args, rank: int, world: int, device: int):
     peak, peak_kind = measured_peaks()
     value = {}
     for p, r in runs.items():
-        ps = dist_sum(r["timed_particle_steps"], world)
-        ms = dist_max(r["timed_device_ms"], world)
-        value[p] = ps / (ms * 1e-3)
+        value[p], _ = aggregate_throughput(r["timed_particle_steps"], r["timed_device_ms"], world)
 
     def roof(r, p):
         launches = max(r["timed_flight_launches"], 1)
@@ -457,8 +455,13 @@ def reference_arm(args, rank: int, world: int):
 _PG = None
 
 
+_ON_GPU = False
+
+
 def dist_init():
-    global _PG
+    """One process per GPU (torchrun's RANK / WORLD_SIZE / LOCAL_RANK):
+    NCCL between GPUs, gloo where there is no GPU (the CPU tests)."""
+    global _PG, _ON_GPU
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -468,10 +471,20 @@ def dist_init():
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        _ON_GPU = torch.cuda.is_available()
+        if _ON_GPU:
+            torch.cuda.set_device(local)
+        dist.init_process_group("nccl" if _ON_GPU else "gloo", timeout=datetime.timedelta(seconds=300))
         _PG = dist
     return rank, world, local
+
+
+def aggregate_throughput(particle_steps: float, device_ms: float, world: int):
+    """Whole-job throughput of the replicas: every rank's particle-steps over
+    the slowest rank's device time.  Returns (particle-steps/s, max ms)."""
+    total = dist_sum(float(particle_steps), world)
+    ms = dist_max(float(device_ms), world)
+    return total / (ms * 1e-3), ms
 
 
 def dist_barrier(world):
@@ -484,7 +497,7 @@ def _reduce(v: float, world: int, op):
         return v
     import torch
 
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    t = torch.tensor([v], dtype=torch.float64, device="cuda" if _ON_GPU else "cpu")
     _PG.all_reduce(t, op=op)
     return float(t.item())
 

@@ -29,6 +29,11 @@ namespace mcb200 {
 #endif
 template <typename R>
 constexpr int kFlightBlocks = sizeof(R) == 4 ? MCB200_FLIGHT_BLOCKS_F32 : MCB200_FLIGHT_BLOCKS_F64;
+// Threads per block of the flight kernels (a tuning define like the above).
+#ifndef MCB200_FLIGHT_THREADS
+#define MCB200_FLIGHT_THREADS 256
+#endif
+constexpr int kFlightThreads = MCB200_FLIGHT_THREADS;
 
 constexpr uint32_t kMetaDead = 1u << 16;
 constexpr uint32_t kMetaUnfinished = 1u << 17;
@@ -156,7 +161,7 @@ __device__ __forceinline__ void fly_interleaved(const FlightCtxT<R> &F, const Sy
 }
 
 template <typename R>
-__global__ void __launch_bounds__(256, kFlightBlocks<R>) flight_kernel(FlightCtxT<R> F, DevParticlesT<R> P,
+__global__ void __launch_bounds__(kFlightThreads, kFlightBlocks<R>) flight_kernel(FlightCtxT<R> F, DevParticlesT<R> P,
                                                                        DevCount n, unsigned int *ticket) {
   const int count = n.get();
   if (count == 0) return;
@@ -168,7 +173,7 @@ __global__ void __launch_bounds__(256, kFlightBlocks<R>) flight_kernel(FlightCtx
 // Copies made during the previous pass (buffer `in`) fly the rest of their
 // step; copies they make go to `F.C`.
 template <typename R>
-__global__ void __launch_bounds__(256, kFlightBlocks<R>) child_flight_kernel(FlightCtxT<R> F, DevChildrenT<R> in,
+__global__ void __launch_bounds__(kFlightThreads, kFlightBlocks<R>) child_flight_kernel(FlightCtxT<R> F, DevChildrenT<R> in,
                                                               unsigned int *ticket) {
   const int count = min((int)*in.count, in.capacity);
   if (count == 0) return;
@@ -226,7 +231,7 @@ constexpr size_t batch_smem_bytes(int ninst) {
 // simulation k's step number (device memory, advanced between steps).
 // Simulations whose bit in `members` is clear contribute no particles.
 template <typename R, bool kChild>
-__global__ void __launch_bounds__(256, kFlightBlocks<R>) batch_flight_kernel(const __grid_constant__ FlightCtxT<R> F,
+__global__ void __launch_bounds__(kFlightThreads, kFlightBlocks<R>) batch_flight_kernel(const __grid_constant__ FlightCtxT<R> F,
                                                                              const BatchInstT<R> *inst,
                                                                              int ninst, uint64_t members,
                                                                              const uint32_t *steps,
@@ -535,12 +540,12 @@ int flight_grid(int n, int block, int sm_count) {
 template <typename R>
 void launch_flight(const FlightCtxT<R> &F, const DevParticlesT<R> &P, DevCount n, unsigned int *ticket, int sm_count,
                    cudaStream_t s) {
-  flight_kernel<R><<<flight_grid<R>(n.max, 256, sm_count), 256, 0, s>>>(F, P, n, ticket);
+  flight_kernel<R><<<flight_grid<R>(n.max, kFlightThreads, sm_count), kFlightThreads, 0, s>>>(F, P, n, ticket);
 }
 template <typename R>
 void launch_child_flight(const FlightCtxT<R> &F, const DevChildrenT<R> &in, int n_hint, unsigned int *ticket,
                          int sm_count, cudaStream_t s) {
-  child_flight_kernel<R><<<flight_grid<R>(n_hint, 256, sm_count), 256, 0, s>>>(F, in, ticket);
+  child_flight_kernel<R><<<flight_grid<R>(n_hint, kFlightThreads, sm_count), kFlightThreads, 0, s>>>(F, in, ticket);
 }
 template <typename R>
 int launch_batch_flight(const FlightCtxT<R> &F, const BatchInstT<R> *inst, int ninst, uint64_t members,
@@ -557,10 +562,11 @@ int launch_batch_flight(const FlightCtxT<R> &F, const BatchInstT<R> *inst, int n
     opted[child ? 1 : 0] = true;
   }
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, smem) != cudaSuccess || per_sm < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kFlightThreads, smem) != cudaSuccess ||
+      per_sm < 1)
     return 1;
   if (blocks_per_sm > 0) per_sm = std::min(per_sm, blocks_per_sm);
-  kernel<<<per_sm * sm_count, 256, smem, s>>>(F, inst, ninst, members, steps, ticket);
+  kernel<<<per_sm * sm_count, kFlightThreads, smem, s>>>(F, inst, ninst, members, steps, ticket);
   return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 void launch_cell_records32(const DevTables &T, const DevMesh &M, float4 *out, int cells, cudaStream_t s) {
