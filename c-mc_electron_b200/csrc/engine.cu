@@ -1,5 +1,6 @@
 // engine.cu -- context, device-table upload and the C ABI of include/mcb200.h.
 #include <algorithm>
+#include <list>
 #include <cmath>
 #include <cstring>
 #include <stdexcept>
@@ -328,6 +329,47 @@ int grid_for(const mcb200_ctx *c, size_t n, int block) {
   const size_t want = (n + block - 1) / block;
   const size_t cap = (size_t)c->sm_count * (size_t)c->grid_per_sm;
   return (int)std::max<size_t>(1, std::min(want, cap));
+}
+
+// MgHierarchy::build for the node grid, stencil and Dirichlet pattern, from
+// a small process-wide cache: the hierarchy depends on nothing else, so the
+// contexts of one device shape at other biases (a bias sweep, the members of
+// a batch, served requests) share one host build.  Entries hold their
+// inputs and match them exactly.  Null when the mesh does not coarsen.
+std::shared_ptr<const MgHierarchy> cached_hierarchy(int px, int py, int pz, const std::vector<double> &X,
+                                                    const std::vector<double> &Y, const std::vector<double> &Z,
+                                                    const std::vector<double> &stencil,
+                                                    const std::vector<uint8_t> &dirichlet) {
+  struct Entry {
+    int px, py, pz;
+    std::vector<double> X, Y, Z, stencil;
+    std::vector<uint8_t> dirichlet;
+    std::shared_ptr<const MgHierarchy> h;
+  };
+  static std::mutex mutex;
+  static std::list<Entry> cache;  // most recent first
+  constexpr size_t kEntries = 4;
+  {
+    std::lock_guard<std::mutex> lock(mutex);
+    for (auto it = cache.begin(); it != cache.end(); ++it)
+      if (it->px == px && it->py == py && it->pz == pz && it->X == X && it->Y == Y && it->Z == Z &&
+          it->dirichlet == dirichlet && it->stencil == stencil) {
+        cache.splice(cache.begin(), cache, it);
+        return cache.front().h;
+      }
+  }
+  std::shared_ptr<const MgHierarchy> h;
+  try {
+    h = std::make_shared<const MgHierarchy>(MgHierarchy::build(px, py, pz, X, Y, Z, stencil, dirichlet));
+  } catch (const std::logic_error &) {
+    return nullptr;
+  } catch (const std::runtime_error &) {
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(mutex);
+  cache.push_front(Entry{px, py, pz, X, Y, Z, stencil, dirichlet, h});
+  if (cache.size() > kEntries) cache.pop_back();
+  return h;
 }
 
 void free_mesh(mcb200_ctx *c) {
@@ -1194,16 +1236,10 @@ int mcb200_set_device(mcb200_ctx *c, const int32_t *material, const double *dono
       for (int i = 0; i < m.nx; ++i) X[i + 1] = X[i] + dx[i];
       for (int j = 0; j < m.ny; ++j) Y[j + 1] = Y[j] + dy[j];
       for (int k = 0; k < m.nz; ++k) Z[k + 1] = Z[k] + dz[k];
-      bool built = false;
-      MgHierarchy h;
-      try {
-        h = MgHierarchy::build(m.nx + 1, m.ny + 1, m.nz + 1, X, Y, Z, s.stencil, s.dirichlet);
-        built = true;
-      } catch (const std::logic_error &) {  // a mesh that does not coarsen: Jacobi preconditioning
-      } catch (const std::runtime_error &) {
-      }
-      if (built) {
-        c->mg = mg_upload(h, c->mesh_owned);
+      const std::shared_ptr<const MgHierarchy> h =
+          cached_hierarchy(m.nx + 1, m.ny + 1, m.nz + 1, X, Y, Z, s.stencil, s.dirichlet);
+      if (h) {  // (none: a mesh that does not coarsen, Jacobi preconditioning)
+        c->mg = mg_upload(*h, c->mesh_owned);
         f.mg = &c->mg;
       }
     }

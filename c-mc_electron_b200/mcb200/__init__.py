@@ -654,7 +654,7 @@ class Server:
     """Bias-point requests served by continuous batching (mcb200_server_*)."""
 
     def __init__(self, table_dir: str = DEFAULT_TABLE_DIR, device: int = 0, precision: int = FLIGHT_FP32,
-                 hbm_budget_bytes: int = 0, max_slots: int = 64, quantum_steps: int = 50, use_graphs: bool = True,
+                 hbm_budget_bytes: int = 0, max_slots: int = 64, quantum_steps: int = 50, use_graphs: bool = False,
                  kelvin: float = 300.0):
         self._lib = lib()
         self._s = ctypes.c_void_p()

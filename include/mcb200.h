@@ -615,7 +615,9 @@ typedef struct {
   size_t hbm_budget_bytes;   /* device memory for requests and warm-start entries (0: 160 GB) */
   int max_slots;             /* concurrent requests (0 or > 64: 64) */
   int quantum_steps;         /* timesteps per round = steps per Ids window (0: 50) */
-  int use_graphs;            /* replay each round's steps from CUDA graphs */
+  int use_graphs;            /* replay each round's steps from CUDA graphs (measured slower here: a
+                                membership change re-captures every graph, and a batched step is
+                                GPU-bound, so replays save little host time; off in the Python API) */
 } mcb200_server_options;
 typedef struct {
   const char *input_path;    /* the deck's input.txt (copied at submission) */
