@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -53,25 +54,61 @@ T *dupload(const std::vector<T> &v, std::vector<void *> &owned) {
   return p;
 }
 
+// Arrays carved from one allocation, each on a 256-byte boundary: a store
+// of a dozen arrays costs one cudaMalloc (a context's set-up otherwise
+// spent tens of milliseconds in allocation calls).
+class Carve {
+ public:
+  template <typename T>
+  void add(T *&p, size_t n) {
+    parts_.push_back({[&p](char *a) { p = reinterpret_cast<T *>(a); }, std::max<size_t>(n, 1) * sizeof(T)});
+  }
+  void commit(std::vector<void *> &owned) {
+    size_t total = 0;
+    for (const auto &q : parts_) total += round_up(q.bytes);
+    void *base = nullptr;
+    ck(cudaMalloc(&base, total), "cudaMalloc");
+    owned.push_back(base);
+    char *cur = static_cast<char *>(base);
+    for (const auto &q : parts_) {
+      q.set(cur);
+      cur += round_up(q.bytes);
+    }
+    parts_.clear();
+  }
+
+ private:
+  struct Part {
+    std::function<void(char *)> set;
+    size_t bytes;
+  };
+  static size_t round_up(size_t b) { return (b + 255) & ~size_t(255); }
+  std::vector<Part> parts_;
+};
+
 template <typename R>
 void alloc_particles(DevParticlesT<R> &d, size_t cap, std::vector<void *> &owned) {
-  d.x = dalloc<R>(cap, owned); d.y = dalloc<R>(cap, owned); d.z = dalloc<R>(cap, owned);
-  d.kx = dalloc<R>(cap, owned); d.ky = dalloc<R>(cap, owned); d.kz = dalloc<R>(cap, owned);
-  d.energy = dalloc<double>(cap, owned); d.charge = dalloc<double>(cap, owned);
-  d.cell = dalloc<uint32_t>(cap, owned); d.itet = dalloc<int32_t>(cap, owned);
-  d.meta = dalloc<uint32_t>(cap, owned); d.uid = dalloc<uint32_t>(cap, owned);
+  Carve k;
+  k.add(d.x, cap); k.add(d.y, cap); k.add(d.z, cap);
+  k.add(d.kx, cap); k.add(d.ky, cap); k.add(d.kz, cap);
+  k.add(d.energy, cap); k.add(d.charge, cap);
+  k.add(d.cell, cap); k.add(d.itet, cap);
+  k.add(d.meta, cap); k.add(d.uid, cap);
+  k.commit(owned);
 }
 
 template <typename R>
 void alloc_children(DevChildrenT<R> &d, int cap, std::vector<void *> &owned) {
-  d.x = dalloc<R>(cap, owned); d.y = dalloc<R>(cap, owned); d.z = dalloc<R>(cap, owned);
-  d.kx = dalloc<R>(cap, owned); d.ky = dalloc<R>(cap, owned); d.kz = dalloc<R>(cap, owned);
-  d.energy = dalloc<double>(cap, owned); d.charge = dalloc<double>(cap, owned);
-  d.left_time = dalloc<double>(cap, owned);
-  d.cell = dalloc<uint32_t>(cap, owned); d.itet = dalloc<int32_t>(cap, owned);
-  d.meta = dalloc<uint32_t>(cap, owned);
-  d.parent_uid = dalloc<uint32_t>(cap, owned); d.sub = dalloc<uint32_t>(cap, owned);
-  d.count = dalloc<unsigned int>(1, owned);
+  Carve k;
+  k.add(d.x, cap); k.add(d.y, cap); k.add(d.z, cap);
+  k.add(d.kx, cap); k.add(d.ky, cap); k.add(d.kz, cap);
+  k.add(d.energy, cap); k.add(d.charge, cap);
+  k.add(d.left_time, cap);
+  k.add(d.cell, cap); k.add(d.itet, cap);
+  k.add(d.meta, cap);
+  k.add(d.parent_uid, cap); k.add(d.sub, cap);
+  k.add(d.count, 1);
+  k.commit(owned);
   d.capacity = cap;
 }
 
