@@ -545,7 +545,10 @@ void launch_flight(const FlightCtxT<R> &F, const DevParticlesT<R> &P, DevCount n
 template <typename R>
 void launch_child_flight(const FlightCtxT<R> &F, const DevChildrenT<R> &in, int n_hint, unsigned int *ticket,
                          int sm_count, cudaStream_t s) {
-  child_flight_kernel<R><<<flight_grid<R>(n_hint, kFlightThreads, sm_count), kFlightThreads, 0, s>>>(F, in, ticket);
+  // One block per SM: a step's copies are few (their lanes refill from the
+  // same counter however many there are), and most generations are empty.
+  const int n = (int)std::min<long long>(n_hint, (long long)sm_count * kFlightThreads);
+  child_flight_kernel<R><<<flight_grid<R>(n, kFlightThreads, sm_count), kFlightThreads, 0, s>>>(F, in, ticket);
 }
 template <typename R>
 int launch_batch_flight(const FlightCtxT<R> &F, const BatchInstT<R> *inst, int ninst, uint64_t members,
