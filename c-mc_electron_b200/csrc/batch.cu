@@ -469,6 +469,12 @@ int mcb200_batch_step(mcb200_batch *b) {
 
 int mcb200_batch_run(mcb200_batch *b, int steps) {
   if (!b || steps < 0) return MCB200_ERR_ARG;
+  try {  // pending statistics joined outside any capture
+    ck(cudaSetDevice(b->device), "cudaSetDevice");
+    for (mcb200_ctx *c : b->m) join_stat(c);
+  } catch (const std::exception &e) {
+    return bfail(b, MCB200_ERR_CUDA, e.what());
+  }
   for (size_t k = 0; k < b->m.size(); ++k) {
     mcb200_ctx *c = b->m[k];
     if (!c->fields_set && !(b->cfg[k].self_consistent && c->device_set))

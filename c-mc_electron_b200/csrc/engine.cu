@@ -398,6 +398,12 @@ void upload_refresh_targets(mcb200_ctx *c, const int32_t *desired_e, const int32
   ck(cudaStreamWaitEvent(c->stream, c->ev_upload, 0), "wait");
 }
 
+void join_stat(mcb200_ctx *c) {
+  if (!c->stat_pending) return;
+  ck(cudaStreamWaitEvent(c->stream, c->ev_stat, 0), "wait");
+  c->stat_pending = false;
+}
+
 // MultipleRefresh scratch for the mesh's cells, allocated with the cells
 // (an allocation at the first refresh would stall a running batch).
 void mr_scratch(mcb200_ctx *c) {
@@ -484,6 +490,9 @@ void init_device_context(mcb200_ctx *c, size_t max_particles) {
   ck(cudaStreamCreateWithFlags(&c->upload, cudaStreamNonBlocking), "cudaStreamCreate");
   ck(cudaEventCreateWithFlags(&c->ev_upload, cudaEventDisableTiming), "cudaEventCreate");
   ck(cudaEventCreateWithFlags(&c->ev_mr_used, cudaEventDisableTiming), "cudaEventCreate");
+  ck(cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking), "cudaStreamCreate");
+  ck(cudaEventCreateWithFlags(&c->ev_aux_in, cudaEventDisableTiming), "cudaEventCreate");
+  ck(cudaEventCreateWithFlags(&c->ev_stat, cudaEventDisableTiming), "cudaEventCreate");
   ck(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device), "device attribute");
   c->capacity = max_particles;
   c->child_cap = (int)std::min<size_t>(std::max<size_t>(max_particles / 8, 4096), 1u << 22);
@@ -804,6 +813,7 @@ int mcb200_upload_particles(mcb200_ctx *c, size_t n, const mcb200_particles *p) 
   if (c->device < 0) return fail(c, MCB200_ERR_STATE, "host-only context");
   try {
     ck(cudaSetDevice(c->device), "cudaSetDevice");
+    join_stat(c);
     std::vector<uint32_t> cell(n), meta(n);
     uint32_t maxuid = 0;
     for (size_t q = 0; q < n; ++q) {
@@ -887,6 +897,7 @@ int mcb200_copy_ensemble(mcb200_ctx *dst, mcb200_ctx *src) {
     return fail(dst, MCB200_ERR_ARG, "mcb200_copy_ensemble: contexts differ in device, precision or mesh");
   try {
     ck(cudaSetDevice(dst->device), "cudaSetDevice");
+    join_stat(dst);
     pull_counts(src);
     ck(cudaStreamSynchronize(dst->stream), "sync");
     if (src->n > dst->capacity) return fail(dst, MCB200_ERR_CAPACITY, "mcb200_copy_ensemble: too many particles");
@@ -944,6 +955,7 @@ int mcb200_seed_particles(mcb200_ctx *c, size_t n, const int32_t *cell_of, const
   if (!c->mesh_set || !c->cells_set) return fail(c, MCB200_ERR_STATE, "mcb200_seed_particles needs mesh and cells");
   try {
     ck(cudaSetDevice(c->device), "cudaSetDevice");
+    join_stat(c);
     pull_counts(c);
   } catch (const CapacityError &e) {
     return fail(c, MCB200_ERR_CAPACITY, e.what());
@@ -1101,6 +1113,11 @@ int mcb200_get_timing(const mcb200_ctx *cc, double *out, int n) {
 
 int mcb200_sync(mcb200_ctx *c) {
   if (!c) return MCB200_ERR_ARG;
+  if (c->stat_pending) {
+    cudaSetDevice(c->device);
+    cudaStreamWaitEvent(c->stream, c->ev_stat, 0);
+    c->stat_pending = false;
+  }
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return fail(c, MCB200_ERR_CUDA, cudaGetErrorString(e));
   try {
@@ -1366,6 +1383,7 @@ int mcb200_multiple_refresh(mcb200_ctx *c, const int32_t *desired_e, const int32
   if (!c->mesh_set) return fail(c, MCB200_ERR_STATE, "mcb200_multiple_refresh before mcb200_set_mesh");
   try {
     ck(cudaSetDevice(c->device), "cudaSetDevice");
+    join_stat(c);
     cudaStream_t s = c->stream;
     const int cells = c->ncells;
     size_t want = 0;
@@ -1559,6 +1577,7 @@ int mcb200_stat_begin(mcb200_ctx *c, int window_steps) {
   if (!c->mesh_set) return fail(c, MCB200_ERR_STATE, "mcb200_stat_begin before mcb200_set_mesh");
   try {
     ck(cudaSetDevice(c->device), "cudaSetDevice");
+    join_stat(c);
     cudaStream_t s = c->stream;
     const int grid = grid_for(c, c->capacity, 256);
     const DevCount n{c->dev_counts, nullptr, (int)c->capacity};
@@ -1601,10 +1620,18 @@ int mcb200_stat_accumulate(mcb200_ctx *c) {
     cudaStream_t s = c->stream;
     const int grid = grid_for(c, c->capacity, 256);
     const DevCount n{c->dev_counts, nullptr, (int)c->capacity};
+    // the particle sums only read the store: they run on the aux stream
+    // beside the deposition / solve / surface rates that follow, and the
+    // next change of the store waits for them (join_stat)
+    join_stat(c);
+    ck(cudaEventRecord(c->ev_aux_in, s), "event");
+    ck(cudaStreamWaitEvent(c->aux, c->ev_aux_in, 0), "wait");
     if (c->precision == MCB200_FLIGHT_FP32)
-      launch_statistic(store<float>(c, c->cur), n, c->mesh, c->ts->dt, c->ss, c->sb, grid, s);
+      launch_statistic(store<float>(c, c->cur), n, c->mesh, c->ts->dt, c->ss, c->sb, grid, c->aux);
     else
-      launch_statistic(store<double>(c, c->cur), n, c->mesh, c->ts->dt, c->ss, c->sb, grid, s);
+      launch_statistic(store<double>(c, c->cur), n, c->mesh, c->ts->dt, c->ss, c->sb, grid, c->aux);
+    ck(cudaEventRecord(c->ev_stat, c->aux), "event");
+    c->stat_pending = true;
     if (c->device_set) {
       // statistic (src/mcmodel.cpp:1184-1199): the Poisson potential and the
       // electrons' (quantum-corrected) one
@@ -1628,6 +1655,7 @@ int mcb200_stat_get(mcb200_ctx *c, const char *name, double *out, size_t n) {
   const size_t nodes = (size_t)c->sb.nodes, cells = (size_t)c->ncells;
   try {
     ck(cudaSetDevice(c->device), "cudaSetDevice");
+    join_stat(c);
     ck(cudaStreamSynchronize(c->stream), "sync");
     if (nm == "steps") {
       if (n < 1) return fail(c, MCB200_ERR_CAPACITY, "output too small");
@@ -1775,6 +1803,7 @@ void surface_rates_enqueue(mcb200_ctx *c, cudaStream_t s) {
 template <typename R>
 void step_prepare(mcb200_ctx *c) {
   cudaStream_t s = c->stream;
+  join_stat(c);  // the flights change the store the statistics read
   ck(cudaMemsetAsync(c->tickets, 0, sizeof(unsigned int) * (1 + mcb200_ctx::kGenerations), s), "memset");
   if constexpr (sizeof(R) == 4) {  // FP32 flight reads the fields as per-cell float records
     launch_cell_records32(c->ts->dt, c->mesh, c->cell32, c->ncells, s);

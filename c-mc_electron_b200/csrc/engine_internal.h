@@ -161,6 +161,11 @@ struct mcb200_ctx {
   // targets from pageable memory); ev_mr_used: the last refresh's reads
   cudaStream_t upload = nullptr;
   cudaEvent_t ev_upload = nullptr, ev_mr_used = nullptr;
+  // the particle statistics run on `aux` beside the deposition and solve
+  // (they only read the store); stat_pending until the stream has joined them
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_aux_in = nullptr, ev_stat = nullptr;
+  bool stat_pending = false;
   std::vector<void *> owned;   // every cudaMalloc of the context
   std::vector<void *> mesh_owned;
   std::shared_ptr<TableSet> ts;  // band tables (host and device), shared by contexts made alike
@@ -253,6 +258,10 @@ struct mcb200_ctx {
     if (flush_buf) cudaFree(flush_buf);
     if (h_pinned) cudaFreeHost(h_pinned);
     if (h_scratch) cudaFreeHost(h_scratch);
+    if (aux) cudaStreamSynchronize(aux);
+    if (ev_aux_in) cudaEventDestroy(ev_aux_in);
+    if (ev_stat) cudaEventDestroy(ev_stat);
+    if (aux) cudaStreamDestroy(aux);
     if (ev_upload) cudaEventDestroy(ev_upload);
     if (ev_mr_used) cudaEventDestroy(ev_mr_used);
     if (upload) cudaStreamDestroy(upload);
@@ -282,6 +291,10 @@ int fail(mcb200_ctx *c, int code, const std::string &msg);
 // have changed them); throws CapacityError once for a store-full flag.
 void pull_counts(mcb200_ctx *c);
 void push_counts(mcb200_ctx *c);
+// The context stream waits for pending particle statistics (before anything
+// that changes the particle store, resets or reads the statistics).  Never
+// inside a stream capture: the batch joins its members first.
+void join_stat(mcb200_ctx *c);
 int grid_for(const mcb200_ctx *c, size_t n, int block);
 void poisson_enqueue(mcb200_ctx *c, cudaStream_t s, double rel_tol, int max_iter, int *iterations,
                      double *rel_residual);
