@@ -63,35 +63,37 @@ struct Decision {
   double tot;    // their total charge
 };
 
-template <typename R>
-__device__ void order_cell_by_uid(DevParticlesT<R> P, int b, int e) {
-  for (int i = b + 1; i < e; ++i) {  // insertion sort on uid, moving whole particles
-    const uint32_t u = P.uid[i];
-    const R x = P.x[i], y = P.y[i], z = P.z[i], kx = P.kx[i], ky = P.ky[i], kz = P.kz[i];
-    const double en = P.energy[i], ch = P.charge[i];
-    const uint32_t cl = P.cell[i], me = P.meta[i];
-    const int32_t it = P.itet[i];
-    int j = i - 1;
-    while (j >= b && P.uid[j] > u) {
-      P.uid[j + 1] = P.uid[j]; P.x[j + 1] = P.x[j]; P.y[j + 1] = P.y[j]; P.z[j + 1] = P.z[j];
-      P.kx[j + 1] = P.kx[j]; P.ky[j + 1] = P.ky[j]; P.kz[j + 1] = P.kz[j];
-      P.energy[j + 1] = P.energy[j]; P.charge[j + 1] = P.charge[j];
-      P.cell[j + 1] = P.cell[j]; P.meta[j + 1] = P.meta[j]; P.itet[j + 1] = P.itet[j];
-      --j;
+// The cell's particles [b, e) in uid order, as keys uid << 32 | index in
+// order[b, e) (shell sort, Ciura's gaps): the refresh visits particles in
+// uid order without moving the store.
+__device__ void order_cell_by_uid(const uint32_t *uid, unsigned long long *order, int b, int e) {
+  const int n = e - b;
+  unsigned long long *a = order + b;
+  for (int i = 0; i < n; ++i) a[i] = ((unsigned long long)uid[b + i] << 32) | (unsigned)(b + i);
+  const int gaps[10] = {3937, 1750, 701, 301, 132, 57, 23, 10, 4, 1};
+  for (int g : gaps) {
+    if (g >= n) continue;
+    for (int i = g; i < n; ++i) {
+      const unsigned long long t = a[i];
+      int j = i;
+      while (j >= g && a[j - g] > t) {
+        a[j] = a[j - g];
+        j -= g;
+      }
+      a[j] = t;
     }
-    P.uid[j + 1] = u; P.x[j + 1] = x; P.y[j + 1] = y; P.z[j + 1] = z;
-    P.kx[j + 1] = kx; P.ky[j + 1] = ky; P.kz[j + 1] = kz;
-    P.energy[j + 1] = en; P.charge[j + 1] = ch;
-    P.cell[j + 1] = cl; P.meta[j + 1] = me; P.itet[j + 1] = it;
   }
 }
+__device__ __forceinline__ int nth(const unsigned long long *order, int k) { return (int)(order[k] & 0xffffffffull); }
 
 // gen_new_par_mr's test (src/MultipleRefresh.cpp:18-33) for one carrier type.
 template <typename R>
-__device__ Decision decide(const DevParticlesT<R> &P, int b, int e, int type, int new_num, const RefreshParams &r) {
+__device__ Decision decide(const DevParticlesT<R> &P, const unsigned long long *order, int b, int e, int type,
+                           int new_num, const RefreshParams &r) {
   Decision d{1, 0, 0.0};
   double tmp = 0;
-  for (int i = b; i < e; ++i) {
+  for (int k = b; k < e; ++k) {
+    const int i = nth(order, k);
     if (((P.meta[i] >> 8) & 255) != (uint32_t)type || fabs(P.charge[i]) < r.pckill) continue;
     d.old_num++;
     d.tot += P.charge[i];
@@ -108,15 +110,15 @@ __device__ Decision decide(const DevParticlesT<R> &P, int b, int e, int type, in
 template <typename R>
 __global__ void refresh_count_kernel(DevParticlesT<R> P, const unsigned int *cell_end, const unsigned int *cell_count,
                                      int cells, const int *desired_e, const int *desired_h, RefreshParams r,
-                                     unsigned int *out_count, unsigned int *new_count) {
+                                     unsigned long long *order, unsigned int *out_count, unsigned int *new_count) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= cells) return;
   const int e = (int)cell_end[c], b = e - (int)cell_count[c];
-  order_cell_by_uid(P, b, e);
+  order_cell_by_uid(P.uid, order, b, e);
   unsigned int total = 0, fresh = 0;
   for (int t = 0; t < 2; ++t) {
     const int want = t == 0 ? desired_e[c] : desired_h[c];
-    const Decision d = decide(P, b, e, t, want, r);
+    const Decision d = decide(P, order, b, e, t, want, r);
     if (d.keep) total += d.old_num;
     else {
       total += want;
@@ -130,8 +132,9 @@ __global__ void refresh_count_kernel(DevParticlesT<R> P, const unsigned int *cel
 template <typename R>
 __global__ void refresh_emit_kernel(DevParticlesT<R> P, const unsigned int *cell_end, const unsigned int *cell_count,
                                     int cells, const int *desired_e, const int *desired_h, RefreshParams r,
-                                    const unsigned int *out_offset, const unsigned int *uid_offset,
-                                    const unsigned int *uid0p, DevParticlesT<R> dst, unsigned long long *mr_gen) {
+                                    const unsigned long long *order, const unsigned int *out_offset,
+                                    const unsigned int *uid_offset, const unsigned int *uid0p, DevParticlesT<R> dst,
+                                    unsigned long long *mr_gen) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= cells) return;
   const int e = (int)cell_end[c], b = e - (int)cell_count[c];
@@ -147,10 +150,12 @@ __global__ void refresh_emit_kernel(DevParticlesT<R> P, const unsigned int *cell
   int produced = 0;
   for (int t = 0; t < 2; ++t) {
     const int want = t == 0 ? desired_e[c] : desired_h[c];
-    const Decision d = decide(P, b, e, t, want, r);
+    const Decision d = decide(P, order, b, e, t, want, r);
     if (d.keep) {
-      for (int i = b; i < e; ++i)
+      for (int k = b; k < e; ++k) {
+        const int i = nth(order, k);
         if (((P.meta[i] >> 8) & 255) == (uint32_t)t && fabs(P.charge[i]) >= r.pckill) copy(i, o++);
+      }
       produced += d.old_num;
       continue;
     }
@@ -161,7 +166,8 @@ __global__ void refresh_emit_kernel(DevParticlesT<R> P, const unsigned int *cell
       const double s = mcb200_uniform(r.seed, (uint32_t)c, r.step, kRefreshSub + t, (uint32_t)q) * fabs(d.tot);
       double w = 0;
       int pick = -1, last = -1;
-      for (int i = b; i < e; ++i) {
+      for (int k = b; k < e; ++k) {
+        const int i = nth(order, k);
         if (((P.meta[i] >> 8) & 255) != (uint32_t)t || fabs(P.charge[i]) < r.pckill) continue;
         last = i;
         w += fabs(P.charge[i]);
@@ -190,27 +196,30 @@ void launch_surface_rates(int cells, const SurfaceRateParams &q, const double *f
 template <typename R>
 void launch_refresh_count(const DevParticlesT<R> &P, const unsigned int *cell_end, const unsigned int *cell_count,
                           int cells, const int *desired_e, const int *desired_h, const RefreshParams &r,
-                          unsigned int *out_count, unsigned int *new_count, cudaStream_t s) {
+                          unsigned long long *order, unsigned int *out_count, unsigned int *new_count,
+                          cudaStream_t s) {
   refresh_count_kernel<R><<<(cells + 127) / 128, 128, 0, s>>>(P, cell_end, cell_count, cells, desired_e, desired_h, r,
-                                                           out_count, new_count);
+                                                           order, out_count, new_count);
 }
 template <typename R>
 void launch_refresh_emit(const DevParticlesT<R> &P, const unsigned int *cell_end, const unsigned int *cell_count,
                          int cells, const int *desired_e, const int *desired_h, const RefreshParams &r,
-                         const unsigned int *out_offset, const unsigned int *uid_offset, const unsigned int *uid0,
-                         const DevParticlesT<R> &dst, unsigned long long *mr_gen, cudaStream_t s) {
+                         const unsigned long long *order, const unsigned int *out_offset,
+                         const unsigned int *uid_offset, const unsigned int *uid0, const DevParticlesT<R> &dst,
+                         unsigned long long *mr_gen, cudaStream_t s) {
   refresh_emit_kernel<R><<<(cells + 127) / 128, 128, 0, s>>>(P, cell_end, cell_count, cells, desired_e, desired_h, r,
-                                                          out_offset, uid_offset, uid0, dst, mr_gen);
+                                                          order, out_offset, uid_offset, uid0, dst, mr_gen);
 }
 
 #define MCB200_INSTANTIATE(R)                                                                                 \
   template void launch_refresh_count<R>(const DevParticlesT<R> &, const unsigned int *, const unsigned int *, \
-                                        int, const int *, const int *, const RefreshParams &, unsigned int *, \
-                                        unsigned int *, cudaStream_t);                                        \
+                                        int, const int *, const int *, const RefreshParams &,                 \
+                                        unsigned long long *, unsigned int *, unsigned int *, cudaStream_t);  \
   template void launch_refresh_emit<R>(const DevParticlesT<R> &, const unsigned int *, const unsigned int *,  \
                                        int, const int *, const int *, const RefreshParams &,                 \
-                                       const unsigned int *, const unsigned int *, const unsigned int *,                 \
-                                       const DevParticlesT<R> &, unsigned long long *, cudaStream_t);
+                                       const unsigned long long *, const unsigned int *, const unsigned int *, \
+                                       const unsigned int *, const DevParticlesT<R> &, unsigned long long *,  \
+                                       cudaStream_t);
 MCB200_INSTANTIATE(double)
 MCB200_INSTANTIATE(float)
 #undef MCB200_INSTANTIATE

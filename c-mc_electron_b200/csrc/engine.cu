@@ -419,6 +419,7 @@ void mr_scratch(mcb200_ctx *c) {
   w.tiles = dalloc<unsigned int>((cells + 1023) / 1024 + 1, c->mesh_owned);
   w.tot = dalloc<unsigned int>(2, c->mesh_owned);
   w.gen = dalloc<unsigned long long>(1, c->mesh_owned);
+  w.order = dalloc<unsigned long long>(std::max<size_t>(c->capacity, 1), c->mesh_owned);
   w.cells = cells;
   w.de_host.clear();
   w.dh_host.clear();
@@ -1407,10 +1408,10 @@ int mcb200_multiple_refresh(mcb200_ctx *c, const int32_t *desired_e, const int32
                        cells, c->mesh.nx, c->mesh.nz, c->hist, c->offsets, c->tile_sums, c->total,
                        grid_for(c, c->capacity, 256), s);
       const DevParticlesT<R> &P = store<R>(c, sorted);
-      launch_refresh_count(P, c->offsets, c->hist, cells, de, dh, r, out_count, new_count, s);
+      launch_refresh_count(P, c->offsets, c->hist, cells, de, dh, r, w.order, out_count, new_count, s);
       launch_exclusive_scan(out_count, out_off, tiles, tot, cells, s);
       launch_exclusive_scan(new_count, uid_off, tiles, tot + 1, cells, s);
-      launch_refresh_emit(P, c->offsets, c->hist, cells, de, dh, r, out_off, uid_off, c->dev_counts + 1,
+      launch_refresh_emit(P, c->offsets, c->hist, cells, de, dh, r, w.order, out_off, uid_off, c->dev_counts + 1,
                           store<R>(c, other), gen, s);
     };
     if (c->precision == MCB200_FLIGHT_FP32) refresh(float{});

@@ -130,6 +130,7 @@ struct MrScratch {
   unsigned int *out_count = nullptr, *new_count = nullptr, *out_off = nullptr, *uid_off = nullptr;
   unsigned int *tiles = nullptr, *tot = nullptr;
   unsigned long long *gen = nullptr;
+  unsigned long long *order = nullptr;  // [capacity]: uid << 32 | slot, each cell's particles in uid order
   std::vector<int> de_host, dh_host;  // the targets last uploaded to de / dh
 };
 
