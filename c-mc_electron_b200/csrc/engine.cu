@@ -1805,14 +1805,15 @@ template <typename R>
 void step_prepare(mcb200_ctx *c) {
   cudaStream_t s = c->stream;
   join_stat(c);  // the flights change the store the statistics read
-  ck(cudaMemsetAsync(c->tickets, 0, sizeof(unsigned int) * (1 + mcb200_ctx::kGenerations), s), "memset");
+  StepCounters z{c->tickets, {}};
+  for (int g = 0; g < mcb200_ctx::kGenerations; ++g) z.count[g] = children<R>(c, g).count;
+  z.count[mcb200_ctx::kGenerations] = c->sink_count;
+  launch_step_reset(z, s);
+  c->launches += 1;
   if constexpr (sizeof(R) == 4) {  // FP32 flight reads the fields as per-cell float records
     launch_cell_records32(c->ts->dt, c->mesh, c->cell32, c->ncells, s);
     c->launches += 1;
   }
-  for (int g = 0; g < mcb200_ctx::kGenerations; ++g)
-    ck(cudaMemsetAsync(children<R>(c, g).count, 0, sizeof(unsigned int), s), "memset");
-  ck(cudaMemsetAsync(c->sink_count, 0, sizeof(unsigned int), s), "memset");
 }
 
 // After the flights of a step: uids for the surviving copies, which join the

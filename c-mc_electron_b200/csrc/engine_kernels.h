@@ -42,6 +42,13 @@ template <typename R>
 void launch_append_children(const ChildSetT<R> &set, uint64_t *keys, uint8_t *alive, uint32_t *uids,
                             unsigned int *next_uid, const DevParticlesT<R> &dst, const unsigned int *n, int capacity,
                             unsigned int *appended, unsigned int *overflow, int grid, cudaStream_t s);
+// The counters a step starts from, zeroed in one launch: the flight tickets
+// and the copy count of every generation and of the sink.
+struct StepCounters {
+  unsigned int *tickets;  // [1 + kChildGenerations]
+  unsigned int *count[kChildGenerations + 1];
+};
+void launch_step_reset(const StepCounters &z, cudaStream_t s);
 // *particle_steps += *n; *n = *sorted_total; *next_uid += *appended.
 void launch_step_finish(unsigned int *n, const unsigned int *sorted_total, unsigned int *next_uid,
                         const unsigned int *appended, unsigned long long *particle_steps, cudaStream_t s);

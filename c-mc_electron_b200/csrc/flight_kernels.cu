@@ -584,6 +584,14 @@ void launch_append_children(const ChildSetT<R> &set, uint64_t *keys, uint8_t *al
   cudaMemsetAsync(appended, 0, sizeof(unsigned int), s);
   children_to_particles<R><<<grid, 256, 0, s>>>(set, uids, alive, dst, n, capacity, appended, overflow);
 }
+__global__ void step_reset_kernel(StepCounters z) {
+  const int t = threadIdx.x;
+  if (t < 1 + kChildGenerations) {
+    z.tickets[t] = 0u;
+    *z.count[t] = 0u;
+  }
+}
+void launch_step_reset(const StepCounters &z, cudaStream_t s) { step_reset_kernel<<<1, 32, 0, s>>>(z); }
 void launch_step_finish(unsigned int *n, const unsigned int *sorted_total, unsigned int *next_uid,
                         const unsigned int *appended, unsigned long long *particle_steps, cudaStream_t s) {
   step_finish<<<1, 32, 0, s>>>(n, sorted_total, next_uid, appended, particle_steps);
