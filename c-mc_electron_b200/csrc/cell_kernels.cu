@@ -53,9 +53,9 @@ __global__ void surface_rates_kernel(int cells, SurfaceRateParams q, const doubl
 }
 
 // ---------------------------------------------------------------------------
-// MultipleRefresh.  Pass 1 (count): order each cell's particles by uid (in
-// place, the cell is contiguous), decide per carrier whether to resample and
-// how many particles the cell will hold.  Pass 2 (emit): write the cell's
+// MultipleRefresh.  Pass 1 (count): index each cell's particles in uid
+// order (the cell is contiguous in the cell-sorted store), decide per carrier
+// whether to resample and how many particles the cell will hold.  Pass 2 (emit): write the cell's
 // new population at its scanned offset.
 struct Decision {
   int keep;      // 1: keep the old population of this type
@@ -132,9 +132,9 @@ __global__ void refresh_count_kernel(DevParticlesT<R> P, const unsigned int *cel
 template <typename R>
 __global__ void refresh_emit_kernel(DevParticlesT<R> P, const unsigned int *cell_end, const unsigned int *cell_count,
                                     int cells, const int *desired_e, const int *desired_h, RefreshParams r,
-                                    const unsigned long long *order, const unsigned int *out_offset,
-                                    const unsigned int *uid_offset, const unsigned int *uid0p, DevParticlesT<R> dst,
-                                    unsigned long long *mr_gen) {
+                                    const unsigned long long *order, double *wsum, int *widx,
+                                    const unsigned int *out_offset, const unsigned int *uid_offset,
+                                    const unsigned int *uid0p, DevParticlesT<R> dst, unsigned long long *mr_gen) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= cells) return;
   const int e = (int)cell_end[c], b = e - (int)cell_count[c];
@@ -160,23 +160,32 @@ __global__ void refresh_emit_kernel(DevParticlesT<R> P, const unsigned int *cell
       continue;
     }
     // draw `want` particles with probability |q| / sum|q| (lower_bound on the
-    // running sum, src/MultipleRefresh.cpp:35-44); the new charge is tot/want
+    // running sum, src/MultipleRefresh.cpp:35-44); the new charge is tot/want.
+    // The running sums of |q| over this type's particles in uid order go to
+    // wsum[b, b + m) once (m = d.old_num >= 1 here: an empty type is kept);
+    // each draw then searches them.  The sums never decrease, so the first
+    // one not below s is the one a scan would stop at.
+    int m = 0;
+    double w = 0;
+    for (int k = b; k < e; ++k) {
+      const int i = nth(order, k);
+      if (((P.meta[i] >> 8) & 255) != (uint32_t)t || fabs(P.charge[i]) < r.pckill) continue;
+      w += fabs(P.charge[i]);
+      wsum[b + m] = w;
+      widx[b + m] = i;
+      ++m;
+    }
     const double aver = d.tot / want;
     for (int q = 0; q < want; ++q) {
       const double s = mcb200_uniform(r.seed, (uint32_t)c, r.step, kRefreshSub + t, (uint32_t)q) * fabs(d.tot);
-      double w = 0;
-      int pick = -1, last = -1;
-      for (int k = b; k < e; ++k) {
-        const int i = nth(order, k);
-        if (((P.meta[i] >> 8) & 255) != (uint32_t)t || fabs(P.charge[i]) < r.pckill) continue;
-        last = i;
-        w += fabs(P.charge[i]);
-        if (w >= s) {  // first running sum not below s
-          pick = i;
-          break;
-        }
+      int lo = 0, hi = m;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (wsum[b + mid] >= s) hi = mid;
+        else lo = mid + 1;
       }
-      if (pick < 0) pick = last;  // s above the last sum (rounding): the reference prints and skips; keep the count
+      // s above the last sum (rounding): the reference prints and skips; keep the count
+      const int pick = widx[b + min(lo, m - 1)];
       copy(pick, o);
       dst.charge[o] = aver;
       dst.uid[o] = uid++;
@@ -204,11 +213,12 @@ void launch_refresh_count(const DevParticlesT<R> &P, const unsigned int *cell_en
 template <typename R>
 void launch_refresh_emit(const DevParticlesT<R> &P, const unsigned int *cell_end, const unsigned int *cell_count,
                          int cells, const int *desired_e, const int *desired_h, const RefreshParams &r,
-                         const unsigned long long *order, const unsigned int *out_offset,
+                         const unsigned long long *order, double *wsum, int *widx, const unsigned int *out_offset,
                          const unsigned int *uid_offset, const unsigned int *uid0, const DevParticlesT<R> &dst,
                          unsigned long long *mr_gen, cudaStream_t s) {
   refresh_emit_kernel<R><<<(cells + 127) / 128, 128, 0, s>>>(P, cell_end, cell_count, cells, desired_e, desired_h, r,
-                                                          order, out_offset, uid_offset, uid0, dst, mr_gen);
+                                                          order, wsum, widx, out_offset, uid_offset, uid0, dst,
+                                                          mr_gen);
 }
 
 #define MCB200_INSTANTIATE(R)                                                                                 \
@@ -217,9 +227,9 @@ void launch_refresh_emit(const DevParticlesT<R> &P, const unsigned int *cell_end
                                         unsigned long long *, unsigned int *, unsigned int *, cudaStream_t);  \
   template void launch_refresh_emit<R>(const DevParticlesT<R> &, const unsigned int *, const unsigned int *,  \
                                        int, const int *, const int *, const RefreshParams &,                 \
-                                       const unsigned long long *, const unsigned int *, const unsigned int *, \
-                                       const unsigned int *, const DevParticlesT<R> &, unsigned long long *,  \
-                                       cudaStream_t);
+                                       const unsigned long long *, double *, int *, const unsigned int *,     \
+                                       const unsigned int *, const unsigned int *, const DevParticlesT<R> &,  \
+                                       unsigned long long *, cudaStream_t);
 MCB200_INSTANTIATE(double)
 MCB200_INSTANTIATE(float)
 #undef MCB200_INSTANTIATE

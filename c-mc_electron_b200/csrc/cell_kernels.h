@@ -38,12 +38,13 @@ void launch_refresh_count(const DevParticlesT<R> &P, const unsigned int *cell_en
                           unsigned long long *order, unsigned int *out_count, unsigned int *new_count,
                           cudaStream_t s);
 // order: one key per store slot, written by the count pass (each cell's
-// particles in uid order) and read by the emit pass.
+// particles in uid order) and read by the emit pass.  wsum / widx: one
+// entry per store slot, the emit pass's running sums and their particles.
 // uid0: device word holding the first new uid (the context's uid counter).
 template <typename R>
 void launch_refresh_emit(const DevParticlesT<R> &P, const unsigned int *cell_end, const unsigned int *cell_count,
                          int cells, const int *desired_e, const int *desired_h, const RefreshParams &r,
-                         const unsigned long long *order, const unsigned int *out_offset,
+                         const unsigned long long *order, double *wsum, int *widx, const unsigned int *out_offset,
                          const unsigned int *uid_offset, const unsigned int *uid0, const DevParticlesT<R> &dst,
                          unsigned long long *mr_gen, cudaStream_t s);
 

@@ -420,6 +420,8 @@ void mr_scratch(mcb200_ctx *c) {
   w.tot = dalloc<unsigned int>(2, c->mesh_owned);
   w.gen = dalloc<unsigned long long>(1, c->mesh_owned);
   w.order = dalloc<unsigned long long>(std::max<size_t>(c->capacity, 1), c->mesh_owned);
+  w.wsum = dalloc<double>(std::max<size_t>(c->capacity, 1), c->mesh_owned);
+  w.widx = dalloc<int>(std::max<size_t>(c->capacity, 1), c->mesh_owned);
   w.cells = cells;
   w.de_host.clear();
   w.dh_host.clear();
@@ -1411,7 +1413,8 @@ int mcb200_multiple_refresh(mcb200_ctx *c, const int32_t *desired_e, const int32
       launch_refresh_count(P, c->offsets, c->hist, cells, de, dh, r, w.order, out_count, new_count, s);
       launch_exclusive_scan(out_count, out_off, tiles, tot, cells, s);
       launch_exclusive_scan(new_count, uid_off, tiles, tot + 1, cells, s);
-      launch_refresh_emit(P, c->offsets, c->hist, cells, de, dh, r, w.order, out_off, uid_off, c->dev_counts + 1,
+      launch_refresh_emit(P, c->offsets, c->hist, cells, de, dh, r, w.order, w.wsum, w.widx, out_off, uid_off,
+                          c->dev_counts + 1,
                           store<R>(c, other), gen, s);
     };
     if (c->precision == MCB200_FLIGHT_FP32) refresh(float{});

@@ -131,6 +131,8 @@ struct MrScratch {
   unsigned int *tiles = nullptr, *tot = nullptr;
   unsigned long long *gen = nullptr;
   unsigned long long *order = nullptr;  // [capacity]: uid << 32 | slot, each cell's particles in uid order
+  double *wsum = nullptr;               // [capacity]: running sums of |q| of the particles a cell draws from
+  int *widx = nullptr;                  // [capacity]: their slots
   std::vector<int> de_host, dh_host;  // the targets last uploaded to de / dh
 };
 
