@@ -120,13 +120,31 @@ struct ChildIO {
 // other particles finish, instead of idling until the slowest one is done.
 // Every particle's draws come from its own stream, so the result does not
 // depend on which lane flies it or when.
-template <typename R, class IO>
+//
+// kLaneEvents (launches of one simulation): the event count of each finished
+// particle is summed in the lane and the warp adds its total to the
+// simulation's counter once, at the end, instead of one atomic on that one
+// address per particle.  A batched launch counts per particle (its particles
+// belong to different simulations).
+template <typename R, bool kLaneEvents, class IO>
 __device__ __forceinline__ void fly_interleaved(const FlightCtxT<R> &F, const SymSmemT<R> &S, const IO &io, int n,
                                                 unsigned int *ticket) {
   FlyerT<R> f(F, S);
   const unsigned lane = threadIdx.x & 31u;
   int p = -1;
   bool exhausted = false;
+  uint32_t events = 0;  // < 2^31 + kMaxEvents: flushed whenever it passes 2^31
+  auto done = [&]() {
+    const int r = f.template finish<!kLaneEvents>();
+    if constexpr (kLaneEvents) {
+      events += (uint32_t)f.loop;
+      if (events >= 0x80000000u) {
+        atomicAdd(&F.Y.counters[kCntEvents], (unsigned long long)events);
+        events = 0;
+      }
+    }
+    return r;
+  };
   for (;;) {
     if (!exhausted) {
       const unsigned need = __ballot_sync(0xffffffffu, p < 0);
@@ -142,7 +160,7 @@ __device__ __forceinline__ void fly_interleaved(const FlightCtxT<R> &F, const Sy
             p = (int)q;
             f.begin();
             if (!(f.left_time > 0)) {
-              io.store(p, f, f.finish());
+              io.store(p, f, done());
               p = -1;
             }
           }
@@ -154,9 +172,15 @@ __device__ __forceinline__ void fly_interleaved(const FlightCtxT<R> &F, const Sy
       continue;
     }
     if (p >= 0 && f.iterate()) {
-      io.store(p, f, f.finish());
+      io.store(p, f, done());
       p = -1;
     }
+  }
+  if constexpr (kLaneEvents) {
+    unsigned long long sum = events;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, off);
+    if (lane == 0 && sum) atomicAdd(&F.Y.counters[kCntEvents], sum);
   }
 }
 
@@ -167,7 +191,7 @@ __global__ void __launch_bounds__(kFlightThreads, kFlightBlocks<R>) flight_kerne
   if (count == 0) return;
   __shared__ SymSmemT<R> S;
   load_sym(S, F.T);
-  fly_interleaved(F, S, StoreIO<R>{P, F.dt}, count, ticket);
+  fly_interleaved<R, true>(F, S, StoreIO<R>{P, F.dt}, count, ticket);
 }
 
 // Copies made during the previous pass (buffer `in`) fly the rest of their
@@ -179,7 +203,7 @@ __global__ void __launch_bounds__(kFlightThreads, kFlightBlocks<R>) child_flight
   if (count == 0) return;
   __shared__ SymSmemT<R> S;
   load_sym(S, F.T);
-  fly_interleaved(F, S, ChildIO<R>{in}, count, ticket);
+  fly_interleaved<R, true>(F, S, ChildIO<R>{in}, count, ticket);
 }
 
 // ---- batched flight ------------------------------------------------------
@@ -261,7 +285,7 @@ __global__ void __launch_bounds__(kFlightThreads, kFlightBlocks<R>) batch_flight
   load_sym(S, F.T);  // ends with a barrier: the table and prefix are visible
   const int total = prefix[ninst];
   if (total == 0) return;
-  fly_interleaved(F, S, BatchIO<R, kChild>{I, prefix, ninst}, total, ticket);
+  fly_interleaved<R, false>(F, S, BatchIO<R, kChild>{I, prefix, ninst}, total, ticket);
 }
 
 // FP32 flight's per-cell records (DevMesh::cell32): the fields in float and
@@ -525,9 +549,18 @@ void launch_seed(const FlightCtx &F, const DevParticlesT<R> &P, int offset, int 
 }
 // Blocks of the persistent flight kernels: enough to fill every SM at the
 // kernel's occupancy, fewer when there are fewer particles than threads.
+// Launch settings are looked up once per device (the current device at the
+// launch) and kept: a process may drive several GPUs.
+constexpr int kMaxDevices = 64;
+inline int current_device() {
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= kMaxDevices) d = 0;
+  return d;
+}
 template <typename R>
 int flight_grid(int n, int block, int sm_count) {
-  static int per_sm = 0;
+  static int per_sm_of[kMaxDevices] = {};
+  int &per_sm = per_sm_of[current_device()];
   if (per_sm == 0) {
     int b = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, flight_kernel<R>, block, 0) != cudaSuccess || b < 1) b = 1;
@@ -557,12 +590,14 @@ int launch_batch_flight(const FlightCtxT<R> &F, const BatchInstT<R> *inst, int n
   if (ninst < 1 || ninst > kMaxBatch) return 1;
   const size_t smem = batch_smem_bytes<R>(ninst);
   auto kernel = child ? batch_flight_kernel<R, true> : batch_flight_kernel<R, false>;
-  static bool opted[2] = {false, false};
-  if (!opted[child ? 1 : 0]) {
+  // the opt-in to more than 48 KB of dynamic shared memory holds per device
+  static bool opted[kMaxDevices][2] = {};
+  bool &done = opted[current_device()][child ? 1 : 0];
+  if (!done) {
     if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)batch_smem_bytes<R>(kMaxBatch)) != cudaSuccess)
       return 1;
-    opted[child ? 1 : 0] = true;
+    done = true;
   }
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kFlightThreads, smem) != cudaSuccess ||

@@ -1352,9 +1352,12 @@ struct FlyerT {
     return !(left_time > 0);
   }
 
-  // Returns 0 done, 1 caught, 2 unfinished (outer-boundary PASS).
+  // Returns 0 done, 1 caught, 2 unfinished (outer-boundary PASS).  A
+  // caller that sums the particles' event counts itself (`loop`, one
+  // simulation per launch) passes kCountEvents = false.
+  template <bool kCountEvents = true>
   __device__ int finish() {
-    atomicAdd(&I->Y.counters[kCntEvents], (unsigned long long)loop);
+    if constexpr (kCountEvents) atomicAdd(&I->Y.counters[kCntEvents], (unsigned long long)loop);
     if (catch_) {
       count(I->Y, kCntCaught);
       return 1;

@@ -21,7 +21,7 @@ from mcb200 import decks
 from oracle_bridge import ORACLE_TABLES, Oracle
 from parity_cases import make_restart
 
-REF_FINFET = "/root/reference/finfet"
+REF_FINFET = os.path.join(os.environ.get("MCB200_REFERENCE", "/root/reference"), "finfet")
 
 
 def _compare(input_path):
