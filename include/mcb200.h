@@ -118,6 +118,10 @@ int mcb200_units(const mcb200_ctx *ctx, double *out, int n);
  * "dose", "scattiie", "scatth", "dosh", "scattiih", "energy". */
 int mcb200_copy_table(const mcb200_ctx *ctx, const char *name, void *out, size_t bytes, size_t *needed);
 
+/* Cells per axis of the mesh set by mcb200_set_mesh (MCB200_ERR_STATE
+ * before it). */
+int mcb200_get_mesh_dims(const mcb200_ctx *ctx, int *nx, int *ny, int *nz);
+
 /* Mesh node coordinates in normalised length (lx: nx+1 values, ...) and,
  * optionally, the cell widths dx/dy/dz (nx, ny, nz values; NULL: taken as
  * node differences).  The reference scales its widths separately from its
@@ -406,9 +410,12 @@ int mcb200_get_tallies(mcb200_ctx *ctx, uint64_t *counters, double *contact, dou
                        double *heat_e, double *heat_h);
 int mcb200_reset_tallies(mcb200_ctx *ctx);
 
-/* Particle store in device memory, in the engine's own layout (what
- * mcb200_step keeps per particle): cell packs i | j << 10 | k << 20; meta
- * packs isym | type << 8, and bit 16 set marks a particle to be dropped. */
+/* Particle store in device memory in the engine's FP64 layout (what
+ * mcb200_step keeps per particle when the flight runs in FP64): absolute
+ * positions, k and energy / charge in double; cell packs
+ * i | j << 10 | k << 20; meta packs isym | type << 8, and bit 16 set marks a
+ * particle to be dropped.  An FP32-flight store (float cell-relative
+ * positions and k) has another layout and cannot be passed here. */
 typedef struct {
   double *x, *y, *z;
   double *kx, *ky, *kz;
@@ -427,15 +434,24 @@ typedef struct {
  * such as a host framework that owns every device buffer and lends out
  * slices of its own pool, or code that must not allocate while other work
  * holds the device.  The caller passes the input and the output arrays
- * (n entries each; particles with meta bit 16 are dropped, *n_out receives
- * how many remain); the scratch is one static device array of
+ * (n entries each, in the FP64 layout above; the two stores must not share
+ * any bytes, else MCB200_ERR_ARG).  Particles with meta bit 16 are dropped
+ * and *n_out receives how many remain.  Every live particle's cell must lie
+ * inside the nx x ny x nz mesh: one that does not is left out of the output
+ * and the call returns MCB200_ERR_ARG (the kernels never index past the
+ * mesh).  The scratch is one static device array of
  * MCB200_STATIC_SORT_MAX_CELLS cells (2 MiB, held by every GPU that loads
  * the library until the process exits), and larger meshes return
  * MCB200_ERR_CAPACITY.  The first call on a device looks the array's device
- * address up and caches it; make that first call before any stream capture.
- * Every call shares the array, so calls that overlap on the GPU (two
- * streams, two threads) race: serialise them.  Order within a cell is not
- * specified.  `stream` is a cudaStream_t (NULL: the legacy default stream). */
+ * address up and caches it; make that first call before any stream capture,
+ * and make no call after cudaDeviceReset (the cached address would be
+ * stale).  Every call shares the array, so calls that overlap on the GPU
+ * (two streams, two threads) race: serialise them.  The call returns when
+ * the sort has finished on `stream` (it reads the kept count and the range
+ * check back).  A CUDA error already pending on the calling thread is left
+ * in place and the call does nothing but return MCB200_ERR_CUDA.  Order
+ * within a cell is not specified.  `stream` is a cudaStream_t (NULL: the
+ * legacy default stream). */
 int mcb200_sort_particles_static(const mcb200_device_particles *in, size_t n, int nx, int ny, int nz,
                                  const mcb200_device_particles *out, size_t *n_out, void *stream);
 
@@ -663,6 +679,19 @@ int mcb200_server_round(mcb200_server *server, int *active, int *pending);
 /* Moves up to `max` finished results out of the server. */
 int mcb200_server_results(mcb200_server *server, mcb200_result *out, int max, int *n);
 int mcb200_server_stats(const mcb200_server *server, mcb200_server_stats_t *stats);
+
+/* The window outputs of the reference's run loop for the context's current
+ * state, written under data_dir: output_stat with current_scatter_info
+ * (src/mcmodel.cpp:971-1161, :756-842) -- `current` (appended), section_current,
+ * electron_num, pot, qc_pot, Electron, Hole and, with heat != 0, heat
+ * (<name><step>, appended as the reference opens them) -- and
+ * output_for_restart (:895-965, par_info_restart<step>).  The sums are those
+ * of the statistics window (mcb200_stat_begin / mcb200_stat_accumulate) of
+ * `window` steps and the tallies since the last reset; dt is the time step,
+ * n_contacts the deck's contacts.  mcb200_run_deck calls the same writer at
+ * the end of every window. */
+int mcb200_write_outputs(mcb200_ctx *ctx, const char *data_dir, int step, int window, double dt, int n_contacts,
+                         int heat);
 
 /* `error` (may be NULL) receives a message on failure. */
 int mcb200_run_deck(const char *input_path, int device, const mcb200_run_options *options,

@@ -10,7 +10,9 @@ existing entry point: mcb200_step with dt = 0 flies nobody and ends with the
 same counting sort by cell.  The two must agree exactly (a sort is a
 permutation) on two calls in a row, the second into a poisoned output.
 Order inside a cell is unspecified, so both sides are compared in
-(cell, uid) order.  This file is collected last on purpose.
+(cell, uid) order.  Particles marked dropped must be left out, cells off
+the mesh and overlapping stores must be refused.  This file is collected
+last on purpose.
 """
 import ctypes
 
@@ -60,7 +62,26 @@ def make_engine(nx=8, ny=6, nz=6, electrons=4000, holes=600):
     return eng, (nx, ny, nz)
 
 
+def sort_fn():
+    lib = mcb200.lib()
+    lib.mcb200_sort_particles_static.argtypes = [ctypes.POINTER(DeviceParticles), ctypes.c_size_t, ctypes.c_int,
+                                                 ctypes.c_int, ctypes.c_int, ctypes.POINTER(DeviceParticles),
+                                                 ctypes.POINTER(ctypes.c_size_t), ctypes.c_void_p]
+    return lib.mcb200_sort_particles_static
+
+
+def to_device(torch, src: dict) -> dict:
+    return {k: torch.from_numpy(src[k].view(np.int32) if src[k].dtype == np.uint32 else src[k]).cuda()
+            for k in FIELDS}
+
+
+def describe(dev: dict) -> DeviceParticles:
+    return DeviceParticles(*[dev[k].data_ptr() for k in FIELDS])
+
+
 def test_static_sort_matches_engine_sort():
+    """Two calls in a row against the engine's own sort, with a few particles
+    marked dropped (meta bit 16); the second call on a caller's stream."""
     torch = pytest.importorskip("torch")
     eng, (nx, ny, nz) = make_engine()
     host = eng.download()
@@ -73,41 +94,82 @@ def test_static_sort_matches_engine_sort():
     eng.close()
 
     src = packed(shuffled)
-    dev_in = {k: torch.from_numpy(src[k].view(np.int32) if src[k].dtype == np.uint32 else src[k]).cuda()
-              for k in FIELDS}
+    dropped = np.random.default_rng(2).choice(n, 37, replace=False)
+    src["meta"][dropped] |= np.uint32(1 << 16)
+    keep = ~np.isin(ref["uid"], src["uid"][dropped])
+    ref = {k: v[keep] for k, v in ref.items()}
+    ref_lin = ref_lin[keep]
+    dev_in = to_device(torch, src)
     dev_out = {k: torch.empty_like(t) for k, t in dev_in.items()}
-    desc_in = DeviceParticles(*[dev_in[k].data_ptr() for k in FIELDS])
-    desc_out = DeviceParticles(*[dev_out[k].data_ptr() for k in FIELDS])
-    lib = mcb200.lib()
-    lib.mcb200_sort_particles_static.argtypes = [ctypes.POINTER(DeviceParticles), ctypes.c_size_t, ctypes.c_int,
-                                                 ctypes.c_int, ctypes.c_int, ctypes.POINTER(DeviceParticles),
-                                                 ctypes.POINTER(ctypes.c_size_t), ctypes.c_void_p]
+    desc_in, desc_out = describe(dev_in), describe(dev_out)
+    sort = sort_fn()
+    side = torch.cuda.Stream()
     for call in range(2):
-        for t in dev_out.values():  # poison the output so every entry must be written
+        for t in dev_out.values():  # poison the output so every kept entry must be written
             t.fill_(-1)
         torch.cuda.synchronize()
         kept = ctypes.c_size_t(0)
-        rc = lib.mcb200_sort_particles_static(ctypes.byref(desc_in), n, nx, ny, nz, ctypes.byref(desc_out),
-                                              ctypes.byref(kept), None)
+        handle = None if call == 0 else ctypes.c_void_p(side.cuda_stream)
+        rc = sort(ctypes.byref(desc_in), n, nx, ny, nz, ctypes.byref(desc_out), ctypes.byref(kept), handle)
         torch.cuda.synchronize()
         assert rc == 0, f"call {call}: status {rc}"
-        assert kept.value == n
-        got = {k: dev_out[k].cpu().numpy() for k in FIELDS}
+        assert kept.value == n - len(dropped)
+        m = kept.value
+        got = {k: dev_out[k][:m].cpu().numpy() for k in FIELDS}
         got = {k: (v.view(np.uint32) if DTYPES[k] == np.uint32 else v) for k, v in got.items()}
         c = got["cell"].astype(np.int64)
         in_order = (((c >> 10) & 1023) * nx + (c & 1023)) * nz + ((c >> 20) & 1023)
         assert np.all(np.diff(in_order) >= 0), f"call {call}: output not grouped by cell"
+        assert not np.isin(got["uid"], src["uid"][dropped]).any(), f"call {call}: a dropped particle was kept"
         got_c, lin = canonical(got, nx, nz)
         assert np.array_equal(lin, ref_lin)
         for k in FIELDS:
             assert np.array_equal(got_c[k], ref[k]), f"call {call}: field {k} differs"
 
 
+def test_static_sort_rejects_cells_off_the_mesh():
+    """A live particle whose cell lies outside the mesh is an argument error;
+    the kernels skip it (no access past the mesh), and a correct call right
+    after gives the full result."""
+    torch = pytest.importorskip("torch")
+    eng, (nx, ny, nz) = make_engine(electrons=800, holes=100)
+    src = packed(eng.download())
+    eng.close()
+    n = len(src["x"])
+    good = {k: v.copy() for k, v in src.items()}
+    src["cell"][5] = np.uint32(nx | (1 << 10))       # i = nx
+    src["cell"][9] = np.uint32(2 | ((ny + 3) << 10))  # j beyond ny
+    src["cell"][11] = np.uint32(1 | (1023 << 20))     # k = 1023
+    dev_in, dev_good = to_device(torch, src), to_device(torch, good)
+    dev_out = {k: torch.empty_like(t) for k, t in dev_in.items()}
+    sort = sort_fn()
+    kept = ctypes.c_size_t(0)
+    rc = sort(ctypes.byref(describe(dev_in)), n, nx, ny, nz, ctypes.byref(describe(dev_out)), ctypes.byref(kept),
+              None)
+    assert rc == 1  # MCB200_ERR_ARG
+    assert kept.value == n - 3
+    rc = sort(ctypes.byref(describe(dev_good)), n, nx, ny, nz, ctypes.byref(describe(dev_out)), ctypes.byref(kept),
+              None)
+    assert rc == 0 and kept.value == n
+
+
+def test_static_sort_rejects_overlapping_stores():
+    torch = pytest.importorskip("torch")
+    eng, (nx, ny, nz) = make_engine(electrons=200, holes=20)
+    src = packed(eng.download())
+    eng.close()
+    n = len(src["x"])
+    dev = to_device(torch, src)
+    sort = sort_fn()
+    same = describe(dev)
+    assert sort(ctypes.byref(same), n, nx, ny, nz, ctypes.byref(same), None, None) == 1
+    other = {k: torch.empty_like(t) for k, t in dev.items()}
+    out = describe(other)
+    out.energy = dev["charge"].data_ptr() + 8  # one output array inside an input array
+    assert sort(ctypes.byref(same), n, nx, ny, nz, ctypes.byref(out), None, None) == 1
+
+
 def test_static_sort_rejects_oversized_mesh():
-    lib = mcb200.lib()
-    lib.mcb200_sort_particles_static.argtypes = [ctypes.POINTER(DeviceParticles), ctypes.c_size_t, ctypes.c_int,
-                                                 ctypes.c_int, ctypes.c_int, ctypes.POINTER(DeviceParticles),
-                                                 ctypes.POINTER(ctypes.c_size_t), ctypes.c_void_p]
     empty = DeviceParticles()
-    rc = lib.mcb200_sort_particles_static(ctypes.byref(empty), 0, 1000, 1000, 1, ctypes.byref(empty), None, None)
+    rc = sort_fn()(ctypes.byref(empty), 0, 1000, 1000, 1, ctypes.byref(empty), None, None)
     assert rc == 4  # MCB200_ERR_CAPACITY: 10^6 cells exceed the static scratch
