@@ -25,7 +25,7 @@ sort), refresh.  Timed twice: FP32 flight and plain FP64 flight.
               electrons, E_x = 10 kV/cm), flight-kernel throughput of both
               precisions
   cpu_baseline  the reference's own routines (CPU oracle: density_and_field
-              every 10 steps + update_particle) on a reduced FinFET, one core
+              every 10 steps + update_particle) on the same FinFET, one core
 
 --impl reference times the same reference routines on all host cores, one
 process per core.
@@ -182,6 +182,18 @@ def measure_precision(args, rank: int, world: int, device: int, precision: str):
 
 
 FINFET_POISSON_EVERY = 10
+FINFET_CARRIERS = 511200  # 300k e- + 50k h+ requested, raised by the per-cell minimum (compute_par_num)
+
+
+def finfet_config(world: int) -> dict:
+    """The FinFET workload both arms run (engine and reference)."""
+    return {"workload": "n-FinFET self-consistent: fin 10x30 nm, Lg 20 nm, 1 nm SiO2, S/D 1e20 cm^-3 (2 nm/dec), "
+                        "channel 1e15 cm^-3, 80x50x40 nonuniform mesh (0.5 nm channel, 2 nm contacts), 300k e- + "
+                        "50k h+ requested (511,200 carriers with the per-cell minimum), Vd 0.7 V, Vg 0.8 V, dt 0.2 "
+                        "fs, surface scattering, Poisson every 10 steps, MultipleRefresh every 50",
+            "carriers": FINFET_CARRIERS,
+            "l2": "L2 evicted (256 MB write) before every timed step on the GPU, eviction not timed",
+            "parallelism": f"replicas{world}"}
 PHASE_PROFILE_STEPS = 60  # steps of the phase-split run (each phase waited for)
 FLUSH_BYTES = 256 << 20  # > 126 MB L2
 
@@ -246,14 +258,9 @@ def engine_arm(args, rank: int, world: int, device: int):
         "metric": METRIC, "value": value["fp32"], "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": r32["timed_device_ms"] / max(r32["timed_steps"], 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "n-FinFET self-consistent: fin 10x30 nm, Lg 20 nm, 1 nm SiO2, S/D 1e20 cm^-3 "
-                               "(2 nm/dec), channel 1e15 cm^-3, 80x50x40 nonuniform mesh (0.5 nm channel, 2 nm "
-                               "contacts), 300k e- + 50k h+ requested (511k carriers with the per-cell minimum), "
-                               "Vd 0.7 V, Vg 0.8 V, dt 0.2 fs, surface scattering, FP64 PCG Poisson every 10 steps, "
-                               "MultipleRefresh every 50; FP32 flight (FP64 energy/time bookkeeping) vs plain FP64",
-                   "carriers_initial": r32["initial_particles"], "precision": "fp32-flight",
-                   "l2": "L2 evicted (256 MB write) before every timed step, eviction not timed",
-                   "parallelism": f"replicas{world}"},
+        "config": finfet_config(world),
+        "precision": "fp32-flight (FP64 energy / time bookkeeping); fp64_plain: all-FP64 flight",
+        "carriers_initial": r32["initial_particles"],
         "e2e": {"value": e2e_ps, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 16 * 6 * 8,
                 "note": "mcb200_run_deck (the main input.txt path) with the contact tallies read back every step; "
@@ -358,7 +365,7 @@ def serve_arm(args, device: int) -> dict:
     (Vg 0-0.8 V in 0.05 V steps x Vd {0.05, 0.7} V x Lg {15, 20, 30} nm,
     50k-1M particles log-uniform) arriving as a Poisson process of 4 req/s
     (seed 5); FP32 flight, HBM budget 160 GB, one Ids window per 50-step
-    round (net flux through the middle third of the section planes), each
+    round (the drain's induced current, Ramo-Shockley), each
     request done when stderr(Ids) < 1% of |Ids| after 6 transient windows
     (2 after a warm start) or at 2000 steps.  Latency = completion - arrival
     (server clock); throughput = particle-steps over the rounds' device time."""
@@ -371,7 +378,7 @@ def serve_arm(args, device: int) -> dict:
         with ClockSampler(device) as clocks:
             res, st, wall = serving.serve(srv, reqs, max_wall_s=900, max_steps=SERVE_MAX_STEPS, min_windows=5,
                                           warm_windows_cold=6, warm_windows_warm=2, poisson_every=10,
-                                          target_rel_err=0.01, ids_sections=True)
+                                          target_rel_err=0.01, ids_estimator=mcb200.IDS_INDUCED)
         srv.close()
     lat = serving.latency_summary(res)
     status = [r["status"] for r in res]
@@ -390,10 +397,10 @@ def serve_arm(args, device: int) -> dict:
 
 # ------------------------------------------------------------ reference (CPU)
 def _oracle_sample(args):
-    """One CPU process: the reference's routines on a reduced FinFET deck
-    (density_and_field every FINFET_POISSON_EVERY steps -- BiCGSTAB standing
-    in for KLU -- and update_particle every step); returns (particle-steps,
-    seconds)."""
+    """One CPU process: the reference's routines on the FinFET deck of the
+    engine arm (density_and_field every FINFET_POISSON_EVERY steps --
+    BiCGSTAB standing in for KLU -- and update_particle every step); returns
+    (particle-steps, seconds).  The deck's initialisation is not timed."""
     seed, electrons, holes, steps = args
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from mcb200 import decks
@@ -415,24 +422,27 @@ def _oracle_sample(args):
     return ps, time.perf_counter() - t0
 
 
-def cpu_baseline(target_s: float = 15.0):
-    ps, t = _oracle_sample((99, 20000, 4000, 3))
-    steps = max(3, min(200, int(target_s / max(t / 3, 1e-6))))
-    ps, t = _oracle_sample((99, 20000, 4000, steps))
+FINFET_REQUEST = (300000, 50000)  # electrons, holes requested in the deck
+
+
+def cpu_baseline(steps: int = 10):
+    """The reference's routines on the engine arm's FinFET (511,200 carriers),
+    one core: one Poisson solve and `steps` flights (about 10-15 s)."""
+    ps, t = _oracle_sample((99, *FINFET_REQUEST, steps))
     return {"value": ps / t, "unit": "particle-steps/s", "cores": 1, "kind": "reference",
             "sample": f"the reference's density_and_field (every {FINFET_POISSON_EVERY} steps) + update_particle on "
-                      f"the FinFET deck with 20000 electrons + 4000 holes requested, {steps} steps, {t:.1f} s, "
+                      f"the engine arm's FinFET deck ({FINFET_CARRIERS} carriers), {steps} steps, {t:.1f} s, "
                       "one core"}
 
 
 def reference_arm(args, rank: int, world: int):
     if rank != 0:
         return None
-    cores = os.cpu_count() or 1
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
     steps = max(3, min(args.steps, 20))
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores) as pool:
-        res = pool.map(_oracle_sample, [(1000 + i, 20000, 4000, steps) for i in range(cores)])
+        res = pool.map(_oracle_sample, [(1000 + i, *FINFET_REQUEST, steps) for i in range(cores)])
     total_ps = sum(r[0] for r in res)
     wall = max(r[1] for r in res)
     value = total_ps / wall
@@ -440,13 +450,13 @@ def reference_arm(args, rank: int, world: int):
         "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": steps,
         "warmup": args.warmup, "ms_per_step": wall / steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": {"workload": "n-FinFET self-consistent (the engine arm's deck) with 20000 electrons + 4000 holes "
-                               "requested per process; the reference's density_and_field every 10 steps + "
-                               "update_particle (FP64, reference CPU code)",
-                   "processes": cores},
+        "config": finfet_config(world),
+        "precision": "all-FP64 (the reference's CPU code)",
+        "processes": cores,
         "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores, "kind": "reference",
-                         "sample": f"{cores} independent processes x {steps} steps of the reference's routines on "
-                                   "the reduced FinFET"},
+                         "sample": f"{cores} independent processes, each {steps} steps of the reference's "
+                                   f"density_and_field (every {FINFET_POISSON_EVERY} steps) + update_particle on the "
+                                   f"engine arm's FinFET deck ({FINFET_CARRIERS} carriers)"},
         "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 

@@ -275,7 +275,12 @@ struct Run {
       ok(mcb200_download_particles(ctx, &hp, n, &got), ctx, "mcb200_download_particles");
       std::vector<double> ec(cells, 0.0), hc(cells, 0.0);
       std::vector<int> en(cells, 0), hn(cells, 0);
-      for (size_t q = 0; q < got; ++q) {
+      // summed in uid order: the store's order within a cell varies from run
+      // to run (the cell sort's atomics), the file must not
+      std::vector<uint32_t> order(got);
+      for (size_t q = 0; q < got; ++q) order[q] = (uint32_t)q;
+      std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return uid[a] < uid[b]; });
+      for (const uint32_t q : order) {
         const size_t c = cidx(pi[0][q], pi[1][q], pi[2][q]);
         if (pi[5][q] == 0) { ec[c] += std::fabs(pd[6][q]); en[c]++; }
         else { hc[c] += std::fabs(pd[6][q]); hn[c]++; }
@@ -481,6 +486,38 @@ extern "C" int mcb200_deck_surface_params(const char *input_path, mcb200_ctx *ct
   *out = s;
   if (poisson_every) *poisson_every = ex.poisson_every;
   return MCB200_OK;
+}
+
+extern "C" int mcb200_write_outputs(mcb200_ctx *ctx, const char *data_dir, int step, int window, double dt,
+                                    int n_contacts, int heat) {
+  if (!ctx || !data_dir || window < 1 || n_contacts < 0 || n_contacts > 16 || !(dt > 0)) return MCB200_ERR_ARG;
+  mcb200_run_report report{};
+  Run r;
+  r.ctx = ctx;
+  r.rep = &report;
+  r.data_dir = data_dir;
+  r.heat = heat != 0;
+  r.info.dt = dt;
+  r.info.n_contacts = n_contacts;
+  int rc = MCB200_OK;
+  try {
+    ok(mcb200_get_mesh_dims(ctx, &r.nx, &r.ny, &r.nz), ctx, "mcb200_get_mesh_dims");
+    ok(mcb200_units(ctx, r.u, 14), ctx, "mcb200_units");
+    r.cells = r.nx * r.ny * r.nz;
+    r.nodes = (r.nx + 1) * (r.ny + 1) * (r.nz + 1);
+    r.node_volume.resize(r.nodes);
+    ok(mcb200_get_array(ctx, "node_volume", r.node_volume.data(), r.nodes), ctx, "node_volume");
+    for (size_t slash = r.data_dir.find('/', 1); slash != std::string::npos; slash = r.data_dir.find('/', slash + 1))
+      ::mkdir(r.data_dir.substr(0, slash).c_str(), 0755);  // the parents first (mkdir -p)
+    ::mkdir(r.data_dir.c_str(), 0755);
+    r.write_outputs(step, window);
+  } catch (const RunError &e) {
+    rc = e.code ? e.code : MCB200_ERR_STATE;
+  } catch (const std::exception &e) {
+    rc = MCB200_ERR_IO;
+  }
+  r.ctx = nullptr;  // the caller's context: not destroyed here
+  return rc;
 }
 
 extern "C" int mcb200_run_deck(const char *input_path, int device, const mcb200_run_options *options,

@@ -609,6 +609,15 @@ int mcb200_units(const mcb200_ctx *c, double *out, int n) {
   return MCB200_OK;
 }
 
+int mcb200_get_mesh_dims(const mcb200_ctx *c, int *nx, int *ny, int *nz) {
+  if (!c || !nx || !ny || !nz) return MCB200_ERR_ARG;
+  if (!c->mesh_set) return MCB200_ERR_STATE;
+  *nx = c->mesh.nx;
+  *ny = c->mesh.ny;
+  *nz = c->mesh.nz;
+  return MCB200_OK;
+}
+
 int mcb200_copy_table(const mcb200_ctx *c, const char *name, void *out, size_t bytes, size_t *needed) {
   if (!c || !name || !needed) return MCB200_ERR_ARG;
   const FullBandTables &t = c->ts->tab;
@@ -713,6 +722,9 @@ int mcb200_set_mesh(mcb200_ctx *c, int nx, int ny, int nz, const double *lx, con
     c->sb.cell_count = dalloc<unsigned long long>(cells, c->mesh_owned);
     c->sb.pot_sum = dalloc<double>(nodes, c->mesh_owned);
     c->sb.qc_pot_sum = dalloc<double>(nodes, c->mesh_owned);
+    c->induced_contact = -1;
+    c->induced_field = nullptr;
+    c->ib = InducedBuffers{};
     c->qc = QuantumDevice{};
     c->qc_pot = nullptr;
     c->pot_scratch = nullptr;
@@ -1187,6 +1199,7 @@ int mcb200_reset_tallies(mcb200_ctx *c) {
       ck(cudaMemsetAsync(c->y.heat_e, 0, sizeof(long long) * nodes, s), "memset");
       ck(cudaMemsetAsync(c->y.heat_h, 0, sizeof(long long) * nodes, s), "memset");
     }
+    if (c->ib.sum) ck(cudaMemsetAsync(c->ib.sum, 0, 2 * sizeof(double), s), "memset");
     ck(cudaStreamSynchronize(s), "sync");
     return MCB200_OK;
   } catch (const std::exception &e) {
@@ -1266,6 +1279,8 @@ int mcb200_set_device(mcb200_ctx *c, const int32_t *material, const double *dono
     c->cg_plan = CgPlan{};
     c->cg_plan.method = c->cg_method;
     c->cg_plan.blocks = c->cg_blocks;
+    c->node_contact = s.contact_of;
+    c->induced_contact = -1;  // a weighting field belongs to the device it was solved for
     c->device_set = true;
     return MCB200_OK;
   } catch (const std::exception &e) {
@@ -1285,21 +1300,117 @@ int mcb200_deposit(mcb200_ctx *c) {
   }
 }
 
+// Cooperative launches of different contexts run one after another on the
+// device (two partly resident cooperative grids could wait on each other):
+// each solve waits for the device's last one and becomes the last one.  The
+// chain is per device and process; hold the lock while enqueueing.
+static std::mutex coop_chain_mutex;
+static cudaEvent_t &coop_chain_event(int device) {
+  static cudaEvent_t chain[64] = {};
+  cudaEvent_t &last = chain[device & 63];
+  if (!last) ck(cudaEventCreateWithFlags(&last, cudaEventDisableTiming), "cudaEventCreate");
+  return last;
+}
+
 int mcb200_solve_poisson(mcb200_ctx *c, double rel_tol, int max_iter, int *iterations, double *rel_residual) {
   if (!c || rel_tol <= 0 || max_iter < 0) return MCB200_ERR_ARG;
   if (!c->device_set) return fail(c, MCB200_ERR_STATE, "mcb200_solve_poisson needs mcb200_set_device");
   try {
     ck(cudaSetDevice(c->device), "cudaSetDevice");
-    // cooperative launches of different contexts run one after another on the
-    // device (see poisson_enqueue); the chain is per device and process
-    static std::mutex chain_mutex;
-    static cudaEvent_t chain[64] = {};
-    std::lock_guard<std::mutex> lock(chain_mutex);
-    cudaEvent_t &last = chain[c->device & 63];
-    if (!last) ck(cudaEventCreateWithFlags(&last, cudaEventDisableTiming), "cudaEventCreate");
+    std::lock_guard<std::mutex> lock(coop_chain_mutex);
+    cudaEvent_t &last = coop_chain_event(c->device);
     ck(cudaStreamWaitEvent(c->stream, last, 0), "wait");
     poisson_enqueue(c, c->stream, rel_tol, max_iter, iterations, rel_residual);
     ck(cudaEventRecord(last, c->stream), "event");
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_set_induced_current(mcb200_ctx *c, int contact) {
+  if (!c) return MCB200_ERR_ARG;
+  if (!c->device_set) return fail(c, MCB200_ERR_STATE, "mcb200_set_induced_current needs mcb200_set_device");
+  if (contact < 0) {
+    c->induced_contact = -1;
+    return MCB200_OK;
+  }
+  const size_t nodes = c->node_contact.size(), cells = (size_t)c->ncells;
+  if (std::find(c->node_contact.begin(), c->node_contact.end(), (int8_t)contact) == c->node_contact.end())
+    return fail(c, MCB200_ERR_ARG, "mcb200_set_induced_current: no node of that contact");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    cudaStream_t s = c->stream;
+    // Laplace's equation on the device's stencil: 1 on the contact's nodes,
+    // 0 on every other contact, no charge, no doping, no built-in potential
+    std::vector<double> bc(nodes, 0.0);
+    for (size_t p = 0; p < nodes; ++p) bc[p] = c->node_contact[p] == contact ? 1.0 : 0.0;
+    std::vector<void *> tmp;
+    struct Free {
+      std::vector<void *> &v;
+      ~Free() { for (void *p : v) cudaFree(p); }
+    } release{tmp};
+    FieldBuffers w = c->fb;
+    double *zero = dalloc<double>(nodes, tmp);
+    ck(cudaMemsetAsync(zero, 0, nodes * sizeof(double), s), "memset");
+    w.bc_vapp = dupload(bc, tmp);
+    w.bc_phims = w.vadd = w.pdop = w.density = zero;
+    w.potential = dalloc<double>(nodes, tmp);
+    ck(cudaMemsetAsync(w.potential, 0, nodes * sizeof(double), s), "memset");
+    w.rhs = dalloc<double>(nodes, tmp);
+    w.poisson_stats = dalloc<double>(3, tmp);
+    ck(cudaMemsetAsync(w.poisson_stats, 0, 3 * sizeof(double), s), "memset");
+    CgPlan plan = c->cg_plan;
+    launch_rhs((int)nodes, w, s);
+    int its = 0;
+    double res = 0;
+    {
+      std::lock_guard<std::mutex> lock(coop_chain_mutex);
+      cudaEvent_t &last = coop_chain_event(c->device);
+      ck(cudaStreamWaitEvent(s, last, 0), "wait");
+      if (cg_prepare(c->mesh, w, 1e-12, s, plan) || cg_launch(c->mesh, w, 50000, s, plan))
+        throw CudaError("weighting-potential solve failed");
+      ck(cudaEventRecord(last, s), "event");
+    }
+    if (cg_finish(c->mesh, w, s, c->h_scratch, &its, &res)) throw CudaError("weighting-potential solve failed");
+    if (!(res <= 1e-10)) return fail(c, MCB200_ERR_STATE, "weighting-potential solve did not converge");
+    if (!c->induced_field) c->induced_field = dalloc<double>(cells * 3, c->mesh_owned);
+    DevMesh m = c->mesh;
+    m.hfield = c->induced_field;            // E_w = -grad phi_w (the hole-felt sign)
+    m.efield = dalloc<double>(cells * 3, tmp);
+    launch_pot2field(m, w.potential, s);
+    ck(cudaGetLastError(), "weighting field");
+    std::vector<double> h(cells * 3);
+    ck(cudaMemcpyAsync(h.data(), c->induced_field, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s), "copy");
+    ck(cudaStreamSynchronize(s), "sync");
+    double emax = 0;
+    for (double v : h) emax = std::max(emax, std::fabs(v));
+    if (!c->ib.sum) {
+      c->ib.bounds = dalloc<unsigned long long>(4, c->mesh_owned);
+      c->ib.acc = dalloc<long long>(1, c->mesh_owned);
+      c->ib.sum = dalloc<double>(2, c->mesh_owned);
+      ck(cudaMemsetAsync(c->ib.acc, 0, sizeof(long long), s), "memset");
+    }
+    ck(cudaMemsetAsync(c->ib.sum, 0, 2 * sizeof(double), s), "memset");
+    c->ib.field = c->induced_field;
+    c->ib.vmax = std::max(c->ts->vmax, 1e-300);
+    c->ib.emax = std::max(emax, 1e-300);
+    c->induced_contact = contact;
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_get_induced_current(mcb200_ctx *c, double *sum, double *steps) {
+  if (!c || !sum) return MCB200_ERR_ARG;
+  if (c->induced_contact < 0) return fail(c, MCB200_ERR_STATE, "no weighting field (mcb200_set_induced_current)");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    ck(cudaMemcpyAsync(c->h_scratch + 13, c->ib.sum, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy");
+    ck(cudaStreamSynchronize(c->stream), "sync");
+    *sum = c->h_scratch[13];
+    if (steps) *steps = c->h_scratch[14];
     return MCB200_OK;
   } catch (const std::exception &e) {
     return fail(c, MCB200_ERR_CUDA, e.what());
@@ -1722,6 +1833,7 @@ int mcb200_get_array(mcb200_ctx *c, const char *name, double *out, size_t n) {
   else if (c->device_set && nm == "rhs") { src = c->fb.rhs; len = nodes; }
   else if (c->device_set && nm == "potential") { src = c->fb.potential; len = nodes; }
   else if (c->qc_set && nm == "qc_potential") { src = c->qc_pot; len = nodes; }
+  else if (c->induced_contact >= 0 && nm == "induced_field") { src = c->induced_field; len = 3 * cells; }
   else if (c->device_set && nm == "stencil") { src = c->fb.stencil; len = 7 * nodes; }
   else return fail(c, MCB200_ERR_ARG, "unknown array " + nm);
   if (n < len) return fail(c, MCB200_ERR_CAPACITY, "output smaller than array " + nm);
@@ -1802,11 +1914,60 @@ void surface_rates_enqueue(mcb200_ctx *c, cudaStream_t s) {
   c->launches += 1;
 }
 
-// Before the flights of a step: work counters, the FP32 per-cell records,
-// and zeroed copy counters of every generation and of the sink.
+// What the flight reads that no earlier kernel of the step has touched --
+// the tetrahedron records, the per-cell motion rules, contacts and surface
+// flags, for FP64 flight the cell fields and doping (FP32 flight reads the
+// per-cell records written just before it), and the store's k and uid
+// arrays (the statistics and the deposition read the rest of the store) --
+// is fetched into L2 by the copy engine before the flight starts, instead
+// of by the first lane that misses on each line.
+// with_tables == false leaves out the band tables (a batched step fetches
+// the tables its members share once).
 template <typename R>
-void step_prepare(mcb200_ctx *c) {
+void prefetch_flight_tables(mcb200_ctx *c, cudaStream_t s, bool with_tables) {
+  const DevTables &T = c->ts->dt;
+  const DevMesh &M = c->mesh;
+  const size_t cells = (size_t)c->ncells;
+  L2Ranges r{};
+  auto add = [&](const void *p, size_t bytes) {
+    if (p && bytes && r.n < L2Ranges::kMax) {
+      r.p[r.n] = p;
+      r.bytes[r.n] = bytes;
+      ++r.n;
+    }
+  };
+  if (with_tables) add(sizeof(R) == 4 ? (const void *)T.f32.tf : (const void *)T.tf,
+                       (size_t)T.nt * (sizeof(R) == 4 ? sizeof(TetFlightT<float>) : sizeof(TetFlightT<double>)));
+  if constexpr (sizeof(R) == 8) {
+    add(M.efield, cells * 3 * sizeof(double));
+    add(M.hfield, cells * 3 * sizeof(double));
+    add(M.da, cells * sizeof(double));
+  }
+  add(M.motion, cells * 6 * sizeof(int));
+  add(M.contact, cells * sizeof(int));
+  add(M.in_surf, cells * sizeof(int));
+  const DevParticlesT<R> P = store<R>(c, c->cur);
+  const size_t n = std::min(c->n, c->capacity);  // the last count read back: a hint, not a bound
+  add(P.kx, n * sizeof(R));
+  add(P.ky, n * sizeof(R));
+  add(P.kz, n * sizeof(R));
+  add(P.uid, n * sizeof(uint32_t));
+  launch_l2_prefetch(r, c->sm_count, s);
+  c->launches += 1;
+}
+
+// Before the flights of a step: the L2 prefetch above, work counters, the
+// FP32 per-cell records, and zeroed copy counters of every generation and
+// of the sink.
+template <typename R>
+void step_prepare(mcb200_ctx *c, bool prefetch_tables) {
   cudaStream_t s = c->stream;
+  prefetch_flight_tables<R>(c, s, prefetch_tables);
+  if (c->induced_contact >= 0) {  // the induced current of the store the step starts from
+    launch_induced_current(store<R>(c, c->cur), DevCount{c->dev_counts, nullptr, (int)c->capacity}, c->mesh,
+                           c->ts->dt, c->ib, grid_for(c, c->capacity, 256), s);
+    c->launches += 3;
+  }
   join_stat(c);  // the flights change the store the statistics read
   StepCounters z{c->tickets, {}};
   for (int g = 0; g < mcb200_ctx::kGenerations; ++g) z.count[g] = children<R>(c, g).count;
@@ -1865,7 +2026,7 @@ void step_impl(mcb200_ctx *c, uint32_t step, uint64_t seed, double dt) {
     c->ev_pending[q] = true;
     ck(cudaEventRecord(ev[0], s), "event");
   }
-  step_prepare<R>(c);
+  step_prepare<R>(c, true);
   // 1. main flight; copies go to generation 0
   F.C = children<R>(c, 0);
   if (ev) ck(cudaEventRecord(ev[1], s), "event");
@@ -1898,8 +2059,20 @@ void step_impl(mcb200_ctx *c, uint32_t step, uint64_t seed, double dt) {
   }
 }
 
-template void step_prepare<float>(mcb200_ctx *);
-template void step_prepare<double>(mcb200_ctx *);
+template <typename R>
+void prefetch_band_tables(mcb200_ctx *c, cudaStream_t s) {
+  const DevTables &T = c->ts->dt;
+  L2Ranges r{};
+  r.p[0] = sizeof(R) == 4 ? (const void *)T.f32.tf : (const void *)T.tf;
+  r.bytes[0] = (size_t)T.nt * (sizeof(R) == 4 ? sizeof(TetFlightT<float>) : sizeof(TetFlightT<double>));
+  r.n = r.p[0] ? 1 : 0;
+  launch_l2_prefetch(r, c->sm_count, s);
+}
+
+template void step_prepare<float>(mcb200_ctx *, bool);
+template void step_prepare<double>(mcb200_ctx *, bool);
+template void prefetch_band_tables<float>(mcb200_ctx *, cudaStream_t);
+template void prefetch_band_tables<double>(mcb200_ctx *, cudaStream_t);
 template void step_tail<float>(mcb200_ctx *);
 template void step_tail<double>(mcb200_ctx *);
 

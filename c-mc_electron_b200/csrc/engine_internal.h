@@ -226,6 +226,11 @@ struct mcb200_ctx {
   SurfaceRateParams surf_q{};
   int stat_steps = 0;
   bool stat_open = false;
+  // induced (Ramo-Shockley) current of one contact (mcb200_set_induced_current)
+  std::vector<int8_t> node_contact;  // host: the contact of each Dirichlet node, -1 elsewhere
+  int induced_contact = -1;
+  double *induced_field = nullptr;   // [cells][3] weighting field (mesh_owned)
+  InducedBuffers ib{};               // the per-step tally (bounds, fixed-point step sum, FP64 running sum)
   // device-resident counts: the step path never waits for them; `n` and
   // `next_uid` above are host copies, valid while !n_stale
   unsigned int *dev_counts = nullptr;         // [0] particles, [1] next uid, [2] store-full flag
@@ -309,8 +314,12 @@ void poisson_finish(mcb200_ctx *c, cudaStream_t s, int *iterations, double *rel_
 void surface_rates_enqueue(mcb200_ctx *c, cudaStream_t s);
 void deposit_enqueue(mcb200_ctx *c, cudaStream_t s);
 // The parts of a transport step around its flights (engine.cu).
+// prefetch_tables: also fetch the band tables the flight reads into L2 (a
+// batched step fetches its members' shared tables once, prefetch_band_tables).
 template <typename R>
-void step_prepare(mcb200_ctx *c);
+void step_prepare(mcb200_ctx *c, bool prefetch_tables);
+template <typename R>
+void prefetch_band_tables(mcb200_ctx *c, cudaStream_t s);
 template <typename R>
 void step_tail(mcb200_ctx *c);
 

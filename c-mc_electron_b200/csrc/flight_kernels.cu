@@ -607,6 +607,30 @@ int launch_batch_flight(const FlightCtxT<R> &F, const BatchInstT<R> *inst, int n
   kernel<<<per_sm * sm_count, kFlightThreads, smem, s>>>(F, inst, ninst, members, steps, ticket);
   return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
+__global__ void l2_prefetch_kernel(L2Ranges r) {
+  constexpr size_t kPiece = 16384;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (int k = 0; k < r.n; ++k) {
+    const char *base = static_cast<const char *>(r.p[k]);
+    const size_t bytes = r.bytes[k] & ~(size_t)15;
+    const size_t pieces = (bytes + kPiece - 1) / kPiece;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < pieces; q += stride) {
+      const size_t off = q * kPiece;
+      const unsigned size = (unsigned)(bytes - off < kPiece ? bytes - off : kPiece);
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(base + off), "r"(size) : "memory");
+    }
+  }
+}
+void launch_l2_prefetch(const L2Ranges &r, int grid, cudaStream_t s) {
+  L2Ranges ok{};  // a range that does not start on a 16-byte boundary is left out (the copy engine needs it)
+  for (int k = 0; k < r.n && k < L2Ranges::kMax; ++k)
+    if (r.p[k] && (reinterpret_cast<uintptr_t>(r.p[k]) & 15u) == 0 && r.bytes[k] >= 16) {
+      ok.p[ok.n] = r.p[k];
+      ok.bytes[ok.n] = r.bytes[k];
+      ++ok.n;
+    }
+  if (ok.n > 0) l2_prefetch_kernel<<<grid, 128, 0, s>>>(ok);
+}
 void launch_cell_records32(const DevTables &T, const DevMesh &M, float4 *out, int cells, cudaStream_t s) {
   if (cells > 0) cell_records32_kernel<<<(cells + 255) / 256, 256, 0, s>>>(T, M, out, cells);
 }

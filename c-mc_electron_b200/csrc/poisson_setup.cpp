@@ -27,6 +27,7 @@ PoissonSetup PoissonSetup::build(int nx, int ny, int nz, const double *dx, const
   s.stencil.assign((size_t)nodes * 7, 0.0);
   s.dirichlet.assign(nodes, 0);
   s.bc_vapp.assign(nodes, 0.0);
+  s.contact_of.assign(nodes, -1);
   s.bc_phims.assign(nodes, 0.0);
 
   // init_cell_data, src/mcmodel.cpp:3213-3218: cell volumes
@@ -114,6 +115,7 @@ PoissonSetup PoissonSetup::build(int nx, int ny, int nz, const double *dx, const
           s.dirichlet[p] = 1;
           s.bc_vapp[p] = vapp[pl.contact];
           s.bc_phims[p] = phims[pl.contact];
+          s.contact_of[p] = (int8_t)pl.contact;
         }
   }
   return s;

@@ -28,6 +28,7 @@ struct PoissonSetup {
   std::vector<double> stencil;  // [nodes][7]: -x, +x, -y, +y, -z, +z, diagonal
   std::vector<uint8_t> dirichlet;   // [nodes] contact rows
   std::vector<double> bc_vapp, bc_phims;  // [nodes] the contact's Vapp and PhiMS on Dirichlet rows
+  std::vector<int8_t> contact_of;         // [nodes] the contact of a Dirichlet row, -1 elsewhere
 
   int nodes() const { return (nx + 1) * (ny + 1) * (nz + 1); }
   int node(int i, int j, int k) const { return (j * (nx + 1) + i) * (nz + 1) + k; }

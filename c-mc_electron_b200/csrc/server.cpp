@@ -131,18 +131,26 @@ size_t free_bytes(int device) {
   return f;
 }
 
-// Ids of the last window, then the tallies restart.  Either the drain
-// contact's current (the reference's current_scatter_info: (CharGen -
-// CharCatch) / (dt * steps) * curr0 * 1e-2), or (ids_sections) the net
-// carrier flux through the y node planes (the reference's section_current,
-// (rcurrent - lcurrent) / (dt * steps) * curr0 * 1e-2) averaged over the
-// middle third of the planes: the same steady-state current with far less
-// noise per window, since every crossing of every plane counts.
+// Ids of the last window, then the tallies restart.  MCB200_IDS_CONTACT:
+// the drain contact's current (the reference's current_scatter_info:
+// (CharGen - CharCatch) / (dt * steps) * curr0 * 1e-2).  MCB200_IDS_SECTIONS:
+// the net carrier flux through the y node planes (the reference's
+// section_current, (rcurrent - lcurrent) / (dt * steps) * curr0 * 1e-2)
+// averaged over the middle third of the planes: the same steady-state
+// current with far less noise, since every crossing of every plane counts.
+// MCB200_IDS_INDUCED: the current the drain carries by induction
+// (Ramo-Shockley, summed over every particle at every step): the same
+// steady-state current with the least noise, since every particle's motion
+// counts, not only its crossings.
 int read_window(Slot &s, int steps) {
   std::vector<double> contact(16 * 6), lc(s.info.ny + 1), rc(s.info.ny + 1);
   if (int e = mcb200_get_tallies(s.ctx, nullptr, contact.data(), lc.data(), rc.data(), nullptr, nullptr)) return e;
   double ids = 0;
-  if (s.req.ids_sections) {
+  if (s.req.ids_estimator == MCB200_IDS_INDUCED) {
+    double sum = 0, n = 0;
+    if (int e = mcb200_get_induced_current(s.ctx, &sum, &n)) return e;
+    ids = n > 0 ? sum / n * s.curr0 * 1e-2 : 0.0;
+  } else if (s.req.ids_estimator == MCB200_IDS_SECTIONS) {
     const int ny = s.info.ny, j0 = ny / 3, j1 = std::max(j0 + 1, ny - ny / 3);
     for (int j = j0; j < j1; ++j) ids += rc[j] - lc[j];
     ids = ids / (j1 - j0) / (s.info.dt * steps) * s.curr0 * 1e-2;
@@ -217,7 +225,8 @@ int admit(mcb200_server *v, Slot &s) {
   }
   auto ctx_err = [&](int rc, const char *what) {
     const std::string m = std::string(what) + ": " + errmsg(s.ctx);
-    mcb200_deck_free(deck);
+    if (deck) mcb200_deck_free(deck);
+    deck = nullptr;
     return sfail(v, rc, m);
   };
   if (v->opt.flight_precision)
@@ -247,6 +256,7 @@ int admit(mcb200_server *v, Slot &s) {
     s.warm = s.req.warm_windows_cold;
   }
   mcb200_deck_free(deck);
+  deck = nullptr;  // the error paths below must not free it again
   if (int rc = mcb200_deposit(s.ctx)) return ctx_err(rc, "mcb200_deposit");
   if (s.info.flag_compute_potential) {
     int it = 0;
@@ -255,6 +265,9 @@ int admit(mcb200_server *v, Slot &s) {
   }
   if (s.info.flag_surface_scatter)
     if (int rc = mcb200_surface_rates(s.ctx, &s.surf, s.eeff.data())) return ctx_err(rc, "surface rates");
+  if (s.req.ids_estimator == MCB200_IDS_INDUCED)
+    if (int rc = mcb200_set_induced_current(s.ctx, std::min(std::max(s.req.drain_contact, 0), 15)))
+      return ctx_err(rc, "weighting field");
   mcb200_reset_tallies(s.ctx);
   mcb200_sync(s.ctx);
   mcb200_particle_steps(s.ctx, &s.psteps0);

@@ -2,7 +2,9 @@
 // stat_step steps (MeshQuantities::statistic, src/mcmodel.cpp:1167-1408):
 // per node and carrier type the CIC-weighted |q| v_x, |q| v_y, |q| v_z,
 // |q| and |q| E of every particle, per cell the particle count, and per node
-// the potential; summed over the steps of a statistics window.
+// the potential; summed over the steps of a statistics window.  Also the
+// current one contact carries by induction (Ramo-Shockley, a tally of the
+// transport step): sum over particles of q v . E_w.
 //
 // Node sums are int64 fixed point (order independent).  A window's scales
 // are fixed when it starts, from bounds every sum respects for the whole
@@ -11,6 +13,7 @@
 // largest group-velocity component of the band tables, |E| <= the energy
 // table's top.
 #include "stat_kernels.h"
+#include "field_kernels.h"
 #include "warp_segments.cuh"
 
 namespace mcb200 {
@@ -106,6 +109,42 @@ __global__ void add_potential_kernel(int nodes, const double *pot, double *sum) 
   if (p < nodes) sum[p] += pot[p];
 }
 
+// The fixed-point unit of one step's induced-current terms: sum |q v . E_w|
+// <= (electrons + holes) * max|q| * sqrt(3) vmax * sqrt(3) emax.
+__device__ __forceinline__ double induced_unit(const unsigned long long *b, double vmax, double emax) {
+  const double qmax = fmax(__longlong_as_double((long long)b[0]), __longlong_as_double((long long)b[1]));
+  const double bound = fmax((double)(b[2] + b[3]) * qmax * vmax * emax * 3.0, 1e-300);
+  return ldexp(1.0, 62 - (int)ceil(log2(bound)));
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) induced_current_kernel(DevParticlesT<R> P, DevCount count, DevMesh M,
+                                                              DevTables T, InducedBuffers B) {
+  const int n = count.get();
+  const double unit = induced_unit(B.bounds, B.vmax, B.emax);
+  long long t = 0;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const uint32_t meta = P.meta[p];
+    if (meta & kStatDead) continue;
+    const uint32_t c = P.cell[p];
+    const int i = c & 1023, j = (c >> 10) & 1023, k = (c >> 20) & 1023;
+    double vx, vy, vz;
+    group_velocity(T, P.itet[p], meta & 255, vx, vy, vz);
+    const double *ew = B.field + 3 * (size_t)((j * M.nx + i) * M.nz + k);
+    t += st_fx(P.charge[p] * (vx * ew[0] + vy * ew[1] + vz * ew[2]), unit);
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
+  if ((threadIdx.x & 31u) == 0 && t) st_put(B.acc, t);
+}
+__global__ void induced_finish_kernel(InducedBuffers B) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    B.sum[0] += (double)*B.acc / induced_unit(B.bounds, B.vmax, B.emax);
+    B.sum[1] += 1.0;
+    *B.acc = 0;
+  }
+}
+
 template <typename R>
 void launch_statistic(const DevParticlesT<R> &P, DevCount n, const DevMesh &M, const DevTables &T, const StatScales &S,
                       const StatBuffers &B, int grid, cudaStream_t s) {
@@ -115,6 +154,17 @@ void launch_add_potential(int nodes, const double *pot, double *sum, cudaStream_
   if (nodes > 0 && pot) add_potential_kernel<<<(nodes + 255) / 256, 256, 0, s>>>(nodes, pot, sum);
 }
 
+template <typename R>
+void launch_induced_current(const DevParticlesT<R> &P, DevCount n, const DevMesh &M, const DevTables &T,
+                            const InducedBuffers &B, int grid, cudaStream_t s) {
+  launch_charge_bounds(P, n, B.bounds, grid, s);
+  induced_current_kernel<R><<<grid, 256, 0, s>>>(P, n, M, T, B);
+  induced_finish_kernel<<<1, 32, 0, s>>>(B);
+}
+template void launch_induced_current<double>(const DevParticlesT<double> &, DevCount, const DevMesh &,
+                                             const DevTables &, const InducedBuffers &, int, cudaStream_t);
+template void launch_induced_current<float>(const DevParticlesT<float> &, DevCount, const DevMesh &,
+                                            const DevTables &, const InducedBuffers &, int, cudaStream_t);
 template void launch_statistic<double>(const DevParticlesT<double> &, DevCount, const DevMesh &, const DevTables &,
                                        const StatScales &, const StatBuffers &, int, cudaStream_t);
 template void launch_statistic<float>(const DevParticlesT<float> &, DevCount, const DevMesh &, const DevTables &,

@@ -29,6 +29,7 @@ FLAG_SURFACE_SCATTER = 1
 FLAG_SURFACE_IMPURITY = 2
 FLAG_HEAT = 4
 FLAG_QUANTUM = 8
+IDS_CONTACT, IDS_SECTIONS, IDS_INDUCED = 0, 1, 2  # serving's Ids estimators (MCB200_IDS_*)
 FLIGHT_FP64 = 0
 FLIGHT_FP32 = 1
 # Poisson preconditioners (mcb200_set_poisson_solver)
@@ -106,7 +107,7 @@ class Request(ctypes.Structure):
                 ("target_rel_err", ctypes.c_double), ("min_windows", ctypes.c_int), ("max_steps", ctypes.c_int),
                 ("warm_windows_cold", ctypes.c_int), ("warm_windows_warm", ctypes.c_int),
                 ("warm_start", ctypes.c_int), ("poisson_every", ctypes.c_int), ("drain_contact", ctypes.c_int),
-                ("ids_sections", ctypes.c_int), ("seed", ctypes.c_uint64), ("arrival_s", ctypes.c_double)]
+                ("ids_estimator", ctypes.c_int), ("seed", ctypes.c_uint64), ("arrival_s", ctypes.c_double)]
 
 
 class Result(ctypes.Structure):
@@ -236,6 +237,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mcb200_elapsed_ms.argtypes = [vp, c.c_int, c.c_int, dp]
     lib.mcb200_stat_accumulate.argtypes = [vp]
     lib.mcb200_stat_get.argtypes = [vp, c.c_char_p, dp, c.c_size_t]
+    lib.mcb200_set_induced_current.argtypes = [vp, c.c_int]
+    lib.mcb200_get_induced_current.argtypes = [vp, dp, dp]
     lib.mcb200_set_potential.argtypes = [vp, dp]
     lib.mcb200_set_potentials.argtypes = [vp, dp, dp]
     lib.mcb200_set_quantum_correction.argtypes = [vp, vp, i32p, i32p, c.c_int]
@@ -470,7 +473,8 @@ class Engine:
 
     def array(self, name: str) -> np.ndarray:
         m = self.mesh
-        per = {"rho": m.ncells, "efield": 3 * m.ncells, "hfield": 3 * m.ncells, "cell_charge_e": m.ncells,
+        per = {"rho": m.ncells, "efield": 3 * m.ncells, "hfield": 3 * m.ncells, "induced_field": 3 * m.ncells,
+               "cell_charge_e": m.ncells,
                "cell_charge_h": m.ncells, "cell_volume": m.ncells, "stencil": 7 * m.nnodes,
                "e_rough": m.ncells, "e_phonon": m.ncells, "h_rough": m.ncells, "h_phonon": m.ncells}
         out = np.zeros(per.get(name, m.nnodes))
@@ -562,6 +566,33 @@ class Engine:
 
     def reset_tallies(self):
         self._check(self._lib.mcb200_reset_tallies(self._ctx), "reset_tallies")
+
+    def set_induced_current(self, contact: int):
+        """Weighting field of `contact` (Ramo-Shockley); every transport
+        step then tallies the current it carries by induction."""
+        self._check(self._lib.mcb200_set_induced_current(self._ctx, int(contact)), "set_induced_current")
+
+    def induced_current(self) -> tuple:
+        """(sum over steps of sum_i q v . E_w, steps) since the last reset."""
+        s, n = ctypes.c_double(), ctypes.c_double()
+        self._check(self._lib.mcb200_get_induced_current(self._ctx, ctypes.byref(s), ctypes.byref(n)),
+                    "get_induced_current")
+        return s.value, n.value
+
+    def stat_begin(self, window_steps: int):
+        self._check(self._lib.mcb200_stat_begin(self._ctx, int(window_steps)), "stat_begin")
+
+    def stat_accumulate(self):
+        self._check(self._lib.mcb200_stat_accumulate(self._ctx), "stat_accumulate")
+
+    def stat(self, name: str, n: int = 0) -> np.ndarray:
+        """A window sum (mcb200_stat_get); n: entries (default: per node,
+        1 for "steps", per cell for "cell_count")."""
+        if not n:
+            n = 1 if name == "steps" else (self.mesh.ncells if name == "cell_count" else self.mesh.nnodes)
+        out = np.zeros(n)
+        self._check(self._lib.mcb200_stat_get(self._ctx, name.encode(), _ptr(out, ctypes.c_double), n), name)
+        return out
 
 
 class Batch:
@@ -687,11 +718,11 @@ class Server:
 
     def submit(self, input_path: str, family: str, bias, seed: int, target_rel_err: float = 0.01,
                min_windows: int = 5, max_steps: int = 0, warm_windows_cold: int = 10, warm_windows_warm: int = 1,
-               warm_start: bool = True, poisson_every: int = 0, drain_contact: int = 1, ids_sections: bool = False,
+               warm_start: bool = True, poisson_every: int = 0, drain_contact: int = 1, ids_estimator: int = 0,
                arrival_s=None) -> int:
         req = Request(os.fspath(input_path).encode(), family.encode(), (ctypes.c_double * 2)(*bias), target_rel_err,
                       min_windows, max_steps, warm_windows_cold, warm_windows_warm, int(warm_start), poisson_every,
-                      drain_contact, int(ids_sections), seed, self.now() if arrival_s is None else arrival_s)
+                      drain_contact, int(ids_estimator), seed, self.now() if arrival_s is None else arrival_s)
         rid = ctypes.c_uint64()
         self._check(self._lib.mcb200_server_submit(self._s, ctypes.byref(req), ctypes.byref(rid)),
                     "mcb200_server_submit")

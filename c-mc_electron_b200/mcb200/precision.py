@@ -109,6 +109,148 @@ def sweep(electrons: int = 100000, warmup: int = 300, blocks: int = 5, block_ste
     return rows
 
 
+# ---------------------------------------------------------------- FinFET
+# The self-consistent n-FinFET of the throughput workload (decks.finfet at
+# its defaults: 511,200 carriers, Vd 0.7 V, Vg 0.8 V, dt 0.2 fs, surface
+# scattering), run from its equilibrium start through FINFET_WARMUP steps,
+# then FINFET_WINDOWS windows of FINFET_WINDOW_STEPS steps.  Per step, as
+# the reference's density() orders it: statistics, deposition (the Poisson
+# solve every FINFET_POISSON_EVERY steps), surface rates, the carrier step;
+# MultipleRefresh every 50 steps.  Phonon events tally heat throughout.
+# Per window: the drain and source contact currents (the reference's
+# `Current = ` of current_scatter_info, A), the section current through the
+# middle third of the y planes (A), the electrons' mean y velocity (m/s) and
+# mean energy (eV) from the statistic() sums, and the heat the carriers give
+# the lattice (eV per step).
+FINFET_WARMUP = 300
+FINFET_WINDOWS = 8
+FINFET_WINDOW_STEPS = 100
+FINFET_POISSON_EVERY = 10
+FINFET_MR_STEP = 50
+FINFET_OBSERVABLES = ("drain_current_a", "source_current_a", "section_current_a", "drift_velocity_y_m_s",
+                      "mean_energy_ev", "heat_ev_per_step")
+
+
+def finfet_observables(window: dict, u: dict, dt: float, steps: int, ny: int) -> dict:
+    """Window observables from its sums: contact tallies [contact][6]
+    (NumParGen, CharGen, EnergyGen, NumParCatch, CharCatch, EnergyCatch),
+    section currents lcurrent / rcurrent [ny + 1], the statistic() sums of
+    the electrons (q, qvy, qe; summed over nodes) and the heat tallies
+    (summed over nodes and carriers), all in the reference's normalised
+    units.  The same function reads the engine's and the oracle's sums."""
+    c = window["contact"]
+    cur = lambda k: (c[k][1] - c[k][4]) / (dt * steps) * u["curr0"] * 1e-2
+    lo, hi = ny // 3, 2 * ny // 3 + 1
+    sec = (np.asarray(window["rcurrent"]) - np.asarray(window["lcurrent"]))[lo:hi].mean() / (dt * steps) * u["curr0"]
+    q = window["electron_q"]
+    return {"drain_current_a": cur(1), "source_current_a": cur(0), "section_current_a": float(sec),
+            "drift_velocity_y_m_s": window["electron_qvy"] / q * u["spr0"] / u["time0"],
+            "mean_energy_ev": window["electron_qe"] / q * u["eV0"],
+            "heat_ev_per_step": window["heat"] * u["eV0"] / steps}
+
+
+def run_finfet(precision: int, seed: int = 1, warmup: int = FINFET_WARMUP, windows: int = FINFET_WINDOWS,
+               window_steps: int = FINFET_WINDOW_STEPS, device: int = 0) -> dict:
+    """The FinFET protocol above on the GPU; returns the per-window
+    observables and run totals."""
+    import tempfile
+
+    from . import Deck, Engine, decks
+
+    with tempfile.TemporaryDirectory() as tmp:
+        d = decks.finfet(tmp, total_step=warmup + windows * window_steps, heat_steps=0, compute_heat=False,
+                         mr_step=FINFET_MR_STEP)
+        deck = Deck(d["input"])
+        root = Engine(max_particles=1, precision=precision, device=device)
+        deck.prepare(root)
+        carriers = int(deck.int_array("electron_num").sum() + deck.int_array("hole_num").sum())
+        eng = Engine(max_particles=2 * carriers + 65536, precision=precision, device=device, like=root)
+        deck.apply(eng)
+        deck.seed(eng, seed)
+        info = deck.info()
+        eeff = deck.int_array("eeff_direction")
+        refresh = (deck.int_array("refresh_electrons"), deck.int_array("refresh_holes"))
+        deck.close()
+    surf = dict(delta_m=0.4e-9, ail_m=1.5e-9, roughness=info["flag_surface_roughness"],
+                phonon=info["flag_surface_phonon"])
+    eng.set_refresh_targets(*refresh)
+    eng._check(lib().mcb200_set_heat_tally(eng._ctx, 1), "mcb200_set_heat_tally")
+    u = eng.units()
+    dt = info["dt"]
+    m = eng.mesh
+    nodes = m.nnodes
+    step = 0
+
+    def advance(n):
+        nonlocal step
+        for _ in range(n):
+            eng._check(lib().mcb200_stat_accumulate(eng._ctx), "mcb200_stat_accumulate")
+            eng.deposit()
+            if step % FINFET_POISSON_EVERY == 0:
+                eng.solve_poisson_async(1e-10, 20000)
+            eng.surface_rates(eeff, **surf)
+            eng.step(step, seed, dt)
+            if step % FINFET_MR_STEP == FINFET_MR_STEP - 1:
+                eng.multiple_refresh(*refresh, step, seed, wait=False)
+            step += 1
+
+    eng.deposit()
+    eng.solve_poisson(1e-10, 20000)
+    eng._check(lib().mcb200_stat_begin(eng._ctx, max(warmup, 1)), "mcb200_stat_begin")
+    advance(warmup)
+    rows = []
+    for _ in range(windows):
+        eng.reset_tallies()
+        eng._check(lib().mcb200_stat_begin(eng._ctx, window_steps), "mcb200_stat_begin")
+        advance(window_steps)
+        t = eng.tallies()
+        w = {"contact": t["contact"][:info["n_contacts"]].tolist(), "lcurrent": t["lcurrent"].tolist(),
+             "rcurrent": t["rcurrent"].tolist(), "electron_q": float(_stat(eng, "electron_q", nodes).sum()),
+             "electron_qvy": float(_stat(eng, "electron_qvy", nodes).sum()),
+             "electron_qe": float(_stat(eng, "electron_qe", nodes).sum()),
+             "heat": float(t["heat_e"].sum() + t["heat_h"].sum())}
+        rows.append(finfet_observables(w, u, dt, window_steps, m.ny))
+    t = eng.tallies()
+    out = {"precision": "fp32" if precision == FLIGHT_FP32 else "fp64", "windows": rows,
+           "particles_end": eng.num_particles(), "no_tet": t["no_tet"], "zero_time": t["zero_time"],
+           "caught": t["caught"]}
+    eng.close()
+    root.close()
+    return out
+
+
+def compare_windows(ref: list, test: list) -> dict:
+    """Per observable: relative error of the test run's mean over the windows
+    against the reference run's, and that difference in standard errors.
+    The runs follow the same protocol from statistically equivalent starts
+    on independent random streams, so window w of one run and window w of
+    the other estimate the same transient value: the error is the mean of
+    the window-by-window differences and its standard error theirs (the
+    transient's drift cancels in each difference)."""
+    out = {}
+    for key in FINFET_OBSERVABLES:
+        a = np.array([w[key] for w in ref])
+        b = np.array([w[key] for w in test])
+        diff = b - a
+        se = float(diff.std(ddof=1) / np.sqrt(len(diff)))
+        d = float(diff.mean())
+        out[key] = {"ref": float(a.mean()), "test": float(b.mean()),
+                    "rel_error": d / abs(a.mean()) if a.mean() else 0.0, "sigmas": d / se if se > 0 else 0.0}
+    return out
+
+
+def finfet_report(seed: int = 1, device: int = 0, oracle_windows: list | None = None) -> dict:
+    """FP32 flight against all-FP64 flight on the FinFET (and both against
+    the reference's own windows when given)."""
+    r64 = run_finfet(FLIGHT_FP64, seed=seed, device=device)
+    r32 = run_finfet(FLIGHT_FP32, seed=seed, device=device)
+    rep = {"fp64": r64, "fp32": r32, "fp32_vs_fp64": compare_windows(r64["windows"], r32["windows"])}
+    if oracle_windows:
+        rep["fp64_vs_oracle"] = compare_windows(oracle_windows, r64["windows"])
+        rep["fp32_vs_oracle"] = compare_windows(oracle_windows, r32["windows"])
+    return rep
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--electrons", type=int, default=100000)

@@ -163,6 +163,25 @@ int mcb200_solve_poisson(mcb200_ctx *ctx, double rel_tol, int max_iter, int *ite
  * optionally reset) here. */
 int mcb200_poisson_stats(mcb200_ctx *ctx, int64_t *solves, int64_t *iterations, double *max_rel_residual, int reset);
 
+/* No counterpart in the reference (which counts particles crossing the
+ * contact planes, current_scatter_info).  The current contact `contact`
+ * (0-based, deck order) carries by induction, Ramo-Shockley: the weighting
+ * potential of the contact (Laplace's equation on the device's Poisson
+ * stencil, 1 on its nodes and 0 on every other contact) is solved once
+ * here and its cell field E_w kept ("induced_field" of mcb200_get_array);
+ * from then on every transport step (mcb200_step, batched steps) starts by
+ * adding the sum over particles of q v . E_w (v the group velocity) to a
+ * tally.  mcb200_get_induced_current returns that tally since the last
+ * mcb200_reset_tallies and the number of steps it covers: sum / steps *
+ * curr0 * 1e-2 (mcb200_units) is in the unit and sign of the reference's
+ * `Current = `, and its time average is the contact's terminal current,
+ * with far less noise per step than the catch / generate balance.  The
+ * particle terms are summed in fixed point, so the tally does not depend
+ * on the store's order.  contact < 0 switches it off; MCB200_ERR_STATE
+ * before mcb200_set_device. */
+int mcb200_set_induced_current(mcb200_ctx *ctx, int contact);
+int mcb200_get_induced_current(mcb200_ctx *ctx, double *sum, double *steps);
+
 #define MCB200_POISSON_AUTO 0      /* multigrid when the mesh has a hierarchy, else Jacobi */
 #define MCB200_POISSON_JACOBI 1    /* Jacobi-preconditioned CG */
 #define MCB200_POISSON_MULTIGRID 2 /* V-cycle-preconditioned CG */
@@ -240,7 +259,9 @@ int mcb200_quantum_potential(mcb200_ctx *ctx, const double *potential, double *o
  * "h_phonon", "efield", "hfield" (3 per cell),
  * "cell_charge_e", "cell_charge_h", "cell_volume" (per cell);
  * "node_density", "node_volume", "node_doping", "vadd", "rhs", "potential"
- * (per node); "stencil" (7 per node). */
+ * (per node); "stencil" (7 per node); "qc_potential" (per node, with a
+ * quantum set-up); "induced_field" (3 per cell, after
+ * mcb200_set_induced_current: the weighting field E_w). */
 int mcb200_get_array(mcb200_ctx *ctx, const char *name, double *out, size_t n);
 
 #define MCB200_FLAG_SURFACE_SCATTER 1   /* Flag_SurfaceScatter */
@@ -647,11 +668,18 @@ typedef struct {
   int warm_start;            /* start from the nearest converged bias of the family, and keep this one */
   int poisson_every;         /* 0: the deck's poisson_step */
   int drain_contact;         /* 0-based contact whose current is Ids */
-  int ids_sections;          /* 1: Ids from the net flux through the middle third of the y planes (section
-                                currents) instead of the contact's generate / catch balance */
+  int ids_estimator;         /* MCB200_IDS_*: how a window's Ids is measured */
   uint64_t seed;
   double arrival_s;          /* arrival time on the server clock (mcb200_server_now), for latency */
 } mcb200_request;
+/* Ids estimators of a request window: the drain contact's generate / catch
+ * balance (the reference's `Current = `), the net flux through the middle
+ * third of the y planes (its section currents), or the current the drain
+ * carries by induction (Ramo-Shockley, mcb200_set_induced_current): all
+ * estimate the same steady-state current, with decreasing noise per window. */
+#define MCB200_IDS_CONTACT 0
+#define MCB200_IDS_SECTIONS 1
+#define MCB200_IDS_INDUCED 2
 #define MCB200_SERVE_CONVERGED 1
 #define MCB200_SERVE_STEP_LIMIT 2
 typedef struct {

@@ -24,15 +24,17 @@
  * (src/mcmodel.cpp:1460-1505) then flies that copy or not depending on cell
  * iteration order.  The engine defines one behaviour: the copy finishes the
  * rest of its step in the same step, drawing from stream
- * sub' = sub * 16 + 1 + k for the k-th copy made by a particle, and gets a
- * permanent uid afterwards in (parent uid, sub') order.  orc_flight_step
- * applies exactly that rule to the reference routines.
+ * sub' = sub * 16 + 1 + k for the k-th copy made by a particle, and, if it
+ * survives that flight, gets a permanent uid afterwards in (parent uid,
+ * sub') order.  orc_flight_step applies exactly that rule to the reference
+ * routines.
  */
 #include <assert.h>
 #include <libgen.h>
 #include <math.h>
 #include <string.h>
 #include <time.h>
+#include <sys/stat.h>
 #include <unistd.h>
 #include <algorithm>
 #include <fstream>
@@ -210,6 +212,11 @@ int orc_set_scalar(const char *name, double v) {
   if (n == "dt") { g_mq->dt = v; return 0; }
   if (n == "flag_quantum_correction") { g_mq->Flag_QuantumCorrection = v != 0; return 0; }
   if (n == "step") { g_mq->step = (int)v; return 0; }
+  if (n == "stat_step") { g_mq->stat_step = (int)v; return 0; }
+  /* surface-roughness delta and correlation length (normalised lengths),
+   * set by the reference's scaling() from constants (src/mcmodel.cpp:4107-4108) */
+  if (n == "SurfSc_delta") { g_mq->SurfSc_delta = v; return 0; }
+  if (n == "SurfSc_ail") { g_mq->SurfSc_ail = v; return 0; }
   return 1;
 }
 
@@ -243,6 +250,23 @@ static Epetra_Vector *cell_vec(const std::string &n) {
   if (n == "p_dop") return mq->p_dop;
   if (n == "p_volume") return mq->p_volume;
   if (n == "p_vadd") return mq->p_vadd;
+  /* statistic() sums (src/mcmodel.cpp:1167-1408) */
+  if (n == "stat_vxE") return mq->stat_vxE;
+  if (n == "stat_vyE") return mq->stat_vyE;
+  if (n == "stat_vzE") return mq->stat_vzE;
+  if (n == "stat_vxH") return mq->stat_vxH;
+  if (n == "stat_vyH") return mq->stat_vyH;
+  if (n == "stat_vzH") return mq->stat_vzH;
+  if (n == "stat_chargeE") return mq->stat_chargeE;
+  if (n == "stat_chargeH") return mq->stat_chargeH;
+  if (n == "stat_energyE") return mq->stat_energyE;
+  if (n == "stat_energyH") return mq->stat_energyH;
+  if (n == "stat_pot") return mq->stat_pot;
+  if (n == "stat_qc_pot") return mq->stat_qc_pot;
+  if (n == "stat_ec") return mq->stat_ec;
+  if (n == "stat_enum") return mq->stat_enum;
+  if (n == "stat_e_heat") return mq->stat_e_heat;
+  if (n == "stat_h_heat") return mq->stat_h_heat;
   return nullptr;
 }
 static Epetra_IntVector *cell_ivec(const std::string &n) {
@@ -508,6 +532,72 @@ int orc_multiple_refresh(uint32_t step) {
   return mq->mr_gen_num;
 }
 
+/* statistic() (src/mcmodel.cpp:1167-1408): one step's sums added to the
+ * stat_* vectors; set_stat_zero() (:715-750) clears them with the tallies. */
+int orc_statistic() {
+  g_mq->statistic();
+  return 0;
+}
+int orc_set_stat_zero() {
+  g_mq->set_stat_zero();
+  return 0;
+}
+
+/* The reference's window outputs for step `step`: output_stat (with
+ * current_scatter_info, src/mcmodel.cpp:971-1161, :756-842) and
+ * output_for_restart (:895-965), written under <dir>/data/ as the reference
+ * writes them under ./data/ (the working directory is restored). */
+int orc_write_outputs(const char *dir, int step) {
+  char saved_cwd[4096];
+  if (!getcwd(saved_cwd, sizeof(saved_cwd))) return 1;
+  if (chdir(dir) != 0) return 1;
+  mkdir("data", 0755);
+  g_mq->step = step;
+  g_mq->output_stat();
+  g_mq->output_for_restart();
+  return chdir(saved_cwd) == 0 ? 0 : 1;
+}
+
+/* One particle of the initial ensemble as init_particle_data makes it
+ * (src/particle_init.cpp:185-215: three uniform draws place it in cell
+ * (i, j, k), then select_kstate, src/mcmodel.cpp:3006-3057, draws its
+ * energy, band, wedge and k), drawing from stream (seed, uid, 0xfffffffd, 0)
+ * -- the per-particle stream of the engine's GPU seeding.  The position
+ * lines are the reference's, restated because init_particle_data loops over
+ * every cell of the deck with one sequential stream.  Out: d as
+ * orc_get_particles' doubles, iv as its ints. */
+int orc_seed_particle(uint64_t seed, uint32_t uid, int i, int j, int k, int type, double charge, double *d, int *iv) {
+  MeshQuantities *mq = g_mq;
+  const uint64_t saved = g_seed;
+  g_seed = seed;
+  set_stream(uid, 0xfffffffdu, 0);
+  Particle p;
+  double lamda = Random();
+  p.x = lamda * lx[i] + (1 - lamda) * lx[i + 1];
+  lamda = Random();
+  p.y = lamda * ly[j] + (1 - lamda) * ly[j + 1];
+  lamda = Random();
+  p.z = lamda * lz[k] + (1 - lamda) * lz[k + 1];
+  p.charge = charge;
+  p.i = i;
+  p.j = j;
+  p.k = k;
+  p.par_type = type;
+  p.seed = mq->seed;
+  p.left_time = mq->dt;
+  p.par_id = (int)uid;
+  p.flag = 1;
+  mq->select_kstate(&p, 0);
+  g_seed = saved;
+  const double dd[9] = {p.x, p.y, p.z, p.kx, p.ky, p.kz, p.charge, p.energy, p.left_time};
+  const int ii[9] = {p.i, p.j, p.k, p.itet, p.isym, p.par_type, p.flag, p.seed, p.par_id};
+  for (int q = 0; q < 9; ++q) {
+    d[q] = dd[q];
+    iv[q] = ii[q];
+  }
+  return 0;
+}
+
 /* Reference charge bookkeeping used by the flight (Rho = screening density):
  * src/mcmodel.cpp:2664-2712. */
 int orc_compute_cell_charge() {
@@ -580,7 +670,11 @@ int orc_flight_step(uint32_t step, int *unfinished) {
   std::sort(children.begin(), children.end(), [](const Child &a, const Child &b) {
     return std::tie(a.parent, a.sub) < std::tie(b.parent, b.sub);
   });
-  for (const Child &ch : children) ch.p->par_id = (int)g_next_uid++;
+  /* uids go to the copies that survive their flight (a copy caught in the
+   * rest of its step is removed below without one), as the engine numbers
+   * them */
+  for (const Child &ch : children)
+    if (ch.p->i >= 0) ch.p->par_id = (int)g_next_uid++;
   for (auto &l : mq->par_list)
     for (auto it = l.begin(); it != l.end();) {
       if (it->i < 0) it = l.erase(it);

@@ -193,5 +193,32 @@ class Oracle:
         n = self.lib.orc_contacts(out.ctypes.data)
         return out[:n]
 
+    def statistic(self):
+        """statistic(): one step's sums added to the stat_* vectors."""
+        self.lib.orc_statistic()
+
+    def set_stat_zero(self):
+        """set_stat_zero(): statistics, contact tallies and section currents cleared."""
+        self.lib.orc_set_stat_zero()
+
+    def write_outputs(self, folder: str, step: int):
+        """output_stat + output_for_restart for `step`, under folder/data/."""
+        self.lib.orc_write_outputs.argtypes = [ctypes.c_char_p, ctypes.c_int]
+        if self.lib.orc_write_outputs(os.path.abspath(folder).encode(), int(step)) != 0:
+            raise RuntimeError("orc_write_outputs failed")
+
+    def seed_particle(self, seed: int, uid: int, i: int, j: int, k: int, carrier: int, charge: float) -> dict:
+        """One initial-ensemble particle (init_particle_data's placement +
+        select_kstate) on the per-particle stream (seed, uid, 0xfffffffd, 0)."""
+        c = ctypes
+        self.lib.orc_seed_particle.argtypes = [c.c_uint64, c.c_uint32, c.c_int, c.c_int, c.c_int, c.c_int,
+                                               c.c_double, c.c_void_p, c.c_void_p]
+        d = np.zeros(9)
+        iv = np.zeros(9, dtype=np.int32)
+        self.lib.orc_seed_particle(seed, uid, i, j, k, carrier, charge, d.ctypes.data, iv.ctypes.data)
+        out = {k_: float(d[q]) for q, k_ in enumerate(D_FIELDS)}
+        out.update({k_: int(iv[q]) for q, k_ in enumerate(I_FIELDS)})
+        return out
+
     def time_update_particle(self, nsteps: int, with_cell_charge: bool = True) -> float:
         return float(self.lib.orc_time_update_particle(nsteps, int(with_cell_charge)))

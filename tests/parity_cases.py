@@ -44,6 +44,25 @@ def engine_from_oracle(orc: Oracle, max_particles: int, flags: int = 0) -> mcb20
     return eng
 
 
+def device_engine_from_oracle(orc: Oracle, max_particles: int = 1 << 16, precision: int = mcb200.FLIGHT_FP64,
+                              flags: int = 0) -> mcb200.Engine:
+    """Engine context carrying the oracle's mesh, cell data and device (doping,
+    materials, contacts), so that it deposits and solves Poisson itself."""
+    eng = mcb200.Engine(table_dir=ORACLE_TABLES, kelvin=orc.scalar("T0"), device=0, max_particles=max_particles,
+                        precision=precision)
+    eng.set_mesh(orc.array("lx"), orc.array("ly"), orc.array("lz"), orc.array("dx"), orc.array("dy"),
+                 orc.array("dz"))
+    eng.set_cells(orc.array("c_motion_rule").astype(np.int32), orc.array("c_da"),
+                  attached_contact=orc.array("c_attached_contact").astype(np.int32),
+                  in_surf_region=orc.array("c_InSurfRegion").astype(np.int32),
+                  nearest_surf=orc.array("c_nearestSurf").astype(np.int32),
+                  surface_dir=orc.array("SurfaceDir").astype(np.int32), flags=flags)
+    vapp, phims, planes = orc.contact_info()
+    eng.set_device(orc.array("c_material").astype(np.int32), orc.array("c_donor"), orc.array("c_acceptor"),
+                   vapp, phims, planes)
+    return eng
+
+
 def push_fields(orc: Oracle, eng: mcb200.Engine):
     """Fields as felt by each carrier (ChargeSign = {-1, +1},
     src/Constant_GlobalVariable_MathFunction.cpp:18) and the screening density."""
@@ -127,6 +146,54 @@ def run_bulk_parity(n_particles: int = 2000, steps: int = 3, seed: int = 11, fie
         worst["heat_oracle"] = orc.array("p_electron_heat")
     eng.close()
     return worst
+
+
+def action_bar(dirpath: str, nx=6, ny=12, nz=5, cell_nm=2.0, vd=0.5, electrons=6000, holes=1200, dt=1e-15) -> dict:
+    """A bar whose cell faces carry every ldg boundary action of HitCell
+    (src/CellHit.cpp:96-211) that the other parity decks leave out, in the
+    reference's deck language: PERIOD on both x faces (Period, :416-432);
+    SCATTOX on both z faces with surface scattering off (Reflect or Diffuse
+    by the carrier's diffuse probability, :243-386); contacts on the two
+    y end planes (source 0 V, drain vd) with, one cell inside the source, a
+    plane that catches carriers going left (CATCH, CatchAtContact :504-543)
+    and generates copies of carriers going right (GENERATE, Generate
+    :435-501); one cell inside the drain, a plane that catches carriers
+    going right without the section-current tally (CATCHGATE, CatchAtGate
+    :545-574) and copies carriers going left (GENREF); REFLECT at the y ends.
+    The end cells are attached to their contacts (attachcontact)."""
+    os.makedirs(dirpath, exist_ok=True)
+    X, Y, Z = nx * cell_nm, ny * cell_nm, nz * cell_nm
+    decks.write_grid(os.path.join(dirpath, "lgrid.txt"), np.arange(nx + 1) * cell_nm, np.arange(ny + 1) * cell_nm,
+                     np.arange(nz + 1) * cell_nm)
+    g = lambda v: f"{v:g}"
+    box = f"0 {g(X)} 0 {g(Y)} 0 {g(Z)}"
+    s_, d_ = cell_nm, Y - cell_nm
+    lines = [
+        "default_par_number 2 1",
+        f"region {box} SILICON",
+        f"donor {box} 1e+25",
+        f"acceptor {box} 1e+21",
+        f"motioncube {box} PASS PASS PASS PASS PASS PASS",
+        f"motionplane 0 0 0 {g(Y)} 0 {g(Z)} UP PERIOD",
+        f"motionplane {g(X)} {g(X)} 0 {g(Y)} 0 {g(Z)} DOWN PERIOD",
+        f"motionplane 0 {g(X)} 0 {g(Y)} 0 0 FRONT SCATTOX",
+        f"motionplane 0 {g(X)} 0 {g(Y)} {g(Z)} {g(Z)} BACK SCATTOX",
+        f"motionplane 0 {g(X)} 0 0 0 {g(Z)} LEFT REFLECT",
+        f"motionplane 0 {g(X)} {g(Y)} {g(Y)} 0 {g(Z)} RIGHT REFLECT",
+        f"motionplane 0 {g(X)} {g(s_)} {g(s_)} 0 {g(Z)} LEFT CATCH",
+        f"motionplane 0 {g(X)} {g(s_)} {g(s_)} 0 {g(Z)} RIGHT GENERATE",
+        f"motionplane 0 {g(X)} {g(d_)} {g(d_)} 0 {g(Z)} RIGHT CATCHGATE",
+        f"motionplane 0 {g(X)} {g(d_)} {g(d_)} 0 {g(Z)} LEFT GENREF",
+        f"attachcontact 0 {g(X)} 0 {g(s_)} 0 {g(Z)} 1",
+        f"attachcontact 0 {g(X)} {g(d_)} {g(Y)} 0 {g(Z)} 2",
+        "contact", "1 0", f"0 {g(X)} 0 0 0 {g(Z)}", "0",
+        "contact", "1 0", f"0 {g(X)} {g(Y)} {g(Y)} 0 {g(Z)}", f"{vd:g}",
+        "end",
+    ]
+    with open(os.path.join(dirpath, "ldg.txt"), "w") as f:
+        f.write("\n".join(lines) + "\n")
+    decks.write_input(os.path.join(dirpath, "input.txt"), dt=dt, ElectronNumber=electrons, HoleNumber=holes)
+    return dict(input=os.path.join(dirpath, "input.txt"))
 
 
 def make_restart(deck: dict, seed: int = 5, restart_step: int = 7) -> np.ndarray:

@@ -19,7 +19,7 @@ import pytest
 import mcb200
 from mcb200 import decks
 from oracle_bridge import ORACLE_TABLES, Oracle
-from parity_cases import make_restart
+from parity_cases import action_bar, make_restart
 
 REF_FINFET = os.path.join(os.environ.get("MCB200_REFERENCE", "/root/reference"), "finfet")
 
@@ -78,6 +78,21 @@ def test_contact_bar_deck():
     with tempfile.TemporaryDirectory() as tmp:
         d = decks.contact_bar(tmp, vd=0.4, electrons=3000, holes=500)
         _compare(d["input"])
+
+
+def test_action_bar_deck():
+    """PERIOD / SCATTOX / CATCH / GENERATE / CATCHGATE / GENREF faces and
+    attachcontact parse to the reference's cell arrays."""
+    with tempfile.TemporaryDirectory() as tmp:
+        d = action_bar(tmp)
+        _compare(d["input"])
+        orc = Oracle()
+        orc.init(d["input"], seed=1)
+        rules = set(orc.array("c_motion_rule").astype(int).tolist())
+        contact = orc.array("c_attached_contact").astype(int)
+    # every action of HitCell appears (PASS 1, REFLECT 2, SCATTOX 3, PERIOD 4, GENERATE 5, GENREF 6, CATCH 7, CATCHGATE 8)
+    assert rules >= {1, 2, 3, 4, 5, 6, 7, 8}, rules
+    assert set(contact.tolist()) == {0, 1, 2}
 
 
 def test_contact_bar_with_surfaces_deck():

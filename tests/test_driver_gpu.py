@@ -168,6 +168,42 @@ def test_run_deck_finfet(precision):
         assert np.isfinite(rep["heat_total"])
 
 
+def test_main_executable_contact_bar():
+    """`mcb200_main input.txt` (the drop-in for the reference's `main
+    input.txt`) on the contact bar, run from the deck's folder as the
+    reference is: exit status 0, ./data/current with one block per
+    statistics window, and the same files, byte for byte, as
+    mcb200_run_deck writes for the same deck and seed."""
+    import shutil
+    import subprocess
+
+    exe = os.path.join(os.path.dirname(mcb200.LIB_PATH), "mcb200_main")
+    assert os.path.exists(exe), exe
+    with tempfile.TemporaryDirectory() as tmp:
+        deck = decks.contact_bar(tmp, vd=0.5, electrons=4000, holes=400)
+        text = open(deck["input"]).read()
+        text = text.replace("total_step=100", "total_step=20").replace("stat_step=1000000", "stat_step=10")
+        open(deck["input"], "w").write(text)
+        env = dict(os.environ, MCB200_TABLES=ORACLE_TABLES)
+        run = subprocess.run([exe, "input.txt", "--quiet", "--seed", "5"], cwd=tmp, env=env, capture_output=True,
+                             text=True, timeout=300)
+        assert run.returncode == 0, run.stderr
+        assert "done: 20 steps" in run.stdout, run.stdout
+        data = os.path.join(tmp, "data")
+        current = open(os.path.join(data, "current")).read()
+        assert current.count("step = ") == 2 and "step = 9" in current and "step = 19" in current, current
+        assert current.count("Current = ") == 2 * 2  # two contacts per window
+        shutil.move(data, os.path.join(tmp, "data_exe"))
+        rep = mcb200.run_deck(deck["input"], data_dir=os.path.join(tmp, "data_lib"), table_dir=ORACLE_TABLES, seed=5)
+        assert rep["steps_done"] == 20
+        names = sorted(os.listdir(os.path.join(tmp, "data_exe")))
+        assert names == sorted(os.listdir(os.path.join(tmp, "data_lib")))
+        for name in names:
+            a = open(os.path.join(tmp, "data_exe", name), "rb").read()
+            b = open(os.path.join(tmp, "data_lib", name), "rb").read()
+            assert a == b, name
+
+
 def test_restart_seed_matches_oracle():
     """Flag_restart seeding (init_particle_data with
     read_par_info_for_restart): per cell and carrier type the same number of

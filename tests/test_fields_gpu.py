@@ -147,3 +147,50 @@ def test_multigrid_finfet():
     finally:
         eng.close()
         deck.close()
+
+
+def test_induced_current_on_the_contact_bar():
+    """Ramo-Shockley on the two-contact bar (uniform silicon, contacts on the
+    y = 0 and y = Y node planes): the drain's weighting potential is y / Y,
+    so its field is (0, -1/Y, 0) in every cell, and the induced-current
+    tally of the transport steps is the sum over steps and particles of
+    q v_y / -Y -- the statistic() velocity sums of the same steps (sum |q|
+    v_y per carrier type) divided by Y."""
+    with tempfile.TemporaryDirectory() as tmp:
+        deck = decks.contact_bar(tmp, vd=0.5, electrons=3000, holes=600)
+        orc = Oracle()
+        orc.init(deck["input"], seed=13)
+    from parity_cases import device_engine_from_oracle
+
+    eng = device_engine_from_oracle(orc)
+    try:
+        eng.upload(orc.particles())
+        eng.deposit()
+        eng.solve_poisson(rel_tol=1e-12, max_iter=50000)
+        eng.set_induced_current(1)
+        ly = orc.array("ly")
+        Y = ly[-1] - ly[0]
+        f = eng.array("induced_field").reshape(-1, 3)
+        assert np.max(np.abs(f[:, [0, 2]])) <= 1e-12 / Y
+        assert np.max(np.abs(f[:, 1] + 1.0 / Y)) <= 1e-9 / Y
+        window = 4
+        eng.stat_begin(window)
+        eng.reset_tallies()
+        dt = orc.scalar("dt")
+        for s in range(window):
+            eng.stat_accumulate()  # the store each transport step starts from
+            eng.deposit()
+            eng.solve_poisson(rel_tol=1e-10)
+            eng.step(s, 13, dt)
+        induced, steps = eng.induced_current()
+        assert steps == window
+        ve, vh = eng.stat("electron_qvy").sum(), eng.stat("hole_qvy").sum()
+        expected = (ve - vh) / Y  # electrons carry q = -|q|, holes +|q|; E_w,y = -1/Y
+        u = eng.units()
+        vbound = 1e6 / (u["spr0"] / u["time0"])  # 1e6 m/s: above any carrier's group velocity
+        scale = (eng.stat("electron_q").sum() + eng.stat("hole_q").sum()) * vbound / Y
+        assert abs(induced - expected) <= 1e-9 * scale, (induced, expected)
+        assert abs(induced) > 1e-4 * scale  # a net drift under the 0.5 V bias
+        eng.set_induced_current(-1)
+    finally:
+        eng.close()

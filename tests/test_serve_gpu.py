@@ -43,19 +43,24 @@ def by_id(results, rid):
     return next(r for r in results if r["id"] == rid)
 
 
-def test_same_result_alone_and_in_mix():
+@pytest.mark.parametrize("estimator", [mcb200.IDS_CONTACT, mcb200.IDS_INDUCED])
+def test_same_result_alone_and_in_mix(estimator):
+    """Also with Ids from the induced (Ramo-Shockley) current: its tally is
+    summed in fixed point per step, so it does not depend on the store's
+    order either."""
+    cold = dict(COLD, ids_estimator=estimator)
     with tempfile.TemporaryDirectory() as tmp:
         a = deck(tmp, "a", 0.4)
         b = deck(tmp, "b", 0.8, lg=20.0)
         c = deck(tmp, "c", 0.0, vd=0.05)
         s1 = mcb200.Server(quantum_steps=10)
-        ida = s1.submit(a, "lg15", (0.4, 0.7), seed=1, **COLD)
+        ida = s1.submit(a, "lg15", (0.4, 0.7), seed=1, **cold)
         alone = by_id(drive(s1), ida)
         s1.close()
         s2 = mcb200.Server(quantum_steps=10)
-        s2.submit(b, "lg20", (0.8, 0.7), seed=2, **COLD)
-        ida2 = s2.submit(a, "lg15", (0.4, 0.7), seed=1, **COLD)
-        s2.submit(c, "lg15", (0.0, 0.05), seed=3, **COLD)
+        s2.submit(b, "lg20", (0.8, 0.7), seed=2, **cold)
+        ida2 = s2.submit(a, "lg15", (0.4, 0.7), seed=1, **cold)
+        s2.submit(c, "lg15", (0.0, 0.05), seed=3, **cold)
         res = drive(s2)
         mixed = by_id(res, ida2)
         assert len(res) == 3 and all(r["status"] == mcb200.SERVE_STEP_LIMIT for r in res)
