@@ -182,14 +182,10 @@ void batch_transport(mcb200_batch *b, uint64_t early = 0) {
   const uint64_t all = all_members(b);
   early &= all;
   if (early == all) early = 0;  // one launch
-  // 1. every member: counters and records for the step, then the stream of
-  //    its flight waits for it; the band tables the members share are
-  //    fetched into L2 once, on the batch stream
-  prefetch_band_tables<R>(b->m[0], b->stream);
-  b->launches += 1;
+  // 1. every member: counters and records for the step, then the stream of its flight waits for it
   for (int k = 0; k < n; ++k) {
     mcb200_ctx *c = b->m[k];
-    step_prepare<R>(c, false);
+    step_prepare<R>(c);
     ck(cudaEventRecord(b->ev_member[k], c->stream), "event");
     ck(cudaStreamWaitEvent((early >> k) & 1 ? b->side : b->stream, b->ev_member[k], 0), "wait");
   }

@@ -1914,55 +1914,12 @@ void surface_rates_enqueue(mcb200_ctx *c, cudaStream_t s) {
   c->launches += 1;
 }
 
-// What the flight reads that no earlier kernel of the step has touched --
-// the tetrahedron records, the per-cell motion rules, contacts and surface
-// flags, for FP64 flight the cell fields and doping (FP32 flight reads the
-// per-cell records written just before it), and the store's k and uid
-// arrays (the statistics and the deposition read the rest of the store) --
-// is fetched into L2 by the copy engine before the flight starts, instead
-// of by the first lane that misses on each line.
-// with_tables == false leaves out the band tables (a batched step fetches
-// the tables its members share once).
+// Before the flights of a step: the induced-current tally (when on), work
+// counters, the FP32 per-cell records, and zeroed copy counters of every
+// generation and of the sink.
 template <typename R>
-void prefetch_flight_tables(mcb200_ctx *c, cudaStream_t s, bool with_tables) {
-  const DevTables &T = c->ts->dt;
-  const DevMesh &M = c->mesh;
-  const size_t cells = (size_t)c->ncells;
-  L2Ranges r{};
-  auto add = [&](const void *p, size_t bytes) {
-    if (p && bytes && r.n < L2Ranges::kMax) {
-      r.p[r.n] = p;
-      r.bytes[r.n] = bytes;
-      ++r.n;
-    }
-  };
-  if (with_tables) add(sizeof(R) == 4 ? (const void *)T.f32.tf : (const void *)T.tf,
-                       (size_t)T.nt * (sizeof(R) == 4 ? sizeof(TetFlightT<float>) : sizeof(TetFlightT<double>)));
-  if constexpr (sizeof(R) == 8) {
-    add(M.efield, cells * 3 * sizeof(double));
-    add(M.hfield, cells * 3 * sizeof(double));
-    add(M.da, cells * sizeof(double));
-  }
-  add(M.motion, cells * 6 * sizeof(int));
-  add(M.contact, cells * sizeof(int));
-  add(M.in_surf, cells * sizeof(int));
-  const DevParticlesT<R> P = store<R>(c, c->cur);
-  const size_t n = std::min(c->n, c->capacity);  // the last count read back: a hint, not a bound
-  add(P.kx, n * sizeof(R));
-  add(P.ky, n * sizeof(R));
-  add(P.kz, n * sizeof(R));
-  add(P.uid, n * sizeof(uint32_t));
-  launch_l2_prefetch(r, c->sm_count, s);
-  c->launches += 1;
-}
-
-// Before the flights of a step: the L2 prefetch above, work counters, the
-// FP32 per-cell records, and zeroed copy counters of every generation and
-// of the sink.
-template <typename R>
-void step_prepare(mcb200_ctx *c, bool prefetch_tables) {
+void step_prepare(mcb200_ctx *c) {
   cudaStream_t s = c->stream;
-  prefetch_flight_tables<R>(c, s, prefetch_tables);
   if (c->induced_contact >= 0) {  // the induced current of the store the step starts from
     launch_induced_current(store<R>(c, c->cur), DevCount{c->dev_counts, nullptr, (int)c->capacity}, c->mesh,
                            c->ts->dt, c->ib, grid_for(c, c->capacity, 256), s);
@@ -2026,7 +1983,7 @@ void step_impl(mcb200_ctx *c, uint32_t step, uint64_t seed, double dt) {
     c->ev_pending[q] = true;
     ck(cudaEventRecord(ev[0], s), "event");
   }
-  step_prepare<R>(c, true);
+  step_prepare<R>(c);
   // 1. main flight; copies go to generation 0
   F.C = children<R>(c, 0);
   if (ev) ck(cudaEventRecord(ev[1], s), "event");
@@ -2059,20 +2016,8 @@ void step_impl(mcb200_ctx *c, uint32_t step, uint64_t seed, double dt) {
   }
 }
 
-template <typename R>
-void prefetch_band_tables(mcb200_ctx *c, cudaStream_t s) {
-  const DevTables &T = c->ts->dt;
-  L2Ranges r{};
-  r.p[0] = sizeof(R) == 4 ? (const void *)T.f32.tf : (const void *)T.tf;
-  r.bytes[0] = (size_t)T.nt * (sizeof(R) == 4 ? sizeof(TetFlightT<float>) : sizeof(TetFlightT<double>));
-  r.n = r.p[0] ? 1 : 0;
-  launch_l2_prefetch(r, c->sm_count, s);
-}
-
-template void step_prepare<float>(mcb200_ctx *, bool);
-template void step_prepare<double>(mcb200_ctx *, bool);
-template void prefetch_band_tables<float>(mcb200_ctx *, cudaStream_t);
-template void prefetch_band_tables<double>(mcb200_ctx *, cudaStream_t);
+template void step_prepare<float>(mcb200_ctx *);
+template void step_prepare<double>(mcb200_ctx *);
 template void step_tail<float>(mcb200_ctx *);
 template void step_tail<double>(mcb200_ctx *);
 

@@ -314,12 +314,8 @@ void poisson_finish(mcb200_ctx *c, cudaStream_t s, int *iterations, double *rel_
 void surface_rates_enqueue(mcb200_ctx *c, cudaStream_t s);
 void deposit_enqueue(mcb200_ctx *c, cudaStream_t s);
 // The parts of a transport step around its flights (engine.cu).
-// prefetch_tables: also fetch the band tables the flight reads into L2 (a
-// batched step fetches its members' shared tables once, prefetch_band_tables).
 template <typename R>
-void step_prepare(mcb200_ctx *c, bool prefetch_tables);
-template <typename R>
-void prefetch_band_tables(mcb200_ctx *c, cudaStream_t s);
+void step_prepare(mcb200_ctx *c);
 template <typename R>
 void step_tail(mcb200_ctx *c);
 

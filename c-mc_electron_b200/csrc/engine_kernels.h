@@ -33,19 +33,6 @@ template <typename R>
 int launch_batch_flight(const FlightCtxT<R> &F, const BatchInstT<R> *inst, int ninst, uint64_t members,
                         const uint32_t *steps, bool child, unsigned int *ticket, int blocks_per_sm, int sm_count,
                         cudaStream_t s);
-// Ranges of device memory brought into L2 ahead of the kernels that read
-// them: each range is split into 16 KB pieces, each fetched by one bulk
-// prefetch of the copy engine (cp.async.bulk.prefetch.L2), so no thread
-// waits for the data.  A range whose start is not 16-byte aligned is left
-// out (allocations are aligned); a tail of fewer than 16 bytes is not
-// fetched.
-struct L2Ranges {
-  static constexpr int kMax = 12;
-  const void *p[kMax];
-  size_t bytes[kMax];
-  int n;
-};
-void launch_l2_prefetch(const L2Ranges &r, int grid, cudaStream_t s);
 // FP32 flight's per-cell records (DevMesh::cell32), [cells][3] float4.
 void launch_cell_records32(const DevTables &T, const DevMesh &M, float4 *out, int cells, cudaStream_t s);
 // The step's surviving copies (all generations) ranked by (parent uid, sub),

@@ -557,11 +557,26 @@ inline int current_device() {
   if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= kMaxDevices) d = 0;
   return d;
 }
+// The flight kernels read their tables through L1 (a few KB of shared
+// memory per block): ask for the largest L1 share of each SM's on-chip
+// memory, rather than leave the split to whatever the driver last chose.
+template <typename R>
+void prefer_l1() {
+  // a hint: a device that refuses it keeps its own split (and the refusal is
+  // not left behind for the next launch check)
+  if (cudaFuncSetAttribute(flight_kernel<R>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           (int)cudaSharedmemCarveoutMaxL1) != cudaSuccess)
+    cudaGetLastError();
+  if (cudaFuncSetAttribute(child_flight_kernel<R>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           (int)cudaSharedmemCarveoutMaxL1) != cudaSuccess)
+    cudaGetLastError();
+}
 template <typename R>
 int flight_grid(int n, int block, int sm_count) {
   static int per_sm_of[kMaxDevices] = {};
   int &per_sm = per_sm_of[current_device()];
   if (per_sm == 0) {
+    prefer_l1<R>();
     int b = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, flight_kernel<R>, block, 0) != cudaSuccess || b < 1) b = 1;
     per_sm = b;
@@ -606,30 +621,6 @@ int launch_batch_flight(const FlightCtxT<R> &F, const BatchInstT<R> *inst, int n
   if (blocks_per_sm > 0) per_sm = std::min(per_sm, blocks_per_sm);
   kernel<<<per_sm * sm_count, kFlightThreads, smem, s>>>(F, inst, ninst, members, steps, ticket);
   return cudaGetLastError() == cudaSuccess ? 0 : 1;
-}
-__global__ void l2_prefetch_kernel(L2Ranges r) {
-  constexpr size_t kPiece = 16384;
-  const size_t stride = (size_t)gridDim.x * blockDim.x;
-  for (int k = 0; k < r.n; ++k) {
-    const char *base = static_cast<const char *>(r.p[k]);
-    const size_t bytes = r.bytes[k] & ~(size_t)15;
-    const size_t pieces = (bytes + kPiece - 1) / kPiece;
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < pieces; q += stride) {
-      const size_t off = q * kPiece;
-      const unsigned size = (unsigned)(bytes - off < kPiece ? bytes - off : kPiece);
-      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(base + off), "r"(size) : "memory");
-    }
-  }
-}
-void launch_l2_prefetch(const L2Ranges &r, int grid, cudaStream_t s) {
-  L2Ranges ok{};  // a range that does not start on a 16-byte boundary is left out (the copy engine needs it)
-  for (int k = 0; k < r.n && k < L2Ranges::kMax; ++k)
-    if (r.p[k] && (reinterpret_cast<uintptr_t>(r.p[k]) & 15u) == 0 && r.bytes[k] >= 16) {
-      ok.p[ok.n] = r.p[k];
-      ok.bytes[ok.n] = r.bytes[k];
-      ++ok.n;
-    }
-  if (ok.n > 0) l2_prefetch_kernel<<<grid, 128, 0, s>>>(ok);
 }
 void launch_cell_records32(const DevTables &T, const DevMesh &M, float4 *out, int cells, cudaStream_t s) {
   if (cells > 0) cell_records32_kernel<<<(cells + 255) / 256, 256, 0, s>>>(T, M, out, cells);

@@ -237,8 +237,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mcb200_elapsed_ms.argtypes = [vp, c.c_int, c.c_int, dp]
     lib.mcb200_stat_accumulate.argtypes = [vp]
     lib.mcb200_stat_get.argtypes = [vp, c.c_char_p, dp, c.c_size_t]
-    lib.mcb200_set_induced_current.argtypes = [vp, c.c_int]
-    lib.mcb200_get_induced_current.argtypes = [vp, dp, dp]
+    if hasattr(lib, "mcb200_set_induced_current"):  # absent from libraries built before it (MCB200_LIBRARY)
+        lib.mcb200_set_induced_current.argtypes = [vp, c.c_int]
+        lib.mcb200_get_induced_current.argtypes = [vp, dp, dp]
     lib.mcb200_set_potential.argtypes = [vp, dp]
     lib.mcb200_set_potentials.argtypes = [vp, dp, dp]
     lib.mcb200_set_quantum_correction.argtypes = [vp, vp, i32p, i32p, c.c_int]

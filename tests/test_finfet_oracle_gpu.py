@@ -88,7 +88,8 @@ def test_finfet_flight_matches_reference(finfet_pair):
     ref = orc.contacts()[:, :5]
     got = t["contact"][: len(ref), :5]
     assert np.array_equal(ref[:, [0, 3]], got[:, [0, 3]])
-    assert np.allclose(got, ref, rtol=1e-12, atol=1e-12 * max(np.abs(ref).max(), 1e-300))
+    # charge / energy sums: int64 fixed point (2^-40 charge, 2^-32 kT per term) against FP64 sums
+    assert np.allclose(got, ref, rtol=1e-9, atol=1e-9 * max(np.abs(ref).max(), 1e-300))
     for side in ("lcurrent", "rcurrent"):
         a = orc.array(side)
-        assert np.allclose(t[side], a, rtol=1e-12, atol=1e-12 * max(np.abs(a).max(), 1e-300)), side
+        assert np.allclose(t[side], a, rtol=1e-9, atol=1e-9 * max(np.abs(a).max(), 1e-300)), side

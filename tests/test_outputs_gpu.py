@@ -69,10 +69,11 @@ def test_boundary_actions_match_oracle():
     assert t["caught"] == int(orc.scalar("catch_par_num"))
     ref, got = _contact_tallies(orc, eng)
     assert np.array_equal(ref[:, [0, 3]], got[:, [0, 3]])  # particle counts
-    assert np.allclose(got, ref, rtol=1e-12, atol=1e-30 + 1e-12 * np.abs(ref).max())
+    # charge / energy sums: int64 fixed point (2^-40 charge, 2^-32 kT per term) against FP64 sums
+    assert np.allclose(got, ref, rtol=1e-9, atol=1e-9 * np.abs(ref).max())
     for side in ("lcurrent", "rcurrent"):
         a, b = orc.array(side), t[side]
-        assert np.allclose(b, a, rtol=1e-12, atol=1e-12 * max(np.abs(a).max(), 1e-300)), side
+        assert np.allclose(b, a, rtol=1e-9, atol=1e-9 * max(np.abs(a).max(), 1e-300)), side
     # every action fired: GENERATE (contact 0) and GENREF (contact 1) copies,
     # CATCH (contact 0) and CATCHGATE (contact 1) catches
     assert ref[0, 0] > 0 and ref[1, 0] > 0, ref
@@ -90,9 +91,15 @@ NUMBER = re.compile(r"^[-+]?(\d+\.?\d*|\.\d+)([eE][-+]?\d+)?$")
 
 
 def _compare_files(a_path, b_path, rel=2e-5):
+    """Same lines and words; numbers equal to `rel` (six printed digits), or
+    within 1e-9 of the file's largest number (a difference of two nearly
+    equal sums: the reference's FP64 leaves rounding residue where the
+    engine's fixed point gives exactly zero)."""
     a = open(a_path).read().split("\n")
     b = open(b_path).read().split("\n")
     assert len(a) == len(b), (os.path.basename(a_path), len(a), len(b))
+    words = [w for line in a for w in line.replace("=", " = ").split() if NUMBER.match(w)]
+    floor = 1e-9 * max([abs(float(w)) for w in words] + [1e-300])
     worst = 0.0
     for la, lb in zip(a, b):
         ta, tb = la.replace("=", " = ").split(), lb.replace("=", " = ").split()
@@ -101,7 +108,7 @@ def _compare_files(a_path, b_path, rel=2e-5):
             if NUMBER.match(wa) and NUMBER.match(wb):
                 x, y = float(wa), float(wb)
                 err = abs(x - y)
-                assert err <= rel * max(abs(x), abs(y)) + 1e-300, (os.path.basename(a_path), la, lb)
+                assert err <= rel * max(abs(x), abs(y)) + floor, (os.path.basename(a_path), la, lb)
                 worst = max(worst, err / max(abs(x), abs(y), 1e-300))
             else:
                 assert wa == wb, (os.path.basename(a_path), la, lb)
