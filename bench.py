@@ -52,7 +52,10 @@ from mcb200.workloads import BULK_BOX as BOX  # noqa: E402
 
 # read + write of the particle state: 80 B (FP64 plain), 56 B (FP32 flight)
 BYTES_PER_PARTICLE_STEP = {"fp64": 160, "fp32": 112}
+# DRAM bytes per particle-step of the flight kernel, from ncu captures of the
+# same workload: the bulk box (its flight arm) and the FinFET (the headline)
 PROFILE_TRAFFIC = {p: os.path.join(ROOT, "profiles", f"flight_{p}_bulk_traffic.json") for p in ("fp64", "fp32")}
+FINFET_TRAFFIC = {p: os.path.join(ROOT, "profiles", f"flight_{p}_finfet_traffic.json") for p in ("fp64", "fp32")}
 
 
 def measured_peaks():
@@ -234,7 +237,7 @@ def engine_arm(args, rank: int, world: int, device: int):
         achieved = BYTES_PER_PARTICLE_STEP[p] * per_launch / (kernel_ms * 1e-3) / 1e9
         traffic = None
         try:
-            with open(PROFILE_TRAFFIC[p]) as f:
+            with open(FINFET_TRAFFIC[p]) as f:
                 traffic = json.load(f)["dram_bytes_per_particle_step"] * per_launch
         except Exception:
             pass

@@ -557,26 +557,11 @@ inline int current_device() {
   if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= kMaxDevices) d = 0;
   return d;
 }
-// The flight kernels read their tables through L1 (a few KB of shared
-// memory per block): ask for the largest L1 share of each SM's on-chip
-// memory, rather than leave the split to whatever the driver last chose.
-template <typename R>
-void prefer_l1() {
-  // a hint: a device that refuses it keeps its own split (and the refusal is
-  // not left behind for the next launch check)
-  if (cudaFuncSetAttribute(flight_kernel<R>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                           (int)cudaSharedmemCarveoutMaxL1) != cudaSuccess)
-    cudaGetLastError();
-  if (cudaFuncSetAttribute(child_flight_kernel<R>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                           (int)cudaSharedmemCarveoutMaxL1) != cudaSuccess)
-    cudaGetLastError();
-}
 template <typename R>
 int flight_grid(int n, int block, int sm_count) {
   static int per_sm_of[kMaxDevices] = {};
   int &per_sm = per_sm_of[current_device()];
   if (per_sm == 0) {
-    prefer_l1<R>();
     int b = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, flight_kernel<R>, block, 0) != cudaSuccess || b < 1) b = 1;
     per_sm = b;

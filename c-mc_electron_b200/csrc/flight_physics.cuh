@@ -44,6 +44,22 @@ constexpr int kMaxEvents = 1000000;
 // FP32 flight: consecutive zero-length events after which a particle is
 // taken as stuck (counted in kCntZeroTime and caught).
 constexpr int kMaxZeroTimeEvents = 64;
+// Opt-in event census (build with -DMCB200_FLIGHT_EVENT_STATS=1): counters
+// 10-15 of the tallies count the flight loop's passes by the event that
+// ended them and the work of the rare shared tails, for the design record
+// (mcb200.flight_events); one atomic per counted event, so never in a
+// timed build.
+#ifndef MCB200_FLIGHT_EVENT_STATS
+#define MCB200_FLIGHT_EVENT_STATS 0
+#endif
+enum EventStat : int {
+  kStatTetFace = 10,    // passes ended at a tetrahedron face
+  kStatCellFace = 11,   // at a cell face
+  kStatScatter = 12,    // at a phonon, impurity or surface event (real or self-scattering)
+  kStatStepEnd = 13,    // at the end of the step
+  kStatStateTries = 14, // get_state draws (tetrahedra tried, accepted or not)
+  kStatWalkSteps = 15,  // tetrahedra visited by the k-space walks
+};
 
 // Arithmetic of the two flight precisions.
 template <typename R> struct FlightReal;
@@ -364,6 +380,7 @@ struct FlyerT {
   __device__ int walk_to(int start, R a, R b, R c) const {
     int it = start;
     for (int s = 0; s < 64; ++s) {
+      if constexpr (MCB200_FLIGHT_EVENT_STATS != 0) count(I->Y, kStatWalkSteps);
       int fmin = -1;
       R dmin = -Real::kContain;
 #pragma unroll
@@ -610,6 +627,8 @@ struct FlyerT {
       if (((Random() * maxdostet) > dostet) && (count2 < 10000)) continue;
       break;
     }
+    if constexpr (MCB200_FLIGHT_EVENT_STATS != 0)
+      atomicAdd(&I->Y.counters[kStatStateTries], (unsigned long long)count2);
     if (count2 >= 10000) {
       self = true;
     } else {
@@ -1274,6 +1293,8 @@ struct FlyerT {
     PhScTf -= Tf;
     ImpScTf -= Tf;
     SurfScTf -= Tf;
+    if constexpr (MCB200_FLIGHT_EVENT_STATS != 0)
+      count(I->Y, flag == 1 ? kStatTetFace : flag == 2 ? kStatCellFace : flag == 6 ? kStatStepEnd : kStatScatter);
     if (flag == 6) left_time = 0;  // Tf == left_time: the step is used up
     else left_time -= Tf;
     phrnl -= g * Tf;
