@@ -500,10 +500,6 @@ void init_device_context(mcb200_ctx *c, size_t max_particles) {
   c->capacity = max_particles;
   c->child_cap = (int)std::min<size_t>(std::max<size_t>(max_particles / 8, 4096), 1u << 22);
   alloc_stores(c);
-  const size_t all_children = (size_t)c->child_cap * mcb200_ctx::kGenerations;
-  c->child_keys = dalloc<uint64_t>(all_children, c->owned);
-  c->child_alive = dalloc<uint8_t>(all_children, c->owned);
-  c->child_uids = dalloc<uint32_t>(all_children, c->owned);
   c->append_count = dalloc<unsigned int>(1, c->owned);
   c->tickets = dalloc<unsigned int>(1 + mcb200_ctx::kGenerations, c->owned);
   c->y.counters = dalloc<unsigned long long>(kCntNumCounters, c->owned);
@@ -1926,7 +1922,7 @@ void step_prepare(mcb200_ctx *c) {
     c->launches += 3;
   }
   join_stat(c);  // the flights change the store the statistics read
-  StepCounters z{c->tickets, {}};
+  StepCounters z{c->tickets, {}, c->append_count};
   for (int g = 0; g < mcb200_ctx::kGenerations; ++g) z.count[g] = children<R>(c, g).count;
   z.count[mcb200_ctx::kGenerations] = c->sink_count;
   launch_step_reset(z, s);
@@ -1946,11 +1942,11 @@ void step_tail(mcb200_ctx *c) {
   const int cap = (int)c->capacity;
   ChildSetT<R> set;
   for (int g = 0; g < mcb200_ctx::kGenerations; ++g) set.g[g] = children<R>(c, g);
-  launch_append_children(set, c->child_keys, c->child_alive, c->child_uids, c->dev_counts + 1, store<R>(c, c->cur),
-                         c->dev_counts, cap, c->append_count, c->dev_counts + 2,
-                         grid_for(c, (size_t)c->child_cap * mcb200_ctx::kGenerations, 256), s);
+  // a step's copies are few: one block per SM strides over them
+  launch_append_children(set, c->dev_counts + 1, store<R>(c, c->cur), c->dev_counts, cap, c->append_count,
+                         c->dev_counts + 2, c->sm_count, s);
   ck(cudaGetLastError(), "append children");
-  c->launches += 3;
+  c->launches += 1;
   const int other = 1 - c->cur;
   launch_cell_sort(store<R>(c, c->cur), DevCount{c->dev_counts, c->append_count, cap}, store<R>(c, other), c->ncells,
                    c->mesh.nx, c->mesh.nz, c->hist, c->offsets, c->tile_sums, c->total, grid_for(c, c->capacity, 256),

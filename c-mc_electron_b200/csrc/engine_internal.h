@@ -188,9 +188,6 @@ struct mcb200_ctx {
   static constexpr int kGenerations = kChildGenerations;
   ChildBuffers cb[kGenerations];
   int child_cap = 0;
-  uint64_t *child_keys = nullptr;
-  uint8_t *child_alive = nullptr;
-  uint32_t *child_uids = nullptr;
   unsigned int *append_count = nullptr;
   unsigned int *tickets = nullptr;  // work counters of the persistent flight launches (main + generations)
   float4 *cell32 = nullptr;         // FP32 flight's per-cell records (mesh-sized)

@@ -37,16 +37,18 @@ int launch_batch_flight(const FlightCtxT<R> &F, const BatchInstT<R> *inst, int n
 void launch_cell_records32(const DevTables &T, const DevMesh &M, float4 *out, int cells, cudaStream_t s);
 // The step's surviving copies (all generations) ranked by (parent uid, sub),
 // given uids from *next_uid on, and appended to `dst` after its *n
-// particles; *appended = surviving copies, *overflow set if the store is full.
+// particles, in one launch; *appended (zeroed by the step reset) counts them,
+// *overflow is set if the store is full.
 template <typename R>
-void launch_append_children(const ChildSetT<R> &set, uint64_t *keys, uint8_t *alive, uint32_t *uids,
-                            unsigned int *next_uid, const DevParticlesT<R> &dst, const unsigned int *n, int capacity,
-                            unsigned int *appended, unsigned int *overflow, int grid, cudaStream_t s);
-// The counters a step starts from, zeroed in one launch: the flight tickets
-// and the copy count of every generation and of the sink.
+void launch_append_children(const ChildSetT<R> &set, unsigned int *next_uid, const DevParticlesT<R> &dst,
+                            const unsigned int *n, int capacity, unsigned int *appended, unsigned int *overflow,
+                            int grid, cudaStream_t s);
+// The counters a step starts from, zeroed in one launch: the flight tickets,
+// the copy count of every generation and of the sink, and the appended count.
 struct StepCounters {
   unsigned int *tickets;  // [1 + kChildGenerations]
   unsigned int *count[kChildGenerations + 1];
+  unsigned int *appended;  // copies appended to the store this step
 };
 void launch_step_reset(const StepCounters &z, cudaStream_t s);
 // *particle_steps += *n; *n = *sorted_total; *next_uid += *appended.

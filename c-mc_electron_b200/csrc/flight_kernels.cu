@@ -8,7 +8,8 @@
 //      caught particles are marked dead in their meta word.
 //   2. child_flight_kernel, repeated: copies made by GENERATE / GENREF fly
 //      the rest of the step (they may make copies of their own).
-//   3. child_rank_kernel: copies get uids next_uid + rank of (parent, sub).
+//   3. append_children_kernel: surviving copies join the store with uids
+//      next_uid + rank of (parent, sub).
 //   4. cell_histogram / cell_scan / cell_scatter: survivors and copies are
 //      counting-sorted by cell into the second particle buffer.
 #include <algorithm>
@@ -308,35 +309,6 @@ __global__ void cell_records32_kernel(DevTables T, DevMesh M, float4 *out, int c
                                        (float)(T.frickel * 4 * kPiD * rho / T.eps_si), (float)(0.120 / T.eV0), 0.0f);
 }
 
-// uid of each surviving copy: *next_uid + number of surviving copies with a
-// smaller (parent uid, sub) key, over all copies of this step (the key set
-// is the concatenation of the child generations).  Blocks stride over the
-// copies; each block compares its 256 keys with all keys, 256 at a time.
-template <typename R>
-__global__ void child_rank_kernel(ChildSetT<R> set, const uint64_t *keys, const uint8_t *alive,
-                                  const unsigned int *next_uid, uint32_t *uid_out) {
-  __shared__ uint64_t tile[256];
-  __shared__ uint8_t tile_alive[256];
-  int n = 0;
-  set.offset(0, &n);
-  const uint32_t uid0 = *next_uid;
-  for (int base_i = blockIdx.x * 256; base_i < n; base_i += gridDim.x * 256) {
-    const int i = base_i + threadIdx.x;
-    const uint64_t my = i < n ? keys[i] : 0;
-    uint32_t rank = 0;
-    for (int base = 0; base < n; base += 256) {
-      const int j = base + threadIdx.x;
-      tile[threadIdx.x] = j < n ? keys[j] : ~0ull;
-      tile_alive[threadIdx.x] = j < n ? alive[j] : 0;
-      __syncthreads();
-      const int m = min(256, n - base);
-      for (int q = 0; q < m; ++q) rank += (tile_alive[q] && tile[q] < my) ? 1u : 0u;
-      __syncthreads();
-    }
-    if (i < n) uid_out[i] = uid0 + rank;
-  }
-}
-
 // ---- counting sort by cell ------------------------------------------------
 __device__ __forceinline__ int cell_linear(uint32_t c, int nx, int nz) {
   return (int)((((c >> 10) & 1023) * nx + (c & 1023)) * nz + ((c >> 20) & 1023));
@@ -366,16 +338,27 @@ __global__ void scan_tiles(const unsigned int *in, unsigned int *out, unsigned i
   if (i < n) out[i] = s[threadIdx.x] - v;
   if (threadIdx.x == 1023) tile_sums[blockIdx.x] = s[1023];
 }
+// Exclusive scan of the tile sums in place, one block of 1024 threads, 1024
+// tiles per pass with the running total carried between passes.
 __global__ void scan_tile_sums(unsigned int *tile_sums, int ntiles, unsigned int *total) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    unsigned int run = 0;
-    for (int t = 0; t < ntiles; ++t) {
-      const unsigned int v = tile_sums[t];
-      tile_sums[t] = run;
-      run += v;
+  __shared__ unsigned int s[1024];
+  unsigned int carry = 0;
+  for (int base = 0; base < ntiles; base += 1024) {
+    const int t = base + threadIdx.x;
+    const unsigned int v = t < ntiles ? tile_sums[t] : 0u;
+    s[threadIdx.x] = v;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+      const unsigned int a = threadIdx.x >= (unsigned)off ? s[threadIdx.x - off] : 0u;
+      __syncthreads();
+      s[threadIdx.x] += a;
+      __syncthreads();
     }
-    *total = run;
+    if (t < ntiles) tile_sums[t] = carry + s[threadIdx.x] - v;
+    carry += s[1023];
+    __syncthreads();
   }
+  if (threadIdx.x == 0) *total = carry;
 }
 __global__ void scan_add(unsigned int *out, const unsigned int *tile_sums, int n) {
   const int i = blockIdx.x * 1024 + threadIdx.x;
@@ -400,63 +383,88 @@ __global__ void cell_scatter(DevParticlesT<R> src, DevCount count, DevParticlesT
   }
 }
 
-// Append the surviving copies (already flown) of every generation to the
-// particle store after its *n particles, with their uids.  `appended` counts
-// every surviving copy; one that would land beyond the store's capacity is
+// The surviving copies of every generation (already flown) join the store
+// after its *n particles, in one launch.  A copy's uid is *next_uid + the
+// number of surviving copies with a smaller (parent uid, sub) key, over all
+// generations (the key set is the concatenation of the generations); each
+// block compares its 256 copies with all copies, 256 at a time.  The place
+// in the store is taken from `appended` (order does not matter: the cell
+// sort follows); a copy that would land beyond the store's capacity is
 // dropped and raises *overflow (the host reports it).
 template <typename R>
-__global__ void children_to_particles(ChildSetT<R> set, const uint32_t *uids, const uint8_t *alive,
-                                      DevParticlesT<R> dst, const unsigned int *n, int capacity,
-                                      unsigned int *appended, unsigned int *overflow) {
-  int total = 0;
-  set.offset(0, &total);
-  const unsigned int n0 = *n;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-    if (!alive[i]) continue;
-    int gen = 0, local = i;
+struct CopyRef {
+  const ChildSetT<R> &set;
+  int cnt[kChildGenerations];
+  __device__ explicit CopyRef(const ChildSetT<R> &s) : set(s) {
 #pragma unroll
-    for (int q = 0; q + 1 < kChildGenerations; ++q) {
-      const int cnt = min((int)*set.g[gen].count, set.g[gen].capacity);
-      if (local >= cnt) {
-        local -= cnt;
-        ++gen;
-      }
-    }
-    const DevChildrenT<R> &c = set.g[gen];
-    const unsigned long long q = (unsigned long long)n0 + atomicAdd(appended, 1u);
-    if (q >= (unsigned long long)capacity) {
-      *overflow = 1u;
-      continue;
-    }
-    dst.x[q] = c.x[local]; dst.y[q] = c.y[local]; dst.z[q] = c.z[local];
-    dst.kx[q] = c.kx[local]; dst.ky[q] = c.ky[local]; dst.kz[q] = c.kz[local];
-    dst.energy[q] = c.energy[local]; dst.charge[q] = c.charge[local];
-    dst.cell[q] = c.cell[local];
-    dst.itet[q] = c.itet[local];
-    dst.meta[q] = c.meta[local] & 0xffffu;
-    dst.uid[q] = uids[i];
+    for (int q = 0; q < kChildGenerations; ++q) cnt[q] = min((int)*set.g[q].count, set.g[q].capacity);
   }
-}
-
-// Rank keys (parent uid, sub) and survival flags of the copies of every
-// generation, concatenated in generation order.
-template <typename R>
-__global__ void child_keys(ChildSetT<R> set, uint64_t *keys, uint8_t *alive) {
-  int total = 0;
-  set.offset(0, &total);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-    int gen = 0, local = i;
+  // generation and index of copy i of the concatenation
+  __device__ __forceinline__ void locate(int i, int &gen, int &local) const {
+    gen = 0;
+    local = i;
 #pragma unroll
-    for (int q = 0; q + 1 < kChildGenerations; ++q) {
-      const int cnt = min((int)*set.g[gen].count, set.g[gen].capacity);
-      if (local >= cnt) {
-        local -= cnt;
+    for (int q = 0; q + 1 < kChildGenerations; ++q)
+      if (gen == q && local >= cnt[q]) {
+        local -= cnt[q];
         ++gen;
       }
-    }
+  }
+  __device__ __forceinline__ void key(int i, uint64_t &k, bool &alive) const {
+    int gen, local;
+    locate(i, gen, local);
     const DevChildrenT<R> &c = set.g[gen];
-    keys[i] = ((uint64_t)c.parent_uid[local] << 32) | c.sub[local];
-    alive[i] = (c.meta[local] & kMetaDead) ? 0 : 1;
+    k = ((uint64_t)c.parent_uid[local] << 32) | c.sub[local];
+    alive = !(c.meta[local] & kMetaDead);
+  }
+};
+
+template <typename R>
+__global__ void append_children_kernel(ChildSetT<R> set, const unsigned int *next_uid, DevParticlesT<R> dst,
+                                       const unsigned int *n, int capacity, unsigned int *appended,
+                                       unsigned int *overflow) {
+  __shared__ uint64_t tile[256];
+  const CopyRef<R> ref(set);
+  int total = 0;
+#pragma unroll
+  for (int q = 0; q < kChildGenerations; ++q) total += ref.cnt[q];
+  if (total == 0) return;
+  const uint32_t uid0 = *next_uid;
+  const unsigned int n0 = *n;
+  for (int base_i = blockIdx.x * 256; base_i < total; base_i += gridDim.x * 256) {
+    const int i = base_i + threadIdx.x;
+    uint64_t my = ~0ull;
+    bool my_alive = false;
+    if (i < total) ref.key(i, my, my_alive);
+    uint32_t rank = 0;
+    for (int base = 0; base < total; base += 256) {
+      const int j = base + threadIdx.x;
+      uint64_t kj = ~0ull;
+      bool aj = false;
+      if (j < total) ref.key(j, kj, aj);
+      tile[threadIdx.x] = aj ? kj : ~0ull;  // a dead copy ranks after every live one
+      __syncthreads();
+      const int m = min(256, total - base);
+      for (int q = 0; q < m; ++q) rank += tile[q] < my ? 1u : 0u;
+      __syncthreads();
+    }
+    if (i < total && my_alive) {
+      int gen, local;
+      ref.locate(i, gen, local);
+      const DevChildrenT<R> &c = set.g[gen];
+      const unsigned long long q = (unsigned long long)n0 + atomicAdd(appended, 1u);
+      if (q >= (unsigned long long)capacity) {
+        *overflow = 1u;
+        continue;
+      }
+      dst.x[q] = c.x[local]; dst.y[q] = c.y[local]; dst.z[q] = c.z[local];
+      dst.kx[q] = c.kx[local]; dst.ky[q] = c.ky[local]; dst.kz[q] = c.kz[local];
+      dst.energy[q] = c.energy[local]; dst.charge[q] = c.charge[local];
+      dst.cell[q] = c.cell[local];
+      dst.itet[q] = c.itet[local];
+      dst.meta[q] = c.meta[local] & 0xffffu;
+      dst.uid[q] = uid0 + rank;
+    }
   }
 }
 
@@ -611,13 +619,10 @@ void launch_cell_records32(const DevTables &T, const DevMesh &M, float4 *out, in
   if (cells > 0) cell_records32_kernel<<<(cells + 255) / 256, 256, 0, s>>>(T, M, out, cells);
 }
 template <typename R>
-void launch_append_children(const ChildSetT<R> &set, uint64_t *keys, uint8_t *alive, uint32_t *uids,
-                            unsigned int *next_uid, const DevParticlesT<R> &dst, const unsigned int *n, int capacity,
-                            unsigned int *appended, unsigned int *overflow, int grid, cudaStream_t s) {
-  child_keys<R><<<grid, 256, 0, s>>>(set, keys, alive);
-  child_rank_kernel<R><<<grid, 256, 0, s>>>(set, keys, alive, next_uid, uids);
-  cudaMemsetAsync(appended, 0, sizeof(unsigned int), s);
-  children_to_particles<R><<<grid, 256, 0, s>>>(set, uids, alive, dst, n, capacity, appended, overflow);
+void launch_append_children(const ChildSetT<R> &set, unsigned int *next_uid, const DevParticlesT<R> &dst,
+                            const unsigned int *n, int capacity, unsigned int *appended, unsigned int *overflow,
+                            int grid, cudaStream_t s) {
+  append_children_kernel<R><<<grid, 256, 0, s>>>(set, next_uid, dst, n, capacity, appended, overflow);
 }
 __global__ void step_reset_kernel(StepCounters z) {
   const int t = threadIdx.x;
@@ -625,6 +630,7 @@ __global__ void step_reset_kernel(StepCounters z) {
     z.tickets[t] = 0u;
     *z.count[t] = 0u;
   }
+  if (t == 0) *z.appended = 0u;
 }
 void launch_step_reset(const StepCounters &z, cudaStream_t s) { step_reset_kernel<<<1, 32, 0, s>>>(z); }
 void launch_step_finish(unsigned int *n, const unsigned int *sorted_total, unsigned int *next_uid,
@@ -635,7 +641,7 @@ void launch_exclusive_scan(const unsigned int *in, unsigned int *out, unsigned i
                            int n, cudaStream_t s) {
   const int tiles = (n + 1023) / 1024;
   scan_tiles<<<tiles, 1024, 0, s>>>(in, out, tile_sums, n);
-  scan_tile_sums<<<1, 32, 0, s>>>(tile_sums, tiles, total);
+  scan_tile_sums<<<1, 1024, 0, s>>>(tile_sums, tiles, total);
   scan_add<<<tiles, 1024, 0, s>>>(out, tile_sums, n);
 }
 template <typename R>
@@ -646,7 +652,7 @@ void launch_cell_sort(const DevParticlesT<R> &src, DevCount n, const DevParticle
   cell_histogram<<<grid, 256, 0, s>>>(src.cell, src.meta, n, nx, nz, hist);
   const int tiles = (ncells + 1023) / 1024;
   scan_tiles<<<tiles, 1024, 0, s>>>(hist, offsets, tile_sums, ncells);
-  scan_tile_sums<<<1, 32, 0, s>>>(tile_sums, tiles, total);
+  scan_tile_sums<<<1, 1024, 0, s>>>(tile_sums, tiles, total);
   scan_add<<<tiles, 1024, 0, s>>>(offsets, tile_sums, ncells);
   cell_scatter<R><<<grid, 256, 0, s>>>(src, n, dst, offsets, nx, nz);
 }
@@ -658,9 +664,9 @@ void launch_cell_sort(const DevParticlesT<R> &src, DevCount n, const DevParticle
                                  cudaStream_t);                                                                 \
   template void launch_child_flight<R>(const FlightCtxT<R> &, const DevChildrenT<R> &, int, unsigned int *, int, \
                                        cudaStream_t);                                                           \
-  template void launch_append_children<R>(const ChildSetT<R> &, uint64_t *, uint8_t *, uint32_t *,             \
-                                          unsigned int *, const DevParticlesT<R> &, const unsigned int *, int,  \
-                                          unsigned int *, unsigned int *, int, cudaStream_t);                   \
+  template void launch_append_children<R>(const ChildSetT<R> &, unsigned int *, const DevParticlesT<R> &,     \
+                                          const unsigned int *, int, unsigned int *, unsigned int *, int,       \
+                                          cudaStream_t);                                                        \
   template int launch_batch_flight<R>(const FlightCtxT<R> &, const BatchInstT<R> *, int, uint64_t,             \
                                       const uint32_t *, bool, unsigned int *, int, int, cudaStream_t);          \
   template void launch_cell_sort<R>(const DevParticlesT<R> &, DevCount, const DevParticlesT<R> &, int, int, int, \
