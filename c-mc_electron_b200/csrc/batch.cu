@@ -510,13 +510,17 @@ int mcb200_batch_autotune(mcb200_batch *b, int trial_steps, mcb200_batch_tuning 
   if (!b || trial_steps < 1) return MCB200_ERR_ARG;
   static const int flight_blocks[] = {1, 2};
   static const int grid_per_sm[] = {2, 4, 8};
-  mcb200_batch_tuning win{0, 0, 0, 1e300, 0, 0};
+  static const int sort_buckets[] = {1, 2, 4, 8};
+  mcb200_batch_tuning win{0, 0, 0, 1e300, 0, 0, 1};
   int tried = 0;
   auto apply = [&](const mcb200_batch_tuning &t) {
     b->blocks_per_sm = t.flight_blocks_per_sm;
     b->overlap = t.overlap != 0;
     b->pair_solves = t.pair_solves != 0;
-    for (mcb200_ctx *c : b->m) c->grid_per_sm = t.grid_per_sm;
+    for (mcb200_ctx *c : b->m) {
+      c->grid_per_sm = t.grid_per_sm;
+      mcb200_set_sort_bucket(c, t.sort_bucket);
+    }
     cudaSetDevice(b->device);
     cudaStreamSynchronize(b->stream);
     b->drop_graphs();  // the graphs hold the previous launch shapes
@@ -555,9 +559,10 @@ int mcb200_batch_autotune(mcb200_batch *b, int trial_steps, mcb200_batch_tuning 
     return MCB200_OK;
   };
   const int overlap0 = b->overlap ? 1 : 0, pair0 = b->pair_solves ? 1 : 0;
+  const int bucket0 = b->m.empty() ? 1 : mcb200_get_sort_bucket(b->m[0]);
   std::vector<mcb200_batch_tuning> shapes;
   for (int fb : flight_blocks)
-    for (int gs : grid_per_sm) shapes.push_back(mcb200_batch_tuning{fb, gs, overlap0, 0.0, 0, pair0});
+    for (int gs : grid_per_sm) shapes.push_back(mcb200_batch_tuning{fb, gs, overlap0, 0.0, 0, pair0, bucket0});
   if (int rc = stage(shapes)) return rc;
   std::vector<mcb200_batch_tuning> modes;  // overlap and pairing, with the fastest launch shapes
   for (int v = 0; v < 4; ++v) {
@@ -567,7 +572,16 @@ int mcb200_batch_autotune(mcb200_batch *b, int trial_steps, mcb200_batch_tuning 
     modes.push_back(t);
   }
   if (int rc = stage(modes)) return rc;
-  tried -= 1;  // the fastest shape was timed in both stages
+  std::vector<mcb200_batch_tuning> widths;  // sort-bucket widths, with the fastest of the above
+  widths.push_back(win);
+  for (int w : sort_buckets)
+    if (w != win.sort_bucket) {
+      mcb200_batch_tuning t = win;
+      t.sort_bucket = w;
+      widths.push_back(t);
+    }
+  if (int rc = stage(widths)) return rc;
+  tried -= 2;  // each stage's first candidate is the previous stage's winner
   win.candidates = tried;
   apply(win);
   if (best) *best = win;

@@ -594,6 +594,17 @@ int mcb200_set_flight_precision(mcb200_ctx *c, int precision) {
 
 int mcb200_get_flight_precision(const mcb200_ctx *c) { return c ? c->precision : -1; }
 
+int mcb200_set_sort_bucket(mcb200_ctx *c, int cells_per_bucket) {
+  if (!c || cells_per_bucket < 1 || cells_per_bucket > 64 || (cells_per_bucket & (cells_per_bucket - 1)))
+    return MCB200_ERR_ARG;
+  int shift = 0;
+  while ((1 << shift) < cells_per_bucket) ++shift;
+  c->sort_shift = shift;  // read when the next step's sort is launched (or captured)
+  return MCB200_OK;
+}
+
+int mcb200_get_sort_bucket(const mcb200_ctx *c) { return c ? 1 << c->sort_shift : -1; }
+
 const char *mcb200_last_error(const mcb200_ctx *ctx) { return ctx ? ctx->error.c_str() : "null context"; }
 
 int mcb200_units(const mcb200_ctx *c, double *out, int n) {
@@ -1514,7 +1525,7 @@ int mcb200_multiple_refresh(mcb200_ctx *c, const int32_t *desired_e, const int32
     auto refresh = [&](auto tag) {
       using R = decltype(tag);
       launch_cell_sort(store<R>(c, c->cur), DevCount{c->dev_counts, nullptr, (int)c->capacity}, store<R>(c, sorted),
-                       cells, c->mesh.nx, c->mesh.nz, c->hist, c->offsets, c->tile_sums, c->total,
+                       cells, c->mesh.nx, c->mesh.nz, c->hist, c->offsets, c->tile_sums, c->total, 0,
                        grid_for(c, c->capacity, 256), s);
       const DevParticlesT<R> &P = store<R>(c, sorted);
       launch_refresh_count(P, c->offsets, c->hist, cells, de, dh, r, w.order, out_count, new_count, s);
@@ -1949,8 +1960,8 @@ void step_tail(mcb200_ctx *c) {
   c->launches += 1;
   const int other = 1 - c->cur;
   launch_cell_sort(store<R>(c, c->cur), DevCount{c->dev_counts, c->append_count, cap}, store<R>(c, other), c->ncells,
-                   c->mesh.nx, c->mesh.nz, c->hist, c->offsets, c->tile_sums, c->total, grid_for(c, c->capacity, 256),
-                   s);
+                   c->mesh.nx, c->mesh.nz, c->hist, c->offsets, c->tile_sums, c->total, c->sort_shift,
+                   grid_for(c, c->capacity, 256), s);
   launch_step_finish(c->dev_counts, c->total, c->dev_counts + 1, c->append_count, c->dev_psteps, s);
   ck(cudaGetLastError(), "cell sort");
   c->launches += 6;

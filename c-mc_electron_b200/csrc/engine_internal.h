@@ -206,6 +206,7 @@ struct mcb200_ctx {
   bool qc_set = false, qc_on = false;
   int sm_count = 148;
   int grid_per_sm = 8;  // blocks per SM of the grid-stride per-step kernels (sort, deposition, copies)
+  int sort_shift = 0;   // the step's counting sort groups 2^sort_shift consecutive cells (mcb200_set_sort_bucket)
   // deposition / Poisson (mcb200_set_device)
   FieldBuffers fb{};
   CgPlan cg_plan;

@@ -61,10 +61,11 @@ void launch_exclusive_scan(const unsigned int *in, unsigned int *out, unsigned i
                            int n, cudaStream_t s);
 // Counting sort of the live particles among the first n (device count) of
 // `src` by cell into `dst`; *total = live particles, offsets = cell starts
-// (after the scatter: cell ends).
+// (after the scatter: cell ends).  With shift > 0 the keys are buckets of
+// 2^shift consecutive cells (hist and offsets per bucket).
 template <typename R>
 void launch_cell_sort(const DevParticlesT<R> &src, DevCount n, const DevParticlesT<R> &dst, int ncells, int nx,
                       int nz, unsigned int *hist, unsigned int *offsets, unsigned int *tile_sums, unsigned int *total,
-                      int grid, cudaStream_t s);
+                      int shift, int grid, cudaStream_t s);
 
 }  // namespace mcb200

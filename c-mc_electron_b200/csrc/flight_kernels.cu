@@ -314,11 +314,14 @@ __device__ __forceinline__ int cell_linear(uint32_t c, int nx, int nz) {
   return (int)((((c >> 10) & 1023) * nx + (c & 1023)) * nz + ((c >> 20) & 1023));
 }
 
+// Buckets of 2^shift consecutive cells of the linear order (z fastest):
+// shift 0 sorts by cell; wider buckets make the histogram and its scan
+// shorter and leave the particles of a bucket in arrival order.
 __global__ void cell_histogram(const uint32_t *cell, const uint32_t *meta, DevCount count, int nx, int nz,
-                               unsigned int *hist) {
+                               unsigned int *hist, int shift) {
   const int n = count.get();
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
-    if (!(meta[p] & kMetaDead)) atomicAdd(&hist[cell_linear(cell[p], nx, nz)], 1u);
+    if (!(meta[p] & kMetaDead)) atomicAdd(&hist[cell_linear(cell[p], nx, nz) >> shift], 1u);
 }
 
 // Exclusive scan of `count` values, single pass per 1024-wide tile plus a
@@ -367,12 +370,12 @@ __global__ void scan_add(unsigned int *out, const unsigned int *tile_sums, int n
 
 template <typename R>
 __global__ void cell_scatter(DevParticlesT<R> src, DevCount count, DevParticlesT<R> dst, unsigned int *cursor, int nx,
-                             int nz) {
+                             int nz, int shift) {
   const int n = count.get();
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
     const uint32_t m = src.meta[p];
     if (m & kMetaDead) continue;
-    const unsigned int q = atomicAdd(&cursor[cell_linear(src.cell[p], nx, nz)], 1u);
+    const unsigned int q = atomicAdd(&cursor[cell_linear(src.cell[p], nx, nz) >> shift], 1u);
     dst.x[q] = src.x[p]; dst.y[q] = src.y[p]; dst.z[q] = src.z[p];
     dst.kx[q] = src.kx[p]; dst.ky[q] = src.ky[p]; dst.kz[q] = src.kz[p];
     dst.energy[q] = src.energy[p]; dst.charge[q] = src.charge[p];
@@ -647,14 +650,15 @@ void launch_exclusive_scan(const unsigned int *in, unsigned int *out, unsigned i
 template <typename R>
 void launch_cell_sort(const DevParticlesT<R> &src, DevCount n, const DevParticlesT<R> &dst, int ncells, int nx,
                       int nz, unsigned int *hist, unsigned int *offsets, unsigned int *tile_sums, unsigned int *total,
-                      int grid, cudaStream_t s) {
-  cudaMemsetAsync(hist, 0, sizeof(unsigned int) * ncells, s);
-  cell_histogram<<<grid, 256, 0, s>>>(src.cell, src.meta, n, nx, nz, hist);
-  const int tiles = (ncells + 1023) / 1024;
-  scan_tiles<<<tiles, 1024, 0, s>>>(hist, offsets, tile_sums, ncells);
+                      int shift, int grid, cudaStream_t s) {
+  const int buckets = (ncells + (1 << shift) - 1) >> shift;
+  cudaMemsetAsync(hist, 0, sizeof(unsigned int) * buckets, s);
+  cell_histogram<<<grid, 256, 0, s>>>(src.cell, src.meta, n, nx, nz, hist, shift);
+  const int tiles = (buckets + 1023) / 1024;
+  scan_tiles<<<tiles, 1024, 0, s>>>(hist, offsets, tile_sums, buckets);
   scan_tile_sums<<<1, 1024, 0, s>>>(tile_sums, tiles, total);
-  scan_add<<<tiles, 1024, 0, s>>>(offsets, tile_sums, ncells);
-  cell_scatter<R><<<grid, 256, 0, s>>>(src, n, dst, offsets, nx, nz);
+  scan_add<<<tiles, 1024, 0, s>>>(offsets, tile_sums, buckets);
+  cell_scatter<R><<<grid, 256, 0, s>>>(src, n, dst, offsets, nx, nz, shift);
 }
 
 #define MCB200_INSTANTIATE(R)                                                                                   \
@@ -670,7 +674,7 @@ void launch_cell_sort(const DevParticlesT<R> &src, DevCount n, const DevParticle
   template int launch_batch_flight<R>(const FlightCtxT<R> &, const BatchInstT<R> *, int, uint64_t,             \
                                       const uint32_t *, bool, unsigned int *, int, int, cudaStream_t);          \
   template void launch_cell_sort<R>(const DevParticlesT<R> &, DevCount, const DevParticlesT<R> &, int, int, int, \
-                                    unsigned int *, unsigned int *, unsigned int *, unsigned int *, int,        \
+                                    unsigned int *, unsigned int *, unsigned int *, unsigned int *, int, int,   \
                                     cudaStream_t);
 MCB200_INSTANTIATE(double)
 MCB200_INSTANTIATE(float)

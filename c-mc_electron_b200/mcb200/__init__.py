@@ -93,7 +93,8 @@ class BatchMember(ctypes.Structure):
 
 class BatchTuning(ctypes.Structure):
     _fields_ = [("flight_blocks_per_sm", ctypes.c_int), ("grid_per_sm", ctypes.c_int), ("overlap", ctypes.c_int),
-                ("ms_per_step", ctypes.c_double), ("candidates", ctypes.c_int), ("pair_solves", ctypes.c_int)]
+                ("ms_per_step", ctypes.c_double), ("candidates", ctypes.c_int), ("pair_solves", ctypes.c_int),
+                ("sort_bucket", ctypes.c_int)]
 
 
 class ServerOptions(ctypes.Structure):
@@ -247,6 +248,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mcb200_set_heat_tally.argtypes = [vp, c.c_int]
     lib.mcb200_set_flight_precision.argtypes = [vp, c.c_int]
     lib.mcb200_get_flight_precision.argtypes = [vp]
+    if hasattr(lib, "mcb200_set_sort_bucket"):
+        lib.mcb200_set_sort_bucket.argtypes = [vp, c.c_int]
+        lib.mcb200_get_sort_bucket.argtypes = [vp]
     return lib
 
 
@@ -331,6 +335,15 @@ class Engine:
     @property
     def precision(self) -> int:
         return self._lib.mcb200_get_flight_precision(self._ctx)
+
+    def set_sort_bucket(self, cells_per_bucket: int):
+        """Cells per bucket of the step's counting sort (a power of two,
+        1-64); results do not depend on it."""
+        self._check(self._lib.mcb200_set_sort_bucket(self._ctx, cells_per_bucket), "mcb200_set_sort_bucket")
+
+    @property
+    def sort_bucket(self) -> int:
+        return self._lib.mcb200_get_sort_bucket(self._ctx)
 
     def units(self) -> dict:
         out = np.zeros(len(UNIT_NAMES))

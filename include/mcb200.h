@@ -103,6 +103,19 @@ const char *mcb200_last_error(const mcb200_ctx *ctx);
 int mcb200_set_flight_precision(mcb200_ctx *ctx, int precision);
 int mcb200_get_flight_precision(const mcb200_ctx *ctx);
 
+/* Sort-bucket width of the step's counting sort (the reference's
+ * local_migrate, src/mcmodel.cpp:1615-1638, moves particles between its
+ * per-cell lists): the store is
+ * grouped by buckets of `cells_per_bucket` consecutive cells of the linear
+ * order (z fastest), a power of two from 1 (by cell, the default) to 64.
+ * Wider buckets shorten the histogram and its scan and leave a bucket's
+ * particles in arrival order.  Results do not depend on it (tallies are
+ * fixed point, draws per particle); only the speed of the sort and of the
+ * passes over the sorted store does.  ERR_ARG for other widths.  The
+ * refresh's own sort stays per cell. */
+int mcb200_set_sort_bucket(mcb200_ctx *ctx, int cells_per_bucket);
+int mcb200_get_sort_bucket(const mcb200_ctx *ctx);
+
 /* Normalisation scales (MeshQuantities::init_phpysical_parameter,
  * src/mcmodel.cpp:4007-4122): out[0..n) = T0, eV0, spr0, time0, conc0,
  * field0, scrt0, pot0, a0pi, sieg, eps_silicon, eps_oxide, curr0, dens0. */
@@ -369,18 +382,21 @@ int mcb200_batch_use_graphs(mcb200_batch *batch, int enable);
 /* Launch shapes picked by measurement: for every candidate (batched-flight
  * blocks per SM in {1, 2} x blocks per SM of the members' per-step kernels
  * -- sort, deposition, copies -- in {2, 4, 8}; then the fastest of those
- * with overlap, pairing and both switched) one untimed and `trial_steps`
- * timed full timesteps (mcb200_batch_run: they advance the simulations like
- * any other steps).  The candidates of each of the two stages are timed in
- * order and again in reverse order, so that a steady drift of the
- * simulations (particle counts) cancels; the fastest mean device time is
- * kept and returned. */
+ * with overlap, pairing and both switched; then the fastest of those with
+ * the members' sort-bucket width in {1, 2, 4, 8} cells,
+ * mcb200_set_sort_bucket) one untimed and `trial_steps` timed full
+ * timesteps (mcb200_batch_run: they advance the simulations like any other
+ * steps).  The candidates of each of the three stages are timed in order
+ * and again in reverse order, so that a steady drift of the simulations
+ * (particle counts) cancels; the fastest mean device time is kept and
+ * returned. */
 typedef struct {
   int flight_blocks_per_sm, grid_per_sm;
   int overlap; /* mcb200_batch_set_overlap */
   double ms_per_step;  /* of the kept setting */
   int candidates;
   int pair_solves; /* mcb200_batch_set_pairing */
+  int sort_bucket; /* cells per sort bucket of every member */
 } mcb200_batch_tuning;
 int mcb200_batch_autotune(mcb200_batch *batch, int trial_steps, mcb200_batch_tuning *best);
 /* Wait for the batch and every member; reports a member's full store. */

@@ -207,3 +207,57 @@ def test_batch_rejects_mixed_tables():
         mcb200.Batch([(a, dt, 1, 0), (b, dt, 2, 0)])
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("precision", [mcb200.FLIGHT_FP64, mcb200.FLIGHT_FP32])
+def test_sort_bucket_width_leaves_results_unchanged(precision):
+    """Members whose step sort groups 8 (FinFETs) or 4 (bulk boxes) cells per
+    bucket (mcb200_set_sort_bucket) end bit-identical to twins sorted by
+    cell, stepped alone: the order of the store changes, no result does."""
+    with tempfile.TemporaryDirectory() as t1, tempfile.TemporaryDirectory() as t2:
+        alone = build(t1, precision)
+        batched = build(t2, precision, like=alone[0][0])
+    for eng, _, _, sc in batched:
+        eng.set_sort_bucket(8 if sc else 4)
+        assert eng.sort_bucket == (8 if sc else 4)
+    with pytest.raises(mcb200.EngineError):
+        batched[0][0].set_sort_bucket(3)
+    assert batched[0][0].sort_bucket == 4
+    first = [0, 3, 5, 2]
+    for step in range(STEPS):
+        for (eng, dt, seed, sc), f in zip(alone, first):
+            density(eng, f + step, sc)
+            eng.step(f + step, seed, dt)
+    batch = mcb200.Batch([(eng, dict(dt=dt, seed=seed, first_step=f, self_consistent=int(sc),
+                                      poisson_every=POISSON_EVERY))
+                          for (eng, dt, seed, sc), f in zip(batched, first)])
+    batch.use_graphs(True)
+    batch.run(STEPS)
+    batch.sync()
+    for (ea, *_), (eb, *_) in zip(alone, batched):
+        a, b = by_uid(ea), by_uid(eb)
+        for k in a:
+            assert np.array_equal(a[k], b[k]), k
+        same_tallies(ea.tallies(), eb.tallies())
+    for k in (2, 3):
+        pa, pb = alone[k][0].array("potential"), batched[k][0].array("potential")
+        assert np.array_equal(pa.view(np.uint64), pb.view(np.uint64))
+    batch.close()
+    for eng, *_ in batched + alone:
+        eng.close()
+
+
+def test_autotune_picks_a_sort_bucket():
+    """The autotuner's three stages (launch shapes, overlap / pairing, sort
+    buckets) end on a setting it timed, and the members keep its width."""
+    with tempfile.TemporaryDirectory() as tmp:
+        members = build(tmp, mcb200.FLIGHT_FP32)
+    batch = mcb200.Batch([(eng, dict(dt=dt, seed=seed, first_step=0, self_consistent=int(sc),
+                                      poisson_every=POISSON_EVERY)) for eng, dt, seed, sc in members])
+    batch.use_graphs(True)
+    t = batch.autotune(2)
+    assert t["sort_bucket"] in (1, 2, 4, 8) and t["candidates"] == 12 and t["ms_per_step"] > 0
+    assert all(eng.sort_bucket == t["sort_bucket"] for eng, *_ in members)
+    batch.close()
+    for eng, *_ in members:
+        eng.close()
