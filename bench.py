@@ -368,9 +368,9 @@ def serve_arm(args, device: int) -> dict:
     (Vg 0-0.8 V in 0.05 V steps x Vd {0.05, 0.7} V x Lg {15, 20, 30} nm,
     50k-1M particles log-uniform) arriving as a Poisson process of 4 req/s
     (seed 5); FP32 flight, HBM budget 160 GB, one Ids window per 50-step
-    round (the drain's induced current, Ramo-Shockley), each
+    round (net flux through the middle third of the section planes), each
     request done when stderr(Ids) < 1% of |Ids| after 6 transient windows
-    (2 after a warm start) or at 2000 steps.  Latency = completion - arrival
+    (2 after a warm start) or at the step cap (2000 by default).  Latency = completion - arrival
     (server clock); throughput = particle-steps over the rounds' device time."""
     import mcb200
     from mcb200 import serving
@@ -379,23 +379,28 @@ def serve_arm(args, device: int) -> dict:
         reqs = serving.make_requests(tmp, n=SERVE_REQUESTS, seed=5, rate=4.0)
         srv = mcb200.Server(device=device, precision=mcb200.FLIGHT_FP32, quantum_steps=SERVE_QUANTUM)
         with ClockSampler(device) as clocks:
-            res, st, wall = serving.serve(srv, reqs, max_wall_s=900, max_steps=SERVE_MAX_STEPS, min_windows=5,
+            res, st, wall = serving.serve(srv, reqs, max_wall_s=900, max_steps=args.serve_max_steps, min_windows=5,
                                           warm_windows_cold=6, warm_windows_warm=2, poisson_every=10,
-                                          target_rel_err=0.01, ids_estimator=mcb200.IDS_INDUCED)
+                                          target_rel_err=0.01, ids_estimator=mcb200.IDS_SECTIONS)
         srv.close()
     lat = serving.latency_summary(res)
     status = [r["status"] for r in res]
+    by_id = {r["id"]: r for r in reqs}
+    rel = [abs(r["ids_stderr"] / r["ids"]) if r["ids"] else float("inf") for r in res]
+    per_request = [[by_id[r["id"]]["lg_nm"], by_id[r["id"]]["vg"], by_id[r["id"]]["vd"], r["particles"], r["steps"],
+                    round(e, 4), r["status"], round(r["done_s"] - r["arrival_s"], 2)] for r, e in zip(res, rel)]
     return {"metric": "bias-point latency", "unit": "s", "p50_s": lat.get("p50_s"), "p99_s": lat.get("p99_s"),
             "mean_s": lat.get("mean_s"), "requests": SERVE_REQUESTS, "completed": len(res),
             "converged": status.count(mcb200.SERVE_CONVERGED), "step_limited": status.count(mcb200.SERVE_STEP_LIMIT),
             "warm_started": sum(1 for r in res if r["warm_from"]),
             "throughput_particle_steps_per_s": st["particle_steps"] / (st["device_ms"] * 1e-3),
             "particle_steps": st["particle_steps"], "rounds": st["rounds"], "wall_s": wall,
-            "median_rel_stderr": float(statistics.median(abs(r["ids_stderr"] / r["ids"]) for r in res if r["ids"]))
-            if res else None,
+            "median_rel_stderr": float(statistics.median(rel)) if res else None,
+            "per_request": per_request,
+            "per_request_fields": ["lg_nm", "vg", "vd", "particles", "steps", "rel_stderr", "status", "latency_s"],
             "clocks": clocks.summary(),
             "config": "32 FinFET bias points, Poisson arrivals 4 req/s, 50k-1M particles, 160 GB budget, "
-                      "target 1% Ids stderr, 2000-step cap, 50-step rounds, FP32 flight"}
+                      f"target 1% Ids stderr, {args.serve_max_steps}-step cap, 50-step rounds, FP32 flight"}
 
 
 # ------------------------------------------------------------ reference (CPU)
@@ -531,9 +536,11 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--particles", type=int, default=2_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="all", choices=["all", "finfet", "batch", "serve"],
+    ap.add_argument("--workload", default="all", choices=["all", "finfet", "finfet32", "batch", "serve"],
                     help="finfet: only the two FinFET arms (no e2e rerun, no bulk box): for profiling; "
-                         "batch: only the batching arm")
+                         "finfet32: one FP32 run of the FinFET deck alone (profiling); batch: only the batching arm")
+    ap.add_argument("--serve-max-steps", type=int, default=SERVE_MAX_STEPS,
+                    help="serving: a request's step cap (it completes earlier when stderr(Ids) < 1%% of Ids)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -544,6 +551,12 @@ def main():
         out = batch_arm(args, local)
     elif args.workload == "serve":
         out = serve_arm(args, local)
+    elif args.workload == "finfet32":
+        r = finfet_run(args, local, "fp32")
+        out = {"workload": "finfet32", "ms_per_step": r["timed_device_ms"] / max(r["timed_steps"], 1),
+               "timed_particle_steps": r["timed_particle_steps"], "timed_steps": r["timed_steps"],
+               "flight_ms_per_launch": r["timed_flight_ms"] / max(r["timed_flight_launches"], 1),
+               "clocks": r["clocks"]}
     else:
         out = engine_arm(args, rank, world, local)
         if args.workload == "all":

@@ -6,16 +6,28 @@ the reference's routines, so it stands for the CPU oracle too).
 The box is the bulk workload's (N_D = 1e17 cm^-3, 300 K, dt = 1 fs, 5 nm
 cells, REFLECT on every face) stretched to 1 um along the field (200 x 10 x
 10 cells) so that within the 0.8 ps measured few electrons reach the far
-wall.  Per field and precision: warm-up steps, then `blocks` windows of
-`block_steps` steps, each averaged with the window statistics
+wall.  Per field, precision and seed: warm-up steps, then `blocks` windows
+of `block_steps` steps, each averaged with the window statistics
 (statistic(), src/mcmodel.cpp:1167-1408): drift velocity
 <v_x> = sum |q| v_x / sum |q| (m/s), mean energy sum |q| E / sum |q| (eV);
 from the store at the end: valley occupation (isym / 8); from the tallies:
-real phonon and impurity events per particle-step.  Standard errors are
-batch means over the windows (velocity, energy), binomial (valleys) and
-Poisson (event counts).
+real phonon and impurity events per particle-step.
 
-    python -m mcb200.precision [--electrons 100000] [--json out.json]
+Errors are statistics over independent runs (seeds): a run's observable is
+its time average, the standard error of a precision's mean is the spread of
+its runs over sqrt(runs), and a difference is judged in units of the
+combined standard error against the Student-t quantile of the 3-sigma
+(99.73 %) level for its degrees of freedom.  Windows of one run are not
+independent (the ensemble's mean energy and velocity relax over ~0.1-1 ps,
+longer than a window), so batch means over them understate the error.
+
+The FinFET half (finfet_report) runs the throughput FinFET the same way in
+both precisions and compares both with the reference's own routines run
+through the same protocol (tests/golden/finfet_oracle_windows.json).
+
+    python -m mcb200.precision [--electrons 100000] [--seeds 8] [--json out.json]
+    python -m mcb200.precision --finfet [--finfet-seeds 6] \
+        [--oracle-runs tests/golden/finfet_oracle_windows.json] [--json out.json]
 """
 from __future__ import annotations
 
@@ -82,29 +94,49 @@ def run_field(field_kv_cm: float, precision: int, electrons: int = 100000, warmu
     }
 
 
-def compare(fp64: dict, fp32: dict) -> dict:
-    """Relative error of every FP32 observable against FP64, and the same in
-    combined standard errors."""
-    out = {}
-    for key, se in (("drift_velocity_m_s", "drift_velocity_se"), ("mean_energy_ev", "mean_energy_se"),
-                    ("phonon_per_particle_step", "phonon_se"), ("impurity_per_particle_step", "impurity_se")):
-        a, b = fp64[key], fp32[key]
-        sig = float(np.hypot(fp64[se], fp32[se]))
-        out[key] = {"fp64": a, "fp32": b, "rel_error": (b - a) / a if a else 0.0,
-                    "sigmas": (b - a) / sig if sig > 0 else 0.0}
-    va, vb = np.array(fp64["valley"]), np.array(fp32["valley"])
-    sa, sb = np.array(fp64["valley_se"]), np.array(fp32["valley_se"])
-    out["valley_max_sigmas"] = float(np.max(np.abs(vb - va) / np.hypot(sa, sb)))
-    out["valley_max_abs_error"] = float(np.max(np.abs(vb - va)))
+def three_sigma_limit(dof: float) -> float:
+    """The two-sided 99.73 % quantile (3 sigma for a normal variable) of
+    Student's t with `dof` degrees of freedom."""
+    from scipy.stats import t
+
+    return float(t.ppf(0.99865, max(dof, 1.0)))
+
+
+def compare_samples(ref, test) -> dict:
+    """Mean of `test` against mean of `ref` (each a list of independent run
+    values): relative error, the difference in combined standard errors, and
+    the 3-sigma-level limit for the Welch degrees of freedom."""
+    a, b = np.asarray(ref, dtype=float), np.asarray(test, dtype=float)
+    va, vb = a.var(ddof=1) / len(a), b.var(ddof=1) / len(b)
+    se = float(np.sqrt(va + vb))
+    dof = (va + vb) ** 2 / (va ** 2 / (len(a) - 1) + vb ** 2 / (len(b) - 1)) if va + vb > 0 else 1e9
+    d = float(b.mean() - a.mean())
+    return {"ref": float(a.mean()), "test": float(b.mean()), "rel_error": d / abs(a.mean()) if a.mean() else 0.0,
+            "sigmas": d / se if se > 0 else 0.0, "se": se, "dof": float(dof), "limit": three_sigma_limit(dof)}
+
+
+SWEEP_KEYS = ("drift_velocity_m_s", "mean_energy_ev", "phonon_per_particle_step", "impurity_per_particle_step")
+
+
+def compare(fp64_runs: list, fp32_runs: list) -> dict:
+    """Every FP32 observable against FP64, over independent runs."""
+    out = {key: compare_samples([r[key] for r in fp64_runs], [r[key] for r in fp32_runs]) for key in SWEEP_KEYS}
+    va = np.array([r["valley"] for r in fp64_runs])
+    vb = np.array([r["valley"] for r in fp32_runs])
+    valleys = [compare_samples(va[:, v], vb[:, v]) for v in range(va.shape[1])]
+    out["valley_max_sigmas"] = float(max(abs(c["sigmas"]) / c["limit"] * 3.0 for c in valleys))
+    out["valley_max_abs_error"] = float(np.max(np.abs(vb.mean(0) - va.mean(0))))
     return out
 
 
 def sweep(electrons: int = 100000, warmup: int = 300, blocks: int = 5, block_steps: int = 100,
-          fields=FIELDS_KV_CM, device: int = 0) -> list:
+          fields=FIELDS_KV_CM, seeds: int = 8, device: int = 0) -> list:
     rows = []
     for f in fields:
-        r64 = run_field(f, FLIGHT_FP64, electrons, warmup, blocks, block_steps, device=device)
-        r32 = run_field(f, FLIGHT_FP32, electrons, warmup, blocks, block_steps, device=device)
+        r64 = [run_field(f, FLIGHT_FP64, electrons, warmup, blocks, block_steps, seed=11 + k, device=device)
+               for k in range(seeds)]
+        r32 = [run_field(f, FLIGHT_FP32, electrons, warmup, blocks, block_steps, seed=11 + k, device=device)
+               for k in range(seeds)]
         rows.append({"field_kv_cm": f, "fp64": r64, "fp32": r32, "error": compare(r64, r32)})
     return rows
 
@@ -219,35 +251,27 @@ def run_finfet(precision: int, seed: int = 1, warmup: int = FINFET_WARMUP, windo
     return out
 
 
-def compare_windows(ref: list, test: list) -> dict:
-    """Per observable: relative error of the test run's mean over the windows
-    against the reference run's, and that difference in standard errors.
-    The runs follow the same protocol from statistically equivalent starts
-    on independent random streams, so window w of one run and window w of
-    the other estimate the same transient value: the error is the mean of
-    the window-by-window differences and its standard error theirs (the
-    transient's drift cancels in each difference)."""
-    out = {}
-    for key in FINFET_OBSERVABLES:
-        a = np.array([w[key] for w in ref])
-        b = np.array([w[key] for w in test])
-        diff = b - a
-        se = float(diff.std(ddof=1) / np.sqrt(len(diff)))
-        d = float(diff.mean())
-        out[key] = {"ref": float(a.mean()), "test": float(b.mean()),
-                    "rel_error": d / abs(a.mean()) if a.mean() else 0.0, "sigmas": d / se if se > 0 else 0.0}
-    return out
+def run_means(runs: list) -> list:
+    """Each run's time average of every observable over its windows."""
+    return [{key: float(np.mean([w[key] for w in r["windows"]])) for key in FINFET_OBSERVABLES} for r in runs]
 
 
-def finfet_report(seed: int = 1, device: int = 0, oracle_windows: list | None = None) -> dict:
-    """FP32 flight against all-FP64 flight on the FinFET (and both against
-    the reference's own windows when given)."""
-    r64 = run_finfet(FLIGHT_FP64, seed=seed, device=device)
-    r32 = run_finfet(FLIGHT_FP32, seed=seed, device=device)
-    rep = {"fp64": r64, "fp32": r32, "fp32_vs_fp64": compare_windows(r64["windows"], r32["windows"])}
-    if oracle_windows:
-        rep["fp64_vs_oracle"] = compare_windows(oracle_windows, r64["windows"])
-        rep["fp32_vs_oracle"] = compare_windows(oracle_windows, r32["windows"])
+def compare_runs(ref_runs: list, test_runs: list) -> dict:
+    """Per observable, the test runs' mean time average against the
+    reference runs' (compare_samples)."""
+    a, b = run_means(ref_runs), run_means(test_runs)
+    return {key: compare_samples([r[key] for r in a], [r[key] for r in b]) for key in FINFET_OBSERVABLES}
+
+
+def finfet_report(seeds=(1, 2, 3, 4, 5, 6), device: int = 0, oracle_runs: list | None = None) -> dict:
+    """FP32 flight against all-FP64 flight on the FinFET over independent
+    seeds (and both against the reference's own runs when given)."""
+    r64 = [run_finfet(FLIGHT_FP64, seed=s, device=device) for s in seeds]
+    r32 = [run_finfet(FLIGHT_FP32, seed=s, device=device) for s in seeds]
+    rep = {"fp64": r64, "fp32": r32, "fp32_vs_fp64": compare_runs(r64, r32)}
+    if oracle_runs:
+        rep["fp64_vs_oracle"] = compare_runs(oracle_runs, r64)
+        rep["fp32_vs_oracle"] = compare_runs(oracle_runs, r32)
     return rep
 
 
@@ -257,16 +281,39 @@ def main():
     ap.add_argument("--warmup", type=int, default=300)
     ap.add_argument("--blocks", type=int, default=5)
     ap.add_argument("--block-steps", type=int, default=100)
+    ap.add_argument("--seeds", type=int, default=8)
     ap.add_argument("--json", default=None)
+    ap.add_argument("--finfet", action="store_true", help="the FinFET half instead of the bulk sweep")
+    ap.add_argument("--finfet-seeds", type=int, default=6)
+    ap.add_argument("--oracle-runs", default=None,
+                    help="FinFET: a JSON file of the reference's runs of the same protocol ({'runs': [...]})")
     a = ap.parse_args()
-    rows = sweep(a.electrons, a.warmup, a.blocks, a.block_steps)
+    if a.finfet:
+        oracle = None
+        if a.oracle_runs:
+            with open(a.oracle_runs) as f:
+                oracle = json.load(f)["runs"]
+        rep = finfet_report(seeds=tuple(range(1, a.finfet_seeds + 1)), oracle_runs=oracle)
+        pairs = [k for k in ("fp32_vs_fp64", "fp64_vs_oracle", "fp32_vs_oracle") if k in rep]
+        print(f"{'observable':>22} {'pair':>15} {'ref':>12} {'test':>12} {'rel':>9} {'sig':>6} {'limit':>6}")
+        for key in FINFET_OBSERVABLES:
+            for pair in pairs:
+                e = rep[pair][key]
+                print(f"{key:>22} {pair:>15} {e['ref']:12.5g} {e['test']:12.5g} {e['rel_error']:9.2e} "
+                      f"{e['sigmas']:6.2f} {e['limit']:6.2f}")
+        if a.json:
+            with open(a.json, "w") as f:
+                json.dump({k: rep[k] for k in pairs} | {"fp64_means": run_means(rep["fp64"]),
+                                                        "fp32_means": run_means(rep["fp32"])}, f, indent=1)
+        return
+    rows = sweep(a.electrons, a.warmup, a.blocks, a.block_steps, seeds=a.seeds)
     print(f"{'E kV/cm':>8} {'vd FP64 m/s':>12} {'vd FP32':>12} {'rel':>8} {'sig':>5}  "
           f"{'E FP64 eV':>9} {'E FP32':>9} {'rel':>8} {'sig':>5}  {'imp rel':>8} {'ph rel':>8} {'valley sig':>10}")
     for r in rows:
         e = r["error"]
         v, en = e["drift_velocity_m_s"], e["mean_energy_ev"]
-        print(f"{r['field_kv_cm']:8.0f} {v['fp64']:12.4g} {v['fp32']:12.4g} {v['rel_error']:8.1e} {v['sigmas']:5.1f}  "
-              f"{en['fp64']:9.4f} {en['fp32']:9.4f} {en['rel_error']:8.1e} {en['sigmas']:5.1f}  "
+        print(f"{r['field_kv_cm']:8.0f} {v['ref']:12.4g} {v['test']:12.4g} {v['rel_error']:8.1e} {v['sigmas']:5.1f}  "
+              f"{en['ref']:9.4f} {en['test']:9.4f} {en['rel_error']:8.1e} {en['sigmas']:5.1f}  "
               f"{e['impurity_per_particle_step']['rel_error']:8.1e} {e['phonon_per_particle_step']['rel_error']:8.1e} "
               f"{e['valley_max_sigmas']:10.1f}")
     if a.json:

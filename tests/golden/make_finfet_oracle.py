@@ -15,7 +15,11 @@ Window sums are read with set_stat_zero() between windows and turned into
 observables by mcb200.precision.finfet_observables, the function the
 engine's windows go through.
 
-    python tests/golden/make_finfet_oracle.py [--seed 1] [--out ...]
+    python tests/golden/make_finfet_oracle.py [--seeds 1 2 3 4 5 6] [--jobs 6] [--out ...]
+
+One run per seed, the runs in parallel processes; the fixture holds every
+run's windows (statistics across independent seeds give honest standard
+errors: windows of one run are correlated).
 """
 import argparse
 import json
@@ -35,17 +39,13 @@ from mcb200 import decks, precision as P  # noqa: E402
 from oracle_bridge import Oracle  # noqa: E402
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--out", default=os.path.join(HERE, "finfet_oracle_windows.json"))
-    a = ap.parse_args()
+def run(seed: int) -> dict:
     warmup, windows, wsteps = P.FINFET_WARMUP, P.FINFET_WINDOWS, P.FINFET_WINDOW_STEPS
     with tempfile.TemporaryDirectory() as tmp:
         d = decks.finfet(tmp, total_step=warmup + windows * wsteps, heat_steps=0, compute_heat=False,
                          mr_step=P.FINFET_MR_STEP)
         orc = Oracle()
-        orc.init(d["input"], seed=a.seed)
+        orc.init(d["input"], seed=seed)
     u = {k: orc.scalar(k) for k in ("spr0", "time0", "eV0", "curr0")}
     orc.set_scalar("SurfSc_delta", 0.4e-9 / u["spr0"])
     orc.set_scalar("SurfSc_ail", 1.5e-9 / u["spr0"])
@@ -82,11 +82,24 @@ def main():
                "electron_qe": float(orc.array("stat_energyE").sum()),
                "heat": float(orc.array("p_electron_heat").sum() + orc.array("p_hole_heat").sum())}
         rows.append(P.finfet_observables(win, u, dt, wsteps, ny))
-        print(f"window {w}: {rows[-1]}  ({time.time() - t0:.0f} s)", flush=True)
-    out = {"protocol": {"warmup": warmup, "windows": windows, "window_steps": wsteps,
-                        "poisson_every": P.FINFET_POISSON_EVERY, "mr_step": P.FINFET_MR_STEP, "seed": a.seed},
-           "particles_end": len(orc.particles()["x"]), "windows": rows,
-           "cpu_seconds": time.time() - t0}
+        print(f"seed {seed} window {w}: {rows[-1]}  ({time.time() - t0:.0f} s)", flush=True)
+    return {"seed": seed, "particles_end": len(orc.particles()["x"]), "windows": rows,
+            "cpu_seconds": time.time() - t0}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--seeds", type=int, nargs="+", default=[1, 2, 3, 4, 5, 6])
+    ap.add_argument("--jobs", type=int, default=6)
+    ap.add_argument("--out", default=os.path.join(HERE, "finfet_oracle_windows.json"))
+    a = ap.parse_args()
+    import multiprocessing as mp
+
+    with mp.get_context("spawn").Pool(min(a.jobs, len(a.seeds))) as pool:
+        runs = pool.map(run, a.seeds)
+    out = {"protocol": {"warmup": P.FINFET_WARMUP, "windows": P.FINFET_WINDOWS, "window_steps": P.FINFET_WINDOW_STEPS,
+                        "poisson_every": P.FINFET_POISSON_EVERY, "mr_step": P.FINFET_MR_STEP},
+           "runs": runs}
     with open(a.out, "w") as f:
         json.dump(out, f, indent=1)
 
