@@ -504,9 +504,10 @@ int orc_poisson_stencil(double *out) {
 
 /* MultipleRefresh (src/MultipleRefresh.cpp:60-143) cell by cell, with the
  * reference's own gen_new_par_mr (:9-58) doing the resampling.  The loop is
- * restated here only to fix the two things the engine defines: a cell's
- * particles are taken in uid order, and each (cell, carrier) draws from
- * stream (seed, cell, step, 0x4d520000 + carrier). */
+ * restated here only to fix the three things the engine defines: a cell's
+ * particles are taken in uid order, each (cell, carrier) draws from
+ * stream (seed, cell, step, 0x4d520000 + carrier), and resampled particles
+ * take new uids in (cell, carrier, draw) order. */
 int orc_multiple_refresh(uint32_t step) {
   MeshQuantities *mq = g_mq;
   int *e_num, *h_num;
@@ -525,6 +526,13 @@ int orc_multiple_refresh(uint32_t step) {
     for (int t = 0; t < 2; ++t) {
       set_stream((uint32_t)c, step, 0x4d520000u + (uint32_t)t);
       const bool redone = mq->gen_new_par_mr(vec[t], t == 0 ? e_num[c] : h_num[c], fresh[t]);
+      /* A resampled particle is a copy of an old one, par_id included; the
+       * reference's single random sequence sets the copies apart at once,
+       * but here draws are keyed by par_id, so each copy gets a uid of its
+       * own as the engine numbers them (cells in order, electrons then
+       * holes, draw order) -- else the copies would fly as one. */
+      if (redone)
+        for (Particle &p : fresh[t]) p.par_id = (int)g_next_uid++;
       for (const Particle &p : redone ? fresh[t] : vec[t]) lst.push_back(p);
     }
     mq->mr_gen_num += (int)lst.size() - (int)before;

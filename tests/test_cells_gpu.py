@@ -76,8 +76,10 @@ def test_multiple_refresh(preload):
     got = eng.download()
     assert gen == gen_ref
     assert len(got["x"]) == len(after["x"])
-    for f in ("x", "y", "z", "kx", "ky", "kz", "energy", "charge", "i", "j", "k", "itet", "isym", "type"):
+    for f in ("x", "y", "z", "kx", "ky", "kz", "energy", "charge", "i", "j", "k", "itet", "isym", "type", "uid"):
         assert np.array_equal(got[f], after[f]), f
+    # resampled particles are new ones: no uid appears twice
+    assert len(np.unique(got["uid"])) == len(got["uid"])
     eng.close()
 
 
