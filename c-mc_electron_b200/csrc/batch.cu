@@ -44,6 +44,12 @@ struct mcb200_batch {
   unsigned int *tickets = nullptr;  // device: work counters of the batched launches (main, 4 copy generations, side)
   bool overlap = true;              // fly the members not solving Poisson beside the solves
   bool pair_solves = true;          // two multigrid solves of the same shape per cooperative launch
+  bool smem_table = false;          // batched flights copy the member table into shared memory (else read in place)
+  // members that fly in launches of their own on their own streams (bit k),
+  // fixed by mcb200_batch_set_solo from the particle counts of that moment
+  uint64_t solo = 0;
+  size_t solo_min = 0;  // their smallest particle count (0: none solo)
+  cudaEvent_t ev_steps = nullptr;  // after the step numbers advanced
   std::vector<unsigned char> snap;  // per member: DevMesh, DevTallies and store parity the tables were built for
   uint64_t steps_done = 0, built_at = 0;
   int blocks_per_sm = 0;  // batched flight grid (0: as many as fit); mcb200_batch_autotune
@@ -62,6 +68,7 @@ struct mcb200_batch {
     if (ev_solved) cudaEventDestroy(ev_solved);
     if (ev_side) cudaEventDestroy(ev_side);
     if (ev_side0) cudaEventDestroy(ev_side0);
+    if (ev_steps) cudaEventDestroy(ev_steps);
     if (tables) cudaFree(tables);
     if (steps) cudaFree(steps);
     if (tickets) cudaFree(tickets);
@@ -106,7 +113,7 @@ void build_tables(mcb200_batch *b) {
     base.Y = c->y;
     base.dt = b->cfg[k].dt;
     base.seed = b->cfg[k].seed;
-    base.step = 0;  // from b->steps at launch
+    base.step = b->member_step[k];  // advanced with b->steps after every step
     base.n = c->dev_counts;
     base.capacity = (int)c->capacity;
     for (int par = 0; par < 2; ++par) {
@@ -155,10 +162,6 @@ bool tables_current(const mcb200_batch *b) {
   return true;
 }
 
-__global__ void advance_steps(uint32_t *steps, int n) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < n) steps[k] += 1;
-}
 
 void join_members(mcb200_batch *b);
 
@@ -174,59 +177,88 @@ uint64_t all_members(const mcb200_batch *b) {
 // Poisson solve); the others fly in the main launch on the batch stream,
 // after which a helper launch on the batch stream draws from the side
 // launch's work counter with the room the solves left.  The copy
-// generations of all members follow.  A particle's flight does not depend
+// generations of all batched members follow.  Solo members (b->solo) fly
+// in launches of their own on their own streams, as mcb200_step does, with
+// the step number read from b->steps.  A particle's flight does not depend
 // on the launch or block that carries it.
 template <typename R>
 void batch_transport(mcb200_batch *b, uint64_t early = 0) {
   const int n = (int)b->m.size();
   const uint64_t all = all_members(b);
-  early &= all;
-  if (early == all) early = 0;  // one launch
-  // 1. every member: counters and records for the step, then the stream of its flight waits for it
+  const uint64_t solo = b->solo & all, batched = all & ~solo;
+  early &= batched;
+  if (early == batched) early = 0;  // one launch
+  // 1. every member: counters and records for the step; a batched member's
+  //    flight stream waits for it, a solo member flies on at once
+  FlightCtxT<R> F;
+  F.T = b->m[0]->ts->dt;
   for (int k = 0; k < n; ++k) {
     mcb200_ctx *c = b->m[k];
     step_prepare<R>(c);
+    if ((solo >> k) & 1) {
+      FlightCtxT<R> Fk;
+      Fk.T = F.T;
+      Fk.M = c->mesh;
+      Fk.Y = c->y;
+      Fk.dt = b->cfg[k].dt;
+      Fk.seed = b->cfg[k].seed;
+      Fk.step = b->member_step[k];
+      Fk.step_dev = b->steps + k;  // graph replays run at later steps
+      enqueue_flights<R>(c, Fk, nullptr);
+      ck(cudaEventRecord(b->ev_member[k], c->stream), "event");  // its flights have read the step
+      continue;
+    }
     ck(cudaEventRecord(b->ev_member[k], c->stream), "event");
     ck(cudaStreamWaitEvent((early >> k) & 1 ? b->side : b->stream, b->ev_member[k], 0), "wait");
   }
   // 2. the batched flights
-  FlightCtxT<R> F;
-  F.T = b->m[0]->ts->dt;
   const int flip = (int)((b->steps_done - b->built_at) & 1);
   const BatchInstT<R> *tab = static_cast<const BatchInstT<R> *>(b->tables);
   const int sms = b->m[0]->sm_count;
   unsigned int *side_ticket = b->tickets + 1 + mcb200_ctx::kGenerations;
-  if (early) {
-    ck(cudaMemsetAsync(side_ticket, 0, sizeof(unsigned int), b->side), "memset");
-    ck(cudaEventRecord(b->ev_side0, b->side), "event");  // the side counter is reset
-    if (launch_batch_flight<R>(F, tab + (size_t)flip * n, n, early, b->steps, false, side_ticket, 1, sms, b->side))
+  if (batched) {
+    if (early) {
+      ck(cudaMemsetAsync(side_ticket, 0, sizeof(unsigned int), b->side), "memset");
+      ck(cudaEventRecord(b->ev_side0, b->side), "event");  // the side counter is reset
+      if (launch_batch_flight<R>(F, tab + (size_t)flip * n, n, early, b->steps, false, side_ticket, 1, sms, b->side,
+                                 b->smem_table))
+        throw std::runtime_error("batched flight launch failed");
+      ck(cudaEventRecord(b->ev_side, b->side), "event");
+    }
+    ck(cudaMemsetAsync(b->tickets, 0, sizeof(unsigned int) * (1 + mcb200_ctx::kGenerations), b->stream), "memset");
+    if (launch_batch_flight<R>(F, tab + (size_t)flip * n, n, batched & ~early, b->steps, false, b->tickets,
+                               b->blocks_per_sm, sms, b->stream, b->smem_table))
       throw std::runtime_error("batched flight launch failed");
-    ck(cudaEventRecord(b->ev_side, b->side), "event");
+    if (early) {  // the helper, then the side launch's end
+      ck(cudaStreamWaitEvent(b->stream, b->ev_side0, 0), "wait");
+      if (launch_batch_flight<R>(F, tab + (size_t)flip * n, n, early, b->steps, false, side_ticket, b->blocks_per_sm,
+                                 sms, b->stream, b->smem_table))
+        throw std::runtime_error("batched flight launch failed");
+      ck(cudaStreamWaitEvent(b->stream, b->ev_side, 0), "wait");
+    }
+    for (int g = 0; g < mcb200_ctx::kGenerations; ++g)
+      if (launch_batch_flight<R>(F, tab + (size_t)(2 + g) * n, n, batched, b->steps, true, b->tickets + 1 + g,
+                                 b->blocks_per_sm, sms, b->stream, b->smem_table))
+        throw std::runtime_error("batched copy flight launch failed");
+    b->launches += 2 + mcb200_ctx::kGenerations + (early ? 2 : 0);
   }
-  ck(cudaMemsetAsync(b->tickets, 0, sizeof(unsigned int) * (1 + mcb200_ctx::kGenerations), b->stream), "memset");
-  if (launch_batch_flight<R>(F, tab + (size_t)flip * n, n, all & ~early, b->steps, false, b->tickets,
-                             b->blocks_per_sm, sms, b->stream))
-    throw std::runtime_error("batched flight launch failed");
-  if (early) {  // the helper, then the side launch's end
-    ck(cudaStreamWaitEvent(b->stream, b->ev_side0, 0), "wait");
-    if (launch_batch_flight<R>(F, tab + (size_t)flip * n, n, early, b->steps, false, side_ticket, b->blocks_per_sm,
-                               sms, b->stream))
-      throw std::runtime_error("batched flight launch failed");
-    ck(cudaStreamWaitEvent(b->stream, b->ev_side, 0), "wait");
-  }
-  for (int g = 0; g < mcb200_ctx::kGenerations; ++g)
-    if (launch_batch_flight<R>(F, tab + (size_t)(2 + g) * n, n, all, b->steps, true, b->tickets + 1 + g,
-                               b->blocks_per_sm, sms, b->stream))
-      throw std::runtime_error("batched copy flight launch failed");
-  advance_steps<<<(n + 63) / 64, 64, 0, b->stream>>>(b->steps, n);
-  ck(cudaGetLastError(), "advance steps");
   ck(cudaEventRecord(b->ev_flight, b->stream), "event");
-  b->launches += 2 + mcb200_ctx::kGenerations + (early ? 2 : 0);
-  // 3. every member: its tail after the flights, on its own stream
+  // 3. every member: its tail after its flights, on its own stream
   for (int k = 0; k < n; ++k) {
     mcb200_ctx *c = b->m[k];
-    ck(cudaStreamWaitEvent(c->stream, b->ev_flight, 0), "wait");
+    if (!((solo >> k) & 1)) ck(cudaStreamWaitEvent(c->stream, b->ev_flight, 0), "wait");
     step_tail<R>(c);
+  }
+  // 4. the step numbers advance once every flight has read them; the solo
+  //    members' next flights wait for that
+  for (int k = 0; k < n; ++k)
+    if ((solo >> k) & 1) ck(cudaStreamWaitEvent(b->stream, b->ev_member[k], 0), "wait");
+  launch_advance_batch_steps<R>(b->steps, static_cast<BatchInstT<R> *>(b->tables), n, 6, b->stream);
+  ck(cudaGetLastError(), "advance steps");
+  if (solo) {
+    ck(cudaEventRecord(b->ev_steps, b->stream), "event");
+    for (int k = 0; k < n; ++k)
+      if ((solo >> k) & 1) ck(cudaStreamWaitEvent(b->m[k]->stream, b->ev_steps, 0), "wait");
   }
   b->steps_done += 1;
   for (uint32_t &st : b->member_step) ++st;
@@ -415,6 +447,7 @@ int mcb200_batch_create(mcb200_ctx *const *ctxs, const mcb200_batch_member *memb
     ck(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking), "cudaStreamCreate");
     ck(cudaEventCreateWithFlags(&b->ev_side, cudaEventDisableTiming), "cudaEventCreate");
     ck(cudaEventCreateWithFlags(&b->ev_side0, cudaEventDisableTiming), "cudaEventCreate");
+    ck(cudaEventCreateWithFlags(&b->ev_steps, cudaEventDisableTiming), "cudaEventCreate");
     ck(cudaEventCreateWithFlags(&b->ev_flight, cudaEventDisableTiming), "cudaEventCreate");
     ck(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming), "cudaEventCreate");
     ck(cudaEventCreateWithFlags(&b->ev_solved, cudaEventDisableTiming), "cudaEventCreate");
@@ -511,23 +544,25 @@ int mcb200_batch_autotune(mcb200_batch *b, int trial_steps, mcb200_batch_tuning 
   static const int flight_blocks[] = {1, 2};
   static const int grid_per_sm[] = {2, 4, 8};
   static const int sort_buckets[] = {1, 2, 4, 8};
-  mcb200_batch_tuning win{0, 0, 0, 1e300, 0, 0, 1};
+  mcb200_batch_tuning win{0, 0, 0, 1e300, 0, 0, 1, 0, 0, 0};
   int tried = 0;
-  auto apply = [&](const mcb200_batch_tuning &t) {
+  auto apply = [&](mcb200_batch_tuning &t) {
     b->blocks_per_sm = t.flight_blocks_per_sm;
     b->overlap = t.overlap != 0;
     b->pair_solves = t.pair_solves != 0;
+    b->smem_table = t.smem_table != 0;
     for (mcb200_ctx *c : b->m) {
       c->grid_per_sm = t.grid_per_sm;
       mcb200_set_sort_bucket(c, t.sort_bucket);
     }
     cudaSetDevice(b->device);
     cudaStreamSynchronize(b->stream);
+    mcb200_batch_set_solo(b, t.solo_min_particles, &t.solo_members);
     b->drop_graphs();  // the graphs hold the previous launch shapes
   };
   // ms per step of one setting: one untimed step (it captures the graphs of
   // this setting), then the timed ones
-  auto measure = [&](const mcb200_batch_tuning &t, double &ms) -> int {
+  auto measure = [&](mcb200_batch_tuning &t, double &ms) -> int {
     apply(t);
     if (int rc = mcb200_batch_run(b, 1)) return rc;
     if (int rc = mcb200_batch_mark(b, 6)) return rc;
@@ -540,7 +575,7 @@ int mcb200_batch_autotune(mcb200_batch *b, int trial_steps, mcb200_batch_tuning 
   // The simulations change while they are timed (particle counts drift), so
   // the candidates of a stage are timed in order and again in reverse order
   // and each keeps the mean of its two times: a linear drift cancels.
-  auto stage = [&](const std::vector<mcb200_batch_tuning> &cands) -> int {
+  auto stage = [&](std::vector<mcb200_batch_tuning> &cands) -> int {
     std::vector<double> sum(cands.size(), 0.0);
     for (int pass = 0; pass < 2; ++pass)
       for (size_t i = 0; i < cands.size(); ++i) {
@@ -559,16 +594,19 @@ int mcb200_batch_autotune(mcb200_batch *b, int trial_steps, mcb200_batch_tuning 
     return MCB200_OK;
   };
   const int overlap0 = b->overlap ? 1 : 0, pair0 = b->pair_solves ? 1 : 0;
-  const int bucket0 = b->m.empty() ? 1 : mcb200_get_sort_bucket(b->m[0]);
+  const int bucket0 = b->m.empty() ? 1 : mcb200_get_sort_bucket(b->m[0]), table0 = b->smem_table ? 1 : 0;
+  const uint64_t solo0 = b->solo_min;
   std::vector<mcb200_batch_tuning> shapes;
   for (int fb : flight_blocks)
-    for (int gs : grid_per_sm) shapes.push_back(mcb200_batch_tuning{fb, gs, overlap0, 0.0, 0, pair0, bucket0});
+    for (int gs : grid_per_sm)
+      shapes.push_back(mcb200_batch_tuning{fb, gs, overlap0, 0.0, 0, pair0, bucket0, table0, solo0, 0});
   if (int rc = stage(shapes)) return rc;
-  std::vector<mcb200_batch_tuning> modes;  // overlap and pairing, with the fastest launch shapes
-  for (int v = 0; v < 4; ++v) {
+  std::vector<mcb200_batch_tuning> modes;  // overlap, pairing and the table's place, with the fastest shapes
+  for (int v = 0; v < 8; ++v) {
     mcb200_batch_tuning t = win;
     t.overlap = v & 1 ? 1 - overlap0 : overlap0;
     t.pair_solves = v & 2 ? 1 - pair0 : pair0;
+    t.smem_table = v & 4 ? 1 - table0 : table0;
     modes.push_back(t);
   }
   if (int rc = stage(modes)) return rc;
@@ -581,7 +619,23 @@ int mcb200_batch_autotune(mcb200_batch *b, int trial_steps, mcb200_batch_tuning 
       widths.push_back(t);
     }
   if (int rc = stage(widths)) return rc;
-  tried -= 2;  // each stage's first candidate is the previous stage's winner
+  // members flying solo: none, all, or those above a quartile of the counts
+  std::vector<uint64_t> counts;
+  for (mcb200_ctx *c : b->m) counts.push_back(mcb200_num_particles(c));
+  std::sort(counts.begin(), counts.end());
+  std::vector<uint64_t> thresholds{0, 1};
+  for (int q = 1; q <= 3; ++q) thresholds.push_back(std::max<uint64_t>(counts[counts.size() * q / 4], 1));
+  std::sort(thresholds.begin(), thresholds.end());
+  thresholds.erase(std::unique(thresholds.begin(), thresholds.end()), thresholds.end());
+  std::vector<mcb200_batch_tuning> solos{win};
+  for (uint64_t t : thresholds)
+    if (t != win.solo_min_particles) {
+      mcb200_batch_tuning c = win;
+      c.solo_min_particles = t;
+      solos.push_back(c);
+    }
+  if (int rc = stage(solos)) return rc;
+  tried -= 3;  // each stage's first candidate is the previous stage's winner
   win.candidates = tried;
   apply(win);
   if (best) *best = win;
@@ -627,6 +681,43 @@ int mcb200_batch_set_overlap(mcb200_batch *b, int enable) {
   cudaSetDevice(b->device);
   cudaStreamSynchronize(b->stream);
   b->overlap = enable != 0;
+  b->drop_graphs();
+  return MCB200_OK;
+}
+
+int mcb200_batch_set_solo(mcb200_batch *b, uint64_t min_particles, int *members) {
+  if (!b) return MCB200_ERR_ARG;
+  try {
+    ck(cudaSetDevice(b->device), "cudaSetDevice");
+    ck(cudaStreamSynchronize(b->stream), "sync");
+    uint64_t mask = 0;
+    int count = 0;
+    for (size_t k = 0; k < b->m.size(); ++k) {
+      mcb200_ctx *c = b->m[k];
+      ck(cudaStreamSynchronize(c->stream), "sync");
+      pull_counts(c);
+      if (min_particles > 0 && c->n >= min_particles) {
+        mask |= 1ull << k;
+        ++count;
+      }
+    }
+    if (mask != b->solo) b->drop_graphs();
+    b->solo = mask;
+    b->solo_min = (size_t)min_particles;
+    if (members) *members = count;
+    return MCB200_OK;
+  } catch (const CapacityError &e) {
+    return bfail(b, MCB200_ERR_CAPACITY, e.what());
+  } catch (const std::exception &e) {
+    return bfail(b, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_batch_set_smem_table(mcb200_batch *b, int enable) {
+  if (!b) return MCB200_ERR_ARG;
+  cudaSetDevice(b->device);
+  cudaStreamSynchronize(b->stream);
+  b->smem_table = enable != 0;
   b->drop_graphs();
   return MCB200_OK;
 }

@@ -98,6 +98,17 @@ void alloc_stores(mcb200_ctx *c) {
   }
 }
 
+// The charge bounds of the current store (its device count) into c->bounds,
+// on the context's stream.  Every path that writes the store calls it after
+// writing, except the step, whose sort computes them.
+void store_bounds(mcb200_ctx *c) {
+  const DevCount n{c->dev_counts, nullptr, (int)c->capacity};
+  const int grid = grid_for(c, c->capacity, 256);
+  if (c->precision == MCB200_FLIGHT_FP32) launch_charge_bounds(store<float>(c, c->cur), n, c->bounds, grid, c->stream);
+  else launch_charge_bounds(store<double>(c, c->cur), n, c->bounds, grid, c->stream);
+  ck(cudaGetLastError(), "charge bounds");
+}
+
 // Uniform k-space locator for the tetrahedron search (see flight_physics.cuh).
 void build_kgrid(mcb200_ctx *c, int g) {
   const FullBandTables &t = c->ts->tab;
@@ -501,6 +512,8 @@ void init_device_context(mcb200_ctx *c, size_t max_particles) {
   c->child_cap = (int)std::min<size_t>(std::max<size_t>(max_particles / 8, 4096), 1u << 22);
   alloc_stores(c);
   c->append_count = dalloc<unsigned int>(1, c->owned);
+  c->bounds = dalloc<unsigned long long>(4, c->owned);
+  ck(cudaMemsetAsync(c->bounds, 0, 4 * sizeof(unsigned long long), c->stream), "memset");
   c->tickets = dalloc<unsigned int>(1 + mcb200_ctx::kGenerations, c->owned);
   c->y.counters = dalloc<unsigned long long>(kCntNumCounters, c->owned);
   c->y.contact = dalloc<long long>(kMaxContacts * 6, c->owned);
@@ -586,6 +599,7 @@ int mcb200_set_flight_precision(mcb200_ctx *c, int precision) {
     c->precision = precision;
     c->cur = 0;
     alloc_stores(c);
+    ck(cudaMemsetAsync(c->bounds, 0, 4 * sizeof(unsigned long long), c->stream), "memset");  // an empty store
     return MCB200_OK;
   } catch (const std::exception &e) {
     return fail(c, MCB200_ERR_CUDA, e.what());
@@ -857,6 +871,7 @@ int mcb200_upload_particles(mcb200_ctx *c, size_t n, const mcb200_particles *p) 
     c->overflow_pending = false;
     ck(cudaMemsetAsync(c->dev_counts + 2, 0, sizeof(unsigned int), c->stream), "memset");
     push_counts(c);
+    store_bounds(c);
     ck(cudaStreamSynchronize(c->stream), "sync");
     return MCB200_OK;
   } catch (const std::exception &e) {
@@ -947,6 +962,7 @@ int mcb200_copy_ensemble(mcb200_ctx *dst, mcb200_ctx *src) {
     dst->overflow_pending = false;
     ck(cudaMemsetAsync(dst->dev_counts + 2, 0, sizeof(unsigned int), dst->stream), "memset");
     push_counts(dst);
+    store_bounds(dst);
     ck(cudaStreamSynchronize(dst->stream), "sync");
     return MCB200_OK;
   } catch (const CapacityError &e) {
@@ -1013,6 +1029,7 @@ int mcb200_seed_particles(mcb200_ctx *c, size_t n, const int32_t *cell_of, const
     c->n += n;
     c->next_uid += (uint32_t)n;
     push_counts(c);
+    store_bounds(c);
     ck(cudaStreamSynchronize(c->stream), "sync");
     for (void *p : tmp) cudaFree(p);
     return MCB200_OK;
@@ -1265,8 +1282,10 @@ int mcb200_set_device(mcb200_ctx *c, const int32_t *material, const double *dono
     f.cg_q = dalloc<double>(nodes, c->mesh_owned);
     f.cg_part = dalloc<double>(3 * kCgMaxGrid, c->mesh_owned);  // the persistent CG's partial sums
     f.cg_scalars = dalloc<double>(16, c->mesh_owned);  // the CG scalars sc[0..9]
-    f.abs_sum = dalloc<unsigned long long>(4, c->mesh_owned);
-    f.dep_scales = dalloc<DepositScales>(1, c->mesh_owned);
+    f.abs_sum = c->bounds;
+    // the cell and node pass clears the sums it reads: they start from zero
+    ck(cudaMemset(f.acc_cell, 0, 3 * cells * sizeof(long long)), "memset");
+    ck(cudaMemset(f.acc_node, 0, nodes * sizeof(long long)), "memset");
     f.poisson_stats = dalloc<double>(3, c->mesh_owned);
     ck(cudaMemset(f.poisson_stats, 0, 3 * sizeof(double)), "memset");
     ck(cudaMemset(f.potential, 0, nodes * sizeof(double)), "memset");
@@ -1393,7 +1412,7 @@ int mcb200_set_induced_current(mcb200_ctx *c, int contact) {
     double emax = 0;
     for (double v : h) emax = std::max(emax, std::fabs(v));
     if (!c->ib.sum) {
-      c->ib.bounds = dalloc<unsigned long long>(4, c->mesh_owned);
+      c->ib.bounds = c->bounds;
       c->ib.acc = dalloc<long long>(1, c->mesh_owned);
       c->ib.sum = dalloc<double>(2, c->mesh_owned);
       ck(cudaMemsetAsync(c->ib.acc, 0, sizeof(long long), s), "memset");
@@ -1525,7 +1544,7 @@ int mcb200_multiple_refresh(mcb200_ctx *c, const int32_t *desired_e, const int32
     auto refresh = [&](auto tag) {
       using R = decltype(tag);
       launch_cell_sort(store<R>(c, c->cur), DevCount{c->dev_counts, nullptr, (int)c->capacity}, store<R>(c, sorted),
-                       cells, c->mesh.nx, c->mesh.nz, c->hist, c->offsets, c->tile_sums, c->total, 0,
+                       cells, c->mesh.nx, c->mesh.nz, c->hist, c->offsets, c->tile_sums, c->total, 0, nullptr,
                        grid_for(c, c->capacity, 256), s);
       const DevParticlesT<R> &P = store<R>(c, sorted);
       launch_refresh_count(P, c->offsets, c->hist, cells, de, dh, r, w.order, out_count, new_count, s);
@@ -1540,10 +1559,11 @@ int mcb200_multiple_refresh(mcb200_ctx *c, const int32_t *desired_e, const int32
     ck(cudaEventRecord(c->ev_mr_used, s), "event");  // the targets are read
     // the refreshed population's size and the uid counter, on the device
     refresh_counts_kernel<<<1, 32, 0, s>>>(c->dev_counts, tot);
-    c->launches += 14;  // cell sort, count, two scans, emit, counts
     ck(cudaGetLastError(), "refresh");
     c->cur = other;
     c->n_stale = true;
+    store_bounds(c);
+    c->launches += 15;  // cell sort, count, two scans, emit, counts, charge bounds
     if (generated) {  // the only result that needs the host to wait
       ck(cudaMemcpyAsync(c->h_scratch + 13, gen, sizeof(long long), cudaMemcpyDeviceToHost, s), "copy");
       ck(cudaStreamSynchronize(s), "sync");
@@ -1898,14 +1918,15 @@ void poisson_finish(mcb200_ctx *c, cudaStream_t s, int *iterations, double *rel_
   c->fields_set = true;
 }
 
-// Deposition of the current store (charge bounds, fixed-point units, cell
-// and node sums) on stream s; nothing waits for the GPU.
+// Deposition of the current store (fixed-point units from its charge
+// bounds, the particle pass, then cell and node sums) on stream s; nothing
+// waits for the GPU.
 void deposit_enqueue(mcb200_ctx *c, cudaStream_t s) {
   const int grid = grid_for(c, c->capacity, 256);
   const DevCount n{c->dev_counts, nullptr, (int)c->capacity};
   if (c->precision == MCB200_FLIGHT_FP32) launch_deposit(store<float>(c, c->cur), n, c->mesh, c->fb, grid, s);
   else launch_deposit(store<double>(c, c->cur), n, c->mesh, c->fb, grid, s);
-  c->launches += 5;  // charge bounds, units, particle deposit, cell and node passes
+  c->launches += 2;  // particle deposit, cell and node pass (units from the store's charge bounds)
   ck(cudaGetLastError(), "deposit");
   c->fields_set = true;
 }
@@ -1930,18 +1951,17 @@ void step_prepare(mcb200_ctx *c) {
   if (c->induced_contact >= 0) {  // the induced current of the store the step starts from
     launch_induced_current(store<R>(c, c->cur), DevCount{c->dev_counts, nullptr, (int)c->capacity}, c->mesh,
                            c->ts->dt, c->ib, grid_for(c, c->capacity, 256), s);
-    c->launches += 3;
+    c->launches += 2;
   }
   join_stat(c);  // the flights change the store the statistics read
   StepCounters z{c->tickets, {}, c->append_count};
   for (int g = 0; g < mcb200_ctx::kGenerations; ++g) z.count[g] = children<R>(c, g).count;
   z.count[mcb200_ctx::kGenerations] = c->sink_count;
-  launch_step_reset(z, s);
+  if constexpr (sizeof(R) == 4)  // FP32 flight reads the fields as per-cell float records
+    launch_records_and_reset(c->ts->dt, c->mesh, c->cell32, c->ncells, z, s);
+  else
+    launch_step_reset(z, s);
   c->launches += 1;
-  if constexpr (sizeof(R) == 4) {  // FP32 flight reads the fields as per-cell float records
-    launch_cell_records32(c->ts->dt, c->mesh, c->cell32, c->ncells, s);
-    c->launches += 1;
-  }
 }
 
 // After the flights of a step: uids for the surviving copies, which join the
@@ -1960,13 +1980,42 @@ void step_tail(mcb200_ctx *c) {
   c->launches += 1;
   const int other = 1 - c->cur;
   launch_cell_sort(store<R>(c, c->cur), DevCount{c->dev_counts, c->append_count, cap}, store<R>(c, other), c->ncells,
-                   c->mesh.nx, c->mesh.nz, c->hist, c->offsets, c->tile_sums, c->total, c->sort_shift,
+                   c->mesh.nx, c->mesh.nz, c->hist, c->offsets, c->tile_sums, c->total, c->sort_shift, c->bounds,
                    grid_for(c, c->capacity, 256), s);
   launch_step_finish(c->dev_counts, c->total, c->dev_counts + 1, c->append_count, c->dev_psteps, s);
   ck(cudaGetLastError(), "cell sort");
   c->launches += 6;
   c->cur = other;
   c->n_stale = true;
+}
+
+// The flights of a step on the context's stream, after step_prepare:
+// 1. the main flight (copies go to generation 0); 2. the copies fly the
+// rest of the step, generation by generation (a generation with no copies
+// returns at once); copies of the last generation are counted in a sink,
+// not flown.  ev (or null): timing events 1 and 2 around the main flight.
+template <typename R>
+void enqueue_flights(mcb200_ctx *c, FlightCtxT<R> F, cudaEvent_t *ev) {
+  cudaStream_t s = c->stream;
+  F.C = children<R>(c, 0);
+  if (ev) ck(cudaEventRecord(ev[1], s), "event");
+  launch_flight(F, store<R>(c, c->cur), DevCount{c->dev_counts, nullptr, (int)c->capacity}, c->tickets, c->sm_count,
+                s);
+  ck(cudaGetLastError(), "flight kernel");
+  if (ev) ck(cudaEventRecord(ev[2], s), "event");
+  c->launches += 1;
+  for (int g = 0; g < mcb200_ctx::kGenerations; ++g) {
+    if (g + 1 < mcb200_ctx::kGenerations) {
+      F.C = children<R>(c, g + 1);
+    } else {
+      F.C = children<R>(c, g);
+      F.C.count = c->sink_count;
+      F.C.capacity = 0;
+    }
+    launch_child_flight(F, children<R>(c, g), c->child_cap, c->tickets + 1 + g, c->sm_count, s);
+    ck(cudaGetLastError(), "child flight kernel");
+    c->launches += 1;
+  }
 }
 
 template <typename R>
@@ -1991,29 +2040,7 @@ void step_impl(mcb200_ctx *c, uint32_t step, uint64_t seed, double dt) {
     ck(cudaEventRecord(ev[0], s), "event");
   }
   step_prepare<R>(c);
-  // 1. main flight; copies go to generation 0
-  F.C = children<R>(c, 0);
-  if (ev) ck(cudaEventRecord(ev[1], s), "event");
-  launch_flight(F, store<R>(c, c->cur), DevCount{c->dev_counts, nullptr, (int)c->capacity}, c->tickets, c->sm_count,
-                s);
-  ck(cudaGetLastError(), "flight kernel");
-  if (ev) ck(cudaEventRecord(ev[2], s), "event");
-  c->launches += 1;
-  // 2. copies fly the rest of the step, generation by generation (a
-  //    generation with no copies returns at once); copies of the last
-  //    generation are counted in a sink, not flown
-  for (int g = 0; g < mcb200_ctx::kGenerations; ++g) {
-    if (g + 1 < mcb200_ctx::kGenerations) {
-      F.C = children<R>(c, g + 1);
-    } else {
-      F.C = children<R>(c, g);
-      F.C.count = c->sink_count;
-      F.C.capacity = 0;
-    }
-    launch_child_flight(F, children<R>(c, g), c->child_cap, c->tickets + 1 + g, c->sm_count, s);
-    ck(cudaGetLastError(), "child flight kernel");
-    c->launches += 1;
-  }
+  enqueue_flights<R>(c, F, ev);
   // 3.-4. append the copies, sort by cell
   step_tail<R>(c);
   if (ev) ck(cudaEventRecord(ev[3], s), "event");
@@ -2027,5 +2054,7 @@ template void step_prepare<float>(mcb200_ctx *);
 template void step_prepare<double>(mcb200_ctx *);
 template void step_tail<float>(mcb200_ctx *);
 template void step_tail<double>(mcb200_ctx *);
+template void enqueue_flights<float>(mcb200_ctx *, FlightCtxT<float>, cudaEvent_t *);
+template void enqueue_flights<double>(mcb200_ctx *, FlightCtxT<double>, cudaEvent_t *);
 
 }  // namespace mcb200::eng

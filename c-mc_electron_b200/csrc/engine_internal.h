@@ -189,6 +189,10 @@ struct mcb200_ctx {
   ChildBuffers cb[kGenerations];
   int child_cap = 0;
   unsigned int *append_count = nullptr;
+  // [4] charge bounds of the current store (charge_bounds_kernel's layout):
+  // the step's sort computes them, every other writer of the store after it
+  // writes (store_bounds); the deposition's fixed-point units come from them
+  unsigned long long *bounds = nullptr;
   unsigned int *tickets = nullptr;  // work counters of the persistent flight launches (main + generations)
   float4 *cell32 = nullptr;         // FP32 flight's per-cell records (mesh-sized)
   // tallies
@@ -316,5 +320,9 @@ template <typename R>
 void step_prepare(mcb200_ctx *c);
 template <typename R>
 void step_tail(mcb200_ctx *c);
+// The main and copy flights of a step on the context's stream (after
+// step_prepare, before step_tail); ev: optional timing events.
+template <typename R>
+void enqueue_flights(mcb200_ctx *c, FlightCtxT<R> F, cudaEvent_t *ev);
 
 }  // namespace mcb200::eng

@@ -32,9 +32,12 @@ struct BatchInstT;
 template <typename R>
 int launch_batch_flight(const FlightCtxT<R> &F, const BatchInstT<R> *inst, int ninst, uint64_t members,
                         const uint32_t *steps, bool child, unsigned int *ticket, int blocks_per_sm, int sm_count,
-                        cudaStream_t s);
-// FP32 flight's per-cell records (DevMesh::cell32), [cells][3] float4.
-void launch_cell_records32(const DevTables &T, const DevMesh &M, float4 *out, int cells, cudaStream_t s);
+                        cudaStream_t s, bool smem_table);
+// steps[k] += 1 and the step field of simulation k in `ntab` consecutive
+// tables of n simulations (the tables the batched flights read in place).
+template <typename R>
+void launch_advance_batch_steps(uint32_t *steps, BatchInstT<R> *tab, int n, int ntab, cudaStream_t s);
+
 // The step's surviving copies (all generations) ranked by (parent uid, sub),
 // given uids from *next_uid on, and appended to `dst` after its *n
 // particles, in one launch; *appended (zeroed by the step reset) counts them,
@@ -51,6 +54,10 @@ struct StepCounters {
   unsigned int *appended;  // copies appended to the store this step
 };
 void launch_step_reset(const StepCounters &z, cudaStream_t s);
+// FP32 flight's per-cell records (DevMesh::cell32), [cells][3] float4, and
+// the step reset of z, in one launch.
+void launch_records_and_reset(const DevTables &T, const DevMesh &M, float4 *out, int cells, const StepCounters &z,
+                              cudaStream_t s);
 // *particle_steps += *n; *n = *sorted_total; *next_uid += *appended.
 void launch_step_finish(unsigned int *n, const unsigned int *sorted_total, unsigned int *next_uid,
                         const unsigned int *appended, unsigned long long *particle_steps, cudaStream_t s);
@@ -62,10 +69,11 @@ void launch_exclusive_scan(const unsigned int *in, unsigned int *out, unsigned i
 // Counting sort of the live particles among the first n (device count) of
 // `src` by cell into `dst`; *total = live particles, offsets = cell starts
 // (after the scatter: cell ends).  With shift > 0 the keys are buckets of
-// 2^shift consecutive cells (hist and offsets per bucket).
+// 2^shift consecutive cells (hist and offsets per bucket).  bounds (or
+// null): the sorted store's charge bounds, as launch_charge_bounds writes.
 template <typename R>
 void launch_cell_sort(const DevParticlesT<R> &src, DevCount n, const DevParticlesT<R> &dst, int ncells, int nx,
                       int nz, unsigned int *hist, unsigned int *offsets, unsigned int *tile_sums, unsigned int *total,
-                      int shift, int grid, cudaStream_t s);
+                      int shift, unsigned long long *bounds, int grid, cudaStream_t s);
 
 }  // namespace mcb200

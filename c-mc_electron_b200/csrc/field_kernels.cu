@@ -3,8 +3,9 @@
 //  * deposit: MeshQuantities::compute_cell_charge (src/mcmodel.cpp:2664-2712)
 //    and particle_to_density (:348-417) in one pass over the particle store,
 //    summed in int64 fixed point so the result does not depend on thread
-//    order.  The fixed-point unit is chosen per call from the store's total
-//    |charge| (every cell or node sum is bounded by it), 2^61 / sum.
+//    order.  The fixed-point unit comes from the store's charge bounds,
+//    count x max |q| per carrier type (every cell or node sum is bounded by
+//    it): 2^61 / bound, rounded to a power of two.
 //  * Poisson: the reference factorises its FV matrix with KLU and solves it
 //    every step (linear_poisson_solver, :2714-2730).  Here the Dirichlet
 //    contact rows are eliminated, which leaves a symmetric positive-definite
@@ -74,20 +75,23 @@ __global__ void __launch_bounds__(256) charge_bounds_kernel(const double *charge
 
 // Fixed-point units from the bounds of charge_bounds_kernel: a sum whose
 // magnitude is below 2^e gets the unit 2^(61 - e) (61 bits of range);
-// empty sums get 1.
+// empty sums get 1.  s[0]: electron cell sums, [1]: hole cell sums, [2]:
+// |q| and node sums.  Every thread that needs them derives them from the
+// four bound words (the store's, current before the deposition starts).
 __device__ double fixed_unit(double bound) {
   if (!(bound > 0.0)) return 1.0;
   int e = 0;
   frexp(bound, &e);  // bound < 2^e
   return ldexp(1.0, 61 - e);
 }
-__global__ void deposit_scales_kernel(const unsigned long long *b, DepositScales *out) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ DepositScales deposit_scales(const unsigned long long *b) {
   const double qe = __longlong_as_double((long long)b[0]), qh = __longlong_as_double((long long)b[1]);
   const double be = (double)b[2] * qe, bh = (double)b[3] * qh;
-  out->s[0] = fixed_unit(be);
-  out->s[1] = fixed_unit(bh);
-  out->s[2] = fixed_unit(be + bh);
+  DepositScales out;
+  out.s[0] = fixed_unit(be);
+  out.s[1] = fixed_unit(bh);
+  out.s[2] = fixed_unit(be + bh);
+  return out;
 }
 
 __device__ __forceinline__ long long fx(double v, double scale) { return __double2ll_rn(v * scale); }
@@ -100,10 +104,10 @@ __device__ __forceinline__ void fx_put(long long *p, long long v) {
 // cell and carrier type add their fixed-point terms before one atomic each.
 template <typename R>
 __global__ void __launch_bounds__(256) deposit_kernel(DevParticlesT<R> P, DevCount count, DevMesh M,
-                                                      const DepositScales *Sp, long long *cell_e, long long *cell_h,
-                                                      long long *cell_abs, long long *node_q) {
+                                                      const unsigned long long *bounds, long long *cell_e,
+                                                      long long *cell_h, long long *cell_abs, long long *node_q) {
   const int n = count.get();
-  const DepositScales S = *Sp;
+  const DepositScales S = deposit_scales(bounds);
   const int px = M.nx + 1, pz = M.nz + 1;
   const double scale = S.s[2];
   const unsigned lane = threadIdx.x & 31u;
@@ -160,27 +164,32 @@ __global__ void __launch_bounds__(256) deposit_kernel(DevParticlesT<R> P, DevCou
   }
 }
 
-// compute_cell_charge's final loop (:2705-2710) and the per-cell sums.
-__global__ void deposit_cells_kernel(int cells, const DepositScales *Sp, const long long *cell_e,
-                                     const long long *cell_h, const long long *cell_abs, const double *cvol,
-                                     const double *da, double *e_out, double *h_out, double *rho_out) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= cells) return;
-  const DepositScales S = *Sp;
-  e_out[c] = (double)cell_e[c] / S.s[0];
-  h_out[c] = (double)cell_h[c] / S.s[1];
-  const double r = (double)cell_abs[c] / S.s[2] / cvol[c];
-  const double half = 0.5 * da[c];
-  rho_out[c] = r > half ? r : half;
-}
-
-// particle_to_density's volume division (:408-416).
-__global__ void deposit_nodes_kernel(int nodes, const DepositScales *Sp, const long long *node_q, const double *pvol,
-                                     double *density) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= nodes) return;
-  const double q = (double)node_q[p] / Sp->s[2];
-  density[p] = fabs(pvol[p]) > 0 ? q / pvol[p] : q;
+// compute_cell_charge's final loop (:2705-2710) with the per-cell sums, and
+// particle_to_density's volume division (:408-416), in one pass: thread t
+// takes cell t and node t.  It clears the fixed-point sums it reads, so the
+// next deposition starts from zero without a memset.
+__global__ void deposit_sums_kernel(int cells, int nodes, const unsigned long long *bounds, long long *cell_e,
+                                    long long *cell_h, long long *cell_abs, const double *cvol, const double *da,
+                                    double *e_out, double *h_out, double *rho_out, long long *node_q,
+                                    const double *pvol, double *density) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= cells && t >= nodes) return;
+  const DepositScales S = deposit_scales(bounds);
+  if (t < cells) {
+    e_out[t] = (double)cell_e[t] / S.s[0];
+    h_out[t] = (double)cell_h[t] / S.s[1];
+    const double r = (double)cell_abs[t] / S.s[2] / cvol[t];
+    const double half = 0.5 * da[t];
+    rho_out[t] = r > half ? r : half;
+    cell_e[t] = 0;
+    cell_h[t] = 0;
+    cell_abs[t] = 0;
+  }
+  if (t < nodes) {
+    const double q = (double)node_q[t] / S.s[2];
+    density[t] = fabs(pvol[t]) > 0 ? q / pvol[t] : q;
+    node_q[t] = 0;
+  }
 }
 
 // compute_rhs, src/mcmodel.cpp:2858-2893.
@@ -427,16 +436,11 @@ template <typename R>
 void launch_deposit(const DevParticlesT<R> &P, DevCount n, const DevMesh &M, const FieldBuffers &f, int grid,
                     cudaStream_t s) {
   const int cells = M.nx * M.ny * M.nz, nodes = (M.nx + 1) * (M.ny + 1) * (M.nz + 1);
-  launch_charge_bounds(P, n, f.abs_sum, grid, s);
-  deposit_scales_kernel<<<1, 32, 0, s>>>(f.abs_sum, f.dep_scales);
-  cudaMemsetAsync(f.acc_cell, 0, sizeof(long long) * 3 * (size_t)cells, s);
-  cudaMemsetAsync(f.acc_node, 0, sizeof(long long) * (size_t)nodes, s);
-  deposit_kernel<R><<<grid, 256, 0, s>>>(P, n, M, f.dep_scales, f.acc_cell, f.acc_cell + cells,
+  deposit_kernel<R><<<grid, 256, 0, s>>>(P, n, M, f.abs_sum, f.acc_cell, f.acc_cell + cells,
                                          f.acc_cell + 2 * (size_t)cells, f.acc_node);
-  deposit_cells_kernel<<<blocks(cells, 256), 256, 0, s>>>(cells, f.dep_scales, f.acc_cell, f.acc_cell + cells,
-                                                           f.acc_cell + 2 * (size_t)cells, f.cvol, M.da, f.cell_e,
-                                                           f.cell_h, const_cast<double *>(M.rho));
-  deposit_nodes_kernel<<<blocks(nodes, 256), 256, 0, s>>>(nodes, f.dep_scales, f.acc_node, f.pvol, f.density);
+  deposit_sums_kernel<<<blocks(std::max(cells, nodes), 256), 256, 0, s>>>(
+      cells, nodes, f.abs_sum, f.acc_cell, f.acc_cell + cells, f.acc_cell + 2 * (size_t)cells, f.cvol, M.da,
+      f.cell_e, f.cell_h, const_cast<double *>(M.rho), f.acc_node, f.pvol, f.density);
 }
 
 template void launch_charge_bounds<double>(const DevParticlesT<double> &, DevCount, unsigned long long *, int,

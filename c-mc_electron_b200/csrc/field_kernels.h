@@ -30,8 +30,7 @@ struct FieldBuffers {
   double *rhs = nullptr, *potential = nullptr;
   double *cg_r = nullptr, *cg_z = nullptr, *cg_p = nullptr, *cg_p1 = nullptr, *cg_q = nullptr, *cg_part = nullptr,
          *cg_scalars = nullptr;
-  unsigned long long *abs_sum = nullptr;   // charge bounds of the last deposit (charge_bounds_kernel)
-  DepositScales *dep_scales = nullptr;        // fixed-point units of the last deposit (device)
+  unsigned long long *abs_sum = nullptr;  // [4] charge bounds of the store (the context's, kept by its writers)
   const MgDevice *mg = nullptr;  // multigrid hierarchy of the stencil (null: Jacobi preconditioning only)
   double *poisson_stats = nullptr;  // [3] solves, iterations, largest relative residual (since the last reset)
 };
@@ -39,8 +38,10 @@ struct FieldBuffers {
 // out[4] = {max |q| bits of electrons, of holes, electron count, hole count}
 template <typename R>
 void launch_charge_bounds(const DevParticlesT<R> &P, DevCount n, unsigned long long *out, int grid, cudaStream_t s);
-// Charge bounds, fixed-point units (f.dep_scales) and the deposition sums,
-// all on the device: nothing waits for the host.
+// The deposition sums, with fixed-point units from the store's charge
+// bounds (f.abs_sum, current when the deposition starts), all on the
+// device: nothing waits for the host.  f.acc_cell and f.acc_node must hold
+// zeros on entry and do again on exit.
 template <typename R>
 void launch_deposit(const DevParticlesT<R> &P, DevCount n, const DevMesh &M, const FieldBuffers &f, int grid,
                     cudaStream_t s);

@@ -54,9 +54,11 @@ template <typename R>
 struct StoreIO {
   DevParticlesT<R> P;
   double dt;
+  uint32_t step;  // the particles' step number (their random streams)
   __device__ bool load(int p, FlyerT<R> &f) const {
     const uint32_t meta = P.meta[p];
     if (meta & kMetaDead) return false;
+    f.step_ = step;
     f.x = P.x[p]; f.y = P.y[p]; f.z = P.z[p];
     f.kx = P.kx[p]; f.ky = P.ky[p]; f.kz = P.kz[p];
     f.energy = P.energy[p];
@@ -86,7 +88,9 @@ struct StoreIO {
 template <typename R>
 struct ChildIO {
   DevChildrenT<R> C;
+  uint32_t step;
   __device__ bool load(int p, FlyerT<R> &f) const {
+    f.step_ = step;
     f.x = C.x[p]; f.y = C.y[p]; f.z = C.z[p];
     f.kx = C.kx[p]; f.ky = C.ky[p]; f.kz = C.kz[p];
     f.energy = C.energy[p];
@@ -192,7 +196,8 @@ __global__ void __launch_bounds__(kFlightThreads, kFlightBlocks<R>) flight_kerne
   if (count == 0) return;
   __shared__ SymSmemT<R> S;
   load_sym(S, F.T);
-  fly_interleaved<R, true>(F, S, StoreIO<R>{P, F.dt}, count, ticket);
+  const uint32_t step = F.step_dev ? *F.step_dev : F.step;
+  fly_interleaved<R, true>(F, S, StoreIO<R>{P, F.dt, step}, count, ticket);
 }
 
 // Copies made during the previous pass (buffer `in`) fly the rest of their
@@ -204,7 +209,8 @@ __global__ void __launch_bounds__(kFlightThreads, kFlightBlocks<R>) child_flight
   if (count == 0) return;
   __shared__ SymSmemT<R> S;
   load_sym(S, F.T);
-  fly_interleaved<R, true>(F, S, ChildIO<R>{in}, count, ticket);
+  const uint32_t step = F.step_dev ? *F.step_dev : F.step;
+  fly_interleaved<R, true>(F, S, ChildIO<R>{in, step}, count, ticket);
 }
 
 // ---- batched flight ------------------------------------------------------
@@ -235,48 +241,61 @@ struct BatchIO {
     const BatchInstT<R> &b = I[k];
     f.I = &b;
     const int p = q - prefix[k];
-    if constexpr (kChild) return ChildIO<R>{b.in}.load(p, f);
-    else return StoreIO<R>{b.P, b.dt}.load(p, f);
+    if constexpr (kChild) return ChildIO<R>{b.in, b.step}.load(p, f);
+    else return StoreIO<R>{b.P, b.dt, b.step}.load(p, f);
   }
   __device__ void store(int q, const FlyerT<R> &f, int r) const {
     const BatchInstT<R> *b = static_cast<const BatchInstT<R> *>(f.I);
     const int p = q - prefix[b - I];
-    if constexpr (kChild) ChildIO<R>{b->in}.store(p, f, r);
-    else StoreIO<R>{b->P, b->dt}.store(p, f, r);
+    if constexpr (kChild) ChildIO<R>{b->in, b->step}.store(p, f, r);
+    else StoreIO<R>{b->P, b->dt, b->step}.store(p, f, r);
   }
 };
 
-// Dynamic shared memory of a batched launch over `ninst` simulations.
+// Dynamic shared memory of a batched launch over `ninst` simulations: the
+// table of simulations (when it is copied there) and the prefix of their
+// particle counts.
 template <typename R>
-constexpr size_t batch_smem_bytes(int ninst) {
-  return (size_t)ninst * sizeof(BatchInstT<R>) + (size_t)(ninst + 1) * sizeof(int);
+constexpr size_t batch_smem_bytes(int ninst, bool table) {
+  return (table ? (size_t)ninst * sizeof(BatchInstT<R>) : 0) + (size_t)(ninst + 1) * sizeof(int);
 }
 
 // F holds the band tables (its per-simulation part is unused); steps[k] is
 // simulation k's step number (device memory, advanced between steps).
 // Simulations whose bit in `members` is clear contribute no particles.
-template <typename R, bool kChild>
+// kSmemTable: every block copies the table into shared memory (about 0.8 KB
+// per simulation, taken from the SM's L1 share) and takes the step numbers
+// from `steps`; otherwise lanes read the table where it lies (global memory,
+// through L1), whose step fields advance_batch_steps keeps current.
+template <typename R, bool kChild, bool kSmemTable>
 __global__ void __launch_bounds__(kFlightThreads, kFlightBlocks<R>) batch_flight_kernel(const __grid_constant__ FlightCtxT<R> F,
                                                                              const BatchInstT<R> *inst,
                                                                              int ninst, uint64_t members,
                                                                              const uint32_t *steps,
                                                                              unsigned int *ticket) {
   extern __shared__ __align__(16) unsigned char batch_smem[];
-  BatchInstT<R> *I = reinterpret_cast<BatchInstT<R> *>(batch_smem);
-  int *prefix = reinterpret_cast<int *>(I + ninst);
   __shared__ SymSmemT<R> S;
-  {
+  const BatchInstT<R> *I;
+  int *prefix;
+  if constexpr (kSmemTable) {
+    BatchInstT<R> *T = reinterpret_cast<BatchInstT<R> *>(batch_smem);
+    prefix = reinterpret_cast<int *>(T + ninst);
     static_assert(sizeof(BatchInstT<R>) % 8 == 0, "the table is copied in 8-byte words");
     const unsigned long long *src = reinterpret_cast<const unsigned long long *>(inst);
-    unsigned long long *dst = reinterpret_cast<unsigned long long *>(I);
+    unsigned long long *dst = reinterpret_cast<unsigned long long *>(T);
     const int words = ninst * (int)(sizeof(BatchInstT<R>) / 8);
     for (int w = threadIdx.x; w < words; w += blockDim.x) dst[w] = src[w];
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int k = 0; k < ninst; ++k) T[k].step = steps[k];
+    I = T;
+  } else {
+    prefix = reinterpret_cast<int *>(batch_smem);
+    I = inst;
   }
-  __syncthreads();
   if (threadIdx.x == 0) {
     int run = 0;
     for (int k = 0; k < ninst; ++k) {
-      I[k].step = steps[k];
       prefix[k] = run;
       if ((members >> k) & 1ull)
         run += kChild ? min((int)*I[k].in.count, I[k].in.capacity) : min((int)*I[k].n, I[k].capacity);
@@ -289,11 +308,37 @@ __global__ void __launch_bounds__(kFlightThreads, kFlightBlocks<R>) batch_flight
   fly_interleaved<R, false>(F, S, BatchIO<R, kChild>{I, prefix, ninst}, total, ticket);
 }
 
+// Step numbers of a batch: steps[k] += 1, and the step field of simulation
+// k in each of the `ntab` tables of n simulations.
+template <typename R>
+__global__ void advance_batch_steps(uint32_t *steps, BatchInstT<R> *tab, int n, int ntab) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const uint32_t v = steps[k] + 1;
+  steps[k] = v;
+  for (int t = 0; t < ntab; ++t) tab[(size_t)t * n + k].step = v;
+}
+template <typename R>
+void launch_advance_batch_steps(uint32_t *steps, BatchInstT<R> *tab, int n, int ntab, cudaStream_t s) {
+  advance_batch_steps<R><<<(n + 63) / 64, 64, 0, s>>>(steps, tab, n, ntab);
+}
+
 // FP32 flight's per-cell records (DevMesh::cell32): the fields in float and
 // the Brooks-Herring factors of GetImpScRate / GetImpScGamma /
 // EleImpScUpdateK (src/ElectronImpurityScatter.cpp:6-306) evaluated once per
 // cell in FP64 from the cell's screening density and doping.
-__global__ void cell_records32_kernel(DevTables T, DevMesh M, float4 *out, int cells) {
+//
+// The step's counters are reset in the same launch (block 0: zeroed work
+// tickets, copy counts and appended count), which the flight then reads.
+__device__ __forceinline__ void reset_step_counters(const StepCounters &z, int t) {
+  if (t < 1 + kChildGenerations) {
+    z.tickets[t] = 0u;
+    *z.count[t] = 0u;
+  }
+  if (t == 0) *z.appended = 0u;
+}
+__global__ void cell_records32_kernel(DevTables T, DevMesh M, float4 *out, int cells, StepCounters z) {
+  if (blockIdx.x == 0) reset_step_counters(z, threadIdx.x);
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= cells) return;
   const double rho = M.rho[c], da = M.da[c];
@@ -316,10 +361,13 @@ __device__ __forceinline__ int cell_linear(uint32_t c, int nx, int nz) {
 
 // Buckets of 2^shift consecutive cells of the linear order (z fastest):
 // shift 0 sorts by cell; wider buckets make the histogram and its scan
-// shorter and leave the particles of a bucket in arrival order.
+// shorter and leave the particles of a bucket in arrival order.  When the
+// scatter will compute the sorted store's charge bounds, they start from
+// zero here.
 __global__ void cell_histogram(const uint32_t *cell, const uint32_t *meta, DevCount count, int nx, int nz,
-                               unsigned int *hist, int shift) {
+                               unsigned int *hist, int shift, unsigned long long *bounds) {
   const int n = count.get();
+  if (bounds && blockIdx.x == 0 && threadIdx.x < 4) bounds[threadIdx.x] = 0ull;
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
     if (!(meta[p] & kMetaDead)) atomicAdd(&hist[cell_linear(cell[p], nx, nz) >> shift], 1u);
 }
@@ -368,21 +416,56 @@ __global__ void scan_add(unsigned int *out, const unsigned int *tile_sums, int n
   if (i < n) out[i] += tile_sums[blockIdx.x];
 }
 
+// bounds (optional, zeroed by the histogram): the sorted store's charge
+// bounds in charge_bounds_kernel's layout, {max |q| bits of electrons, of
+// holes, electron count, hole count}, from the particles this pass moves.
 template <typename R>
-__global__ void cell_scatter(DevParticlesT<R> src, DevCount count, DevParticlesT<R> dst, unsigned int *cursor, int nx,
-                             int nz, int shift) {
+__global__ void __launch_bounds__(256) cell_scatter(DevParticlesT<R> src, DevCount count, DevParticlesT<R> dst,
+                                                    unsigned int *cursor, int nx, int nz, int shift,
+                                                    unsigned long long *bounds) {
   const int n = count.get();
+  unsigned long long mx[2] = {0, 0}, cnt[2] = {0, 0};
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
     const uint32_t m = src.meta[p];
     if (m & kMetaDead) continue;
     const unsigned int q = atomicAdd(&cursor[cell_linear(src.cell[p], nx, nz) >> shift], 1u);
+    const double charge = src.charge[p];
     dst.x[q] = src.x[p]; dst.y[q] = src.y[p]; dst.z[q] = src.z[p];
     dst.kx[q] = src.kx[p]; dst.ky[q] = src.ky[p]; dst.kz[q] = src.kz[p];
-    dst.energy[q] = src.energy[p]; dst.charge[q] = src.charge[p];
+    dst.energy[q] = src.energy[p]; dst.charge[q] = charge;
     dst.cell[q] = src.cell[p];
     dst.itet[q] = src.itet[p];
     dst.meta[q] = m & 0xffffu;
     dst.uid[q] = src.uid[p];
+    const int t = ((m >> 8) & 255) == 0 ? 0 : 1;
+    const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(charge));
+    mx[t] = b > mx[t] ? b : mx[t];
+    cnt[t] += 1;
+  }
+  if (bounds == nullptr) return;  // uniform over the grid
+  __shared__ unsigned long long red[4][8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int t = 0; t < 2; ++t) {
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long om = __shfl_down_sync(0xffffffffu, mx[t], o);
+      mx[t] = om > mx[t] ? om : mx[t];
+      cnt[t] += __shfl_down_sync(0xffffffffu, cnt[t], o);
+    }
+    if (lane == 0) {
+      red[t][warp] = mx[t];
+      red[2 + t][warp] = cnt[t];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    const int v = threadIdx.x;
+    unsigned long long a = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) a = v < 2 ? (red[v][w] > a ? red[v][w] : a) : a + red[v][w];
+    if (v < 2) {
+      if (a) atomicMax(bounds + v, a);
+    } else if (a) {
+      atomicAdd(bounds + v, a);
+    }
   }
 }
 
@@ -597,18 +680,21 @@ void launch_child_flight(const FlightCtxT<R> &F, const DevChildrenT<R> &in, int 
 template <typename R>
 int launch_batch_flight(const FlightCtxT<R> &F, const BatchInstT<R> *inst, int ninst, uint64_t members,
                         const uint32_t *steps, bool child, unsigned int *ticket, int blocks_per_sm, int sm_count,
-                        cudaStream_t s) {
+                        cudaStream_t s, bool smem_table) {
   if (ninst < 1 || ninst > kMaxBatch) return 1;
-  const size_t smem = batch_smem_bytes<R>(ninst);
-  auto kernel = child ? batch_flight_kernel<R, true> : batch_flight_kernel<R, false>;
-  // the opt-in to more than 48 KB of dynamic shared memory holds per device
-  static bool opted[kMaxDevices][2] = {};
-  bool &done = opted[current_device()][child ? 1 : 0];
-  if (!done) {
-    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)batch_smem_bytes<R>(kMaxBatch)) != cudaSuccess)
-      return 1;
-    done = true;
+  const size_t smem = batch_smem_bytes<R>(ninst, smem_table);
+  auto kernel = smem_table ? (child ? batch_flight_kernel<R, true, true> : batch_flight_kernel<R, false, true>)
+                           : (child ? batch_flight_kernel<R, true, false> : batch_flight_kernel<R, false, false>);
+  if (smem_table) {
+    // the opt-in to more than 48 KB of dynamic shared memory holds per device
+    static bool opted[kMaxDevices][2] = {};
+    bool &done = opted[current_device()][child ? 1 : 0];
+    if (!done) {
+      if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)batch_smem_bytes<R>(kMaxBatch, true)) != cudaSuccess)
+        return 1;
+      done = true;
+    }
   }
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kFlightThreads, smem) != cudaSuccess ||
@@ -618,8 +704,9 @@ int launch_batch_flight(const FlightCtxT<R> &F, const BatchInstT<R> *inst, int n
   kernel<<<per_sm * sm_count, kFlightThreads, smem, s>>>(F, inst, ninst, members, steps, ticket);
   return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
-void launch_cell_records32(const DevTables &T, const DevMesh &M, float4 *out, int cells, cudaStream_t s) {
-  if (cells > 0) cell_records32_kernel<<<(cells + 255) / 256, 256, 0, s>>>(T, M, out, cells);
+void launch_records_and_reset(const DevTables &T, const DevMesh &M, float4 *out, int cells, const StepCounters &z,
+                              cudaStream_t s) {
+  cell_records32_kernel<<<std::max((cells + 255) / 256, 1), 256, 0, s>>>(T, M, out, cells, z);
 }
 template <typename R>
 void launch_append_children(const ChildSetT<R> &set, unsigned int *next_uid, const DevParticlesT<R> &dst,
@@ -627,14 +714,7 @@ void launch_append_children(const ChildSetT<R> &set, unsigned int *next_uid, con
                             int grid, cudaStream_t s) {
   append_children_kernel<R><<<grid, 256, 0, s>>>(set, next_uid, dst, n, capacity, appended, overflow);
 }
-__global__ void step_reset_kernel(StepCounters z) {
-  const int t = threadIdx.x;
-  if (t < 1 + kChildGenerations) {
-    z.tickets[t] = 0u;
-    *z.count[t] = 0u;
-  }
-  if (t == 0) *z.appended = 0u;
-}
+__global__ void step_reset_kernel(StepCounters z) { reset_step_counters(z, threadIdx.x); }
 void launch_step_reset(const StepCounters &z, cudaStream_t s) { step_reset_kernel<<<1, 32, 0, s>>>(z); }
 void launch_step_finish(unsigned int *n, const unsigned int *sorted_total, unsigned int *next_uid,
                         const unsigned int *appended, unsigned long long *particle_steps, cudaStream_t s) {
@@ -650,15 +730,15 @@ void launch_exclusive_scan(const unsigned int *in, unsigned int *out, unsigned i
 template <typename R>
 void launch_cell_sort(const DevParticlesT<R> &src, DevCount n, const DevParticlesT<R> &dst, int ncells, int nx,
                       int nz, unsigned int *hist, unsigned int *offsets, unsigned int *tile_sums, unsigned int *total,
-                      int shift, int grid, cudaStream_t s) {
+                      int shift, unsigned long long *bounds, int grid, cudaStream_t s) {
   const int buckets = (ncells + (1 << shift) - 1) >> shift;
   cudaMemsetAsync(hist, 0, sizeof(unsigned int) * buckets, s);
-  cell_histogram<<<grid, 256, 0, s>>>(src.cell, src.meta, n, nx, nz, hist, shift);
+  cell_histogram<<<grid, 256, 0, s>>>(src.cell, src.meta, n, nx, nz, hist, shift, bounds);
   const int tiles = (buckets + 1023) / 1024;
   scan_tiles<<<tiles, 1024, 0, s>>>(hist, offsets, tile_sums, buckets);
   scan_tile_sums<<<1, 1024, 0, s>>>(tile_sums, tiles, total);
   scan_add<<<tiles, 1024, 0, s>>>(offsets, tile_sums, buckets);
-  cell_scatter<R><<<grid, 256, 0, s>>>(src, n, dst, offsets, nx, nz, shift);
+  cell_scatter<R><<<grid, 256, 0, s>>>(src, n, dst, offsets, nx, nz, shift, bounds);
 }
 
 #define MCB200_INSTANTIATE(R)                                                                                   \
@@ -672,10 +752,11 @@ void launch_cell_sort(const DevParticlesT<R> &src, DevCount n, const DevParticle
                                           const unsigned int *, int, unsigned int *, unsigned int *, int,       \
                                           cudaStream_t);                                                        \
   template int launch_batch_flight<R>(const FlightCtxT<R> &, const BatchInstT<R> *, int, uint64_t,             \
-                                      const uint32_t *, bool, unsigned int *, int, int, cudaStream_t);          \
+                                      const uint32_t *, bool, unsigned int *, int, int, cudaStream_t, bool);    \
+  template void launch_advance_batch_steps<R>(uint32_t *, BatchInstT<R> *, int, int, cudaStream_t);           \
   template void launch_cell_sort<R>(const DevParticlesT<R> &, DevCount, const DevParticlesT<R> &, int, int, int, \
-                                    unsigned int *, unsigned int *, unsigned int *, unsigned int *, int, int,   \
-                                    cudaStream_t);
+                                    unsigned int *, unsigned int *, unsigned int *, unsigned int *, int,        \
+                                    unsigned long long *, int, cudaStream_t);
 MCB200_INSTANTIATE(double)
 MCB200_INSTANTIATE(float)
 #undef MCB200_INSTANTIATE

@@ -138,6 +138,9 @@ struct FlightInstT {  // one simulation: its mesh and fields, tallies, copy buff
   double dt;
   uint64_t seed;
   uint32_t step;
+  // when set, the step number is read here on the device instead (launches
+  // captured in a CUDA graph and replayed at later steps)
+  const uint32_t *step_dev = nullptr;
 };
 template <typename R>
 struct FlightCtxT : FlightInstT<R> {  // plus the band tables, shared by every simulation
@@ -155,7 +158,7 @@ struct BatchInstT : FlightInstT<R> {
   int capacity;
   int pad_;
 };
-constexpr int kMaxBatch = 64;  // simulations per batched launch (their table sits in shared memory)
+constexpr int kMaxBatch = 64;  // simulations per batched launch (their table fits in shared memory)
 using FlightCtx = FlightCtxT<double>;
 
 __device__ __forceinline__ void tally_add_i64(long long *p, double v, double scale) {
@@ -171,8 +174,9 @@ struct FlyerT {
   const FlightCtxT<R> &F;      // the tables (F.T)
   const SymSmemT<R> &S;
   const FlightInstT<R> *I;     // the simulation of the current particle (F itself unless batched)
-  // random stream and the cached Philox block (index rblk, words rw0..rw3)
-  uint32_t uid, sub, n;
+  // random stream (uid, step_, sub; step_ set by the launch's IO from the
+  // simulation's step) and the cached Philox block (index rblk, words rw0..rw3)
+  uint32_t uid, sub, n, step_;
   uint32_t rblk, rw0, rw1, rw2, rw3;
   // particle registers (MeshQuantities members, include/mcmodel.h:215-233)
   R x, y, z, kx, ky, kz;
@@ -198,7 +202,7 @@ struct FlyerT {
   enum : int { kFsNone = 0, kFsPhonon = 1, kFsIonize = 2, kFsDiffuse = 3 };
   enum : int { kLocNone = 0, kLocBZ = 1, kLocImpurity = 2 };
 
-  __device__ FlyerT(const FlightCtxT<R> &f, const SymSmemT<R> &s) : F(f), S(s), I(&f) {}
+  __device__ FlyerT(const FlightCtxT<R> &f, const SymSmemT<R> &s) : F(f), S(s), I(&f), step_(f.step) {}
 
   __device__ __forceinline__ void start_stream(uint32_t u, uint32_t sb) {
     uid = u;
@@ -219,7 +223,7 @@ struct FlyerT {
         u = mcb200_bits_to_unit(rw3, rw2);
       } else {
         const mcb200_philox_block w =
-            mcb200_philox4x32_10(b, uid, I->step, sub, (uint32_t)I->seed, (uint32_t)(I->seed >> 32));
+            mcb200_philox4x32_10(b, uid, step_, sub, (uint32_t)I->seed, (uint32_t)(I->seed >> 32));
         rblk = b;
         rw2 = w.w[2];
         rw3 = w.w[3];
@@ -231,7 +235,7 @@ struct FlyerT {
       const uint32_t b = n >> 2;
       if (b != rblk) {
         const mcb200_philox_block w =
-            mcb200_philox4x32_10(b, uid, I->step, sub, (uint32_t)I->seed, (uint32_t)(I->seed >> 32));
+            mcb200_philox4x32_10(b, uid, step_, sub, (uint32_t)I->seed, (uint32_t)(I->seed >> 32));
         rblk = b;
         rw0 = w.w[0];
         rw1 = w.w[1];

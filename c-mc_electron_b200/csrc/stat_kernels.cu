@@ -157,7 +157,6 @@ void launch_add_potential(int nodes, const double *pot, double *sum, cudaStream_
 template <typename R>
 void launch_induced_current(const DevParticlesT<R> &P, DevCount n, const DevMesh &M, const DevTables &T,
                             const InducedBuffers &B, int grid, cudaStream_t s) {
-  launch_charge_bounds(P, n, B.bounds, grid, s);
   induced_current_kernel<R><<<grid, 256, 0, s>>>(P, n, M, T, B);
   induced_finish_kernel<<<1, 32, 0, s>>>(B);
 }

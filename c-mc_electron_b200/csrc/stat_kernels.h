@@ -30,12 +30,13 @@ void launch_add_potential(int nodes, const double *pot, double *sum, cudaStream_
 // over live particles of q v . E_w (v the group velocity, E_w[cells][3] the
 // contact's weighting field) added to sum[0], and 1 to sum[1] (steps).  The
 // particle terms are summed in int64 fixed point (acc) with a unit from the
-// store's charge bounds (bounds[4], computed here), so the result does not
+// store's charge bounds (bounds[4], the context's, kept current by every
+// writer of the store), so the result does not
 // depend on the store's order; the step's total is then added to the FP64
 // running sum by one thread.  vmax, emax: bounds on |v| and |E_w| components.
 struct InducedBuffers {
   const double *field = nullptr;
-  unsigned long long *bounds = nullptr;  // [4] charge bounds of the store
+  const unsigned long long *bounds = nullptr;  // [4] charge bounds of the store
   long long *acc = nullptr;              // [1]
   double *sum = nullptr;                 // [2]
   double vmax = 0, emax = 0;

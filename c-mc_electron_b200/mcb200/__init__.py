@@ -94,7 +94,8 @@ class BatchMember(ctypes.Structure):
 class BatchTuning(ctypes.Structure):
     _fields_ = [("flight_blocks_per_sm", ctypes.c_int), ("grid_per_sm", ctypes.c_int), ("overlap", ctypes.c_int),
                 ("ms_per_step", ctypes.c_double), ("candidates", ctypes.c_int), ("pair_solves", ctypes.c_int),
-                ("sort_bucket", ctypes.c_int)]
+                ("sort_bucket", ctypes.c_int), ("smem_table", ctypes.c_int),
+                ("solo_min_particles", ctypes.c_uint64), ("solo_members", ctypes.c_int)]
 
 
 class ServerOptions(ctypes.Structure):
@@ -169,6 +170,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mcb200_batch_set_grid.argtypes = [vp, c.c_int]
     lib.mcb200_batch_set_overlap.argtypes = [vp, c.c_int]
     lib.mcb200_batch_set_pairing.argtypes = [vp, c.c_int]
+    if hasattr(lib, "mcb200_batch_set_smem_table"):
+        lib.mcb200_batch_set_smem_table.argtypes = [vp, c.c_int]
+    if hasattr(lib, "mcb200_batch_set_solo"):
+        lib.mcb200_batch_set_solo.argtypes = [vp, c.c_uint64, c.POINTER(c.c_int)]
     lib.mcb200_batch_mark.argtypes = [vp, c.c_int]
     lib.mcb200_batch_elapsed_ms.argtypes = [vp, c.c_int, c.c_int, dp]
     lib.mcb200_batch_info.argtypes = [vp, c.POINTER(c.c_int), c.POINTER(c.c_uint64), c.POINTER(c.c_uint64),
@@ -658,9 +663,7 @@ class Batch:
         """Launch shapes picked by timing real steps (mcb200_batch_autotune)."""
         t = BatchTuning()
         self._check(self._lib.mcb200_batch_autotune(self._b, trial_steps, ctypes.byref(t)), "mcb200_batch_autotune")
-        return {"flight_blocks_per_sm": t.flight_blocks_per_sm, "grid_per_sm": t.grid_per_sm,
-                "overlap": t.overlap, "pair_solves": t.pair_solves, "ms_per_step": t.ms_per_step,
-                "candidates": t.candidates}
+        return {name: getattr(t, name) for name, _ in BatchTuning._fields_}
 
     def use_graphs(self, enable: bool = True):
         self._check(self._lib.mcb200_batch_use_graphs(self._b, int(enable)), "mcb200_batch_use_graphs")
@@ -670,6 +673,19 @@ class Batch:
 
     def set_grid(self, blocks_per_sm: int):
         self._check(self._lib.mcb200_batch_set_grid(self._b, blocks_per_sm), "mcb200_batch_set_grid")
+
+    def set_solo(self, min_particles: int) -> int:
+        """Members with at least min_particles particles (0: none) fly in
+        launches of their own; returns how many."""
+        k = ctypes.c_int()
+        self._check(self._lib.mcb200_batch_set_solo(self._b, int(min_particles), ctypes.byref(k)),
+                    "mcb200_batch_set_solo")
+        return k.value
+
+    def set_smem_table(self, enable: bool = True):
+        """Copy the member table into each flight block's shared memory
+        (default off: read in place)."""
+        self._check(self._lib.mcb200_batch_set_smem_table(self._b, int(bool(enable))), "mcb200_batch_set_smem_table")
 
     def set_overlap(self, enable: bool = True):
         """Fly the members not solving Poisson beside the solves (default on)."""

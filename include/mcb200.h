@@ -382,14 +382,16 @@ int mcb200_batch_use_graphs(mcb200_batch *batch, int enable);
 /* Launch shapes picked by measurement: for every candidate (batched-flight
  * blocks per SM in {1, 2} x blocks per SM of the members' per-step kernels
  * -- sort, deposition, copies -- in {2, 4, 8}; then the fastest of those
- * with overlap, pairing and both switched; then the fastest of those with
- * the members' sort-bucket width in {1, 2, 4, 8} cells,
- * mcb200_set_sort_bucket) one untimed and `trial_steps` timed full
- * timesteps (mcb200_batch_run: they advance the simulations like any other
- * steps).  The candidates of each of the three stages are timed in order
- * and again in reverse order, so that a steady drift of the simulations
- * (particle counts) cancels; the fastest mean device time is kept and
- * returned. */
+ * with every combination of overlap, pairing and the member table's place
+ * switched; then the fastest of those with the members' sort-bucket width
+ * in {1, 2, 4, 8} cells (mcb200_set_sort_bucket); then the fastest of those
+ * with no member, every member, or the members above the first, second or
+ * third quartile of the particle counts flying solo (mcb200_batch_set_solo))
+ * one untimed and `trial_steps` timed full timesteps (mcb200_batch_run:
+ * they advance the simulations like any other steps).  The candidates of
+ * each of the four stages are timed in order and again in reverse order,
+ * so that a steady drift of the simulations (particle counts) cancels; the
+ * fastest mean device time is kept and returned. */
 typedef struct {
   int flight_blocks_per_sm, grid_per_sm;
   int overlap; /* mcb200_batch_set_overlap */
@@ -397,6 +399,9 @@ typedef struct {
   int candidates;
   int pair_solves; /* mcb200_batch_set_pairing */
   int sort_bucket; /* cells per sort bucket of every member */
+  int smem_table;  /* mcb200_batch_set_smem_table */
+  uint64_t solo_min_particles; /* mcb200_batch_set_solo (0: none) */
+  int solo_members;            /* members flying solo with it */
 } mcb200_batch_tuning;
 int mcb200_batch_autotune(mcb200_batch *batch, int trial_steps, mcb200_batch_tuning *best);
 /* Wait for the batch and every member; reports a member's full store. */
@@ -410,6 +415,22 @@ int mcb200_batch_set_grid(mcb200_batch *batch, int blocks_per_sm);
  * and a helper launch then takes over what is left of the first launch's
  * particles.  The result is the same either way. */
 int mcb200_batch_set_overlap(mcb200_batch *batch, int enable);
+/* Solo members (default none): members holding at least min_particles
+ * particles now (0: none) fly in launches of their own on their own streams
+ * -- the flight and copy flights of mcb200_step, the step number read on the
+ * device so that graph replays stay right -- while the others share the
+ * batched launches.  Large members fill the GPU alone and gain nothing from
+ * sharing a launch; their own launches overlap the batched ones and start
+ * their tails without waiting for every member's flight.  The set is fixed
+ * until the next call; *members (or null) receives its size.  The result is
+ * the same either way. */
+int mcb200_batch_set_solo(mcb200_batch *batch, uint64_t min_particles, int *members);
+/* Member table (default off): every block of a batched flight copies the
+ * table of members (about 0.8 KB each) into shared memory, instead of its
+ * lanes reading it from device memory through L1.  The copy costs L1
+ * capacity (the shared-memory carve-out grows with it); the reads in place
+ * cost L1 traffic.  The result is the same either way. */
+int mcb200_batch_set_smem_table(mcb200_batch *batch, int enable);
 /* Pairing (default on): two due multigrid Poisson solves whose hierarchies
  * have the same depth, smoothing and solve grid run in one cooperative
  * launch of twice the grid (each on its own half, exactly as alone: the
