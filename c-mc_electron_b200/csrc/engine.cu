@@ -518,6 +518,8 @@ void init_device_context(mcb200_ctx *c, size_t max_particles) {
   c->y.counters = dalloc<unsigned long long>(kCntNumCounters, c->owned);
   c->y.contact = dalloc<long long>(kMaxContacts * 6, c->owned);
   c->total = dalloc<unsigned int>(1, c->owned);
+  c->finish_blocks = dalloc<unsigned int>(2, c->owned);
+  ck(cudaMemsetAsync(c->finish_blocks, 0, 2 * sizeof(unsigned int), c->stream), "memset");
   c->dev_counts = dalloc<unsigned int>(4, c->owned);
   c->dev_psteps = dalloc<unsigned long long>(1, c->owned);
   c->sink_count = dalloc<unsigned int>(1, c->owned);
@@ -1979,12 +1981,19 @@ void step_tail(mcb200_ctx *c) {
   ck(cudaGetLastError(), "append children");
   c->launches += 1;
   const int other = 1 - c->cur;
+  StepFinish fin;  // by the scatter's last block
+  fin.n = c->dev_counts;
+  fin.sorted_total = c->total;
+  fin.next_uid = c->dev_counts + 1;
+  fin.appended = c->append_count;
+  fin.particle_steps = c->dev_psteps;
+  fin.blocks = c->finish_blocks;
+  fin.scan_blocks = c->finish_blocks + 1;
   launch_cell_sort(store<R>(c, c->cur), DevCount{c->dev_counts, c->append_count, cap}, store<R>(c, other), c->ncells,
                    c->mesh.nx, c->mesh.nz, c->hist, c->offsets, c->tile_sums, c->total, c->sort_shift, c->bounds,
-                   grid_for(c, c->capacity, 256), s);
-  launch_step_finish(c->dev_counts, c->total, c->dev_counts + 1, c->append_count, c->dev_psteps, s);
+                   grid_for(c, c->capacity, 256), s, fin);
   ck(cudaGetLastError(), "cell sort");
-  c->launches += 6;
+  c->launches += 3;  // histogram, scans, scatter
   c->cur = other;
   c->n_stale = true;
 }

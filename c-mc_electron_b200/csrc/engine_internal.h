@@ -193,6 +193,7 @@ struct mcb200_ctx {
   // the step's sort computes them, every other writer of the store after it
   // writes (store_bounds); the deposition's fixed-point units come from them
   unsigned long long *bounds = nullptr;
+  unsigned int *finish_blocks = nullptr;  // [2] blocks of the step's scatter / scan done (zero between steps)
   unsigned int *tickets = nullptr;  // work counters of the persistent flight launches (main + generations)
   float4 *cell32 = nullptr;         // FP32 flight's per-cell records (mesh-sized)
   // tallies

@@ -58,9 +58,20 @@ void launch_step_reset(const StepCounters &z, cudaStream_t s);
 // the step reset of z, in one launch.
 void launch_records_and_reset(const DevTables &T, const DevMesh &M, float4 *out, int cells, const StepCounters &z,
                               cudaStream_t s);
-// *particle_steps += *n; *n = *sorted_total; *next_uid += *appended.
-void launch_step_finish(unsigned int *n, const unsigned int *sorted_total, unsigned int *next_uid,
-                        const unsigned int *appended, unsigned long long *particle_steps, cudaStream_t s);
+// The end of a step, done by the last block of the sort's scatter (n null:
+// none): *particle_steps += *n; *n = *sorted_total; *next_uid += *appended.
+// blocks, scan_blocks: counters that are zero between launches.  A sort
+// with a StepFinish leaves `offsets` as tile-local cell ends (nothing reads
+// them after the step's sort).
+struct StepFinish {
+  unsigned int *n = nullptr;
+  const unsigned int *sorted_total = nullptr;
+  unsigned int *next_uid = nullptr;
+  const unsigned int *appended = nullptr;
+  unsigned long long *particle_steps = nullptr;
+  unsigned int *blocks = nullptr;
+  unsigned int *scan_blocks = nullptr;
+};
 template <typename R>
 void launch_seed(const FlightCtx &F, const DevParticlesT<R> &P, int offset, int n, const int *cell_of,
                  const double *charge, int type, uint32_t uid0, int grid, cudaStream_t s);
@@ -74,6 +85,7 @@ void launch_exclusive_scan(const unsigned int *in, unsigned int *out, unsigned i
 template <typename R>
 void launch_cell_sort(const DevParticlesT<R> &src, DevCount n, const DevParticlesT<R> &dst, int ncells, int nx,
                       int nz, unsigned int *hist, unsigned int *offsets, unsigned int *tile_sums, unsigned int *total,
-                      int shift, unsigned long long *bounds, int grid, cudaStream_t s);
+                      int shift, unsigned long long *bounds, int grid, cudaStream_t s,
+                      const StepFinish &finish = StepFinish{});
 
 }  // namespace mcb200

@@ -10,8 +10,9 @@
 //      the rest of the step (they may make copies of their own).
 //   3. append_children_kernel: surviving copies join the store with uids
 //      next_uid + rank of (parent, sub).
-//   4. cell_histogram / cell_scan / cell_scatter: survivors and copies are
-//      counting-sorted by cell into the second particle buffer.
+//   4. cell_histogram / scan_tiles / cell_scatter: survivors and copies are
+//      counting-sorted by cell into the second particle buffer; the
+//      scatter's last block makes the sorted count the particle count.
 #include <algorithm>
 
 #include "engine_kernels.h"
@@ -374,29 +375,14 @@ __global__ void cell_histogram(const uint32_t *cell, const uint32_t *meta, DevCo
 
 // Exclusive scan of `count` values, single pass per 1024-wide tile plus a
 // tile-sum pass (cells are at most ~10^6, so three small launches suffice).
-__global__ void scan_tiles(const unsigned int *in, unsigned int *out, unsigned int *tile_sums, int n) {
-  __shared__ unsigned int s[1024];
-  const int i = blockIdx.x * 1024 + threadIdx.x;
-  const unsigned int v = i < n ? in[i] : 0u;
-  s[threadIdx.x] = v;
-  __syncthreads();
-  for (int off = 1; off < 1024; off <<= 1) {
-    unsigned int t = threadIdx.x >= (unsigned)off ? s[threadIdx.x - off] : 0u;
-    __syncthreads();
-    s[threadIdx.x] += t;
-    __syncthreads();
-  }
-  if (i < n) out[i] = s[threadIdx.x] - v;
-  if (threadIdx.x == 1023) tile_sums[blockIdx.x] = s[1023];
-}
-// Exclusive scan of the tile sums in place, one block of 1024 threads, 1024
-// tiles per pass with the running total carried between passes.
-__global__ void scan_tile_sums(unsigned int *tile_sums, int ntiles, unsigned int *total) {
+// Exclusive scan of the tile sums in place by one block of 1024 threads,
+// 1024 tiles per pass with the running total carried between passes.
+__device__ void scan_tile_sums_block(unsigned int *tile_sums, int ntiles, unsigned int *total) {
   __shared__ unsigned int s[1024];
   unsigned int carry = 0;
   for (int base = 0; base < ntiles; base += 1024) {
     const int t = base + threadIdx.x;
-    const unsigned int v = t < ntiles ? tile_sums[t] : 0u;
+    const unsigned int v = t < ntiles ? __ldcg(tile_sums + t) : 0u;  // written by other blocks: read at L2
     s[threadIdx.x] = v;
     __syncthreads();
     for (int off = 1; off < 1024; off <<= 1) {
@@ -411,6 +397,41 @@ __global__ void scan_tile_sums(unsigned int *tile_sums, int ntiles, unsigned int
   }
   if (threadIdx.x == 0) *total = carry;
 }
+
+// Exclusive scan of each 1024-wide tile, and its sum into tile_sums.  With
+// `blocks` (a counter that is zero between launches) the last block to
+// finish then scans the tile sums too (scan_tile_sums' work, one launch
+// fewer).
+__global__ void scan_tiles(const unsigned int *in, unsigned int *out, unsigned int *tile_sums, int n,
+                           unsigned int *blocks, unsigned int *total) {
+  __shared__ unsigned int s[1024];
+  __shared__ bool last;
+  const int i = blockIdx.x * 1024 + threadIdx.x;
+  const unsigned int v = i < n ? in[i] : 0u;
+  s[threadIdx.x] = v;
+  __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {
+    unsigned int t = threadIdx.x >= (unsigned)off ? s[threadIdx.x - off] : 0u;
+    __syncthreads();
+    s[threadIdx.x] += t;
+    __syncthreads();
+  }
+  if (i < n) out[i] = s[threadIdx.x] - v;
+  if (threadIdx.x == 1023) tile_sums[blockIdx.x] = s[1023];
+  if (blocks == nullptr) return;  // uniform over the grid
+  if (threadIdx.x == 1023) {
+    __threadfence();
+    last = atomicAdd(blocks, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;  // uniform over the block
+  __threadfence();
+  scan_tile_sums_block(tile_sums, (int)gridDim.x, total);
+  if (threadIdx.x == 0) *blocks = 0u;
+}
+__global__ void scan_tile_sums(unsigned int *tile_sums, int ntiles, unsigned int *total) {
+  scan_tile_sums_block(tile_sums, ntiles, total);
+}
 __global__ void scan_add(unsigned int *out, const unsigned int *tile_sums, int n) {
   const int i = blockIdx.x * 1024 + threadIdx.x;
   if (i < n) out[i] += tile_sums[blockIdx.x];
@@ -419,16 +440,23 @@ __global__ void scan_add(unsigned int *out, const unsigned int *tile_sums, int n
 // bounds (optional, zeroed by the histogram): the sorted store's charge
 // bounds in charge_bounds_kernel's layout, {max |q| bits of electrons, of
 // holes, electron count, hole count}, from the particles this pass moves.
+// finish (optional): the end of the step, by the grid's last block to
+// finish (every block has read the count by then).
+// tile_base (optional): cursor holds tile-local offsets and the tile's
+// exclusive prefix is added (scan_add's work, one launch fewer; the cursor
+// then ends as tile-local cell ends).
 template <typename R>
 __global__ void __launch_bounds__(256) cell_scatter(DevParticlesT<R> src, DevCount count, DevParticlesT<R> dst,
                                                     unsigned int *cursor, int nx, int nz, int shift,
-                                                    unsigned long long *bounds) {
+                                                    unsigned long long *bounds, StepFinish finish,
+                                                    const unsigned int *tile_base) {
   const int n = count.get();
   unsigned long long mx[2] = {0, 0}, cnt[2] = {0, 0};
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
     const uint32_t m = src.meta[p];
     if (m & kMetaDead) continue;
-    const unsigned int q = atomicAdd(&cursor[cell_linear(src.cell[p], nx, nz) >> shift], 1u);
+    const int key = cell_linear(src.cell[p], nx, nz) >> shift;
+    const unsigned int q = atomicAdd(&cursor[key], 1u) + (tile_base ? tile_base[key >> 10] : 0u);
     const double charge = src.charge[p];
     dst.x[q] = src.x[p]; dst.y[q] = src.y[p]; dst.z[q] = src.z[p];
     dst.kx[q] = src.kx[p]; dst.ky[q] = src.ky[p]; dst.kz[q] = src.kz[p];
@@ -442,29 +470,44 @@ __global__ void __launch_bounds__(256) cell_scatter(DevParticlesT<R> src, DevCou
     mx[t] = b > mx[t] ? b : mx[t];
     cnt[t] += 1;
   }
-  if (bounds == nullptr) return;  // uniform over the grid
-  __shared__ unsigned long long red[4][8];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int t = 0; t < 2; ++t) {
-    for (int o = 16; o > 0; o >>= 1) {
-      const unsigned long long om = __shfl_down_sync(0xffffffffu, mx[t], o);
-      mx[t] = om > mx[t] ? om : mx[t];
-      cnt[t] += __shfl_down_sync(0xffffffffu, cnt[t], o);
+  if (bounds != nullptr) {  // uniform over the grid
+    __shared__ unsigned long long red[4][8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int t = 0; t < 2; ++t) {
+      for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long om = __shfl_down_sync(0xffffffffu, mx[t], o);
+        mx[t] = om > mx[t] ? om : mx[t];
+        cnt[t] += __shfl_down_sync(0xffffffffu, cnt[t], o);
+      }
+      if (lane == 0) {
+        red[t][warp] = mx[t];
+        red[2 + t][warp] = cnt[t];
+      }
     }
-    if (lane == 0) {
-      red[t][warp] = mx[t];
-      red[2 + t][warp] = cnt[t];
+    __syncthreads();
+    if (threadIdx.x < 4) {
+      const int v = threadIdx.x;
+      unsigned long long a = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) a = v < 2 ? (red[v][w] > a ? red[v][w] : a) : a + red[v][w];
+      if (v < 2) {
+        if (a) atomicMax(bounds + v, a);
+      } else if (a) {
+        atomicAdd(bounds + v, a);
+      }
     }
   }
-  __syncthreads();
-  if (threadIdx.x < 4) {
-    const int v = threadIdx.x;
-    unsigned long long a = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) a = v < 2 ? (red[v][w] > a ? red[v][w] : a) : a + red[v][w];
-    if (v < 2) {
-      if (a) atomicMax(bounds + v, a);
-    } else if (a) {
-      atomicAdd(bounds + v, a);
+  if (finish.n != nullptr) {  // uniform over the grid
+    __syncthreads();  // every thread of the block has read the count
+    if (threadIdx.x == 0) {
+      __threadfence();
+      const unsigned int done = atomicAdd(finish.blocks, 1u);
+      if (done == gridDim.x - 1) {  // the last block: every block has read the count
+        __threadfence();
+        *finish.particle_steps += *finish.n;
+        *finish.n = *finish.sorted_total;
+        *finish.next_uid += *finish.appended;
+        *finish.blocks = 0u;
+      }
     }
   }
 }
@@ -551,18 +594,6 @@ __global__ void append_children_kernel(ChildSetT<R> set, const unsigned int *nex
       dst.meta[q] = c.meta[local] & 0xffffu;
       dst.uid[q] = uid0 + rank;
     }
-  }
-}
-
-// End of a step: the sorted store's count becomes the particle count, the
-// uid counter advances past this step's copies, and the particles flown this
-// step (the count at its start) are added to the particle-step total.
-__global__ void step_finish(unsigned int *n, const unsigned int *sorted_total, unsigned int *next_uid,
-                            const unsigned int *appended, unsigned long long *particle_steps) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    *particle_steps += *n;
-    *n = *sorted_total;
-    *next_uid += *appended;
   }
 }
 
@@ -716,29 +747,32 @@ void launch_append_children(const ChildSetT<R> &set, unsigned int *next_uid, con
 }
 __global__ void step_reset_kernel(StepCounters z) { reset_step_counters(z, threadIdx.x); }
 void launch_step_reset(const StepCounters &z, cudaStream_t s) { step_reset_kernel<<<1, 32, 0, s>>>(z); }
-void launch_step_finish(unsigned int *n, const unsigned int *sorted_total, unsigned int *next_uid,
-                        const unsigned int *appended, unsigned long long *particle_steps, cudaStream_t s) {
-  step_finish<<<1, 32, 0, s>>>(n, sorted_total, next_uid, appended, particle_steps);
-}
 void launch_exclusive_scan(const unsigned int *in, unsigned int *out, unsigned int *tile_sums, unsigned int *total,
                            int n, cudaStream_t s) {
   const int tiles = (n + 1023) / 1024;
-  scan_tiles<<<tiles, 1024, 0, s>>>(in, out, tile_sums, n);
+  scan_tiles<<<tiles, 1024, 0, s>>>(in, out, tile_sums, n, nullptr, nullptr);
   scan_tile_sums<<<1, 1024, 0, s>>>(tile_sums, tiles, total);
   scan_add<<<tiles, 1024, 0, s>>>(out, tile_sums, n);
 }
 template <typename R>
 void launch_cell_sort(const DevParticlesT<R> &src, DevCount n, const DevParticlesT<R> &dst, int ncells, int nx,
                       int nz, unsigned int *hist, unsigned int *offsets, unsigned int *tile_sums, unsigned int *total,
-                      int shift, unsigned long long *bounds, int grid, cudaStream_t s) {
+                      int shift, unsigned long long *bounds, int grid, cudaStream_t s, const StepFinish &finish) {
   const int buckets = (ncells + (1 << shift) - 1) >> shift;
   cudaMemsetAsync(hist, 0, sizeof(unsigned int) * buckets, s);
   cell_histogram<<<grid, 256, 0, s>>>(src.cell, src.meta, n, nx, nz, hist, shift, bounds);
   const int tiles = (buckets + 1023) / 1024;
-  scan_tiles<<<tiles, 1024, 0, s>>>(hist, offsets, tile_sums, buckets);
+  if (finish.n != nullptr) {
+    // the step's sort: the tile sums scanned by scan_tiles' last block, the
+    // tile prefixes added by the scatter, the step ended by its last block
+    scan_tiles<<<tiles, 1024, 0, s>>>(hist, offsets, tile_sums, buckets, finish.scan_blocks, total);
+    cell_scatter<R><<<grid, 256, 0, s>>>(src, n, dst, offsets, nx, nz, shift, bounds, finish, tile_sums);
+    return;
+  }
+  scan_tiles<<<tiles, 1024, 0, s>>>(hist, offsets, tile_sums, buckets, nullptr, nullptr);
   scan_tile_sums<<<1, 1024, 0, s>>>(tile_sums, tiles, total);
   scan_add<<<tiles, 1024, 0, s>>>(offsets, tile_sums, buckets);
-  cell_scatter<R><<<grid, 256, 0, s>>>(src, n, dst, offsets, nx, nz, shift, bounds);
+  cell_scatter<R><<<grid, 256, 0, s>>>(src, n, dst, offsets, nx, nz, shift, bounds, finish, nullptr);
 }
 
 #define MCB200_INSTANTIATE(R)                                                                                   \
@@ -756,7 +790,7 @@ void launch_cell_sort(const DevParticlesT<R> &src, DevCount n, const DevParticle
   template void launch_advance_batch_steps<R>(uint32_t *, BatchInstT<R> *, int, int, cudaStream_t);           \
   template void launch_cell_sort<R>(const DevParticlesT<R> &, DevCount, const DevParticlesT<R> &, int, int, int, \
                                     unsigned int *, unsigned int *, unsigned int *, unsigned int *, int,        \
-                                    unsigned long long *, int, cudaStream_t);
+                                    unsigned long long *, int, cudaStream_t, const StepFinish &);
 MCB200_INSTANTIATE(double)
 MCB200_INSTANTIATE(float)
 #undef MCB200_INSTANTIATE
