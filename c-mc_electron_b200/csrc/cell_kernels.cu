@@ -13,6 +13,7 @@
 //    its own stream (seed, cell, step, kRefreshSub + type).  Resampled
 //    particles get fresh uids in (cell, type, draw) order.
 #include "cell_kernels.h"
+#include "pdl.cuh"
 
 namespace mcb200 {
 
@@ -21,6 +22,7 @@ constexpr double kPiC = 3.141592653589793238462643e0;
 __global__ void surface_rates_kernel(int cells, SurfaceRateParams q, const double *field, const double *rho,
                                      const int *eeff_dir, double *e_rough, double *e_phon, double *h_rough,
                                      double *h_phon) {
+  pdl_wait();
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= cells) return;
   const double Rho = rho[c];
@@ -199,8 +201,8 @@ __global__ void refresh_emit_kernel(DevParticlesT<R> P, const unsigned int *cell
 void launch_surface_rates(int cells, const SurfaceRateParams &q, const double *field, const double *rho,
                           const int *eeff_dir, double *e_rough, double *e_phon, double *h_rough, double *h_phon,
                           cudaStream_t s) {
-  surface_rates_kernel<<<(cells + 255) / 256, 256, 0, s>>>(cells, q, field, rho, eeff_dir, e_rough, e_phon, h_rough,
-                                                           h_phon);
+  launch_pdl(surface_rates_kernel, (cells + 255) / 256, 256, 0, s, cells, q, field, rho, eeff_dir, e_rough, e_phon,
+             h_rough, h_phon);
 }
 template <typename R>
 void launch_refresh_count(const DevParticlesT<R> &P, const unsigned int *cell_end, const unsigned int *cell_count,

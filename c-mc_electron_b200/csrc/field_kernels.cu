@@ -21,6 +21,7 @@
 #include "device_state.cuh"
 #include "field_kernels.h"
 #include "poisson_common.cuh"
+#include "pdl.cuh"
 #include "warp_segments.cuh"
 
 namespace mcb200 {
@@ -106,6 +107,7 @@ template <typename R>
 __global__ void __launch_bounds__(256) deposit_kernel(DevParticlesT<R> P, DevCount count, DevMesh M,
                                                       const unsigned long long *bounds, long long *cell_e,
                                                       long long *cell_h, long long *cell_abs, long long *node_q) {
+  pdl_wait();
   const int n = count.get();
   const DepositScales S = deposit_scales(bounds);
   const int px = M.nx + 1, pz = M.nz + 1;
@@ -172,6 +174,7 @@ __global__ void deposit_sums_kernel(int cells, int nodes, const unsigned long lo
                                     long long *cell_h, long long *cell_abs, const double *cvol, const double *da,
                                     double *e_out, double *h_out, double *rho_out, long long *node_q,
                                     const double *pvol, double *density) {
+  pdl_wait();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= cells && t >= nodes) return;
   const DepositScales S = deposit_scales(bounds);
@@ -436,11 +439,12 @@ template <typename R>
 void launch_deposit(const DevParticlesT<R> &P, DevCount n, const DevMesh &M, const FieldBuffers &f, int grid,
                     cudaStream_t s) {
   const int cells = M.nx * M.ny * M.nz, nodes = (M.nx + 1) * (M.ny + 1) * (M.nz + 1);
-  deposit_kernel<R><<<grid, 256, 0, s>>>(P, n, M, f.abs_sum, f.acc_cell, f.acc_cell + cells,
-                                         f.acc_cell + 2 * (size_t)cells, f.acc_node);
-  deposit_sums_kernel<<<blocks(std::max(cells, nodes), 256), 256, 0, s>>>(
-      cells, nodes, f.abs_sum, f.acc_cell, f.acc_cell + cells, f.acc_cell + 2 * (size_t)cells, f.cvol, M.da,
-      f.cell_e, f.cell_h, const_cast<double *>(M.rho), f.acc_node, f.pvol, f.density);
+  launch_pdl(deposit_kernel<R>, grid, 256, 0, s, P, n, M, (const unsigned long long *)f.abs_sum, f.acc_cell,
+             f.acc_cell + cells, f.acc_cell + 2 * (size_t)cells, f.acc_node);
+  launch_pdl(deposit_sums_kernel, blocks(std::max(cells, nodes), 256), 256, 0, s, cells, nodes,
+             (const unsigned long long *)f.abs_sum, f.acc_cell, f.acc_cell + cells, f.acc_cell + 2 * (size_t)cells,
+             (const double *)f.cvol, M.da, f.cell_e, f.cell_h, const_cast<double *>(M.rho), f.acc_node,
+             (const double *)f.pvol, f.density);
 }
 
 template void launch_charge_bounds<double>(const DevParticlesT<double> &, DevCount, unsigned long long *, int,

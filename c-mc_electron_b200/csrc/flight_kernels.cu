@@ -17,6 +17,7 @@
 
 #include "engine_kernels.h"
 #include "flight_physics.cuh"
+#include "pdl.cuh"
 #include "flight_physics_impl.cuh"
 
 namespace mcb200 {
@@ -193,10 +194,11 @@ __device__ __forceinline__ void fly_interleaved(const FlightCtxT<R> &F, const Sy
 template <typename R>
 __global__ void __launch_bounds__(kFlightThreads, kFlightBlocks<R>) flight_kernel(FlightCtxT<R> F, DevParticlesT<R> P,
                                                                        DevCount n, unsigned int *ticket) {
+  __shared__ SymSmemT<R> S;
+  load_sym(S, F.T);  // the band tables: nothing the kernel ahead writes
+  pdl_wait();
   const int count = n.get();
   if (count == 0) return;
-  __shared__ SymSmemT<R> S;
-  load_sym(S, F.T);
   const uint32_t step = F.step_dev ? *F.step_dev : F.step;
   fly_interleaved<R, true>(F, S, StoreIO<R>{P, F.dt, step}, count, ticket);
 }
@@ -206,6 +208,7 @@ __global__ void __launch_bounds__(kFlightThreads, kFlightBlocks<R>) flight_kerne
 template <typename R>
 __global__ void __launch_bounds__(kFlightThreads, kFlightBlocks<R>) child_flight_kernel(FlightCtxT<R> F, DevChildrenT<R> in,
                                                               unsigned int *ticket) {
+  pdl_wait();
   const int count = min((int)*in.count, in.capacity);
   if (count == 0) return;
   __shared__ SymSmemT<R> S;
@@ -339,6 +342,7 @@ __device__ __forceinline__ void reset_step_counters(const StepCounters &z, int t
   if (t == 0) *z.appended = 0u;
 }
 __global__ void cell_records32_kernel(DevTables T, DevMesh M, float4 *out, int cells, StepCounters z) {
+  pdl_wait();
   if (blockIdx.x == 0) reset_step_counters(z, threadIdx.x);
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= cells) return;
@@ -367,6 +371,7 @@ __device__ __forceinline__ int cell_linear(uint32_t c, int nx, int nz) {
 // zero here.
 __global__ void cell_histogram(const uint32_t *cell, const uint32_t *meta, DevCount count, int nx, int nz,
                                unsigned int *hist, int shift, unsigned long long *bounds) {
+  pdl_wait();
   const int n = count.get();
   if (bounds && blockIdx.x == 0 && threadIdx.x < 4) bounds[threadIdx.x] = 0ull;
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
@@ -406,6 +411,7 @@ __global__ void scan_tiles(const unsigned int *in, unsigned int *out, unsigned i
                            unsigned int *blocks, unsigned int *total) {
   __shared__ unsigned int s[1024];
   __shared__ bool last;
+  pdl_wait();
   const int i = blockIdx.x * 1024 + threadIdx.x;
   const unsigned int v = i < n ? in[i] : 0u;
   s[threadIdx.x] = v;
@@ -450,6 +456,7 @@ __global__ void __launch_bounds__(256) cell_scatter(DevParticlesT<R> src, DevCou
                                                     unsigned int *cursor, int nx, int nz, int shift,
                                                     unsigned long long *bounds, StepFinish finish,
                                                     const unsigned int *tile_base) {
+  pdl_wait();
   const int n = count.get();
   unsigned long long mx[2] = {0, 0}, cnt[2] = {0, 0};
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
@@ -553,6 +560,7 @@ __global__ void append_children_kernel(ChildSetT<R> set, const unsigned int *nex
                                        const unsigned int *n, int capacity, unsigned int *appended,
                                        unsigned int *overflow) {
   __shared__ uint64_t tile[256];
+  pdl_wait();
   const CopyRef<R> ref(set);
   int total = 0;
 #pragma unroll
@@ -698,7 +706,7 @@ int flight_grid(int n, int block, int sm_count) {
 template <typename R>
 void launch_flight(const FlightCtxT<R> &F, const DevParticlesT<R> &P, DevCount n, unsigned int *ticket, int sm_count,
                    cudaStream_t s) {
-  flight_kernel<R><<<flight_grid<R>(n.max, kFlightThreads, sm_count), kFlightThreads, 0, s>>>(F, P, n, ticket);
+  launch_pdl(flight_kernel<R>, flight_grid<R>(n.max, kFlightThreads, sm_count), kFlightThreads, 0, s, F, P, n, ticket);
 }
 template <typename R>
 void launch_child_flight(const FlightCtxT<R> &F, const DevChildrenT<R> &in, int n_hint, unsigned int *ticket,
@@ -706,7 +714,7 @@ void launch_child_flight(const FlightCtxT<R> &F, const DevChildrenT<R> &in, int 
   // One block per SM: a step's copies are few (their lanes refill from the
   // same counter however many there are), and most generations are empty.
   const int n = (int)std::min<long long>(n_hint, (long long)sm_count * kFlightThreads);
-  child_flight_kernel<R><<<flight_grid<R>(n, kFlightThreads, sm_count), kFlightThreads, 0, s>>>(F, in, ticket);
+  launch_pdl(child_flight_kernel<R>, flight_grid<R>(n, kFlightThreads, sm_count), kFlightThreads, 0, s, F, in, ticket);
 }
 template <typename R>
 int launch_batch_flight(const FlightCtxT<R> &F, const BatchInstT<R> *inst, int ninst, uint64_t members,
@@ -737,13 +745,13 @@ int launch_batch_flight(const FlightCtxT<R> &F, const BatchInstT<R> *inst, int n
 }
 void launch_records_and_reset(const DevTables &T, const DevMesh &M, float4 *out, int cells, const StepCounters &z,
                               cudaStream_t s) {
-  cell_records32_kernel<<<std::max((cells + 255) / 256, 1), 256, 0, s>>>(T, M, out, cells, z);
+  launch_pdl(cell_records32_kernel, std::max((cells + 255) / 256, 1), 256, 0, s, T, M, out, cells, z);
 }
 template <typename R>
 void launch_append_children(const ChildSetT<R> &set, unsigned int *next_uid, const DevParticlesT<R> &dst,
                             const unsigned int *n, int capacity, unsigned int *appended, unsigned int *overflow,
                             int grid, cudaStream_t s) {
-  append_children_kernel<R><<<grid, 256, 0, s>>>(set, next_uid, dst, n, capacity, appended, overflow);
+  launch_pdl(append_children_kernel<R>, grid, 256, 0, s, set, next_uid, dst, n, capacity, appended, overflow);
 }
 __global__ void step_reset_kernel(StepCounters z) { reset_step_counters(z, threadIdx.x); }
 void launch_step_reset(const StepCounters &z, cudaStream_t s) { step_reset_kernel<<<1, 32, 0, s>>>(z); }
@@ -765,8 +773,8 @@ void launch_cell_sort(const DevParticlesT<R> &src, DevCount n, const DevParticle
   if (finish.n != nullptr) {
     // the step's sort: the tile sums scanned by scan_tiles' last block, the
     // tile prefixes added by the scatter, the step ended by its last block
-    scan_tiles<<<tiles, 1024, 0, s>>>(hist, offsets, tile_sums, buckets, finish.scan_blocks, total);
-    cell_scatter<R><<<grid, 256, 0, s>>>(src, n, dst, offsets, nx, nz, shift, bounds, finish, tile_sums);
+    launch_pdl(scan_tiles, tiles, 1024, 0, s, hist, offsets, tile_sums, buckets, finish.scan_blocks, total);
+    launch_pdl(cell_scatter<R>, grid, 256, 0, s, src, n, dst, offsets, nx, nz, shift, bounds, finish, tile_sums);
     return;
   }
   scan_tiles<<<tiles, 1024, 0, s>>>(hist, offsets, tile_sums, buckets, nullptr, nullptr);
