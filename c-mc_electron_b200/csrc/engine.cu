@@ -759,6 +759,7 @@ int mcb200_set_mesh(mcb200_ctx *c, int nx, int ny, int nz, const double *lx, con
     c->stat_open = false;
     m.cell32 = c->cell32;
     c->hist = dalloc<unsigned int>(cells, c->mesh_owned);
+    ck(cudaMemsetAsync(c->hist, 0, sizeof(unsigned int) * cells, c->stream), "memset");  // zero between sorts
     c->offsets = dalloc<unsigned int>(cells, c->mesh_owned);
     c->tile_sums = dalloc<unsigned int>((cells + 1023) / 1024 + 1, c->mesh_owned);
     ck(cudaStreamSynchronize(c->stream), "sync");
@@ -1559,6 +1560,7 @@ int mcb200_multiple_refresh(mcb200_ctx *c, const int32_t *desired_e, const int32
     if (c->precision == MCB200_FLIGHT_FP32) refresh(float{});
     else refresh(double{});
     ck(cudaEventRecord(c->ev_mr_used, s), "event");  // the targets are read
+    ck(cudaMemsetAsync(c->hist, 0, sizeof(unsigned int) * cells, s), "memset");  // the step's sort expects zeros
     // the refreshed population's size and the uid counter, on the device
     refresh_counts_kernel<<<1, 32, 0, s>>>(c->dev_counts, tot);
     ck(cudaGetLastError(), "refresh");
@@ -1955,7 +1957,6 @@ void step_prepare(mcb200_ctx *c) {
                            c->ts->dt, c->ib, grid_for(c, c->capacity, 256), s);
     c->launches += 2;
   }
-  join_stat(c);  // the flights change the store the statistics read
   StepCounters z{c->tickets, {}, c->append_count};
   for (int g = 0; g < mcb200_ctx::kGenerations; ++g) z.count[g] = children<R>(c, g).count;
   z.count[mcb200_ctx::kGenerations] = c->sink_count;
@@ -1964,6 +1965,7 @@ void step_prepare(mcb200_ctx *c) {
   else
     launch_step_reset(z, s);
   c->launches += 1;
+  join_stat(c);  // the flights change the store the statistics read (the records and counters do not)
 }
 
 // After the flights of a step: uids for the surviving copies, which join the

@@ -62,7 +62,9 @@ void launch_records_and_reset(const DevTables &T, const DevMesh &M, float4 *out,
 // none): *particle_steps += *n; *n = *sorted_total; *next_uid += *appended.
 // blocks, scan_blocks: counters that are zero between launches.  A sort
 // with a StepFinish leaves `offsets` as tile-local cell ends (nothing reads
-// them after the step's sort).
+// them after the step's sort) and `hist` zero, and expects it zero (the
+// refresh's sort, without one, zeroes it first and the refresh zeroes it
+// again when done).
 struct StepFinish {
   unsigned int *n = nullptr;
   const unsigned int *sorted_total = nullptr;
