@@ -374,8 +374,16 @@ __global__ void cell_histogram(const uint32_t *cell, const uint32_t *meta, DevCo
   pdl_wait();
   const int n = count.get();
   if (bounds && blockIdx.x == 0 && threadIdx.x < 4) bounds[threadIdx.x] = 0ull;
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
-    if (!(meta[p] & kMetaDead)) atomicAdd(&hist[cell_linear(cell[p], nx, nz) >> shift], 1u);
+  // a warp walks 32 consecutive particles; lanes of the same bucket (a
+  // cell-sorted store holds runs of them) add their count with one atomic
+  const unsigned lane = threadIdx.x & 31u;
+  for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += gridDim.x * blockDim.x) {
+    const int p = base + (int)lane;
+    unsigned int key = 0xffffffffu;
+    if (p < n && !(meta[p] & kMetaDead)) key = (unsigned int)(cell_linear(cell[p], nx, nz) >> shift);
+    const unsigned int peers = __match_any_sync(0xffffffffu, key);
+    if (key != 0xffffffffu && (int)lane == __ffs(peers) - 1) atomicAdd(&hist[key], (unsigned int)__popc(peers));
+  }
 }
 
 // Exclusive scan of `count` values, single pass per 1024-wide tile plus a
@@ -406,14 +414,16 @@ __device__ void scan_tile_sums_block(unsigned int *tile_sums, int ntiles, unsign
 // Exclusive scan of each 1024-wide tile, and its sum into tile_sums.  With
 // `blocks` (a counter that is zero between launches) the last block to
 // finish then scans the tile sums too (scan_tile_sums' work, one launch
-// fewer).
+// fewer).  clear (or null): the input, zeroed once read (the step's sort
+// keeps its histogram zero between sorts, so no memset precedes it).
 __global__ void scan_tiles(const unsigned int *in, unsigned int *out, unsigned int *tile_sums, int n,
-                           unsigned int *blocks, unsigned int *total) {
+                           unsigned int *blocks, unsigned int *total, unsigned int *clear) {
   __shared__ unsigned int s[1024];
   __shared__ bool last;
   pdl_wait();
   const int i = blockIdx.x * 1024 + threadIdx.x;
   const unsigned int v = i < n ? in[i] : 0u;
+  if (clear && i < n) clear[i] = 0u;
   s[threadIdx.x] = v;
   __syncthreads();
   for (int off = 1; off < 1024; off <<= 1) {
@@ -459,11 +469,21 @@ __global__ void __launch_bounds__(256) cell_scatter(DevParticlesT<R> src, DevCou
   pdl_wait();
   const int n = count.get();
   unsigned long long mx[2] = {0, 0}, cnt[2] = {0, 0};
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
-    const uint32_t m = src.meta[p];
-    if (m & kMetaDead) continue;
-    const int key = cell_linear(src.cell[p], nx, nz) >> shift;
-    const unsigned int q = atomicAdd(&cursor[key], 1u) + (tile_base ? tile_base[key >> 10] : 0u);
+  // lanes of the same bucket take consecutive slots with one atomic
+  const unsigned lane = threadIdx.x & 31u;
+  for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += gridDim.x * blockDim.x) {
+    const int p = base + (int)lane;
+    const uint32_t m = p < n ? src.meta[p] : kMetaDead;
+    const bool live = !(m & kMetaDead);
+    const unsigned int key = live ? (unsigned int)(cell_linear(src.cell[p], nx, nz) >> shift) : 0xffffffffu;
+    const unsigned int peers = __match_any_sync(0xffffffffu, key);
+    const int leader = __ffs(peers) - 1;
+    unsigned int first = 0;
+    if (live && (int)lane == leader) first = atomicAdd(&cursor[key], (unsigned int)__popc(peers));
+    first = __shfl_sync(0xffffffffu, first, leader);
+    if (!live) continue;
+    const unsigned int q = first + (unsigned int)__popc(peers & ((1u << lane) - 1u)) +
+                           (tile_base ? tile_base[key >> 10] : 0u);
     const double charge = src.charge[p];
     dst.x[q] = src.x[p]; dst.y[q] = src.y[p]; dst.z[q] = src.z[p];
     dst.kx[q] = src.kx[p]; dst.ky[q] = src.ky[p]; dst.kz[q] = src.kz[p];
@@ -758,7 +778,7 @@ void launch_step_reset(const StepCounters &z, cudaStream_t s) { step_reset_kerne
 void launch_exclusive_scan(const unsigned int *in, unsigned int *out, unsigned int *tile_sums, unsigned int *total,
                            int n, cudaStream_t s) {
   const int tiles = (n + 1023) / 1024;
-  scan_tiles<<<tiles, 1024, 0, s>>>(in, out, tile_sums, n, nullptr, nullptr);
+  scan_tiles<<<tiles, 1024, 0, s>>>(in, out, tile_sums, n, nullptr, nullptr, nullptr);
   scan_tile_sums<<<1, 1024, 0, s>>>(tile_sums, tiles, total);
   scan_add<<<tiles, 1024, 0, s>>>(out, tile_sums, n);
 }
@@ -767,17 +787,21 @@ void launch_cell_sort(const DevParticlesT<R> &src, DevCount n, const DevParticle
                       int nz, unsigned int *hist, unsigned int *offsets, unsigned int *tile_sums, unsigned int *total,
                       int shift, unsigned long long *bounds, int grid, cudaStream_t s, const StepFinish &finish) {
   const int buckets = (ncells + (1 << shift) - 1) >> shift;
-  cudaMemsetAsync(hist, 0, sizeof(unsigned int) * buckets, s);
-  cell_histogram<<<grid, 256, 0, s>>>(src.cell, src.meta, n, nx, nz, hist, shift, bounds);
   const int tiles = (buckets + 1023) / 1024;
   if (finish.n != nullptr) {
-    // the step's sort: the tile sums scanned by scan_tiles' last block, the
-    // tile prefixes added by the scatter, the step ended by its last block
-    launch_pdl(scan_tiles, tiles, 1024, 0, s, hist, offsets, tile_sums, buckets, finish.scan_blocks, total);
+    // the step's sort: the histogram starts from the zeros the last one
+    // left, the tile sums are scanned by scan_tiles' last block (which also
+    // clears the histogram), the tile prefixes added by the scatter, the
+    // step ended by its last block
+    launch_pdl(cell_histogram, grid, 256, 0, s, src.cell, src.meta, n, nx, nz, hist, shift, bounds);
+    launch_pdl(scan_tiles, tiles, 1024, 0, s, (const unsigned int *)hist, offsets, tile_sums, buckets,
+               finish.scan_blocks, total, hist);
     launch_pdl(cell_scatter<R>, grid, 256, 0, s, src, n, dst, offsets, nx, nz, shift, bounds, finish, tile_sums);
     return;
   }
-  scan_tiles<<<tiles, 1024, 0, s>>>(hist, offsets, tile_sums, buckets, nullptr, nullptr);
+  cudaMemsetAsync(hist, 0, sizeof(unsigned int) * buckets, s);
+  cell_histogram<<<grid, 256, 0, s>>>(src.cell, src.meta, n, nx, nz, hist, shift, bounds);
+  scan_tiles<<<tiles, 1024, 0, s>>>(hist, offsets, tile_sums, buckets, nullptr, nullptr, nullptr);
   scan_tile_sums<<<1, 1024, 0, s>>>(tile_sums, tiles, total);
   scan_add<<<tiles, 1024, 0, s>>>(offsets, tile_sums, buckets);
   cell_scatter<R><<<grid, 256, 0, s>>>(src, n, dst, offsets, nx, nz, shift, bounds, finish, nullptr);
