@@ -370,7 +370,9 @@ def serve_arm(args, device: int) -> dict:
     (seed 5); FP32 flight, HBM budget 160 GB, one Ids window per 50-step
     round (net flux through the middle third of the section planes), each
     request done when stderr(Ids) < 1% of |Ids| after 6 transient windows
-    (2 after a warm start) or at the step cap (2000 by default).  Latency = completion - arrival
+    (2 after a warm start) or at the step cap (2000 by default); a request
+    warm-starts from the nearest converged bias of its Lg, failing that from
+    the nearest running request of its Lg past its transient.  Latency = completion - arrival
     (server clock); throughput = particle-steps over the rounds' device time."""
     import mcb200
     from mcb200 import serving
@@ -381,7 +383,8 @@ def serve_arm(args, device: int) -> dict:
         with ClockSampler(device) as clocks:
             res, st, wall = serving.serve(srv, reqs, max_wall_s=900, max_steps=args.serve_max_steps, min_windows=5,
                                           warm_windows_cold=6, warm_windows_warm=2, poisson_every=10,
-                                          target_rel_err=0.01, ids_estimator=mcb200.IDS_SECTIONS)
+                                          target_rel_err=0.01, ids_estimator=mcb200.IDS_SECTIONS,
+                                          warm_start=mcb200.WARM_SETTLED)
         srv.close()
     lat = serving.latency_summary(res)
     status = [r["status"] for r in res]
@@ -400,7 +403,8 @@ def serve_arm(args, device: int) -> dict:
             "per_request_fields": ["lg_nm", "vg", "vd", "particles", "steps", "rel_stderr", "status", "latency_s"],
             "clocks": clocks.summary(),
             "config": "32 FinFET bias points, Poisson arrivals 4 req/s, 50k-1M particles, 160 GB budget, "
-                      f"target 1% Ids stderr, {args.serve_max_steps}-step cap, 50-step rounds, FP32 flight"}
+                      f"target 1% Ids stderr, {args.serve_max_steps}-step cap, 50-step rounds, FP32 flight, "
+                      "warm starts from converged or settled requests of the same Lg"}
 
 
 # ------------------------------------------------------------ reference (CPU)

@@ -200,8 +200,11 @@ int admit(mcb200_server *v, Slot &s) {
     start += (size_t)en[c] + hn[c];
     target += (size_t)s.refresh_e[c] + s.refresh_h[c];
   }
-  // a warm start: the nearest converged bias of the family
+  // a warm start: the nearest converged bias of the family; with
+  // MCB200_WARM_SETTLED, failing that, the nearest running request of the
+  // family past its transient (its ensemble as the last round left it)
   WarmEntry *from = nullptr;
+  const Slot *from_slot = nullptr;
   if (s.req.warm_start) {
     double best = INFINITY;
     for (auto &w : v->cache) {
@@ -213,8 +216,20 @@ int admit(mcb200_server *v, Slot &s) {
       }
     }
   }
+  if (!from && s.req.warm_start == MCB200_WARM_SETTLED) {
+    double best = INFINITY;
+    for (const auto &a : v->active) {
+      if (a->family != s.family || a->warm > 0 || a->windows.empty()) continue;
+      const double d = std::hypot(a->req.bias[0] - s.req.bias[0], a->req.bias[1] - s.req.bias[1]);
+      if (d < best) {
+        best = d;
+        from_slot = a.get();
+      }
+    }
+  }
+  mcb200_ctx *donor = from ? from->ctx : (from_slot ? from_slot->ctx : nullptr);
   size_t from_n = 0;
-  if (from) from_n = mcb200_num_particles(from->ctx);
+  if (donor) from_n = mcb200_num_particles(donor);
   const size_t big = std::max(std::max(start, target), from_n);
   const size_t capacity = big + big / 4 + 65536;
   const size_t before = free_bytes(v->opt.device);
@@ -243,13 +258,17 @@ int admit(mcb200_server *v, Slot &s) {
   // the refresh targets go to the device now, not at the first refresh inside a running batch
   if (int rc = mcb200_set_refresh_targets(s.ctx, s.refresh_e.data(), s.refresh_h.data()))
     return ctx_err(rc, "mcb200_set_refresh_targets");
-  if (from) {
-    if (int rc = mcb200_copy_ensemble(s.ctx, from->ctx)) return ctx_err(rc, "mcb200_copy_ensemble");
+  if (donor) {
+    if (int rc = mcb200_copy_ensemble(s.ctx, donor)) return ctx_err(rc, "mcb200_copy_ensemble");
     // to this deck's carrier targets, as a refresh would
     if (int rc = mcb200_multiple_refresh(s.ctx, s.refresh_e.data(), s.refresh_h.data(), 0, s.req.seed, nullptr))
       return ctx_err(rc, "warm-start refresh");
-    from->last_use = ++v->use_counter;
-    s.warm_from = from->request;
+    if (from) {
+      from->last_use = ++v->use_counter;
+      s.warm_from = from->request;
+    } else {
+      s.warm_from = from_slot->id;
+    }
     s.warm = s.req.warm_windows_warm;
   } else {
     if (int rc = mcb200_seed_deck(s.ctx, deck, s.req.seed)) return deck_err(rc, "mcb200_seed_deck");
@@ -365,6 +384,7 @@ double mcb200_server_now(const mcb200_server *v) { return v ? v->now() : 0.0; }
 
 int mcb200_server_submit(mcb200_server *v, const mcb200_request *req, uint64_t *id) {
   if (!v || !req || !req->input_path || !req->family) return MCB200_ERR_ARG;
+  if (req->warm_start < MCB200_WARM_OFF || req->warm_start > MCB200_WARM_SETTLED) return MCB200_ERR_ARG;
   auto s = std::make_unique<Slot>();
   s->id = v->next_id++;
   s->req = *req;

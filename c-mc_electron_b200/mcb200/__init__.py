@@ -30,6 +30,7 @@ FLAG_SURFACE_IMPURITY = 2
 FLAG_HEAT = 4
 FLAG_QUANTUM = 8
 IDS_CONTACT, IDS_SECTIONS, IDS_INDUCED = 0, 1, 2  # serving's Ids estimators (MCB200_IDS_*)
+WARM_OFF, WARM_CONVERGED, WARM_SETTLED = 0, 1, 2  # serving's warm-start donors (MCB200_WARM_*)
 FLIGHT_FP64 = 0
 FLIGHT_FP32 = 1
 # Poisson preconditioners (mcb200_set_poisson_solver)
@@ -748,7 +749,7 @@ class Server:
 
     def submit(self, input_path: str, family: str, bias, seed: int, target_rel_err: float = 0.01,
                min_windows: int = 5, max_steps: int = 0, warm_windows_cold: int = 10, warm_windows_warm: int = 1,
-               warm_start: bool = True, poisson_every: int = 0, drain_contact: int = 1, ids_estimator: int = 0,
+               warm_start: int = WARM_CONVERGED, poisson_every: int = 0, drain_contact: int = 1, ids_estimator: int = 0,
                arrival_s=None) -> int:
         req = Request(os.fspath(input_path).encode(), family.encode(), (ctypes.c_double * 2)(*bias), target_rel_err,
                       min_windows, max_steps, warm_windows_cold, warm_windows_warm, int(warm_start), poisson_every,

@@ -702,7 +702,10 @@ typedef struct {
   int max_steps;             /* complete at this many steps regardless (0: no limit) */
   int warm_windows_cold;     /* windows discarded as transient after a cold start */
   int warm_windows_warm;     /* ... after a warm start */
-  int warm_start;            /* start from the nearest converged bias of the family, and keep this one */
+  int warm_start;            /* MCB200_WARM_*: start from the nearest converged bias of the family (and
+                                keep this one when it converges); MCB200_WARM_SETTLED: failing a
+                                converged one, from the nearest running request of the family that is
+                                past its transient windows */
   int poisson_every;         /* 0: the deck's poisson_step */
   int drain_contact;         /* 0-based contact whose current is Ids */
   int ids_estimator;         /* MCB200_IDS_*: how a window's Ids is measured */
@@ -714,6 +717,9 @@ typedef struct {
  * third of the y planes (its section currents), or the current the drain
  * carries by induction (Ramo-Shockley, mcb200_set_induced_current): all
  * estimate the same steady-state current, with decreasing noise per window. */
+#define MCB200_WARM_OFF 0
+#define MCB200_WARM_CONVERGED 1
+#define MCB200_WARM_SETTLED 2
 #define MCB200_IDS_CONTACT 0
 #define MCB200_IDS_SECTIONS 1
 #define MCB200_IDS_INDUCED 2

@@ -88,6 +88,32 @@ def test_warm_start_from_nearest_bias():
         s.close()
 
 
+def test_warm_start_from_a_settled_running_request():
+    """MCB200_WARM_SETTLED: with no converged bias of the family cached, a
+    request starts from the nearest running request of its family that is
+    past its transient windows; MCB200_WARM_CONVERGED waits for a converged
+    one (and starts cold here), another family never donates."""
+    with tempfile.TemporaryDirectory() as tmp:
+        kw = dict(COLD, max_steps=30)
+        s = mcb200.Server(quantum_steps=10)
+        ida = s.submit(deck(tmp, "a", 0.4), "lg15", (0.4, 0.7), seed=1, **kw)
+        s.round()  # a has one window: past its (empty) transient
+        idb = s.submit(deck(tmp, "b", 0.45), "lg15", (0.45, 0.7), seed=2, **dict(kw, warm_start=mcb200.WARM_SETTLED))
+        idc = s.submit(deck(tmp, "c", 0.5), "lg15", (0.5, 0.7), seed=3, **dict(kw, warm_start=mcb200.WARM_CONVERGED))
+        far = s.submit(deck(tmp, "far", 0.8, lg=20.0), "lg20", (0.8, 0.7), seed=4,
+                       **dict(kw, warm_start=mcb200.WARM_SETTLED))
+        with pytest.raises(mcb200.EngineError):
+            s.submit(deck(tmp, "bad", 0.4), "lg15", (0.4, 0.7), seed=5, **dict(kw, warm_start=3))
+        res = drive(s)
+        s.close()
+    assert by_id(res, ida)["warm_from"] == 0
+    assert by_id(res, idb)["warm_from"] == ida
+    assert by_id(res, idc)["warm_from"] == 0
+    assert by_id(res, far)["warm_from"] == 0
+    assert all(r["status"] == mcb200.SERVE_STEP_LIMIT and r["steps"] == 30 for r in res)
+    assert by_id(res, idb)["particles"] > 0 and by_id(res, idb)["ids"] != 0.0
+
+
 def test_budget_queues_the_second_request():
     with tempfile.TemporaryDirectory() as tmp:
         a, a2 = deck(tmp, "a", 0.4), deck(tmp, "a2", 0.5)
