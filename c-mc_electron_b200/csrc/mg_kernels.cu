@@ -49,38 +49,70 @@ __device__ __forceinline__ void trace(int) {}
 
 // (A x)[n] with the 7-point stencil of the CG (-x, +x, -y, +y, -z, +z,
 // diagonal).  x is zero on Dirichlet nodes and isolated nodes have no
-// couplings, so no neighbour needs masking.
+// couplings, so no neighbour needs masking.  A coefficient towards a
+// neighbour off the grid is zero (the finite-volume assembly adds only
+// in-grid couplings), so an off-grid neighbour's index is clamped to the
+// node itself: every load is unconditional and independent, and the exact
+// zero products leave the sum as the branchy form would make it.
 __device__ __forceinline__ double apply7(const double *st7, const Grid3 &g, const double *x, int n) {
   int i, j, k;
   node_ijk(n, g, i, j, k);
   const double *a = st7 + (size_t)n * 7;
+  const int sx = g.pz, sy = g.px * g.pz;
   double acc = a[6] * x[n];
-  if (i > 0) acc += a[0] * x[n - g.pz];
-  if (i + 1 < g.px) acc += a[1] * x[n + g.pz];
-  if (j > 0) acc += a[2] * x[n - g.px * g.pz];
-  if (j + 1 < g.py) acc += a[3] * x[n + g.px * g.pz];
-  if (k > 0) acc += a[4] * x[n - 1];
-  if (k + 1 < g.pz) acc += a[5] * x[n + 1];
+  acc += a[0] * x[i > 0 ? n - sx : n];
+  acc += a[1] * x[i + 1 < g.px ? n + sx : n];
+  acc += a[2] * x[j > 0 ? n - sy : n];
+  acc += a[3] * x[j + 1 < g.py ? n + sy : n];
+  acc += a[4] * x[k > 0 ? n - 1 : n];
+  acc += a[5] * x[k + 1 < g.pz ? n + 1 : n];
   return acc;
 }
 
-// (A x)[n] with a level's 27-point Galerkin stencil, entry ((di+1)*3 + (dj+1))*3 + (dk+1).
-__device__ __forceinline__ double apply27(const MgDevLevel &L, const double *x, int n) {
+// Lanes that share one node of a level of n nodes, with `stride` threads on
+// the level: 8, 4 or 2 where every group still gets a node, else 1.  The
+// coarse levels have far fewer nodes than the grid has threads; splitting
+// a node's 27 couplings over a group puts more independent loads in flight
+// per node and shortens the pass, which is latency-bound.
+__device__ __forceinline__ int lanes_per_node(int n, int stride) {
+  return n * 8 <= stride ? 8 : n * 4 <= stride ? 4 : n * 2 <= stride ? 2 : 1;
+}
+
+// Sum over an aligned group of G lanes of a warp; every lane of the group
+// gets the same bits (a butterfly adds the same two operands on both sides).
+template <int G>
+__device__ __forceinline__ double group_sum(double v) {
+  if constexpr (G > 1) {
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned mask = ((1u << G) - 1u) << (lane & ~(unsigned)(G - 1));
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+  }
+  return v;
+}
+
+// Lane g's share of (A x)[n] with a level's 27-point Galerkin stencil,
+// entry ((di+1)*3 + (dj+1))*3 + (dk+1): the (di, dj) rows g, g + G, ...
+// (all nine, in order, for G = 1).  Off-grid couplings are zero (the
+// Galerkin product couples existing coarse nodes only), so off-grid
+// indices are clamped as in apply7.
+template <int G>
+__device__ __forceinline__ double apply27_part(const MgDevLevel &L, const double *x, int n, int g) {
   int i, j, k;
   node_ijk(n, Grid3{L.px, L.py, L.pz}, i, j, k);
   const double *a = L.st + (size_t)n * 27;
+  const int km = k > 0 ? -1 : 0, kp = k + 1 < L.pz ? 1 : 0;
   double acc = 0.0;
-  for (int di = -1; di <= 1; ++di) {
-    const int i2 = i + di;
-    if (i2 < 0 || i2 >= L.px) continue;
-    for (int dj = -1; dj <= 1; ++dj) {
-      const int j2 = j + dj;
-      if (j2 < 0 || j2 >= L.py) continue;
-      const double *ar = a + ((di + 1) * 3 + (dj + 1)) * 3;
+#pragma unroll
+  for (int t = 0; t < (9 + G - 1) / G; ++t) {
+    const int row = g + t * G;
+    if (row < 9) {
+      const int i2 = min(max(i + row / 3 - 1, 0), L.px - 1), j2 = min(max(j + row % 3 - 1, 0), L.py - 1);
+      const double *ar = a + row * 3;
       const int base = (j2 * L.px + i2) * L.pz + k;
-      if (k > 0) acc += ar[0] * x[base - 1];
+      acc += ar[0] * x[base + km];
       acc += ar[1] * x[base];
-      if (k + 1 < L.pz) acc += ar[2] * x[base + 1];
+      acc += ar[2] * x[base + kp];
     }
   }
   return acc;
@@ -95,10 +127,6 @@ struct Solve {
 
   __device__ double *X(int l) const { return (cur >> l) & 1u ? mg.L[l].xb : mg.L[l].xa; }
   __device__ double *Xo(int l) const { return (cur >> l) & 1u ? mg.L[l].xa : mg.L[l].xb; }
-  __device__ double A(int l, const double *x, int n) const {
-    return l == 0 ? apply7(st7, g0, x, n) : apply27(mg.L[l], x, n);
-  }
-
   // First sweep from a zero iterate: x = omega D^-1 b (level 0's isolated
   // rows: D^-1 b), for node n.
   __device__ void first(int l, int n, double b) const {
@@ -106,67 +134,102 @@ struct Solve {
     X(l)[n] = L.dir[n] ? (l == 0 ? L.dinv[n] * b : 0.0) : L.omega * L.dinv[n] * b;
   }
   // One damped-Jacobi sweep into the other buffer; returns sum b.x_new of
-  // this thread's nodes when `dot`.
-  __device__ double sweep(int l, bool dot) {
+  // this thread's nodes when `dot`.  Level 0 one node a thread (7-point);
+  // a coarser level G lanes a node (lanes_per_node), lane 0 writing.
+  template <int G>
+  __device__ double sweep_level(int l, bool dot) const {
     const MgDevLevel &L = mg.L[l];
     const double *xc = X(l), *b = L.b;
     double *xn = Xo(l);
+    const int g = tid % G;
     double acc = 0.0;
-    for (int n = tid; n < L.n; n += stride) {
-      const double bn = b[n], dn = L.dinv[n], ax = A(l, xc, n), xn0 = xc[n];
+    for (int n = tid / G; n < L.n; n += stride / G) {
+      const double ax = l == 0 ? apply7(st7, g0, xc, n) : group_sum<G>(apply27_part<G>(L, xc, n, g));
+      if (g != 0) continue;
+      const double bn = b[n], dn = L.dinv[n], xn0 = xc[n];
       double v = xn0 + L.omega * dn * (bn - ax);
       if (L.dir[n]) v = l == 0 ? dn * bn : 0.0;
       xn[n] = v;
       if (dot) acc += bn * v;
     }
+    return acc;
+  }
+  __device__ double sweep(int l, bool dot) {
+    const int G = l == 0 ? 1 : lanes_per_node(mg.L[l].n, stride);
+    const double acc = G == 8   ? sweep_level<8>(l, dot)
+                       : G == 4 ? sweep_level<4>(l, dot)
+                       : G == 2 ? sweep_level<2>(l, dot)
+                                : sweep_level<1>(l, dot);
     cur ^= 1u << l;
     return acc;
   }
-  __device__ void residual(int l) const {
+  template <int G>
+  __device__ void residual_level(int l) const {
     const MgDevLevel &L = mg.L[l];
     const double *x = X(l);
-    for (int n = tid; n < L.n; n += stride) {
-      const double v = L.b[n] - A(l, x, n);
+    const int g = tid % G;
+    for (int n = tid / G; n < L.n; n += stride / G) {
+      const double ax = l == 0 ? apply7(st7, g0, x, n) : group_sum<G>(apply27_part<G>(L, x, n, g));
+      if (g != 0) continue;
+      const double v = L.b[n] - ax;
       L.r[n] = L.dir[n] ? 0.0 : v;
     }
+  }
+  __device__ void residual(int l) const {
+    const int G = l == 0 ? 1 : lanes_per_node(mg.L[l].n, stride);
+    if (G == 8) residual_level<8>(l);
+    else if (G == 4) residual_level<4>(l);
+    else if (G == 2) residual_level<2>(l);
+    else residual_level<1>(l);
   }
   // b_{l+1} = P^T r_l, and the first sweep of level l+1 unless it is the
   // coarsest.  The 27 taps of a coarse node are the products of its three
   // per-axis tap triples; off-grid taps have weight 0 and a clamped index,
-  // so every load is independent of the others.
-  __device__ void restrict_to(int l) const {
+  // so every load is independent of the others.  G lanes a coarse node
+  // (lanes_per_node), each the (x, y) tap rows g, g + G, ... of the nine.
+  template <int G>
+  __device__ void restrict_level(int l) const {
     const MgDevLevel &F = mg.L[l], &C = mg.L[l + 1];
     const bool smooth = l + 2 < mg.levels;
     const Grid3 gc{C.px, C.py, C.pz};
-    for (int c = tid; c < C.n; c += stride) {
+    const int g = tid % G;
+    for (int c = tid / G; c < C.n; c += stride / G) {
       int ci, cj, ck;
       node_ijk(c, gc, ci, cj, ck);
       const int fi = F.keep[0][ci], fj = F.keep[1][cj], fk = F.keep[2][ck];
-      double wx[3], wy[3], wz[3];
-      int ix[3], jy[3], kz[3];
+      double wz[3];
+      int kz[3];
 #pragma unroll
       for (int t = 0; t < 3; ++t) {
-        wx[t] = F.rtap[0][3 * ci + t];
-        wy[t] = F.rtap[1][3 * cj + t];
         wz[t] = F.rtap[2][3 * ck + t];
-        ix[t] = min(max(fi - 1 + t, 0), F.px - 1);
-        jy[t] = min(max(fj - 1 + t, 0), F.py - 1);
         kz[t] = min(max(fk - 1 + t, 0), F.pz - 1);
       }
       double acc = 0.0;
 #pragma unroll
-      for (int b = 0; b < 3; ++b)
+      for (int t = 0; t < (9 + G - 1) / G; ++t) {
+        const int row = g + t * G;
+        if (row < 9) {
+          const int b = row / 3, a = row % 3;
+          const double wab = F.rtap[0][3 * ci + a] * F.rtap[1][3 * cj + b];
+          const int ix = min(max(fi - 1 + a, 0), F.px - 1), jy = min(max(fj - 1 + b, 0), F.py - 1);
+          const double *frow = F.r + (jy * F.px + ix) * F.pz;
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          const double wab = wx[a] * wy[b];
-          const double *row = F.r + (jy[b] * F.px + ix[a]) * F.pz;
-#pragma unroll
-          for (int d = 0; d < 3; ++d) acc += wab * wz[d] * row[kz[d]];
+          for (int d = 0; d < 3; ++d) acc += wab * wz[d] * frow[kz[d]];
         }
+      }
+      acc = group_sum<G>(acc);
+      if (g != 0) continue;
       if (C.dir[c]) acc = 0.0;
       C.b[c] = acc;
       if (smooth) first(l + 1, c, acc);
     }
+  }
+  __device__ void restrict_to(int l) const {
+    const int G = lanes_per_node(mg.L[l + 1].n, stride);
+    if (G == 8) restrict_level<8>(l);
+    else if (G == 4) restrict_level<4>(l);
+    else if (G == 2) restrict_level<2>(l);
+    else restrict_level<1>(l);
   }
   // x_l += P x_{l+1} on the free rows.
   __device__ void prolong(int l) const {
