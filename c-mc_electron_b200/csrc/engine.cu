@@ -1282,6 +1282,7 @@ int mcb200_set_device(mcb200_ctx *c, const int32_t *material, const double *dono
     f.cg_z = dalloc<double>(nodes, c->mesh_owned);
     f.cg_p = dalloc<double>(nodes, c->mesh_owned);
     f.cg_p1 = dalloc<double>(nodes, c->mesh_owned);
+    f.cg_r1 = dalloc<double>(nodes, c->mesh_owned);
     f.cg_q = dalloc<double>(nodes, c->mesh_owned);
     f.cg_part = dalloc<double>(3 * kCgMaxGrid, c->mesh_owned);  // the persistent CG's partial sums
     f.cg_scalars = dalloc<double>(16, c->mesh_owned);  // the CG scalars sc[0..9]

@@ -516,7 +516,7 @@ MgSystem cg_mg_system(const DevMesh &M, const FieldBuffers &f, int max_iter) {
   y.mg.L[0].xa = f.cg_z;
   y.st7 = f.stencil;
   y.dirichlet = f.dirichlet;
-  y.x = f.potential; y.r = f.cg_r; y.p0 = f.cg_p; y.p1 = f.cg_p1; y.q = f.cg_q; y.part = f.cg_part;
+  y.x = f.potential; y.r = f.cg_r; y.r1 = f.cg_r1; y.p0 = f.cg_p; y.p1 = f.cg_p1; y.q = f.cg_q; y.part = f.cg_part;
   y.sc = f.cg_scalars;
   y.px = M.nx + 1; y.py = M.ny + 1; y.pz = M.nz + 1;
   y.max_iter = max_iter;
@@ -529,7 +529,8 @@ int cg_launch(const DevMesh &M, const FieldBuffers &f, int max_iter, cudaStream_
   double *x = f.potential, *r = f.cg_r, *z = f.cg_z, *p0 = f.cg_p, *p1 = f.cg_p1, *q = f.cg_q, *part = f.cg_part;
   double *sc = f.cg_scalars;
   if (plan.used == kCgMultigrid) {
-    if (launch_cg_mg(nodes, g, f.stencil, f.dirichlet, x, r, z, p0, p1, q, part, sc, max_iter, *f.mg, plan.grid, s) !=
+    if (launch_cg_mg(nodes, g, f.stencil, f.dirichlet, x, r, f.cg_r1, z, p0, p1, q, part, sc, max_iter, *f.mg,
+                     plan.grid, s) !=
         cudaSuccess)
       return 1;
   } else {

@@ -28,7 +28,7 @@ struct FieldBuffers {
   double *density = nullptr;                    // p_par_charge (charge / node volume)
   // Poisson
   double *rhs = nullptr, *potential = nullptr;
-  double *cg_r = nullptr, *cg_z = nullptr, *cg_p = nullptr, *cg_p1 = nullptr, *cg_q = nullptr, *cg_part = nullptr,
+  double *cg_r = nullptr, *cg_r1 = nullptr, *cg_z = nullptr, *cg_p = nullptr, *cg_p1 = nullptr, *cg_q = nullptr, *cg_part = nullptr,
          *cg_scalars = nullptr;
   unsigned long long *abs_sum = nullptr;  // [4] charge bounds of the store (the context's, kept by its writers)
   const MgDevice *mg = nullptr;  // multigrid hierarchy of the stencil (null: Jacobi preconditioning only)

@@ -123,7 +123,8 @@ struct Solve {
   const double *st7;
   Grid3 g0;
   int tid, stride;
-  unsigned cur;  // bit l: level l's iterate is in xb (else xa)
+  unsigned cur;      // bit l: level l's iterate is in xb (else xa)
+  const double *b0;  // level 0's right side: the CG residual buffer of this iteration
 
   __device__ double *X(int l) const { return (cur >> l) & 1u ? mg.L[l].xb : mg.L[l].xa; }
   __device__ double *Xo(int l) const { return (cur >> l) & 1u ? mg.L[l].xa : mg.L[l].xb; }
@@ -139,7 +140,7 @@ struct Solve {
   template <int G>
   __device__ double sweep_level(int l, bool dot) const {
     const MgDevLevel &L = mg.L[l];
-    const double *xc = X(l), *b = L.b;
+    const double *xc = X(l), *b = l == 0 ? b0 : L.b;
     double *xn = Xo(l);
     const int g = tid % G;
     double acc = 0.0;
@@ -171,7 +172,7 @@ struct Solve {
     for (int n = tid / G; n < L.n; n += stride / G) {
       const double ax = l == 0 ? apply7(st7, g0, x, n) : group_sum<G>(apply27_part<G>(L, x, n, g));
       if (g != 0) continue;
-      const double v = L.b[n] - ax;
+      const double v = (l == 0 ? b0 : L.b)[n] - ax;
       L.r[n] = L.dir[n] ? 0.0 : v;
     }
   }
@@ -287,11 +288,13 @@ struct Solve {
     return acc;
   }
 
-  // z = M r.  On entry level 0's first sweep is in X(0) (levels > 1); on
-  // exit X(0) holds z, part_rz the block partials of r.z (block vb of the
-  // solve), and the grid has synchronised.  Without `work` only the grid
-  // barriers are taken (a block of a finished solve sharing the launch).
-  __device__ void vcycle(cg::grid_group &grid, double *part_rz, int vb, bool work) {
+  // z = M r.  On entry level 0's first sweep is in X(0) (levels > 1), and
+  // with `have_r0` level 0's residual of it too (the CG update computes it,
+  // one grid barrier fewer); on exit X(0) holds z, part_rz the block
+  // partials of r.z (block vb of the solve), and the grid has synchronised.
+  // Without `work` only the grid barriers are taken (a block of a finished
+  // solve sharing the launch).
+  __device__ void vcycle(cg::grid_group &grid, double *part_rz, int vb, bool work, bool have_r0) {
     const int L = mg.levels;
     double rz = 0.0;
     if (L == 1) {
@@ -303,9 +306,11 @@ struct Solve {
           grid.sync();
           trace(10 * l + 1);
         }
-        if (work) residual(l);
-        grid.sync();
-        trace(10 * l + 2);
+        if (l > 0 || !have_r0) {
+          if (work) residual(l);
+          grid.sync();
+          trace(10 * l + 2);
+        }
         if (work) restrict_to(l);
         grid.sync();
         trace(10 * l + 3);
@@ -365,7 +370,12 @@ __device__ __forceinline__ void cg_mg_body(const MgGroup<K> &G) {
   const uint8_t *dirichlet = Y.dirichlet;
   double *x = Y.x, *r = Y.r, *q = Y.q;
   double *part_pq = Y.part, *part_rz = Y.part + nblk, *part_rr = Y.part + 2 * nblk;
-  Solve S{Y.mg, st7, g, vb * kRedBlock + (int)threadIdx.x, nblk * kRedBlock, 0u};
+  Solve S{Y.mg, st7, g, vb * kRedBlock + (int)threadIdx.x, nblk * kRedBlock, 0u, r};
+  // the CG update computes level 0's residual of the next V-cycle's first
+  // sweep (one smoothing sweep: nothing runs between the two), reading the
+  // neighbours' old residuals; so r alternates between two buffers
+  const bool fuse_r0 = Y.mg.levels > 1 && Y.mg.nu == 1;
+  const MgDevLevel &L0 = Y.mg.L[0];
   bool done[K];
   int it[K];
   bool any = false;
@@ -384,7 +394,7 @@ __device__ __forceinline__ void cg_mg_body(const MgGroup<K> &G) {
         for (int n = S.tid; n < nodes; n += S.stride) S.first(0, n, r[n]);
       grid.sync();
     }
-    S.vcycle(grid, part_rz, vb, work);
+    S.vcycle(grid, part_rz, vb, work, false);
     if (work) rz = sum_partials(part_rz, nblk);
   }
   const double *pin = Y.p0;
@@ -433,7 +443,41 @@ __device__ __forceinline__ void cg_mg_body(const MgGroup<K> &G) {
     grid.sync();
     trace(100);
     double a2 = 0.0;
-    if (work) {
+    if (work && fuse_r0) {
+      const double alpha = rz / sum_partials(part_pq, nblk);
+      const double *rin = S.b0;
+      double *rout = rin == r ? Y.r1 : r;
+      double *x0 = S.X(0);
+      // first-sweep value of node m from its updated residual, as first(0)
+      auto first0 = [&](int m) { return dirichlet[m] ? 0.0 : L0.fscale[m] * (rin[m] - alpha * q[m]); };
+      const int sx = g.pz, sy = g.px * g.pz;
+      for (int n = S.tid; n < nodes; n += S.stride) {
+        double rn = rin[n];
+        if (!dirichlet[n]) {
+          x[n] += alpha * pout[n];
+          rn = rin[n] - alpha * q[n];
+          a2 += rn * rn;
+        }
+        rout[n] = rn;
+        const double f = dirichlet[n] ? 0.0 : L0.fscale[n] * rn;
+        x0[n] = f;
+        // level 0's residual of the first sweep (apply7's terms and order;
+        // an off-grid neighbour has a zero coefficient and is clamped)
+        int i, j, k;
+        node_ijk(n, g, i, j, k);
+        const double *a = st7 + (size_t)n * 7;
+        double acc = a[6] * f;
+        acc += a[0] * first0(i > 0 ? n - sx : n);
+        acc += a[1] * first0(i + 1 < g.px ? n + sx : n);
+        acc += a[2] * first0(j > 0 ? n - sy : n);
+        acc += a[3] * first0(j + 1 < g.py ? n + sy : n);
+        acc += a[4] * first0(k > 0 ? n - 1 : n);
+        acc += a[5] * first0(k + 1 < g.pz ? n + 1 : n);
+        const double v = rn - acc;
+        L0.r[n] = L0.dir[n] ? 0.0 : v;
+      }
+      S.b0 = rout;
+    } else if (work) {
       const double alpha = rz / sum_partials(part_pq, nblk);
       for (int n = S.tid; n < nodes; n += S.stride) {
         if (dirichlet[n]) {
@@ -464,7 +508,7 @@ __device__ __forceinline__ void cg_mg_body(const MgGroup<K> &G) {
     }
     if (!more) break;
     const bool cycle = work && !done[me];
-    S.vcycle(grid, part_rz, vb, cycle);
+    S.vcycle(grid, part_rz, vb, cycle, fuse_r0);
     if (cycle) {
       const double rz_new = sum_partials(part_rz, nblk);
       beta = rz_new / rz;
@@ -544,6 +588,11 @@ MgDevice mg_upload(const MgHierarchy &h, std::vector<void *> &owned) {
     }
     L.xb = scratch(L.n, owned);
     L.r = scratch(L.n, owned);
+    if (l == 0) {
+      std::vector<double> fs(L.n);
+      for (int n = 0; n < L.n; ++n) fs[n] = s.dir[n] ? s.dinv[n] : s.omega * s.dinv[n];
+      L.fscale = upload(fs, owned);
+    }
     if (l + 1 < d.levels) {
       const MgAxis *ax[3] = {&s.ax, &s.ay, &s.az};
       const std::vector<int> *kp[3] = {&s.kx, &s.ky, &s.kz};
@@ -610,8 +659,8 @@ int cg_mg_max_grid() { return co_resident((const void *)cg_mg_persistent); }
 bool cg_mg_pair_fits(int grid) { return grid > 0 && 2 * grid <= co_resident((const void *)cg_mg_pair); }
 
 cudaError_t launch_cg_mg(int nodes, const Grid3 &g, const double *st7, const uint8_t *dirichlet, double *x, double *r,
-                         double *z, double *p0, double *p1, double *q, double *part, double *sc, int max_iter,
-                         const MgDevice &mg, int grid, cudaStream_t s) {
+                         double *r1, double *z, double *p0, double *p1, double *q, double *part, double *sc,
+                         int max_iter, const MgDevice &mg, int grid, cudaStream_t s) {
   if (nodes != g.px * g.py * g.pz) return cudaErrorInvalidValue;
   MgGroup<1> G;
   MgSystem &y = G.s[0];
@@ -620,7 +669,7 @@ cudaError_t launch_cg_mg(int nodes, const Grid3 &g, const double *st7, const uin
   y.mg.L[0].xa = z;
   y.st7 = st7;
   y.dirichlet = dirichlet;
-  y.x = x; y.r = r; y.p0 = p0; y.p1 = p1; y.q = q; y.part = part; y.sc = sc;
+  y.x = x; y.r = r; y.r1 = r1; y.p0 = p0; y.p1 = p1; y.q = q; y.part = part; y.sc = sc;
   y.px = g.px; y.py = g.py; y.pz = g.pz;
   y.max_iter = max_iter;
   G.grid = grid;

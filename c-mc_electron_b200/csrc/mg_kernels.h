@@ -24,6 +24,9 @@ struct MgDevLevel {
   const double2 *wmap[3] = {nullptr, nullptr, nullptr};
   const int *keep[3] = {nullptr, nullptr, nullptr};
   const double *rtap[3] = {nullptr, nullptr, nullptr};  // [3 * coarse] restriction taps (mg_setup.h)
+  // level 0 only: [n] the first sweep's factor, x = fscale b (dinv on
+  // decoupled rows, omega dinv elsewhere: the same product as the sweep's)
+  const double *fscale = nullptr;
 };
 
 struct MgDevice {
@@ -44,8 +47,8 @@ MgDevice mg_upload(const MgHierarchy &h, std::vector<void *> &owned);
 // launch.
 struct Grid3;
 cudaError_t launch_cg_mg(int nodes, const Grid3 &g, const double *st7, const uint8_t *dirichlet, double *x, double *r,
-                         double *z, double *p0, double *p1, double *q, double *part, double *sc, int max_iter,
-                         const MgDevice &mg, int grid, cudaStream_t s);
+                         double *r1, double *z, double *p0, double *p1, double *q, double *part, double *sc,
+                         int max_iter, const MgDevice &mg, int grid, cudaStream_t s);
 // Largest cooperative grid of the MG kernel on the current device (blocks per SM x SMs); 0 if unavailable.
 int cg_mg_max_grid();
 
@@ -55,7 +58,9 @@ struct MgSystem {
   MgDevice mg;
   const double *st7 = nullptr;
   const uint8_t *dirichlet = nullptr;
-  double *x = nullptr, *r = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr, *part = nullptr, *sc = nullptr;
+  // r and r1: the CG residual, alternating each iteration (r holds it on entry)
+  double *x = nullptr, *r = nullptr, *r1 = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr, *part = nullptr,
+         *sc = nullptr;
   int px = 0, py = 0, pz = 0, max_iter = 0;
 };
 // Two solves in one cooperative launch of 2 x `grid` blocks: blocks [0, grid)
