@@ -173,7 +173,7 @@ uint64_t all_members(const mcb200_batch *b) {
 // The transport part of a step (mcb200_step for every member): the tables
 // must be current.  The members in `early` (none of them waiting for work on
 // the batch stream) fly on the side stream as soon as their own streams are
-// ready, one block per SM (it fits beside the two blocks per SM of a
+// ready, one block per SM (it fits beside the 512-thread block per SM of a
 // Poisson solve); the others fly in the main launch on the batch stream,
 // after which a helper launch on the batch stream draws from the side
 // launch's work counter with the room the solves left.  The copy

@@ -499,10 +499,10 @@ int cg_prepare(const DevMesh &M, const FieldBuffers &f, double rel_tol, cudaStre
     }
     if (most < 1) return 1;
     most = std::min(most, kCgMaxGrid);
-    // the V-cycle's short phases are barrier-bound: two blocks per SM
-    // measured fastest on the FinFET mesh (fewer blocks arrive at each
-    // barrier; more would idle on its coarse levels)
-    const int fallback = use_mg ? std::min(most, 2 * sms) : most;
+    // the V-cycle's short phases are barrier-bound: one 512-thread block
+    // per SM measured fastest on the FinFET mesh (fewer blocks arrive at
+    // each barrier; more would idle on its coarse levels)
+    const int fallback = use_mg ? std::min(most, cg_mg_blocks_per_sm() * sms) : most;
     plan.grid = plan.blocks > 0 ? std::min(plan.blocks, most) : fallback;
     plan.used = use_mg ? kCgMultigrid : kCgJacobi;
   }

@@ -52,7 +52,7 @@ constexpr int kCgMaxGrid = 1024;
 enum CgMethod { kCgAuto = 0, kCgJacobi = 1, kCgMultigrid = 2 };
 struct CgPlan {
   int method = kCgAuto;  // kCgAuto: multigrid when the hierarchy exists
-  int blocks = 0;        // requested grid (0: Jacobi the largest co-resident grid up to kCgMaxGrid, multigrid 2 per SM)
+  int blocks = 0;        // requested grid (0: Jacobi the largest co-resident grid up to kCgMaxGrid, multigrid 1 per SM)
   int grid = 0;          // grid in use (0 until the first solve)
   int used = 0;          // kCgJacobi or kCgMultigrid, set by the last solve
   unsigned long long launches = 0;

@@ -28,6 +28,21 @@ namespace cg = cooperative_groups;
 
 namespace {
 
+// Threads per block of the solve kernels and blocks per SM of the default
+// grid (tuning defines).  With at most 64 registers a thread (1024 threads
+// of registers per SM), kMgBlock x 1024 / kMgBlock blocks fill the SM.
+// Measured on the FinFET solve (same 75,776 threads): one 512-thread block
+// per SM 3 % faster than two of 256 (half the blocks arrive at each grid
+// barrier); 1024 threads on one block per SM, or 512 x 2, slower.
+#ifndef MCB200_MG_BLOCK
+#define MCB200_MG_BLOCK 512
+#endif
+#ifndef MCB200_MG_BLOCKS_PER_SM
+#define MCB200_MG_BLOCKS_PER_SM 1
+#endif
+constexpr int kMgBlock = MCB200_MG_BLOCK;
+static_assert(kMgBlock % 32 == 0 && 1024 % kMgBlock == 0, "MCB200_MG_BLOCK: 32-1024, dividing 1024");
+
 #ifdef MCB200_MG_TRACE
 // Opt-in phase trace (build with -DMCB200_MG_TRACE): block 0 records
 // (phase id, %globaltimer) after every barrier of the first solve.
@@ -335,7 +350,7 @@ struct Solve {
         }
       }
     }
-    const double bs = block_sum<kRedBlock>(rz);
+    const double bs = block_sum<kMgBlock>(rz);
     if (threadIdx.x == 0 && work) part_rz[vb] = bs;
     grid.sync();
     trace(7);
@@ -370,7 +385,7 @@ __device__ __forceinline__ void cg_mg_body(const MgGroup<K> &G) {
   const uint8_t *dirichlet = Y.dirichlet;
   double *x = Y.x, *r = Y.r, *q = Y.q;
   double *part_pq = Y.part, *part_rz = Y.part + nblk, *part_rr = Y.part + 2 * nblk;
-  Solve S{Y.mg, st7, g, vb * kRedBlock + (int)threadIdx.x, nblk * kRedBlock, 0u, r};
+  Solve S{Y.mg, st7, g, vb * kMgBlock + (int)threadIdx.x, nblk * kMgBlock, 0u, r};
   // the CG update computes level 0's residual of the next V-cycle's first
   // sweep (one smoothing sweep: nothing runs between the two), reading the
   // neighbours' old residuals; so r alternates between two buffers
@@ -395,7 +410,7 @@ __device__ __forceinline__ void cg_mg_body(const MgGroup<K> &G) {
       grid.sync();
     }
     S.vcycle(grid, part_rz, vb, work, false);
-    if (work) rz = sum_partials(part_rz, nblk);
+    if (work) rz = sum_partials<kMgBlock>(part_rz, nblk);
   }
   const double *pin = Y.p0;
   double *pout = Y.p1;
@@ -438,13 +453,13 @@ __device__ __forceinline__ void cg_mg_body(const MgGroup<K> &G) {
         v += pn * acc;
       }
     }
-    const double bs = block_sum<kRedBlock>(v);
+    const double bs = block_sum<kMgBlock>(v);
     if (threadIdx.x == 0 && work) part_pq[vb] = bs;
     grid.sync();
     trace(100);
     double a2 = 0.0;
     if (work && fuse_r0) {
-      const double alpha = rz / sum_partials(part_pq, nblk);
+      const double alpha = rz / sum_partials<kMgBlock>(part_pq, nblk);
       const double *rin = S.b0;
       double *rout = rin == r ? Y.r1 : r;
       double *x0 = S.X(0);
@@ -478,7 +493,7 @@ __device__ __forceinline__ void cg_mg_body(const MgGroup<K> &G) {
       }
       S.b0 = rout;
     } else if (work) {
-      const double alpha = rz / sum_partials(part_pq, nblk);
+      const double alpha = rz / sum_partials<kMgBlock>(part_pq, nblk);
       for (int n = S.tid; n < nodes; n += S.stride) {
         if (dirichlet[n]) {
           if (Y.mg.levels > 1) S.X(0)[n] = 0.0;
@@ -491,7 +506,7 @@ __device__ __forceinline__ void cg_mg_body(const MgGroup<K> &G) {
         if (Y.mg.levels > 1) S.first(0, n, rn);
       }
     }
-    const double b2 = block_sum<kRedBlock>(a2);
+    const double b2 = block_sum<kMgBlock>(a2);
     if (threadIdx.x == 0 && work) part_rr[vb] = b2;
     grid.sync();
     trace(101);
@@ -500,7 +515,7 @@ __device__ __forceinline__ void cg_mg_body(const MgGroup<K> &G) {
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       if (!act[k]) continue;
-      const double rk = sum_partials(G.s[k].part + 2 * nblk, nblk);
+      const double rk = sum_partials<kMgBlock>(G.s[k].part + 2 * nblk, nblk);
       if (k == me) rr = rk;
       ++it[k];
       done[k] = rk <= G.s[k].sc[9];
@@ -510,7 +525,7 @@ __device__ __forceinline__ void cg_mg_body(const MgGroup<K> &G) {
     const bool cycle = work && !done[me];
     S.vcycle(grid, part_rz, vb, cycle, fuse_r0);
     if (cycle) {
-      const double rz_new = sum_partials(part_rz, nblk);
+      const double rz_new = sum_partials<kMgBlock>(part_rz, nblk);
       beta = rz_new / rz;
       rz = rz_new;
       const double *t = pout;
@@ -534,15 +549,15 @@ __device__ __forceinline__ void cg_mg_body(const MgGroup<K> &G) {
 #ifndef MCB200_SOLVE_CARVEOUT
 #define MCB200_SOLVE_CARVEOUT -1
 #endif
-// At most 64 registers a thread: two blocks of a solve and one 256-thread
-// block of the flight kernels fit in an SM's registers together (a solve
-// can run beside a flight), and four blocks of the pair kernel fit alone.
+// At most 64 registers a thread: a solve's block (512 threads) and one
+// 256-thread block of the flight kernels fit in an SM's registers together
+// (a solve can run beside a flight), and two blocks of the pair kernel fit alone.
 // (Measured on the FinFET: the cap costs the solo solve about 2 %; without
 // it the compiler's choice was slower still.)
-__global__ void __launch_bounds__(kRedBlock, 4) cg_mg_persistent(const __grid_constant__ MgGroup<1> G) {
+__global__ void __launch_bounds__(kMgBlock, 1024 / kMgBlock) cg_mg_persistent(const __grid_constant__ MgGroup<1> G) {
   cg_mg_body<1>(G);
 }
-__global__ void __launch_bounds__(kRedBlock, 4) cg_mg_pair(const __grid_constant__ MgGroup<2> G) {
+__global__ void __launch_bounds__(kMgBlock, 1024 / kMgBlock) cg_mg_pair(const __grid_constant__ MgGroup<2> G) {
   cg_mg_body<2>(G);
 }
 
@@ -647,7 +662,7 @@ static int co_resident(const void *kernel) {
   configure_solve_kernels(dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-  if (!coop || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kRedBlock, 0) != cudaSuccess) {
+  if (!coop || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kMgBlock, 0) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
@@ -655,6 +670,8 @@ static int co_resident(const void *kernel) {
 }
 
 int cg_mg_max_grid() { return co_resident((const void *)cg_mg_persistent); }
+
+int cg_mg_blocks_per_sm() { return MCB200_MG_BLOCKS_PER_SM; }
 
 bool cg_mg_pair_fits(int grid) { return grid > 0 && 2 * grid <= co_resident((const void *)cg_mg_pair); }
 
@@ -676,7 +693,7 @@ cudaError_t launch_cg_mg(int nodes, const Grid3 &g, const double *st7, const uin
   int dev = 0;
   if (cudaGetDevice(&dev) == cudaSuccess) configure_solve_kernels(dev);
   void *args[] = {&G};
-  return cudaLaunchCooperativeKernel((const void *)cg_mg_persistent, grid, kRedBlock, args, 0, s);
+  return cudaLaunchCooperativeKernel((const void *)cg_mg_persistent, grid, kMgBlock, args, 0, s);
 }
 
 cudaError_t launch_cg_mg_pair(const MgSystem a[2], int grid, cudaStream_t s) {
@@ -687,7 +704,7 @@ cudaError_t launch_cg_mg_pair(const MgSystem a[2], int grid, cudaStream_t s) {
   G.s[1] = a[1];
   G.grid = grid;
   void *args[] = {&G};
-  return cudaLaunchCooperativeKernel((const void *)cg_mg_pair, 2 * grid, kRedBlock, args, 0, s);
+  return cudaLaunchCooperativeKernel((const void *)cg_mg_pair, 2 * grid, kMgBlock, args, 0, s);
 }
 
 }  // namespace mcb200

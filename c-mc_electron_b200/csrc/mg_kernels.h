@@ -51,6 +51,8 @@ cudaError_t launch_cg_mg(int nodes, const Grid3 &g, const double *st7, const uin
                          int max_iter, const MgDevice &mg, int grid, cudaStream_t s);
 // Largest cooperative grid of the MG kernel on the current device (blocks per SM x SMs); 0 if unavailable.
 int cg_mg_max_grid();
+// The MG kernel's default grid, per SM (MCB200_MG_BLOCKS_PER_SM).
+int cg_mg_blocks_per_sm();
 
 // One solve's arguments, as launch_cg_mg takes them (mg with level 0's b and
 // xa bound to r and z).

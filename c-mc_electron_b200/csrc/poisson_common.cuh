@@ -19,26 +19,30 @@ __device__ __forceinline__ void node_ijk(int p, const Grid3 &g, int &i, int &j, 
 
 constexpr int kRedBlock = 256;
 
-// Fixed-order block partial sums of a[i]*b[i] (first stage of a dot product).
+// Sum of v over a block of B threads (a multiple of 32), the same bits in
+// every thread and on every call: a butterfly within each warp, then every
+// thread adds the warp sums in warp order.
 template <int B>
 __device__ __forceinline__ double block_sum(double v) {
-  __shared__ double s[B];
-  s[threadIdx.x] = v;
+  static_assert(B % 32 == 0 && B <= 1024, "block_sum: whole warps");
+  __shared__ double s[B / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = v;
   __syncthreads();
-  for (int o = B / 2; o > 0; o >>= 1) {
-    if (threadIdx.x < o) s[threadIdx.x] += s[threadIdx.x + o];
-    __syncthreads();
-  }
-  const double r = s[0];
+  double r = s[0];
+#pragma unroll
+  for (int w = 1; w < B / 32; ++w) r += s[w];
   __syncthreads();
   return r;
 }
 
-// Sum of n partials, read in the same order by every block.
+// Sum of n partials, read in the same order by every block of B threads.
+template <int B = kRedBlock>
 __device__ __forceinline__ double sum_partials(const double *part, int n) {
   double v = 0.0;
-  for (int i = threadIdx.x; i < n; i += kRedBlock) v += part[i];
-  return block_sum<kRedBlock>(v);
+  for (int i = threadIdx.x; i < n; i += B) v += part[i];
+  return block_sum<B>(v);
 }
 
 }  // namespace mcb200

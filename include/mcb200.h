@@ -199,7 +199,7 @@ int mcb200_get_induced_current(mcb200_ctx *ctx, double *sum, double *steps);
 #define MCB200_POISSON_JACOBI 1    /* Jacobi-preconditioned CG */
 #define MCB200_POISSON_MULTIGRID 2 /* V-cycle-preconditioned CG */
 /* Preconditioner and cooperative grid (blocks; 0 = automatic: Jacobi the
- * largest co-resident grid, multigrid two blocks per SM) of the following
+ * largest co-resident grid, multigrid one 512-thread block per SM) of the following
  * solves.  No counterpart in the reference. */
 int mcb200_set_poisson_solver(mcb200_ctx *ctx, int method, int blocks);
 /* Preconditioner (MCB200_POISSON_JACOBI / _MULTIGRID) and grid of the last
