@@ -320,7 +320,8 @@ void batch_full_step(mcb200_batch *b, uint64_t due) {
       if (k1 >= 0) {
         mcb200_ctx *c1 = b->m[k1];
         launched[k1] = 1;
-        const MgSystem two[2] = {cg_mg_system(c0->mesh, c0->fb, kMaxIter), cg_mg_system(c1->mesh, c1->fb, kMaxIter)};
+        const MgSystem two[2] = {cg_mg_system(c0->mesh, c0->fb, kMaxIter, c0->cg_plan.rel_tol2),
+                                 cg_mg_system(c1->mesh, c1->fb, kMaxIter, c1->cg_plan.rel_tol2)};
         ck(launch_cg_mg_pair(two, c0->cg_plan.grid, b->stream), "paired Poisson solve");
         c0->cg_plan.launches += 1;
         c1->cg_plan.launches += 1;

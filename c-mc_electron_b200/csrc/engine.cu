@@ -1402,7 +1402,7 @@ int mcb200_set_induced_current(mcb200_ctx *c, int contact) {
         throw CudaError("weighting-potential solve failed");
       ck(cudaEventRecord(last, s), "event");
     }
-    if (cg_finish(c->mesh, w, s, c->h_scratch, &its, &res)) throw CudaError("weighting-potential solve failed");
+    if (cg_finish(c->mesh, w, plan, s, c->h_scratch, &its, &res)) throw CudaError("weighting-potential solve failed");
     if (!(res <= 1e-10)) return fail(c, MCB200_ERR_STATE, "weighting-potential solve did not converge");
     if (!c->induced_field) c->induced_field = dalloc<double>(cells * 3, c->mesh_owned);
     DevMesh m = c->mesh;
@@ -1907,7 +1907,8 @@ void poisson_enqueue(mcb200_ctx *c, cudaStream_t s, double rel_tol, int max_iter
 }
 
 void poisson_finish(mcb200_ctx *c, cudaStream_t s, int *iterations, double *rel_residual) {
-  if (cg_finish(c->mesh, c->fb, s, c->h_scratch, iterations, rel_residual)) throw CudaError("Poisson solve failed");
+  if (cg_finish(c->mesh, c->fb, c->cg_plan, s, c->h_scratch, iterations, rel_residual))
+    throw CudaError("Poisson solve failed");
   if (c->qc_on) {  // compute_field, src/mcmodel.cpp:2240-2262
     launch_effective_potential(c->qc, c->fb.potential, c->qc_pot, s);
     launch_pot2field(c->mesh, c->fb.potential, s, c->qc_pot);
@@ -1916,10 +1917,9 @@ void poisson_finish(mcb200_ctx *c, cudaStream_t s, int *iterations, double *rel_
     launch_pot2field(c->mesh, c->fb.potential, s);
   }
   ck(cudaGetLastError(), "pot2field");
-  // rhs, the solve's set-up / dots / persistent CG / true residual /
-  // statistics (16 with Jacobi preconditioning, 13 with multigrid: no
-  // Jacobi z0 or r.z0), pot2field
-  c->launches += c->cg_plan.used == kCgMultigrid ? 15 : 18;
+  // rhs, the solve (Jacobi: set-up, dots, persistent CG, true residual and
+  // statistics in 16 launches; multigrid: one), pot2field
+  c->launches += c->cg_plan.used == kCgMultigrid ? 3 : 18;
   c->fields_set = true;
 }
 
@@ -1978,9 +1978,9 @@ void step_tail(mcb200_ctx *c) {
   const int cap = (int)c->capacity;
   ChildSetT<R> set;
   for (int g = 0; g < mcb200_ctx::kGenerations; ++g) set.g[g] = children<R>(c, g);
-  // a step's copies are few: one block per SM strides over them
+  // a step's copies are few: four blocks per SM, 32 copies a block, stride over them
   launch_append_children(set, c->dev_counts + 1, store<R>(c, c->cur), c->dev_counts, cap, c->append_count,
-                         c->dev_counts + 2, c->sm_count, s);
+                         c->dev_counts + 2, 4 * c->sm_count, s);
   ck(cudaGetLastError(), "append children");
   c->launches += 1;
   const int other = 1 - c->cur;

@@ -473,18 +473,19 @@ int cg_prepare(const DevMesh &M, const FieldBuffers &f, double rel_tol, cudaStre
   const bool use_mg = f.mg && plan.method != kCgJacobi;
   if (plan.method == kCgMultigrid && !f.mg) return 1;
   double *sc = f.cg_scalars;
-  // ||b_free|| with the Dirichlet values folded in
-  set_dirichlet<<<nb, 256, 0, s>>>(nodes, f.dirichlet, f.rhs, f.potential);
-  folded_rhs<<<nb, 256, 0, s>>>(nodes, g, f.stencil, f.dirichlet, f.rhs, f.cg_q);
-  dot(nodes, f.cg_q, f.cg_q, f.cg_part, sc + 6, s);
-  // r = b - A x (x: the previous potential, a warm start)
-  stencil_apply<<<nb, 256, 0, s>>>(nodes, g, f.stencil, f.dirichlet, f.potential, f.rhs, f.cg_r);
-  if (!use_mg) {
+  plan.rel_tol2 = rel_tol * rel_tol;
+  if (!use_mg) {  // the multigrid launch does its own set-up
+    // ||b_free|| with the Dirichlet values folded in
+    set_dirichlet<<<nb, 256, 0, s>>>(nodes, f.dirichlet, f.rhs, f.potential);
+    folded_rhs<<<nb, 256, 0, s>>>(nodes, g, f.stencil, f.dirichlet, f.rhs, f.cg_q);
+    dot(nodes, f.cg_q, f.cg_q, f.cg_part, sc + 6, s);
+    // r = b - A x (x: the previous potential, a warm start)
+    stencil_apply<<<nb, 256, 0, s>>>(nodes, g, f.stencil, f.dirichlet, f.potential, f.rhs, f.cg_r);
     cg_init<<<nb, 256, 0, s>>>(nodes, f.cg_r, f.diag_inv, f.cg_z, f.cg_p, f.dirichlet, f.rhs, f.potential);
     dot(nodes, f.cg_r, f.cg_z, f.cg_part, sc + 0, s);
+    dot(nodes, f.cg_r, f.cg_r, f.cg_part, sc + 3, s);
+    cg_setup<<<1, 1, 0, s>>>(sc, plan.rel_tol2);
   }
-  dot(nodes, f.cg_r, f.cg_r, f.cg_part, sc + 3, s);
-  cg_setup<<<1, 1, 0, s>>>(sc, rel_tol * rel_tol);
   // the persistent launch's grid, fixed per context (so is the reduction order)
   if (plan.grid == 0 || plan.used != (use_mg ? kCgMultigrid : kCgJacobi)) {
     int dev = 0, sms = 0, per_sm = 0, coop = 0, most = 0;
@@ -509,7 +510,7 @@ int cg_prepare(const DevMesh &M, const FieldBuffers &f, double rel_tol, cudaStre
   return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 
-MgSystem cg_mg_system(const DevMesh &M, const FieldBuffers &f, int max_iter) {
+MgSystem cg_mg_system(const DevMesh &M, const FieldBuffers &f, int max_iter, double rel_tol2) {
   MgSystem y;
   y.mg = *f.mg;
   y.mg.L[0].b = f.cg_r;
@@ -518,6 +519,9 @@ MgSystem cg_mg_system(const DevMesh &M, const FieldBuffers &f, int max_iter) {
   y.dirichlet = f.dirichlet;
   y.x = f.potential; y.r = f.cg_r; y.r1 = f.cg_r1; y.p0 = f.cg_p; y.p1 = f.cg_p1; y.q = f.cg_q; y.part = f.cg_part;
   y.sc = f.cg_scalars;
+  y.rhs = f.rhs;
+  y.stats = f.poisson_stats;
+  y.rel_tol2 = rel_tol2;
   y.px = M.nx + 1; y.py = M.ny + 1; y.pz = M.nz + 1;
   y.max_iter = max_iter;
   return y;
@@ -529,10 +533,7 @@ int cg_launch(const DevMesh &M, const FieldBuffers &f, int max_iter, cudaStream_
   double *x = f.potential, *r = f.cg_r, *z = f.cg_z, *p0 = f.cg_p, *p1 = f.cg_p1, *q = f.cg_q, *part = f.cg_part;
   double *sc = f.cg_scalars;
   if (plan.used == kCgMultigrid) {
-    if (launch_cg_mg(nodes, g, f.stencil, f.dirichlet, x, r, f.cg_r1, z, p0, p1, q, part, sc, max_iter, *f.mg,
-                     plan.grid, s) !=
-        cudaSuccess)
-      return 1;
+    if (launch_cg_mg(cg_mg_system(M, f, max_iter, plan.rel_tol2), plan.grid, s) != cudaSuccess) return 1;
   } else {
     int nodes_arg = nodes, max_arg = max_iter;
     Grid3 g_arg = g;
@@ -546,16 +547,18 @@ int cg_launch(const DevMesh &M, const FieldBuffers &f, int max_iter, cudaStream_
   return 0;
 }
 
-int cg_finish(const DevMesh &M, const FieldBuffers &f, cudaStream_t s, double *host_scratch, int *iterations,
-              double *rel_residual) {
+int cg_finish(const DevMesh &M, const FieldBuffers &f, const CgPlan &plan, cudaStream_t s, double *host_scratch,
+              int *iterations, double *rel_residual) {
   const int nodes = (M.nx + 1) * (M.ny + 1) * (M.nz + 1);
   const int nb = blocks(nodes, 256);
   double *sc = f.cg_scalars;
-  // true residual of the final iterate, and the running statistics
-  stencil_apply<<<nb, 256, 0, s>>>(nodes, Grid3{M.nx + 1, M.ny + 1, M.nz + 1}, f.stencil, f.dirichlet, f.potential,
-                                   f.rhs, f.cg_r);
-  dot(nodes, f.cg_r, f.cg_r, f.cg_part, sc + 3, s);
-  poisson_stats_kernel<<<1, 32, 0, s>>>(sc, f.poisson_stats);
+  if (plan.used != kCgMultigrid) {  // (the multigrid launch ends with both)
+    // true residual of the final iterate, and the running statistics
+    stencil_apply<<<nb, 256, 0, s>>>(nodes, Grid3{M.nx + 1, M.ny + 1, M.nz + 1}, f.stencil, f.dirichlet,
+                                     f.potential, f.rhs, f.cg_r);
+    dot(nodes, f.cg_r, f.cg_r, f.cg_part, sc + 3, s);
+    poisson_stats_kernel<<<1, 32, 0, s>>>(sc, f.poisson_stats);
+  }
   if (!iterations && !rel_residual) return cudaGetLastError() == cudaSuccess ? 0 : 1;  // nothing waits
   cudaMemcpyAsync(host_scratch, sc, 10 * sizeof(double), cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return 1;
@@ -568,7 +571,7 @@ int cg_finish(const DevMesh &M, const FieldBuffers &f, cudaStream_t s, double *h
 int cg_solve(const DevMesh &M, const FieldBuffers &f, double rel_tol, int max_iter, cudaStream_t s,
              double *host_scratch, int *iterations, double *rel_residual, CgPlan &plan) {
   if (cg_prepare(M, f, rel_tol, s, plan) || cg_launch(M, f, max_iter, s, plan)) return 1;
-  return cg_finish(M, f, s, host_scratch, iterations, rel_residual);
+  return cg_finish(M, f, plan, s, host_scratch, iterations, rel_residual);
 }
 
 void launch_pot2field(const DevMesh &M, const double *pot, cudaStream_t s, const double *pot_e) {

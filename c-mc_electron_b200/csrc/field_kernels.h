@@ -55,6 +55,7 @@ struct CgPlan {
   int blocks = 0;        // requested grid (0: Jacobi the largest co-resident grid up to kCgMaxGrid, multigrid 1 per SM)
   int grid = 0;          // grid in use (0 until the first solve)
   int used = 0;          // kCgJacobi or kCgMultigrid, set by the last solve
+  double rel_tol2 = 0;   // the last cg_prepare's rel_tol^2
   unsigned long long launches = 0;
 };
 // Returns 0 on success; host_scratch must hold 10 doubles (pinned).  With
@@ -63,15 +64,17 @@ struct CgPlan {
 int cg_solve(const DevMesh &M, const FieldBuffers &f, double rel_tol, int max_iter, cudaStream_t s,
              double *host_scratch, int *iterations, double *rel_residual, CgPlan &plan);
 // cg_solve in three parts, for callers that launch several solves together:
-// the set-up (right side, residual, tolerances, the plan's grid), the
-// persistent launch, the true residual and statistics.  Each returns 0 on
-// success.  cg_mg_system: the multigrid launch's arguments (plan.used ==
-// kCgMultigrid, after cg_prepare) for launch_cg_mg_pair.
+// the set-up (Jacobi: residual and tolerances; both: the plan's grid and
+// tolerance), the persistent launch (multigrid: set-up, iterations, true
+// residual and statistics in one), then (Jacobi) the true residual and
+// statistics and (both) the results to the host when asked for.  Each
+// returns 0 on success.  cg_mg_system: the multigrid launch's arguments
+// (plan.used == kCgMultigrid, after cg_prepare) for launch_cg_mg_pair.
 int cg_prepare(const DevMesh &M, const FieldBuffers &f, double rel_tol, cudaStream_t s, CgPlan &plan);
 int cg_launch(const DevMesh &M, const FieldBuffers &f, int max_iter, cudaStream_t s, CgPlan &plan);
-int cg_finish(const DevMesh &M, const FieldBuffers &f, cudaStream_t s, double *host_scratch, int *iterations,
-              double *rel_residual);
-MgSystem cg_mg_system(const DevMesh &M, const FieldBuffers &f, int max_iter);
+int cg_finish(const DevMesh &M, const FieldBuffers &f, const CgPlan &plan, cudaStream_t s, double *host_scratch,
+              int *iterations, double *rel_residual);
+MgSystem cg_mg_system(const DevMesh &M, const FieldBuffers &f, int max_iter, double rel_tol2);
 // Fields of both carriers from pot; with pot_e, the electrons' from pot_e.
 void launch_pot2field(const DevMesh &M, const double *pot, cudaStream_t s, const double *pot_e = nullptr);
 

@@ -542,11 +542,14 @@ __global__ void __launch_bounds__(256) cell_scatter(DevParticlesT<R> src, DevCou
 // The surviving copies of every generation (already flown) join the store
 // after its *n particles, in one launch.  A copy's uid is *next_uid + the
 // number of surviving copies with a smaller (parent uid, sub) key, over all
-// generations (the key set is the concatenation of the generations); each
-// block compares its 256 copies with all copies, 256 at a time.  The place
-// in the store is taken from `appended` (order does not matter: the cell
-// sort follows); a copy that would land beyond the store's capacity is
-// dropped and raises *overflow (the host reports it).
+// generations (the key set is the concatenation of the generations).  A
+// block ranks 32 copies at a time, one a lane: the keys of all copies are
+// staged through shared memory in chunks, each of the eight warps counts
+// the smaller live keys of every eighth one (a broadcast read per compare),
+// and the eight counts of a lane are added.  The place in the store is
+// taken from `appended` (order does not matter: the cell sort follows); a
+// copy that would land beyond the store's capacity is dropped and raises
+// *overflow (the host reports it).
 template <typename R>
 struct CopyRef {
   const ChildSetT<R> &set;
@@ -576,10 +579,13 @@ struct CopyRef {
 };
 
 template <typename R>
-__global__ void append_children_kernel(ChildSetT<R> set, const unsigned int *next_uid, DevParticlesT<R> dst,
-                                       const unsigned int *n, int capacity, unsigned int *appended,
-                                       unsigned int *overflow) {
-  __shared__ uint64_t tile[256];
+__global__ void __launch_bounds__(256) append_children_kernel(ChildSetT<R> set, const unsigned int *next_uid,
+                                                              DevParticlesT<R> dst, const unsigned int *n,
+                                                              int capacity, unsigned int *appended,
+                                                              unsigned int *overflow) {
+  constexpr int kChunk = 2048;
+  __shared__ uint64_t keys[kChunk];
+  __shared__ uint32_t part[8][32];
   pdl_wait();
   const CopyRef<R> ref(set);
   int total = 0;
@@ -588,39 +594,46 @@ __global__ void append_children_kernel(ChildSetT<R> set, const unsigned int *nex
   if (total == 0) return;
   const uint32_t uid0 = *next_uid;
   const unsigned int n0 = *n;
-  for (int base_i = blockIdx.x * 256; base_i < total; base_i += gridDim.x * 256) {
-    const int i = base_i + threadIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int base_i = blockIdx.x * 32; base_i < total; base_i += gridDim.x * 32) {
+    const int i = base_i + lane;
     uint64_t my = ~0ull;
     bool my_alive = false;
     if (i < total) ref.key(i, my, my_alive);
     uint32_t rank = 0;
-    for (int base = 0; base < total; base += 256) {
-      const int j = base + threadIdx.x;
-      uint64_t kj = ~0ull;
-      bool aj = false;
-      if (j < total) ref.key(j, kj, aj);
-      tile[threadIdx.x] = aj ? kj : ~0ull;  // a dead copy ranks after every live one
+    for (int base = 0; base < total; base += kChunk) {
+      const int m = min(kChunk, total - base);
+      __syncthreads();  // the previous chunk (and the previous group's counts) are consumed
+      for (int j = threadIdx.x; j < m; j += 256) {
+        uint64_t kj;
+        bool aj;
+        ref.key(base + j, kj, aj);
+        keys[j] = aj ? kj : ~0ull;  // a dead copy ranks after every live one
+      }
       __syncthreads();
-      const int m = min(256, total - base);
-      for (int q = 0; q < m; ++q) rank += tile[q] < my ? 1u : 0u;
-      __syncthreads();
+      for (int q = warp; q < m; q += 8) rank += keys[q] < my ? 1u : 0u;
     }
-    if (i < total && my_alive) {
+    part[warp][lane] = rank;
+    __syncthreads();
+    if (warp == 0 && i < total && my_alive) {
+      uint32_t r = 0;
+#pragma unroll
+      for (int w = 0; w < 8; ++w) r += part[w][lane];
       int gen, local;
       ref.locate(i, gen, local);
       const DevChildrenT<R> &c = set.g[gen];
       const unsigned long long q = (unsigned long long)n0 + atomicAdd(appended, 1u);
       if (q >= (unsigned long long)capacity) {
         *overflow = 1u;
-        continue;
+      } else {
+        dst.x[q] = c.x[local]; dst.y[q] = c.y[local]; dst.z[q] = c.z[local];
+        dst.kx[q] = c.kx[local]; dst.ky[q] = c.ky[local]; dst.kz[q] = c.kz[local];
+        dst.energy[q] = c.energy[local]; dst.charge[q] = c.charge[local];
+        dst.cell[q] = c.cell[local];
+        dst.itet[q] = c.itet[local];
+        dst.meta[q] = c.meta[local] & 0xffffu;
+        dst.uid[q] = uid0 + r;
       }
-      dst.x[q] = c.x[local]; dst.y[q] = c.y[local]; dst.z[q] = c.z[local];
-      dst.kx[q] = c.kx[local]; dst.ky[q] = c.ky[local]; dst.kz[q] = c.kz[local];
-      dst.energy[q] = c.energy[local]; dst.charge[q] = c.charge[local];
-      dst.cell[q] = c.cell[local];
-      dst.itet[q] = c.itet[local];
-      dst.meta[q] = c.meta[local] & 0xffffu;
-      dst.uid[q] = uid0 + rank;
     }
   }
 }

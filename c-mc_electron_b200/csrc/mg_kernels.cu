@@ -357,15 +357,42 @@ struct Solve {
   }
 };
 
-// CG scalars as in the Jacobi solve: [0] rz, [3] rr, [6] ||b||^2, [7]
-// converged, [8] iterations, [9] (rel_tol ||b||)^2.  z = M r for the
-// initial residual is computed here.
+// CG scalars as in the Jacobi solve: [0] rz, [3] rr (on exit the true
+// residual's), [6] ||b||^2, [7] converged at the start, [8] iterations, [9]
+// (rel_tol ||b||)^2, all written here, as is z = M r for the initial residual.
 //
 // K solves share the launch: block b works for solve b / grid on its own
 // grid of `grid` blocks (local block b % grid), so each solve runs as it
 // would alone.  Every block follows every solve's residual norm (each
 // computes the same fixed-order sums), so all blocks agree on when the
 // launch ends; a block whose solve has finished takes only the barriers.
+// b_ff[n] and (b_ff - A x)[n] of the eliminated system: the free rows'
+// right side with the Dirichlet neighbours' values folded in, and its
+// residual (zero on Dirichlet rows).  x holds the Dirichlet values on
+// Dirichlet nodes.  The folded_rhs / stencil_apply terms in their order.
+__device__ __forceinline__ void folded_residual(const MgSystem &Y, const Grid3 &g, const double *x, int n,
+                                                double &bf, double &rn) {
+  if (Y.dirichlet[n]) {
+    bf = rn = 0.0;
+    return;
+  }
+  int i, j, k;
+  node_ijk(n, g, i, j, k);
+  const double *a = Y.st7 + (size_t)n * 7;
+  double acc = a[6] * x[n], fold = 0.0;
+  const int nb[6] = {i > 0 ? n - g.pz : -1, i + 1 < g.px ? n + g.pz : -1, j > 0 ? n - g.px * g.pz : -1,
+                     j + 1 < g.py ? n + g.px * g.pz : -1, k > 0 ? n - 1 : -1, k + 1 < g.pz ? n + 1 : -1};
+#pragma unroll
+  for (int t = 0; t < 6; ++t) {
+    const int m = nb[t];
+    if (m < 0 || a[t] == 0.0) continue;
+    if (Y.dirichlet[m]) fold += a[t] * x[m];
+    else acc += a[t] * x[m];
+  }
+  bf = Y.rhs[n] - fold;
+  rn = bf - acc;
+}
+
 template <int K>
 struct MgGroup {
   MgSystem s[K];
@@ -391,16 +418,50 @@ __device__ __forceinline__ void cg_mg_body(const MgGroup<K> &G) {
   // neighbours' old residuals; so r alternates between two buffers
   const bool fuse_r0 = Y.mg.levels > 1 && Y.mg.nu == 1;
   const MgDevLevel &L0 = Y.mg.L[0];
+  // set-up: the Dirichlet values into x, then r = b_ff - A x (x: the
+  // previous potential, a warm start) and the partials of ||b_ff||^2, ||r||^2
+  for (int n = S.tid; n < nodes; n += S.stride)
+    if (dirichlet[n]) x[n] = Y.rhs[n];
+  grid.sync();
+  {
+    double bb = 0.0, r2 = 0.0;
+    for (int n = S.tid; n < nodes; n += S.stride) {
+      double bf, rn;
+      folded_residual(Y, g, x, n, bf, rn);
+      r[n] = rn;
+      bb += bf * bf;
+      r2 += rn * rn;
+    }
+    const double s1 = block_sum<kMgBlock>(bb), s2 = block_sum<kMgBlock>(r2);
+    if (threadIdx.x == 0) {
+      part_pq[vb] = s1;
+      part_rr[vb] = s2;
+    }
+  }
+  grid.sync();
   bool done[K];
   int it[K];
+  double tol2[K];
   bool any = false;
+  double bnorm2 = 0.0, rr = 0.0, rz = 0.0, beta = 0.0;
 #pragma unroll
   for (int k = 0; k < K; ++k) {
-    done[k] = G.s[k].sc[7] != 0.0;
+    const double b2 = sum_partials<kMgBlock>(G.s[k].part, nblk);
+    const double r2 = sum_partials<kMgBlock>(G.s[k].part + 2 * nblk, nblk);
+    tol2[k] = G.s[k].rel_tol2 * b2;
+    done[k] = r2 <= tol2[k];  // converged already when the warm start meets the tolerance
     it[k] = 0;
     any = any || !done[k];
+    if (k == me) {
+      bnorm2 = b2;
+      rr = r2;
+    }
   }
-  double rr = Y.sc[3], rz = 0.0, beta = 0.0;
+  if (vb == 0 && threadIdx.x == 0) {
+    Y.sc[6] = bnorm2;
+    Y.sc[7] = done[me] ? 1.0 : 0.0;
+    Y.sc[9] = tol2[me];
+  }
   trace(0);
   if (any) {
     const bool work = !done[me];
@@ -518,7 +579,7 @@ __device__ __forceinline__ void cg_mg_body(const MgGroup<K> &G) {
       const double rk = sum_partials<kMgBlock>(G.s[k].part + 2 * nblk, nblk);
       if (k == me) rr = rk;
       ++it[k];
-      done[k] = rk <= G.s[k].sc[9];
+      done[k] = rk <= tol2[k];
       more = more || !done[k];
     }
     if (!more) break;
@@ -533,10 +594,33 @@ __device__ __forceinline__ void cg_mg_body(const MgGroup<K> &G) {
       pin = t;
     }
   }
+  // the true residual of the final iterate (the recurrence's drifts from
+  // it), and the solve's statistics.  The barrier: every block has read the
+  // partials the loop ended on (the last update of x is behind one too).
+  grid.sync();
+  {
+    double r2 = 0.0;
+    for (int n = S.tid; n < nodes; n += S.stride) {
+      double bf, rn;
+      folded_residual(Y, g, x, n, bf, rn);
+      r[n] = rn;
+      r2 += rn * rn;
+    }
+    const double s2 = block_sum<kMgBlock>(r2);
+    if (threadIdx.x == 0) part_rr[vb] = s2;
+  }
+  grid.sync();
+  rr = sum_partials<kMgBlock>(part_rr, nblk);
   if (vb == 0 && threadIdx.x == 0) {
     Y.sc[0] = rz;
     Y.sc[3] = rr;
     Y.sc[8] = it[me];
+    if (Y.stats) {
+      const double bnorm = sqrt(bnorm2) > 0 ? sqrt(bnorm2) : 1.0;
+      Y.stats[0] += 1.0;
+      Y.stats[1] += it[me];
+      Y.stats[2] = fmax(Y.stats[2], sqrt(rr) / bnorm);
+    }
   }
 }
 
@@ -675,20 +759,9 @@ int cg_mg_blocks_per_sm() { return MCB200_MG_BLOCKS_PER_SM; }
 
 bool cg_mg_pair_fits(int grid) { return grid > 0 && 2 * grid <= co_resident((const void *)cg_mg_pair); }
 
-cudaError_t launch_cg_mg(int nodes, const Grid3 &g, const double *st7, const uint8_t *dirichlet, double *x, double *r,
-                         double *r1, double *z, double *p0, double *p1, double *q, double *part, double *sc,
-                         int max_iter, const MgDevice &mg, int grid, cudaStream_t s) {
-  if (nodes != g.px * g.py * g.pz) return cudaErrorInvalidValue;
+cudaError_t launch_cg_mg(const MgSystem &y, int grid, cudaStream_t s) {
   MgGroup<1> G;
-  MgSystem &y = G.s[0];
-  y.mg = mg;
-  y.mg.L[0].b = r;
-  y.mg.L[0].xa = z;
-  y.st7 = st7;
-  y.dirichlet = dirichlet;
-  y.x = x; y.r = r; y.r1 = r1; y.p0 = p0; y.p1 = p1; y.q = q; y.part = part; y.sc = sc;
-  y.px = g.px; y.py = g.py; y.pz = g.pz;
-  y.max_iter = max_iter;
+  G.s[0] = y;
   G.grid = grid;
   int dev = 0;
   if (cudaGetDevice(&dev) == cudaSuccess) configure_solve_kernels(dev);

@@ -41,14 +41,13 @@ struct MgDevice {
 // allocation is appended to `owned` (freed by the caller with cudaFree).
 MgDevice mg_upload(const MgHierarchy &h, std::vector<void *> &owned);
 
-// The CG iterations of one solve with the V-cycle as preconditioner, in one
-// cooperative launch of `grid` blocks; the CG vectors and scalars are those
-// of the Jacobi solve (field_kernels.cu).  Returns the cudaError_t of the
+// One solve with the V-cycle as preconditioner, in one cooperative launch
+// of `grid` blocks: the set-up (the Dirichlet values into x, the initial
+// residual and the norms), every CG iteration, the true residual of the
+// final iterate and the solve statistics.  Returns the cudaError_t of the
 // launch.
-struct Grid3;
-cudaError_t launch_cg_mg(int nodes, const Grid3 &g, const double *st7, const uint8_t *dirichlet, double *x, double *r,
-                         double *r1, double *z, double *p0, double *p1, double *q, double *part, double *sc,
-                         int max_iter, const MgDevice &mg, int grid, cudaStream_t s);
+struct MgSystem;
+cudaError_t launch_cg_mg(const MgSystem &y, int grid, cudaStream_t s);
 // Largest cooperative grid of the MG kernel on the current device (blocks per SM x SMs); 0 if unavailable.
 int cg_mg_max_grid();
 // The MG kernel's default grid, per SM (MCB200_MG_BLOCKS_PER_SM).
@@ -60,9 +59,12 @@ struct MgSystem {
   MgDevice mg;
   const double *st7 = nullptr;
   const uint8_t *dirichlet = nullptr;
-  // r and r1: the CG residual, alternating each iteration (r holds it on entry)
+  // r and r1: the CG residual, alternating each iteration
   double *x = nullptr, *r = nullptr, *r1 = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr, *part = nullptr,
          *sc = nullptr;
+  const double *rhs = nullptr;  // right side (Dirichlet rows: the contact values)
+  double *stats = nullptr;      // [3] solves, iterations, largest relative residual (accumulated)
+  double rel_tol2 = 0.0;        // converged when ||r||^2 <= rel_tol2 ||b_ff||^2
   int px = 0, py = 0, pz = 0, max_iter = 0;
 };
 // Two solves in one cooperative launch of 2 x `grid` blocks: blocks [0, grid)
