@@ -1302,7 +1302,7 @@ int mcb200_set_device(mcb200_ctx *c, const int32_t *material, const double *dono
       const std::shared_ptr<const MgHierarchy> h =
           cached_hierarchy(m.nx + 1, m.ny + 1, m.nz + 1, X, Y, Z, s.stencil, s.dirichlet);
       if (h) {  // (none: a mesh that does not coarsen, Jacobi preconditioning)
-        c->mg = mg_upload(*h, c->mesh_owned);
+        c->mg = mg_upload(*h, s.stencil, c->mesh_owned);
         f.mg = &c->mg;
       }
     }

@@ -62,6 +62,15 @@ __device__ __forceinline__ void trace(int id) {
 __device__ __forceinline__ void trace(int) {}
 #endif
 
+// The coefficients of node n in a level's stencil, stored coefficient-major
+// ([coefficient][node], `stride` nodes): the lanes of a warp, on consecutive
+// nodes, read consecutive doubles for each coefficient.
+struct CoefRow {
+  const double *st;
+  int stride;
+  __device__ __forceinline__ double operator[](int t) const { return st[(size_t)t * stride]; }
+};
+
 // (A x)[n] with the 7-point stencil of the CG (-x, +x, -y, +y, -z, +z,
 // diagonal).  x is zero on Dirichlet nodes and isolated nodes have no
 // couplings, so no neighbour needs masking.  A coefficient towards a
@@ -72,7 +81,7 @@ __device__ __forceinline__ void trace(int) {}
 __device__ __forceinline__ double apply7(const double *st7, const Grid3 &g, const double *x, int n) {
   int i, j, k;
   node_ijk(n, g, i, j, k);
-  const double *a = st7 + (size_t)n * 7;
+  const CoefRow a{st7 + n, g.px * g.py * g.pz};
   const int sx = g.pz, sy = g.px * g.pz;
   double acc = a[6] * x[n];
   acc += a[0] * x[i > 0 ? n - sx : n];
@@ -115,7 +124,7 @@ template <int G>
 __device__ __forceinline__ double apply27_part(const MgDevLevel &L, const double *x, int n, int g) {
   int i, j, k;
   node_ijk(n, Grid3{L.px, L.py, L.pz}, i, j, k);
-  const double *a = L.st + (size_t)n * 27;
+  const CoefRow a{L.st + n, L.n};
   const int km = k > 0 ? -1 : 0, kp = k + 1 < L.pz ? 1 : 0;
   double acc = 0.0;
 #pragma unroll
@@ -123,11 +132,10 @@ __device__ __forceinline__ double apply27_part(const MgDevLevel &L, const double
     const int row = g + t * G;
     if (row < 9) {
       const int i2 = min(max(i + row / 3 - 1, 0), L.px - 1), j2 = min(max(j + row % 3 - 1, 0), L.py - 1);
-      const double *ar = a + row * 3;
       const int base = (j2 * L.px + i2) * L.pz + k;
-      acc += ar[0] * x[base + km];
-      acc += ar[1] * x[base];
-      acc += ar[2] * x[base + kp];
+      acc += a[row * 3] * x[base + km];
+      acc += a[row * 3 + 1] * x[base];
+      acc += a[row * 3 + 2] * x[base + kp];
     }
   }
   return acc;
@@ -378,7 +386,7 @@ __device__ __forceinline__ void folded_residual(const MgSystem &Y, const Grid3 &
   }
   int i, j, k;
   node_ijk(n, g, i, j, k);
-  const double *a = Y.st7 + (size_t)n * 7;
+  const CoefRow a{Y.mg.L[0].st + n, g.px * g.py * g.pz};
   double acc = a[6] * x[n], fold = 0.0;
   const int nb[6] = {i > 0 ? n - g.pz : -1, i + 1 < g.px ? n + g.pz : -1, j > 0 ? n - g.px * g.pz : -1,
                      j + 1 < g.py ? n + g.px * g.pz : -1, k > 0 ? n - 1 : -1, k + 1 < g.pz ? n + 1 : -1};
@@ -408,7 +416,7 @@ __device__ __forceinline__ void cg_mg_body(const MgGroup<K> &G) {
   const MgSystem &Y = G.s[me];
   const Grid3 g{Y.px, Y.py, Y.pz};
   const int nodes = g.px * g.py * g.pz;
-  const double *st7 = Y.st7;
+  const double *st7 = Y.mg.L[0].st;  // coefficient-major copy of the CG's 7-point stencil
   const uint8_t *dirichlet = Y.dirichlet;
   double *x = Y.x, *r = Y.r, *q = Y.q;
   double *part_pq = Y.part, *part_rz = Y.part + nblk, *part_rr = Y.part + 2 * nblk;
@@ -498,7 +506,7 @@ __device__ __forceinline__ void cg_mg_body(const MgGroup<K> &G) {
         // z and p vanish on Dirichlet nodes, so neighbours need no mask
         int i, j, k;
         node_ijk(n, g, i, j, k);
-        const double *a = st7 + (size_t)n * 7;
+        const CoefRow a{st7 + n, nodes};
         // (pin is not read in the first iteration: it holds no p yet)
         auto P = [&](int m) { return first ? z[m] : z[m] + beta * pin[m]; };
         const double pn = P(n);
@@ -541,7 +549,7 @@ __device__ __forceinline__ void cg_mg_body(const MgGroup<K> &G) {
         // an off-grid neighbour has a zero coefficient and is clamped)
         int i, j, k;
         node_ijk(n, g, i, j, k);
-        const double *a = st7 + (size_t)n * 7;
+        const CoefRow a{st7 + n, nodes};
         double acc = a[6] * f;
         acc += a[0] * first0(i > 0 ? n - sx : n);
         acc += a[1] * first0(i + 1 < g.px ? n + sx : n);
@@ -666,7 +674,7 @@ double *scratch(size_t n, std::vector<void *> &owned) {
 
 }  // namespace
 
-MgDevice mg_upload(const MgHierarchy &h, std::vector<void *> &owned) {
+MgDevice mg_upload(const MgHierarchy &h, const std::vector<double> &stencil7, std::vector<void *> &owned) {
   MgDevice d;
   d.levels = (int)h.levels.size();
   if (d.levels < 1 || d.levels > kMgMaxLevels) throw std::runtime_error("multigrid: bad level count");
@@ -678,7 +686,14 @@ MgDevice mg_upload(const MgHierarchy &h, std::vector<void *> &owned) {
     L.pz = s.pz;
     L.n = s.nodes();
     L.omega = s.omega;
-    L.st = upload(s.st, owned);
+    // stencils coefficient-major: level 0 the CG's 7-point one, else the 27-point Galerkin one
+    const std::vector<double> &src = l == 0 ? stencil7 : s.st;
+    const int w = l == 0 ? 7 : 27;
+    if (src.size() != (size_t)L.n * w) throw std::runtime_error("multigrid: stencil size");
+    std::vector<double> cm(src.size());
+    for (int n = 0; n < L.n; ++n)
+      for (int t = 0; t < w; ++t) cm[(size_t)t * L.n + n] = src[(size_t)n * w + t];
+    L.st = upload(cm, owned);
     L.dinv = upload(s.dinv, owned);
     L.dir = upload(s.dir, owned);
     if (l > 0) {

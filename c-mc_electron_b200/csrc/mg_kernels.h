@@ -13,7 +13,7 @@ namespace mcb200 {
 struct MgDevLevel {
   int px = 0, py = 0, pz = 0, n = 0;
   double omega = 0.0;
-  const double *st = nullptr;    // [n][27] Galerkin stencil (levels >= 1)
+  const double *st = nullptr;    // stencil, coefficient-major: [7][n] the CG's (level 0), [27][n] Galerkin
   const double *dinv = nullptr;  // [n] 1 / diagonal, 0 on Dirichlet rows
   const uint8_t *dir = nullptr;  // [n] decoupled rows
   double *b = nullptr, *xa = nullptr, *xb = nullptr, *r = nullptr;  // right side, iterate (ping-pong), residual
@@ -36,10 +36,12 @@ struct MgDevice {
   MgDevLevel L[kMgMaxLevels];
 };
 
-// Copies the hierarchy to the device.  Level 0's b and xa are left null: the
-// solve binds them to the CG residual and preconditioned residual.  Every
+// Copies the hierarchy to the device, with stencil7 ([nodes][7], the CG's)
+// as level 0's stencil; every stencil goes coefficient-major.  Level 0's b
+// and xa are left null: the solve binds them to the CG residual and
+// preconditioned residual.  Every
 // allocation is appended to `owned` (freed by the caller with cudaFree).
-MgDevice mg_upload(const MgHierarchy &h, std::vector<void *> &owned);
+MgDevice mg_upload(const MgHierarchy &h, const std::vector<double> &stencil7, std::vector<void *> &owned);
 
 // One solve with the V-cycle as preconditioner, in one cooperative launch
 // of `grid` blocks: the set-up (the Dirichlet values into x, the initial
