@@ -266,7 +266,8 @@ def engine_arm(args, rank: int, world: int, device: int):
         "carriers_initial": r32["initial_particles"],
         "e2e": {"value": e2e_ps, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 16 * 6 * 8,
-                "note": "mcb200_run_deck (the main input.txt path) with the contact tallies read back every step; "
+                "note": "mcb200_run_deck (the main input.txt path) with the contact tallies read back every step "
+                        "(pipelined: a step's 768 B are read while the next step runs); "
                         "the deck is read and uploaded once, the self-consistent state stays on the device, so no "
                         "per-step host input exists"},
         "roofline": roof(r32, "fp32"),

@@ -407,12 +407,18 @@ struct Run {
         ok(mcb200_mark(ctx, 3 + 2 * pair), ctx, "mcb200_mark");
         pair_used[pair] = true;
       }
-      if (opt.readback_every_step)
-        ok(mcb200_get_tallies(ctx, nullptr, readback.data(), nullptr, nullptr, nullptr, nullptr), ctx, "tallies");
+      if (opt.readback_every_step) {
+        // this step's contact tallies to the host without waiting; the
+        // previous step's are read while this one runs on the GPU
+        ok(mcb200_tallies_enqueue(ctx, step & 1), ctx, "mcb200_tallies_enqueue");
+        if (step > first) ok(mcb200_tallies_collect(ctx, (step - 1) & 1, readback.data()), ctx, "tallies");
+      }
       if (step % info.stat_step == info.stat_step - 1) output(step, info.stat_step);
       if (opt.verbose && step % std::max(1, info.stat_step / 10) == 0)
         std::printf("step %d: %zu particles\n", step, mcb200_num_particles(ctx));
     }
+    if (opt.readback_every_step && steps > 0)
+      ok(mcb200_tallies_collect(ctx, (first + steps - 1) & 1, readback.data()), ctx, "tallies");
     for (int pair = 0; pair < 3; ++pair) settle(pair);
     if (steps > warm) {
       ok(mcb200_mark(ctx, 1), ctx, "mcb200_mark");

@@ -1212,6 +1212,56 @@ int mcb200_get_tallies(mcb200_ctx *c, uint64_t *counters, double *contact, doubl
   }
 }
 
+int mcb200_tallies_enqueue(mcb200_ctx *c, int slot) {
+  if (!c || slot < 0 || slot >= mcb200_ctx::kTallyRing) return MCB200_ERR_ARG;
+  if (!c->mesh_set) return fail(c, MCB200_ERR_STATE, "mcb200_tallies_enqueue before mcb200_set_mesh");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    constexpr int kRow = kMaxContacts * 6 + 1;
+    if (!c->h_tally) {
+      ck(cudaMallocHost(&c->h_tally, sizeof(long long) * kRow * mcb200_ctx::kTallyRing), "cudaMallocHost");
+      for (cudaEvent_t &e : c->ev_tally) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+    }
+    long long *row = c->h_tally + (size_t)slot * kRow;
+    ck(cudaMemcpyAsync(row, c->y.contact, sizeof(long long) * kMaxContacts * 6, cudaMemcpyDeviceToHost, c->stream),
+       "copy");
+    row[kMaxContacts * 6] = 0;
+    // the store-full flag (dev_counts[2]) beside them
+    ck(cudaMemcpyAsync(row + kMaxContacts * 6, c->dev_counts + 2, sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                       c->stream),
+       "copy");
+    ck(cudaEventRecord(c->ev_tally[slot], c->stream), "event");
+    c->tally_pending[slot] = true;
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
+int mcb200_tallies_collect(mcb200_ctx *c, int slot, double *contact) {
+  if (!c || slot < 0 || slot >= mcb200_ctx::kTallyRing || !contact) return MCB200_ERR_ARG;
+  if (!c->tally_pending[slot]) return fail(c, MCB200_ERR_STATE, "mcb200_tallies_collect: nothing enqueued in the slot");
+  try {
+    ck(cudaSetDevice(c->device), "cudaSetDevice");
+    ck(cudaEventSynchronize(c->ev_tally[slot]), "sync");
+    c->tally_pending[slot] = false;
+    const long long *v = c->h_tally + (size_t)slot * (kMaxContacts * 6 + 1);
+    for (int i = 0; i < kMaxContacts; ++i) {
+      contact[i * 6 + 0] = (double)v[i * 6 + 0];
+      contact[i * 6 + 1] = (double)v[i * 6 + 1] / kChargeScale;
+      contact[i * 6 + 2] = (double)v[i * 6 + 2] / kEnergyScale;
+      contact[i * 6 + 3] = (double)v[i * 6 + 3];
+      contact[i * 6 + 4] = (double)v[i * 6 + 4] / kChargeScale;
+      contact[i * 6 + 5] = (double)v[i * 6 + 5] / kEnergyScale;
+    }
+    if ((unsigned int)v[kMaxContacts * 6])
+      return fail(c, MCB200_ERR_CAPACITY, "particle store full: GENERATE copies beyond the context capacity were dropped");
+    return MCB200_OK;
+  } catch (const std::exception &e) {
+    return fail(c, MCB200_ERR_CUDA, e.what());
+  }
+}
+
 int mcb200_reset_tallies(mcb200_ctx *c) {
   if (!c) return MCB200_ERR_ARG;
   try {

@@ -219,6 +219,12 @@ struct mcb200_ctx {
   int cg_method = kCgAuto, cg_blocks = 0;   // mcb200_set_poisson_solver
   bool device_set = false;
   double *h_scratch = nullptr;  // pinned, 16 doubles
+  // pipelined contact-tally readback (mcb200_tallies_enqueue / _collect):
+  // kTallyRing slots of the contact tallies and the store-full flag, pinned
+  static constexpr int kTallyRing = 4;
+  long long *h_tally = nullptr;              // [kTallyRing][kMaxContacts * 6 + 1]
+  cudaEvent_t ev_tally[kTallyRing] = {};
+  bool tally_pending[kTallyRing] = {};
   // window statistics (mcb200_stat_*)
   StatBuffers sb{};
   StatScales ss{};
@@ -269,6 +275,9 @@ struct mcb200_ctx {
     if (flush_buf) cudaFree(flush_buf);
     if (h_pinned) cudaFreeHost(h_pinned);
     if (h_scratch) cudaFreeHost(h_scratch);
+    if (h_tally) cudaFreeHost(h_tally);
+    for (cudaEvent_t e : ev_tally)
+      if (e) cudaEventDestroy(e);
     if (aux) cudaStreamSynchronize(aux);
     if (ev_aux_in) cudaEventDestroy(ev_aux_in);
     if (ev_stat) cudaEventDestroy(ev_stat);

@@ -244,6 +244,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.mcb200_elapsed_ms.argtypes = [vp, c.c_int, c.c_int, dp]
     lib.mcb200_stat_accumulate.argtypes = [vp]
     lib.mcb200_stat_get.argtypes = [vp, c.c_char_p, dp, c.c_size_t]
+    if hasattr(lib, "mcb200_tallies_enqueue"):  # absent from libraries built before it (MCB200_LIBRARY)
+        lib.mcb200_tallies_enqueue.argtypes = [vp, c.c_int]
+        lib.mcb200_tallies_collect.argtypes = [vp, c.c_int, dp]
     if hasattr(lib, "mcb200_set_induced_current"):  # absent from libraries built before it (MCB200_LIBRARY)
         lib.mcb200_set_induced_current.argtypes = [vp, c.c_int]
         lib.mcb200_get_induced_current.argtypes = [vp, dp, dp]
@@ -583,6 +586,19 @@ class Engine:
         out = {name: int(counters[i]) for i, name in enumerate(COUNTER_NAMES)}
         out.update(contact=contact.reshape(16, 6), lcurrent=lcur, rcurrent=rcur, heat_e=he, heat_h=hh)
         return out
+
+    def tallies_enqueue(self, slot: int):
+        """Copy the contact tallies into ring slot `slot` (0-3) without
+        waiting (mcb200_tallies_enqueue)."""
+        self._check(self._lib.mcb200_tallies_enqueue(self._ctx, int(slot)), "tallies_enqueue")
+
+    def tallies_collect(self, slot: int) -> np.ndarray:
+        """The contact tallies of slot `slot` ([16, 6], as tallies()['contact']),
+        waiting for that copy only."""
+        contact = np.zeros(16 * 6)
+        self._check(self._lib.mcb200_tallies_collect(self._ctx, int(slot), _ptr(contact, ctypes.c_double)),
+                    "tallies_collect")
+        return contact.reshape(16, 6)
 
     def reset_tallies(self):
         self._check(self._lib.mcb200_reset_tallies(self._ctx), "reset_tallies")

@@ -467,6 +467,16 @@ int mcb200_elapsed_ms(mcb200_ctx *ctx, int from, int to, double *ms);
 int mcb200_get_tallies(mcb200_ctx *ctx, uint64_t *counters, double *contact, double *lcurrent, double *rcurrent,
                        double *heat_e, double *heat_h);
 int mcb200_reset_tallies(mcb200_ctx *ctx);
+/* Pipelined readback of the contact tallies (mcb200_get_tallies' contact[16*6]
+ * layout).  mcb200_tallies_enqueue copies them, as the work enqueued so far
+ * leaves them, into slot `slot` (0..3) of a pinned host ring and returns at
+ * once; mcb200_tallies_collect waits for that copy alone (work enqueued after
+ * it keeps running) and converts it.  Collecting step s's tallies after step
+ * s+1 is enqueued keeps the GPU busy while the host reads.  A store that
+ * dropped GENERATE copies is reported by the collect (MCB200_ERR_CAPACITY).
+ * No counterpart in the reference (its tallies are host memory). */
+int mcb200_tallies_enqueue(mcb200_ctx *ctx, int slot);
+int mcb200_tallies_collect(mcb200_ctx *ctx, int slot, double *contact);
 
 /* Particle store in device memory in the engine's FP64 layout (what
  * mcb200_step keeps per particle when the flight runs in FP64): absolute
@@ -628,7 +638,8 @@ typedef struct {
   uint64_t seed;             /* 0: 1 */
   int verbose;
   int warmup_steps;          /* transport steps run before the timed ones (counted in max_steps) */
-  int readback_every_step;   /* read the tallies back to the host after every step */
+  int readback_every_step;   /* read the contact tallies back to the host every step (pipelined: a step's
+                                copy is read once the next step is enqueued; mcb200_tallies_enqueue) */
   size_t flush_l2_bytes;     /* >0: before every timed step write this many bytes (L2 eviction), timed apart */
   int profile_phases;        /* wait for the GPU after every phase so that report->phase_s holds the
                                 device-side time per phase (slows the run; 0: phases are only enqueued

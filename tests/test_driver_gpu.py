@@ -154,6 +154,19 @@ def test_run_deck_contact_bar(precision):
         _check_outputs(data, 39)
 
 
+def test_run_deck_readback_every_step_changes_nothing():
+    """The per-step (pipelined) readback of the contact tallies only reads:
+    the run ends with the same particles, current and outputs."""
+    with tempfile.TemporaryDirectory() as tmp:
+        deck = decks.contact_bar(tmp, vd=0.5, electrons=6000, holes=600)
+        text = open(deck["input"]).read().replace("total_step=100", "total_step=30")
+        open(deck["input"], "w").write(text)
+        reps = [mcb200.run_deck(deck["input"], precision=mcb200.FLIGHT_FP64, table_dir=ORACLE_TABLES,
+                                write_outputs=False, readback_every_step=rb) for rb in (False, True)]
+    for k in ("steps_done", "final_particles", "last_current", "poisson_solves"):
+        assert reps[0][k] == reps[1][k], k
+
+
 @pytest.mark.parametrize("precision", [mcb200.FLIGHT_FP64, mcb200.FLIGHT_FP32])
 def test_run_deck_finfet(precision):
     with tempfile.TemporaryDirectory() as tmp:

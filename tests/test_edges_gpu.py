@@ -9,7 +9,9 @@
 * a store too small for the GENERATE copies of a step: the step keeps the
   store full, drops the excess copies, counts them, and the next call that
   reports a status returns MCB200_ERR_CAPACITY (the reference grows its
-  lists without bound; a fixed device store must report instead).
+  lists without bound; a fixed device store must report instead);
+* the pipelined tally readback returns the tallies as they were when the
+  copy was enqueued, after later steps have run, and refuses an empty slot.
 """
 import tempfile
 
@@ -101,4 +103,26 @@ def test_store_full_of_copies_reports_capacity():
             eng.download()
     assert eng.num_particles() <= n  # the store never holds more than its capacity
     assert eng.tallies()["generated"] > 0
+    eng.close()
+
+
+def test_pipelined_tallies_are_snapshots():
+    with tempfile.TemporaryDirectory() as tmp:
+        orc = _bar_oracle(tmp, 5)
+    orc.density_and_field()
+    eng = device_engine_from_oracle(orc)
+    push_fields(orc, eng)
+    eng.upload(orc.particles())
+    dt = orc.scalar("dt")
+    with pytest.raises(mcb200.EngineError, match="nothing enqueued"):
+        eng.tallies_collect(3)
+    snaps = []
+    for s in range(3):
+        eng.step(s, 5, dt)
+        eng.tallies_enqueue(s)
+        snaps.append(eng.tallies()["contact"].copy())  # the same state, read synchronously
+    eng.step(3, 5, dt)  # more work after the copies
+    for s in range(3):
+        assert np.array_equal(eng.tallies_collect(s), snaps[s]), s
+    assert snaps[2][:, 0].sum() + snaps[2][:, 3].sum() > 0  # the bar generated or caught something
     eng.close()
