@@ -231,9 +231,11 @@ def engine_arm(args, rank: int, world: int, device: int):
         value[p], _ = aggregate_throughput(r["timed_particle_steps"], r["timed_device_ms"], world)
 
     def roof(r, p):
-        launches = max(r["timed_flight_launches"], 1)
-        per_launch = r["timed_particle_steps"] / launches
-        kernel_ms = r["timed_flight_ms"] / launches
+        # the flight's device time is sampled on one timed step in ten (events
+        # on every step would cost the others their overlapped launches); one
+        # main flight per step
+        per_launch = r["timed_particle_steps"] / max(r["timed_steps"], 1)
+        kernel_ms = r["timed_flight_ms"] / max(r["timed_flight_launches"], 1)
         achieved = BYTES_PER_PARTICLE_STEP[p] * per_launch / (kernel_ms * 1e-3) / 1e9
         traffic = None
         try:

@@ -250,6 +250,8 @@ struct mcb200_ctx {
   // CUDA-event timing on the context's stream (mcb200_timing): a ring of
   // per-step event quadruples, read back when a slot is reused or on demand
   bool timing = false;
+  int timing_period = 1;      // one step in timing_period is bracketed by events
+  uint64_t timing_count = 0;  // steps since timing was turned on
   static constexpr int kTimingRing = 64;
   cudaEvent_t ev[kTimingRing][4] = {};
   bool ev_pending[kTimingRing] = {};

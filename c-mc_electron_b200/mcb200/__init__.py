@@ -548,7 +548,9 @@ class Engine:
         self._check(self._lib.mcb200_seed_particles(self._ctx, cell_of.size, _ptr(cell_of, ctypes.c_int32),
                                                     _ptr(charge, ctypes.c_double), carrier_type, seed), "seed")
 
-    def set_timing(self, enable: bool = True):
+    def set_timing(self, enable=True):
+        """Time steps with CUDA events: False off, True every step, an int k
+        one step in k (mcb200_set_timing)."""
         self._check(self._lib.mcb200_set_timing(self._ctx, int(enable)), "set_timing")
 
     def timing(self) -> dict:

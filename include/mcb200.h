@@ -445,9 +445,14 @@ int mcb200_batch_info(const mcb200_batch *batch, int *members, uint64_t *steps_d
                       uint64_t *graph_captures, uint64_t *graph_replays);
 
 /* Device timing of mcb200_step with CUDA events on the context's own stream
- * (enable != 0 resets the accumulators and turns timing on).
- * mcb200_get_timing: out[0..n) = flight-kernel ms, flight-kernel launches,
- * whole-step ms, steps, particles flown, engine kernel launches. */
+ * (enable != 0 resets the accumulators and turns timing on): enable = k >= 1
+ * brackets one step in k (the first, then every k-th) with events; the
+ * others run without them, since an event between two kernels costs the
+ * second its overlap with the tail of the first (on the FinFET, events on
+ * every step cost 3 % of the step).
+ * mcb200_get_timing: out[0..n) = flight-kernel ms and flight-kernel launches
+ * of the timed steps, whole-step ms and steps timed, particles flown (all
+ * steps), engine kernel launches (all steps). */
 int mcb200_set_timing(mcb200_ctx *ctx, int enable);
 int mcb200_get_timing(const mcb200_ctx *ctx, double *out, int n);
 

@@ -11,7 +11,9 @@
   reports a status returns MCB200_ERR_CAPACITY (the reference grows its
   lists without bound; a fixed device store must report instead);
 * the pipelined tally readback returns the tallies as they were when the
-  copy was enqueued, after later steps have run, and refuses an empty slot.
+  copy was enqueued, after later steps have run, and refuses an empty slot;
+* sampled step timing (one step in k bracketed by events) counts the
+  sampled steps' flights and every step's particles.
 """
 import tempfile
 
@@ -125,4 +127,25 @@ def test_pipelined_tallies_are_snapshots():
     for s in range(3):
         assert np.array_equal(eng.tallies_collect(s), snaps[s]), s
     assert snaps[2][:, 0].sum() + snaps[2][:, 3].sum() > 0  # the bar generated or caught something
+    eng.close()
+
+
+def test_sampled_step_timing():
+    with tempfile.TemporaryDirectory() as tmp:
+        orc = _bar_oracle(tmp, 7)
+    orc.density_and_field()
+    eng = device_engine_from_oracle(orc)
+    push_fields(orc, eng)
+    eng.upload(orc.particles())
+    dt = orc.scalar("dt")
+    eng.set_timing(3)
+    for s in range(7):
+        eng.step(s, 7, dt)
+    t = eng.timing()
+    assert t["flight_launches"] == 3 and t["steps"] == 3  # steps 0, 3 and 6
+    assert t["flight_ms"] > 0 and t["step_ms"] >= t["flight_ms"]
+    assert t["particles_flown"] == eng.particle_steps()  # every step's particles
+    eng.set_timing(1)
+    eng.step(7, 7, dt)
+    assert eng.timing()["flight_launches"] == 1
     eng.close()
