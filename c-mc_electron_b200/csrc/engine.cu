@@ -1224,6 +1224,8 @@ int mcb200_tallies_enqueue(mcb200_ctx *c, int slot) {
       ck(cudaMallocHost(&c->h_tally, sizeof(long long) * kRow * mcb200_ctx::kTallyRing), "cudaMallocHost");
       for (cudaEvent_t &e : c->ev_tally) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
     }
+    // a slot enqueued before and not collected: its copy lands first
+    if (c->tally_pending[slot]) ck(cudaEventSynchronize(c->ev_tally[slot]), "sync");
     long long *row = c->h_tally + (size_t)slot * kRow;
     ck(cudaMemcpyAsync(row, c->y.contact, sizeof(long long) * kMaxContacts * 6, cudaMemcpyDeviceToHost, c->stream),
        "copy");

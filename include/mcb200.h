@@ -477,7 +477,8 @@ int mcb200_reset_tallies(mcb200_ctx *ctx);
  * leaves them, into slot `slot` (0..3) of a pinned host ring and returns at
  * once; mcb200_tallies_collect waits for that copy alone (work enqueued after
  * it keeps running) and converts it.  Collecting step s's tallies after step
- * s+1 is enqueued keeps the GPU busy while the host reads.  A store that
+ * s+1 is enqueued keeps the GPU busy while the host reads (enqueueing a slot
+ * that holds an uncollected copy first waits for that copy).  A store that
  * dropped GENERATE copies is reported by the collect (MCB200_ERR_CAPACITY).
  * No counterpart in the reference (its tallies are host memory). */
 int mcb200_tallies_enqueue(mcb200_ctx *ctx, int slot);
